@@ -1,0 +1,344 @@
+"""Benchmark of the superblock Kronecker H*psi (one step = one matvec of one
+sector) on B200, against the reference's CPU batched path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|ladder] [--precision fp64]
+
+Prints one JSON line on rank 0.  Multi-GPU runs (torchrun, one rank per GPU)
+are independent replicas of the sector (the path is single-GPU; see the
+design notes), timed on the device as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Kron-matvec TFLOP/s"
+UNIT = "TFLOP/s"
+FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=500)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="c2", choices=["c2", "ladder"])
+    p.add_argument("--precision", default="fp64", choices=["fp64"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def make_problem(name):
+    from dmrgpp_b200 import superblock as sb
+    if name == "c2":
+        return sb.c2_problem()
+    return sb.ladder_problem()
+
+
+def workload_config(prob, name):
+    return {"workload": prob.name + (" (synthetic Kronecker-matvec microbench)" if name == "c2"
+                                     else ""),
+            "sector_dim": prob.dim, "npatches": prob.npatches, "noperator": prob.noperator,
+            "triples": len(prob.triples()), "f_alg_per_step": prob.flops(),
+            "operator_bytes": prob.operator_bytes()}
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """NVML samples of SM clock and throttle reasons while running."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "hw_power_brake_slowdown": 0x80, "sw_power_cap": 0x4}
+
+    def __init__(self, index=0, period=0.005):
+        self.samples, self.reasons, self.ok = [], set(), False
+        self.period = period
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+        self._stop = threading.Event()
+        self.active = threading.Event()
+
+    def _run(self):
+        while not self._stop.is_set():
+            if self.active.is_set():
+                try:
+                    self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h,
+                                                                       self.nv.NVML_CLOCK_SM))
+                    r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                    for name, bit in self.REASONS.items():
+                        if r & bit:
+                            self.reasons.add(name)
+                except Exception:
+                    pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self.ok:
+            self.t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------- CPU baselines
+def cpu_baseline(prob, f_alg, calls=30):
+    """The reference's own BatchedGemmCpu (compiled from its sources into
+    oracle/_ref) on all host cores; the scalar C restatement if that build
+    is absent.  Median of `calls` matvecs after one warm-up."""
+    import oracle
+    x = np.random.default_rng(7).standard_normal(prob.dim)
+    if oracle.ref_available():
+        rk = oracle.RefKron(prob)
+        rk.apply(x)
+        ts = []
+        for _ in range(calls):
+            t0 = time.perf_counter()
+            rk.apply(x)
+            ts.append(time.perf_counter() - t0)
+        t = statistics.median(ts)
+        cores = int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
+        return {"value": f_alg / t / 1e12, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"median of {calls} full matvecs of the same sector by "
+                          "Dmrg::BatchedGemmCpu::matrixVector (OpenBLAS dgemm)",
+                "s_per_matvec": t}
+    oracle.build()
+    calls = 3
+    oracle.kron_apply(prob, x)
+    ts = []
+    for _ in range(calls):
+        t0 = time.perf_counter()
+        oracle.kron_apply(prob, x)
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+    return {"value": f_alg / t / 1e12, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"median of {calls} full matvecs by the scalar C restatement",
+            "s_per_matvec": t}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    prob = make_problem(args.workload)
+    f_alg = prob.flops()
+    import oracle
+    if not oracle.ref_available():
+        oracle.build()
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference CPU build (oracle/_ref) not present"}))
+        return 0
+    rk = oracle.RefKron(prob)
+    x = np.random.default_rng(7).standard_normal(prob.dim)
+    for _ in range(max(args.warmup, 1)):
+        rk.apply(x)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rk.apply(x)
+    dt = time.perf_counter() - t0
+    value = f_alg * args.steps / dt / 1e12
+    cores = int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded N(0,1) sector blocks)", "impl": "reference",
+            "config": workload_config(prob, args.workload),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"{args.steps} full matvecs by "
+                                       "Dmrg::BatchedGemmCpu::matrixVector on host cores"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------- our arm
+def measured_fp64_peak(torch, dev):
+    """cuBLAS DGEMM 8192^3 (best of 5), the FP64 tensor-pipe denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = None
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        t = s.elapsed_time(e) / 1e3
+        best = t if best is None else min(best, t)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def read_traffic(workload):
+    path = os.path.join(ROOT, "profiles", f"grouped_dgemm_{workload}_traffic.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path)).get("bytes_per_matvec")
+        except Exception:
+            return None
+    return None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    from dmrgpp_b200 import plugin
+    prob = make_problem(args.workload)
+    f_alg = prob.flops()
+    # one dedicated stream for the handle, the flush and the timing events
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    bg = plugin.BatchedGemm.from_problem(prob, stream=stream.cuda_stream, device=local)
+    D = prob.dim
+    x_host = torch.from_numpy(np.random.default_rng(100 + rank).standard_normal(D)).pin_memory()
+    y_host = torch.empty(D, dtype=torch.float64).pin_memory()
+    xd = x_host.to(dev)
+    yd = torch.empty_like(xd)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timing: events around each matvec, L2 flushed
+    # between steps (outside the events)
+    for _ in range(args.warmup):
+        bg.apply_Htarget(xd, yd)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    with clocks:
+        barrier()
+        clocks.active.set()
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            bg.apply_Htarget(xd, yd)
+            ends[i].record(stream)
+        barrier()
+        clocks.active.clear()
+    t_dev = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / 1e3
+    t_dev = max_over_ranks(t_dev)
+    value = world * f_alg * args.steps / t_dev / 1e12
+    per_launch_s = t_dev / args.steps
+
+    # ---- end to end through the C ABI with host buffers (H2D + D2H inside)
+    xh, yh = x_host.numpy(), y_host.numpy()
+    for _ in range(max(3, args.warmup // 4)):
+        bg.apply_Htarget(xh, yh)
+    e_st = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e_en = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    for i in range(args.steps):
+        flush.zero_()
+        e_st[i].record(stream)
+        bg.apply_Htarget(xh, yh)        # synchronous: copies in, 2 kernels, copies out
+        e_en[i].record(stream)
+    barrier()
+    t_e2e = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(e_st, e_en)) / 1e3)
+    e2e = world * f_alg * args.steps / t_e2e / 1e12
+
+    # ---- sanity: the result the timing produced is H*x
+    if rank == 0:
+        import oracle
+        y_chk = oracle.kron_apply(prob, xh)
+        err = float(np.abs(yh - y_chk).max() / np.abs(y_chk).max())
+        if err > 1e-12:
+            raise SystemExit(f"bench result differs from the oracle: rel err {err:.3e}")
+
+    peak = measured_fp64_peak(torch, dev) if rank == 0 else None
+    bg.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    achieved = f_alg / per_launch_s / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded N(0,1) sector blocks)",
+        "config": dict(workload_config(prob, args.workload),
+                       precision=args.precision,
+                       l2="flushed between timed steps (256 MiB write outside the events)",
+                       parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * D,
+                "d2h_bytes_per_step": 8 * D,
+                "ms_per_step": t_e2e / args.steps * 1e3,
+                "path": "dmrgpp_kron_apply(host x, host y) through the C ABI, pinned buffers"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": UNIT,
+                     "frac": achieved / peak if peak else None,
+                     "traffic": read_traffic(args.workload),
+                     "kernel": "grouped_dgemm_kernel (pass 1 + pass 2 launches of one matvec)",
+                     "peak_source": "measured live: cuBLAS DGEMM 8192^3 FP64 (no FP64 entry "
+                                    "in MEASURED_PEAKS.json)"},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(prob, f_alg)
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,82 @@
+"""ctypes binding of the in-tree CUDA library (``include/dmrgpp_kron.h``).
+
+The library is the product path: there is no fallback.  Importing this module
+fails loudly if ``_lib/libdmrgpp_kron.so`` is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libdmrgpp_kron.so")
+
+OK, INVALID_ARG, OOM, CUDA_ERROR, TIMEOUT, NOT_SUPPORTED, NOT_CONVERGED = range(7)
+FP64, SPLIT_BF16, TF32X3 = 0, 1, 2
+STATUS_NAMES = {OK: "OK", INVALID_ARG: "INVALID_ARG", OOM: "OOM", CUDA_ERROR: "CUDA_ERROR",
+                TIMEOUT: "TIMEOUT", NOT_SUPPORTED: "NOT_SUPPORTED",
+                NOT_CONVERGED: "NOT_CONVERGED"}
+
+_sz = ctypes.c_size_t
+_szp = ctypes.POINTER(ctypes.c_size_t)
+_dp = ctypes.POINTER(ctypes.c_double)
+_vpp = ctypes.POINTER(ctypes.c_void_p)
+
+
+class KronDesc(ctypes.Structure):
+    _fields_ = [("noperator", _sz), ("npatches", _sz), ("left_patch_size", _szp),
+                ("right_patch_size", _szp), ("Amatrix", _vpp), ("ld_Amatrix", _szp),
+                ("Bmatrix", _vpp), ("ld_Bmatrix", _szp), ("precision", ctypes.c_int),
+                ("stream", ctypes.c_void_p), ("device", ctypes.c_int)]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("ntriples", _sz), ("dim", _sz), ("f_alg", ctypes.c_double),
+                ("operator_bytes", _sz), ("bx_bytes", _sz), ("pass1_tiles", _sz),
+                ("pass2_tiles", _sz)]
+
+
+# every symbol include/dmrgpp_kron.h declares, with (restype, argtypes)
+SIGNATURES = {
+    "dmrgpp_version": (ctypes.c_char_p, []),
+    "dmrgpp_kron_create": (ctypes.c_int, [ctypes.POINTER(KronDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "dmrgpp_kron_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dmrgpp_kron_apply": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_int]),
+    "dmrgpp_kron_dim": (ctypes.c_int, [ctypes.c_void_p, _szp]),
+    "dmrgpp_kron_flops": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "dmrgpp_kron_plan_info_get": (ctypes.c_int, [ctypes.POINTER(KronDesc),
+                                                 ctypes.POINTER(PlanInfo)]),
+    "dmrgpp_kron_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+}
+
+
+class DmrgppError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"CUDA library {LIB_PATH} is missing; build it with "
+                "`python -m dmrgpp_b200.build` (there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status, handle=None):
+    if status != OK:
+        msg = lib().dmrgpp_kron_last_error(handle)
+        raise DmrgppError(status, msg.decode() if msg else "")

@@ -1,0 +1,94 @@
+// Host-side schedule of one superblock sector's H*x as two grouped GEMM
+// passes over the contributing (i,j,k) triples.
+//
+// Pass 1, one GEMM per input patch j (all output rows stacked, like the
+// reference CPU batched path, BatchedGemmCpu.h:168-246):
+//     BX_j (M_j x l_j) = Bstack_j (M_j x r_j) * X_j (r_j x l_j)
+// where Bstack_j stacks B_k(i,j) for every contributing (i,k), in (i,k)
+// order, and M_j is the sum of those r_i.
+// Pass 2, one GEMM per output patch i (the plugin's second vbatch,
+// apply_Htarget_sparse_not_ready.cpp:330-449):
+//     Y_i (r_i x l_i) = sum over (j,k) of BX_j[rows of (i,k)] * A_k(i,j)^T
+// The transposed A blocks are packed once (AT = A^T, l_j x l_i) so both
+// passes read their B operand K-contiguous.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace dmrgpp {
+
+// One K-segment of an output tile: C += A(M x K) * B(K x N), column-major,
+// offsets relative to the pass's A and B base pointers.
+struct alignas(16) GemmSeg {
+	long long a_off;
+	long long b_off;
+	int       lda;
+	int       ldb;
+	int       K;
+	int       pad;
+};
+
+// One CTA's output tile [m0, m0+BM) x [n0, n0+BN) of an M x N matrix at
+// c_off (leading dimension ldc), summed over segments [seg_begin, seg_end).
+struct alignas(16) GemmTile {
+	long long c_off;
+	int       ldc;
+	int       M;
+	int       N;
+	int       m0;
+	int       n0;
+	int       seg_begin;
+	int       seg_end;
+	int       pad;
+};
+
+struct Triple {
+	int i, j, k;
+};
+
+struct KronPlan {
+	size_t np = 0, nop = 0;
+	std::vector<long long> l, r;        // patch sizes
+	std::vector<long long> xy_start;    // np+1 offsets into X / Y
+	std::vector<Triple>    triples;     // contributing (i,j,k), (i,j,k) order
+	double                 f_alg = 0.0; // sum 2 r_i l_j (r_j + l_i)
+
+	// packed operator buffer (doubles)
+	std::vector<long long> bstack_off; // per input patch j
+	std::vector<long long> M;          // rows of Bstack_j / BX_j
+	std::vector<long long> at_off;     // per triple: packed A^T block
+	long long              op_elems = 0;
+
+	// intermediate BX buffer (doubles)
+	std::vector<long long> bx_off;     // per input patch j
+	std::vector<long long> row_off;    // per triple: first row of (i,k) in BX_j
+	long long              bx_elems = 0;
+
+	// launch lists
+	std::vector<GemmSeg>  seg1, seg2;
+	std::vector<GemmTile> tile1, tile2;
+	int                   bm = 64, bn = 64;
+
+	long long dim() const { return xy_start.empty() ? 0 : xy_start.back(); }
+};
+
+// Validates the plugin tables and builds the plan.  Returns an empty string on
+// success, otherwise the reason.  pack_host (optional) receives the packed
+// operator buffer (op_elems doubles).
+std::string build_kron_plan(size_t               noperator,
+                            size_t               npatches,
+                            const size_t*        lsz,
+                            const size_t*        rsz,
+                            const double* const* A,
+                            const size_t*        ldA,
+                            const double* const* B,
+                            const size_t*        ldB,
+                            int                  bm,
+                            int                  bn,
+                            KronPlan&            plan,
+                            std::vector<double>* pack_host);
+
+} // namespace dmrgpp

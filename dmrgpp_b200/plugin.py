@@ -1,0 +1,149 @@
+"""Host-side mirror of the DMRG++ GPU plugin interface.
+
+``BatchedGemm`` has the constructor arguments and the ``apply_Htarget``
+method of ``template<class T> class BatchedGemm`` in
+``dmrg/GPUPlugin/BatchedGemm.h:11-56`` (instantiated for double,
+``BatchedGemm.cpp:117``).  Every call goes through the C ABI of
+``include/dmrgpp_kron.h`` into the sm_100a kernels; a CUDA-side failure
+raises ``DmrgppError`` instead of the reference's assert/printf.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import FP64, SPLIT_BF16, TF32X3, DmrgppError  # noqa: F401
+
+
+def _size_array(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.uint64))
+
+
+class _DescTables:
+    """Keeps the ctypes descriptor and everything it points to alive."""
+
+    def __init__(self, noperator, npatches, left_patch_size, right_patch_size, Amatrix,
+                 ld_Amatrix, Bmatrix, ld_Bmatrix, precision, stream, device):
+        tot = npatches * npatches * noperator
+        if len(Amatrix) != tot or len(Bmatrix) != tot:
+            raise ValueError(f"tables must have npatches^2*noperator = {tot} entries")
+        self.l = _size_array(left_patch_size)
+        self.r = _size_array(right_patch_size)
+        if len(self.l) != npatches or len(self.r) != npatches:
+            raise ValueError("patch-size arrays must have npatches entries")
+        self.keep = []
+
+        def ptr(m):
+            if m is None:
+                return None
+            if isinstance(m, int):
+                return m
+            a = np.asarray(m)
+            if a.dtype != np.float64:
+                raise TypeError("blocks must be float64")
+            if a.ndim == 2 and not a.flags.f_contiguous:
+                a = np.asfortranarray(a)
+            self.keep.append(a)
+            return a.ctypes.data
+
+        self.A = (ctypes.c_void_p * tot)(*[ptr(m) for m in Amatrix])
+        self.B = (ctypes.c_void_p * tot)(*[ptr(m) for m in Bmatrix])
+        self.ldA = _size_array(ld_Amatrix)
+        self.ldB = _size_array(ld_Bmatrix)
+        if len(self.ldA) != tot or len(self.ldB) != tot:
+            raise ValueError("leading-dimension arrays must match the tables")
+        szp = ctypes.POINTER(ctypes.c_size_t)
+        self.desc = _capi.KronDesc(
+            noperator, npatches, self.l.ctypes.data_as(szp), self.r.ctypes.data_as(szp),
+            ctypes.cast(self.A, ctypes.POINTER(ctypes.c_void_p)), self.ldA.ctypes.data_as(szp),
+            ctypes.cast(self.B, ctypes.POINTER(ctypes.c_void_p)), self.ldB.ctypes.data_as(szp),
+            int(precision), stream, int(device))
+
+
+class BatchedGemm:
+    """y = H x for one superblock sector on the GPU.
+
+    Arguments follow ``BatchedGemm(noperator, npatches, left_patch_size,
+    right_patch_size, Amatrix, ld_Amatrix, Bmatrix, ld_Bmatrix)``: tables of
+    ``npatches*npatches*noperator`` column-major blocks indexed
+    ``outPatch + inPatch*npatches + k*npatches^2`` (None = absent).
+    """
+
+    def __init__(self, noperator: int, npatches: int, left_patch_size: Sequence[int],
+                 right_patch_size: Sequence[int], Amatrix, ld_Amatrix, Bmatrix, ld_Bmatrix,
+                 precision: int = FP64, stream: Optional[int] = None, device: int = -1):
+        L = _capi.lib()
+        t = _DescTables(noperator, npatches, left_patch_size, right_patch_size, Amatrix,
+                        ld_Amatrix, Bmatrix, ld_Bmatrix, precision, stream, device)
+        h = ctypes.c_void_p()
+        _capi.check(L.dmrgpp_kron_create(ctypes.byref(t.desc), ctypes.byref(h)))
+        self._h = h
+        self._lib = L
+        d = ctypes.c_size_t()
+        _capi.check(L.dmrgpp_kron_dim(h, ctypes.byref(d)), h)
+        self.dim = int(d.value)
+        f = ctypes.c_double()
+        _capi.check(L.dmrgpp_kron_flops(h, ctypes.byref(f)), h)
+        self.f_alg = float(f.value)
+
+    @classmethod
+    def from_problem(cls, prob, **kw) -> "BatchedGemm":
+        A, ldA, B, ldB = prob.tables()
+        return cls(prob.noperator, prob.npatches, prob.lsz, prob.rsz, A, ldA, B, ldB, **kw)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def apply_Htarget(self, vin, vout) -> None:
+        """vout = H vin in patch order.  numpy arrays are host buffers (copied
+        in and out); torch CUDA tensors are used in place on the device."""
+        on_dev, px, py = self._pointers(vin, vout)
+        _capi.check(self._lib.dmrgpp_kron_apply(self._h, px, py, on_dev), self._h)
+
+    def __call__(self, x):
+        if hasattr(x, "is_cuda") and x.is_cuda:
+            import torch
+            y = torch.empty_like(x)
+        else:
+            y = np.empty(self.dim)
+        self.apply_Htarget(x, y)
+        return y
+
+    def _pointers(self, vin, vout):
+        if hasattr(vin, "data_ptr"):
+            for v in (vin, vout):
+                if not (v.is_cuda and v.is_contiguous() and str(v.dtype) == "torch.float64"
+                        and v.numel() == self.dim):
+                    raise ValueError("device vectors must be contiguous float64 CUDA tensors "
+                                     f"of length {self.dim}")
+            return 1, vin.data_ptr(), vout.data_ptr()
+        for v in (vin, vout):
+            if not (isinstance(v, np.ndarray) and v.dtype == np.float64 and v.flags.c_contiguous
+                    and v.size == self.dim):
+                raise ValueError(f"host vectors must be contiguous float64 of length {self.dim}")
+        return 0, vin.ctypes.data, vout.ctypes.data
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.dmrgpp_kron_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def plan_info(prob, precision: int = FP64) -> dict:
+    """Host-only planning statistics of a sector (no GPU needed)."""
+    A, ldA, B, ldB = prob.tables()
+    t = _DescTables(prob.noperator, prob.npatches, prob.lsz, prob.rsz, A, ldA, B, ldB,
+                    precision, None, -1)
+    info = _capi.PlanInfo()
+    _capi.check(_capi.lib().dmrgpp_kron_plan_info_get(ctypes.byref(t.desc), ctypes.byref(info)))
+    return {f: getattr(info, f) for f, _ in _capi.PlanInfo._fields_}

@@ -1,0 +1,132 @@
+/*
+ * dmrgpp_kron.h -- C ABI of the B200 superblock Hamiltonian-times-vector
+ * engine for DMRG++.
+ *
+ * It replaces the GPU plugin behind DMRG_BATCHED_GEMM_TYPE=Plugin
+ * (dmrg/GPUPlugin/BatchedGemm.h:11-56, selected by
+ * dmrg/Engine/MatrixVectorKron/BatchedGemmInclude.hh:7-9 and driven by
+ * dmrg/Engine/MatrixVectorKron/BatchedGemmPluginSc.h:40-189).
+ *
+ * One handle holds one symmetry sector of the superblock:
+ *   npatches patches; patch p pairs a left group of l_p states with a right
+ *   group of r_p states.  The sector vector is the concatenation, in patch
+ *   order, of column-major r_p x l_p blocks X_p.
+ *   noperator Kronecker terms; term k has blocks A_k(i,j) (l_i x l_j) and
+ *   B_k(i,j) (r_i x r_j), column-major.
+ *   y = H x  means  Y_i = sum_{j,k} B_k(i,j) X_j A_k(i,j)^T.
+ *
+ * Table convention (identical to the plugin's, BatchedGemmPluginSc.h:95-113):
+ *   Amatrix[i + j*npatches + k*npatches*npatches] points to A_k(i,j) with
+ *   leading dimension ld_Amatrix[same index]; NULL (or an all-zero block)
+ *   means the term does not couple patch j to patch i (setup_nC.cpp:67-121).
+ *   Bmatrix / ld_Bmatrix likewise.  The caller's blocks are read during
+ *   dmrgpp_kron_create only; the handle keeps its own packed device copy.
+ *
+ * Errors: every entry point returns a dmrgpp_status.  The reference reports
+ * errors with assert/printf and C++ exceptions; a C++ caller converts a
+ * non-OK status into its own exception (include/BatchedGemm.h does).
+ * dmrgpp_kron_last_error() gives a human-readable reason.
+ *
+ * Threading: a handle is used by one host thread at a time; distinct handles
+ * may run concurrently on distinct streams.
+ */
+#ifndef DMRGPP_KRON_H
+#define DMRGPP_KRON_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+	DMRGPP_OK            = 0,
+	DMRGPP_INVALID_ARG   = 1,
+	DMRGPP_OOM           = 2,
+	DMRGPP_CUDA_ERROR    = 3,
+	DMRGPP_TIMEOUT       = 4,
+	DMRGPP_NOT_SUPPORTED = 5,
+	DMRGPP_NOT_CONVERGED = 6
+} dmrgpp_status;
+
+/* Arithmetic of the Kronecker GEMMs.  FP64 is the plain method. */
+typedef enum {
+	DMRGPP_FP64       = 0,
+	DMRGPP_SPLIT_BF16 = 1,
+	DMRGPP_TF32X3     = 2
+} dmrgpp_precision;
+
+typedef struct dmrgpp_kron_s* dmrgpp_kron_handle;
+
+/* Mirrors the constructor arguments of BatchedGemm<T>
+ * (dmrg/GPUPlugin/BatchedGemm.h:22-29): noperator, npatches,
+ * left_patch_size, right_patch_size, Amatrix, ld_Amatrix, Bmatrix,
+ * ld_Bmatrix; plus the arithmetic mode, the CUDA stream on which every
+ * operation of the handle is enqueued (cudaStream_t; NULL is the default
+ * stream) and the device (-1: current). */
+typedef struct {
+	size_t               noperator;
+	size_t               npatches;
+	const size_t*        left_patch_size;
+	const size_t*        right_patch_size;
+	const double* const* Amatrix;
+	const size_t*        ld_Amatrix;
+	const double* const* Bmatrix;
+	const size_t*        ld_Bmatrix;
+	int                  precision;
+	void*                stream;
+	int                  device;
+} dmrgpp_kron_desc;
+
+/* Replaces BatchedGemm<T>::BatchedGemm (dmrg/GPUPlugin/BatchedGemm.cpp:8-69,
+ * which calls setup_sparse_batch, setup_sparse_batch.cpp:14-379): validates
+ * the tables, finds the contributing (i,j,k) triples, packs the operators on
+ * the device and builds the launch schedule. */
+int dmrgpp_kron_create(const dmrgpp_kron_desc* desc, dmrgpp_kron_handle* out);
+
+/* Replaces BatchedGemm<T>::~BatchedGemm (dmrg/GPUPlugin/BatchedGemm.cpp:72-79). */
+int dmrgpp_kron_destroy(dmrgpp_kron_handle h);
+
+/* Replaces BatchedGemm<T>::apply_Htarget (dmrg/GPUPlugin/BatchedGemm.cpp:81-115,
+ * apply_Htarget_sparse_not_ready.cpp:14-478): y = H x (overwrite) in patch
+ * order.  on_device = 0: x and y are host pointers (copied in and out on the
+ * handle's stream; the call returns when y is written).  on_device = 1: x
+ * and y are device pointers; the call only enqueues work on the stream. */
+int dmrgpp_kron_apply(dmrgpp_kron_handle h, const double* x, double* y, int on_device);
+
+/* Sector dimension D = sum_p l_p r_p (xy_patch_start, setup_sparse_batch.cpp:98-103). */
+int dmrgpp_kron_dim(dmrgpp_kron_handle h, size_t* dim);
+
+/* Algorithmic flops of one apply: sum over contributing triples of
+ * 2 r_i l_j (r_j + l_i) (dmrg/GPUPlugin/cal_kron_flops.cpp:27-33 method 1,
+ * summed as estimate_work.cpp:114-151). */
+int dmrgpp_kron_flops(dmrgpp_kron_handle h, double* f_alg);
+
+/* Host-only planning statistics (no device work; usable without a GPU):
+ * number of contributing triples, F_alg, packed operator bytes and the
+ * bytes of the intermediate BX buffer. */
+typedef struct {
+	size_t ntriples;
+	size_t dim;
+	double f_alg;
+	size_t operator_bytes;
+	size_t bx_bytes;
+	size_t pass1_tiles;
+	size_t pass2_tiles;
+} dmrgpp_kron_plan_info;
+
+int dmrgpp_kron_plan_info_get(const dmrgpp_kron_desc* desc, dmrgpp_kron_plan_info* info);
+
+/* Last error message of a handle, or of the calling thread's last failed
+ * create when h is NULL.  Never returns NULL. */
+const char* dmrgpp_kron_last_error(dmrgpp_kron_handle h);
+
+/* Library version string. */
+const char* dmrgpp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DMRGPP_KRON_H */

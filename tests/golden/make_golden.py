@@ -1,0 +1,172 @@
+"""Generates the golden fixtures in this folder from the reference tree.
+
+Run here (it needs the reference sources and the oracle harness built from
+them):  python tests/golden/make_golden.py
+
+* batchedgemm_1patch.json -- the known-answer case of the reference unit test
+  dmrg/Engine/tests/test_BatchedGemm.cpp:171-259: one patch, one operator,
+  A 2x2, B 3x3, vin of 6 entries, all drawn from std::mt19937_64(123456789)
+  with std::uniform_real_distribution<double>(-1,1) in the test's order; the
+  expected Y = B X A^T is recomputed by the test's own loops and by the
+  reference BatchedGemmCpu compiled from its sources.
+* kron_data31.npz -- the H*v dump TestSuite/inputs/kron_data31_0_ref.txt
+  (KronLogger format, dmrg/Engine/MatrixVectorKron/KronLogger.hh:112-174,
+  Heisenberg L=8) converted to plugin tables: records with
+  performTranspose=1 hold the stored lower block, so the table receives its
+  transpose (KronConnections.h:141-172).  The file has no output vector; y is
+  computed by the reference BatchedGemmCpu and stored with the fixture.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = "/root/reference"
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from dmrgpp_b200.superblock import KronProblem  # noqa: E402
+
+RNG_PROGRAM = r"""
+#include <cstdio>
+#include <random>
+int main() {
+  std::mt19937_64 rng(123456789);
+  std::uniform_real_distribution<double> dist(-1.0, 1.0);
+  double A[2][2], B[3][3], v[6];
+  for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) A[i][j] = dist(rng);
+  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) B[i][j] = dist(rng);
+  for (int i = 0; i < 6; i++) v[i] = dist(rng);
+  for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) std::printf("%.17g\n", A[i][j]);
+  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) std::printf("%.17g\n", B[i][j]);
+  for (int i = 0; i < 6; i++) std::printf("%.17g\n", v[i]);
+}
+"""
+
+
+def batchedgemm_1patch():
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "rng.cpp")
+        exe = os.path.join(d, "rng")
+        open(src, "w").write(RNG_PROGRAM)
+        subprocess.run(["g++", "-O0", "-o", exe, src], check=True)
+        vals = [float(s) for s in subprocess.run([exe], capture_output=True, text=True,
+                                                  check=True).stdout.split()]
+    A = np.array(vals[0:4]).reshape(2, 2)      # A(i,j) filled row by row
+    B = np.array(vals[4:13]).reshape(3, 3)
+    vin = np.array(vals[13:19])
+    X = vin.reshape(2, 3).T                    # X(row,col) = vin[row + col*3]
+    Y = np.zeros((3, 2))
+    BX = np.zeros((3, 2))
+    for i in range(3):                          # the test's own loops
+        for j in range(2):
+            BX[i, j] = sum(B[i, k] * X[k, j] for k in range(3))
+    for i in range(3):
+        for j in range(2):
+            Y[i, j] = sum(BX[i, k] * A[j, k] for k in range(2))
+    expected = Y.T.reshape(-1)                  # expected[row + col*3]
+    prob = KronProblem(np.array([2]), np.array([3]), 1,
+                       {(0, 0, 0): np.asfortranarray(A)}, {(0, 0, 0): np.asfortranarray(B)},
+                       name="test_BatchedGemm-1patch")
+    yref = oracle.RefKron(prob).apply(vin)
+    assert np.allclose(yref, expected, rtol=1e-14, atol=1e-15)
+    out = {"source": "dmrg/Engine/tests/test_BatchedGemm.cpp:171-259",
+           "A": A.tolist(), "B": B.tolist(), "vin": vin.tolist(),
+           "expected": expected.tolist(), "reference_batched_gemm_cpu": yref.tolist()}
+    with open(os.path.join(HERE, "batchedgemm_1patch.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("batchedgemm_1patch.json: max |ref - expected| =", np.abs(yref - expected).max())
+
+
+def _read_matrix(lines, pos):
+    """KronLogger block: either 'rows cols' + dense rows, or MatrixMarket."""
+    head = lines[pos].strip()
+    if head.startswith("%%MatrixMarket"):
+        rows, cols, nnz = map(int, lines[pos + 1].split())
+        m = np.zeros((rows, cols))
+        for t in range(nnz):
+            i, j, v = lines[pos + 2 + t].split()
+            m[int(i) - 1, int(j) - 1] = float(v)
+        return m, pos + 2 + nnz
+    rows, cols = map(int, head.split())
+    m = np.array([[float(x) for x in lines[pos + 1 + r].split()] for r in range(rows)])
+    return m.reshape(rows, cols), pos + 1 + rows
+
+
+def kron_data31():
+    path = os.path.join(REF, "TestSuite", "inputs", "kron_data31_0_ref.txt")
+    lines = open(path).read().splitlines()
+    pos = lines.index("Vector")
+    n = int(lines[pos + 1])
+    vin = np.array([float(lines[pos + 2 + i]) for i in range(n)])
+    pos = pos + 2 + n
+    recs = []
+    while pos < len(lines):
+        if lines[pos].startswith("# nc, total"):
+            f = [int(x) for x in lines[pos + 1].split()]
+            nc, total, outp, inp, ic, adj, tr, offx, offy = f
+            assert lines[pos + 2].startswith("## A:")
+            A, pos = _read_matrix(lines, pos + 3)
+            assert lines[pos].startswith("## B:")
+            B, pos = _read_matrix(lines, pos + 1)
+            if tr:  # stored lower block, applied transposed
+                A, B = A.T, B.T
+            recs.append((outp, inp, ic, offx, offy, A, B))
+        else:
+            pos += 1
+    nc, npatch = nc, total
+    lsz = np.zeros(npatch, dtype=np.int64)
+    rsz = np.zeros(npatch, dtype=np.int64)
+    offs = {}
+    Ad, Bd = {}, {}
+    for outp, inp, ic, offx, offy, A, B in recs:
+        lsz[outp], rsz[outp] = A.shape[0], B.shape[0]
+        lsz[inp], rsz[inp] = A.shape[1], B.shape[1]
+        offs[outp], offs[inp] = offx, offy
+        Ad[(outp, inp, ic)] = np.asfortranarray(A)
+        Bd[(outp, inp, ic)] = np.asfortranarray(B)
+    prob = KronProblem(lsz, rsz, nc, Ad, Bd, name="kron_data31")
+    assert prob.dim == n
+    assert all(prob.xy_start[p] == offs[p] for p in offs)
+    y = oracle.RefKron(prob).apply(vin)
+    rq = float(vin @ y / (vin @ vin))
+    keys = sorted(Ad)
+    np.savez_compressed(
+        os.path.join(HERE, "kron_data31.npz"), lsz=lsz, rsz=rsz, noperator=nc, vin=vin,
+        y_reference=y, rayleigh=rq, keys=np.array(keys, dtype=np.int64),
+        A=np.concatenate([Ad[k].ravel(order="F") for k in keys]),
+        B=np.concatenate([Bd[k].ravel(order="F") for k in keys]),
+        source=np.array("TestSuite/inputs/kron_data31_0_ref.txt"))
+    print("kron_data31.npz: patches", npatch, "records", len(recs), "dim", n,
+          "Rayleigh quotient", rq)
+
+
+def load_kron_data31():
+    z = np.load(os.path.join(HERE, "kron_data31.npz"))
+    lsz, rsz = z["lsz"], z["rsz"]
+    Ad, Bd = {}, {}
+    pa = pb = 0
+    for i, j, k in z["keys"]:
+        i, j, k = int(i), int(j), int(k)
+        na, nb = lsz[i] * lsz[j], rsz[i] * rsz[j]
+        Ad[(i, j, k)] = np.asfortranarray(z["A"][pa:pa + na].reshape(lsz[j], lsz[i]).T)
+        Bd[(i, j, k)] = np.asfortranarray(z["B"][pb:pb + nb].reshape(rsz[j], rsz[i]).T)
+        pa += na
+        pb += nb
+    prob = KronProblem(lsz, rsz, int(z["noperator"]), Ad, Bd, name="kron_data31")
+    return prob, z["vin"], z["y_reference"], float(z["rayleigh"])
+
+
+if __name__ == "__main__":
+    oracle.build()
+    batchedgemm_1patch()
+    kron_data31()
+    prob, vin, y, rq = load_kron_data31()
+    assert np.allclose(oracle.kron_apply(prob, vin), y, rtol=1e-13, atol=1e-15)

@@ -1,0 +1,100 @@
+"""The C-ABI library without a GPU: it loads, exports every declared symbol,
+plans sectors on the host exactly like the oracle, and rejects bad input
+with status codes (all checks happen before any device work)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from dmrgpp_b200 import superblock as sb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if f.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", f)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            names |= set(re.findall(r"\b(dmrgpp_[a-z0-9_]+)\s*\(", src))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol(cuda_lib):
+    names = declared_symbols()
+    assert "dmrgpp_kron_create" in names and "dmrgpp_kron_apply" in names
+    missing = [n for n in names if not hasattr(cuda_lib, n)]
+    assert not missing, missing
+
+
+def test_version(cuda_lib):
+    from dmrgpp_b200 import _capi
+    assert _capi.lib().dmrgpp_version().startswith(b"dmrgpp-b200")
+
+
+@pytest.mark.parametrize("seed", range(5))
+def test_host_plan_matches_oracle(cuda_lib, oracle_built, seed):
+    from dmrgpp_b200 import plugin
+    prob = sb.random_problem(npatches=3 + seed, noperator=1 + seed % 4, max_size=40, seed=seed,
+                             zero_block_rate=0.25)
+    info = plugin.plan_info(prob)
+    assert info["ntriples"] == len(prob.triples())
+    assert info["dim"] == prob.dim
+    assert info["f_alg"] == oracle_built.kron_flops(prob)
+
+
+def test_plan_of_microbench_sector(cuda_lib):
+    from dmrgpp_b200 import plugin
+    info = plugin.plan_info(sb.c2_problem())
+    assert info["ntriples"] == 103
+    assert info["dim"] == 76406
+    assert info["f_alg"] == 130138856.0
+
+
+def _desc_for(prob):
+    from dmrgpp_b200 import plugin
+    A, ldA, B, ldB = prob.tables()
+    return plugin._DescTables(prob.noperator, prob.npatches, prob.lsz, prob.rsz, A, ldA, B, ldB,
+                              0, None, -1)
+
+
+def test_invalid_inputs_are_rejected_with_status(cuda_lib):
+    from dmrgpp_b200 import _capi, plugin
+    prob = sb.random_problem(3, 2, seed=2)
+    # empty patch (the reference asserts 1 <= size, setup_sparse_batch.cpp:70-71)
+    bad = sb.random_problem(3, 2, seed=2)
+    bad.lsz = bad.lsz.copy()
+    bad.lsz[1] = 0
+    t = _desc_for(bad)
+    h = ctypes.c_void_p()
+    rc = cuda_lib.dmrgpp_kron_create(ctypes.byref(t.desc), ctypes.byref(h))
+    assert rc == _capi.INVALID_ARG and not h.value
+    assert b"empty" in cuda_lib.dmrgpp_kron_last_error(None)
+    # leading dimension smaller than the block
+    t = _desc_for(prob)
+    k = next(i for i in range(len(t.ldA)) if t.A[i])
+    t.ldA[k] = 0
+    rc = cuda_lib.dmrgpp_kron_create(ctypes.byref(t.desc), ctypes.byref(h))
+    assert rc == _capi.INVALID_ARG
+    # unknown precision mode
+    t = _desc_for(prob)
+    t.desc.precision = 7
+    assert cuda_lib.dmrgpp_kron_create(ctypes.byref(t.desc), ctypes.byref(h)) == _capi.INVALID_ARG
+    # null descriptor / output
+    assert cuda_lib.dmrgpp_kron_create(None, ctypes.byref(h)) == _capi.INVALID_ARG
+    assert cuda_lib.dmrgpp_kron_create(ctypes.byref(t.desc), None) == _capi.INVALID_ARG
+    # destroy(NULL) is a no-op
+    assert cuda_lib.dmrgpp_kron_destroy(None) == _capi.OK
+    with pytest.raises(ValueError):
+        plugin.BatchedGemm(1, 2, [1, 1], [1, 1], [None], [0], [None], [0])
+
+
+def test_missing_library_fails_loudly(monkeypatch):
+    from dmrgpp_b200 import _capi
+    monkeypatch.setattr(_capi, "LIB_PATH", "/nonexistent/libdmrgpp_kron.so")
+    monkeypatch.setattr(_capi, "_lib", None)
+    with pytest.raises(ImportError):
+        _capi.lib()

@@ -1,0 +1,118 @@
+"""Parity of the CUDA H*x path (through the C ABI) with the oracle.
+
+FP64 tolerance: max |y - y_oracle| <= 1e-12 * max |y_oracle| (the reference
+unit test's epsilon, test_BatchedGemm.cpp:232-257); runs are also required
+to be bitwise reproducible from call to call.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from dmrgpp_b200 import superblock as sb
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+RTOL = 1e-12
+
+
+def rel_err(y, ref):
+    return float(np.abs(y - ref).max() / max(np.abs(ref).max(), 1e-300))
+
+
+def gpu_apply(prob, x, **kw):
+    from dmrgpp_b200 import plugin
+    bg = plugin.BatchedGemm.from_problem(prob, **kw)
+    try:
+        return bg(np.ascontiguousarray(x))
+    finally:
+        bg.close()
+
+
+def test_known_answer_of_reference_unit_test(cuda_lib, cuda_device):
+    g = json.load(open(os.path.join(GOLDEN, "batchedgemm_1patch.json")))
+    prob = sb.KronProblem(np.array([2]), np.array([3]), 1,
+                          {(0, 0, 0): np.asfortranarray(np.array(g["A"]))},
+                          {(0, 0, 0): np.asfortranarray(np.array(g["B"]))})
+    y = gpu_apply(prob, np.array(g["vin"]))
+    np.testing.assert_allclose(y, g["expected"], rtol=1e-12, atol=0)
+
+
+def test_kron_data31_dump(cuda_lib, cuda_device):
+    from make_golden import load_kron_data31
+    prob, vin, y_ref, rq = load_kron_data31()
+    y = gpu_apply(prob, vin)
+    assert rel_err(y, y_ref) < RTOL
+    assert abs(vin @ y / (vin @ vin) - rq) < 1e-13
+
+
+@pytest.mark.parametrize("seed,np_,K,maxs", [(0, 3, 1, 5), (1, 5, 3, 17), (2, 8, 5, 40),
+                                             (3, 4, 2, 100), (4, 6, 4, 70), (5, 2, 2, 200),
+                                             (6, 10, 6, 33), (7, 1, 1, 1)])
+def test_random_ragged_sectors(cuda_lib, cuda_device, oracle_built, seed, np_, K, maxs):
+    prob = sb.random_problem(npatches=np_, noperator=K, max_size=maxs, seed=seed,
+                             zero_block_rate=0.2)
+    x = np.random.default_rng(seed).standard_normal(prob.dim)
+    y = gpu_apply(prob, x)
+    assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL
+
+
+def test_large_patches_multi_tile(cuda_lib, cuda_device, oracle_built):
+    # patch sizes above the 64x64 tile and odd leading dimensions
+    prob = sb.random_problem(npatches=3, noperator=2, max_size=300, min_size=190, seed=11,
+                             zero_block_rate=0.0)
+    x = np.random.default_rng(2).standard_normal(prob.dim)
+    y = gpu_apply(prob, x)
+    assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL
+
+
+def test_output_patch_without_terms_is_zeroed(cuda_lib, cuda_device, oracle_built):
+    rng = np.random.default_rng(3)
+    l, r = np.array([4, 3, 5]), np.array([2, 6, 3])
+    A = {(0, 0, 0): np.asfortranarray(rng.standard_normal((4, 4))),
+         (2, 0, 0): np.asfortranarray(rng.standard_normal((5, 4)))}
+    B = {(0, 0, 0): np.asfortranarray(rng.standard_normal((2, 2))),
+         (2, 0, 0): np.asfortranarray(rng.standard_normal((3, 2)))}
+    prob = sb.KronProblem(l, r, 1, A, B)
+    from dmrgpp_b200 import plugin
+    bg = plugin.BatchedGemm.from_problem(prob)
+    x = rng.standard_normal(prob.dim)
+    y = np.full(prob.dim, np.nan)
+    bg.apply_Htarget(x, y)
+    assert np.all(y[8:26] == 0.0)
+    assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL
+
+
+def test_microbench_sector_host_and_device_pointers(cuda_lib, cuda_device, oracle_built):
+    import torch
+    from dmrgpp_b200 import plugin
+    prob = sb.c2_problem()
+    x = sb.random_unit_vector(prob.dim, seed=5)
+    y_or = oracle_built.kron_apply(prob, x)
+    bg = plugin.BatchedGemm.from_problem(prob,
+                                         stream=torch.cuda.current_stream().cuda_stream)
+    y_host = bg(x)
+    assert rel_err(y_host, y_or) < RTOL
+    xd = torch.from_numpy(x).to(cuda_device)
+    yd = torch.empty_like(xd)
+    bg.apply_Htarget(xd, yd)
+    torch.cuda.synchronize()
+    y_dev = yd.cpu().numpy()
+    assert np.array_equal(y_dev, y_host)          # same kernels, same order
+    for _ in range(3):                             # bitwise reproducible
+        assert np.array_equal(bg(x), y_host)
+    bg.close()
+
+
+def test_symmetric_operator_gives_symmetric_products(cuda_lib, cuda_device):
+    prob = sb.c2_problem()
+    rng = np.random.default_rng(8)
+    u, v = rng.standard_normal(prob.dim), rng.standard_normal(prob.dim)
+    from dmrgpp_b200 import plugin
+    bg = plugin.BatchedGemm.from_problem(prob)
+    a, b = u @ bg(v), v @ bg(u)
+    assert abs(a - b) < 1e-11 * (abs(a) + abs(b))
+    # linearity
+    np.testing.assert_allclose(bg(2.0 * u - 3.0 * v), 2.0 * bg(u) - 3.0 * bg(v), rtol=1e-12,
+                               atol=1e-10)
