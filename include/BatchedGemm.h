@@ -1,0 +1,107 @@
+// BatchedGemm.h -- C++ drop-in for dmrg/GPUPlugin/BatchedGemm.h:11-56.
+//
+// Same class template name, same constructor arguments
+// (noperator, npatches, left_patch_size, right_patch_size, Amatrix,
+// ld_Amatrix, Bmatrix, ld_Bmatrix) and the same operation y = H x, backed by
+// the B200 library through the C ABI of dmrgpp_kron.h.  Differences, all
+// deliberate:
+//   * apply_Htarget takes raw pointers (const T* vin, T* vout) instead of
+//     Kokkos::View<..., SharedSpace>; the only caller,
+//     BatchedGemmPluginSc::matrixVector (BatchedGemmPluginSc.h:139-161),
+//     passes vin.data() / vout.data() (host memory) instead of building
+//     SharedSpace mirrors.  A device-pointer overload is provided for callers
+//     that keep vectors resident on the GPU.
+//   * errors throw std::runtime_error carrying the library's message instead
+//     of assert/printf (dmrg_malloc_cuda.cpp:24-29).
+//   * only T = double is implemented; the complex<double> instantiation of the
+//     reference (BatchedGemm.cpp:119) is declared but rejected at compile time.
+#ifndef DMRGPP_B200_BATCHEDGEMM_H
+#define DMRGPP_B200_BATCHEDGEMM_H
+
+#include "dmrgpp_kron.h"
+
+#include <cstddef>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+template <typename T> class BatchedGemm {
+
+	static_assert(std::is_same<T, double>::value,
+	              "the B200 library implements BatchedGemm<double> only");
+
+public:
+
+	using SizeType       = std::size_t; // PsimagLite SizeType (AllocatorCpu.h:44)
+	using VectorSizeType = std::vector<SizeType>;
+
+	BatchedGemm(SizeType         noperator,
+	            SizeType         npatches,
+	            VectorSizeType&  left_patch_size,
+	            VectorSizeType&  right_patch_size,
+	            std::vector<T*>& Amatrix,
+	            VectorSizeType&  ld_Amatrix,
+	            std::vector<T*>& Bmatrix,
+	            VectorSizeType&  ld_Bmatrix,
+	            int              precision = DMRGPP_FP64,
+	            void*            stream    = nullptr)
+	    : handle_(nullptr)
+	    , dim_(0)
+	{
+		dmrgpp_kron_desc d {};
+		d.noperator        = noperator;
+		d.npatches         = npatches;
+		d.left_patch_size  = left_patch_size.data();
+		d.right_patch_size = right_patch_size.data();
+		d.Amatrix          = const_cast<const double* const*>(Amatrix.data());
+		d.ld_Amatrix       = ld_Amatrix.data();
+		d.Bmatrix          = const_cast<const double* const*>(Bmatrix.data());
+		d.ld_Bmatrix       = ld_Bmatrix.data();
+		d.precision        = precision;
+		d.stream           = stream;
+		d.device           = -1;
+		check(dmrgpp_kron_create(&d, &handle_), nullptr);
+		check(dmrgpp_kron_dim(handle_, &dim_), handle_);
+	}
+
+	// vout = H vin, both host vectors in patch order (BatchedGemm.cpp:81-115).
+	void apply_Htarget(const T* vin, T* vout) const
+	{
+		check(dmrgpp_kron_apply(handle_, vin, vout, 0), handle_);
+	}
+
+	// vout = H vin with device-resident vectors; enqueued on the handle's stream.
+	void apply_Htarget_device(const T* vin_dev, T* vout_dev) const
+	{
+		check(dmrgpp_kron_apply(handle_, vin_dev, vout_dev, 1), handle_);
+	}
+
+	SizeType size() const { return dim_; }
+
+	double flops() const
+	{
+		double f = 0;
+		check(dmrgpp_kron_flops(handle_, &f), handle_);
+		return f;
+	}
+
+	~BatchedGemm() { dmrgpp_kron_destroy(handle_); }
+
+	BatchedGemm(const BatchedGemm&)            = delete;
+	BatchedGemm& operator=(const BatchedGemm&) = delete;
+
+private:
+
+	static void check(int status, dmrgpp_kron_handle h)
+	{
+		if (status != DMRGPP_OK)
+			throw std::runtime_error(std::string("dmrgpp-b200: ")
+			                         + dmrgpp_kron_last_error(h));
+	}
+
+	dmrgpp_kron_handle handle_;
+	SizeType           dim_;
+};
+
+#endif // DMRGPP_B200_BATCHEDGEMM_H

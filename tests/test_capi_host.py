@@ -98,3 +98,39 @@ def test_missing_library_fails_loudly(monkeypatch):
     monkeypatch.setattr(_capi, "_lib", None)
     with pytest.raises(ImportError):
         _capi.lib()
+
+
+CPP_SHIM_PROGRAM = r"""
+#include "BatchedGemm.h"
+#include <cstdio>
+#include <vector>
+int main() {
+  std::vector<std::size_t> l = {2, 0}, r = {3, 1}, ld(8, 0);   // patch 1 has an empty left group
+  std::vector<double*> A(8, nullptr), B(8, nullptr);
+  try {
+    BatchedGemm<double> bg(2, 2, l, r, A, ld, B, ld);
+    std::printf("constructed\n");
+    return 1;
+  } catch (const std::runtime_error& e) {
+    std::printf("caught: %s\n", e.what());
+    return 0;
+  }
+}
+"""
+
+
+def test_cpp_dropin_header_compiles_links_and_throws(cuda_lib, tmp_path):
+    """include/BatchedGemm.h (the C++ drop-in for dmrg/GPUPlugin/BatchedGemm.h)
+    builds against the library and turns a status code into an exception."""
+    import subprocess
+    from dmrgpp_b200 import _capi
+    src = tmp_path / "shim.cpp"
+    exe = tmp_path / "shim"
+    src.write_text(CPP_SHIM_PROGRAM)
+    libdir = os.path.dirname(_capi.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src),
+                    "-L" + libdir, "-ldmrgpp_kron", "-Wl,-rpath," + libdir, "-o", str(exe)],
+                   check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "caught: dmrgpp-b200:" in r.stdout and "empty" in r.stdout
