@@ -48,7 +48,11 @@ SIGNATURES = {
     "dmrgpp_kron_plan_info_get": (ctypes.c_int, [ctypes.POINTER(KronDesc),
                                                  ctypes.POINTER(PlanInfo)]),
     "dmrgpp_kron_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "dmrgpp_kron_apply_noalloc": (ctypes.c_int, [ctypes.POINTER(KronDesc), ctypes.c_void_p,
+                                                 ctypes.c_void_p]),
+    "dmrgpp_kron_noalloc_last_error": (ctypes.c_char_p, []),
 }
+NOALLOC_SCRATCH_BYTES = 16 << 20
 
 
 class DmrgppError(RuntimeError):

@@ -118,6 +118,27 @@ typedef struct {
 
 int dmrgpp_kron_plan_info_get(const dmrgpp_kron_desc* desc, dmrgpp_kron_plan_info* info);
 
+/* No counterpart in the reference.  One-shot y = H x that performs no device
+ * memory allocation, for callers that cannot call cudaMalloc (for example
+ * code running while another component owns all device memory through its
+ * own allocator, or a runtime that forbids allocation after start-up).
+ * desc is read as by dmrgpp_kron_create (host tables, FP64 only); x and y
+ * are device pointers of the sector dimension; the work is enqueued on
+ * desc->stream and the call returns without waiting for it.
+ * All scratch (packed operators, the pass-1 buffer, launch lists) lives in
+ * one file-scope device array of DMRGPP_NOALLOC_SCRATCH_BYTES that every GPU
+ * which loads the library holds until the process exits; a sector needing
+ * more is rejected with DMRGPP_INVALID_ARG.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) and sets kernel
+ * attributes, so make that first call before any stream capture.  Every call
+ * shares the one array: calls that may overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller.  Each call
+ * rewrites every scratch byte it reads, so no clearing is needed between
+ * calls.  Errors: dmrgpp_kron_noalloc_last_error(). */
+#define DMRGPP_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+int dmrgpp_kron_apply_noalloc(const dmrgpp_kron_desc* desc, const double* x, double* y);
+const char* dmrgpp_kron_noalloc_last_error(void);
+
 /* Last error message of a handle, or of the calling thread's last failed
  * create when h is NULL.  Never returns NULL. */
 const char* dmrgpp_kron_last_error(dmrgpp_kron_handle h);
