@@ -44,6 +44,8 @@ SIGNATURES = {
     "dmrgpp_kron_apply": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_int]),
     "dmrgpp_kron_dim": (ctypes.c_int, [ctypes.c_void_p, _szp]),
+    "dmrgpp_kron_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "dmrgpp_kron_test_stall_dependency": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dmrgpp_kron_flops": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "dmrgpp_kron_plan_info_get": (ctypes.c_int, [ctypes.POINTER(KronDesc),
                                                  ctypes.POINTER(PlanInfo)]),
@@ -53,6 +55,25 @@ SIGNATURES = {
     "dmrgpp_kron_noalloc_last_error": (ctypes.c_char_p, []),
 }
 NOALLOC_SCRATCH_BYTES = 16 << 20
+
+
+class LanczosParams(ctypes.Structure):
+    _fields_ = [("steps", _sz), ("min_steps", _sz), ("eigs_for_stop", _sz),
+                ("tolerance", ctypes.c_double), ("reortho", ctypes.c_int),
+                ("check_every", ctypes.c_int)]
+
+
+SIGNATURES.update({
+    "dmrgpp_lanczos_params_init": (None, [ctypes.POINTER(LanczosParams)]),
+    "dmrgpp_lanczos_lowest": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LanczosParams),
+                                             ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_void_p,
+                                             _szp]),
+    "dmrgpp_tridiag_eigen": (ctypes.c_int, [_sz, _dp, _dp, _dp, _dp]),
+    "dmrgpp_gather": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _sz,
+                                     ctypes.c_void_p]),
+    "dmrgpp_scatter": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _sz,
+                                      ctypes.c_void_p]),
+})
 
 
 class DmrgppError(RuntimeError):

@@ -1,7 +1,9 @@
 // C ABI of the Kronecker H*x engine (include/dmrgpp_kron.h).
 #include "dmrgpp_kron.h"
 #include "kron_gemm.cuh"
+#include "kron_persistent.cuh"
 #include "kron_plan.h"
+#include "handle.h"
 
 #include <cuda_runtime.h>
 
@@ -12,22 +14,7 @@
 
 #define DMRGPP_VERSION_STRING "dmrgpp-b200 0.1"
 
-struct dmrgpp_kron_s {
-	int                 device     = 0;
-	cudaStream_t        stream     = nullptr;
-	int                 precision  = DMRGPP_FP64;
-	dmrgpp::KronPlan    plan;
-	double*             d_ops   = nullptr; // packed Bstack_j and A^T blocks
-	double*             d_bx    = nullptr; // pass-1 output (scratch)
-	double*             d_x     = nullptr; // staging for host-pointer applies
-	double*             d_y     = nullptr;
-	dmrgpp::GemmSeg*    d_seg1  = nullptr;
-	dmrgpp::GemmSeg*    d_seg2  = nullptr;
-	dmrgpp::GemmTile*   d_tile1 = nullptr;
-	dmrgpp::GemmTile*   d_tile2 = nullptr;
-	void*               d_lists = nullptr; // one allocation behind the four lists
-	std::string         err;
-};
+
 
 namespace {
 
@@ -73,11 +60,19 @@ void release(dmrgpp_kron_handle h)
 {
 	if (!h)
 		return;
+	dmrgpp::release_lanczos(h);
 	cudaFree(h->d_ops);
 	cudaFree(h->d_bx);
 	cudaFree(h->d_x);
 	cudaFree(h->d_y);
 	cudaFree(h->d_lists);
+	cudaFree(h->d_ctr);
+	cudaFree(h->d_part);
+	if (h->err_host)
+		cudaFreeHost(h->err_host);
+	h->err_host = h->err_dev = nullptr;
+	h->d_ctr                 = nullptr;
+	h->d_part                = nullptr;
 	h->d_ops = h->d_bx = h->d_x = h->d_y = nullptr;
 	h->d_lists                           = nullptr;
 	h->stream                            = nullptr;
@@ -110,7 +105,57 @@ int check_desc(const dmrgpp_kron_desc* d)
 	return DMRGPP_OK;
 }
 
+// After the stream has drained: a wait inside the persistent kernel that
+// gave up leaves its counters dirty; report it and restore a clean state.
+int check_error_word(dmrgpp_kron_handle h)
+{
+	if (!h->err_host || *reinterpret_cast<volatile int*>(h->err_host) == 0)
+		return DMRGPP_OK;
+	*h->err_host      = 0;
+	const size_t nctr = 3 + h->plan.np + size_t(h->plan.n_split_tiles);
+	cudaMemsetAsync(h->d_ctr, 0, nctr * sizeof(unsigned), h->stream);
+	cudaStreamSynchronize(h->stream);
+	return fail(h, DMRGPP_TIMEOUT, "a dependency wait in the H*x kernel gave up; result invalid");
+}
+
 } // namespace
+
+namespace dmrgpp {
+
+int handle_fail(dmrgpp_kron_handle h, int status, const std::string& msg)
+{
+	return fail(h, status, msg);
+}
+
+int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
+{
+	const auto& P = h->plan;
+	cudaError_t e;
+	dmrgpp::PersistentArgs pa {};
+	pa.ops           = h->d_ops;
+	pa.x             = X;
+	pa.bx            = h->d_bx;
+	pa.y             = Y;
+	pa.partial       = h->d_part;
+	pa.seg1          = h->d_seg1;
+	pa.pseg2         = h->d_pseg2;
+	pa.items         = h->d_items;
+	pa.n1_of_j       = h->d_n1;
+	pa.work_counter  = h->d_ctr;
+	pa.done          = h->d_ctr + 3;
+	pa.arrive        = h->d_ctr + 3 + P.np;
+	pa.test_extra_wait = h->test_stall;
+	pa.error         = h->err_dev;
+	pa.n_items       = int(P.items.size());
+	pa.np            = int(P.np);
+	pa.n_split_tiles = P.n_split_tiles;
+	if ((e = dmrgpp::launch_persistent(pa, h->tile, h->grid, h->stream)))
+		return cuda_fail(h, e, "H*x launch");
+	return DMRGPP_OK;
+
+}
+
+} // namespace dmrgpp
 
 extern "C" {
 
@@ -222,26 +267,55 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 	if ((e = cudaMalloc(&h->d_y, dim * sizeof(double))))
 		return bail(e, "cudaMalloc(y)");
 
-	const size_t nseg  = P.seg1.size() + P.seg2.size();
-	const size_t ntile = P.tile1.size() + P.tile2.size();
-	const size_t bytes = nseg * sizeof(dmrgpp::GemmSeg) + ntile * sizeof(dmrgpp::GemmTile);
-	if ((e = cudaMalloc(&h->d_lists, bytes ? bytes : 16)))
-		return bail(e, "cudaMalloc(lists)");
-	std::vector<unsigned char> lists(bytes);
-	unsigned char*             p = lists.data();
-	auto put = [&](const void* src, size_t n) {
+	int bk = 16;
+	if ((e = dmrgpp::persistent_config(bm, &h->grid, &bk)))
+		return bail(e, "persistent kernel attributes");
+	h->tile = bm;
+	dmrgpp::build_persistent_schedule(h->plan, bk, h->grid);
+
+	// every list in one allocation, each chunk on a 16-byte boundary
+	std::vector<unsigned char> lists;
+	std::vector<size_t>        offs;
+	auto add = [&](const void* src, size_t n) {
+		offs.push_back(lists.size());
+		lists.resize(lists.size() + ((n + 15) / 16) * 16);
 		if (n)
-			std::memcpy(p, src, n);
-		void* dev = static_cast<unsigned char*>(h->d_lists) + (p - lists.data());
-		p += n;
-		return dev;
+			std::memcpy(lists.data() + offs.back(), src, n);
 	};
-	h->d_seg1  = (dmrgpp::GemmSeg*)put(P.seg1.data(), P.seg1.size() * sizeof(dmrgpp::GemmSeg));
-	h->d_seg2  = (dmrgpp::GemmSeg*)put(P.seg2.data(), P.seg2.size() * sizeof(dmrgpp::GemmSeg));
-	h->d_tile1 = (dmrgpp::GemmTile*)put(P.tile1.data(), P.tile1.size() * sizeof(dmrgpp::GemmTile));
-	h->d_tile2 = (dmrgpp::GemmTile*)put(P.tile2.data(), P.tile2.size() * sizeof(dmrgpp::GemmTile));
-	if (bytes && (e = cudaMemcpy(h->d_lists, lists.data(), bytes, cudaMemcpyHostToDevice)))
+	add(P.seg1.data(), P.seg1.size() * sizeof(dmrgpp::GemmSeg));
+	add(P.seg2.data(), P.seg2.size() * sizeof(dmrgpp::GemmSeg));
+	add(P.tile1.data(), P.tile1.size() * sizeof(dmrgpp::GemmTile));
+	add(P.tile2.data(), P.tile2.size() * sizeof(dmrgpp::GemmTile));
+	add(P.items.data(), P.items.size() * sizeof(dmrgpp::KronItem));
+	add(P.pseg2.data(), P.pseg2.size() * sizeof(dmrgpp::GemmSeg));
+	add(P.n1_of_j.data(), P.n1_of_j.size() * sizeof(int));
+	if ((e = cudaMalloc(&h->d_lists, lists.empty() ? 16 : lists.size())))
+		return bail(e, "cudaMalloc(lists)");
+	auto at = [&](int i) { return static_cast<unsigned char*>(h->d_lists) + offs[i]; };
+	h->d_seg1  = reinterpret_cast<dmrgpp::GemmSeg*>(at(0));
+	h->d_seg2  = reinterpret_cast<dmrgpp::GemmSeg*>(at(1));
+	h->d_tile1 = reinterpret_cast<dmrgpp::GemmTile*>(at(2));
+	h->d_tile2 = reinterpret_cast<dmrgpp::GemmTile*>(at(3));
+	h->d_items = reinterpret_cast<dmrgpp::KronItem*>(at(4));
+	h->d_pseg2 = reinterpret_cast<dmrgpp::GemmSeg*>(at(5));
+	h->d_n1    = reinterpret_cast<int*>(at(6));
+	if (!lists.empty()
+	    && (e = cudaMemcpy(h->d_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
 		return bail(e, "upload lists");
+
+	const size_t nctr = 3 + P.np + size_t(P.n_split_tiles);
+	if ((e = cudaMalloc(&h->d_ctr, nctr * sizeof(unsigned))))
+		return bail(e, "cudaMalloc(counters)");
+	if ((e = cudaMemset(h->d_ctr, 0, nctr * sizeof(unsigned))))
+		return bail(e, "clear counters");
+	const size_t part_elems = size_t(P.partial_slots) * size_t(dmrgpp::persistent_tile_elems(bm));
+	if ((e = cudaMalloc(&h->d_part, (part_elems ? part_elems : 1) * sizeof(double))))
+		return bail(e, "cudaMalloc(partials)");
+	if ((e = cudaHostAlloc(reinterpret_cast<void**>(&h->err_host), sizeof(int), cudaHostAllocMapped)))
+		return bail(e, "cudaHostAlloc(error word)");
+	*h->err_host = 0;
+	if ((e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&h->err_dev), h->err_host, 0)))
+		return bail(e, "error word mapping");
 	if (!pack.empty()
 	    && (e = cudaMemcpy(h->d_ops, pack.data(), pack.size() * sizeof(double), cudaMemcpyHostToDevice)))
 		return bail(e, "upload operators");
@@ -294,20 +368,36 @@ int dmrgpp_kron_apply(dmrgpp_kron_handle h, const double* x, double* y, int on_d
 	    && (e = cudaMemcpyAsync(h->d_x, x, dim * sizeof(double), cudaMemcpyHostToDevice, h->stream)))
 		return cuda_fail(h, e, "copy x to device");
 
-	dmrgpp::GemmArgs a1 { h->d_ops, X, h->d_bx, h->d_seg1, h->d_tile1, int(P.tile1.size()) };
-	if ((e = dmrgpp::launch_grouped_dgemm(a1, P.bm, P.bn, h->stream)))
-		return cuda_fail(h, e, "pass 1 launch");
-	dmrgpp::GemmArgs a2 { h->d_bx, h->d_ops, Y, h->d_seg2, h->d_tile2, int(P.tile2.size()) };
-	if ((e = dmrgpp::launch_grouped_dgemm(a2, P.bm, P.bn, h->stream)))
-		return cuda_fail(h, e, "pass 2 launch");
+	if (int rc = dmrgpp::kron_apply_device(h, X, Y))
+		return rc;
 
 	if (!on_device) {
 		if ((e = cudaMemcpyAsync(y, h->d_y, dim * sizeof(double), cudaMemcpyDeviceToHost, h->stream)))
 			return cuda_fail(h, e, "copy y to host");
 		if ((e = cudaStreamSynchronize(h->stream)))
 			return cuda_fail(h, e, "apply");
+		return check_error_word(h);
 	}
 	return DMRGPP_OK;
+}
+
+int dmrgpp_kron_test_stall_dependency(dmrgpp_kron_handle h, int on)
+{
+	if (!h)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "null handle");
+	h->test_stall = on ? 1 : 0;
+	return DMRGPP_OK;
+}
+
+int dmrgpp_kron_synchronize(dmrgpp_kron_handle h)
+{
+	if (!h)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "null handle");
+	DeviceGuard g(h->device);
+	cudaError_t e = cudaStreamSynchronize(h->stream);
+	if (e != cudaSuccess)
+		return cuda_fail(h, e, "synchronize");
+	return check_error_word(h);
 }
 
 } // extern "C"

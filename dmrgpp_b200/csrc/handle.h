@@ -1,0 +1,56 @@
+// Internal definition of a sector handle (opaque in include/dmrgpp_kron.h),
+// shared by the C-ABI translation units.
+#pragma once
+
+#include "dmrgpp_kron.h"
+#include "kron_plan.h"
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+namespace dmrgpp {
+struct LanczosWork; // device buffers of the eigensolvers, created on first use
+}
+
+struct dmrgpp_kron_s {
+	int                 device     = 0;
+	cudaStream_t        stream     = nullptr;
+	int                 precision  = DMRGPP_FP64;
+	dmrgpp::KronPlan    plan;
+	double*             d_ops   = nullptr; // packed Bstack_j and A^T blocks
+	double*             d_bx    = nullptr; // pass-1 output (scratch)
+	double*             d_x     = nullptr; // staging for host-pointer applies
+	double*             d_y     = nullptr;
+	dmrgpp::GemmSeg*    d_seg1  = nullptr;
+	dmrgpp::GemmSeg*    d_seg2  = nullptr;
+	dmrgpp::GemmTile*   d_tile1 = nullptr;
+	dmrgpp::GemmTile*   d_tile2 = nullptr;
+	void*               d_lists = nullptr; // one allocation behind every list
+	// persistent single-launch form
+	int                 tile    = 32;
+	int                 grid    = 0;
+	dmrgpp::KronItem*   d_items = nullptr;
+	dmrgpp::GemmSeg*    d_pseg2 = nullptr;
+	int*                d_n1    = nullptr;
+	unsigned*           d_ctr   = nullptr; // work counters, done[np], arrive[split tiles]
+	double*             d_part  = nullptr; // split-K partial tiles
+	int*                err_host = nullptr; // mapped pinned word written by the kernel
+	int*                err_dev  = nullptr;
+	int                 test_stall = 0;     // dmrgpp_kron_test_stall_dependency
+	dmrgpp::LanczosWork* lanczos = nullptr;
+	std::string         err;
+};
+
+namespace dmrgpp {
+
+// Enqueues y = H x on h->stream (device pointers); no synchronisation.
+int kron_apply_device(dmrgpp_kron_handle h, const double* x, double* y);
+
+// Records msg as the handle's last error and returns status.
+int handle_fail(dmrgpp_kron_handle h, int status, const std::string& msg);
+
+// Releases the eigensolver buffers of a handle (lanczos.cu).
+void release_lanczos(dmrgpp_kron_handle h);
+
+} // namespace dmrgpp

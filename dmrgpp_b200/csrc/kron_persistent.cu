@@ -1,0 +1,234 @@
+// One persistent launch for a whole sector H*x: pass-1 tiles and (K-split)
+// pass-2 tiles are pulled from one work queue by a fixed grid of CTAs.
+//
+// Ordering: every pass-1 item precedes every pass-2 item in the queue.  A
+// pass-2 item first waits until all pass-1 tiles of the input patches its
+// K-slice reads are complete (per-patch completion counters).  Pass-1 items
+// never wait, and an item is only dequeued after all earlier items were
+// dequeued by running CTAs, so the waits always end; they are still bounded
+// in time (kWaitLimitNs); a wait that gives up raises the abort word, which
+// ends every other wait, and the host-visible error word, and the launch
+// runs to its end with an invalid result instead of hanging.
+//
+// Split-K: the parts of one output tile write partial tiles to their own
+// slots; the part that arrives last sums the slots in slot order and stores
+// the tile, so the result does not depend on arrival order (bitwise
+// reproducible).
+//
+// Counters are returned to zero by the last CTA to leave, so consecutive
+// launches (and CUDA-graph replays) need no memset.
+#include "kron_persistent.cuh"
+#include "tile_dmma.cuh"
+
+namespace dmrgpp {
+namespace {
+
+// Upper bound of one dependency wait (nanoseconds of %globaltimer).  A legal
+// wait lasts at most one pass-1 tile (microseconds to a millisecond).
+constexpr unsigned long long kWaitLimitNs = 200ull * 1000ull * 1000ull;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+	return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
+{
+	unsigned v;
+	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+
+template <class C>
+__device__ __forceinline__ void
+store_tile(const tile::Acc<C>& acc, double* Cp, int ldc, int m0, int n0, int M, int N)
+{
+#pragma unroll
+	for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+		for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+			for (int h = 0; h < 2; ++h) {
+				const int row = m0 + tile::acc_row<C>(mi);
+				const int col = n0 + tile::acc_col<C>(ni, h);
+				if (row < M && col < N)
+					Cp[(long long)col * ldc + row] = acc.v[mi][ni][h];
+			}
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::THREADS) kron_persistent_kernel(PersistentArgs a)
+{
+	extern __shared__ __align__(16) double smem[];
+	__shared__ int s_item;
+	__shared__ int s_last;
+	const int      tid = threadIdx.x;
+	tile::Acc<C>   acc;
+
+	for (;;) {
+		if (tid == 0)
+			s_item = int(atomicAdd(&a.work_counter[0], 1u));
+		__syncthreads();
+		const int it = s_item;
+		__syncthreads();
+		if (it >= a.n_items)
+			break;
+		const KronItem w = a.items[it];
+
+		if (w.kind == 0) {
+			tile::mma_tile<C>(acc, smem, a.ops, a.x, a.seg1, w.seg_begin, w.seg_end, w.m0, w.n0,
+			                  w.M, w.N);
+			store_tile<C>(acc, a.bx + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
+			__syncthreads();
+			if (tid == 0) {
+				__threadfence();
+				atomicAdd(&a.done[w.producer], 1u);
+			}
+			continue;
+		}
+
+		if (tid == 0) {
+			int last_dep = -1;
+			for (int s = w.seg_begin; s < w.seg_end; ++s) {
+				const int j = a.pseg2[s].dep;
+				if (j == last_dep)
+					continue;
+				last_dep              = j;
+				const unsigned target = unsigned(a.n1_of_j[j] + (j == 0 ? a.test_extra_wait : 0));
+				const unsigned long long t0 = globaltimer_ns();
+				while (ld_acquire(&a.done[j]) < target) {
+					if (ld_acquire(&a.work_counter[2]) != 0u)
+						break; // another wait already gave up
+					if (globaltimer_ns() - t0 > kWaitLimitNs) {
+						atomicExch(&a.work_counter[2], 1u);
+						*reinterpret_cast<volatile int*>(a.error) = 1;
+						__threadfence_system();
+						break;
+					}
+					__nanosleep(128);
+				}
+			}
+		}
+		__syncthreads();
+		tile::mma_tile<C>(acc, smem, a.bx, a.ops, a.pseg2, w.seg_begin, w.seg_end, w.m0, w.n0,
+		                  w.M, w.N);
+		if (w.kind == 1) {
+			store_tile<C>(acc, a.y + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
+			continue;
+		}
+
+		// split part: partial tile to its slot, the last part reduces
+		constexpr int TE = C::BM * C::BN;
+		double*       part = a.partial + (long long)(w.slot + w.part) * TE;
+#pragma unroll
+		for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+			for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+				for (int h = 0; h < 2; ++h)
+					part[tile::acc_col<C>(ni, h) * C::BM + tile::acc_row<C>(mi)] = acc.v[mi][ni][h];
+		__syncthreads();
+		if (tid == 0) {
+			__threadfence();
+			const unsigned old = atomicAdd(&a.arrive[w.tile], 1u);
+			s_last             = (old == unsigned(w.nsplit - 1));
+			if (s_last)
+				__threadfence();
+		}
+		__syncthreads();
+		if (!s_last)
+			continue;
+		const double* slots = a.partial + (long long)w.slot * TE;
+		double*       Cp    = a.y + w.c_off;
+#pragma unroll
+		for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+			for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+				for (int h = 0; h < 2; ++h) {
+					const int r   = tile::acc_row<C>(mi);
+					const int c   = tile::acc_col<C>(ni, h);
+					const int e   = c * C::BM + r;
+					double    sum = __ldcg(slots + e);
+					for (int p = 1; p < w.nsplit; ++p)
+						sum += __ldcg(slots + (long long)p * TE + e);
+					const int row = w.m0 + r, col = w.n0 + c;
+					if (row < w.M && col < w.N)
+						Cp[(long long)col * w.ldc + row] = sum;
+				}
+	}
+
+	// the last CTA out returns every counter to zero for the next launch
+	if (tid == 0) {
+		__threadfence();
+		const unsigned old = atomicAdd(&a.work_counter[1], 1u);
+		if (old == gridDim.x - 1) {
+			for (int j = 0; j < a.np; ++j)
+				a.done[j] = 0u;
+			for (int t = 0; t < a.n_split_tiles; ++t)
+				a.arrive[t] = 0u;
+			a.work_counter[0] = 0u;
+			a.work_counter[2] = 0u;
+			__threadfence();
+			a.work_counter[1] = 0u;
+		}
+	}
+}
+
+using PCfg32 = tile::Cfg<32, 32, 16, 16, 16, 4>;
+using PCfg64 = tile::Cfg<64, 64, 16, 32, 32, 3>;
+
+template <class C> cudaError_t init_one(int* blocks_per_sm)
+{
+	cudaError_t e = cudaFuncSetAttribute(kron_persistent_kernel<C>,
+	                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::SMEM));
+	if (e != cudaSuccess)
+		return e;
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kron_persistent_kernel<C>,
+	                                                     C::THREADS, C::SMEM);
+}
+
+} // namespace
+
+cudaError_t persistent_config(int tile, int* grid, int* bk)
+{
+	int         dev = 0, sms = 0, per_sm = 0;
+	cudaError_t e = cudaGetDevice(&dev);
+	if (e == cudaSuccess)
+		e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	if (e != cudaSuccess)
+		return e;
+	if (tile == 32) {
+		e   = init_one<PCfg32>(&per_sm);
+		*bk = PCfg32::BK;
+	} else if (tile == 64) {
+		e   = init_one<PCfg64>(&per_sm);
+		*bk = PCfg64::BK;
+	} else {
+		return cudaErrorInvalidValue;
+	}
+	if (e != cudaSuccess)
+		return e;
+	*grid = sms * (per_sm > 0 ? per_sm : 1);
+	return cudaSuccess;
+}
+
+int persistent_tile_elems(int tile) { return tile * tile; }
+
+cudaError_t launch_persistent(const PersistentArgs& a, int tile, int grid, cudaStream_t stream)
+{
+	if (a.n_items <= 0)
+		return cudaSuccess;
+	const int g = grid < a.n_items ? grid : a.n_items;
+	if (tile == 32)
+		kron_persistent_kernel<PCfg32><<<g, PCfg32::THREADS, PCfg32::SMEM, stream>>>(a);
+	else if (tile == 64)
+		kron_persistent_kernel<PCfg64><<<g, PCfg64::THREADS, PCfg64::SMEM, stream>>>(a);
+	else
+		return cudaErrorInvalidValue;
+	return cudaGetLastError();
+}
+
+} // namespace dmrgpp

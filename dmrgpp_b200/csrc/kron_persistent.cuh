@@ -1,0 +1,38 @@
+// Persistent single-launch form of the sector H*x (see kron_persistent.cu).
+#pragma once
+
+#include "kron_plan.h"
+
+#include <cuda_runtime.h>
+
+namespace dmrgpp {
+
+struct PersistentArgs {
+	const double*   ops;     // packed Bstack_j and A^T blocks
+	const double*   x;       // sector vector in
+	double*         bx;      // pass-1 results
+	double*         y;       // sector vector out
+	double*         partial; // split-K partial tiles
+	const GemmSeg*  seg1;
+	const GemmSeg*  pseg2;
+	const KronItem* items;
+	const int*      n1_of_j;
+	unsigned*       work_counter; // [0] next item, [1] CTAs that left, [2] abort
+	unsigned*       done;         // per input patch: finished pass-1 tiles
+	unsigned*       arrive;       // per split tile: finished parts
+	int*            error;        // set to nonzero when a wait gave up
+	int             n_items;
+	int             np;
+	int             n_split_tiles;
+	int             test_extra_wait; // 0; >0 makes waits on patch 0 unsatisfiable (tests)
+};
+
+// Sets kernel attributes on the current device and returns the persistent
+// grid (SMs x resident CTAs) and the k-chunk of the tile configuration.
+cudaError_t persistent_config(int tile, int* grid, int* bk);
+
+int persistent_tile_elems(int tile);
+
+cudaError_t launch_persistent(const PersistentArgs& a, int tile, int grid, cudaStream_t stream);
+
+} // namespace dmrgpp

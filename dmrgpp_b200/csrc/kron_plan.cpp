@@ -194,6 +194,7 @@ std::string build_kron_plan(size_t               noperator,
 		s.b_off = plan.xy_start[j];
 		s.ldb   = int(plan.r[j]);
 		s.K     = int(plan.r[j]);
+		s.dep   = int(j);
 		const int sb = int(plan.seg1.size());
 		plan.seg1.push_back(s);
 		add_tiles(plan.tile1, plan.bx_off[j], plan.M[j], plan.M[j], plan.l[j], sb, sb + 1, bm, bn);
@@ -213,6 +214,7 @@ std::string build_kron_plan(size_t               noperator,
 			s.b_off = plan.at_off[t];
 			s.ldb   = int(plan.l[tr.j]);
 			s.K     = int(plan.l[tr.j]);
+			s.dep   = tr.j;
 			plan.seg2.push_back(s);
 		}
 		const int se = int(plan.seg2.size());
@@ -220,6 +222,116 @@ std::string build_kron_plan(size_t               noperator,
 	}
 	order_tiles(plan.tile2, plan.seg2);
 	return std::string();
+}
+
+void build_persistent_schedule(KronPlan& plan, int bk, int grid)
+{
+	plan.items.clear();
+	plan.pseg2.clear();
+	plan.n1_of_j.assign(plan.np, 0);
+	plan.n_split_tiles = 0;
+	plan.partial_slots = 0;
+
+	for (const GemmTile& t : plan.tile1) {
+		KronItem w {};
+		w.c_off     = t.c_off;
+		w.ldc       = t.ldc;
+		w.M         = t.M;
+		w.N         = t.N;
+		w.m0        = t.m0;
+		w.n0        = t.n0;
+		w.seg_begin = t.seg_begin;
+		w.seg_end   = t.seg_end;
+		w.kind      = 0;
+		w.producer  = plan.seg1[t.seg_begin].dep;
+		plan.n1_of_j[w.producer]++;
+		plan.items.push_back(w);
+	}
+	plan.n1_items = int(plan.items.size());
+
+	// K-slice length: none when the tiles alone give ~2 items per CTA,
+	// otherwise aim at ~2 pass-2 items per CTA, at least 4 chunks each
+	long long total_k = 0;
+	for (const GemmTile& t : plan.tile2)
+		for (int s = t.seg_begin; s < t.seg_end; ++s)
+			total_k += plan.seg2[s].K;
+	long long k_target = 1LL << 40;
+	if ((long long)plan.tile2.size() < 2LL * grid && grid > 0) {
+		k_target = total_k / (2LL * grid);
+		k_target = std::max<long long>(k_target, 4LL * bk);
+		k_target = (k_target + bk - 1) / bk * bk;
+	}
+	const int max_split = 16;
+
+	std::vector<KronItem> p2;
+	for (const GemmTile& t : plan.tile2) {
+		long long kt = 0;
+		for (int s = t.seg_begin; s < t.seg_end; ++s)
+			kt += plan.seg2[s].K;
+		int nsplit = int(std::min<long long>((kt + k_target - 1) / k_target, max_split));
+		nsplit     = std::max(nsplit, 1);
+		long long chunk = (kt + nsplit - 1) / nsplit;
+		chunk           = (chunk + bk - 1) / bk * bk;
+		if (chunk > 0)
+			nsplit = int(std::max<long long>(1, (kt + chunk - 1) / chunk));
+
+		KronItem base {};
+		base.c_off = t.c_off;
+		base.ldc   = t.ldc;
+		base.M     = t.M;
+		base.N     = t.N;
+		base.m0    = t.m0;
+		base.n0    = t.n0;
+		if (nsplit == 1) {
+			base.kind      = 1;
+			base.seg_begin = int(plan.pseg2.size());
+			for (int s = t.seg_begin; s < t.seg_end; ++s)
+				plan.pseg2.push_back(plan.seg2[s]);
+			base.seg_end = int(plan.pseg2.size());
+			p2.push_back(base);
+			continue;
+		}
+		base.kind   = 2;
+		base.tile   = plan.n_split_tiles++;
+		base.nsplit = nsplit;
+		base.slot   = int(plan.partial_slots);
+		plan.partial_slots += nsplit;
+		// walk the tile's segments, cutting them into parts of `chunk` K
+		int       s  = t.seg_begin;
+		long long k0 = 0; // offset inside segment s
+		for (int part = 0; part < nsplit; ++part) {
+			KronItem w  = base;
+			w.part      = part;
+			w.seg_begin = int(plan.pseg2.size());
+			long long need = chunk;
+			while (need > 0 && s < t.seg_end) {
+				const GemmSeg& g    = plan.seg2[s];
+				const long long take = std::min<long long>(need, g.K - k0);
+				GemmSeg        piece = g;
+				piece.a_off += k0 * g.lda; // A = BX_j columns k0..
+				piece.b_off += k0;         // B = A^T rows k0.. (K-contiguous)
+				piece.K = int(take);
+				plan.pseg2.push_back(piece);
+				need -= take;
+				k0 += take;
+				if (k0 == g.K) {
+					++s;
+					k0 = 0;
+				}
+			}
+			w.seg_end = int(plan.pseg2.size());
+			p2.push_back(w);
+		}
+	}
+	auto cost = [&](const KronItem& w) {
+		long long k = 0;
+		for (int s = w.seg_begin; s < w.seg_end; ++s)
+			k += plan.pseg2[s].K;
+		return k;
+	};
+	std::stable_sort(p2.begin(), p2.end(),
+	                 [&](const KronItem& a, const KronItem& b) { return cost(a) > cost(b); });
+	plan.items.insert(plan.items.end(), p2.begin(), p2.end());
 }
 
 } // namespace dmrgpp

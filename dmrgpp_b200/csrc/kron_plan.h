@@ -28,7 +28,7 @@ struct alignas(16) GemmSeg {
 	int       lda;
 	int       ldb;
 	int       K;
-	int       pad;
+	int       dep; // input patch j whose pass-1 result the segment reads (pass 2)
 };
 
 // One CTA's output tile [m0, m0+BM) x [n0, n0+BN) of an M x N matrix at
@@ -42,6 +42,30 @@ struct alignas(16) GemmTile {
 	int       n0;
 	int       seg_begin;
 	int       seg_end;
+	int       pad;
+};
+
+// One work item of the persistent launch (kron_persistent.cu).
+//   kind 0: pass-1 tile of input patch `producer` (segments index seg1)
+//   kind 1: pass-2 output tile, whole K range (segments index pseg2)
+//   kind 2: part `part` of `nsplit` K-slices of pass-2 output tile `tile`;
+//           partial result goes to slot `slot + part`, the last part to
+//           arrive sums the slots in order 0..nsplit-1 and writes the tile
+struct alignas(16) KronItem {
+	long long c_off;
+	int       ldc;
+	int       M;
+	int       N;
+	int       m0;
+	int       n0;
+	int       seg_begin;
+	int       seg_end;
+	int       kind;
+	int       producer;
+	int       tile;
+	int       nsplit;
+	int       slot;
+	int       part;
 	int       pad;
 };
 
@@ -67,10 +91,18 @@ struct KronPlan {
 	std::vector<long long> row_off;    // per triple: first row of (i,k) in BX_j
 	long long              bx_elems = 0;
 
-	// launch lists
+	// launch lists of the two-launch form (pass 1 then pass 2)
 	std::vector<GemmSeg>  seg1, seg2;
 	std::vector<GemmTile> tile1, tile2;
 	int                   bm = 64, bn = 64;
+
+	// persistent form: pass-1 items first, then pass-2 items (K-split)
+	std::vector<KronItem> items;
+	std::vector<GemmSeg>  pseg2;         // pass-2 segments sliced per item
+	std::vector<int>      n1_of_j;       // pass-1 items per input patch
+	int                   n1_items = 0;
+	int                   n_split_tiles = 0;
+	long long             partial_slots = 0;
 
 	long long dim() const { return xy_start.empty() ? 0 : xy_start.back(); }
 };
@@ -90,5 +122,10 @@ std::string build_kron_plan(size_t               noperator,
                             int                  bn,
                             KronPlan&            plan,
                             std::vector<double>* pack_host);
+
+// Builds plan.items / pseg2 / n1_of_j for a persistent launch of `grid`
+// CTAs: pass-2 output tiles are cut into K-slices (multiples of bk, on any
+// k boundary) when there are too few tiles to keep every CTA busy.
+void build_persistent_schedule(KronPlan& plan, int bk, int grid);
 
 } // namespace dmrgpp

@@ -1,0 +1,549 @@
+// Device-resident Lanczos for the lowest eigenpair of one sector, plus the
+// bandwidth-bound vector kernels it is made of and the sector gather/scatter.
+//
+// The recurrence follows PsimagLite's LanczosCore::decomposition
+// (PsimagLite/src/PsimagLite/LanczosCore.h:147-272) and
+// LanczosVectors::oneStepDecomposition / reorthoIfNecessary
+// (LanczosVectors.h:203-271) step by step: normalise the initial vector,
+// V1 = H V0 - a0 V0, then for j >= 1: V2 = H V1, a_j = <V2,V1>,
+// V2 -= a_j V1 + b_j V0, b_{j+1} = |V2|, V2 /= b_{j+1}, optional full
+// reorthogonalisation against the stored vectors and renormalisation, then
+// the stopping test on the lowest Ritz values (LanczosCore.h:222-240).
+// Differences: the reorthogonalisation computes all projections from the
+// same vector (classical Gram-Schmidt, two GEMV passes over the stored basis)
+// where the reference subtracts them one at a time; and the host reads a_j,
+// b_j back every `check_every` steps, applying the stopping test to each step
+// in order (steps run past the stopping point are discarded).
+//
+// Reductions are deterministic: per-block partials in fixed-size grids, the
+// last block to finish (arrival counter) sums them in block order.
+#include "dmrgpp_kron.h"
+#include "handle.h"
+#include "tridiag.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+namespace dmrgpp {
+
+namespace {
+
+constexpr int kThreads   = 256;
+constexpr int kMaxBlocks = 296; // 2 per SM of a B200
+constexpr int kRowChunk  = 1024; // rows per block iteration of the basis GEMVs
+constexpr int kMaxCols   = 1024; // stored Lanczos vectors per solve
+
+// blocks of the basis GEMVs: up to 2 per SM, at least 256 rows each
+int basis_blocks_for(size_t n)
+{
+	const size_t b = (n + 255) / 256;
+	return int(std::max<size_t>(1, std::min<size_t>(b, kMaxBlocks)));
+}
+
+int blocks_for(size_t n)
+{
+	const size_t b = (n + size_t(kThreads) * 8 - 1) / (size_t(kThreads) * 8);
+	return int(std::max<size_t>(1, std::min<size_t>(b, kMaxBlocks)));
+}
+
+__device__ __forceinline__ double block_sum(double v, double* red)
+{
+	for (int o = 16; o > 0; o >>= 1)
+		v += __shfl_down_sync(0xffffffffu, v, o);
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (lane == 0)
+		red[warp] = v;
+	__syncthreads();
+	double s = 0.0;
+	if (threadIdx.x == 0)
+		for (int w = 0; w < kThreads / 32; ++w)
+			s += red[w];
+	__syncthreads();
+	return s; // valid in thread 0
+}
+
+// Called by thread 0 after writing this block's partial: true in the last
+// block to arrive; the counter is reset for the next launch.
+__device__ __forceinline__ bool last_block(unsigned* ctr)
+{
+	__threadfence();
+	const unsigned old = atomicAdd(ctr, 1u);
+	if (old == gridDim.x - 1) {
+		__threadfence();
+		*ctr = 0u;
+		return true;
+	}
+	return false;
+}
+
+// out = sum over blocks, in block order
+__device__ __forceinline__ double sum_partials(const double* partial, int nblk)
+{
+	double s = 0.0;
+	for (int b = 0; b < nblk; ++b)
+		s += __ldcg(partial + b);
+	return s;
+}
+
+// *out = <x, y>
+__global__ void __launch_bounds__(kThreads)
+k_dot(const double* __restrict__ x, const double* __restrict__ y, size_t n, double* out,
+      double* partial, unsigned* ctr)
+{
+	__shared__ double red[kThreads / 32];
+	__shared__ bool   last;
+	double            s = 0.0;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads)
+		s += x[i] * y[i];
+	s = block_sum(s, red);
+	if (threadIdx.x == 0) {
+		partial[blockIdx.x] = s;
+		last                = last_block(ctr);
+		if (last)
+			*out = sum_partials(partial, gridDim.x);
+	}
+}
+
+// dst = src / sqrt(*nrm2) (nrm2 = <src,src> from k_dot)
+__global__ void __launch_bounds__(kThreads)
+k_scale_rsqrt(const double* src, double* dst, size_t n, const double* nrm2)
+{
+	const double a = 1.0 / sqrt(*nrm2);
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads)
+		dst[i] = src[i] * a;
+}
+
+// v2 = v2 - alpha*v1 - beta*v0 (v0 may be null); *beta_out = |v2|
+__global__ void __launch_bounds__(kThreads)
+k_lanczos_update(double* __restrict__ v2, const double* __restrict__ v1,
+                 const double* __restrict__ v0, size_t n, const double* alpha,
+                 const double* beta, double* beta_out, double* partial, unsigned* ctr)
+{
+	__shared__ double red[kThreads / 32];
+	const double      a = *alpha;
+	const double      b = v0 ? *beta : 0.0;
+	double            s = 0.0;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		double w = v2[i] - a * v1[i];
+		if (v0)
+			w -= b * v0[i];
+		v2[i] = w;
+		s += w * w;
+	}
+	s = block_sum(s, red);
+	if (threadIdx.x == 0) {
+		partial[blockIdx.x] = s;
+		if (last_block(ctr))
+			*beta_out = sqrt(sum_partials(partial, gridDim.x));
+	}
+}
+
+// v *= 1 / *s when *s > 0 (LanczosVectors.h:233-237)
+__global__ void __launch_bounds__(kThreads) k_scale_inv(double* v, size_t n, const double* s)
+{
+	const double d = *s;
+	if (!(d > 0.0))
+		return;
+	const double a = 1.0 / d;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads)
+		v[i] *= a;
+}
+
+// r[c] = <V[:,c], v> for c < ncols.  Each warp owns columns warp, warp+8, ...;
+// the block walks its rows in chunks staged in shared memory.
+__global__ void __launch_bounds__(kThreads)
+k_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* __restrict__ v,
+             size_t n, double* r, double* partial, unsigned* ctr)
+{
+	__shared__ double vs[kRowChunk];
+	__shared__ double acc[kMaxCols];
+	__shared__ bool   last;
+	const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int c = threadIdx.x; c < ncols; c += kThreads)
+		acc[c] = 0.0;
+	const size_t rows_per_block = (n + gridDim.x - 1) / gridDim.x;
+	const size_t r0             = size_t(blockIdx.x) * rows_per_block;
+	const size_t r1             = std::min(n, r0 + rows_per_block);
+	for (size_t base = r0; base < r1; base += kRowChunk) {
+		const int len = int(std::min<size_t>(kRowChunk, r1 - base));
+		__syncthreads();
+		for (int i = threadIdx.x; i < len; i += kThreads)
+			vs[i] = v[base + i];
+		__syncthreads();
+		for (int c = warp; c < ncols; c += kThreads / 32) {
+			const double* col = V + size_t(c) * ld + base;
+			double        s   = 0.0;
+			for (int i = lane; i < len; i += 32)
+				s += col[i] * vs[i];
+			for (int o = 16; o > 0; o >>= 1)
+				s += __shfl_down_sync(0xffffffffu, s, o);
+			if (lane == 0)
+				acc[c] += s;
+		}
+	}
+	__syncthreads();
+	for (int c = threadIdx.x; c < ncols; c += kThreads)
+		partial[size_t(blockIdx.x) * kMaxCols + c] = acc[c];
+	__syncthreads();
+	if (threadIdx.x == 0)
+		last = last_block(ctr);
+	__syncthreads();
+	if (last)
+		for (int c = threadIdx.x; c < ncols; c += kThreads) {
+			double s = 0.0;
+			for (int b = 0; b < int(gridDim.x); ++b)
+				s += __ldcg(partial + size_t(b) * kMaxCols + c);
+			r[c] = s;
+		}
+}
+
+// v -= V[:, 0..ncols) r ; *nrm_out = |v|
+__global__ void __launch_bounds__(kThreads)
+k_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t ld, int ncols,
+                 const double* __restrict__ r, size_t n, double* nrm_out, double* partial,
+                 unsigned* ctr)
+{
+	__shared__ double rs[kMaxCols];
+	__shared__ double red[kThreads / 32];
+	for (int c = threadIdx.x; c < ncols; c += kThreads)
+		rs[c] = r[c];
+	__syncthreads();
+	double s = 0.0;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		double w = v[i];
+		for (int c = 0; c < ncols; ++c)
+			w -= V[size_t(c) * ld + i] * rs[c];
+		v[i] = w;
+		s += w * w;
+	}
+	s = block_sum(s, red);
+	if (threadIdx.x == 0) {
+		partial[blockIdx.x] = s;
+		if (last_block(ctr))
+			*nrm_out = sqrt(sum_partials(partial, gridDim.x));
+	}
+}
+
+// z = sum_c coef[c] V[:, c] (LanczosVectors::excitedVector, LanczosVectors.h:192-201)
+__global__ void __launch_bounds__(kThreads)
+k_basis_combine(double* __restrict__ z, const double* __restrict__ V, size_t ld, int ncols,
+                const double* __restrict__ coef, size_t n)
+{
+	__shared__ double cs[kMaxCols];
+	for (int c = threadIdx.x; c < ncols; c += kThreads)
+		cs[c] = coef[c];
+	__syncthreads();
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		double w = 0.0;
+		for (int c = 0; c < ncols; ++c)
+			w += cs[c] * V[size_t(c) * ld + i];
+		z[i] = w;
+	}
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_gather(const double* __restrict__ src, const long long* __restrict__ idx,
+         double* __restrict__ dst, size_t n)
+{
+	for (size_t q = blockIdx.x * size_t(kThreads) + threadIdx.x; q < n;
+	     q += size_t(gridDim.x) * kThreads)
+		dst[q] = src[idx[q]];
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_scatter(const double* __restrict__ src, const long long* __restrict__ idx,
+          double* __restrict__ dst, size_t n)
+{
+	for (size_t q = blockIdx.x * size_t(kThreads) + threadIdx.x; q < n;
+	     q += size_t(gridDim.x) * kThreads)
+		dst[idx[q]] = src[q];
+}
+
+} // namespace
+
+// Device buffers of the eigensolver of one handle.
+struct LanczosWork {
+	size_t    dim     = 0;
+	int       cols    = 0;       // columns of V
+	double*   V       = nullptr; // dim x cols, column-major
+	double*   scal    = nullptr; // alpha[cols], beta[cols+1], work[8]
+	double*   partial = nullptr; // kMaxBlocks * kMaxCols
+	double*   r       = nullptr; // projection coefficients / Ritz coefficients
+	unsigned* ctr     = nullptr; // arrival counters (one per reduction kernel)
+	double*   host    = nullptr; // pinned mirror of alpha/beta
+};
+
+void release_lanczos(dmrgpp_kron_handle h)
+{
+	LanczosWork* w = h->lanczos;
+	if (!w)
+		return;
+	cudaFree(w->V);
+	cudaFree(w->scal);
+	cudaFree(w->partial);
+	cudaFree(w->r);
+	cudaFree(w->ctr);
+	if (w->host)
+		cudaFreeHost(w->host);
+	delete w;
+	h->lanczos = nullptr;
+}
+
+namespace {
+
+int cuda_status(dmrgpp_kron_handle h, cudaError_t e, const char* where)
+{
+	return handle_fail(h, e == cudaErrorMemoryAllocation ? DMRGPP_OOM : DMRGPP_CUDA_ERROR,
+	                   std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+int ensure_work(dmrgpp_kron_handle h, size_t dim, int cols)
+{
+	LanczosWork* w = h->lanczos;
+	if (w && w->dim == dim && w->cols >= cols)
+		return DMRGPP_OK;
+	release_lanczos(h);
+	w           = new LanczosWork();
+	h->lanczos  = w;
+	w->dim      = dim;
+	w->cols     = cols;
+	cudaError_t e;
+	if ((e = cudaMalloc(&w->V, dim * size_t(cols) * sizeof(double))))
+		return cuda_status(h, e, "cudaMalloc(Lanczos basis)");
+	if ((e = cudaMalloc(&w->scal, (2 * size_t(cols) + 16) * sizeof(double))))
+		return cuda_status(h, e, "cudaMalloc(Lanczos scalars)");
+	if ((e = cudaMalloc(&w->partial, size_t(kMaxBlocks) * kMaxCols * sizeof(double))))
+		return cuda_status(h, e, "cudaMalloc(partials)");
+	if ((e = cudaMalloc(&w->r, size_t(kMaxCols) * sizeof(double))))
+		return cuda_status(h, e, "cudaMalloc(coefficients)");
+	if ((e = cudaMalloc(&w->ctr, 16 * sizeof(unsigned))))
+		return cuda_status(h, e, "cudaMalloc(counters)");
+	if ((e = cudaMemset(w->ctr, 0, 16 * sizeof(unsigned))))
+		return cuda_status(h, e, "clear counters");
+	if ((e = cudaMemset(w->scal, 0, (2 * size_t(cols) + 16) * sizeof(double))))
+		return cuda_status(h, e, "clear scalars");
+	if ((e = cudaHostAlloc(&w->host, (2 * size_t(cols) + 16) * sizeof(double), 0)))
+		return cuda_status(h, e, "cudaHostAlloc(scalars)");
+	return DMRGPP_OK;
+}
+
+} // namespace
+} // namespace dmrgpp
+
+using dmrgpp::LanczosWork;
+
+extern "C" {
+
+void dmrgpp_lanczos_params_init(dmrgpp_lanczos_params* p)
+{
+	if (!p)
+		return;
+	p->steps         = 200;   // ParametersForSolver.h:97 (LanczosSteps)
+	p->min_steps     = 4;     // ParametersForSolver.h:102
+	p->eigs_for_stop = 1;     // ParametersForSolver.h:105
+	p->tolerance     = 1e-12; // ParametersForSolver.h:103
+	p->reortho       = 1;     // Options=reortho
+	p->check_every   = 8;
+}
+
+int dmrgpp_tridiag_eigen(size_t n, const double* diag, const double* offdiag, double* eigs,
+                         double* vectors)
+{
+	if (n == 0)
+		return DMRGPP_OK;
+	if (!diag || !eigs || (n > 1 && !offdiag) || n > (1u << 20))
+		return DMRGPP_INVALID_ARG;
+	std::copy(diag, diag + n, eigs);
+	return dmrgpp::tridiag_eigen(int(n), eigs, offdiag, vectors) ? DMRGPP_OK
+	                                                            : DMRGPP_NOT_CONVERGED;
+}
+
+int dmrgpp_gather(const double* src, const int64_t* idx, double* dst, size_t n, void* stream)
+{
+	if (n == 0)
+		return DMRGPP_OK;
+	if (!src || !idx || !dst)
+		return DMRGPP_INVALID_ARG;
+	const int nb = dmrgpp::blocks_for(n);
+	dmrgpp::k_gather<<<nb, dmrgpp::kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+	    src, reinterpret_cast<const long long*>(idx), dst, n);
+	return cudaGetLastError() == cudaSuccess ? DMRGPP_OK : DMRGPP_CUDA_ERROR;
+}
+
+int dmrgpp_scatter(const double* src, const int64_t* idx, double* dst, size_t n, void* stream)
+{
+	if (n == 0)
+		return DMRGPP_OK;
+	if (!src || !idx || !dst)
+		return DMRGPP_INVALID_ARG;
+	const int nb = dmrgpp::blocks_for(n);
+	dmrgpp::k_scatter<<<nb, dmrgpp::kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+	    src, reinterpret_cast<const long long*>(idx), dst, n);
+	return cudaGetLastError() == cudaSuccess ? DMRGPP_OK : DMRGPP_CUDA_ERROR;
+}
+
+int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
+                          const dmrgpp_lanczos_params* p,
+                          const double*               init,
+                          int                         on_device,
+                          double*                     energy,
+                          double*                     z,
+                          size_t*                     steps_taken)
+{
+	using namespace dmrgpp;
+	if (!h)
+		return DMRGPP_INVALID_ARG;
+	if (!p || !init || !energy || !z)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "null argument");
+	if (p->steps < 1 || p->check_every < 1 || p->eigs_for_stop < 1)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "steps, check_every and eigs_for_stop must be >= 1");
+	const size_t D = size_t(h->plan.dim());
+	size_t       maxn = std::min(p->steps, D); // LanczosCore.h:177-178
+	if (maxn + 1 > size_t(kMaxCols))
+		return handle_fail(h, DMRGPP_INVALID_ARG, "at most 1023 Lanczos steps");
+
+	int prev = -1;
+	cudaGetDevice(&prev);
+	if (prev != h->device)
+		cudaSetDevice(h->device);
+	struct Restore {
+		int dev, prev;
+		~Restore()
+		{
+			if (dev != prev && prev >= 0)
+				cudaSetDevice(prev);
+		}
+	} restore { h->device, prev };
+
+	if (int rc = ensure_work(h, D, int(maxn) + 1))
+		return rc;
+	LanczosWork* w  = h->lanczos;
+	cudaStream_t st = h->stream;
+	const int    nb = blocks_for(D);
+	const int    nbb = basis_blocks_for(D);
+	double*      V  = w->V;
+	double*      alpha = w->scal;
+	double*      beta  = w->scal + w->cols;
+	double*      work  = w->scal + 2 * size_t(w->cols); // [0] norm^2 of init, [1] reortho norm
+	auto         col   = [&](size_t c) { return V + c * D; };
+	cudaError_t  e;
+
+	// V0 = init / |init|  (LanczosCore.h:166-175)
+	if (!on_device) {
+		if ((e = cudaMemcpyAsync(col(1), init, D * sizeof(double), cudaMemcpyHostToDevice, st)))
+			return cuda_status(h, e, "copy initial vector");
+	} else if ((e = cudaMemcpyAsync(col(1), init, D * sizeof(double), cudaMemcpyDeviceToDevice, st))) {
+		return cuda_status(h, e, "copy initial vector");
+	}
+	k_dot<<<nb, kThreads, 0, st>>>(col(1), col(1), D, work, w->partial, w->ctr);
+	k_scale_rsqrt<<<nb, kThreads, 0, st>>>(col(1), col(0), D, work);
+	cudaMemsetAsync(beta, 0, sizeof(double), st); // beta_0 = 0
+
+	// first step (LanczosCore.h:186-208)
+	if (int rc = kron_apply_device(h, col(0), col(1)))
+		return rc;
+	k_dot<<<nb, kThreads, 0, st>>>(col(1), col(0), D, alpha, w->partial, w->ctr + 1);
+	k_lanczos_update<<<nb, kThreads, 0, st>>>(col(1), col(0), nullptr, D, alpha, beta, beta + 1,
+	                                          w->partial, w->ctr + 2);
+	k_scale_inv<<<nb, kThreads, 0, st>>>(col(1), D, beta + 1);
+
+	std::vector<double> a_host, b_host(1, 0.0), eold(p->eigs_for_stop, 0.0), eigs;
+	size_t              j_stop = 0;
+	bool                done   = false;
+	size_t              j      = 1;
+	while (!done && j < maxn) {
+		const size_t jend = std::min(maxn, j + size_t(p->check_every));
+		for (size_t jj = j; jj < jend; ++jj) {
+			// oneStepDecomposition (LanczosVectors.h:203-241), V2 lives in column jj+1
+			double* v0 = col(jj - 1);
+			double* v1 = col(jj);
+			double* v2 = col(jj + 1);
+			if (int rc = kron_apply_device(h, v1, v2))
+				return rc;
+			k_dot<<<nb, kThreads, 0, st>>>(v2, v1, D, alpha + jj, w->partial, w->ctr + 1);
+			k_lanczos_update<<<nb, kThreads, 0, st>>>(v2, v1, v0, D, alpha + jj, beta + jj,
+			                                          beta + jj + 1, w->partial, w->ctr + 2);
+			k_scale_inv<<<nb, kThreads, 0, st>>>(v2, D, beta + jj + 1);
+			if (p->reortho) { // reorthoIfNecessary (LanczosVectors.h:243-271)
+				const int nc = int(jj) + 1;
+				k_basis_dots<<<nbb, kThreads, 0, st>>>(V, D, nc, v2, D, w->r, w->partial, w->ctr + 3);
+				k_basis_subtract<<<nbb, kThreads, 0, st>>>(v2, V, D, nc, w->r, D, work + 1,
+				                                          w->partial, w->ctr + 4);
+				k_scale_inv<<<nb, kThreads, 0, st>>>(v2, D, work + 1);
+			}
+		}
+		if ((e = cudaGetLastError()))
+			return cuda_status(h, e, "Lanczos step launch");
+		// alpha[0..jend) and beta[0..jend] back to the host
+		if ((e = cudaMemcpyAsync(w->host, w->scal, 2 * size_t(w->cols) * sizeof(double),
+		                         cudaMemcpyDeviceToHost, st)))
+			return cuda_status(h, e, "read alpha/beta");
+		if ((e = cudaStreamSynchronize(st)))
+			return cuda_status(h, e, "Lanczos steps");
+		if (h->err_host && *reinterpret_cast<volatile int*>(h->err_host))
+			return handle_fail(h, DMRGPP_TIMEOUT, "H*x kernel wait gave up during Lanczos");
+		const double* ah = w->host;
+		const double* bh = w->host + w->cols;
+		// stopping test per step, in order (LanczosCore.h:215-240)
+		for (size_t jj = j; jj < jend; ++jj) {
+			const size_t n = jj + 1;
+			std::vector<double> d(ah, ah + n), off(bh + 1, bh + n);
+			if (!tridiag_eigen(int(n), d.data(), off.data(), nullptr))
+				return handle_fail(h, DMRGPP_NOT_CONVERGED, "tridiagonal eigensolve failed");
+			const size_t ne   = std::min(p->eigs_for_stop, n);
+			double       dmax = 0.0;
+			for (size_t k = 0; k < ne; ++k) {
+				dmax    = std::max(dmax, std::fabs(d[k] - eold[k]));
+				eold[k] = d[k];
+			}
+			bool exit_flag = dmax < p->tolerance || jj == maxn - 1;
+			if ((exit_flag && D <= 4) || (exit_flag && jj >= p->min_steps)) {
+				j_stop = jj;
+				done   = true;
+				break;
+			}
+		}
+		j = jend;
+	}
+	if (!done)
+		j_stop = maxn - 1;
+	if (maxn == 1)
+		j_stop = 0;
+
+	// Ritz vector of the (j_stop+1)-dimensional tridiagonal (LanczosSolver.h:76-84)
+	const size_t        n = j_stop + 1;
+	std::vector<double> d(w->host, w->host + n), off(w->host + w->cols + 1, w->host + w->cols + n),
+	    zt(n * n);
+	if (maxn == 1) { // no loop ran: alpha[0] has not been read back yet
+		if ((e = cudaMemcpy(w->host, w->scal, sizeof(double), cudaMemcpyDeviceToHost)))
+			return cuda_status(h, e, "read alpha");
+		d[0] = w->host[0];
+	}
+	if (!tridiag_eigen(int(n), d.data(), off.data(), zt.data()))
+		return handle_fail(h, DMRGPP_NOT_CONVERGED, "tridiagonal eigensolve failed");
+	*energy = d[0];
+	if ((e = cudaMemcpyAsync(w->r, zt.data(), n * sizeof(double), cudaMemcpyHostToDevice, st)))
+		return cuda_status(h, e, "upload Ritz coefficients");
+	double* zdst = on_device ? z : col(j_stop + 1); // that column is free after the solve
+	k_basis_combine<<<nb, kThreads, 0, st>>>(zdst, V, D, int(n), w->r, D);
+	if (!on_device
+	    && (e = cudaMemcpyAsync(z, zdst, D * sizeof(double), cudaMemcpyDeviceToHost, st)))
+		return cuda_status(h, e, "copy Ritz vector");
+	if ((e = cudaStreamSynchronize(st)))
+		return cuda_status(h, e, "Ritz vector");
+	if (steps_taken)
+		*steps_taken = j_stop;
+	return DMRGPP_OK;
+}
+
+} // extern "C"

@@ -127,6 +127,35 @@ class BatchedGemm:
                 raise ValueError(f"host vectors must be contiguous float64 of length {self.dim}")
         return 0, vin.ctypes.data, vout.ctypes.data
 
+    def lanczos_lowest(self, init, steps: int = 200, min_steps: int = 4,
+                       tolerance: float = 1e-12, eigs_for_stop: int = 1, reortho: bool = True,
+                       check_every: int = 8):
+        """Lowest eigenpair by the device Lanczos (the reference's
+        LanczosSolver::computeAllStatesBelow for one state).  Returns
+        (energy, ritz_vector, steps).  numpy init -> numpy vector; a torch
+        CUDA tensor -> a torch CUDA tensor."""
+        L = self._lib
+        p = _capi.LanczosParams()
+        L.dmrgpp_lanczos_params_init(ctypes.byref(p))
+        p.steps, p.min_steps, p.tolerance = steps, min_steps, tolerance
+        p.eigs_for_stop, p.reortho, p.check_every = eigs_for_stop, int(reortho), check_every
+        e = ctypes.c_double()
+        n = ctypes.c_size_t()
+        if hasattr(init, "data_ptr"):
+            import torch
+            z = torch.empty_like(init)
+            self._pointers(init, z)
+            rc = L.dmrgpp_lanczos_lowest(self._h, ctypes.byref(p), init.data_ptr(), 1,
+                                         ctypes.byref(e), z.data_ptr(), ctypes.byref(n))
+        else:
+            init = np.ascontiguousarray(init, dtype=np.float64)
+            z = np.empty(self.dim)
+            self._pointers(init, z)
+            rc = L.dmrgpp_lanczos_lowest(self._h, ctypes.byref(p), init.ctypes.data, 0,
+                                         ctypes.byref(e), z.ctypes.data, ctypes.byref(n))
+        _capi.check(rc, self._h)
+        return e.value, z, int(n.value)
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.dmrgpp_kron_destroy(self._h)
@@ -137,6 +166,23 @@ class BatchedGemm:
             self.close()
         except Exception:
             pass
+
+
+def tridiag_eigen(diag, offdiag, vectors: bool = True):
+    """Eigenvalues (ascending) and eigenvectors of a symmetric tridiagonal
+    matrix by the library's host solver."""
+    d = np.ascontiguousarray(diag, dtype=np.float64)
+    e = np.ascontiguousarray(offdiag, dtype=np.float64)
+    n = len(d)
+    w = np.empty(n)
+    Z = np.empty((n, n), order="F") if vectors else None
+    dp = ctypes.POINTER(ctypes.c_double)
+    rc = _capi.lib().dmrgpp_tridiag_eigen(n, d.ctypes.data_as(dp),
+                                          e.ctypes.data_as(dp) if n > 1 else None,
+                                          w.ctypes.data_as(dp),
+                                          Z.ctypes.data_as(dp) if vectors else None)
+    _capi.check(rc)
+    return (w, Z) if vectors else w
 
 
 def plan_info(prob, precision: int = FP64) -> dict:

@@ -95,6 +95,19 @@ int dmrgpp_kron_destroy(dmrgpp_kron_handle h);
  * and y are device pointers; the call only enqueues work on the stream. */
 int dmrgpp_kron_apply(dmrgpp_kron_handle h, const double* x, double* y, int on_device);
 
+/* Waits for the handle's stream and reports errors of work enqueued by
+ * device-pointer applies (DMRGPP_TIMEOUT if a dependency wait inside the
+ * kernel gave up, DMRGPP_CUDA_ERROR for a CUDA failure).  No counterpart in
+ * the reference, whose apply is synchronous. */
+int dmrgpp_kron_synchronize(dmrgpp_kron_handle h);
+
+/* Test hook (no counterpart in the reference): with on != 0 every following
+ * apply makes the kernel's dependency waits on input patch 0 unsatisfiable,
+ * so they run into their time limit (about 0.2 s) and the apply reports
+ * DMRGPP_TIMEOUT; the handle stays usable.  Used to test failure detection
+ * without faulting the GPU. */
+int dmrgpp_kron_test_stall_dependency(dmrgpp_kron_handle h, int on);
+
 /* Sector dimension D = sum_p l_p r_p (xy_patch_start, setup_sparse_batch.cpp:98-103). */
 int dmrgpp_kron_dim(dmrgpp_kron_handle h, size_t* dim);
 
@@ -138,6 +151,43 @@ int dmrgpp_kron_plan_info_get(const dmrgpp_kron_desc* desc, dmrgpp_kron_plan_inf
 #define DMRGPP_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 int dmrgpp_kron_apply_noalloc(const dmrgpp_kron_desc* desc, const double* x, double* y);
 const char* dmrgpp_kron_noalloc_last_error(void);
+
+/* ---- Eigensolver on the device (replaces PsimagLite::LanczosSolver for one
+ * sector, PsimagLite/src/PsimagLite/LanczosSolver.h:68-88 with
+ * LanczosCore.h:147-272 and LanczosVectors.h:192-271) ---- */
+typedef struct {
+	size_t steps;         /* LanczosSteps, maximum steps (default 200) */
+	size_t min_steps;     /* MinSteps (default 4) */
+	size_t eigs_for_stop; /* EigsForStop: lowest Ritz values watched (default 1) */
+	double tolerance;     /* LanczosEps: stop when they change by less (default 1e-12) */
+	int    reortho;       /* full reorthogonalisation, Options=reortho (default 1) */
+	int    check_every;   /* steps enqueued between stopping tests on the host (default 8) */
+} dmrgpp_lanczos_params;
+
+/* Fills the reference's defaults (ParametersForSolver.h:93-120). */
+void dmrgpp_lanczos_params_init(dmrgpp_lanczos_params* p);
+
+/* Lowest eigenpair of the sector's H by Lanczos from init (patch order).
+ * The Lanczos vectors stay on the device.  on_device: init and z are device
+ * pointers (else host).  energy = lowest Ritz value of the final tridiagonal,
+ * z = its Ritz vector (unit norm), steps_taken = the step at which the
+ * stopping test passed.  Synchronous. */
+int dmrgpp_lanczos_lowest(dmrgpp_kron_handle h, const dmrgpp_lanczos_params* p,
+                          const double* init, int on_device, double* energy, double* z,
+                          size_t* steps_taken);
+
+/* Host helper: eigenvalues (ascending) and, when vectors != NULL, eigenvectors
+ * (n x n column-major) of the symmetric tridiagonal matrix diag/offdiag; the
+ * role of dstedc in TridiagonalMatrix.cpp:21. */
+int dmrgpp_tridiag_eigen(size_t n, const double* diag, const double* offdiag, double* eigs,
+                         double* vectors);
+
+/* Sector gather / scatter on the device (InitKronHamiltonian.h:158-221 copyIn,
+ * InitKronBase.h:315-360 copyOut): dst[q] = src[idx[q]] and dst[idx[q]] =
+ * src[q] for q < n, with idx the map from patch order to the sector's
+ * positions in super-basis order; enqueued on stream (cudaStream_t). */
+int dmrgpp_gather(const double* src, const int64_t* idx, double* dst, size_t n, void* stream);
+int dmrgpp_scatter(const double* src, const int64_t* idx, double* dst, size_t n, void* stream);
 
 /* Last error message of a handle, or of the calling thread's last failed
  * create when h is NULL.  Never returns NULL. */

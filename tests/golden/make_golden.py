@@ -170,3 +170,31 @@ if __name__ == "__main__":
     kron_data31()
     prob, vin, y, rq = load_kron_data31()
     assert np.allclose(oracle.kron_apply(prob, vin), y, rtol=1e-13, atol=1e-15)
+
+
+def lanczos_fixtures():
+    """Lowest eigenpairs by the reference's PsimagLite::LanczosSolver (compiled
+    from the reference sources, matvec = the reference BatchedGemmCpu) from
+    seeded initial vectors, with reortho, LanczosEps 1e-12, 200 steps."""
+    from dmrgpp_b200 import superblock as sb
+    out = {}
+    cases = {"kron_data31": load_kron_data31()[0],
+             "random_sym_6x3": sb.random_problem(6, 3, max_size=14, seed=77, symmetric=True),
+             "microbench_1024": sb.c2_problem()}
+    for name, prob in cases.items():
+        init = np.random.default_rng(2024).standard_normal(prob.dim)
+        rk = oracle.RefKron(prob)
+        e, z, steps = rk.lanczos(init, steps=200, min_steps=4, tolerance=1e-12, reortho=True)
+        exact = None
+        if prob.dim <= 3000:
+            exact = float(np.linalg.eigvalsh(prob.dense())[0])
+        out[name] = {"energy": e, "steps": steps, "dim": prob.dim, "exact": exact,
+                     "init_seed": 2024, "z_head": z[:8].tolist(),
+                     "z_norm": float(np.linalg.norm(z))}
+        print(name, "E =", repr(e), "steps", steps, "exact", exact)
+    with open(os.path.join(HERE, "lanczos_reference.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
+if __name__ == "__main__" and "--lanczos" in sys.argv:
+    lanczos_fixtures()

@@ -116,3 +116,44 @@ def test_symmetric_operator_gives_symmetric_products(cuda_lib, cuda_device):
     # linearity
     np.testing.assert_allclose(bg(2.0 * u - 3.0 * v), 2.0 * bg(u) - 3.0 * bg(v), rtol=1e-12,
                                atol=1e-10)
+
+
+def test_dependency_wait_times_out_and_handle_recovers(cuda_lib, cuda_device, oracle_built):
+    """Failure detection without a GPU fault: the test hook makes the kernel's
+    waits on input patch 0 unsatisfiable; they give up after their time limit,
+    the apply reports TIMEOUT, and the next apply is correct again."""
+    from dmrgpp_b200 import _capi, plugin
+    prob = sb.c2_problem()
+    x = sb.random_unit_vector(prob.dim, seed=9)
+    bg = plugin.BatchedGemm.from_problem(prob)
+    y_ok = bg(x)
+    assert cuda_lib.dmrgpp_kron_test_stall_dependency(bg.handle, 1) == _capi.OK
+    with pytest.raises(_capi.DmrgppError) as ei:
+        bg(x)
+    assert ei.value.status == _capi.TIMEOUT
+    assert cuda_lib.dmrgpp_kron_test_stall_dependency(bg.handle, 0) == _capi.OK
+    y_again = bg(x)
+    assert np.array_equal(y_again, y_ok)
+    assert rel_err(y_again, oracle_built.kron_apply(prob, x)) < RTOL
+    bg.close()
+
+
+def test_device_pointer_applies_then_synchronize(cuda_lib, cuda_device, oracle_built):
+    """Back-to-back asynchronous applies on one stream (the persistent kernel
+    resets its own counters between launches), checked after one sync."""
+    import torch
+    from dmrgpp_b200 import _capi, plugin
+    prob = sb.random_problem(npatches=9, noperator=5, max_size=150, seed=31)
+    s = torch.cuda.Stream()
+    bg = plugin.BatchedGemm.from_problem(prob, stream=s.cuda_stream)
+    rng = np.random.default_rng(4)
+    xs = [rng.standard_normal(prob.dim) for _ in range(4)]
+    with torch.cuda.stream(s):
+        xd = [torch.from_numpy(x).to(cuda_device) for x in xs]
+        yd = [torch.empty_like(v) for v in xd]
+    for a, b in zip(xd, yd):
+        bg.apply_Htarget(a, b)
+    assert cuda_lib.dmrgpp_kron_synchronize(bg.handle) == _capi.OK
+    for x, y in zip(xs, yd):
+        assert rel_err(y.cpu().numpy(), oracle_built.kron_apply(prob, x)) < RTOL
+    bg.close()
