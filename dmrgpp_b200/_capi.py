@@ -71,6 +71,11 @@ SIGNATURES.update({
     "dmrgpp_tridiag_eigen": (ctypes.c_int, [_sz, _dp, _dp, _dp, _dp]),
     "dmrgpp_gather": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _sz,
                                      ctypes.c_void_p]),
+    "dmrgpp_kron_get_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int)]),
+    "dmrgpp_kron_set_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "dmrgpp_kron_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_int), _dp]),
     "dmrgpp_scatter": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _sz,
                                       ctypes.c_void_p]),
 })

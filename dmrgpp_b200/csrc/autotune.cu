@@ -1,0 +1,196 @@
+// Autotuner of the persistent H*x launch.
+//
+// The reference hard-codes its GPU tiling ("tuned" constants for one GH200
+// input, BatchedGemmKokkos.h:110-130).  Here each sector is timed under every
+// tile configuration (kron_persistent.cuh) and work split (pass-2 items per
+// CTA), the fastest is kept, and the choice is cached in a text file keyed
+// by a signature of the sector-size histogram (patch sizes, Kronecker terms,
+// contributing triples) and the GPU name, so that sectors of the same shape
+// in later sweep steps or runs skip the timing.
+#include "dmrgpp_kron.h"
+#include "handle.h"
+#include "kron_persistent.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace {
+
+using dmrgpp::KronPlan;
+
+// FNV-1a over the sector's shape
+std::string sector_signature(const KronPlan& P, const char* gpu)
+{
+	unsigned long long h   = 1469598103934665603ull;
+	auto               mix = [&](unsigned long long v) {
+                for (int b = 0; b < 8; ++b) {
+                        h ^= (v >> (8 * b)) & 0xffu;
+                        h *= 1099511628211ull;
+                }
+	};
+	mix(P.np);
+	mix(P.nop);
+	for (size_t p = 0; p < P.np; ++p) {
+		mix((unsigned long long)P.l[p]);
+		mix((unsigned long long)P.r[p]);
+	}
+	mix(P.triples.size());
+	for (const auto& t : P.triples)
+		mix((unsigned long long)(t.i * 65536 + t.j));
+	for (const char* c = gpu; *c; ++c)
+		mix((unsigned long long)(unsigned char)*c);
+	char buf[32];
+	std::snprintf(buf, sizeof(buf), "%016llx", h);
+	return buf;
+}
+
+bool cache_lookup(const char* path, const std::string& sig, int* cfg, int* ipc, double* us)
+{
+	if (!path)
+		return false;
+	std::ifstream f(path);
+	std::string   line;
+	bool          found = false;
+	while (std::getline(f, line)) {
+		std::istringstream in(line);
+		std::string        s;
+		int                c = -1, i = 0;
+		double             t = 0;
+		if (in >> s >> c >> i >> t && s == sig && c >= 0 && c < dmrgpp::kNumTileCfgs && i > 0) {
+			*cfg  = c;
+			*ipc  = i;
+			*us   = t;
+			found = true; // the last entry wins
+		}
+	}
+	return found;
+}
+
+void cache_store(const char* path, const std::string& sig, int cfg, int ipc, double us)
+{
+	if (!path)
+		return;
+	std::ofstream f(path, std::ios::app);
+	f << sig << ' ' << cfg << ' ' << ipc << ' ' << us << '\n';
+}
+
+} // namespace
+
+extern "C" {
+
+int dmrgpp_kron_get_config(dmrgpp_kron_handle h, int* cfg, int* items_per_cta)
+{
+	if (!h || !cfg || !items_per_cta)
+		return DMRGPP_INVALID_ARG;
+	*cfg           = h->cfg;
+	*items_per_cta = h->items_per_cta;
+	return DMRGPP_OK;
+}
+
+int dmrgpp_kron_set_config(dmrgpp_kron_handle h, int cfg, int items_per_cta)
+{
+	if (!h)
+		return DMRGPP_INVALID_ARG;
+	if (cfg < 0 || cfg >= dmrgpp::kNumTileCfgs || items_per_cta < 1 || items_per_cta > 64)
+		return dmrgpp::handle_fail(h, DMRGPP_INVALID_ARG, "unknown tile configuration");
+	int prev = -1;
+	cudaGetDevice(&prev);
+	if (prev != h->device)
+		cudaSetDevice(h->device);
+	cudaStreamSynchronize(h->stream);
+	const int rc = dmrgpp::configure_schedule(h, cfg, items_per_cta);
+	if (prev != h->device && prev >= 0)
+		cudaSetDevice(prev);
+	return rc;
+}
+
+int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps, int* cfg_out,
+                         double* us_out)
+{
+	using namespace dmrgpp;
+	if (!h)
+		return DMRGPP_INVALID_ARG;
+	if (reps < 1)
+		reps = 10;
+	int prev = -1;
+	cudaGetDevice(&prev);
+	if (prev != h->device)
+		cudaSetDevice(h->device);
+	struct Restore {
+		int dev, prev;
+		~Restore()
+		{
+			if (dev != prev && prev >= 0)
+				cudaSetDevice(prev);
+		}
+	} restore { h->device, prev };
+
+	cudaDeviceProp prop {};
+	cudaGetDeviceProperties(&prop, h->device);
+	const std::string sig = sector_signature(h->plan, prop.name);
+	int               cfg = 0, ipc = 2;
+	double            us  = 0.0;
+	if (cache_lookup(cache_path, sig, &cfg, &ipc, &us)) {
+		if (int rc = configure_schedule(h, cfg, ipc))
+			return rc;
+		if (cfg_out)
+			*cfg_out = cfg;
+		if (us_out)
+			*us_out = us;
+		return DMRGPP_OK;
+	}
+
+	cudaEvent_t e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	cudaStreamSynchronize(h->stream);
+	const int ipcs[] = { 1, 2, 4 };
+	double    best   = -1.0;
+	int       bcfg = h->cfg, bipc = h->items_per_cta;
+	for (int c = 0; c < kNumTileCfgs; ++c)
+		for (int i : ipcs) {
+			if (configure_schedule(h, c, i) != DMRGPP_OK)
+				continue;
+			bool ok = true;
+			for (int w = 0; w < 2 && ok; ++w)
+				ok = kron_apply_device(h, h->d_x, h->d_y) == DMRGPP_OK;
+			double tmin = 1e30;
+			for (int r = 0; r < reps && ok; ++r) {
+				cudaEventRecord(e0, h->stream);
+				ok = kron_apply_device(h, h->d_x, h->d_y) == DMRGPP_OK;
+				cudaEventRecord(e1, h->stream);
+				cudaEventSynchronize(e1);
+				float ms = 0.f;
+				cudaEventElapsedTime(&ms, e0, e1);
+				tmin = std::min(tmin, double(ms) * 1e3);
+			}
+			if (ok && cudaStreamSynchronize(h->stream) == cudaSuccess && h->err_host
+			    && *reinterpret_cast<volatile int*>(h->err_host) == 0
+			    && (best < 0 || tmin < best)) {
+				best = tmin;
+				bcfg = c;
+				bipc = i;
+			}
+		}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (best < 0)
+		return handle_fail(h, DMRGPP_CUDA_ERROR, "autotune: no configuration ran");
+	if (int rc = configure_schedule(h, bcfg, bipc))
+		return rc;
+	cache_store(cache_path, sig, bcfg, bipc, best);
+	if (cfg_out)
+		*cfg_out = bcfg;
+	if (us_out)
+		*us_out = best;
+	return DMRGPP_OK;
+}
+
+} // extern "C"

@@ -149,10 +149,72 @@ int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 	pa.n_items       = int(P.items.size());
 	pa.np            = int(P.np);
 	pa.n_split_tiles = P.n_split_tiles;
-	if ((e = dmrgpp::launch_persistent(pa, h->tile, h->grid, h->stream)))
+	if ((e = dmrgpp::launch_persistent(pa, h->cfg, h->grid, h->stream)))
 		return cuda_fail(h, e, "H*x launch");
 	return DMRGPP_OK;
 
+}
+
+int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
+{
+	int         grid = 0, tile = 0, bk = 0;
+	cudaError_t e    = persistent_config(cfg, &grid, &tile, &bk);
+	if (e != cudaSuccess)
+		return cuda_fail(h, e, "persistent kernel attributes");
+	KronPlan& P = h->plan;
+	if (tile != P.bm || P.tile1.size() + P.tile2.size() == 0)
+		build_tile_lists(P, tile, tile);
+	build_persistent_schedule(P, bk, grid, items_per_cta);
+	h->cfg           = cfg;
+	h->grid          = grid;
+	h->tile          = tile;
+	h->items_per_cta = items_per_cta;
+
+	// every list in one allocation, each chunk on a 16-byte boundary
+	std::vector<unsigned char> lists;
+	std::vector<size_t>        offs;
+	auto add = [&](const void* src, size_t n) {
+		offs.push_back(lists.size());
+		lists.resize(lists.size() + ((n + 15) / 16) * 16);
+		if (n)
+			std::memcpy(lists.data() + offs.back(), src, n);
+	};
+	add(P.seg1.data(), P.seg1.size() * sizeof(GemmSeg));
+	add(P.seg2.data(), P.seg2.size() * sizeof(GemmSeg));
+	add(P.tile1.data(), P.tile1.size() * sizeof(GemmTile));
+	add(P.tile2.data(), P.tile2.size() * sizeof(GemmTile));
+	add(P.items.data(), P.items.size() * sizeof(KronItem));
+	add(P.pseg2.data(), P.pseg2.size() * sizeof(GemmSeg));
+	add(P.n1_of_j.data(), P.n1_of_j.size() * sizeof(int));
+	cudaFree(h->d_lists);
+	cudaFree(h->d_ctr);
+	cudaFree(h->d_part);
+	h->d_lists = nullptr;
+	h->d_ctr   = nullptr;
+	h->d_part  = nullptr;
+	if ((e = cudaMalloc(&h->d_lists, lists.empty() ? 16 : lists.size())))
+		return cuda_fail(h, e, "cudaMalloc(lists)");
+	auto at    = [&](int i) { return static_cast<unsigned char*>(h->d_lists) + offs[i]; };
+	h->d_seg1  = reinterpret_cast<GemmSeg*>(at(0));
+	h->d_seg2  = reinterpret_cast<GemmSeg*>(at(1));
+	h->d_tile1 = reinterpret_cast<GemmTile*>(at(2));
+	h->d_tile2 = reinterpret_cast<GemmTile*>(at(3));
+	h->d_items = reinterpret_cast<KronItem*>(at(4));
+	h->d_pseg2 = reinterpret_cast<GemmSeg*>(at(5));
+	h->d_n1    = reinterpret_cast<int*>(at(6));
+	if (!lists.empty()
+	    && (e = cudaMemcpy(h->d_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
+		return cuda_fail(h, e, "upload lists");
+
+	const size_t nctr = 3 + P.np + size_t(P.n_split_tiles);
+	if ((e = cudaMalloc(&h->d_ctr, nctr * sizeof(unsigned))))
+		return cuda_fail(h, e, "cudaMalloc(counters)");
+	if ((e = cudaMemset(h->d_ctr, 0, nctr * sizeof(unsigned))))
+		return cuda_fail(h, e, "clear counters");
+	const size_t part_elems = size_t(P.partial_slots) * size_t(tile) * size_t(tile);
+	if ((e = cudaMalloc(&h->d_part, (part_elems ? part_elems : 1) * sizeof(double))))
+		return cuda_fail(h, e, "cudaMalloc(partials)");
+	return DMRGPP_OK;
 }
 
 } // namespace dmrgpp
@@ -267,55 +329,17 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 	if ((e = cudaMalloc(&h->d_y, dim * sizeof(double))))
 		return bail(e, "cudaMalloc(y)");
 
-	int bk = 16;
-	if ((e = dmrgpp::persistent_config(bm, &h->grid, &bk)))
-		return bail(e, "persistent kernel attributes");
-	h->tile = bm;
-	dmrgpp::build_persistent_schedule(h->plan, bk, h->grid);
-
-	// every list in one allocation, each chunk on a 16-byte boundary
-	std::vector<unsigned char> lists;
-	std::vector<size_t>        offs;
-	auto add = [&](const void* src, size_t n) {
-		offs.push_back(lists.size());
-		lists.resize(lists.size() + ((n + 15) / 16) * 16);
-		if (n)
-			std::memcpy(lists.data() + offs.back(), src, n);
-	};
-	add(P.seg1.data(), P.seg1.size() * sizeof(dmrgpp::GemmSeg));
-	add(P.seg2.data(), P.seg2.size() * sizeof(dmrgpp::GemmSeg));
-	add(P.tile1.data(), P.tile1.size() * sizeof(dmrgpp::GemmTile));
-	add(P.tile2.data(), P.tile2.size() * sizeof(dmrgpp::GemmTile));
-	add(P.items.data(), P.items.size() * sizeof(dmrgpp::KronItem));
-	add(P.pseg2.data(), P.pseg2.size() * sizeof(dmrgpp::GemmSeg));
-	add(P.n1_of_j.data(), P.n1_of_j.size() * sizeof(int));
-	if ((e = cudaMalloc(&h->d_lists, lists.empty() ? 16 : lists.size())))
-		return bail(e, "cudaMalloc(lists)");
-	auto at = [&](int i) { return static_cast<unsigned char*>(h->d_lists) + offs[i]; };
-	h->d_seg1  = reinterpret_cast<dmrgpp::GemmSeg*>(at(0));
-	h->d_seg2  = reinterpret_cast<dmrgpp::GemmSeg*>(at(1));
-	h->d_tile1 = reinterpret_cast<dmrgpp::GemmTile*>(at(2));
-	h->d_tile2 = reinterpret_cast<dmrgpp::GemmTile*>(at(3));
-	h->d_items = reinterpret_cast<dmrgpp::KronItem*>(at(4));
-	h->d_pseg2 = reinterpret_cast<dmrgpp::GemmSeg*>(at(5));
-	h->d_n1    = reinterpret_cast<int*>(at(6));
-	if (!lists.empty()
-	    && (e = cudaMemcpy(h->d_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
-		return bail(e, "upload lists");
-
-	const size_t nctr = 3 + P.np + size_t(P.n_split_tiles);
-	if ((e = cudaMalloc(&h->d_ctr, nctr * sizeof(unsigned))))
-		return bail(e, "cudaMalloc(counters)");
-	if ((e = cudaMemset(h->d_ctr, 0, nctr * sizeof(unsigned))))
-		return bail(e, "clear counters");
-	const size_t part_elems = size_t(P.partial_slots) * size_t(dmrgpp::persistent_tile_elems(bm));
-	if ((e = cudaMalloc(&h->d_part, (part_elems ? part_elems : 1) * sizeof(double))))
-		return bail(e, "cudaMalloc(partials)");
 	if ((e = cudaHostAlloc(reinterpret_cast<void**>(&h->err_host), sizeof(int), cudaHostAllocMapped)))
 		return bail(e, "cudaHostAlloc(error word)");
 	*h->err_host = 0;
 	if ((e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&h->err_dev), h->err_host, 0)))
 		return bail(e, "error word mapping");
+	if (int rc = dmrgpp::configure_schedule(h, bm == 32 ? 0 : 2, 2)) {
+		const std::string why = h->err;
+		release(h);
+		delete h;
+		return fail(nullptr, rc, why);
+	}
 	if (!pack.empty()
 	    && (e = cudaMemcpy(h->d_ops, pack.data(), pack.size() * sizeof(double), cudaMemcpyHostToDevice)))
 		return bail(e, "upload operators");

@@ -28,8 +28,10 @@ struct dmrgpp_kron_s {
 	dmrgpp::GemmTile*   d_tile2 = nullptr;
 	void*               d_lists = nullptr; // one allocation behind every list
 	// persistent single-launch form
+	int                 cfg     = 0;  // tile configuration (kron_persistent.cuh)
 	int                 tile    = 32;
 	int                 grid    = 0;
+	int                 items_per_cta = 2;
 	dmrgpp::KronItem*   d_items = nullptr;
 	dmrgpp::GemmSeg*    d_pseg2 = nullptr;
 	int*                d_n1    = nullptr;
@@ -46,6 +48,10 @@ namespace dmrgpp {
 
 // Enqueues y = H x on h->stream (device pointers); no synchronisation.
 int kron_apply_device(dmrgpp_kron_handle h, const double* x, double* y);
+
+// (Re)builds and uploads the persistent schedule of h for tile configuration
+// cfg (0..kNumTileCfgs-1), aiming at items_per_cta work items per CTA.
+int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta);
 
 // Records msg as the handle's last error and returns status.
 int handle_fail(dmrgpp_kron_handle h, int status, const std::string& msg);

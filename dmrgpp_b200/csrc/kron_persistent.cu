@@ -62,102 +62,125 @@ template <class C>
 __global__ void __launch_bounds__(C::THREADS) kron_persistent_kernel(PersistentArgs a)
 {
 	extern __shared__ __align__(16) double smem[];
-	__shared__ int s_item;
-	__shared__ int s_last;
-	const int      tid = threadIdx.x;
-	tile::Acc<C>   acc;
+	__shared__ __align__(16) KronItem s_w[1];
+	__shared__ __align__(16) GemmSeg  s_seg[kMaxItemSegs];
+	__shared__ int                    s_next;
+	__shared__ int                    s_last;
+	const int                         tid = threadIdx.x;
+	tile::Acc<C>                      acc;
+	constexpr int                     kSegWords = int(sizeof(GemmSeg) / sizeof(int));
+	constexpr int                     kItemVec  = int(sizeof(KronItem) / 16);
+	static_assert(sizeof(KronItem) % 16 == 0, "descriptor copy");
 
+	// Work distribution: the first item of every CTA is its block index;
+	// later items are claimed one at a time, when the previous one is done,
+	// from a counter offset by the grid size.  Claiming only when free keeps
+	// the pass-1 items (which pass-2 items wait on) from queueing behind
+	// long items.
+	const int cur = 0;
+	if (tid == 0)
+		s_next = int(blockIdx.x);
 	for (;;) {
-		if (tid == 0)
-			s_item = int(atomicAdd(&a.work_counter[0], 1u));
 		__syncthreads();
-		const int it = s_item;
-		__syncthreads();
+		const int it = s_next;
 		if (it >= a.n_items)
 			break;
-		const KronItem w = a.items[it];
+		if (tid < kItemVec)
+			reinterpret_cast<int4*>(&s_w[0])[tid] = reinterpret_cast<const int4*>(a.items + it)[tid];
+		__syncthreads();
+		const KronItem& w    = s_w[cur];
+		const int       nseg = w.seg_end - w.seg_begin;
+		if (nseg > 1) {
+			const GemmSeg* gseg = (w.kind == 0 ? a.seg1 : a.pseg2) + w.seg_begin;
+			for (int q = tid; q < nseg * kSegWords; q += C::THREADS)
+				reinterpret_cast<int*>(s_seg)[q] = reinterpret_cast<const int*>(gseg)[q];
+		} else if (tid < kSegWords) {
+			reinterpret_cast<int*>(s_seg)[tid] = reinterpret_cast<const int*>(&w.seg0)[tid];
+		}
+		__syncthreads();
 
 		if (w.kind == 0) {
-			tile::mma_tile<C>(acc, smem, a.ops, a.x, a.seg1, w.seg_begin, w.seg_end, w.m0, w.n0,
-			                  w.M, w.N);
+			tile::mma_tile<C>(acc, smem, a.ops, a.x, s_seg, 0, nseg, w.m0, w.n0, w.M, w.N);
 			store_tile<C>(acc, a.bx + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
 			__syncthreads();
 			if (tid == 0) {
 				__threadfence();
 				atomicAdd(&a.done[w.producer], 1u);
 			}
-			continue;
-		}
-
-		if (tid == 0) {
-			int last_dep = -1;
-			for (int s = w.seg_begin; s < w.seg_end; ++s) {
-				const int j = a.pseg2[s].dep;
-				if (j == last_dep)
-					continue;
-				last_dep              = j;
-				const unsigned target = unsigned(a.n1_of_j[j] + (j == 0 ? a.test_extra_wait : 0));
-				const unsigned long long t0 = globaltimer_ns();
-				while (ld_acquire(&a.done[j]) < target) {
-					if (ld_acquire(&a.work_counter[2]) != 0u)
-						break; // another wait already gave up
-					if (globaltimer_ns() - t0 > kWaitLimitNs) {
-						atomicExch(&a.work_counter[2], 1u);
-						*reinterpret_cast<volatile int*>(a.error) = 1;
-						__threadfence_system();
-						break;
+		} else {
+			if (tid == 0) {
+				int last_dep = -1;
+				for (int s = 0; s < nseg; ++s) {
+					const int j = s_seg[s].dep;
+					if (j == last_dep)
+						continue;
+					last_dep = j;
+					const unsigned target =
+					    unsigned(a.n1_of_j[j] + (j == 0 ? a.test_extra_wait : 0));
+					const unsigned long long t0 = globaltimer_ns();
+					while (ld_acquire(&a.done[j]) < target) {
+						if (ld_acquire(&a.work_counter[2]) != 0u)
+							break; // another wait already gave up
+						if (globaltimer_ns() - t0 > kWaitLimitNs) {
+							atomicExch(&a.work_counter[2], 1u);
+							*reinterpret_cast<volatile int*>(a.error) = 1;
+							__threadfence_system();
+							break;
+						}
+						__nanosleep(128);
 					}
-					__nanosleep(128);
+				}
+			}
+			__syncthreads();
+			tile::mma_tile<C>(acc, smem, a.bx, a.ops, s_seg, 0, nseg, w.m0, w.n0, w.M, w.N);
+			if (w.kind == 1) {
+				store_tile<C>(acc, a.y + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
+			} else {
+				// split part: partial tile to its slot, the last part reduces
+				constexpr int TE   = C::BM * C::BN;
+				double*       part = a.partial + (long long)(w.slot + w.part) * TE;
+#pragma unroll
+				for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+					for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+						for (int h = 0; h < 2; ++h)
+							part[tile::acc_col<C>(ni, h) * C::BM + tile::acc_row<C>(mi)]
+							    = acc.v[mi][ni][h];
+				__syncthreads();
+				if (tid == 0) {
+					__threadfence();
+					const unsigned old = atomicAdd(&a.arrive[w.tile], 1u);
+					s_last             = (old == unsigned(w.nsplit - 1));
+					if (s_last)
+						__threadfence();
+				}
+				__syncthreads();
+				if (s_last) {
+					const double* slots = a.partial + (long long)w.slot * TE;
+					double*       Cp    = a.y + w.c_off;
+#pragma unroll
+					for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+						for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+							for (int h = 0; h < 2; ++h) {
+								const int r   = tile::acc_row<C>(mi);
+								const int c   = tile::acc_col<C>(ni, h);
+								const int e   = c * C::BM + r;
+								double    sum = __ldcg(slots + e);
+								for (int p = 1; p < w.nsplit; ++p)
+									sum += __ldcg(slots + (long long)p * TE + e);
+								const int row = w.m0 + r, col = w.n0 + c;
+								if (row < w.M && col < w.N)
+									Cp[(long long)col * w.ldc + row] = sum;
+							}
 				}
 			}
 		}
-		__syncthreads();
-		tile::mma_tile<C>(acc, smem, a.bx, a.ops, a.pseg2, w.seg_begin, w.seg_end, w.m0, w.n0,
-		                  w.M, w.N);
-		if (w.kind == 1) {
-			store_tile<C>(acc, a.y + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
-			continue;
-		}
-
-		// split part: partial tile to its slot, the last part reduces
-		constexpr int TE = C::BM * C::BN;
-		double*       part = a.partial + (long long)(w.slot + w.part) * TE;
-#pragma unroll
-		for (int mi = 0; mi < C::MI; ++mi)
-#pragma unroll
-			for (int ni = 0; ni < C::NI; ++ni)
-#pragma unroll
-				for (int h = 0; h < 2; ++h)
-					part[tile::acc_col<C>(ni, h) * C::BM + tile::acc_row<C>(mi)] = acc.v[mi][ni][h];
-		__syncthreads();
-		if (tid == 0) {
-			__threadfence();
-			const unsigned old = atomicAdd(&a.arrive[w.tile], 1u);
-			s_last             = (old == unsigned(w.nsplit - 1));
-			if (s_last)
-				__threadfence();
-		}
-		__syncthreads();
-		if (!s_last)
-			continue;
-		const double* slots = a.partial + (long long)w.slot * TE;
-		double*       Cp    = a.y + w.c_off;
-#pragma unroll
-		for (int mi = 0; mi < C::MI; ++mi)
-#pragma unroll
-			for (int ni = 0; ni < C::NI; ++ni)
-#pragma unroll
-				for (int h = 0; h < 2; ++h) {
-					const int r   = tile::acc_row<C>(mi);
-					const int c   = tile::acc_col<C>(ni, h);
-					const int e   = c * C::BM + r;
-					double    sum = __ldcg(slots + e);
-					for (int p = 1; p < w.nsplit; ++p)
-						sum += __ldcg(slots + (long long)p * TE + e);
-					const int row = w.m0 + r, col = w.n0 + c;
-					if (row < w.M && col < w.N)
-						Cp[(long long)col * w.ldc + row] = sum;
-				}
+		__syncthreads(); // everyone is done with s_w and s_seg
+		if (tid == 0)
+			s_next = int(gridDim.x + atomicAdd(&a.work_counter[0], 1u));
 	}
 
 	// the last CTA out returns every counter to zero for the next launch
@@ -177,8 +200,13 @@ __global__ void __launch_bounds__(C::THREADS) kron_persistent_kernel(PersistentA
 	}
 }
 
-using PCfg32 = tile::Cfg<32, 32, 16, 16, 16, 4>;
-using PCfg64 = tile::Cfg<64, 64, 16, 32, 32, 3>;
+// Tile configurations a handle can run (kron_persistent.cuh, KronTileCfg).
+using PCfg0 = tile::Cfg<32, 32, 16, 16, 16, 4>;
+using PCfg1 = tile::Cfg<32, 32, 32, 16, 16, 3>;
+using PCfg2 = tile::Cfg<64, 64, 16, 32, 32, 3>;
+using PCfg3 = tile::Cfg<64, 64, 32, 32, 32, 3>;
+using PCfg4 = tile::Cfg<32, 32, 32, 16, 16, 4>;
+using PCfg5 = tile::Cfg<32, 32, 64, 16, 16, 3>;
 
 template <class C> cudaError_t init_one(int* blocks_per_sm)
 {
@@ -190,9 +218,15 @@ template <class C> cudaError_t init_one(int* blocks_per_sm)
 	                                                     C::THREADS, C::SMEM);
 }
 
+template <class C> void describe(int* tile, int* bk)
+{
+	*tile = C::BM;
+	*bk   = C::BK;
+}
+
 } // namespace
 
-cudaError_t persistent_config(int tile, int* grid, int* bk)
+cudaError_t persistent_config(int cfg, int* grid, int* tile, int* bk)
 {
 	int         dev = 0, sms = 0, per_sm = 0;
 	cudaError_t e = cudaGetDevice(&dev);
@@ -200,14 +234,14 @@ cudaError_t persistent_config(int tile, int* grid, int* bk)
 		e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	if (e != cudaSuccess)
 		return e;
-	if (tile == 32) {
-		e   = init_one<PCfg32>(&per_sm);
-		*bk = PCfg32::BK;
-	} else if (tile == 64) {
-		e   = init_one<PCfg64>(&per_sm);
-		*bk = PCfg64::BK;
-	} else {
-		return cudaErrorInvalidValue;
+	switch (cfg) {
+	case 0: e = init_one<PCfg0>(&per_sm); describe<PCfg0>(tile, bk); break;
+	case 1: e = init_one<PCfg1>(&per_sm); describe<PCfg1>(tile, bk); break;
+	case 2: e = init_one<PCfg2>(&per_sm); describe<PCfg2>(tile, bk); break;
+	case 3: e = init_one<PCfg3>(&per_sm); describe<PCfg3>(tile, bk); break;
+	case 4: e = init_one<PCfg4>(&per_sm); describe<PCfg4>(tile, bk); break;
+	case 5: e = init_one<PCfg5>(&per_sm); describe<PCfg5>(tile, bk); break;
+	default: return cudaErrorInvalidValue;
 	}
 	if (e != cudaSuccess)
 		return e;
@@ -215,19 +249,20 @@ cudaError_t persistent_config(int tile, int* grid, int* bk)
 	return cudaSuccess;
 }
 
-int persistent_tile_elems(int tile) { return tile * tile; }
-
-cudaError_t launch_persistent(const PersistentArgs& a, int tile, int grid, cudaStream_t stream)
+cudaError_t launch_persistent(const PersistentArgs& a, int cfg, int grid, cudaStream_t stream)
 {
 	if (a.n_items <= 0)
 		return cudaSuccess;
 	const int g = grid < a.n_items ? grid : a.n_items;
-	if (tile == 32)
-		kron_persistent_kernel<PCfg32><<<g, PCfg32::THREADS, PCfg32::SMEM, stream>>>(a);
-	else if (tile == 64)
-		kron_persistent_kernel<PCfg64><<<g, PCfg64::THREADS, PCfg64::SMEM, stream>>>(a);
-	else
-		return cudaErrorInvalidValue;
+	switch (cfg) {
+	case 0: kron_persistent_kernel<PCfg0><<<g, PCfg0::THREADS, PCfg0::SMEM, stream>>>(a); break;
+	case 1: kron_persistent_kernel<PCfg1><<<g, PCfg1::THREADS, PCfg1::SMEM, stream>>>(a); break;
+	case 2: kron_persistent_kernel<PCfg2><<<g, PCfg2::THREADS, PCfg2::SMEM, stream>>>(a); break;
+	case 3: kron_persistent_kernel<PCfg3><<<g, PCfg3::THREADS, PCfg3::SMEM, stream>>>(a); break;
+	case 4: kron_persistent_kernel<PCfg4><<<g, PCfg4::THREADS, PCfg4::SMEM, stream>>>(a); break;
+	case 5: kron_persistent_kernel<PCfg5><<<g, PCfg5::THREADS, PCfg5::SMEM, stream>>>(a); break;
+	default: return cudaErrorInvalidValue;
+	}
 	return cudaGetLastError();
 }
 

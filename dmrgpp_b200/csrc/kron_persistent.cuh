@@ -27,12 +27,16 @@ struct PersistentArgs {
 	int             test_extra_wait; // 0; >0 makes waits on patch 0 unsatisfiable (tests)
 };
 
-// Sets kernel attributes on the current device and returns the persistent
-// grid (SMs x resident CTAs) and the k-chunk of the tile configuration.
-cudaError_t persistent_config(int tile, int* grid, int* bk);
+// Tile configurations (output tile, k-chunk, pipeline depth):
+//   0: 32x32, k16, 4 stages   1: 32x32, k32, 3 stages
+//   2: 64x64, k16, 3 stages   3: 64x64, k32, 3 stages
+//   4: 32x32, k32, 4 stages   5: 32x32, k64, 3 stages
+constexpr int kNumTileCfgs = 6;
 
-int persistent_tile_elems(int tile);
+// Sets kernel attributes of configuration cfg on the current device and
+// returns its persistent grid (SMs x resident CTAs), tile edge and k-chunk.
+cudaError_t persistent_config(int cfg, int* grid, int* tile, int* bk);
 
-cudaError_t launch_persistent(const PersistentArgs& a, int tile, int grid, cudaStream_t stream);
+cudaError_t launch_persistent(const PersistentArgs& a, int cfg, int grid, cudaStream_t stream);
 
 } // namespace dmrgpp

@@ -68,6 +68,55 @@ void order_tiles(std::vector<GemmTile>& tiles, const std::vector<GemmSeg>& segs)
 
 } // namespace
 
+void build_tile_lists(KronPlan& plan, int bm, int bn)
+{
+	const size_t np = plan.np;
+	const size_t nt = plan.triples.size();
+	plan.bm         = bm;
+	plan.bn         = bn;
+	plan.seg1.clear();
+	plan.seg2.clear();
+	plan.tile1.clear();
+	plan.tile2.clear();
+	// pass 1: one segment and a tile grid per input patch with work
+	for (size_t j = 0; j < np; ++j) {
+		if (plan.M[j] == 0)
+			continue;
+		GemmSeg s {};
+		s.a_off = plan.bstack_off[j];
+		s.lda   = int(plan.M[j]);
+		s.b_off = plan.xy_start[j];
+		s.ldb   = int(plan.r[j]);
+		s.K     = int(plan.r[j]);
+		s.dep   = int(j);
+		const int sb = int(plan.seg1.size());
+		plan.seg1.push_back(s);
+		add_tiles(plan.tile1, plan.bx_off[j], plan.M[j], plan.M[j], plan.l[j], sb, sb + 1, bm, bn);
+	}
+	order_tiles(plan.tile1, plan.seg1);
+
+	// pass 2: per output patch, the (j,k) segments in plugin order; a patch
+	// without contributions still gets tiles so Y_i is overwritten with 0
+	size_t t = 0;
+	for (size_t i = 0; i < np; ++i) {
+		const int sb = int(plan.seg2.size());
+		for (; t < nt && plan.triples[t].i == int(i); ++t) {
+			const Triple& tr = plan.triples[t];
+			GemmSeg       s {};
+			s.a_off = plan.bx_off[tr.j] + plan.row_off[t];
+			s.lda   = int(plan.M[tr.j]);
+			s.b_off = plan.at_off[t];
+			s.ldb   = int(plan.l[tr.j]);
+			s.K     = int(plan.l[tr.j]);
+			s.dep   = tr.j;
+			plan.seg2.push_back(s);
+		}
+		const int se = int(plan.seg2.size());
+		add_tiles(plan.tile2, plan.xy_start[i], plan.r[i], plan.r[i], plan.l[i], sb, se, bm, bn);
+	}
+	order_tiles(plan.tile2, plan.seg2);
+}
+
 std::string build_kron_plan(size_t               noperator,
                             size_t               npatches,
                             const size_t*        lsz,
@@ -184,47 +233,11 @@ std::string build_kron_plan(size_t               noperator,
 		}
 	}
 
-	// pass 1: one segment and a tile grid per input patch with work
-	for (size_t j = 0; j < np; ++j) {
-		if (plan.M[j] == 0)
-			continue;
-		GemmSeg s {};
-		s.a_off = plan.bstack_off[j];
-		s.lda   = int(plan.M[j]);
-		s.b_off = plan.xy_start[j];
-		s.ldb   = int(plan.r[j]);
-		s.K     = int(plan.r[j]);
-		s.dep   = int(j);
-		const int sb = int(plan.seg1.size());
-		plan.seg1.push_back(s);
-		add_tiles(plan.tile1, plan.bx_off[j], plan.M[j], plan.M[j], plan.l[j], sb, sb + 1, bm, bn);
-	}
-	order_tiles(plan.tile1, plan.seg1);
-
-	// pass 2: per output patch, the (j,k) segments in plugin order; a patch
-	// without contributions still gets tiles so Y_i is overwritten with 0
-	size_t t = 0;
-	for (size_t i = 0; i < np; ++i) {
-		const int sb = int(plan.seg2.size());
-		for (; t < nt && plan.triples[t].i == int(i); ++t) {
-			const Triple& tr = plan.triples[t];
-			GemmSeg       s {};
-			s.a_off = plan.bx_off[tr.j] + plan.row_off[t];
-			s.lda   = int(plan.M[tr.j]);
-			s.b_off = plan.at_off[t];
-			s.ldb   = int(plan.l[tr.j]);
-			s.K     = int(plan.l[tr.j]);
-			s.dep   = tr.j;
-			plan.seg2.push_back(s);
-		}
-		const int se = int(plan.seg2.size());
-		add_tiles(plan.tile2, plan.xy_start[i], plan.r[i], plan.r[i], plan.l[i], sb, se, bm, bn);
-	}
-	order_tiles(plan.tile2, plan.seg2);
+	build_tile_lists(plan, bm, bn);
 	return std::string();
 }
 
-void build_persistent_schedule(KronPlan& plan, int bk, int grid)
+void build_persistent_schedule(KronPlan& plan, int bk, int grid, int items_per_cta)
 {
 	plan.items.clear();
 	plan.pseg2.clear();
@@ -249,15 +262,17 @@ void build_persistent_schedule(KronPlan& plan, int bk, int grid)
 	}
 	plan.n1_items = int(plan.items.size());
 
-	// K-slice length: none when the tiles alone give ~2 items per CTA,
-	// otherwise aim at ~2 pass-2 items per CTA, at least 4 chunks each
+	// K-slice length: none when the tiles alone give `items_per_cta` items per
+	// CTA, otherwise aim at that many pass-2 items per CTA, at least 4 chunks
+	// each; no item holds more than kMaxItemSegs segments
 	long long total_k = 0;
 	for (const GemmTile& t : plan.tile2)
 		for (int s = t.seg_begin; s < t.seg_end; ++s)
 			total_k += plan.seg2[s].K;
 	long long k_target = 1LL << 40;
-	if ((long long)plan.tile2.size() < 2LL * grid && grid > 0) {
-		k_target = total_k / (2LL * grid);
+	const long long want = (long long)items_per_cta * grid;
+	if ((long long)plan.tile2.size() < want && grid > 0) {
+		k_target = total_k / want;
 		k_target = std::max<long long>(k_target, 4LL * bk);
 		k_target = (k_target + bk - 1) / bk * bk;
 	}
@@ -271,9 +286,7 @@ void build_persistent_schedule(KronPlan& plan, int bk, int grid)
 		int nsplit = int(std::min<long long>((kt + k_target - 1) / k_target, max_split));
 		nsplit     = std::max(nsplit, 1);
 		long long chunk = (kt + nsplit - 1) / nsplit;
-		chunk           = (chunk + bk - 1) / bk * bk;
-		if (chunk > 0)
-			nsplit = int(std::max<long long>(1, (kt + chunk - 1) / chunk));
+		chunk           = std::max<long long>(bk, (chunk + bk - 1) / bk * bk);
 
 		KronItem base {};
 		base.c_off = t.c_off;
@@ -282,32 +295,19 @@ void build_persistent_schedule(KronPlan& plan, int bk, int grid)
 		base.N     = t.N;
 		base.m0    = t.m0;
 		base.n0    = t.n0;
-		if (nsplit == 1) {
-			base.kind      = 1;
-			base.seg_begin = int(plan.pseg2.size());
-			for (int s = t.seg_begin; s < t.seg_end; ++s)
-				plan.pseg2.push_back(plan.seg2[s]);
-			base.seg_end = int(plan.pseg2.size());
-			p2.push_back(base);
-			continue;
-		}
-		base.kind   = 2;
-		base.tile   = plan.n_split_tiles++;
-		base.nsplit = nsplit;
-		base.slot   = int(plan.partial_slots);
-		plan.partial_slots += nsplit;
-		// walk the tile's segments, cutting them into parts of `chunk` K
+		// cut the tile's segments into parts of `chunk` K (and <= kMaxItemSegs pieces)
+		std::vector<KronItem> parts;
 		int       s  = t.seg_begin;
 		long long k0 = 0; // offset inside segment s
-		for (int part = 0; part < nsplit; ++part) {
+		do {
 			KronItem w  = base;
-			w.part      = part;
 			w.seg_begin = int(plan.pseg2.size());
 			long long need = chunk;
-			while (need > 0 && s < t.seg_end) {
-				const GemmSeg& g    = plan.seg2[s];
+			while (need > 0 && s < t.seg_end
+			       && int(plan.pseg2.size()) - w.seg_begin < kMaxItemSegs) {
+				const GemmSeg&  g    = plan.seg2[s];
 				const long long take = std::min<long long>(need, g.K - k0);
-				GemmSeg        piece = g;
+				GemmSeg         piece = g;
 				piece.a_off += k0 * g.lda; // A = BX_j columns k0..
 				piece.b_off += k0;         // B = A^T rows k0.. (K-contiguous)
 				piece.K = int(take);
@@ -320,8 +320,23 @@ void build_persistent_schedule(KronPlan& plan, int bk, int grid)
 				}
 			}
 			w.seg_end = int(plan.pseg2.size());
-			p2.push_back(w);
+			parts.push_back(w);
+		} while (s < t.seg_end);
+		if (parts.size() == 1) {
+			parts[0].kind = 1;
+			p2.push_back(parts[0]);
+			continue;
 		}
+		const int tile_id = plan.n_split_tiles++;
+		for (size_t q = 0; q < parts.size(); ++q) {
+			parts[q].kind   = 2;
+			parts[q].tile   = tile_id;
+			parts[q].nsplit = int(parts.size());
+			parts[q].slot   = int(plan.partial_slots);
+			parts[q].part   = int(q);
+			p2.push_back(parts[q]);
+		}
+		plan.partial_slots += (long long)parts.size();
 	}
 	auto cost = [&](const KronItem& w) {
 		long long k = 0;
@@ -332,6 +347,11 @@ void build_persistent_schedule(KronPlan& plan, int bk, int grid)
 	std::stable_sort(p2.begin(), p2.end(),
 	                 [&](const KronItem& a, const KronItem& b) { return cost(a) > cost(b); });
 	plan.items.insert(plan.items.end(), p2.begin(), p2.end());
+	for (KronItem& w : plan.items) {
+		const std::vector<GemmSeg>& segs = w.kind == 0 ? plan.seg1 : plan.pseg2;
+		if (w.seg_end > w.seg_begin)
+			w.seg0 = segs[size_t(w.seg_begin)];
+	}
 }
 
 } // namespace dmrgpp

@@ -52,6 +52,7 @@ struct alignas(16) GemmTile {
 //           partial result goes to slot `slot + part`, the last part to
 //           arrive sums the slots in order 0..nsplit-1 and writes the tile
 struct alignas(16) KronItem {
+	GemmSeg   seg0; // copy of the first segment (most items have only one)
 	long long c_off;
 	int       ldc;
 	int       M;
@@ -123,9 +124,16 @@ std::string build_kron_plan(size_t               noperator,
                             KronPlan&            plan,
                             std::vector<double>* pack_host);
 
+// (Re)builds the two-launch tile lists seg1/tile1/seg2/tile2 of a planned
+// sector for bm x bn output tiles.
+void build_tile_lists(KronPlan& plan, int bm, int bn);
+
+// Most K-segments one work item may hold (they are staged in shared memory).
+constexpr int kMaxItemSegs = 32;
+
 // Builds plan.items / pseg2 / n1_of_j for a persistent launch of `grid`
 // CTAs: pass-2 output tiles are cut into K-slices (multiples of bk, on any
-// k boundary) when there are too few tiles to keep every CTA busy.
-void build_persistent_schedule(KronPlan& plan, int bk, int grid);
+// k boundary) when there are fewer than items_per_cta tiles per CTA.
+void build_persistent_schedule(KronPlan& plan, int bk, int grid, int items_per_cta = 2);
 
 } // namespace dmrgpp

@@ -156,6 +156,25 @@ class BatchedGemm:
         _capi.check(rc, self._h)
         return e.value, z, int(n.value)
 
+    def autotune(self, cache_path: Optional[str] = None, reps: int = 10):
+        """Picks the fastest tile configuration / work split for this sector
+        (cached by sector shape in cache_path).  Returns (cfg, microseconds)."""
+        cfg = ctypes.c_int()
+        us = ctypes.c_double()
+        path = cache_path.encode() if cache_path else None
+        _capi.check(self._lib.dmrgpp_kron_autotune(self._h, path, reps, ctypes.byref(cfg),
+                                                   ctypes.byref(us)), self._h)
+        return cfg.value, us.value
+
+    def set_config(self, cfg: int, items_per_cta: int = 2) -> None:
+        _capi.check(self._lib.dmrgpp_kron_set_config(self._h, cfg, items_per_cta), self._h)
+
+    def get_config(self):
+        c, i = ctypes.c_int(), ctypes.c_int()
+        _capi.check(self._lib.dmrgpp_kron_get_config(self._h, ctypes.byref(c), ctypes.byref(i)),
+                    self._h)
+        return c.value, i.value
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.dmrgpp_kron_destroy(self._h)

@@ -202,3 +202,54 @@ def random_problem(npatches: int, noperator: int, max_size: int = 12, seed: int 
 def random_unit_vector(dim: int, seed: int = 1) -> np.ndarray:
     v = np.random.default_rng(seed).standard_normal(dim)
     return v / np.linalg.norm(v)
+
+
+def ladder_problem(total_states: int = 16000, sigma: float = 2.5, seed: int = 20261203,
+                   min_group: int = 1, name: str = "") -> KronProblem:
+    """Sector shaped like a two-leg Hubbard ladder superblock at m ~ 4000
+    (left and right blocks of `total_states` states each, 4 states per site).
+    Left groups are (N_up, N_down) pairs whose sizes follow a 2-D discretised
+    Gaussian (width sigma in particle number); patch p pairs left group
+    (nu, nd) with the right group that completes the target (N_up, N_down),
+    whose size follows the same histogram.  K = 10 terms: H_L x I, I x H_R and
+    8 hopping terms c^dag_{s,leg} x c_{s,leg} (2 spins x 2 legs x 2
+    directions), each moving one particle of one spin across the boundary,
+    so it couples patches whose (nu, nd) differ by one.  Blocks are dense
+    N(0,1) (H_L, H_R symmetrised; the two directions are transposes), the
+    synthetic stand-in for operators of a real sweep."""
+    rng = np.random.default_rng(seed)
+    R = int(np.ceil(4 * sigma))
+    qs = [(a, b) for a in range(-R, R + 1) for b in range(-R, R + 1)]
+    w = np.array([np.exp(-(a * a + b * b) / (2 * sigma * sigma)) for a, b in qs])
+    n = np.floor(total_states * w / w.sum()).astype(np.int64)
+    n[np.argmax(w)] += total_states - int(n.sum())
+    keep = [i for i in range(len(qs)) if n[i] >= min_group]
+    qs = [qs[i] for i in keep]
+    n = n[keep]
+    index = {q: p for p, q in enumerate(qs)}
+    l = n.copy()
+    r = np.array([n[index[(-a, -b)]] for a, b in qs], dtype=np.int64)
+    A, B = {}, {}
+    for p in range(len(qs)):
+        A[(p, p, 0)] = _sym(rng, l[p])
+        B[(p, p, 0)] = np.asfortranarray(np.eye(r[p]))
+        A[(p, p, 1)] = np.asfortranarray(np.eye(l[p]))
+        B[(p, p, 1)] = _sym(rng, r[p])
+    k = 2
+    for spin in range(2):
+        for leg in range(2):
+            for p, (a, b) in enumerate(qs):
+                q_to = (a + 1, b) if spin == 0 else (a, b + 1)
+                if q_to not in index:
+                    continue
+                q = index[q_to]
+                cd = rng.standard_normal((l[q], l[p]))  # c^dag on the left: p -> q
+                c = rng.standard_normal((r[q], r[p]))   # c on the right
+                A[(q, p, k)] = np.asfortranarray(cd)
+                B[(q, p, k)] = np.asfortranarray(c)
+                A[(p, q, k + 1)] = np.asfortranarray(cd.T)
+                B[(p, q, k + 1)] = np.asfortranarray(c.T)
+            k += 2
+    return KronProblem(l, r, 10, A, B,
+                       name=name or f"hubbard-ladder-like-{total_states}x{total_states}-"
+                                    f"{len(qs)}sec-K10")

@@ -152,6 +152,23 @@ int dmrgpp_kron_plan_info_get(const dmrgpp_kron_desc* desc, dmrgpp_kron_plan_inf
 int dmrgpp_kron_apply_noalloc(const dmrgpp_kron_desc* desc, const double* x, double* y);
 const char* dmrgpp_kron_noalloc_last_error(void);
 
+/* ---- Launch tuning (no counterpart in the reference, whose GPU tiling is a
+ * set of fixed constants, BatchedGemmKokkos.h:110-130) ----
+ * Tile configurations of the H*x kernel: 0: 32x32 tiles, k-chunk 16;
+ * 1: 32x32, k32; 2: 64x64, k16; 3: 64x64, k32; 4: 32x32, k32, deeper
+ * pipeline; 5: 32x32, k64.  items_per_cta: pass-2 work
+ * items per resident CTA below which output tiles are split along K. */
+int dmrgpp_kron_get_config(dmrgpp_kron_handle h, int* cfg, int* items_per_cta);
+int dmrgpp_kron_set_config(dmrgpp_kron_handle h, int cfg, int items_per_cta);
+
+/* Times every configuration on this sector (reps applies each, minimum
+ * kept), keeps the fastest and returns it with its time in microseconds.
+ * cache_path (may be NULL): text file of earlier choices keyed by a
+ * signature of the sector-size histogram and the GPU name; a hit skips the
+ * timing, a miss appends the new choice. */
+int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps, int* cfg,
+                         double* us);
+
 /* ---- Eigensolver on the device (replaces PsimagLite::LanczosSolver for one
  * sector, PsimagLite/src/PsimagLite/LanczosSolver.h:68-88 with
  * LanczosCore.h:147-272 and LanczosVectors.h:192-271) ---- */

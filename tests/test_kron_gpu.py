@@ -157,3 +157,47 @@ def test_device_pointer_applies_then_synchronize(cuda_lib, cuda_device, oracle_b
     for x, y in zip(xs, yd):
         assert rel_err(y.cpu().numpy(), oracle_built.kron_apply(prob, x)) < RTOL
     bg.close()
+
+
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("ipc", [1, 4])
+def test_every_tile_configuration(cuda_lib, cuda_device, oracle_built, cfg, ipc):
+    """Each tile configuration / work split of the persistent kernel, on a
+    sector with ragged patches (1..150) and many K-segments per output tile."""
+    from dmrgpp_b200 import plugin
+    prob = sb.random_problem(npatches=12, noperator=4, max_size=150, seed=40 + cfg,
+                             density=0.6, zero_block_rate=0.1)
+    x = np.random.default_rng(cfg).standard_normal(prob.dim)
+    bg = plugin.BatchedGemm.from_problem(prob)
+    bg.set_config(cfg, ipc)
+    assert bg.get_config() == (cfg, ipc)
+    y = bg(x)
+    assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL
+    assert np.array_equal(bg(x), y)
+    bg.close()
+
+
+def test_autotune_then_cache_hit(cuda_lib, cuda_device, oracle_built, tmp_path):
+    from dmrgpp_b200 import plugin
+    prob = sb.c2_problem()
+    x = sb.random_unit_vector(prob.dim, seed=12)
+    cache = str(tmp_path / "tune.txt")
+    bg = plugin.BatchedGemm.from_problem(prob)
+    cfg, us = bg.autotune(cache, reps=3)
+    assert 0 <= cfg <= 5 and us > 0
+    assert rel_err(bg(x), oracle_built.kron_apply(prob, x)) < RTOL
+    bg.close()
+    lines = open(cache).read().split("\n")
+    assert len([ln for ln in lines if ln.strip()]) == 1
+    bg2 = plugin.BatchedGemm.from_problem(prob)
+    cfg2, us2 = bg2.autotune(cache, reps=3)      # cache hit: same choice, no new line
+    assert (cfg2, us2) == (cfg, pytest.approx(us, rel=1e-6))
+    assert len([ln for ln in open(cache).read().split("\n") if ln.strip()]) == 1
+    bg2.close()
+
+
+def test_ladder_shaped_sector(cuda_lib, cuda_device, oracle_built):
+    prob = sb.ladder_problem(total_states=1500, sigma=2.0, seed=3)
+    x = np.random.default_rng(5).standard_normal(prob.dim)
+    y = gpu_apply(prob, x)
+    assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL
