@@ -45,6 +45,7 @@ SIGNATURES = {
                                          ctypes.c_int]),
     "dmrgpp_kron_dim": (ctypes.c_int, [ctypes.c_void_p, _szp]),
     "dmrgpp_kron_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "dmrgpp_kron_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dmrgpp_kron_test_stall_dependency": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dmrgpp_kron_flops": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "dmrgpp_kron_plan_info_get": (ctypes.c_int, [ctypes.POINTER(KronDesc),

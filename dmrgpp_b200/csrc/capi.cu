@@ -4,9 +4,11 @@
 #include "kron_persistent.cuh"
 #include "kron_plan.h"
 #include "handle.h"
+#include "tc_gemm.cuh"
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -61,6 +63,18 @@ void release(dmrgpp_kron_handle h)
 	if (!h)
 		return;
 	dmrgpp::release_lanczos(h);
+	cudaFree(h->m_ops_hi);
+	cudaFree(h->m_ops_lo);
+	cudaFree(h->m_xs_hi);
+	cudaFree(h->m_xs_lo);
+	cudaFree(h->m_bxs_hi);
+	cudaFree(h->m_bxs_lo);
+	cudaFree(h->m_xmap);
+	cudaFree(h->m_lists);
+	h->m_ops_hi = h->m_ops_lo = h->m_xs_hi = h->m_xs_lo = h->m_bxs_hi = h->m_bxs_lo = nullptr;
+	h->m_xmap   = nullptr;
+	h->m_lists  = nullptr;
+	h->mixed_ready = false;
 	cudaFree(h->d_ops);
 	cudaFree(h->d_bx);
 	cudaFree(h->d_x);
@@ -105,8 +119,9 @@ int check_desc(const dmrgpp_kron_desc* d)
 	return DMRGPP_OK;
 }
 
-// After the stream has drained: a wait inside the persistent kernel that
-// gave up leaves its counters dirty; report it and restore a clean state.
+// After the stream has drained: a wait inside a kernel that gave up (the
+// persistent kernel leaves its counters dirty); report it and restore a
+// clean state.
 int check_error_word(dmrgpp_kron_handle h)
 {
 	if (!h->err_host || *reinterpret_cast<volatile int*>(h->err_host) == 0)
@@ -115,7 +130,7 @@ int check_error_word(dmrgpp_kron_handle h)
 	const size_t nctr = 3 + h->plan.np + size_t(h->plan.n_split_tiles);
 	cudaMemsetAsync(h->d_ctr, 0, nctr * sizeof(unsigned), h->stream);
 	cudaStreamSynchronize(h->stream);
-	return fail(h, DMRGPP_TIMEOUT, "a dependency wait in the H*x kernel gave up; result invalid");
+	return fail(h, DMRGPP_TIMEOUT, "a bounded wait in an H*x kernel gave up; result invalid");
 }
 
 } // namespace
@@ -127,8 +142,44 @@ int handle_fail(dmrgpp_kron_handle h, int status, const std::string& msg)
 	return fail(h, status, msg);
 }
 
+int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
+{
+	const MixedPlan& mp = h->plan.mixed;
+	cudaError_t      e;
+	if ((e = tc_split_x(X, h->m_xmap, h->m_xs_hi, h->m_xs_lo, h->plan.dim(), h->stream)))
+		return cuda_fail(h, e, "x split launch");
+	TcArgs a1 {};
+	a1.A_hi   = h->m_ops_hi;
+	a1.A_lo   = h->m_ops_lo;
+	a1.B_hi   = h->m_xs_hi;
+	a1.B_lo   = h->m_xs_lo;
+	a1.C_hi   = h->m_bxs_hi;
+	a1.C_lo   = h->m_bxs_lo;
+	a1.segs   = h->m_seg1;
+	a1.tiles  = h->m_tile1;
+	a1.ntiles = int(mp.tile1.size());
+	a1.error  = h->err_dev;
+	if ((e = tc_launch(a1, mp.bn, true, h->stream)))
+		return cuda_fail(h, e, "tensor-core pass 1 launch");
+	TcArgs a2 {};
+	a2.A_hi   = h->m_bxs_hi;
+	a2.A_lo   = h->m_bxs_lo;
+	a2.B_hi   = h->m_ops_hi;
+	a2.B_lo   = h->m_ops_lo;
+	a2.Cd     = Y;
+	a2.segs   = h->m_seg2;
+	a2.tiles  = h->m_tile2;
+	a2.ntiles = int(mp.tile2.size());
+	a2.error  = h->err_dev;
+	if ((e = tc_launch(a2, mp.bn, false, h->stream)))
+		return cuda_fail(h, e, "tensor-core pass 2 launch");
+	return DMRGPP_OK;
+}
+
 int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 {
+	if (h->precision == DMRGPP_TF32X3)
+		return mixed_apply_device(h, X, Y);
 	const auto& P = h->plan;
 	cudaError_t e;
 	dmrgpp::PersistentArgs pa {};
@@ -153,6 +204,67 @@ int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 		return cuda_fail(h, e, "H*x launch");
 	return DMRGPP_OK;
 
+}
+
+int build_mixed(dmrgpp_kron_handle h, const dmrgpp_kron_desc* d)
+{
+	std::vector<float> hi, lo;
+	std::vector<int>   xmap;
+	size_t             maxs = 0;
+	for (size_t p = 0; p < h->plan.np; ++p)
+		maxs = std::max<size_t>(maxs, size_t(std::max(h->plan.l[p], h->plan.r[p])));
+	const int   bn  = maxs > 96 ? 128 : 64;
+	std::string msg = build_mixed_plan(h->plan, d->Amatrix, d->ld_Amatrix, d->Bmatrix,
+	                                   d->ld_Bmatrix, bn, &hi, &lo, &xmap);
+	if (!msg.empty())
+		return fail(h, DMRGPP_INVALID_ARG, msg);
+	const MixedPlan& mp = h->plan.mixed;
+	cudaError_t      e  = tc_init();
+	if (e != cudaSuccess)
+		return cuda_fail(h, e, "tensor-core kernel attributes");
+	auto fbytes = [](long long n) { return size_t(n > 0 ? n : 1) * sizeof(float); };
+	if ((e = cudaMalloc(&h->m_ops_hi, fbytes(mp.ops_elems))) || (e = cudaMalloc(&h->m_ops_lo, fbytes(mp.ops_elems)))
+	    || (e = cudaMalloc(&h->m_xs_hi, fbytes(mp.xs_elems))) || (e = cudaMalloc(&h->m_xs_lo, fbytes(mp.xs_elems)))
+	    || (e = cudaMalloc(&h->m_bxs_hi, fbytes(mp.bxs_elems)))
+	    || (e = cudaMalloc(&h->m_bxs_lo, fbytes(mp.bxs_elems)))
+	    || (e = cudaMalloc(&h->m_xmap, size_t(std::max<long long>(h->plan.dim(), 1)) * sizeof(int))))
+		return cuda_fail(h, e, "cudaMalloc(mixed-precision buffers)");
+	// K padding must read as zero
+	if ((e = cudaMemset(h->m_xs_hi, 0, fbytes(mp.xs_elems))) || (e = cudaMemset(h->m_xs_lo, 0, fbytes(mp.xs_elems)))
+	    || (e = cudaMemset(h->m_bxs_hi, 0, fbytes(mp.bxs_elems)))
+	    || (e = cudaMemset(h->m_bxs_lo, 0, fbytes(mp.bxs_elems))))
+		return cuda_fail(h, e, "clear mixed-precision buffers");
+	if (!hi.empty()
+	    && ((e = cudaMemcpy(h->m_ops_hi, hi.data(), hi.size() * sizeof(float), cudaMemcpyHostToDevice))
+	        || (e = cudaMemcpy(h->m_ops_lo, lo.data(), lo.size() * sizeof(float), cudaMemcpyHostToDevice))))
+		return cuda_fail(h, e, "upload mixed-precision operators");
+	if (!xmap.empty()
+	    && (e = cudaMemcpy(h->m_xmap, xmap.data(), xmap.size() * sizeof(int), cudaMemcpyHostToDevice)))
+		return cuda_fail(h, e, "upload x map");
+	std::vector<unsigned char> lists;
+	std::vector<size_t>        offs;
+	auto add = [&](const void* src, size_t n) {
+		offs.push_back(lists.size());
+		lists.resize(lists.size() + ((n + 15) / 16) * 16);
+		if (n)
+			std::memcpy(lists.data() + offs.back(), src, n);
+	};
+	add(mp.seg1.data(), mp.seg1.size() * sizeof(GemmSeg));
+	add(mp.seg2.data(), mp.seg2.size() * sizeof(GemmSeg));
+	add(mp.tile1.data(), mp.tile1.size() * sizeof(GemmTile));
+	add(mp.tile2.data(), mp.tile2.size() * sizeof(GemmTile));
+	if ((e = cudaMalloc(&h->m_lists, lists.empty() ? 16 : lists.size())))
+		return cuda_fail(h, e, "cudaMalloc(mixed lists)");
+	auto at    = [&](int i) { return static_cast<unsigned char*>(h->m_lists) + offs[i]; };
+	h->m_seg1  = reinterpret_cast<GemmSeg*>(at(0));
+	h->m_seg2  = reinterpret_cast<GemmSeg*>(at(1));
+	h->m_tile1 = reinterpret_cast<GemmTile*>(at(2));
+	h->m_tile2 = reinterpret_cast<GemmTile*>(at(3));
+	if (!lists.empty()
+	    && (e = cudaMemcpy(h->m_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
+		return cuda_fail(h, e, "upload mixed lists");
+	h->mixed_ready = true;
+	return DMRGPP_OK;
 }
 
 int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
@@ -268,8 +380,8 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 	*out = nullptr;
 	if (int rc = check_desc(d))
 		return rc;
-	if (d->precision != DMRGPP_FP64)
-		return fail(nullptr, DMRGPP_NOT_SUPPORTED, "precision mode not built into this library");
+	if (d->precision == DMRGPP_SPLIT_BF16)
+		return fail(nullptr, DMRGPP_NOT_SUPPORTED, "split-BF16 is not built into this library");
 
 	dmrgpp_kron_handle h = new (std::nothrow) dmrgpp_kron_s();
 	if (!h)
@@ -343,6 +455,14 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 	if (!pack.empty()
 	    && (e = cudaMemcpy(h->d_ops, pack.data(), pack.size() * sizeof(double), cudaMemcpyHostToDevice)))
 		return bail(e, "upload operators");
+	if (d->precision == DMRGPP_TF32X3) {
+		if (int rc = dmrgpp::build_mixed(h, d)) {
+			const std::string why = h->err;
+			release(h);
+			delete h;
+			return fail(nullptr, rc, why);
+		}
+	}
 	*out = h;
 	return DMRGPP_OK;
 }
@@ -411,6 +531,18 @@ int dmrgpp_kron_test_stall_dependency(dmrgpp_kron_handle h, int on)
 		return fail(nullptr, DMRGPP_INVALID_ARG, "null handle");
 	h->test_stall = on ? 1 : 0;
 	return DMRGPP_OK;
+}
+
+int dmrgpp_kron_set_precision(dmrgpp_kron_handle h, int precision)
+{
+	if (!h)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "null handle");
+	if (precision == DMRGPP_FP64 || (precision == DMRGPP_TF32X3 && h->mixed_ready)) {
+		h->precision = precision;
+		return DMRGPP_OK;
+	}
+	return fail(h, DMRGPP_NOT_SUPPORTED,
+	            "precision not available on this handle (create it with that precision)");
 }
 
 int dmrgpp_kron_synchronize(dmrgpp_kron_handle h)

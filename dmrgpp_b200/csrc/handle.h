@@ -40,6 +40,20 @@ struct dmrgpp_kron_s {
 	int*                err_host = nullptr; // mapped pinned word written by the kernel
 	int*                err_dev  = nullptr;
 	int                 test_stall = 0;     // dmrgpp_kron_test_stall_dependency
+	// mixed-precision (TF32x3 tensor-core) form, built when requested
+	bool                mixed_ready = false;
+	float*              m_ops_hi = nullptr; // packed operators, TF32 hi / lo
+	float*              m_ops_lo = nullptr;
+	float*              m_xs_hi  = nullptr; // x split, K-major, zero padding
+	float*              m_xs_lo  = nullptr;
+	float*              m_bxs_hi = nullptr; // pass-1 result split
+	float*              m_bxs_lo = nullptr;
+	int*                m_xmap   = nullptr; // sector vector -> x split offsets
+	void*               m_lists  = nullptr; // seg1, seg2, tile1, tile2
+	dmrgpp::GemmSeg*    m_seg1 = nullptr;
+	dmrgpp::GemmSeg*    m_seg2 = nullptr;
+	dmrgpp::GemmTile*   m_tile1 = nullptr;
+	dmrgpp::GemmTile*   m_tile2 = nullptr;
 	dmrgpp::LanczosWork* lanczos = nullptr;
 	std::string         err;
 };
@@ -48,6 +62,10 @@ namespace dmrgpp {
 
 // Enqueues y = H x on h->stream (device pointers); no synchronisation.
 int kron_apply_device(dmrgpp_kron_handle h, const double* x, double* y);
+
+// Builds and uploads the TF32x3 tensor-core form of the sector (the desc's
+// host tables are read again).
+int build_mixed(dmrgpp_kron_handle h, const dmrgpp_kron_desc* d);
 
 // (Re)builds and uploads the persistent schedule of h for tile configuration
 // cfg (0..kNumTileCfgs-1), aiming at items_per_cta work items per CTA.

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstring>
 #include <numeric>
 
 namespace dmrgpp {
@@ -352,6 +353,184 @@ void build_persistent_schedule(KronPlan& plan, int bk, int grid, int items_per_c
 		if (w.seg_end > w.seg_begin)
 			w.seg0 = segs[size_t(w.seg_begin)];
 	}
+}
+
+} // namespace dmrgpp
+
+namespace dmrgpp {
+
+namespace {
+
+float tf32_round(float f)
+{
+	unsigned u;
+	std::memcpy(&u, &f, 4);
+	if ((u & 0x7f800000u) != 0x7f800000u) // finite: round the magnitude half away from zero
+		u = (u + 0x1000u) & ~0x1fffu;
+	float r;
+	std::memcpy(&r, &u, 4);
+	return r;
+}
+
+long long round32(long long x) { return (x + 31) / 32 * 32; }
+
+void add_tc_tiles(std::vector<GemmTile>& tiles, long long c_off, long long ldc, long long M,
+                  long long N, int sb, int se, int bm, int bn)
+{
+	for (long long n0 = 0; n0 < N; n0 += bn)
+		for (long long m0 = 0; m0 < M; m0 += bm) {
+			GemmTile t {};
+			t.c_off     = c_off;
+			t.ldc       = int(ldc);
+			t.M         = int(M);
+			t.N         = int(N);
+			t.m0        = int(m0);
+			t.n0        = int(n0);
+			t.seg_begin = sb;
+			t.seg_end   = se;
+			tiles.push_back(t);
+		}
+}
+
+} // namespace
+
+void split_tf32(double v, float* hi, float* lo)
+{
+	const float h = tf32_round(float(v));
+	*hi           = h;
+	*lo           = tf32_round(float(v - double(h)));
+}
+
+std::string build_mixed_plan(KronPlan&            plan,
+                             const double* const* A,
+                             const size_t*        ldA,
+                             const double* const* B,
+                             const size_t*        ldB,
+                             int                  bn,
+                             std::vector<float>*  ops_hi,
+                             std::vector<float>*  ops_lo,
+                             std::vector<int>*    x_map)
+{
+	MixedPlan& mp   = plan.mixed;
+	mp              = MixedPlan();
+	mp.bn           = bn;
+	const size_t np = plan.np, nt = plan.triples.size(), np2 = np * np;
+	mp.P.resize(np);
+	mp.Q.resize(np);
+	for (size_t p = 0; p < np; ++p) {
+		mp.P[p] = round32(plan.r[p]);
+		mp.Q[p] = round32(plan.l[p]);
+	}
+	long long off = 0;
+	mp.bs_off.assign(np, 0);
+	for (size_t j = 0; j < np; ++j) {
+		mp.bs_off[j] = off;
+		off += plan.M[j] * mp.P[j];
+	}
+	mp.at_off.assign(nt, 0);
+	for (size_t t = 0; t < nt; ++t) {
+		mp.at_off[t] = off;
+		off += plan.l[plan.triples[t].i] * mp.Q[plan.triples[t].j];
+	}
+	mp.ops_elems = off;
+	off          = 0;
+	mp.xs_off.assign(np, 0);
+	for (size_t p = 0; p < np; ++p) {
+		mp.xs_off[p] = off;
+		off += plan.l[p] * mp.P[p];
+	}
+	mp.xs_elems = off;
+	off         = 0;
+	mp.bxs_off.assign(np, 0);
+	for (size_t j = 0; j < np; ++j) {
+		mp.bxs_off[j] = off;
+		off += plan.M[j] * mp.Q[j];
+	}
+	mp.bxs_elems = off;
+	if (mp.ops_elems > INT_MAX || mp.xs_elems > INT_MAX || mp.bxs_elems > INT_MAX)
+		return "sector too large for the mixed-precision layout";
+
+	if (ops_hi && ops_lo) {
+		ops_hi->assign(size_t(mp.ops_elems), 0.0f);
+		ops_lo->assign(size_t(mp.ops_elems), 0.0f);
+		float* H = ops_hi->data();
+		float* L = ops_lo->data();
+		for (size_t t = 0; t < nt; ++t) {
+			const Triple& tr = plan.triples[t];
+			const size_t  ix = size_t(tr.i) + size_t(tr.j) * np + size_t(tr.k) * np2;
+			// Bstack_j row (row_off + q), column c = B_k(i,j)(q, c), K-major
+			const double*   b  = B[ix];
+			const long long Pj = mp.P[tr.j];
+			for (long long q = 0; q < plan.r[tr.i]; ++q) {
+				const long long row = plan.row_off[t] + q;
+				for (long long c = 0; c < plan.r[tr.j]; ++c)
+					split_tf32(b[q + c * (long long)ldB[ix]], H + mp.bs_off[tr.j] + row * Pj + c,
+					           L + mp.bs_off[tr.j] + row * Pj + c);
+			}
+			// A^T: column n (< l_i) holds A_k(i,j)(n, 0..l_j), pitch Q_j
+			const double*   a  = A[ix];
+			const long long Qj = mp.Q[tr.j];
+			for (long long n = 0; n < plan.l[tr.i]; ++n)
+				for (long long k = 0; k < plan.l[tr.j]; ++k)
+					split_tf32(a[n + k * (long long)ldA[ix]], H + mp.at_off[t] + n * Qj + k,
+					           L + mp.at_off[t] + n * Qj + k);
+		}
+	}
+	if (x_map) {
+		x_map->assign(size_t(plan.dim()), 0);
+		for (size_t p = 0; p < np; ++p)
+			for (long long n = 0; n < plan.l[p]; ++n)
+				for (long long k = 0; k < plan.r[p]; ++k)
+					(*x_map)[size_t(plan.xy_start[p] + k + n * plan.r[p])]
+					    = int(mp.xs_off[p] + n * mp.P[p] + k);
+	}
+
+	// pass 1: C = BX_j split (row-major, pitch Q_j)
+	for (size_t j = 0; j < np; ++j) {
+		if (plan.M[j] == 0)
+			continue;
+		GemmSeg s {};
+		s.a_off = mp.bs_off[j];
+		s.lda   = int(mp.P[j]);
+		s.b_off = mp.xs_off[j];
+		s.ldb   = int(mp.P[j]);
+		s.K     = int(mp.P[j]);
+		s.dep   = int(j);
+		const int sb = int(mp.seg1.size());
+		mp.seg1.push_back(s);
+		add_tc_tiles(mp.tile1, mp.bxs_off[j], mp.Q[j], plan.M[j], plan.l[j], sb, sb + 1, mp.bm, bn);
+	}
+	// pass 2: C = Y_i (FP64, column-major)
+	size_t t = 0;
+	for (size_t i = 0; i < np; ++i) {
+		const int sb = int(mp.seg2.size());
+		for (; t < nt && plan.triples[t].i == int(i); ++t) {
+			const Triple& tr = plan.triples[t];
+			GemmSeg       s {};
+			s.a_off = mp.bxs_off[tr.j] + plan.row_off[t] * mp.Q[tr.j];
+			s.lda   = int(mp.Q[tr.j]);
+			s.b_off = mp.at_off[t];
+			s.ldb   = int(mp.Q[tr.j]);
+			s.K     = int(mp.Q[tr.j]);
+			s.dep   = tr.j;
+			mp.seg2.push_back(s);
+		}
+		add_tc_tiles(mp.tile2, plan.xy_start[i], plan.r[i], plan.r[i], plan.l[i], sb,
+		             int(mp.seg2.size()), mp.bm, bn);
+	}
+	auto kcost = [](const std::vector<GemmSeg>& segs, const GemmTile& g) {
+		long long k = 0;
+		for (int s = g.seg_begin; s < g.seg_end; ++s)
+			k += segs[s].K;
+		return k;
+	};
+	std::stable_sort(mp.tile1.begin(), mp.tile1.end(), [&](const GemmTile& x, const GemmTile& y) {
+		return kcost(mp.seg1, x) > kcost(mp.seg1, y);
+	});
+	std::stable_sort(mp.tile2.begin(), mp.tile2.end(), [&](const GemmTile& x, const GemmTile& y) {
+		return kcost(mp.seg2, x) > kcost(mp.seg2, y);
+	});
+	return std::string();
 }
 
 } // namespace dmrgpp

@@ -74,6 +74,27 @@ struct Triple {
 	int i, j, k;
 };
 
+// Layout of the mixed-precision (tensor-core) form of a sector.  Every
+// operand is K-major with K padded to a multiple of 32 (zeros), split into
+// hi and lo parts of identical layout; offsets and pitches are in floats.
+//   pass 1: A = Bstack_j (M_j rows, pitch P_j = round32(r_j))
+//           B = X_j split (l_j columns, pitch P_j)
+//           C = BX_j split (M_j rows, pitch Q_j = round32(l_j))
+//   pass 2: A = rows of (i,k) in BX_j (pitch Q_j)
+//           B = A_k(i,j)^T (l_i columns, pitch Q_j)
+//           C = Y_i, FP64 column-major
+struct MixedPlan {
+	std::vector<long long> P, Q;        // per patch
+	std::vector<long long> bs_off;      // per input patch: Bstack_j in ops
+	std::vector<long long> at_off;      // per triple: A^T in ops
+	std::vector<long long> xs_off;      // per patch: X_j in the x split buffer
+	std::vector<long long> bxs_off;     // per input patch: BX_j in the BX split buffer
+	long long              ops_elems = 0, xs_elems = 0, bxs_elems = 0;
+	std::vector<GemmSeg>   seg1, seg2;
+	std::vector<GemmTile>  tile1, tile2;
+	int                    bm = 128, bn = 64;
+};
+
 struct KronPlan {
 	size_t np = 0, nop = 0;
 	std::vector<long long> l, r;        // patch sizes
@@ -105,6 +126,8 @@ struct KronPlan {
 	int                   n_split_tiles = 0;
 	long long             partial_slots = 0;
 
+	MixedPlan mixed;
+
 	long long dim() const { return xy_start.empty() ? 0 : xy_start.back(); }
 };
 
@@ -123,6 +146,25 @@ std::string build_kron_plan(size_t               noperator,
                             int                  bn,
                             KronPlan&            plan,
                             std::vector<double>* pack_host);
+
+// Builds plan.mixed for bn-wide tensor-core tiles.  When ops_hi/ops_lo are
+// given, packs the operators (hi and lo TF32 parts stored as floats); x_map
+// (optional, dim entries) receives, for each element of the sector vector,
+// its offset in the x split buffer.
+std::string build_mixed_plan(KronPlan&            plan,
+                             const double* const* A,
+                             const size_t*        ldA,
+                             const double* const* B,
+                             const size_t*        ldB,
+                             int                  bn,
+                             std::vector<float>*  ops_hi,
+                             std::vector<float>*  ops_lo,
+                             std::vector<int>*    x_map);
+
+// Splits v into a TF32 high part and a TF32 remainder (host side of the
+// operator packing; round to nearest, ties away from zero, like the
+// device conversion cvt.rna.tf32.f32).
+void split_tf32(double v, float* hi, float* lo);
 
 // (Re)builds the two-launch tile lists seg1/tile1/seg2/tile2 of a planned
 // sector for bm x bn output tiles.

@@ -1,0 +1,34 @@
+// Mixed-precision (TF32x3) grouped GEMM on tcgen05 tensor cores (tc_gemm.cu).
+#pragma once
+
+#include "kron_plan.h"
+
+#include <cuda_runtime.h>
+
+namespace dmrgpp {
+
+struct TcArgs {
+	const float*    A_hi; // base of the pass's A operands (hi part)
+	const float*    A_lo;
+	const float*    B_hi;
+	const float*    B_lo;
+	float*          C_hi; // pass 1: K-major split output
+	float*          C_lo;
+	double*         Cd;   // pass 2: FP64 column-major output
+	const GemmSeg*  segs;
+	const GemmTile* tiles;
+	int             ntiles;
+	int*            error; // set to 2 when an mbarrier wait gave up
+};
+
+// Kernel attributes on the current device; call once per device.
+cudaError_t tc_init();
+
+// One grouped pass over a.ntiles tiles of 128 x bn (bn = 64 or 128).
+cudaError_t tc_launch(const TcArgs& a, int bn, bool pass1, cudaStream_t stream);
+
+// x (patch order, FP64) -> TF32 hi/lo parts at map[e].
+cudaError_t tc_split_x(const double* x, const int* map, float* hi, float* lo, long long n,
+                       cudaStream_t stream);
+
+} // namespace dmrgpp

@@ -166,6 +166,10 @@ class BatchedGemm:
                                                    ctypes.byref(us)), self._h)
         return cfg.value, us.value
 
+    def set_precision(self, precision: int) -> None:
+        """FP64 or the mixed mode the handle was created with."""
+        _capi.check(self._lib.dmrgpp_kron_set_precision(self._h, precision), self._h)
+
     def set_config(self, cfg: int, items_per_cta: int = 2) -> None:
         _capi.check(self._lib.dmrgpp_kron_set_config(self._h, cfg, items_per_cta), self._h)
 

@@ -95,6 +95,11 @@ int dmrgpp_kron_destroy(dmrgpp_kron_handle h);
  * and y are device pointers; the call only enqueues work on the stream. */
 int dmrgpp_kron_apply(dmrgpp_kron_handle h, const double* x, double* y, int on_device);
 
+/* Switches the arithmetic of later applies (and of the eigensolvers) between
+ * DMRGPP_FP64 and the mixed mode the handle was created with; FP64 is always
+ * available.  No counterpart in the reference. */
+int dmrgpp_kron_set_precision(dmrgpp_kron_handle h, int precision);
+
 /* Waits for the handle's stream and reports errors of work enqueued by
  * device-pointer applies (DMRGPP_TIMEOUT if a dependency wait inside the
  * kernel gave up, DMRGPP_CUDA_ERROR for a CUDA failure).  No counterpart in

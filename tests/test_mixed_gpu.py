@@ -1,0 +1,82 @@
+"""TF32x3 tensor-core (tcgen05) H*x against the FP64 oracle.
+
+Each FP64 operand is split into two TF32 parts and three products are
+accumulated in FP32, so the result carries ~2^-21 relative error per product
+plus FP32 accumulation; the bar here is max |y - y_oracle| <= 2e-5 max
+|y_oracle| (the FP64 path keeps its 1e-12 bar)."""
+import numpy as np
+import pytest
+
+from dmrgpp_b200 import superblock as sb
+
+pytestmark = pytest.mark.gpu
+RTOL_MIXED = 2e-5
+
+
+def rel_err(y, ref):
+    return float(np.abs(y - ref).max() / max(np.abs(ref).max(), 1e-300))
+
+
+def mixed(prob, **kw):
+    from dmrgpp_b200 import plugin
+    return plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3, **kw)
+
+
+@pytest.mark.parametrize("l,r", [(8, 8), (40, 24), (128, 128), (130, 70)])
+def test_single_patch(cuda_lib, cuda_device, oracle_built, l, r):
+    rng = np.random.default_rng(l + r)
+    A = {(0, 0, 0): np.asfortranarray(rng.standard_normal((l, l)))}
+    B = {(0, 0, 0): np.asfortranarray(rng.standard_normal((r, r)))}
+    prob = sb.KronProblem(np.array([l]), np.array([r]), 1, A, B)
+    x = rng.standard_normal(prob.dim)
+    bg = mixed(prob)
+    y = bg(x)
+    bg.close()
+    assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL_MIXED
+
+
+@pytest.mark.parametrize("seed,np_,K,maxs", [(0, 3, 1, 5), (1, 5, 3, 17), (2, 8, 5, 70),
+                                             (3, 4, 2, 200), (4, 10, 4, 33)])
+def test_random_ragged_sectors(cuda_lib, cuda_device, oracle_built, seed, np_, K, maxs):
+    prob = sb.random_problem(npatches=np_, noperator=K, max_size=maxs, seed=seed,
+                             zero_block_rate=0.2)
+    x = np.random.default_rng(seed).standard_normal(prob.dim)
+    bg = mixed(prob)
+    y = bg(x)
+    bg.close()
+    assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL_MIXED
+
+
+def test_microbench_and_precision_switch(cuda_lib, cuda_device, oracle_built):
+    from dmrgpp_b200 import plugin
+    prob = sb.c2_problem()
+    x = sb.random_unit_vector(prob.dim, seed=2)
+    ref = oracle_built.kron_apply(prob, x)
+    bg = mixed(prob)
+    y_mixed = bg(x)
+    assert rel_err(y_mixed, ref) < RTOL_MIXED
+    assert np.array_equal(bg(x), y_mixed)            # deterministic
+    bg.set_precision(plugin.FP64)
+    assert rel_err(bg(x), ref) < 1e-12
+    bg.set_precision(plugin.TF32X3)
+    assert np.array_equal(bg(x), y_mixed)
+    bg.close()
+
+
+def test_ladder_shaped_sector(cuda_lib, cuda_device, oracle_built):
+    prob = sb.ladder_problem(total_states=2000, sigma=2.0, seed=4)
+    x = np.random.default_rng(6).standard_normal(prob.dim)
+    bg = mixed(prob)
+    y = bg(x)
+    bg.close()
+    assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL_MIXED
+
+
+def test_fp64_handle_refuses_mixed_switch(cuda_lib, cuda_device):
+    from dmrgpp_b200 import _capi, plugin
+    prob = sb.random_problem(3, 2, seed=1)
+    bg = plugin.BatchedGemm.from_problem(prob)
+    with pytest.raises(_capi.DmrgppError) as ei:
+        bg.set_precision(plugin.TF32X3)
+    assert ei.value.status == _capi.NOT_SUPPORTED
+    bg.close()
