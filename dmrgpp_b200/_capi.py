@@ -64,6 +64,43 @@ class LanczosParams(ctypes.Structure):
                 ("check_every", ctypes.c_int)]
 
 
+class DavidsonParams(ctypes.Structure):
+    _fields_ = [("max_iterations", _sz), ("max_subspace", _sz), ("tolerance", ctypes.c_double),
+                ("preconditioner", ctypes.c_int), ("mlp", ctypes.c_void_p),
+                ("mixed_tolerance", ctypes.c_double), ("denominator_floor", ctypes.c_double)]
+
+
+class DavidsonStats(ctypes.Structure):
+    _fields_ = [("iterations", _sz), ("mixed_matvecs", _sz), ("fp64_matvecs", _sz),
+                ("restarts", _sz), ("residual_norm", ctypes.c_double), ("converged", ctypes.c_int)]
+
+
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_MLP = 0, 1, 2
+_fp = ctypes.POINTER(ctypes.c_float)
+_vp = ctypes.c_void_p
+
+SIGNATURES.update({
+    "dmrgpp_davidson_params_init": (None, [ctypes.POINTER(DavidsonParams)]),
+    "dmrgpp_davidson_lowest": (ctypes.c_int, [_vp, ctypes.POINTER(DavidsonParams), _vp, ctypes.c_int,
+                                              _dp, _vp, ctypes.POINTER(DavidsonStats)]),
+    "dmrgpp_correction_solve": (ctypes.c_int, [_vp, _vp, ctypes.c_double, _vp, _vp, ctypes.c_int,
+                                               ctypes.c_double, ctypes.POINTER(ctypes.c_int), _dp]),
+    "dmrgpp_kron_diagonal": (ctypes.c_int, [_vp, _vp]),
+    "dmrgpp_mlp_num_params": (_sz, []),
+    "dmrgpp_mlp_create": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_void_p)]),
+    "dmrgpp_mlp_destroy": (ctypes.c_int, [_vp]),
+    "dmrgpp_mlp_get_params": (ctypes.c_int, [_vp, _fp, _sz]),
+    "dmrgpp_mlp_set_params": (ctypes.c_int, [_vp, _fp, _sz]),
+    "dmrgpp_mlp_get_grads": (ctypes.c_int, [_vp, _fp, _sz]),
+    "dmrgpp_mlp_features": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, _sz, _vp, _vp]),
+    "dmrgpp_mlp_forward": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp]),
+    "dmrgpp_mlp_backward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _dp, _vp]),
+    "dmrgpp_mlp_adam_step": (ctypes.c_int, [_vp, ctypes.c_float, _vp]),
+    "dmrgpp_mlp_precondition": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp,
+                                               _sz, _vp]),
+    "dmrgpp_mlp_last_error": (ctypes.c_char_p, [_vp]),
+})
+
 SIGNATURES.update({
     "dmrgpp_lanczos_params_init": (None, [ctypes.POINTER(LanczosParams)]),
     "dmrgpp_lanczos_lowest": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LanczosParams),

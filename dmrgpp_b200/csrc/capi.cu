@@ -63,6 +63,9 @@ void release(dmrgpp_kron_handle h)
 	if (!h)
 		return;
 	dmrgpp::release_lanczos(h);
+	dmrgpp::release_davidson(h);
+	cudaFree(h->d_diag);
+	h->d_diag = nullptr;
 	cudaFree(h->m_ops_hi);
 	cudaFree(h->m_ops_lo);
 	cudaFree(h->m_xs_hi);
@@ -455,6 +458,15 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 	if (!pack.empty()
 	    && (e = cudaMemcpy(h->d_ops, pack.data(), pack.size() * sizeof(double), cudaMemcpyHostToDevice)))
 		return bail(e, "upload operators");
+	{
+		std::vector<double> diag;
+		dmrgpp::sector_diagonal(h->plan, d->Amatrix, d->ld_Amatrix, d->Bmatrix, d->ld_Bmatrix, diag);
+		if ((e = cudaMalloc(&h->d_diag, std::max<size_t>(diag.size(), 1) * sizeof(double))))
+			return bail(e, "cudaMalloc(diagonal)");
+		if (!diag.empty()
+		    && (e = cudaMemcpy(h->d_diag, diag.data(), diag.size() * sizeof(double), cudaMemcpyHostToDevice)))
+			return bail(e, "upload diagonal");
+	}
 	if (d->precision == DMRGPP_TF32X3) {
 		if (int rc = dmrgpp::build_mixed(h, d)) {
 			const std::string why = h->err;

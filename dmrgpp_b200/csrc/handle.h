@@ -10,7 +10,8 @@
 #include <string>
 
 namespace dmrgpp {
-struct LanczosWork; // device buffers of the eigensolvers, created on first use
+struct LanczosWork;  // device buffers of the eigensolvers, created on first use
+struct DavidsonWork;
 }
 
 struct dmrgpp_kron_s {
@@ -55,6 +56,8 @@ struct dmrgpp_kron_s {
 	dmrgpp::GemmTile*   m_tile1 = nullptr;
 	dmrgpp::GemmTile*   m_tile2 = nullptr;
 	dmrgpp::LanczosWork* lanczos = nullptr;
+	double*             d_diag = nullptr; // diagonal of H (patch order)
+	dmrgpp::DavidsonWork* davidson = nullptr;
 	std::string         err;
 };
 
@@ -76,5 +79,6 @@ int handle_fail(dmrgpp_kron_handle h, int status, const std::string& msg);
 
 // Releases the eigensolver buffers of a handle (lanczos.cu).
 void release_lanczos(dmrgpp_kron_handle h);
+void release_davidson(dmrgpp_kron_handle h);
 
 } // namespace dmrgpp

@@ -394,6 +394,25 @@ void add_tc_tiles(std::vector<GemmTile>& tiles, long long c_off, long long ldc, 
 
 } // namespace
 
+void sector_diagonal(const KronPlan& plan, const double* const* A, const size_t* ldA,
+                     const double* const* B, const size_t* ldB, std::vector<double>& diag)
+{
+	const size_t np = plan.np, np2 = np * np;
+	diag.assign(size_t(plan.dim()), 0.0);
+	for (const Triple& tr : plan.triples) {
+		if (tr.i != tr.j)
+			continue;
+		const size_t    ix = size_t(tr.i) + size_t(tr.i) * np + size_t(tr.k) * np2;
+		const long long li = plan.l[tr.i], ri = plan.r[tr.i];
+		double*         d  = diag.data() + plan.xy_start[tr.i];
+		for (long long il = 0; il < li; ++il) {
+			const double a = A[ix][il + il * (long long)ldA[ix]];
+			for (long long ir = 0; ir < ri; ++ir)
+				d[ir + il * ri] += a * B[ix][ir + ir * (long long)ldB[ix]];
+		}
+	}
+}
+
 void split_tf32(double v, float* hi, float* lo)
 {
 	const float h = tf32_round(float(v));

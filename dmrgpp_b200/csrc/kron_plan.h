@@ -161,6 +161,12 @@ std::string build_mixed_plan(KronPlan&            plan,
                              std::vector<float>*  ops_lo,
                              std::vector<int>*    x_map);
 
+// Diagonal of the sector's H in patch order: element (iR, iL) of patch i is
+// sum_k A_k(i,i)(iL,iL) * B_k(i,i)(iR,iR) over the contributing diagonal
+// triples (the input of diagonal preconditioners).
+void sector_diagonal(const KronPlan& plan, const double* const* A, const size_t* ldA,
+                     const double* const* B, const size_t* ldB, std::vector<double>& diag);
+
 // Splits v into a TF32 high part and a TF32 remainder (host side of the
 // operator packing; round to nearest, ties away from zero, like the
 // device conversion cvt.rna.tf32.f32).

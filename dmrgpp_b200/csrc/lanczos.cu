@@ -547,3 +547,450 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Davidson for the lowest eigenpair (no counterpart in the reference, which
+// only has Lanczos): the correction of each step comes from a preconditioner
+// applied to the residual -- none, the diagonal (Jacobi) one, or the learned
+// MLP of mlp.cu -- and the search space is orthonormalised on the device.
+// With a mixed-precision handle the first phase runs every matvec in the
+// handle's mixed mode and the second restarts from its Ritz vector in FP64,
+// so the energy and residual that are reported are FP64 quantities.
+// ---------------------------------------------------------------------------
+#include "mlp.h"
+
+namespace dmrgpp {
+
+namespace {
+
+// r = hu - theta*u, *nrm = |r|
+__global__ void __launch_bounds__(kThreads)
+k_residual(const double* __restrict__ hu, const double* __restrict__ u, double theta,
+           double* __restrict__ r, size_t n, double* nrm, double* partial, unsigned* ctr)
+{
+	__shared__ double red[kThreads / 32];
+	double            s = 0.0;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		const double w = hu[i] - theta * u[i];
+		r[i]           = w;
+		s += w * w;
+	}
+	s = block_sum(s, red);
+	if (threadIdx.x == 0) {
+		partial[blockIdx.x] = s;
+		if (last_block(ctr))
+			*nrm = sqrt(sum_partials(partial, gridDim.x));
+	}
+}
+
+// diagonal (Jacobi) correction: t = r / (theta - d), denominators kept away
+// from zero
+__global__ void __launch_bounds__(kThreads)
+k_jacobi(const double* __restrict__ r, const double* __restrict__ d, double theta, double floor_,
+         double* __restrict__ t, size_t n)
+{
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		double den = theta - d[i];
+		if (fabs(den) < floor_)
+			den = den < 0 ? -floor_ : floor_;
+		t[i] = r[i] / den;
+	}
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_copy(const double* __restrict__ src, double* __restrict__ dst, size_t n)
+{
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads)
+		dst[i] = src[i];
+}
+
+} // namespace
+
+struct DavidsonWork {
+	size_t    dim     = 0;
+	int       mmax    = 0;
+	double*   V       = nullptr; // dim x mmax, orthonormal basis
+	double*   W       = nullptr; // dim x mmax, H V
+	double*   u       = nullptr; // Ritz vector, H u, residual, correction
+	double*   hu      = nullptr;
+	double*   r       = nullptr;
+	double*   t       = nullptr;
+	double*   coef    = nullptr; // kMaxCols
+	double*   scal    = nullptr; // scalars written by reductions
+	double*   partial = nullptr;
+	unsigned* ctr     = nullptr;
+	double*   host    = nullptr; // pinned, kMaxCols + 8
+};
+
+void release_davidson(dmrgpp_kron_handle h)
+{
+	DavidsonWork* w = h->davidson;
+	if (!w)
+		return;
+	cudaFree(w->V);
+	cudaFree(w->W);
+	cudaFree(w->u);
+	cudaFree(w->coef);
+	cudaFree(w->scal);
+	cudaFree(w->partial);
+	cudaFree(w->ctr);
+	if (w->host)
+		cudaFreeHost(w->host);
+	delete w;
+	h->davidson = nullptr;
+}
+
+namespace {
+
+int ensure_davidson(dmrgpp_kron_handle h, size_t dim, int mmax)
+{
+	DavidsonWork* w = h->davidson;
+	if (w && w->dim == dim && w->mmax >= mmax)
+		return DMRGPP_OK;
+	release_davidson(h);
+	w           = new DavidsonWork();
+	h->davidson = w;
+	w->dim      = dim;
+	w->mmax     = mmax;
+	cudaError_t e;
+	if ((e = cudaMalloc(&w->V, dim * size_t(mmax) * sizeof(double)))
+	    || (e = cudaMalloc(&w->W, dim * size_t(mmax) * sizeof(double)))
+	    || (e = cudaMalloc(&w->u, 4 * dim * sizeof(double)))
+	    || (e = cudaMalloc(&w->coef, size_t(kMaxCols) * sizeof(double)))
+	    || (e = cudaMalloc(&w->scal, 16 * sizeof(double)))
+	    || (e = cudaMalloc(&w->partial, size_t(kMaxBlocks) * kMaxCols * sizeof(double)))
+	    || (e = cudaMalloc(&w->ctr, 16 * sizeof(unsigned)))
+	    || (e = cudaMemset(w->ctr, 0, 16 * sizeof(unsigned)))
+	    || (e = cudaHostAlloc(&w->host, (size_t(kMaxCols) + 8) * sizeof(double), 0)))
+		return cuda_status(h, e, "Davidson buffers");
+	w->hu = w->u + dim;
+	w->r  = w->u + 2 * dim;
+	w->t  = w->u + 3 * dim;
+	return DMRGPP_OK;
+}
+
+} // namespace
+} // namespace dmrgpp
+
+extern "C" {
+
+void dmrgpp_davidson_params_init(dmrgpp_davidson_params* p)
+{
+	if (!p)
+		return;
+	p->max_iterations  = 500;
+	p->max_subspace    = 32;
+	p->tolerance       = 1e-8;
+	p->preconditioner  = DMRGPP_PRECOND_JACOBI;
+	p->mlp             = nullptr;
+	p->mixed_tolerance = 1e-4;
+	p->denominator_floor = 1e-3;
+}
+
+int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
+                           const dmrgpp_davidson_params* p,
+                           const double*                 init,
+                           int                           on_device,
+                           double*                       energy,
+                           double*                       z,
+                           dmrgpp_davidson_stats*        stats)
+{
+	using namespace dmrgpp;
+	if (!h)
+		return DMRGPP_INVALID_ARG;
+	if (!p || !init || !energy || !z)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "null argument");
+	if (p->max_subspace < 2 || p->max_subspace > 512 || p->max_iterations < 1)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "max_subspace must be in [2, 512]");
+	if (p->preconditioner == DMRGPP_PRECOND_MLP && !p->mlp)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "learned preconditioner selected without a network");
+	const size_t D = size_t(h->plan.dim());
+	int          prev = -1;
+	cudaGetDevice(&prev);
+	if (prev != h->device)
+		cudaSetDevice(h->device);
+	struct Restore {
+		int dev, prev;
+		~Restore()
+		{
+			if (dev != prev && prev >= 0)
+				cudaSetDevice(prev);
+		}
+	} restore { h->device, prev };
+
+	const int mmax = int(p->max_subspace);
+	if (int rc = ensure_davidson(h, D, mmax))
+		return rc;
+	DavidsonWork* w   = h->davidson;
+	cudaStream_t  st  = h->stream;
+	const int     nb  = blocks_for(D);
+	const int     nbb = basis_blocks_for(D);
+	cudaError_t   e;
+	auto          Vc  = [&](int c) { return w->V + size_t(c) * D; };
+	auto          Wc  = [&](int c) { return w->W + size_t(c) * D; };
+
+	// two phases when the handle computes in a mixed mode
+	const int user_precision = h->precision;
+	int       phase          = user_precision == DMRGPP_FP64 ? 1 : 0;
+	dmrgpp_davidson_stats s {};
+
+	if ((e = cudaMemcpyAsync(w->t, init, D * sizeof(double),
+	                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st)))
+		return cuda_status(h, e, "copy initial vector");
+
+	const size_t        mm = static_cast<size_t>(mmax);
+	std::vector<double> G(mm * mm, 0.0), ev(mm, 0.0), evec(mm * mm, 0.0);
+	int    k       = 0;
+	double theta   = 0.0, rnorm = 0.0;
+	double best_mixed = 1e300;
+	int    stall   = 0;
+	bool   converged = false;
+	auto   set_phase = [&](int ph) {
+                phase        = ph;
+                h->precision = (ph == 0) ? user_precision : DMRGPP_FP64;
+	};
+	set_phase(phase);
+	int rc = DMRGPP_OK;
+
+	for (size_t it = 0; it < p->max_iterations; ++it) {
+		// orthonormalise the correction against the basis (two classical
+		// Gram-Schmidt passes) and append it
+		for (int pass = 0; pass < (k > 0 ? 2 : 0); ++pass) {
+			k_basis_dots<<<nbb, kThreads, 0, st>>>(w->V, D, k, w->t, D, w->coef, w->partial, w->ctr + 0);
+			k_basis_subtract<<<nbb, kThreads, 0, st>>>(w->t, w->V, D, k, w->coef, D, w->scal + 0,
+			                                          w->partial, w->ctr + 1);
+		}
+		k_dot<<<nb, kThreads, 0, st>>>(w->t, w->t, D, w->scal + 1, w->partial, w->ctr + 2);
+		k_scale_rsqrt<<<nb, kThreads, 0, st>>>(w->t, Vc(k), D, w->scal + 1);
+		if ((rc = kron_apply_device(h, Vc(k), Wc(k))))
+			break;
+		if (phase == 0)
+			++s.mixed_matvecs;
+		else
+			++s.fp64_matvecs;
+		// new column of the projected matrix G = V^T H V
+		k_basis_dots<<<nbb, kThreads, 0, st>>>(w->V, D, k + 1, Wc(k), D, w->coef, w->partial, w->ctr + 3);
+		if ((e = cudaMemcpyAsync(w->host, w->coef, size_t(k + 1) * sizeof(double),
+		                         cudaMemcpyDeviceToHost, st))
+		    || (e = cudaStreamSynchronize(st))) {
+			rc = cuda_status(h, e, "Davidson projection");
+			break;
+		}
+		if (h->err_host && *reinterpret_cast<volatile int*>(h->err_host)) {
+			rc = handle_fail(h, DMRGPP_TIMEOUT, "H*x kernel wait gave up during Davidson");
+			break;
+		}
+		for (int i = 0; i <= k; ++i) {
+			G[size_t(i) + size_t(k) * mmax] = w->host[i];
+			G[size_t(k) + size_t(i) * mmax] = w->host[i];
+		}
+		++k;
+		// Rayleigh-Ritz on the k-dimensional space
+		std::vector<double> Gk(size_t(k) * size_t(k));
+		for (int j = 0; j < k; ++j)
+			for (int i = 0; i < k; ++i)
+				Gk[size_t(i) + size_t(j) * k] = G[size_t(i) + size_t(j) * mmax];
+		sym_eigen(k, Gk.data(), ev.data(), evec.data());
+		theta = ev[0];
+		if ((e = cudaMemcpyAsync(w->coef, evec.data(), size_t(k) * sizeof(double),
+		                         cudaMemcpyHostToDevice, st))) {
+			rc = cuda_status(h, e, "Ritz coefficients");
+			break;
+		}
+		k_basis_combine<<<nbb, kThreads, 0, st>>>(w->u, w->V, D, k, w->coef, D);
+		k_basis_combine<<<nbb, kThreads, 0, st>>>(w->hu, w->W, D, k, w->coef, D);
+		k_residual<<<nb, kThreads, 0, st>>>(w->hu, w->u, theta, w->r, D, w->scal + 2, w->partial,
+		                                    w->ctr + 4);
+		if ((e = cudaMemcpyAsync(w->host, w->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st))
+		    || (e = cudaStreamSynchronize(st))) {
+			rc = cuda_status(h, e, "Davidson residual");
+			break;
+		}
+		rnorm = w->host[0];
+		++s.iterations;
+		const double scale = std::max(1.0, std::fabs(theta));
+		if (phase == 1 && rnorm <= p->tolerance * scale) {
+			converged = true;
+			break;
+		}
+		bool restart = (k == mmax);
+		if (phase == 0) {
+			// leave the mixed phase once its residual is small or stalls
+			if (rnorm < 0.9 * best_mixed) {
+				best_mixed = rnorm;
+				stall      = 0;
+			} else {
+				++stall;
+			}
+			if (rnorm <= p->mixed_tolerance * scale || stall >= 8) {
+				set_phase(1);
+				restart = true; // the FP64 phase starts from the Ritz vector alone
+			}
+		}
+		if (restart) {
+			// V = [u], W = [H u] (recomputed in FP64 on the phase change)
+			k_copy<<<nb, kThreads, 0, st>>>(w->u, w->t, D);
+			k = 0;
+			if (phase == 1 && s.fp64_matvecs == 0) {
+				++s.restarts;
+				continue; // t = u is orthonormalised and multiplied in the next pass
+			}
+			k_dot<<<nb, kThreads, 0, st>>>(w->u, w->u, D, w->scal + 1, w->partial, w->ctr + 2);
+			k_scale_rsqrt<<<nb, kThreads, 0, st>>>(w->u, Vc(0), D, w->scal + 1);
+			k_scale_rsqrt<<<nb, kThreads, 0, st>>>(w->hu, Wc(0), D, w->scal + 1);
+			G[0] = theta;
+			k    = 1;
+			++s.restarts;
+		}
+		// correction from the preconditioner
+		if (p->preconditioner == DMRGPP_PRECOND_JACOBI) {
+			k_jacobi<<<nb, kThreads, 0, st>>>(w->r, h->d_diag, theta,
+			                                  p->denominator_floor * std::max(1.0, std::fabs(theta)),
+			                                  w->t, D);
+		} else if (p->preconditioner == DMRGPP_PRECOND_MLP) {
+			if ((rc = mlp_precondition(static_cast<dmrgpp_mlp_handle>(p->mlp), h->d_diag, w->r,
+			                           theta, rnorm, w->t, D, st))) {
+				handle_fail(h, rc, "learned preconditioner failed");
+				break;
+			}
+		} else {
+			k_copy<<<nb, kThreads, 0, st>>>(w->r, w->t, D);
+		}
+		if ((e = cudaGetLastError())) {
+			rc = cuda_status(h, e, "Davidson launch");
+			break;
+		}
+	}
+	h->precision = user_precision;
+	if (rc)
+		return rc;
+	s.residual_norm = rnorm;
+	s.converged     = converged ? 1 : 0;
+	// the Ritz vector u is normalised by construction (V orthonormal, |s| = 1)
+	if ((e = cudaMemcpyAsync(z, w->u, D * sizeof(double),
+	                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st))
+	    || (e = cudaStreamSynchronize(st)))
+		return cuda_status(h, e, "copy Ritz vector");
+	*energy = theta;
+	if (stats)
+		*stats = s;
+	return converged ? DMRGPP_OK : handle_fail(h, DMRGPP_NOT_CONVERGED, "Davidson did not converge");
+}
+
+} // extern "C"
+
+namespace dmrgpp {
+namespace {
+
+// y += a x
+__global__ void __launch_bounds__(kThreads)
+k_axpy(double a, const double* __restrict__ x, double* __restrict__ y, size_t n)
+{
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads)
+		y[i] += a * x[i];
+}
+
+// y = x + a y
+__global__ void __launch_bounds__(kThreads)
+k_xpay(const double* __restrict__ x, double a, double* __restrict__ y, size_t n)
+{
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads)
+		y[i] = x[i] + a * y[i];
+}
+
+} // namespace
+} // namespace dmrgpp
+
+extern "C" {
+
+int dmrgpp_kron_diagonal(dmrgpp_kron_handle h, double* diag)
+{
+	if (!h || !diag)
+		return DMRGPP_INVALID_ARG;
+	const size_t D = size_t(h->plan.dim());
+	return cudaMemcpyAsync(diag, h->d_diag, D * sizeof(double), cudaMemcpyDeviceToDevice, h->stream)
+	        == cudaSuccess
+	    ? DMRGPP_OK
+	    : DMRGPP_CUDA_ERROR;
+}
+
+int dmrgpp_correction_solve(dmrgpp_kron_handle h, const double* u, double theta, const double* r,
+                            double* t, int max_iterations, double rel_tolerance, int* iterations,
+                            double* rel_residual)
+{
+	using namespace dmrgpp;
+	if (!h || !u || !r || !t || max_iterations < 1)
+		return DMRGPP_INVALID_ARG;
+	const size_t D  = size_t(h->plan.dim());
+	if (int rc = ensure_davidson(h, D, 2))
+		return rc;
+	DavidsonWork* w  = h->davidson;
+	cudaStream_t  st = h->stream;
+	const int     nb = blocks_for(D);
+	// work vectors: res = w->hu, p = w->r, q = w->t, Aq = second basis column
+	double*      res = w->hu;
+	double*      p   = w->r;
+	double*      q   = w->t;
+	double*      Aq  = w->V + D;
+	double*      sc  = w->scal;
+	auto read = [&](double* dev, int count, double* host) {
+		return cudaMemcpyAsync(host, dev, size_t(count) * sizeof(double), cudaMemcpyDeviceToHost, st)
+		        == cudaSuccess
+		    && cudaStreamSynchronize(st) == cudaSuccess;
+	};
+	auto project = [&](double* v) { // v -= u (u . v)
+		k_dot<<<nb, kThreads, 0, st>>>(u, v, D, sc + 5, w->partial, w->ctr + 5);
+		double uv = 0;
+		if (!read(sc + 5, 1, &uv))
+			return false;
+		k_axpy<<<nb, kThreads, 0, st>>>(-uv, u, v, D);
+		return true;
+	};
+	// t = 0, res = -(I - uu^T) r, p = res
+	cudaMemsetAsync(t, 0, D * sizeof(double), st);
+	cudaMemsetAsync(res, 0, D * sizeof(double), st);
+	k_axpy<<<nb, kThreads, 0, st>>>(-1.0, r, res, D);
+	if (!project(res))
+		return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+	cudaMemcpyAsync(p, res, D * sizeof(double), cudaMemcpyDeviceToDevice, st);
+	double rr = 0, b0 = 0;
+	k_dot<<<nb, kThreads, 0, st>>>(res, res, D, sc + 6, w->partial, w->ctr + 6);
+	if (!read(sc + 6, 1, &rr))
+		return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+	b0 = std::sqrt(rr);
+	int it = 0;
+	for (; it < max_iterations && std::sqrt(rr) > rel_tolerance * b0 && b0 > 0; ++it) {
+		// Aq = P (H - theta) P p  (p stays orthogonal to u)
+		cudaMemcpyAsync(q, p, D * sizeof(double), cudaMemcpyDeviceToDevice, st);
+		if (int rc = kron_apply_device(h, q, Aq))
+			return rc;
+		k_axpy<<<nb, kThreads, 0, st>>>(-theta, q, Aq, D);
+		if (!project(Aq))
+			return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+		double pAp = 0;
+		k_dot<<<nb, kThreads, 0, st>>>(p, Aq, D, sc + 7, w->partial, w->ctr + 7);
+		if (!read(sc + 7, 1, &pAp) || !(pAp > 0))
+			break; // the projected operator is not positive definite here
+		const double alpha = rr / pAp;
+		k_axpy<<<nb, kThreads, 0, st>>>(alpha, p, t, D);
+		k_axpy<<<nb, kThreads, 0, st>>>(-alpha, Aq, res, D);
+		double rr_new = 0;
+		k_dot<<<nb, kThreads, 0, st>>>(res, res, D, sc + 6, w->partial, w->ctr + 6);
+		if (!read(sc + 6, 1, &rr_new))
+			return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+		k_xpay<<<nb, kThreads, 0, st>>>(res, rr_new / rr, p, D);
+		rr = rr_new;
+	}
+	if (iterations)
+		*iterations = it;
+	if (rel_residual)
+		*rel_residual = b0 > 0 ? std::sqrt(rr) / b0 : 0.0;
+	return cudaStreamSynchronize(st) == cudaSuccess ? DMRGPP_OK : handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+}
+
+} // extern "C"

@@ -1,0 +1,558 @@
+// Learned Davidson preconditioner: a small MLP trained on the GPU by the
+// project's own forward and backward kernels (no counterpart in the
+// reference, which has no Davidson solver).
+//
+// Per element e of a sector vector, with s = max(1, |theta|),
+// rms = |r| / sqrt(n), f0 = (d_e - theta)/s, f1 = r_e / rms:
+//   features x_e = [f0, f1, f1 f0 / (f0^2 + 0.05^2), 1 / (1 + (f0 / 0.05)^2)]
+//   h1 = tanh(W1 x + b1), h2 = tanh(W2 h1 + b2), o = w3 . h2 + b3
+//   correction t_e = o * rms / s
+// (the third feature makes the diagonal (Jacobi) correction -r/(d-theta) a
+// linear function of the inputs).  Training minimises the mean squared error
+// between o and the scaled exact correction t*_e * s / rms.
+//
+// Parameters are kept in FP32 (master copy, Adam state); inference runs
+// with BF16 copies of the weights and FP32 accumulation.  Contractions use
+// one tiled FP32 GEMM kernel whose reduction order is fixed, so training is
+// bitwise reproducible.
+#include "dmrgpp_kron.h"
+#include "mlp.h"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace dmrgpp {
+namespace {
+
+constexpr int   F  = kMlpFeatures;
+constexpr int   H  = kMlpWidth;
+constexpr float kDelta = 0.05f;
+
+// parameter offsets (floats)
+constexpr size_t kW1 = 0;
+constexpr size_t kB1 = kW1 + size_t(H) * F;
+constexpr size_t kW2 = kB1 + H;
+constexpr size_t kB2 = kW2 + size_t(H) * H;
+constexpr size_t kW3 = kB2 + H;
+constexpr size_t kB3 = kW3 + H;
+constexpr size_t kNumParams = kB3 + 1;
+
+} // namespace
+} // namespace dmrgpp
+
+struct dmrgpp_mlp_s {
+	int            device  = 0;
+	float*         params  = nullptr; // FP32 master
+	float*         grads   = nullptr;
+	float*         adam_m  = nullptr;
+	float*         adam_v  = nullptr;
+	int            adam_t  = 0;
+	__nv_bfloat16* wbf     = nullptr; // BF16 copy of all parameters (inference)
+	float*         pinf    = nullptr; // the BF16 copy widened to FP32
+	bool           bf_dirty = true;
+	int            cap     = 0;       // rows of the training / inference buffers
+	float*         x       = nullptr; // cap x F
+	float*         h1      = nullptr; // cap x H
+	float*         h2      = nullptr; // cap x H
+	float*         out     = nullptr; // cap
+	float*         gout    = nullptr; // cap
+	float*         dz      = nullptr; // cap x H
+	float*         dz1     = nullptr; // cap x H
+	double*        loss    = nullptr; // device scalar
+	double*        partial = nullptr;
+	unsigned*      ctr     = nullptr;
+	int            last_rows = 0;
+	std::string    err;
+};
+
+namespace dmrgpp {
+namespace {
+
+thread_local std::string g_mlp_error;
+
+int mlp_fail(dmrgpp_mlp_handle m, int status, const std::string& msg)
+{
+	if (m)
+		m->err = msg;
+	else
+		g_mlp_error = msg;
+	return status;
+}
+
+int mlp_cuda(dmrgpp_mlp_handle m, cudaError_t e, const char* where)
+{
+	return mlp_fail(m, e == cudaErrorMemoryAllocation ? DMRGPP_OOM : DMRGPP_CUDA_ERROR,
+	                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+__device__ __forceinline__ void features(double d, double r, double theta, double s, double rms,
+                                         float* x)
+{
+	const float f0 = float((d - theta) / s);
+	const float f1 = rms > 0 ? float(r / rms) : 0.f;
+	x[0]           = f0;
+	x[1]           = f1;
+	x[2]           = f1 * f0 / (f0 * f0 + kDelta * kDelta);
+	const float q  = f0 / kDelta;
+	x[3]           = 1.f / (1.f + q * q);
+}
+
+__global__ void k_features(const double* __restrict__ d, const double* __restrict__ r, double theta,
+                           double s, double rms, size_t n, float* __restrict__ x)
+{
+	for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n;
+	     e += size_t(gridDim.x) * blockDim.x)
+		features(d[e], r[e], theta, s, rms, x + e * F);
+}
+
+// C (M x N, row-major, ldc) = op(A) * op(B) (+ C if accumulate); op(A) is
+// M x K, op(B) is K x N.  TA: A stored K x M (row-major) instead of M x K.
+// TB: B stored N x K instead of K x N.  64 x 64 tiles, k-steps of 16, each
+// of 256 threads owns a 4 x 4 block; the k order is fixed.
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256)
+k_sgemm(int M, int N, int K, const float* __restrict__ A, int lda, const float* __restrict__ B,
+        int ldb, float* __restrict__ C, int ldc, int accumulate)
+{
+	__shared__ float As[16][64 + 4];
+	__shared__ float Bs[16][64 + 4];
+	const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+	const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+	float     acc[4][4] = {};
+	for (int k0 = 0; k0 < K; k0 += 16) {
+		for (int q = threadIdx.x; q < 16 * 64; q += 256) {
+			const int kk = q / 64, mm = q % 64;
+			const int gm = m0 + mm, gk = k0 + kk;
+			float     v  = 0.f;
+			if (gm < M && gk < K)
+				v = TA ? A[size_t(gk) * lda + gm] : A[size_t(gm) * lda + gk];
+			As[kk][mm] = v;
+			const int gn = n0 + mm;
+			float     w  = 0.f;
+			if (gn < N && gk < K)
+				w = TB ? B[size_t(gn) * ldb + gk] : B[size_t(gk) * ldb + gn];
+			Bs[kk][mm] = w;
+		}
+		__syncthreads();
+#pragma unroll
+		for (int kk = 0; kk < 16; ++kk) {
+			float a[4], b[4];
+#pragma unroll
+			for (int i = 0; i < 4; ++i) {
+				a[i] = As[kk][ty * 4 + i];
+				b[i] = Bs[kk][tx * 4 + i];
+			}
+#pragma unroll
+			for (int i = 0; i < 4; ++i)
+#pragma unroll
+				for (int j = 0; j < 4; ++j)
+					acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+		}
+		__syncthreads();
+	}
+#pragma unroll
+	for (int i = 0; i < 4; ++i)
+#pragma unroll
+		for (int j = 0; j < 4; ++j) {
+			const int gm = m0 + ty * 4 + i, gn = n0 + tx * 4 + j;
+			if (gm < M && gn < N) {
+				float* c = C + size_t(gm) * ldc + gn;
+				*c       = accumulate ? *c + acc[i][j] : acc[i][j];
+			}
+		}
+}
+
+template <bool TA, bool TB>
+void sgemm(int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc,
+           bool accumulate, cudaStream_t st)
+{
+	dim3 grid((N + 63) / 64, (M + 63) / 64);
+	k_sgemm<TA, TB><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, accumulate ? 1 : 0);
+}
+
+// Z (rows x H) += bias; Z = tanh(Z)
+__global__ void k_bias_tanh(float* __restrict__ Z, const float* __restrict__ b, size_t rows)
+{
+	for (size_t q = blockIdx.x * size_t(blockDim.x) + threadIdx.x; q < rows * H;
+	     q += size_t(gridDim.x) * blockDim.x)
+		Z[q] = tanhf(Z[q] + b[q % H]);
+}
+
+// out[b] = h2[b,:] . w3 + b3  (one warp per row)
+__global__ void k_head(const float* __restrict__ h2, const float* __restrict__ w3, const float* b3,
+                       float* __restrict__ out, int rows)
+{
+	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+	if (warp >= rows)
+		return;
+	float s = 0.f;
+	for (int j = lane; j < H; j += 32)
+		s = fmaf(h2[size_t(warp) * H + j], w3[j], s);
+	for (int o = 16; o > 0; o >>= 1)
+		s += __shfl_down_sync(0xffffffffu, s, o);
+	if (lane == 0)
+		out[warp] = s + b3[0];
+}
+
+// loss = sum w_b (o_b - y_b)^2 / rows, gout_b = 2 w_b (o_b - y_b) / rows
+__global__ void k_mse(const float* __restrict__ o, const float* __restrict__ y,
+                      const float* __restrict__ wgt, int rows, float* __restrict__ gout,
+                      double* loss, double* partial, unsigned* ctr)
+{
+	__shared__ double red[8];
+	double            s = 0.0;
+	for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < rows; b += gridDim.x * blockDim.x) {
+		const float wb = wgt ? wgt[b] : 1.f;
+		const float d  = o[b] - y[b];
+		gout[b]        = 2.f * wb * d / float(rows);
+		s += double(wb) * double(d) * double(d);
+	}
+	for (int off = 16; off > 0; off >>= 1)
+		s += __shfl_down_sync(0xffffffffu, s, off);
+	if ((threadIdx.x & 31) == 0)
+		red[threadIdx.x >> 5] = s;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int w = 0; w < int(blockDim.x >> 5); ++w)
+			t += red[w];
+		partial[blockIdx.x] = t;
+		__threadfence();
+		if (atomicAdd(ctr, 1u) == gridDim.x - 1) {
+			__threadfence();
+			double tot = 0.0;
+			for (int b = 0; b < int(gridDim.x); ++b)
+				tot += __ldcg(partial + b);
+			*loss = tot / double(rows);
+			*ctr  = 0u;
+		}
+	}
+}
+
+// dz = (gout[b] * w3[j]) * (1 - h2^2)
+__global__ void k_head_back(const float* __restrict__ gout, const float* __restrict__ w3,
+                            const float* __restrict__ h2, float* __restrict__ dz, size_t rows)
+{
+	for (size_t q = blockIdx.x * size_t(blockDim.x) + threadIdx.x; q < rows * H;
+	     q += size_t(gridDim.x) * blockDim.x) {
+		const float h = h2[q];
+		dz[q]         = gout[q / H] * w3[q % H] * (1.f - h * h);
+	}
+}
+
+// dz *= (1 - h^2)
+__global__ void k_tanh_back(float* __restrict__ dz, const float* __restrict__ h, size_t n)
+{
+	for (size_t q = blockIdx.x * size_t(blockDim.x) + threadIdx.x; q < n;
+	     q += size_t(gridDim.x) * blockDim.x)
+		dz[q] *= 1.f - h[q] * h[q];
+}
+
+// g[j] = sum_b M[b, j] (fixed order), cols columns of a rows x cols matrix
+__global__ void k_colsum(const float* __restrict__ Mx, int rows, int cols, float* __restrict__ g)
+{
+	const int j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= cols)
+		return;
+	float s = 0.f;
+	for (int b = 0; b < rows; ++b)
+		s += Mx[size_t(b) * cols + j];
+	g[j] = s;
+}
+
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, size_t n, float lr, float b1, float b2, float eps,
+                       float c1, float c2)
+{
+	for (size_t q = blockIdx.x * size_t(blockDim.x) + threadIdx.x; q < n;
+	     q += size_t(gridDim.x) * blockDim.x) {
+		const float gq = g[q];
+		m[q]           = b1 * m[q] + (1.f - b1) * gq;
+		v[q]           = b2 * v[q] + (1.f - b2) * gq * gq;
+		p[q] -= lr * (m[q] / c1) / (sqrtf(v[q] / c2) + eps);
+	}
+}
+
+__global__ void k_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ q, size_t n)
+{
+	for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * blockDim.x)
+		q[i] = __float2bfloat16_rn(p[i]);
+}
+
+__global__ void k_from_bf16(const __nv_bfloat16* __restrict__ q, float* __restrict__ p, size_t n)
+{
+	for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * blockDim.x)
+		p[i] = __bfloat162float(q[i]);
+}
+
+// t_e = o_e * rms / s
+__global__ void k_scale_out(const float* __restrict__ o, double scale, double* __restrict__ t, size_t n)
+{
+	for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n;
+	     e += size_t(gridDim.x) * blockDim.x)
+		t[e] = double(o[e]) * scale;
+}
+
+int grid_for(size_t n, int threads = 256)
+{
+	size_t b = (n + threads - 1) / threads;
+	return int(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
+}
+
+int ensure_rows(dmrgpp_mlp_handle m, int rows)
+{
+	if (rows <= m->cap)
+		return DMRGPP_OK;
+	cudaFree(m->x);
+	cudaFree(m->h1);
+	cudaFree(m->h2);
+	cudaFree(m->out);
+	cudaFree(m->gout);
+	cudaFree(m->dz);
+	cudaFree(m->dz1);
+	m->x = m->h1 = m->h2 = m->out = m->gout = m->dz = m->dz1 = nullptr;
+	m->cap                                                   = 0;
+	cudaError_t e;
+	const size_t r = size_t(rows);
+	if ((e = cudaMalloc(&m->x, r * F * sizeof(float))) || (e = cudaMalloc(&m->h1, r * H * sizeof(float)))
+	    || (e = cudaMalloc(&m->h2, r * H * sizeof(float))) || (e = cudaMalloc(&m->out, r * sizeof(float)))
+	    || (e = cudaMalloc(&m->gout, r * sizeof(float))) || (e = cudaMalloc(&m->dz, r * H * sizeof(float)))
+	    || (e = cudaMalloc(&m->dz1, r * H * sizeof(float))))
+		return mlp_cuda(m, e, "MLP row buffers");
+	m->cap = rows;
+	return DMRGPP_OK;
+}
+
+// FP32 forward of `rows` feature rows x (rows x F) with parameter set P;
+// fills m->h1, m->h2, m->out
+void forward(dmrgpp_mlp_handle m, const float* P, const float* x, int rows, cudaStream_t st)
+{
+	sgemm<false, true>(rows, H, F, x, F, P + kW1, F, m->h1, H, false, st);
+	k_bias_tanh<<<grid_for(size_t(rows) * H), 256, 0, st>>>(m->h1, P + kB1, size_t(rows));
+	sgemm<false, true>(rows, H, H, m->h1, H, P + kW2, H, m->h2, H, false, st);
+	k_bias_tanh<<<grid_for(size_t(rows) * H), 256, 0, st>>>(m->h2, P + kB2, size_t(rows));
+	k_head<<<(rows * 32 + 255) / 256, 256, 0, st>>>(m->h2, P + kW3, P + kB3, m->out, rows);
+}
+
+} // namespace
+
+int mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, double theta,
+                     double rnorm, double* t, size_t n, cudaStream_t st)
+{
+	if (!m)
+		return DMRGPP_INVALID_ARG;
+	const double s   = std::max(1.0, std::fabs(theta));
+	const double rms = rnorm / std::sqrt(double(n > 0 ? n : 1));
+	if (m->bf_dirty) {
+		k_to_bf16<<<grid_for(kNumParams), 256, 0, st>>>(m->params, m->wbf, kNumParams);
+		m->bf_dirty = false;
+	}
+	// inference weights: BF16 values widened to FP32 (the network as it ships)
+	k_from_bf16<<<grid_for(kNumParams), 256, 0, st>>>(m->wbf, m->pinf, kNumParams);
+	const float* pinf = m->pinf;
+	const int chunk = 1 << 16;
+	if (int rc = ensure_rows(m, int(std::min<size_t>(n, chunk))))
+		return rc;
+	for (size_t e0 = 0; e0 < n; e0 += chunk) {
+		const int rows = int(std::min<size_t>(chunk, n - e0));
+		k_features<<<grid_for(size_t(rows)), 256, 0, st>>>(diag + e0, r + e0, theta, s, rms,
+		                                                  size_t(rows), m->x);
+		forward(m, pinf, m->x, rows, st);
+		k_scale_out<<<grid_for(size_t(rows)), 256, 0, st>>>(m->out, rms / s, t + e0, size_t(rows));
+	}
+	cudaError_t e = cudaGetLastError();
+	return e == cudaSuccess ? DMRGPP_OK : mlp_cuda(m, e, "MLP inference");
+}
+
+} // namespace dmrgpp
+
+extern "C" {
+
+size_t dmrgpp_mlp_num_params(void) { return dmrgpp::kNumParams; }
+
+const char* dmrgpp_mlp_last_error(dmrgpp_mlp_handle m) { return m ? m->err.c_str() : dmrgpp::g_mlp_error.c_str(); }
+
+int dmrgpp_mlp_create(unsigned long long seed, dmrgpp_mlp_handle* out)
+{
+	using namespace dmrgpp;
+	if (!out)
+		return mlp_fail(nullptr, DMRGPP_INVALID_ARG, "null output");
+	*out                = nullptr;
+	dmrgpp_mlp_handle m = new dmrgpp_mlp_s();
+	cudaGetDevice(&m->device);
+	// Glorot-uniform weights, zero biases, from a seeded host generator
+	std::vector<float>               p(kNumParams, 0.f);
+	std::mt19937_64                  rng(seed);
+	auto                             fill = [&](size_t off, int fan_in, int fan_out, size_t count) {
+                const float a = std::sqrt(6.f / float(fan_in + fan_out));
+                std::uniform_real_distribution<float> u(-a, a);
+                for (size_t i = 0; i < count; ++i)
+                        p[off + i] = u(rng);
+	};
+	fill(kW1, F, H, size_t(H) * F);
+	fill(kW2, H, H, size_t(H) * H);
+	fill(kW3, H, 1, size_t(H));
+	cudaError_t e;
+	if ((e = cudaMalloc(&m->params, kNumParams * sizeof(float)))
+	    || (e = cudaMalloc(&m->grads, kNumParams * sizeof(float)))
+	    || (e = cudaMalloc(&m->adam_m, kNumParams * sizeof(float)))
+	    || (e = cudaMalloc(&m->adam_v, kNumParams * sizeof(float)))
+	    || (e = cudaMalloc(&m->wbf, kNumParams * sizeof(__nv_bfloat16)))
+	    || (e = cudaMalloc(&m->pinf, kNumParams * sizeof(float)))
+	    || (e = cudaMalloc(&m->loss, sizeof(double)))
+	    || (e = cudaMalloc(&m->partial, 4096 * sizeof(double)))
+	    || (e = cudaMalloc(&m->ctr, sizeof(unsigned))) || (e = cudaMemset(m->ctr, 0, sizeof(unsigned)))
+	    || (e = cudaMemset(m->adam_m, 0, kNumParams * sizeof(float)))
+	    || (e = cudaMemset(m->adam_v, 0, kNumParams * sizeof(float)))
+	    || (e = cudaMemcpy(m->params, p.data(), kNumParams * sizeof(float), cudaMemcpyHostToDevice))) {
+		const int rc = mlp_cuda(nullptr, e, "MLP create");
+		dmrgpp_mlp_destroy(m);
+		return rc;
+	}
+	*out = m;
+	return DMRGPP_OK;
+}
+
+int dmrgpp_mlp_destroy(dmrgpp_mlp_handle m)
+{
+	if (!m)
+		return DMRGPP_OK;
+	cudaDeviceSynchronize();
+	cudaFree(m->params);
+	cudaFree(m->grads);
+	cudaFree(m->adam_m);
+	cudaFree(m->adam_v);
+	cudaFree(m->wbf);
+	cudaFree(m->pinf);
+	cudaFree(m->loss);
+	cudaFree(m->partial);
+	cudaFree(m->ctr);
+	cudaFree(m->x);
+	cudaFree(m->h1);
+	cudaFree(m->h2);
+	cudaFree(m->out);
+	cudaFree(m->gout);
+	cudaFree(m->dz);
+	cudaFree(m->dz1);
+	delete m;
+	return DMRGPP_OK;
+}
+
+int dmrgpp_mlp_get_params(dmrgpp_mlp_handle m, float* host, size_t n)
+{
+	if (!m || !host || n != dmrgpp::kNumParams)
+		return DMRGPP_INVALID_ARG;
+	return cudaMemcpy(host, m->params, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess
+	    ? DMRGPP_OK
+	    : DMRGPP_CUDA_ERROR;
+}
+
+int dmrgpp_mlp_set_params(dmrgpp_mlp_handle m, const float* host, size_t n)
+{
+	if (!m || !host || n != dmrgpp::kNumParams)
+		return DMRGPP_INVALID_ARG;
+	m->bf_dirty = true;
+	m->adam_t   = 0;
+	cudaMemset(m->adam_m, 0, n * sizeof(float));
+	cudaMemset(m->adam_v, 0, n * sizeof(float));
+	return cudaMemcpy(m->params, host, n * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess
+	    ? DMRGPP_OK
+	    : DMRGPP_CUDA_ERROR;
+}
+
+int dmrgpp_mlp_get_grads(dmrgpp_mlp_handle m, float* host, size_t n)
+{
+	if (!m || !host || n != dmrgpp::kNumParams)
+		return DMRGPP_INVALID_ARG;
+	return cudaMemcpy(host, m->grads, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess
+	    ? DMRGPP_OK
+	    : DMRGPP_CUDA_ERROR;
+}
+
+int dmrgpp_mlp_features(const double* diag, const double* r, double theta, double rnorm, size_t n,
+                        float* x, void* stream)
+{
+	if (!diag || !r || !x)
+		return DMRGPP_INVALID_ARG;
+	const double s   = std::max(1.0, std::fabs(theta));
+	const double rms = rnorm / std::sqrt(double(n > 0 ? n : 1));
+	dmrgpp::k_features<<<dmrgpp::grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+	    diag, r, theta, s, rms, n, x);
+	return cudaGetLastError() == cudaSuccess ? DMRGPP_OK : DMRGPP_CUDA_ERROR;
+}
+
+int dmrgpp_mlp_forward(dmrgpp_mlp_handle m, const float* x, int rows, float* out, void* stream)
+{
+	using namespace dmrgpp;
+	if (!m || !x || rows < 1)
+		return DMRGPP_INVALID_ARG;
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	if (int rc = ensure_rows(m, rows))
+		return rc;
+	forward(m, m->params, x, rows, st);
+	m->last_rows = rows;
+	if (out && cudaMemcpyAsync(out, m->out, size_t(rows) * sizeof(float), cudaMemcpyDeviceToDevice, st))
+		return mlp_fail(m, DMRGPP_CUDA_ERROR, "copy output");
+	return cudaGetLastError() == cudaSuccess ? DMRGPP_OK : mlp_fail(m, DMRGPP_CUDA_ERROR, "forward");
+}
+
+int dmrgpp_mlp_backward(dmrgpp_mlp_handle m, const float* x, const float* y, const float* weight,
+                        double* loss, void* stream)
+{
+	using namespace dmrgpp;
+	if (!m || !x || !y || m->last_rows < 1)
+		return DMRGPP_INVALID_ARG;
+	cudaStream_t st   = static_cast<cudaStream_t>(stream);
+	const int    rows = m->last_rows;
+	const float* P    = m->params;
+	float*       G    = m->grads;
+	const int    nbm  = std::min(4096, (rows + 255) / 256);
+	k_mse<<<nbm, 256, 0, st>>>(m->out, y, weight, rows, m->gout, m->loss, m->partial, m->ctr);
+	// head: dw3 = h2^T gout, db3 = sum gout
+	sgemm<true, false>(H, 1, rows, m->h2, H, m->gout, 1, G + kW3, 1, false, st);
+	k_colsum<<<1, 32, 0, st>>>(m->gout, rows, 1, G + kB3);
+	// layer 2: dz2 = gout w3 (1 - h2^2); dW2 = dz2^T h1; db2 = colsum dz2
+	k_head_back<<<grid_for(size_t(rows) * H), 256, 0, st>>>(m->gout, P + kW3, m->h2, m->dz, size_t(rows));
+	sgemm<true, false>(H, H, rows, m->dz, H, m->h1, H, G + kW2, H, false, st);
+	k_colsum<<<(H + 255) / 256, 256, 0, st>>>(m->dz, rows, H, G + kB2);
+	// layer 1: dz1 = (dz2 W2) (1 - h1^2); dW1 = dz1^T x; db1 = colsum dz1
+	sgemm<false, false>(rows, H, H, m->dz, H, P + kW2, H, m->dz1, H, false, st);
+	k_tanh_back<<<grid_for(size_t(rows) * H), 256, 0, st>>>(m->dz1, m->h1, size_t(rows) * H);
+	sgemm<true, false>(H, F, rows, m->dz1, H, x, F, G + kW1, F, false, st);
+	k_colsum<<<(H + 255) / 256, 256, 0, st>>>(m->dz1, rows, H, G + kB1);
+	if (loss && cudaMemcpyAsync(loss, m->loss, sizeof(double), cudaMemcpyDeviceToHost, st))
+		return mlp_fail(m, DMRGPP_CUDA_ERROR, "read loss");
+	if (cudaStreamSynchronize(st) != cudaSuccess)
+		return mlp_fail(m, DMRGPP_CUDA_ERROR, "backward");
+	return DMRGPP_OK;
+}
+
+int dmrgpp_mlp_adam_step(dmrgpp_mlp_handle m, float lr, void* stream)
+{
+	using namespace dmrgpp;
+	if (!m)
+		return DMRGPP_INVALID_ARG;
+	m->adam_t++;
+	const float b1 = 0.9f, b2 = 0.999f;
+	const float c1 = 1.f - std::pow(b1, float(m->adam_t)), c2 = 1.f - std::pow(b2, float(m->adam_t));
+	k_adam<<<grid_for(kNumParams), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+	    m->params, m->grads, m->adam_m, m->adam_v, kNumParams, lr, b1, b2, 1e-8f, c1, c2);
+	m->bf_dirty = true;
+	return cudaGetLastError() == cudaSuccess ? DMRGPP_OK : DMRGPP_CUDA_ERROR;
+}
+
+int dmrgpp_mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, double theta,
+                            double rnorm, double* t, size_t n, void* stream)
+{
+	return dmrgpp::mlp_precondition(m, diag, r, theta, rnorm, t, n, static_cast<cudaStream_t>(stream));
+}
+
+} // extern "C"

@@ -102,3 +102,65 @@ bool tridiag_eigen(int n, double* d, const double* off, double* z)
 }
 
 } // namespace dmrgpp
+
+namespace dmrgpp {
+
+bool sym_eigen(int n, const double* a, double* w, double* v)
+{
+	// cyclic Jacobi rotations (Golub and Van Loan, section 8.5): robust and
+	// accurate for the small projected matrices of the Davidson solver
+	std::vector<double> m(a, a + size_t(n) * size_t(n));
+	for (int i = 0; i < n; ++i)
+		for (int j = 0; j < n; ++j)
+			v[size_t(i) + size_t(j) * size_t(n)] = (i == j) ? 1.0 : 0.0;
+	auto M = [&](int i, int j) -> double& { return m[size_t(i) + size_t(j) * size_t(n)]; };
+	auto V = [&](int i, int j) -> double& { return v[size_t(i) + size_t(j) * size_t(n)]; };
+	for (int sweep = 0; sweep < 100; ++sweep) {
+		double off = 0.0, tot = 0.0;
+		for (int i = 0; i < n; ++i)
+			for (int j = 0; j < n; ++j) {
+				tot += M(i, j) * M(i, j);
+				if (i != j)
+					off += M(i, j) * M(i, j);
+			}
+		if (off <= 1e-30 * tot || off == 0.0)
+			break;
+		for (int p = 0; p < n - 1; ++p)
+			for (int q = p + 1; q < n; ++q) {
+				const double apq = M(p, q);
+				if (apq == 0.0)
+					continue;
+				const double theta = (M(q, q) - M(p, p)) / (2.0 * apq);
+				const double t     = std::copysign(1.0, theta) / (std::fabs(theta) + std::hypot(theta, 1.0));
+				const double c     = 1.0 / std::hypot(t, 1.0);
+				const double s     = t * c;
+				for (int k = 0; k < n; ++k) { // columns p, q
+					const double mkp = M(k, p), mkq = M(k, q);
+					M(k, p)          = c * mkp - s * mkq;
+					M(k, q)          = s * mkp + c * mkq;
+				}
+				for (int k = 0; k < n; ++k) { // rows p, q
+					const double mpk = M(p, k), mqk = M(q, k);
+					M(p, k)          = c * mpk - s * mqk;
+					M(q, k)          = s * mpk + c * mqk;
+				}
+				for (int k = 0; k < n; ++k) {
+					const double vkp = V(k, p), vkq = V(k, q);
+					V(k, p)          = c * vkp - s * vkq;
+					V(k, q)          = s * vkp + c * vkq;
+				}
+			}
+	}
+	std::vector<int> order(static_cast<size_t>(n));
+	std::iota(order.begin(), order.end(), 0);
+	std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return M(x, x) < M(y, y); });
+	std::vector<double> vv(v, v + size_t(n) * size_t(n));
+	for (int i = 0; i < n; ++i) {
+		w[i] = M(order[size_t(i)], order[size_t(i)]);
+		std::copy(vv.begin() + size_t(order[size_t(i)]) * size_t(n),
+		          vv.begin() + size_t(order[size_t(i)] + 1) * size_t(n), v + size_t(i) * size_t(n));
+	}
+	return true;
+}
+
+} // namespace dmrgpp

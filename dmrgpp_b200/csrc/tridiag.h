@@ -10,3 +10,11 @@ namespace dmrgpp {
 bool tridiag_eigen(int n, double* d, const double* off, double* z);
 
 } // namespace dmrgpp
+
+namespace dmrgpp {
+
+// Eigenvalues (ascending, w) and eigenvectors (v: n x n column-major) of the
+// dense symmetric matrix a (n x n column-major) by cyclic Jacobi rotations.
+bool sym_eigen(int n, const double* a, double* w, double* v);
+
+} // namespace dmrgpp

@@ -156,6 +156,59 @@ class BatchedGemm:
         _capi.check(rc, self._h)
         return e.value, z, int(n.value)
 
+    def davidson_lowest(self, init, preconditioner: int = 1, mlp=None, tolerance: float = 1e-8,
+                        max_iterations: int = 500, max_subspace: int = 32,
+                        mixed_tolerance: float = 1e-4, denominator_floor: float = 1e-3,
+                        raise_on_no_convergence: bool = True):
+        """Lowest eigenpair by the device Davidson.  preconditioner: 0 none,
+        1 Jacobi, 2 learned (mlp = dmrgpp_b200.mlp.MLPPreconditioner).
+        Returns (energy, ritz_vector, stats dict)."""
+        L = self._lib
+        p = _capi.DavidsonParams()
+        L.dmrgpp_davidson_params_init(ctypes.byref(p))
+        p.max_iterations, p.max_subspace, p.tolerance = max_iterations, max_subspace, tolerance
+        p.preconditioner = preconditioner
+        p.mlp = mlp.handle if mlp is not None else None
+        p.mixed_tolerance, p.denominator_floor = mixed_tolerance, denominator_floor
+        st = _capi.DavidsonStats()
+        e = ctypes.c_double()
+        if hasattr(init, "data_ptr"):
+            import torch
+            z = torch.empty_like(init)
+            self._pointers(init, z)
+            rc = L.dmrgpp_davidson_lowest(self._h, ctypes.byref(p), init.data_ptr(), 1,
+                                          ctypes.byref(e), z.data_ptr(), ctypes.byref(st))
+        else:
+            init = np.ascontiguousarray(init, dtype=np.float64)
+            z = np.empty(self.dim)
+            self._pointers(init, z)
+            rc = L.dmrgpp_davidson_lowest(self._h, ctypes.byref(p), init.ctypes.data, 0,
+                                          ctypes.byref(e), z.ctypes.data, ctypes.byref(st))
+        if rc != _capi.NOT_CONVERGED or raise_on_no_convergence:
+            _capi.check(rc, self._h)
+        stats = {f: getattr(st, f) for f, _ in _capi.DavidsonStats._fields_}
+        return e.value, z, stats
+
+    def diagonal(self):
+        """Diagonal of H (torch CUDA tensor, patch order)."""
+        import torch
+        d = torch.empty(self.dim, dtype=torch.float64, device="cuda")
+        _capi.check(self._lib.dmrgpp_kron_diagonal(self._h, d.data_ptr()), self._h)
+        torch.cuda.synchronize()
+        return d
+
+    def correction_solve(self, u, theta: float, r, max_iterations: int = 500,
+                         rel_tolerance: float = 1e-10):
+        """Exact correction t (torch CUDA tensors) of (I-uu^T)(H-theta)(I-uu^T) t = -r."""
+        import torch
+        t = torch.empty_like(u)
+        its = ctypes.c_int()
+        res = ctypes.c_double()
+        _capi.check(self._lib.dmrgpp_correction_solve(self._h, u.data_ptr(), theta, r.data_ptr(),
+                                                      t.data_ptr(), max_iterations, rel_tolerance,
+                                                      ctypes.byref(its), ctypes.byref(res)), self._h)
+        return t, its.value, res.value
+
     def autotune(self, cache_path: Optional[str] = None, reps: int = 10):
         """Picks the fastest tile configuration / work split for this sector
         (cached by sector shape in cache_path).  Returns (cfg, microseconds)."""

@@ -155,6 +155,32 @@ def spin_chain_like(sizes_left, sizes_right=None, seed: int = 20261203,
     return KronProblem(l, r, 5, A, B, name=name)
 
 
+def spin_chain_dominant(sizes, seed: int = 20261203, mixing: float = 0.15,
+                        name: str = "spin-chain-diagonal-dominant") -> KronProblem:
+    """Like spin_chain_like, but with block Hamiltonians close to diagonal in
+    their own basis (sorted level energies plus weak N(0, mixing^2) mixing)
+    and weaker boundary couplings, as for blocks expressed in bases close to
+    their energy eigenstates; the diagonal of H then carries the spectrum."""
+    p = spin_chain_like(sizes, seed=seed, name=name)
+    rng = np.random.default_rng(seed + 1)
+    for (i, j, k), a in list(p.A.items()):
+        if k == 0:   # H_L (x) I
+            n = a.shape[0]
+            h = np.diag(np.sort(rng.uniform(-4.0, 4.0, n))) + mixing * _sym(rng, n)
+            p.A[(i, j, k)] = np.asfortranarray(h)
+        elif k == 1:  # I (x) H_R
+            n = p.B[(i, j, k)].shape[0]
+            h = np.diag(np.sort(rng.uniform(-4.0, 4.0, n))) + mixing * _sym(rng, n)
+            p.B[(i, j, k)] = np.asfortranarray(h)
+        else:        # S.S couplings across the boundary
+            p.A[(i, j, k)] = np.asfortranarray(0.3 * a)
+    # keep S- = (S+)^T after the rescaling
+    for (i, j, k) in list(p.A):
+        if k == 4:
+            p.A[(i, j, 4)] = np.asfortranarray(p.A[(j, i, 3)].T)
+    return p
+
+
 def c2_problem(seed: int = 20261203) -> KronProblem:
     """Synthetic Kronecker-matvec microbench: left = right = 1024 states in 21
     Sz groups (discretised Gaussian, sigma = 4 groups), K = 5 terms,

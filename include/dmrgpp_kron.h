@@ -113,6 +113,9 @@ int dmrgpp_kron_synchronize(dmrgpp_kron_handle h);
  * without faulting the GPU. */
 int dmrgpp_kron_test_stall_dependency(dmrgpp_kron_handle h, int on);
 
+/* The diagonal of the sector's H (patch order) into diag (device pointer). */
+int dmrgpp_kron_diagonal(dmrgpp_kron_handle h, double* diag);
+
 /* Sector dimension D = sum_p l_p r_p (xy_patch_start, setup_sparse_batch.cpp:98-103). */
 int dmrgpp_kron_dim(dmrgpp_kron_handle h, size_t* dim);
 
@@ -197,6 +200,80 @@ void dmrgpp_lanczos_params_init(dmrgpp_lanczos_params* p);
 int dmrgpp_lanczos_lowest(dmrgpp_kron_handle h, const dmrgpp_lanczos_params* p,
                           const double* init, int on_device, double* energy, double* z,
                           size_t* steps_taken);
+
+/* ---- Davidson with a preconditioned correction (no counterpart in the
+ * reference, whose only eigensolver for this path is Lanczos) ---- */
+typedef struct dmrgpp_mlp_s* dmrgpp_mlp_handle;
+
+typedef enum {
+	DMRGPP_PRECOND_NONE   = 0, /* correction = residual */
+	DMRGPP_PRECOND_JACOBI = 1, /* correction = r / (theta - diag(H)) */
+	DMRGPP_PRECOND_MLP    = 2  /* learned: dmrgpp_mlp_* network */
+} dmrgpp_preconditioner;
+
+typedef struct {
+	size_t            max_iterations;    /* default 500 */
+	size_t            max_subspace;      /* restart size, default 32 */
+	double            tolerance;         /* stop when |r| <= tolerance * max(1, |theta|), default 1e-8 */
+	int               preconditioner;    /* dmrgpp_preconditioner, default Jacobi */
+	dmrgpp_mlp_handle mlp;               /* network for DMRGPP_PRECOND_MLP */
+	double            mixed_tolerance;   /* mixed handles: leave the mixed phase below this, default 1e-4 */
+	double            denominator_floor; /* Jacobi: |theta - d| >= floor * max(1,|theta|), default 1e-3 */
+} dmrgpp_davidson_params;
+
+typedef struct {
+	size_t iterations;    /* Rayleigh-Ritz steps */
+	size_t mixed_matvecs; /* H*x in the handle's mixed mode */
+	size_t fp64_matvecs;  /* H*x in FP64 */
+	size_t restarts;
+	double residual_norm; /* final FP64 |H u - theta u| */
+	int    converged;
+} dmrgpp_davidson_stats;
+
+void dmrgpp_davidson_params_init(dmrgpp_davidson_params* p);
+
+/* Lowest eigenpair by Davidson from init (patch order).  On a handle created
+ * with a mixed precision, the matvecs run in that mode until the residual
+ * falls below mixed_tolerance (or stalls), then the solver restarts from its
+ * Ritz vector in FP64 (FP64 refinement): the returned energy is the FP64
+ * Rayleigh quotient and the convergence test is on the FP64 residual.
+ * Returns DMRGPP_NOT_CONVERGED (with the best pair) after max_iterations. */
+int dmrgpp_davidson_lowest(dmrgpp_kron_handle h, const dmrgpp_davidson_params* p,
+                           const double* init, int on_device, double* energy, double* z,
+                           dmrgpp_davidson_stats* stats);
+
+/* Exact correction for training the learned preconditioner: solves
+ * (I - u u^T)(H - theta)(I - u u^T) t = -r, t orthogonal to u, by conjugate
+ * gradients in FP64 on the device (u unit norm, r orthogonal to u, theta
+ * below the second eigenvalue).  All vectors are device pointers. */
+int dmrgpp_correction_solve(dmrgpp_kron_handle h, const double* u, double theta, const double* r,
+                            double* t, int max_iterations, double rel_tolerance, int* iterations,
+                            double* rel_residual);
+
+/* ---- Learned preconditioner: per-element MLP 4 -> 256 -> 256 -> 1 ----
+ * Trained on the GPU by these kernels (FP32 master weights, Adam); inference
+ * uses BF16 weights with FP32 accumulation.  All arrays are device pointers
+ * unless named host. */
+size_t      dmrgpp_mlp_num_params(void);
+int         dmrgpp_mlp_create(unsigned long long seed, dmrgpp_mlp_handle* out);
+int         dmrgpp_mlp_destroy(dmrgpp_mlp_handle m);
+int         dmrgpp_mlp_get_params(dmrgpp_mlp_handle m, float* host, size_t n);
+int         dmrgpp_mlp_set_params(dmrgpp_mlp_handle m, const float* host, size_t n);
+int         dmrgpp_mlp_get_grads(dmrgpp_mlp_handle m, float* host, size_t n);
+/* features x (n x 4, float) of residual r at Ritz value theta with |r| = rnorm */
+int         dmrgpp_mlp_features(const double* diag, const double* r, double theta, double rnorm,
+                                size_t n, float* x, void* stream);
+/* FP32 forward of rows feature rows (activations kept for backward); out may be NULL */
+int         dmrgpp_mlp_forward(dmrgpp_mlp_handle m, const float* x, int rows, float* out, void* stream);
+/* gradients of the weighted mean squared error against targets y for the last
+ * forward (weight may be NULL); *loss (host) receives the loss; synchronous */
+int         dmrgpp_mlp_backward(dmrgpp_mlp_handle m, const float* x, const float* y,
+                                const float* weight, double* loss, void* stream);
+int         dmrgpp_mlp_adam_step(dmrgpp_mlp_handle m, float lr, void* stream);
+/* t = learned correction of residual r (what the Davidson solver applies) */
+int         dmrgpp_mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r,
+                                    double theta, double rnorm, double* t, size_t n, void* stream);
+const char* dmrgpp_mlp_last_error(dmrgpp_mlp_handle m);
 
 /* Host helper: eigenvalues (ascending) and, when vectors != NULL, eigenvectors
  * (n x n column-major) of the symmetric tridiagonal matrix diag/offdiag; the
