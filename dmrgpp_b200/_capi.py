@@ -75,6 +75,11 @@ class DavidsonStats(ctypes.Structure):
                 ("restarts", _sz), ("residual_norm", ctypes.c_double), ("converged", ctypes.c_int)]
 
 
+class RefineStats(ctypes.Structure):
+    _fields_ = [("outer_iterations", _sz), ("inner_matvecs", _sz), ("fp64_matvecs", _sz),
+                ("residual_norm", ctypes.c_double), ("converged", ctypes.c_int)]
+
+
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_MLP = 0, 1, 2
 _fp = ctypes.POINTER(ctypes.c_float)
 _vp = ctypes.c_void_p
@@ -86,6 +91,8 @@ SIGNATURES.update({
     "dmrgpp_correction_solve": (ctypes.c_int, [_vp, _vp, ctypes.c_double, _vp, _vp, ctypes.c_int,
                                                ctypes.c_double, ctypes.POINTER(ctypes.c_int), _dp]),
     "dmrgpp_kron_diagonal": (ctypes.c_int, [_vp, _vp]),
+    "dmrgpp_refine_lowest": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                            ctypes.c_double, _dp, ctypes.POINTER(RefineStats)]),
     "dmrgpp_mlp_num_params": (_sz, []),
     "dmrgpp_mlp_create": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_void_p)]),
     "dmrgpp_mlp_destroy": (ctypes.c_int, [_vp]),

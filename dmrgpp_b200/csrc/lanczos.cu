@@ -33,20 +33,29 @@ namespace dmrgpp {
 namespace {
 
 constexpr int kThreads   = 256;
-constexpr int kMaxBlocks = 296; // 2 per SM of a B200
+constexpr int kMaxBlocks = 1184; // 8 per SM of a B200
+constexpr int kDotBlocks = 296;  // grids of the basis projections (2 per SM)
 constexpr int kRowChunk  = 1024; // rows per block iteration of the basis GEMVs
 constexpr int kMaxCols   = 1024; // stored Lanczos vectors per solve
 
-// blocks of the basis GEMVs: up to 2 per SM, at least 256 rows each
+// blocks of the basis GEMVs: at least 256 rows each; the projections
+// (k_basis_dots, whose last block reduces kDotBlocks x columns partials) use
+// at most kDotBlocks, the row-parallel ones up to kMaxBlocks
 int basis_blocks_for(size_t n)
 {
 	const size_t b = (n + 255) / 256;
 	return int(std::max<size_t>(1, std::min<size_t>(b, kMaxBlocks)));
 }
 
+int dots_blocks_for(size_t n)
+{
+	const size_t b = (n + 255) / 256;
+	return int(std::max<size_t>(1, std::min<size_t>(b, kDotBlocks)));
+}
+
 int blocks_for(size_t n)
 {
-	const size_t b = (n + size_t(kThreads) * 8 - 1) / (size_t(kThreads) * 8);
+	const size_t b = (n + size_t(kThreads) * 4 - 1) / (size_t(kThreads) * 4);
 	return int(std::max<size_t>(1, std::min<size_t>(b, kMaxBlocks)));
 }
 
@@ -80,13 +89,27 @@ __device__ __forceinline__ bool last_block(unsigned* ctr)
 	return false;
 }
 
-// out = sum over blocks, in block order
-__device__ __forceinline__ double sum_partials(const double* partial, int nblk)
+// Grid-wide sum of one value per block, deterministic: every block stores its
+// value, the last block to arrive sums them with all its threads (fixed
+// strided order, then a fixed tree) and thread 0 writes *out (its square root
+// when root is set).  All threads of every block must call it.
+__device__ __forceinline__ void grid_sum(double block_value, double* partial, unsigned* ctr,
+                                         double* out, bool root, double* red)
 {
-	double s = 0.0;
-	for (int b = 0; b < nblk; ++b)
-		s += __ldcg(partial + b);
-	return s;
+	__shared__ bool last;
+	if (threadIdx.x == 0) {
+		partial[blockIdx.x] = block_value;
+		last                = last_block(ctr);
+	}
+	__syncthreads();
+	if (!last)
+		return;
+	double t = 0.0;
+	for (int b = threadIdx.x; b < int(gridDim.x); b += blockDim.x)
+		t += __ldcg(partial + b);
+	t = block_sum(t, red);
+	if (threadIdx.x == 0)
+		*out = root ? sqrt(t) : t;
 }
 
 // *out = <x, y>
@@ -95,18 +118,12 @@ k_dot(const double* __restrict__ x, const double* __restrict__ y, size_t n, doub
       double* partial, unsigned* ctr)
 {
 	__shared__ double red[kThreads / 32];
-	__shared__ bool   last;
 	double            s = 0.0;
 	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
 	     i += size_t(gridDim.x) * kThreads)
 		s += x[i] * y[i];
 	s = block_sum(s, red);
-	if (threadIdx.x == 0) {
-		partial[blockIdx.x] = s;
-		last                = last_block(ctr);
-		if (last)
-			*out = sum_partials(partial, gridDim.x);
-	}
+	grid_sum(s, partial, ctr, out, false, red);
 }
 
 // dst = src / sqrt(*nrm2) (nrm2 = <src,src> from k_dot)
@@ -138,11 +155,7 @@ k_lanczos_update(double* __restrict__ v2, const double* __restrict__ v1,
 		s += w * w;
 	}
 	s = block_sum(s, red);
-	if (threadIdx.x == 0) {
-		partial[blockIdx.x] = s;
-		if (last_block(ctr))
-			*beta_out = sqrt(sum_partials(partial, gridDim.x));
-	}
+	grid_sum(s, partial, ctr, beta_out, true, red);
 }
 
 // v *= 1 / *s when *s > 0 (LanczosVectors.h:233-237)
@@ -180,9 +193,17 @@ k_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* _
 		__syncthreads();
 		for (int c = warp; c < ncols; c += kThreads / 32) {
 			const double* col = V + size_t(c) * ld + base;
-			double        s   = 0.0;
-			for (int i = lane; i < len; i += 32)
-				s += col[i] * vs[i];
+			double        s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+			int           i  = lane;
+			for (; i + 96 < len; i += 128) {
+				s0 += col[i] * vs[i];
+				s1 += col[i + 32] * vs[i + 32];
+				s2 += col[i + 64] * vs[i + 64];
+				s3 += col[i + 96] * vs[i + 96];
+			}
+			for (; i < len; i += 32)
+				s0 += col[i] * vs[i];
+			double s = (s0 + s1) + (s2 + s3);
 			for (int o = 16; o > 0; o >>= 1)
 				s += __shfl_down_sync(0xffffffffu, s, o);
 			if (lane == 0)
@@ -226,11 +247,7 @@ k_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t ld
 		s += w * w;
 	}
 	s = block_sum(s, red);
-	if (threadIdx.x == 0) {
-		partial[blockIdx.x] = s;
-		if (last_block(ctr))
-			*nrm_out = sqrt(sum_partials(partial, gridDim.x));
-	}
+	grid_sum(s, partial, ctr, nrm_out, true, red);
 }
 
 // z = sum_c coef[c] V[:, c] (LanczosVectors::excitedVector, LanczosVectors.h:192-201)
@@ -431,6 +448,7 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 	cudaStream_t st = h->stream;
 	const int    nb = blocks_for(D);
 	const int    nbb = basis_blocks_for(D);
+	const int    nbd = dots_blocks_for(D);
 	double*      V  = w->V;
 	double*      alpha = w->scal;
 	double*      beta  = w->scal + w->cols;
@@ -476,7 +494,7 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 			k_scale_inv<<<nb, kThreads, 0, st>>>(v2, D, beta + jj + 1);
 			if (p->reortho) { // reorthoIfNecessary (LanczosVectors.h:243-271)
 				const int nc = int(jj) + 1;
-				k_basis_dots<<<nbb, kThreads, 0, st>>>(V, D, nc, v2, D, w->r, w->partial, w->ctr + 3);
+				k_basis_dots<<<nbd, kThreads, 0, st>>>(V, D, nc, v2, D, w->r, w->partial, w->ctr + 3);
 				k_basis_subtract<<<nbb, kThreads, 0, st>>>(v2, V, D, nc, w->r, D, work + 1,
 				                                          w->partial, w->ctr + 4);
 				k_scale_inv<<<nb, kThreads, 0, st>>>(v2, D, work + 1);
@@ -577,11 +595,7 @@ k_residual(const double* __restrict__ hu, const double* __restrict__ u, double t
 		s += w * w;
 	}
 	s = block_sum(s, red);
-	if (threadIdx.x == 0) {
-		partial[blockIdx.x] = s;
-		if (last_block(ctr))
-			*nrm = sqrt(sum_partials(partial, gridDim.x));
-	}
+	grid_sum(s, partial, ctr, nrm, true, red);
 }
 
 // diagonal (Jacobi) correction: t = r / (theta - d), denominators kept away
@@ -728,6 +742,7 @@ int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
 	cudaStream_t  st  = h->stream;
 	const int     nb  = blocks_for(D);
 	const int     nbb = basis_blocks_for(D);
+	const int     nbd = dots_blocks_for(D);
 	cudaError_t   e;
 	auto          Vc  = [&](int c) { return w->V + size_t(c) * D; };
 	auto          Wc  = [&](int c) { return w->W + size_t(c) * D; };
@@ -759,7 +774,7 @@ int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
 		// orthonormalise the correction against the basis (two classical
 		// Gram-Schmidt passes) and append it
 		for (int pass = 0; pass < (k > 0 ? 2 : 0); ++pass) {
-			k_basis_dots<<<nbb, kThreads, 0, st>>>(w->V, D, k, w->t, D, w->coef, w->partial, w->ctr + 0);
+			k_basis_dots<<<nbd, kThreads, 0, st>>>(w->V, D, k, w->t, D, w->coef, w->partial, w->ctr + 0);
 			k_basis_subtract<<<nbb, kThreads, 0, st>>>(w->t, w->V, D, k, w->coef, D, w->scal + 0,
 			                                          w->partial, w->ctr + 1);
 		}
@@ -772,7 +787,7 @@ int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
 		else
 			++s.fp64_matvecs;
 		// new column of the projected matrix G = V^T H V
-		k_basis_dots<<<nbb, kThreads, 0, st>>>(w->V, D, k + 1, Wc(k), D, w->coef, w->partial, w->ctr + 3);
+		k_basis_dots<<<nbd, kThreads, 0, st>>>(w->V, D, k + 1, Wc(k), D, w->coef, w->partial, w->ctr + 3);
 		if ((e = cudaMemcpyAsync(w->host, w->coef, size_t(k + 1) * sizeof(double),
 		                         cudaMemcpyDeviceToHost, st))
 		    || (e = cudaStreamSynchronize(st))) {
@@ -894,13 +909,52 @@ k_axpy(double a, const double* __restrict__ x, double* __restrict__ y, size_t n)
 		y[i] += a * x[i];
 }
 
-// y = x + a y
+// y -= (*a) x  (scalar from a reduction kernel)
 __global__ void __launch_bounds__(kThreads)
-k_xpay(const double* __restrict__ x, double a, double* __restrict__ y, size_t n)
+k_axpy_neg_dev(const double* a, const double* __restrict__ x, double* __restrict__ y, size_t n)
 {
+	const double c = *a;
 	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
 	     i += size_t(gridDim.x) * kThreads)
-		y[i] = x[i] + a * y[i];
+		y[i] -= c * x[i];
+}
+
+// conjugate-gradient update with device scalars: alpha = rr / pAp;
+// t += alpha p; res -= alpha Aq; *rr_next = |res|^2.  A non-positive pAp (or
+// an earlier one, *broken) freezes the iteration: alpha = 0 and *broken = 1.
+__global__ void __launch_bounds__(kThreads)
+k_cg_update(double* __restrict__ t, double* __restrict__ res, const double* __restrict__ p,
+            const double* __restrict__ Aq, const double* rr, const double* pAp, double* rr_next,
+            double* broken, size_t n, double* partial, unsigned* ctr)
+{
+	__shared__ double red[kThreads / 32];
+	const bool        stop  = *broken != 0.0 || !(*pAp > 0.0);
+	const double      alpha = stop ? 0.0 : *rr / *pAp;
+	if (stop && blockIdx.x == 0 && threadIdx.x == 0)
+		*broken = 1.0;
+	double s = 0.0;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		t[i] += alpha * p[i];
+		const double w = res[i] - alpha * Aq[i];
+		res[i]         = w;
+		s += w * w;
+	}
+	s = block_sum(s, red);
+	grid_sum(s, partial, ctr, rr_next, false, red);
+}
+
+// p = res + (rr_next / rr) p, skipped once the iteration is frozen
+__global__ void __launch_bounds__(kThreads)
+k_cg_direction(double* __restrict__ p, const double* __restrict__ res, const double* rr_next,
+               const double* rr, const double* broken, size_t n)
+{
+	if (*broken != 0.0)
+		return;
+	const double beta = *rr > 0.0 ? *rr_next / *rr : 0.0;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads)
+		p[i] = res[i] + beta * p[i];
 }
 
 } // namespace
@@ -926,71 +980,166 @@ int dmrgpp_correction_solve(dmrgpp_kron_handle h, const double* u, double theta,
 	using namespace dmrgpp;
 	if (!h || !u || !r || !t || max_iterations < 1)
 		return DMRGPP_INVALID_ARG;
-	const size_t D  = size_t(h->plan.dim());
+	const size_t D = size_t(h->plan.dim());
 	if (int rc = ensure_davidson(h, D, 2))
 		return rc;
 	DavidsonWork* w  = h->davidson;
 	cudaStream_t  st = h->stream;
 	const int     nb = blocks_for(D);
-	// work vectors: res = w->hu, p = w->r, q = w->t, Aq = second basis column
-	double*      res = w->hu;
-	double*      p   = w->r;
-	double*      q   = w->t;
-	double*      Aq  = w->V + D;
-	double*      sc  = w->scal;
+	// vectors: res = w->hu, p = w->r, Aq = second basis column; scalars
+	// sc[0] = u.v, sc[1] = pAp, sc[2], sc[3] = |res|^2 (alternating),
+	// sc[4] = frozen flag
+	double*     res = w->hu;
+	double*     p   = w->r;
+	double*     Aq  = w->V + D;
+	double*     sc  = w->scal;
+	cudaError_t e;
 	auto read = [&](double* dev, int count, double* host) {
 		return cudaMemcpyAsync(host, dev, size_t(count) * sizeof(double), cudaMemcpyDeviceToHost, st)
 		        == cudaSuccess
 		    && cudaStreamSynchronize(st) == cudaSuccess;
 	};
-	auto project = [&](double* v) { // v -= u (u . v)
-		k_dot<<<nb, kThreads, 0, st>>>(u, v, D, sc + 5, w->partial, w->ctr + 5);
-		double uv = 0;
-		if (!read(sc + 5, 1, &uv))
-			return false;
-		k_axpy<<<nb, kThreads, 0, st>>>(-uv, u, v, D);
-		return true;
-	};
 	// t = 0, res = -(I - uu^T) r, p = res
 	cudaMemsetAsync(t, 0, D * sizeof(double), st);
 	cudaMemsetAsync(res, 0, D * sizeof(double), st);
+	cudaMemsetAsync(sc + 4, 0, sizeof(double), st);
 	k_axpy<<<nb, kThreads, 0, st>>>(-1.0, r, res, D);
-	if (!project(res))
-		return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+	k_dot<<<nb, kThreads, 0, st>>>(u, res, D, sc + 0, w->partial, w->ctr + 5);
+	k_axpy_neg_dev<<<nb, kThreads, 0, st>>>(sc + 0, u, res, D);
 	cudaMemcpyAsync(p, res, D * sizeof(double), cudaMemcpyDeviceToDevice, st);
-	double rr = 0, b0 = 0;
-	k_dot<<<nb, kThreads, 0, st>>>(res, res, D, sc + 6, w->partial, w->ctr + 6);
-	if (!read(sc + 6, 1, &rr))
+	k_dot<<<nb, kThreads, 0, st>>>(res, res, D, sc + 2, w->partial, w->ctr + 6);
+	double host[4] = { 0, 0, 0, 0 };
+	if (!read(sc + 2, 1, host))
 		return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
-	b0 = std::sqrt(rr);
-	int it = 0;
-	for (; it < max_iterations && std::sqrt(rr) > rel_tolerance * b0 && b0 > 0; ++it) {
-		// Aq = P (H - theta) P p  (p stays orthogonal to u)
-		cudaMemcpyAsync(q, p, D * sizeof(double), cudaMemcpyDeviceToDevice, st);
-		if (int rc = kron_apply_device(h, q, Aq))
-			return rc;
-		k_axpy<<<nb, kThreads, 0, st>>>(-theta, q, Aq, D);
-		if (!project(Aq))
+	const double b0  = std::sqrt(host[0]);
+	double       rrh = host[0];
+	int          it  = 0;
+	int          cur = 0; // |res|^2 of the current iterate lives in sc[2 + cur]
+	while (it < max_iterations && b0 > 0 && std::sqrt(rrh) > rel_tolerance * b0) {
+		const int burst = std::min(8, max_iterations - it);
+		for (int q = 0; q < burst; ++q, ++it) {
+			// Aq = P (H - theta) p  (p orthogonal to u up to round-off)
+			if (int rc = kron_apply_device(h, p, Aq))
+				return rc;
+			k_axpy<<<nb, kThreads, 0, st>>>(-theta, p, Aq, D);
+			k_dot<<<nb, kThreads, 0, st>>>(u, Aq, D, sc + 0, w->partial, w->ctr + 5);
+			k_axpy_neg_dev<<<nb, kThreads, 0, st>>>(sc + 0, u, Aq, D);
+			k_dot<<<nb, kThreads, 0, st>>>(p, Aq, D, sc + 1, w->partial, w->ctr + 7);
+			k_cg_update<<<nb, kThreads, 0, st>>>(t, res, p, Aq, sc + 2 + cur, sc + 1, sc + 3 - cur,
+			                                     sc + 4, D, w->partial, w->ctr + 6);
+			k_cg_direction<<<nb, kThreads, 0, st>>>(p, res, sc + 3 - cur, sc + 2 + cur, sc + 4, D);
+			cur ^= 1;
+		}
+		if ((e = cudaGetLastError()))
+			return cuda_status(h, e, "correction solve launch");
+		if (!read(sc + 2, 3, host))
 			return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
-		double pAp = 0;
-		k_dot<<<nb, kThreads, 0, st>>>(p, Aq, D, sc + 7, w->partial, w->ctr + 7);
-		if (!read(sc + 7, 1, &pAp) || !(pAp > 0))
-			break; // the projected operator is not positive definite here
-		const double alpha = rr / pAp;
-		k_axpy<<<nb, kThreads, 0, st>>>(alpha, p, t, D);
-		k_axpy<<<nb, kThreads, 0, st>>>(-alpha, Aq, res, D);
-		double rr_new = 0;
-		k_dot<<<nb, kThreads, 0, st>>>(res, res, D, sc + 6, w->partial, w->ctr + 6);
-		if (!read(sc + 6, 1, &rr_new))
-			return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
-		k_xpay<<<nb, kThreads, 0, st>>>(res, rr_new / rr, p, D);
-		rr = rr_new;
+		rrh = host[cur];
+		if (host[2] != 0.0)
+			break; // the projected operator was not positive definite
 	}
 	if (iterations)
 		*iterations = it;
 	if (rel_residual)
-		*rel_residual = b0 > 0 ? std::sqrt(rr) / b0 : 0.0;
-	return cudaStreamSynchronize(st) == cudaSuccess ? DMRGPP_OK : handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+		*rel_residual = b0 > 0 ? std::sqrt(rrh) / b0 : 0.0;
+	return cudaStreamSynchronize(st) == cudaSuccess ? DMRGPP_OK
+	                                                : handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// FP64 residual refinement of an approximate lowest eigenvector computed with
+// mixed-precision matvecs: each outer step forms the FP64 Rayleigh quotient
+// theta = <psi|H|psi> and residual r = H psi - theta psi, solves the
+// projected correction equation (I - psi psi^T)(H - theta)(I - psi psi^T) t
+// = -r by conjugate gradients with the handle's (mixed) matvecs, and sets
+// psi <- (psi + t)/|psi + t|.  No counterpart in the reference.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int dmrgpp_refine_lowest(dmrgpp_kron_handle h, double* psi, int max_outer, double tolerance,
+                         int inner_iterations, double inner_tolerance, double* energy,
+                         dmrgpp_refine_stats* stats)
+{
+	using namespace dmrgpp;
+	if (!h || !psi || !energy || max_outer < 0 || inner_iterations < 1)
+		return DMRGPP_INVALID_ARG;
+	const size_t D = size_t(h->plan.dim());
+	int          prev = -1;
+	cudaGetDevice(&prev);
+	if (prev != h->device)
+		cudaSetDevice(h->device);
+	struct Restore {
+		int dev, prev;
+		~Restore()
+		{
+			if (dev != prev && prev >= 0)
+				cudaSetDevice(prev);
+		}
+	} restore { h->device, prev };
+	if (int rc = ensure_davidson(h, D, 2))
+		return rc;
+	DavidsonWork* w    = h->davidson;
+	cudaStream_t  st   = h->stream;
+	const int     nb   = blocks_for(D);
+	double*       hpsi = w->W;     // W column 0
+	double*       r    = w->W + D; // W column 1
+	double*       t    = w->V;     // V column 0 (the correction solve uses column 1)
+	const int     user = h->precision;
+	dmrgpp_refine_stats s {};
+	double        theta = 0.0, rnorm = 0.0;
+	int           rc    = DMRGPP_OK;
+	cudaError_t   e;
+	for (int outer = 0; outer <= max_outer; ++outer) {
+		// normalise psi, then FP64 Rayleigh quotient and residual
+		k_dot<<<nb, kThreads, 0, st>>>(psi, psi, D, w->scal + 8, w->partial, w->ctr + 8);
+		k_scale_rsqrt<<<nb, kThreads, 0, st>>>(psi, psi, D, w->scal + 8);
+		h->precision = DMRGPP_FP64;
+		rc           = kron_apply_device(h, psi, hpsi);
+		h->precision = user;
+		if (rc)
+			break;
+		++s.fp64_matvecs;
+		k_dot<<<nb, kThreads, 0, st>>>(psi, hpsi, D, w->scal + 9, w->partial, w->ctr + 9);
+		if ((e = cudaMemcpyAsync(w->host, w->scal + 9, sizeof(double), cudaMemcpyDeviceToHost, st))
+		    || (e = cudaStreamSynchronize(st))) {
+			rc = cuda_status(h, e, "refinement Rayleigh quotient");
+			break;
+		}
+		theta = w->host[0];
+		k_residual<<<nb, kThreads, 0, st>>>(hpsi, psi, theta, r, D, w->scal + 10, w->partial,
+		                                    w->ctr + 10);
+		if ((e = cudaMemcpyAsync(w->host, w->scal + 10, sizeof(double), cudaMemcpyDeviceToHost, st))
+		    || (e = cudaStreamSynchronize(st))) {
+			rc = cuda_status(h, e, "refinement residual");
+			break;
+		}
+		rnorm = w->host[0];
+		s.outer_iterations = size_t(outer);
+		if (rnorm <= tolerance * std::max(1.0, std::fabs(theta))) {
+			s.converged = 1;
+			break;
+		}
+		if (outer == max_outer)
+			break;
+		int    its = 0;
+		double rel = 0.0;
+		if ((rc = dmrgpp_correction_solve(h, psi, theta, r, t, inner_iterations, inner_tolerance, &its,
+		                                  &rel)))
+			break;
+		s.inner_matvecs += size_t(its);
+		k_axpy<<<nb, kThreads, 0, st>>>(1.0, t, psi, D);
+	}
+	if (rc)
+		return rc;
+	if (h->err_host && *reinterpret_cast<volatile int*>(h->err_host))
+		return handle_fail(h, DMRGPP_TIMEOUT, "H*x kernel wait gave up during refinement");
+	*energy         = theta;
+	s.residual_norm = rnorm;
+	if (stats)
+		*stats = s;
+	return s.converged ? DMRGPP_OK : handle_fail(h, DMRGPP_NOT_CONVERGED, "refinement did not converge");
 }
 
 } // extern "C"

@@ -189,6 +189,22 @@ class BatchedGemm:
         stats = {f: getattr(st, f) for f, _ in _capi.DavidsonStats._fields_}
         return e.value, z, stats
 
+    def refine_lowest(self, psi, max_outer: int = 6, tolerance: float = 1e-9,
+                      inner_iterations: int = 200, inner_tolerance: float = 1e-4,
+                      raise_on_no_convergence: bool = True):
+        """FP64 residual refinement of psi (torch CUDA tensor, updated in place);
+        the correction solves use the handle's current precision.  Returns
+        (energy, stats dict)."""
+        st = _capi.RefineStats()
+        e = ctypes.c_double()
+        self._pointers(psi, psi)
+        rc = self._lib.dmrgpp_refine_lowest(self._h, psi.data_ptr(), max_outer, tolerance,
+                                            inner_iterations, inner_tolerance, ctypes.byref(e),
+                                            ctypes.byref(st))
+        if rc != _capi.NOT_CONVERGED or raise_on_no_convergence:
+            _capi.check(rc, self._h)
+        return e.value, {f: getattr(st, f) for f, _ in _capi.RefineStats._fields_}
+
     def diagonal(self):
         """Diagonal of H (torch CUDA tensor, patch order)."""
         import torch

@@ -1,0 +1,100 @@
+"""Sector eigensolves as they occur in one finite-sweep step, timed on the
+device: the plain FP64 method (Lanczos with full reorthogonalisation, the
+reference's PsimagLite::LanczosSolver configuration) against the
+mixed-precision Davidson with FP64 refinement and a learned (or diagonal)
+preconditioner.  Energies are compared per site and states by overlap."""
+from __future__ import annotations
+
+import os
+import time
+from typing import Dict
+
+import numpy as np
+
+from . import plugin
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LADDER_WEIGHTS = os.path.join(HERE, "weights", "ladder_mlp.npz")
+
+
+def _timed(fn):
+    import torch
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    a.record()
+    out = fn()
+    b.record()
+    b.synchronize()
+    return out, a.elapsed_time(b) / 1e3, time.perf_counter() - t0
+
+
+def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int = 300,
+                  tolerance: float = 1e-9, mixed_steps: int = 100,
+                  refine_inner: int = 60, with_davidson: bool = True) -> Dict:
+    """Lowest state of one sector by
+      fp64_lanczos           -- the plain method: FP64 Lanczos, full reorthogonalisation,
+                                eigenvalue-change tolerance 1e-12 (reference defaults);
+      fp64_davidson          -- FP64 Davidson, Jacobi correction, |r| <= tolerance |E|
+                                (the converged FP64 pair the others are compared with);
+      mixed_lanczos_refined  -- TF32x3 Lanczos (FP64 recurrence and reorthogonalisation)
+                                for mixed_steps steps, then FP64 Rayleigh-quotient and
+                                residual refinement with TF32x3 correction solves;
+      mixed_davidson         -- TF32x3 Davidson with the learned (or Jacobi)
+                                correction, FP64 restart phase.
+    Seconds are device time around each whole solve (host work included)."""
+    import torch
+    bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+    init = torch.from_numpy(np.random.default_rng(seed).standard_normal(prob.dim)).cuda()
+    out = {"sector_dim": prob.dim, "f_alg_per_matvec": prob.flops(), "sites": sites}
+
+    bg.set_precision(plugin.FP64)
+    bg.autotune(None, reps=3)
+    (e_l, z_l, n_l), t_l, _ = _timed(lambda: bg.lanczos_lowest(init, steps=lanczos_steps,
+                                                              tolerance=1e-12))
+    out["fp64_lanczos"] = {"energy": e_l, "seconds": t_l, "matvecs": n_l + 1}
+
+    (e_j, z_j, s_j), t_j, _ = _timed(lambda: bg.davidson_lowest(
+        init, preconditioner=1, tolerance=tolerance, max_iterations=4000,
+        raise_on_no_convergence=False))
+    out["fp64_davidson"] = {"energy": e_j, "seconds": t_j, "matvecs": s_j["fp64_matvecs"],
+                            "converged": s_j["converged"]}
+
+    def compare(e, z):
+        return {"abs_dE_per_site_vs_fp64": abs(e - e_j) / sites,
+                "one_minus_overlap_vs_fp64": 1.0 - abs(float(torch.dot(z, z_j))),
+                "abs_dE_per_site_vs_fp64_lanczos": abs(e - e_l) / sites}
+
+    bg.set_precision(plugin.TF32X3)
+
+    def mixed_refined():
+        e1, z1, n1 = bg.lanczos_lowest(init, steps=mixed_steps, tolerance=1e-4)
+        e2, st = bg.refine_lowest(z1, max_outer=8, tolerance=tolerance,
+                                  inner_iterations=refine_inner, inner_tolerance=1e-5,
+                                  raise_on_no_convergence=False)
+        return e2, z1, n1, st
+    (e_r, z_r, n_r, st_r), t_r, _ = _timed(mixed_refined)
+    out["mixed_lanczos_refined"] = dict(
+        energy=e_r, seconds=t_r, mixed_lanczos_steps=n_r + 1,
+        refine_mixed_matvecs=st_r["inner_matvecs"], fp64_matvecs=st_r["fp64_matvecs"],
+        converged=st_r["converged"], **compare(e_r, z_r))
+    out["speedup_vs_fp64_lanczos"] = t_l / t_r
+
+    if with_davidson:
+        pre = 2 if mlp is not None else 1
+        (e_m, z_m, s_m), t_m, _ = _timed(lambda: bg.davidson_lowest(
+            init, preconditioner=pre, mlp=mlp, tolerance=tolerance, max_iterations=4000,
+            raise_on_no_convergence=False))
+        out["mixed_davidson"] = dict(
+            energy=e_m, seconds=t_m, mixed_matvecs=s_m["mixed_matvecs"],
+            fp64_matvecs=s_m["fp64_matvecs"], converged=s_m["converged"],
+            preconditioner="learned" if mlp is not None else "jacobi", **compare(e_m, z_m))
+    bg.close()
+    return out
+
+
+def load_ladder_mlp():
+    from .mlp import MLPPreconditioner
+    if os.path.exists(LADDER_WEIGHTS):
+        return MLPPreconditioner.load(LADDER_WEIGHTS)
+    return None

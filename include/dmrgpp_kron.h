@@ -250,6 +250,27 @@ int dmrgpp_correction_solve(dmrgpp_kron_handle h, const double* u, double theta,
                             double* t, int max_iterations, double rel_tolerance, int* iterations,
                             double* rel_residual);
 
+/* FP64 residual refinement of an approximate lowest eigenvector psi (device,
+ * patch order, updated in place), typically the Ritz vector of a solve with
+ * mixed-precision matvecs.  Each outer step computes in FP64 the Rayleigh
+ * quotient theta and residual r = H psi - theta psi; while |r| > tolerance *
+ * max(1, |theta|) it solves the projected correction equation
+ * (I - psi psi^T)(H - theta)(I - psi psi^T) t = -r by conjugate gradients
+ * with the handle's current (mixed) matvecs (inner_iterations,
+ * inner_tolerance) and sets psi <- (psi + t) / |psi + t|.  energy = final
+ * FP64 Rayleigh quotient.  No counterpart in the reference. */
+typedef struct {
+	size_t outer_iterations;
+	size_t inner_matvecs; /* matvecs of the correction solves (handle precision) */
+	size_t fp64_matvecs;
+	double residual_norm; /* final FP64 |H psi - theta psi| */
+	int    converged;
+} dmrgpp_refine_stats;
+
+int dmrgpp_refine_lowest(dmrgpp_kron_handle h, double* psi, int max_outer, double tolerance,
+                         int inner_iterations, double inner_tolerance, double* energy,
+                         dmrgpp_refine_stats* stats);
+
 /* ---- Learned preconditioner: per-element MLP 4 -> 256 -> 256 -> 1 ----
  * Trained on the GPU by these kernels (FP32 master weights, Adam); inference
  * uses BF16 weights with FP32 accumulation.  All arrays are device pointers
