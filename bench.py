@@ -37,6 +37,8 @@ def parse():
     p.add_argument("--workload", default="c2", choices=["c2", "ladder"])
     p.add_argument("--precision", default="fp64", choices=["fp64"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-sweep", action="store_true",
+                   help="skip the ladder-sector solve and mixed-precision measurements")
     return p.parse_args()
 
 
@@ -212,6 +214,46 @@ def read_traffic(workload):
     return None
 
 
+def ladder_measurements(torch, dev, stream):
+    """Ladder-shaped sector (16000 x 16000 states, 241 (N_up, N_down) patches,
+    K = 10, D = 3.37e6): the H*x throughput in FP64 and TF32x3, and one
+    sector eigensolve as in a finite-sweep step, plain FP64 Lanczos against
+    TF32x3 Lanczos + FP64 refinement (dmrgpp_b200.sweep)."""
+    from dmrgpp_b200 import plugin, sweep
+    from dmrgpp_b200 import superblock as sb
+    prob = sb.ladder_problem()
+    f = prob.flops()
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    bg = plugin.BatchedGemm.from_problem(prob, stream=stream.cuda_stream,
+                                         precision=plugin.TF32X3)
+    bg.set_precision(plugin.FP64)
+    bg.autotune(None, reps=3)
+    x = torch.from_numpy(np.random.default_rng(5).standard_normal(prob.dim)).to(dev)
+    y = torch.empty_like(x)
+    out = {"workload": prob.name, "sector_dim": prob.dim, "f_alg_per_matvec": f,
+           "sites": 64}
+    for name, prec in (("fp64", plugin.FP64), ("tf32x3", plugin.TF32X3)):
+        bg.set_precision(prec)
+        for _ in range(3):
+            bg.apply_Htarget(x, y)
+        ts = []
+        for _ in range(10):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            bg.apply_Htarget(x, y)
+            b.record(stream)
+            ts.append((a, b))
+        torch.cuda.synchronize()
+        t = statistics.median(a.elapsed_time(b) for a, b in ts) / 1e3
+        out[f"matvec_{name}"] = {"ms": t * 1e3, "tflops_alg": f / t / 1e12}
+    bg.close()
+    out["matvec_speedup_tf32x3_vs_fp64"] = out["matvec_fp64"]["ms"] / out["matvec_tf32x3"]["ms"]
+    out["solve"] = sweep.sector_solves(prob, sites=64, mixed_steps=100, refine_inner=60,
+                                       with_davidson=False)
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -232,6 +274,7 @@ def run_ours(args):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     bg = plugin.BatchedGemm.from_problem(prob, stream=stream.cuda_stream, device=local)
+    tuned_cfg, tuned_us = bg.autotune(None, reps=5)
     D = prob.dim
     x_host = torch.from_numpy(np.random.default_rng(100 + rank).standard_normal(D)).pin_memory()
     y_host = torch.empty(D, dtype=torch.float64).pin_memory()
@@ -299,6 +342,9 @@ def run_ours(args):
 
     peak = measured_fp64_peak(torch, dev) if rank == 0 else None
     bg.close()
+    sweep_step = None
+    if rank == 0 and world == 1 and not args.no_sweep:
+        sweep_step = ladder_measurements(torch, dev, stream)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -326,7 +372,10 @@ def run_ours(args):
                                     "in MEASURED_PEAKS.json)"},
         "gpu_launches": args.steps,
         "clocks": clocks.summary(),
+        "tuning": {"tile_config": tuned_cfg, "autotune_best_us": tuned_us},
     }
+    if sweep_step is not None:
+        line["sweep_step"] = sweep_step
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(prob, f_alg)
     print(json.dumps(line))
