@@ -13,6 +13,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import sys
 import threading
@@ -205,13 +206,14 @@ def measured_fp64_peak(torch, dev):
 
 
 def read_traffic(workload):
-    path = os.path.join(ROOT, "profiles", f"grouped_dgemm_{workload}_traffic.json")
-    if os.path.exists(path):
-        try:
-            return json.load(open(path)).get("bytes_per_matvec")
-        except Exception:
-            return None
-    return None
+    """dram__bytes_read.sum + dram__bytes_write.sum of one kron_persistent
+    launch on this workload, from the committed ncu summary (a line
+    `traffic_bytes_per_launch: N`)."""
+    path = os.path.join(ROOT, "profiles", f"kron_persistent_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"^traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read(), re.M)
+    return float(m.group(1)) if m else None
 
 
 def ladder_measurements(torch, dev, stream):

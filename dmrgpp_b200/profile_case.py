@@ -1,0 +1,61 @@
+"""Runs a fixed number of H*x applies (or one sector solve) of a named sector
+on cuda:0 and nothing else, so that a profiler's launch list and captures see
+only the kernels of that workload.
+
+    python -m dmrgpp_b200.profile_case c2 [--precision fp64|tf32x3] [--applies N]
+                                          [--config C --ipc I]
+    python -m dmrgpp_b200.profile_case ladder --states 4000 --precision tf32x3
+    python -m dmrgpp_b200.profile_case ladder --states 4000 --solve lanczos
+
+Workloads: c2 = the 1024 x 1024-state, 21-group, K=5 microbench sector;
+ladder = the ladder-shaped (N_up, N_down) sector with `--states` left and
+right states (K = 10).  Prints one line "ok <dim> <F_alg> <|y|>" at the end.
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+
+
+def main(argv=None) -> int:
+    p = argparse.ArgumentParser()
+    p.add_argument("workload", choices=["c2", "ladder"])
+    p.add_argument("--states", type=int, default=4000, help="ladder: left = right states")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"])
+    p.add_argument("--applies", type=int, default=6)
+    p.add_argument("--config", type=int, default=None, help="FP64 tile configuration")
+    p.add_argument("--ipc", type=int, default=2, help="FP64 items per CTA")
+    p.add_argument("--solve", default=None, choices=["lanczos"],
+                   help="run one FP64 Lanczos solve instead of bare applies")
+    p.add_argument("--steps", type=int, default=60)
+    a = p.parse_args(argv)
+
+    import torch
+    from . import plugin
+    from . import superblock as sb
+
+    prob = (sb.c2_problem() if a.workload == "c2"
+            else sb.ladder_problem(total_states=a.states, sigma=2.5, seed=9))
+    prec = plugin.TF32X3 if a.precision == "tf32x3" else plugin.FP64
+    s = torch.cuda.Stream()
+    torch.cuda.set_stream(s)
+    bg = plugin.BatchedGemm.from_problem(prob, stream=s.cuda_stream, precision=prec)
+    if prec == plugin.FP64 and a.config is not None:
+        bg.set_config(a.config, a.ipc)
+    x = torch.from_numpy(sb.random_unit_vector(prob.dim)).cuda()
+    y = torch.empty_like(x)
+    if a.solve == "lanczos":
+        e, z, n = bg.lanczos_lowest(x, steps=a.steps, tolerance=1e-12)
+        y = z
+        print("E", e, "steps", n)
+    else:
+        for _ in range(a.applies):
+            bg.apply_Htarget(x, y)
+    torch.cuda.synchronize()
+    print("ok", prob.dim, prob.flops(), float(y.norm()))
+    bg.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
