@@ -161,6 +161,7 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 	a1.segs   = h->m_seg1;
 	a1.tiles  = h->m_tile1;
 	a1.ntiles = int(mp.tile1.size());
+	a1.grid   = h->m_grid;
 	a1.error  = h->err_dev;
 	if ((e = tc_launch(a1, mp.bn, true, h->stream)))
 		return cuda_fail(h, e, "tensor-core pass 1 launch");
@@ -173,6 +174,7 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 	a2.segs   = h->m_seg2;
 	a2.tiles  = h->m_tile2;
 	a2.ntiles = int(mp.tile2.size());
+	a2.grid   = h->m_grid;
 	a2.error  = h->err_dev;
 	if ((e = tc_launch(a2, mp.bn, false, h->stream)))
 		return cuda_fail(h, e, "tensor-core pass 2 launch");
@@ -225,6 +227,8 @@ int build_mixed(dmrgpp_kron_handle h, const dmrgpp_kron_desc* d)
 	cudaError_t      e  = tc_init();
 	if (e != cudaSuccess)
 		return cuda_fail(h, e, "tensor-core kernel attributes");
+	if ((e = cudaDeviceGetAttribute(&h->m_grid, cudaDevAttrMultiProcessorCount, h->device)))
+		return cuda_fail(h, e, "SM count");
 	auto fbytes = [](long long n) { return size_t(n > 0 ? n : 1) * sizeof(float); };
 	if ((e = cudaMalloc(&h->m_ops_hi, fbytes(mp.ops_elems))) || (e = cudaMalloc(&h->m_ops_lo, fbytes(mp.ops_elems)))
 	    || (e = cudaMalloc(&h->m_xs_hi, fbytes(mp.xs_elems))) || (e = cudaMalloc(&h->m_xs_lo, fbytes(mp.xs_elems)))

@@ -50,6 +50,7 @@ struct dmrgpp_kron_s {
 	float*              m_bxs_hi = nullptr; // pass-1 result split
 	float*              m_bxs_lo = nullptr;
 	int*                m_xmap   = nullptr; // sector vector -> x split offsets
+	int                 m_grid   = 0;       // persistent CTAs of the tensor-core passes
 	void*               m_lists  = nullptr; // seg1, seg2, tile1, tile2
 	dmrgpp::GemmSeg*    m_seg1 = nullptr;
 	dmrgpp::GemmSeg*    m_seg2 = nullptr;

@@ -434,36 +434,38 @@ std::string build_mixed_plan(KronPlan&            plan,
 	mp              = MixedPlan();
 	mp.bn           = bn;
 	const size_t np = plan.np, nt = plan.triples.size(), np2 = np * np;
-	mp.P.resize(np);
-	mp.Q.resize(np);
-	for (size_t p = 0; p < np; ++p) {
-		mp.P[p] = round32(plan.r[p]);
-		mp.Q[p] = round32(plan.l[p]);
+	// (i,k) groups of Bstack_j / BX_j, in triple order, each padded to 8 rows
+	mp.Mp.assign(np, 0);
+	mp.group_row.assign(nt, 0);
+	for (size_t t = 0; t < nt; ++t) {
+		const Triple& tr = plan.triples[t];
+		mp.group_row[t]  = mp.Mp[tr.j];
+		mp.Mp[tr.j] += round8(plan.r[tr.i]);
 	}
 	long long off = 0;
 	mp.bs_off.assign(np, 0);
 	for (size_t j = 0; j < np; ++j) {
 		mp.bs_off[j] = off;
-		off += plan.M[j] * mp.P[j];
+		off += mp.Mp[j] * round32(plan.r[j]);
 	}
 	mp.at_off.assign(nt, 0);
 	for (size_t t = 0; t < nt; ++t) {
 		mp.at_off[t] = off;
-		off += plan.l[plan.triples[t].i] * mp.Q[plan.triples[t].j];
+		off += round8(plan.l[plan.triples[t].i]) * round32(plan.l[plan.triples[t].j]);
 	}
 	mp.ops_elems = off;
 	off          = 0;
 	mp.xs_off.assign(np, 0);
 	for (size_t p = 0; p < np; ++p) {
 		mp.xs_off[p] = off;
-		off += plan.l[p] * mp.P[p];
+		off += round8(plan.l[p]) * round32(plan.r[p]);
 	}
 	mp.xs_elems = off;
 	off         = 0;
 	mp.bxs_off.assign(np, 0);
 	for (size_t j = 0; j < np; ++j) {
 		mp.bxs_off[j] = off;
-		off += plan.M[j] * mp.Q[j];
+		off += mp.Mp[j] * round32(plan.l[j]);
 	}
 	mp.bxs_elems = off;
 	if (mp.ops_elems > INT_MAX || mp.xs_elems > INT_MAX || mp.bxs_elems > INT_MAX)
@@ -477,47 +479,52 @@ std::string build_mixed_plan(KronPlan&            plan,
 		for (size_t t = 0; t < nt; ++t) {
 			const Triple& tr = plan.triples[t];
 			const size_t  ix = size_t(tr.i) + size_t(tr.j) * np + size_t(tr.k) * np2;
-			// Bstack_j row (row_off + q), column c = B_k(i,j)(q, c), K-major
+			// Bstack_j row (group_row + q), K index c: B_k(i,j)(q, c)
 			const double*   b  = B[ix];
-			const long long Pj = mp.P[tr.j];
+			const long long Mj = mp.Mp[tr.j];
 			for (long long q = 0; q < plan.r[tr.i]; ++q) {
-				const long long row = plan.row_off[t] + q;
-				for (long long c = 0; c < plan.r[tr.j]; ++c)
-					split_tf32(b[q + c * (long long)ldB[ix]], H + mp.bs_off[tr.j] + row * Pj + c,
-					           L + mp.bs_off[tr.j] + row * Pj + c);
+				const long long row = mp.group_row[t] + q;
+				for (long long c = 0; c < plan.r[tr.j]; ++c) {
+					const long long o = mp.bs_off[tr.j] + chunked_offset(Mj, row, c);
+					split_tf32(b[q + c * (long long)ldB[ix]], H + o, L + o);
+				}
 			}
-			// A^T: column n (< l_i) holds A_k(i,j)(n, 0..l_j), pitch Q_j
+			// A^T row n (< l_i), K index k (< l_j): A_k(i,j)(n, k)
 			const double*   a  = A[ix];
-			const long long Qj = mp.Q[tr.j];
+			const long long Ri = round8(plan.l[tr.i]);
 			for (long long n = 0; n < plan.l[tr.i]; ++n)
-				for (long long k = 0; k < plan.l[tr.j]; ++k)
-					split_tf32(a[n + k * (long long)ldA[ix]], H + mp.at_off[t] + n * Qj + k,
-					           L + mp.at_off[t] + n * Qj + k);
+				for (long long k = 0; k < plan.l[tr.j]; ++k) {
+					const long long o = mp.at_off[t] + chunked_offset(Ri, n, k);
+					split_tf32(a[n + k * (long long)ldA[ix]], H + o, L + o);
+				}
 		}
 	}
 	if (x_map) {
+		// X_p(iR, iL) -> row iL, K index iR of the x split
 		x_map->assign(size_t(plan.dim()), 0);
-		for (size_t p = 0; p < np; ++p)
+		for (size_t p = 0; p < np; ++p) {
+			const long long Lp = round8(plan.l[p]);
 			for (long long n = 0; n < plan.l[p]; ++n)
 				for (long long k = 0; k < plan.r[p]; ++k)
 					(*x_map)[size_t(plan.xy_start[p] + k + n * plan.r[p])]
-					    = int(mp.xs_off[p] + n * mp.P[p] + k);
+					    = int(mp.xs_off[p] + chunked_offset(Lp, n, k));
+		}
 	}
 
-	// pass 1: C = BX_j split (row-major, pitch Q_j)
+	// pass 1: C = BX_j split (every padded row, K-chunks of l_j)
 	for (size_t j = 0; j < np; ++j) {
-		if (plan.M[j] == 0)
+		if (mp.Mp[j] == 0)
 			continue;
 		GemmSeg s {};
 		s.a_off = mp.bs_off[j];
-		s.lda   = int(mp.P[j]);
+		s.lda   = int(mp.Mp[j]);
 		s.b_off = mp.xs_off[j];
-		s.ldb   = int(mp.P[j]);
-		s.K     = int(mp.P[j]);
+		s.ldb   = int(round8(plan.l[j]));
+		s.K     = int(round32(plan.r[j]));
 		s.dep   = int(j);
 		const int sb = int(mp.seg1.size());
 		mp.seg1.push_back(s);
-		add_tc_tiles(mp.tile1, mp.bxs_off[j], mp.Q[j], plan.M[j], plan.l[j], sb, sb + 1, mp.bm, bn);
+		add_tc_tiles(mp.tile1, mp.bxs_off[j], mp.Mp[j], mp.Mp[j], plan.l[j], sb, sb + 1, mp.bm, bn);
 	}
 	// pass 2: C = Y_i (FP64, column-major)
 	size_t t = 0;
@@ -526,11 +533,11 @@ std::string build_mixed_plan(KronPlan&            plan,
 		for (; t < nt && plan.triples[t].i == int(i); ++t) {
 			const Triple& tr = plan.triples[t];
 			GemmSeg       s {};
-			s.a_off = mp.bxs_off[tr.j] + plan.row_off[t] * mp.Q[tr.j];
-			s.lda   = int(mp.Q[tr.j]);
+			s.a_off = mp.bxs_off[tr.j] + mp.group_row[t] * 32;
+			s.lda   = int(mp.Mp[tr.j]);
 			s.b_off = mp.at_off[t];
-			s.ldb   = int(mp.Q[tr.j]);
-			s.K     = int(mp.Q[tr.j]);
+			s.ldb   = int(round8(plan.l[i]));
+			s.K     = int(round32(plan.l[tr.j]));
 			s.dep   = tr.j;
 			mp.seg2.push_back(s);
 		}

@@ -75,16 +75,34 @@ struct Triple {
 };
 
 // Layout of the mixed-precision (tensor-core) form of a sector.  Every
-// operand is K-major with K padded to a multiple of 32 (zeros), split into
-// hi and lo parts of identical layout; offsets and pitches are in floats.
-//   pass 1: A = Bstack_j (M_j rows, pitch P_j = round32(r_j))
-//           B = X_j split (l_j columns, pitch P_j)
-//           C = BX_j split (M_j rows, pitch Q_j = round32(l_j))
-//   pass 2: A = rows of (i,k) in BX_j (pitch Q_j)
-//           B = A_k(i,j)^T (l_i columns, pitch Q_j)
+// operand is a "chunked K-major" matrix: rows padded to a multiple of 8 (Rp),
+// K padded to a multiple of 32 with zeros, stored chunk by chunk (32 K values
+// = 128 bytes per row), each chunk Rp rows x 128 bytes with the 16-byte
+// pieces of row r at position (piece ^ (r % 8)) -- the 128-byte swizzle that
+// tcgen05.mma reads through a shared-memory descriptor.  A 128-row tile of
+// one chunk is therefore one contiguous block, copied to shared memory by
+// one bulk copy.  Element (row, k) sits at chunked_offset(Rp, row, k).  Every
+// operand has a hi and a lo TF32 part of identical layout; offsets are floats.
+//   pass 1: A = Bstack_j (Mp_j rows: the (i,k) groups, each r_i rows padded
+//               to 8, at group_row[t]), K = r_j
+//           B = X_j split (Lp_j = round8(l_j) rows), K = r_j
+//           C = BX_j split (Mp_j rows, K = l_j for pass 2)
+//   pass 2: A = the (i,k) group of BX_j, K = l_j
+//           B = A_k(i,j)^T (round8(l_i) rows), K = l_j
 //           C = Y_i, FP64 column-major
+// GemmSeg of the mixed passes: a_off/b_off = float offset of the tile row 0
+// in chunk 0, lda/ldb = padded rows of the containing matrix (the chunk
+// stride is 32 times that), K = K padded to 32.  GemmTile: ldc = padded rows
+// of BX_j (pass 1) or r_i (pass 2).
+inline long long round8(long long x) { return (x + 7) / 8 * 8; }
+inline long long chunked_offset(long long rows_pad, long long row, long long k)
+{
+	return (k >> 5) * rows_pad * 32 + row * 32 + ((((k >> 2) & 7) ^ (row & 7)) << 2) + (k & 3);
+}
+
 struct MixedPlan {
-	std::vector<long long> P, Q;        // per patch
+	std::vector<long long> Mp;          // per input patch: padded rows of Bstack_j / BX_j
+	std::vector<long long> group_row;   // per triple: first row of (i,k) in Bstack_j / BX_j
 	std::vector<long long> bs_off;      // per input patch: Bstack_j in ops
 	std::vector<long long> at_off;      // per triple: A^T in ops
 	std::vector<long long> xs_off;      // per patch: X_j in the x split buffer

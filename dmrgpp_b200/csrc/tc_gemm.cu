@@ -4,20 +4,31 @@
 // one tile accumulates a_hi*b_hi + a_hi*b_lo + a_lo*b_hi in FP32 in tensor
 // memory (the a_lo*b_lo term is below the FP32 accumulation error).
 //
-// One CTA (4 warps) computes a 128 x BN output tile of a grouped pass
-// (kron_plan.h, MixedPlan): for every K-segment of the tile, 32-wide k-chunks
-// of A (128 rows) and B (BN rows), both K-major and split into hi/lo, are
-// staged by cp.async into shared memory in the 128-byte-swizzled K-major
-// layout that tcgen05.mma reads through shared-memory descriptors; thread 0
-// issues 3 x 4 MMAs (M=128, N=BN, K=8) per chunk into one TMEM accumulator
-// and commits them to the chunk's mbarrier, which frees the stage for the
-// next load.  The epilogue reads the accumulator with tcgen05.ld (warp w owns
-// TMEM lanes 32w..32w+31 = tile rows) and either splits it again into hi/lo
-// (pass 1, the A operand of pass 2) or widens it to FP64 (pass 2, y).
+// Persistent, warp-specialised CTAs (one per SM), each walking the tile list
+// of one grouped pass (kron_plan.h, MixedPlan) with stride gridDim.x:
+//   warp 0, one thread: producer.  For every 32-wide k-chunk of every
+//     K-segment of its tiles it waits until the ring stage is free, arms the
+//     stage's mbarrier with the byte count and issues four bulk copies
+//     (cp.async.bulk, global -> shared, completion counted on the mbarrier):
+//     the hi and lo parts of the A tile (128 rows) and of the B tile (BN
+//     rows).  The operands are stored chunked and pre-swizzled
+//     (MixedPlan), so each copy is one contiguous block that lands in the
+//     128-byte-swizzled K-major layout tcgen05.mma reads.
+//   warp 1, one thread: MMA issuer.  Per chunk it waits for the stage's
+//     bytes, issues 3 x 4 MMAs (M = 128, N = BN, K = 8) into the tile's TMEM
+//     accumulator and commits them to the stage's "empty" mbarrier; after
+//     the tile's last chunk it commits to the accumulator's "full" mbarrier.
+//     Two accumulators (2 x BN TMEM columns) alternate between tiles, so one
+//     tile's epilogue overlaps the next tile's loads and MMAs.
+//   warps 2-5: epilogue.  Warp w reads TMEM lanes 32(w % 4) .. +31 (tile
+//     rows) with tcgen05.ld and either splits the result into the hi/lo
+//     chunked layout of the next pass (pass 1: BX, the A operand of pass 2)
+//     or widens it to FP64 (pass 2: y), then frees the accumulator.
 //
-// Every mbarrier wait is bounded in time; a wait that gives up sets the
-// error word, waits (bounded) for the tensor core once more, frees TMEM and
-// leaves the tile unwritten.
+// Every mbarrier wait is bounded in time and also ends when another role
+// has given up (shared abort flag); a wait that gives up sets the error
+// word.  Before the CTA exits, the producer waits (bounded) for its last
+// copies and the MMA thread for its last MMAs, and TMEM is freed.
 #include "tc_gemm.cuh"
 
 #include <cstdint>
@@ -25,10 +36,10 @@
 namespace dmrgpp {
 namespace {
 
-constexpr int                kBM         = 128;
-constexpr int                kBK         = 32; // TF32 elements = 128 bytes per row per chunk
-constexpr unsigned long long kWaitNs     = 500ull * 1000ull * 1000ull;
-constexpr int                kTcThreads  = 128;
+constexpr int                kBM        = 128;
+constexpr int                kBK        = 32; // TF32 elements = 128 bytes per row per chunk
+constexpr unsigned long long kWaitNs    = 500ull * 1000ull * 1000ull;
+constexpr int                kTcThreads = 192; // producer, MMA, 4 epilogue warps
 
 __device__ __forceinline__ unsigned smem_addr(const void* p)
 {
@@ -42,45 +53,57 @@ __device__ __forceinline__ unsigned long long now_ns()
 	return t;
 }
 
-__device__ __forceinline__ void cp_async_16(unsigned dst, const void* src, bool pred)
-{
-	const int n = pred ? 16 : 0;
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(n)
-	             : "memory");
-}
-
-__device__ __forceinline__ void cp_async_commit()
-{
-	asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-
-template <int N> __device__ __forceinline__ void cp_async_wait()
-{
-	asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 __device__ __forceinline__ void mbar_init(unsigned addr, unsigned count)
 {
 	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(addr), "r"(count) : "memory");
 }
 
+__device__ __forceinline__ void mbar_expect_tx(unsigned addr, unsigned bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(addr), "r"(bytes)
+	             : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned addr)
+{
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(addr) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(unsigned addr, unsigned parity)
+{
+	unsigned ok;
+	asm volatile("{\n\t.reg .pred p;\n\t"
+	             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+	             "selp.u32 %0, 1, 0, p;\n\t}\n"
+	             : "=r"(ok)
+	             : "r"(addr), "r"(parity)
+	             : "memory");
+	return ok != 0;
+}
+
 // true once the phase of the given parity has completed; false after kWaitNs
-__device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity)
+// or, when abort is given, as soon as *abort is set
+__device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity, const volatile int* abort)
 {
 	const unsigned long long t0 = now_ns();
 	for (;;) {
-		unsigned ok;
-		asm volatile("{\n\t.reg .pred p;\n\t"
-		             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-		             "selp.u32 %0, 1, 0, p;\n\t}\n"
-		             : "=r"(ok)
-		             : "r"(addr), "r"(parity)
-		             : "memory");
-		if (ok)
+		if (mbar_try(addr, parity))
 			return true;
+		if (abort && *abort)
+			return false;
 		if (now_ns() - t0 > kWaitNs)
 			return false;
 	}
+}
+
+// bulk copy global -> this CTA's shared memory, completion counted in bytes
+// on the mbarrier (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned mbar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+	                 dst),
+	             "l"(src), "r"(bytes), "r"(mbar)
+	             : "memory");
 }
 
 // shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
@@ -143,69 +166,246 @@ __device__ __forceinline__ float tf32_rna(float f)
 	return __uint_as_float(u);
 }
 
+__device__ __forceinline__ int round8_dev(int x) { return (x + 7) & ~7; }
+
 template <int BN> struct TcLayout {
 	static constexpr int A_BYTES     = kBM * 128;
 	static constexpr int B_BYTES     = BN * 128;
 	static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
 };
 
-// one 32-wide k-chunk of the hi/lo A (128 rows) and B (BN rows) tiles,
-// 16-byte pieces placed at chunk ^ (row % 8) inside each 128-byte row
-template <int BN>
-__device__ __forceinline__ void load_chunk(unsigned stage, const TcArgs& a, const GemmSeg& sg, int k0,
-                                           const GemmTile& t)
+__device__ __forceinline__ int tile_chunks(const TcArgs& a, const GemmTile& t)
 {
-	using L = TcLayout<BN>;
-	constexpr int A_PIECES = kBM * 8 / kTcThreads;
-	constexpr int B_PIECES = BN * 8 / kTcThreads;
-#pragma unroll
-	for (int e = 0; e < A_PIECES; ++e) {
-		const int      idx  = threadIdx.x + e * kTcThreads;
-		const int      row  = idx >> 3;
-		const int      c    = idx & 7;
-		const bool     p    = t.m0 + row < t.M;
-		const long long off = sg.a_off + (long long)(t.m0 + (p ? row : 0)) * sg.lda + k0 + c * 4;
-		const unsigned dst  = unsigned(row * 128 + ((c ^ (row & 7)) << 4));
-		cp_async_16(stage + dst, a.A_hi + off, p);
-		cp_async_16(stage + L::A_BYTES + dst, a.A_lo + off, p);
+	int n = 0;
+	for (int s = t.seg_begin; s < t.seg_end; ++s)
+		n += a.segs[s].K / kBK;
+	return n;
+}
+
+__device__ __forceinline__ void give_up(volatile int* abort, int* error)
+{
+	*abort = 1;
+	atomicExch(error, 2);
+}
+
+// ---------------------------------------------------------------- producer
+template <int BN, int STAGES>
+__device__ void producer(const TcArgs& a, unsigned base, unsigned full0, unsigned empty0,
+                         volatile int* abort)
+{
+	using L    = TcLayout<BN>;
+	unsigned g = 0; // chunks issued
+	bool     ok = true;
+	for (int ti = blockIdx.x; ti < a.ntiles && ok; ti += gridDim.x) {
+		const GemmTile t     = a.tiles[ti];
+		const int      rowsA = min(kBM, round8_dev(t.M) - t.m0);
+		const int      rowsB = min(BN, round8_dev(t.N) - t.n0);
+		const unsigned ba = unsigned(rowsA) * 128u, bb = unsigned(rowsB) * 128u;
+		for (int s = t.seg_begin; s < t.seg_end && ok; ++s) {
+			const GemmSeg   sg = a.segs[s];
+			const int       nk = sg.K / kBK;
+			const long long ao = sg.a_off + (long long)t.m0 * kBK;
+			const long long bo = sg.b_off + (long long)t.n0 * kBK;
+			const long long as = (long long)sg.lda * kBK, bs = (long long)sg.ldb * kBK;
+			for (int c = 0; c < nk; ++c) {
+				const unsigned st = g % STAGES;
+				if (g >= STAGES && !mbar_wait(empty0 + 8 * st, ((g / STAGES) - 1) & 1, abort)) {
+					ok = false;
+					break;
+				}
+				const unsigned fb = full0 + 8 * st;
+				const unsigned sa = base + st * unsigned(L::STAGE_BYTES);
+				mbar_expect_tx(fb, 2 * (ba + bb));
+				bulk_g2s(sa, a.A_hi + ao + c * as, ba, fb);
+				bulk_g2s(sa + L::A_BYTES, a.A_lo + ao + c * as, ba, fb);
+				bulk_g2s(sa + 2 * L::A_BYTES, a.B_hi + bo + c * bs, bb, fb);
+				bulk_g2s(sa + 2 * L::A_BYTES + L::B_BYTES, a.B_lo + bo + c * bs, bb, fb);
+				++g;
+			}
+		}
 	}
+	if (!ok)
+		give_up(abort, a.error);
+	// the latest phase of every stage still written to must have landed
+	// before the CTA may exit
+	for (unsigned q = g > STAGES ? g - STAGES : 0; q < g; ++q)
+		mbar_wait(full0 + 8 * (q % STAGES), (q / STAGES) & 1, nullptr);
+}
+
+// ---------------------------------------------------------------- MMA issuer
+template <int BN, int STAGES>
+__device__ void mma_issuer(const TcArgs& a, unsigned base, unsigned tmem, unsigned full0,
+                           unsigned empty0, unsigned accf0, unsigned acce0, unsigned drain,
+                           volatile int* abort)
+{
+	using L               = TcLayout<BN>;
+	const unsigned idesc  = idesc_tf32<BN>();
+	unsigned       g      = 0; // chunks consumed
+	unsigned       tc     = 0; // tiles accumulated
+	bool           ok     = true;
+	bool           issued = false;
+	for (int ti = blockIdx.x; ti < a.ntiles && ok; ti += gridDim.x) {
+		const GemmTile t     = a.tiles[ti];
+		const int      total = tile_chunks(a, t);
+		if (total == 0)
+			continue;
+		const unsigned b = tc & 1;
+		if (tc >= 2 && !mbar_wait(acce0 + 8 * b, ((tc >> 1) - 1) & 1, abort)) {
+			ok = false;
+			break;
+		}
+		tc_fence_after();
+		const unsigned d = tmem + b * unsigned(BN);
+		for (int q = 0; q < total; ++q) {
+			const unsigned st = g % STAGES;
+			if (!mbar_wait(full0 + 8 * st, (g / STAGES) & 1, abort)) {
+				ok = false;
+				break;
+			}
+			tc_fence_after();
+			const unsigned sa  = base + st * unsigned(L::STAGE_BYTES);
+			const unsigned ahi = sa, alo = sa + L::A_BYTES;
+			const unsigned bhi = sa + 2 * L::A_BYTES, blo = bhi + L::B_BYTES;
 #pragma unroll
-	for (int e = 0; e < B_PIECES; ++e) {
-		const int      idx  = threadIdx.x + e * kTcThreads;
-		const int      row  = idx >> 3;
-		const int      c    = idx & 7;
-		const bool     p    = t.n0 + row < t.N;
-		const long long off = sg.b_off + (long long)(t.n0 + (p ? row : 0)) * sg.ldb + k0 + c * 4;
-		const unsigned dst  = unsigned(row * 128 + ((c ^ (row & 7)) << 4));
-		cp_async_16(stage + 2 * L::A_BYTES + dst, a.B_hi + off, p);
-		cp_async_16(stage + 2 * L::A_BYTES + L::B_BYTES + dst, a.B_lo + off, p);
+			for (int ks = 0; ks < kBK / 8; ++ks) {
+				const unsigned kb = unsigned(ks * 32); // 8 TF32 = 32 bytes along K
+				mma_tf32(d, smem_desc(ahi + kb), smem_desc(bhi + kb), idesc, (q | ks) != 0);
+				mma_tf32(d, smem_desc(ahi + kb), smem_desc(blo + kb), idesc, 1u);
+				mma_tf32(d, smem_desc(alo + kb), smem_desc(bhi + kb), idesc, 1u);
+			}
+			mma_commit(empty0 + 8 * st); // frees the stage once these MMAs are done
+			issued = true;
+			++g;
+		}
+		if (!ok)
+			break;
+		mma_commit(accf0 + 8 * b);
+		++tc;
+	}
+	if (!ok)
+		give_up(abort, a.error);
+	// every MMA this thread issued must be complete before TMEM is freed
+	if (issued) {
+		mma_commit(drain);
+		if (!mbar_wait(drain, 0, nullptr))
+			give_up(abort, a.error);
 	}
 }
 
-template <int BN, int STAGES, bool PASS1>
-__global__ void __launch_bounds__(kTcThreads) tc_gemm_tf32x3_kernel(TcArgs a)
+// ---------------------------------------------------------------- epilogue
+template <int BN, bool PASS1>
+__device__ __forceinline__ void store_chunk(const TcArgs& a, const GemmTile& t, int grow, int c0,
+                                            const float (&v)[32])
 {
-	using L = TcLayout<BN>;
+	const int col0 = t.n0 + c0;
+	if (grow >= t.M || col0 >= t.N)
+		return;
+	if (PASS1) {
+		// one 128-byte row of chunk col0 / 32 of BX_j (hi and lo); columns
+		// past N are the K padding of pass 2 and must be zero
+		const long long o  = t.c_off + (long long)(col0 >> 5) * t.ldc * kBK + (long long)grow * kBK;
+		float*          hi = a.C_hi + o;
+		float*          lo = a.C_lo + o;
+#pragma unroll
+		for (int q = 0; q < 8; ++q) {
+			float hv[4], lv[4];
+#pragma unroll
+			for (int e = 0; e < 4; ++e) {
+				const float x = (col0 + 4 * q + e < t.N) ? v[4 * q + e] : 0.f;
+				hv[e]         = tf32_rna(x);
+				lv[e]         = tf32_rna(x - hv[e]);
+			}
+			const int pos                          = (q ^ (grow & 7)) << 2;
+			*reinterpret_cast<float4*>(hi + pos) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+			*reinterpret_cast<float4*>(lo + pos) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+		}
+	} else {
+		double* y = a.Cd + t.c_off;
+#pragma unroll
+		for (int i = 0; i < 32; ++i) {
+			const int gcol = col0 + i;
+			if (gcol < t.N)
+				y[(long long)gcol * t.ldc + grow] = double(v[i]);
+		}
+	}
+}
+
+template <int BN, bool PASS1>
+__device__ void epilogue(const TcArgs& a, unsigned tmem, unsigned accf0, unsigned acce0,
+                         volatile int* abort)
+{
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int quarter = warp & 3; // TMEM lanes this warp may read
+	const int row     = quarter * 32 + lane;
+	unsigned  tc      = 0;
+	bool      ok      = true;
+	for (int ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) {
+		const GemmTile t     = a.tiles[ti];
+		const int      total = tile_chunks(a, t);
+		const int      grow  = t.m0 + row;
+		float          v[32];
+		if (total == 0) { // output tile without terms: zeros
+#pragma unroll
+			for (int i = 0; i < 32; ++i)
+				v[i] = 0.f;
+			for (int c0 = 0; c0 < BN; c0 += 32)
+				store_chunk<BN, PASS1>(a, t, grow, c0, v);
+			continue;
+		}
+		const unsigned b = tc & 1;
+		if (!mbar_wait(accf0 + 8 * b, (tc >> 1) & 1, abort)) {
+			ok = false;
+			break;
+		}
+		tc_fence_after();
+		for (int c0 = 0; c0 < BN; c0 += 32) {
+			tmem_ld32(tmem + (unsigned(quarter * 32) << 16) + b * unsigned(BN) + unsigned(c0), v);
+			store_chunk<BN, PASS1>(a, t, grow, c0, v);
+		}
+		tc_fence_before();
+		__syncwarp();
+		if (lane == 0)
+			mbar_arrive(acce0 + 8 * b);
+		++tc;
+	}
+	if (!ok && lane == 0)
+		give_up(abort, a.error);
+}
+
+template <int BN, int STAGES, bool PASS1>
+__global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_tf32x3_kernel(TcArgs a)
+{
 	extern __shared__ unsigned char smem_raw[];
-	__shared__ __align__(8) unsigned long long mbar[STAGES];
+	__shared__ __align__(8) unsigned long long bars[2 * STAGES + 5];
 	__shared__ unsigned                        tmem_slot;
+	__shared__ volatile int                    abort_flag;
 
-	const unsigned base = (smem_addr(smem_raw) + 1023u) & ~1023u; // 1024-aligned stages
-	const GemmTile t    = a.tiles[blockIdx.x];
-	const int      tid  = threadIdx.x;
-	const int      warp = tid >> 5;
-	const int      lane = tid & 31;
+	const unsigned base   = (smem_addr(smem_raw) + 1023u) & ~1023u; // 1024-aligned stages
+	const unsigned full0  = smem_addr(&bars[0]);
+	const unsigned empty0 = smem_addr(&bars[STAGES]);
+	const unsigned accf0  = smem_addr(&bars[2 * STAGES]);
+	const unsigned acce0  = smem_addr(&bars[2 * STAGES + 2]);
+	const unsigned drain  = smem_addr(&bars[2 * STAGES + 4]);
+	const int      warp   = threadIdx.x >> 5;
 
-	if (warp == 0) {
+	if (warp == 1) {
 		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
 		                 smem_addr(&tmem_slot)),
-		             "r"(unsigned(BN))
+		             "r"(unsigned(2 * BN))
 		             : "memory");
 		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
 	}
-	if (tid == 0) {
-		for (int s = 0; s < STAGES; ++s)
-			mbar_init(smem_addr(&mbar[s]), 1);
+	if (threadIdx.x == 0) {
+		abort_flag = 0;
+		for (int s = 0; s < STAGES; ++s) {
+			mbar_init(full0 + 8 * s, 1);
+			mbar_init(empty0 + 8 * s, 1);
+		}
+		for (int b = 0; b < 2; ++b) {
+			mbar_init(accf0 + 8 * b, 1);
+			mbar_init(acce0 + 8 * b, 4); // one arrival per epilogue warp
+		}
+		mbar_init(drain, 1);
 		asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 	}
 	tc_fence_before();
@@ -213,128 +413,26 @@ __global__ void __launch_bounds__(kTcThreads) tc_gemm_tf32x3_kernel(TcArgs a)
 	tc_fence_after();
 	const unsigned tmem = tmem_slot;
 
-	int total = 0;
-	for (int s = t.seg_begin; s < t.seg_end; ++s)
-		total += (a.segs[s].K + kBK - 1) / kBK;
-
-	int     ls = t.seg_begin, lk = 0;
-	GemmSeg cur {};
-	if (ls < t.seg_end)
-		cur = a.segs[ls];
-	auto issue = [&](int stage) {
-		load_chunk<BN>(base + unsigned(stage * L::STAGE_BYTES), a, cur, lk, t);
-		lk += kBK;
-		if (lk >= cur.K) {
-			lk = 0;
-			if (++ls < t.seg_end)
-				cur = a.segs[ls];
-		}
-	};
-
-#pragma unroll
-	for (int st = 0; st < STAGES - 1; ++st) {
-		if (st < total)
-			issue(st);
-		cp_async_commit();
+	if (warp == 0) {
+		if ((threadIdx.x & 31) == 0)
+			producer<BN, STAGES>(a, base, full0, empty0, &abort_flag);
+	} else if (warp == 1) {
+		if ((threadIdx.x & 31) == 0)
+			mma_issuer<BN, STAGES>(a, base, tmem, full0, empty0, accf0, acce0, drain, &abort_flag);
+	} else {
+		epilogue<BN, PASS1>(a, tmem, accf0, acce0, &abort_flag);
 	}
-	bool           ok     = true;
-	int            issued = 0; // chunks whose MMAs were committed
-	const unsigned idesc  = idesc_tf32<BN>();
-	for (int it = 0; it < total; ++it) {
-		cp_async_wait<STAGES - 2>();
-		asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-		ok = __syncthreads_and(ok) != 0; // uniform: a timed-out wait stops every thread
-		if (!ok)
-			break;
-		if (tid == 0) {
-			tc_fence_after();
-			const unsigned sa = base + unsigned((it % STAGES) * L::STAGE_BYTES);
-			const unsigned ahi = sa, alo = sa + L::A_BYTES;
-			const unsigned bhi = sa + 2 * L::A_BYTES, blo = bhi + L::B_BYTES;
-#pragma unroll
-			for (int ks = 0; ks < kBK / 8; ++ks) {
-				const unsigned kb = unsigned(ks * 32); // 8 TF32 = 32 bytes along K
-				mma_tf32(tmem, smem_desc(ahi + kb), smem_desc(bhi + kb), idesc, (it | ks) != 0);
-				mma_tf32(tmem, smem_desc(ahi + kb), smem_desc(blo + kb), idesc, 1u);
-				mma_tf32(tmem, smem_desc(alo + kb), smem_desc(bhi + kb), idesc, 1u);
-			}
-			mma_commit(smem_addr(&mbar[it % STAGES]));
-		}
-		issued = it + 1;
-		const int nxt = it + STAGES - 1;
-		if (nxt < total) {
-			// the target stage was last read by the MMAs of chunk it-1
-			if (it >= 1)
-				ok = mbar_wait(smem_addr(&mbar[(it - 1) % STAGES]), unsigned(((it - 1) / STAGES) & 1))
-				    && ok;
-			issue(nxt % STAGES);
-		}
-		cp_async_commit();
-	}
-	cp_async_wait<0>();
-	// the last commit covers every MMA issued before it; after a timeout this
-	// is the (bounded) drain before TMEM is read or freed
-	if (issued > 0 && !mbar_wait(smem_addr(&mbar[(issued - 1) % STAGES]),
-	                             unsigned(((issued - 1) / STAGES) & 1)))
-		ok = false;
-	ok = __syncthreads_and(ok) != 0;
-	tc_fence_after();
-	if (!ok)
-		atomicExch(a.error, 2);
-
-	// epilogue: warp w holds tile rows 32w..32w+31 (TMEM lanes)
-	const int row  = warp * 32 + lane;
-	const int grow = t.m0 + row;
-	for (int c0 = 0; c0 < BN; c0 += 32) {
-		float v[32];
-		if (total > 0) {
-			tmem_ld32(tmem + (unsigned(warp * 32) << 16) + unsigned(c0), v);
-		} else {
-#pragma unroll
-			for (int i = 0; i < 32; ++i)
-				v[i] = 0.f;
-		}
-		if (!ok || grow >= t.M || t.n0 + c0 >= t.N)
-			continue;
-		if (PASS1) {
-			// K-major row of the next pass; columns past N carry exact zeros
-			// (zero-filled B rows), which keep the K padding zero
-			float*          hi  = a.C_hi + t.c_off + (long long)grow * t.ldc + t.n0 + c0;
-			float*          lo  = a.C_lo + t.c_off + (long long)grow * t.ldc + t.n0 + c0;
-#pragma unroll
-			for (int q = 0; q < 8; ++q) {
-				float4 h, l;
-				h.x = tf32_rna(v[4 * q + 0]);
-				h.y = tf32_rna(v[4 * q + 1]);
-				h.z = tf32_rna(v[4 * q + 2]);
-				h.w = tf32_rna(v[4 * q + 3]);
-				l.x = tf32_rna(v[4 * q + 0] - h.x);
-				l.y = tf32_rna(v[4 * q + 1] - h.y);
-				l.z = tf32_rna(v[4 * q + 2] - h.z);
-				l.w = tf32_rna(v[4 * q + 3] - h.w);
-				reinterpret_cast<float4*>(hi)[q] = h;
-				reinterpret_cast<float4*>(lo)[q] = l;
-			}
-		} else {
-			double* y = a.Cd + t.c_off;
-#pragma unroll
-			for (int i = 0; i < 32; ++i) {
-				const int gcol = t.n0 + c0 + i;
-				if (gcol < t.N)
-					y[(long long)gcol * t.ldc + grow] = double(v[i]);
-			}
-		}
-	}
-
+	__syncwarp();
 	tc_fence_before();
 	__syncthreads();
-	if (warp == 0)
+	tc_fence_after();
+	if (warp == 1)
 		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-		             "r"(unsigned(BN))
+		             "r"(unsigned(2 * BN))
 		             : "memory");
 }
 
-// x (FP64, patch order) -> K-major TF32 hi/lo split buffers
+// x (FP64, patch order) -> TF32 hi/lo parts in the chunked layout
 __global__ void __launch_bounds__(256)
 split_x_kernel(const double* __restrict__ x, const int* __restrict__ map, float* __restrict__ hi,
                float* __restrict__ lo, long long n)
@@ -348,7 +446,7 @@ split_x_kernel(const double* __restrict__ x, const int* __restrict__ map, float*
 	}
 }
 
-template <int BN, int STAGES, bool PASS1> constexpr size_t tc_smem()
+template <int BN, int STAGES> constexpr size_t tc_smem()
 {
 	return size_t(STAGES) * TcLayout<BN>::STAGE_BYTES + 1024;
 }
@@ -356,21 +454,30 @@ template <int BN, int STAGES, bool PASS1> constexpr size_t tc_smem()
 template <int BN, int STAGES, bool PASS1> cudaError_t tc_init_one()
 {
 	return cudaFuncSetAttribute(tc_gemm_tf32x3_kernel<BN, STAGES, PASS1>,
-	                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                            int(tc_smem<BN, STAGES, PASS1>()));
+	                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(tc_smem<BN, STAGES>()));
+}
+
+// ring depth: as many stages as fit in 227 KB with the 1 KB alignment slack
+constexpr int kStages64  = 4; // 4 x 48 KB
+constexpr int kStages128 = 3; // 3 x 64 KB
+
+template <int BN, int STAGES, bool PASS1> void launch_one(const TcArgs& a, cudaStream_t stream)
+{
+	const int grid = a.grid < a.ntiles ? a.grid : a.ntiles;
+	tc_gemm_tf32x3_kernel<BN, STAGES, PASS1><<<grid, kTcThreads, tc_smem<BN, STAGES>(), stream>>>(a);
 }
 
 } // namespace
 
 cudaError_t tc_init()
 {
-	cudaError_t e = tc_init_one<64, 3, true>();
+	cudaError_t e = tc_init_one<64, kStages64, true>();
 	if (e == cudaSuccess)
-		e = tc_init_one<64, 3, false>();
+		e = tc_init_one<64, kStages64, false>();
 	if (e == cudaSuccess)
-		e = tc_init_one<128, 3, true>();
+		e = tc_init_one<128, kStages128, true>();
 	if (e == cudaSuccess)
-		e = tc_init_one<128, 3, false>();
+		e = tc_init_one<128, kStages128, false>();
 	return e;
 }
 
@@ -378,16 +485,18 @@ cudaError_t tc_launch(const TcArgs& a, int bn, bool pass1, cudaStream_t stream)
 {
 	if (a.ntiles <= 0)
 		return cudaSuccess;
+	if (a.grid <= 0)
+		return cudaErrorInvalidValue;
 	if (bn == 64) {
 		if (pass1)
-			tc_gemm_tf32x3_kernel<64, 3, true><<<a.ntiles, kTcThreads, tc_smem<64, 3, true>(), stream>>>(a);
+			launch_one<64, kStages64, true>(a, stream);
 		else
-			tc_gemm_tf32x3_kernel<64, 3, false><<<a.ntiles, kTcThreads, tc_smem<64, 3, false>(), stream>>>(a);
+			launch_one<64, kStages64, false>(a, stream);
 	} else if (bn == 128) {
 		if (pass1)
-			tc_gemm_tf32x3_kernel<128, 3, true><<<a.ntiles, kTcThreads, tc_smem<128, 3, true>(), stream>>>(a);
+			launch_one<128, kStages128, true>(a, stream);
 		else
-			tc_gemm_tf32x3_kernel<128, 3, false><<<a.ntiles, kTcThreads, tc_smem<128, 3, false>(), stream>>>(a);
+			launch_one<128, kStages128, false>(a, stream);
 	} else {
 		return cudaErrorInvalidValue;
 	}

@@ -18,13 +18,15 @@ struct TcArgs {
 	const GemmSeg*  segs;
 	const GemmTile* tiles;
 	int             ntiles;
+	int             grid;  // persistent CTAs (one per SM); at most ntiles are launched
 	int*            error; // set to 2 when an mbarrier wait gave up
 };
 
 // Kernel attributes on the current device; call once per device.
 cudaError_t tc_init();
 
-// One grouped pass over a.ntiles tiles of 128 x bn (bn = 64 or 128).
+// One grouped pass over a.ntiles tiles of 128 x bn (bn = 64 or 128) by
+// min(a.grid, a.ntiles) persistent CTAs.
 cudaError_t tc_launch(const TcArgs& a, int bn, bool pass1, cudaStream_t stream);
 
 // x (patch order, FP64) -> TF32 hi/lo parts at map[e].

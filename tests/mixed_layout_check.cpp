@@ -1,0 +1,222 @@
+// Host emulation of the TF32x3 tensor-core passes over the chunked,
+// pre-swizzled operand layout that build_mixed_plan produces.  Checks, on
+// the CPU, what the kernel in tc_gemm.cu relies on:
+//   * every bulk copy the producer would issue (A and B tiles of every
+//     k-chunk of every segment) starts 16-byte aligned, has a size that is a
+//     multiple of 16 bytes and lies inside its operand buffer;
+//   * copies that start on a 128-row tile row 0 start on an 8-row swizzle
+//     group, so the pre-swizzled rows land where the descriptor expects them;
+//   * the epilogue's stores stay inside their buffers;
+//   * pass 1 + pass 2 computed from these buffers (hi*hi + hi*lo + lo*hi in
+//     double, stale rows included as NaN) reproduce the FP64 H*x.
+// Usage: mixed_layout_check seed npatches noperator max_size bn
+// Prints "ok <max relative error>" or "FAIL <reason>" (exit code 1).
+#include "kron_plan.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <limits>
+#include <random>
+#include <vector>
+
+using namespace dmrgpp;
+
+namespace {
+
+int fail(const char* why, long long a = 0, long long b = 0)
+{
+	std::printf("FAIL %s %lld %lld\n", why, a, b);
+	return 1;
+}
+
+struct Buf {
+	const float* hi;
+	const float* lo;
+	long long    n;
+};
+
+} // namespace
+
+int main(int argc, char** argv)
+{
+	if (argc < 6)
+		return fail("usage");
+	const unsigned seed = unsigned(std::atoi(argv[1]));
+	const int      np   = std::atoi(argv[2]);
+	const int      nop  = std::atoi(argv[3]);
+	const int      maxs = std::atoi(argv[4]);
+	const int      bn   = std::atoi(argv[5]);
+	std::mt19937_64 rng(seed);
+	std::uniform_int_distribution<int>     size(1, maxs);
+	std::uniform_real_distribution<double> val(-1.0, 1.0);
+	std::uniform_real_distribution<double> coin(0.0, 1.0);
+
+	std::vector<size_t> l(np), r(np);
+	for (int p = 0; p < np; ++p) {
+		l[p] = size_t(size(rng));
+		r[p] = size_t(size(rng));
+	}
+	const size_t               nt = size_t(np) * np * nop;
+	std::vector<std::vector<double>> Ast(nt), Bst(nt);
+	std::vector<const double*> A(nt, nullptr), B(nt, nullptr);
+	std::vector<size_t>        ldA(nt, 0), ldB(nt, 0);
+	for (int k = 0; k < nop; ++k)
+		for (int j = 0; j < np; ++j)
+			for (int i = 0; i < np; ++i) {
+				if (coin(rng) < 0.35)
+					continue;
+				const size_t ix = size_t(i) + size_t(j) * np + size_t(k) * np * np;
+				Ast[ix].resize(l[i] * l[j]);
+				Bst[ix].resize(r[i] * r[j]);
+				for (double& v : Ast[ix])
+					v = val(rng);
+				for (double& v : Bst[ix])
+					v = val(rng);
+				A[ix]   = Ast[ix].data();
+				B[ix]   = Bst[ix].data();
+				ldA[ix] = l[i];
+				ldB[ix] = r[i];
+			}
+
+	KronPlan    plan;
+	std::string msg = build_kron_plan(size_t(nop), size_t(np), l.data(), r.data(), A.data(),
+	                                  ldA.data(), B.data(), ldB.data(), 64, 64, plan, nullptr);
+	if (!msg.empty())
+		return fail(msg.c_str());
+	std::vector<float> ohi, olo;
+	std::vector<int>   xmap;
+	msg = build_mixed_plan(plan, A.data(), ldA.data(), B.data(), ldB.data(), bn, &ohi, &olo, &xmap);
+	if (!msg.empty())
+		return fail(msg.c_str());
+	const MixedPlan& mp = plan.mixed;
+	const long long  D  = plan.dim();
+
+	std::vector<double> x(static_cast<size_t>(D)), y_ref(static_cast<size_t>(D), 0.0);
+	for (double& v : x)
+		v = val(rng);
+	// FP64 reference: Y_i = sum B_k(i,j) X_j A_k(i,j)^T
+	for (const Triple& t : plan.triples) {
+		const size_t ix = size_t(t.i) + size_t(t.j) * np + size_t(t.k) * np * np;
+		const long long ri = r[t.i], rj = r[t.j], li = l[t.i], lj = l[t.j];
+		for (long long a = 0; a < ri; ++a)
+			for (long long b = 0; b < li; ++b) {
+				double s = 0;
+				for (long long c = 0; c < rj; ++c)
+					for (long long d = 0; d < lj; ++d)
+						s += B[ix][a + c * ri] * x[size_t(plan.xy_start[t.j] + c + d * rj)]
+						    * A[ix][b + d * li];
+				y_ref[size_t(plan.xy_start[t.i] + a + b * ri)] += s;
+			}
+	}
+
+	// x split (zero K padding, like the cleared device buffer + split_x)
+	std::vector<float> xs_hi(size_t(mp.xs_elems), 0.f), xs_lo(size_t(mp.xs_elems), 0.f);
+	for (long long e = 0; e < D; ++e) {
+		const int d = xmap[size_t(e)];
+		if (d < 0 || d >= mp.xs_elems)
+			return fail("x map out of range", e, d);
+		split_tf32(x[size_t(e)], &xs_hi[size_t(d)], &xs_lo[size_t(d)]);
+	}
+	const float nanf = std::numeric_limits<float>::quiet_NaN();
+	std::vector<float>  bx_hi(size_t(mp.bxs_elems), nanf), bx_lo(size_t(mp.bxs_elems), nanf);
+	std::vector<double> y(size_t(D), std::numeric_limits<double>::quiet_NaN());
+
+	const int BM = mp.bm;
+	auto check_copy = [&](const Buf& b, long long off, long long rows) -> bool {
+		const long long bytes = rows * 128;
+		return off >= 0 && (off * 4) % 16 == 0 && bytes % 16 == 0 && bytes > 0
+		    && off + rows * 32 <= b.n;
+	};
+	// emulate one pass; returns 0 on success
+	auto pass = [&](const std::vector<GemmSeg>& segs, const std::vector<GemmTile>& tiles, Buf Ab,
+	                Buf Bb, bool pass1) -> int {
+		std::vector<double> acc(size_t(BM) * bn);
+		for (const GemmTile& t : tiles) {
+			const int rowsA = std::min<int>(BM, int(round8(t.M)) - t.m0);
+			const int rowsB = std::min<int>(bn, int(round8(t.N)) - t.n0);
+			if (rowsA <= 0 || rowsB <= 0)
+				return fail("empty copy", rowsA, rowsB);
+			std::fill(acc.begin(), acc.end(), 0.0);
+			int chunks = 0;
+			for (int s = t.seg_begin; s < t.seg_end; ++s) {
+				const GemmSeg& g = segs[size_t(s)];
+				if (g.K % 32 != 0 || g.a_off % 8 != 0 || g.b_off % 8 != 0)
+					return fail("segment alignment", g.K, g.a_off);
+				for (int c = 0; c < g.K / 32; ++c, ++chunks) {
+					const long long ao = g.a_off + (long long)t.m0 * 32 + (long long)c * g.lda * 32;
+					const long long bo = g.b_off + (long long)t.n0 * 32 + (long long)c * g.ldb * 32;
+					if (!check_copy(Ab, ao, rowsA) || !check_copy(Bb, bo, rowsB))
+						return fail("copy out of bounds", ao, bo);
+					// shared-memory image: fresh rows, stale (NaN) rows beyond
+					for (int m = 0; m < BM; ++m)
+						for (int n = 0; n < bn; ++n) {
+							if (m >= rowsA || n >= rowsB) {
+								if (m < t.M - t.m0 && n < t.N - t.n0)
+									return fail("valid output reads a stale row", m, n);
+								acc[size_t(m) * bn + n] = std::nan("");
+								continue;
+							}
+							double sum = 0;
+							for (int k = 0; k < 32; ++k) {
+								// swizzled position inside the copied block
+								const long long pa = ao + m * 32 + ((((k >> 2) ^ (m & 7)) << 2) | (k & 3));
+								const long long pb = bo + n * 32 + ((((k >> 2) ^ (n & 7)) << 2) | (k & 3));
+								const double    ah = Ab.hi[pa], al = Ab.lo[pa];
+								const double    bh = Bb.hi[pb], bl = Bb.lo[pb];
+								sum += ah * bh + ah * bl + al * bh;
+							}
+							acc[size_t(m) * bn + n] += sum;
+						}
+				}
+			}
+			for (int m = 0; m < BM; ++m) {
+				const int grow = t.m0 + m;
+				for (int c0 = 0; c0 < bn; c0 += 32) {
+					const int col0 = t.n0 + c0;
+					if (grow >= t.M || col0 >= t.N)
+						continue;
+					for (int e = 0; e < 32; ++e) {
+						const int    gcol = col0 + e;
+						const double v    = chunks ? acc[size_t(m) * bn + c0 + e] : 0.0;
+						if (pass1) {
+							const long long o = t.c_off + (long long)(col0 >> 5) * t.ldc * 32
+							    + (long long)grow * 32 + ((((e >> 2) ^ (grow & 7)) << 2) | (e & 3));
+							if (o < 0 || o >= mp.bxs_elems)
+								return fail("BX store out of bounds", o, mp.bxs_elems);
+							float h, lo;
+							split_tf32(gcol < t.N ? double(float(v)) : 0.0, &h, &lo);
+							bx_hi[size_t(o)] = h;
+							bx_lo[size_t(o)] = lo;
+						} else if (gcol < t.N) {
+							const long long o = t.c_off + (long long)gcol * t.ldc + grow;
+							if (o < 0 || o >= D)
+								return fail("y store out of bounds", o, D);
+							y[size_t(o)] = v;
+						}
+					}
+				}
+			}
+		}
+		return 0;
+	};
+	const Buf ops {ohi.data(), olo.data(), mp.ops_elems};
+	const Buf xsb {xs_hi.data(), xs_lo.data(), mp.xs_elems};
+	const Buf bxb {bx_hi.data(), bx_lo.data(), mp.bxs_elems};
+	if (pass(mp.seg1, mp.tile1, ops, xsb, true))
+		return 1;
+	if (pass(mp.seg2, mp.tile2, bxb, ops, false))
+		return 1;
+	double err = 0, ref = 0;
+	for (long long e = 0; e < D; ++e) {
+		if (!std::isfinite(y[size_t(e)]))
+			return fail("y not written or not finite", e, 0);
+		err = std::max(err, std::fabs(y[size_t(e)] - y_ref[size_t(e)]));
+		ref = std::max(ref, std::fabs(y_ref[size_t(e)]));
+	}
+	const double rel = ref > 0 ? err / ref : err;
+	if (rel > 1e-5)
+		return fail("result differs from FP64", (long long)(rel * 1e9), 0);
+	std::printf("ok %.3e\n", rel);
+	return 0;
+}
