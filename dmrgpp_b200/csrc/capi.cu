@@ -161,7 +161,8 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 	a1.segs   = h->m_seg1;
 	a1.tiles  = h->m_tile1;
 	a1.ntiles = int(mp.tile1.size());
-	a1.grid   = h->m_grid;
+	a1.grid   = h->m_grid1;
+	a1.starts = h->m_starts1;
 	a1.error  = h->err_dev;
 	if ((e = tc_launch(a1, mp.bn, true, h->stream)))
 		return cuda_fail(h, e, "tensor-core pass 1 launch");
@@ -174,7 +175,8 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 	a2.segs   = h->m_seg2;
 	a2.tiles  = h->m_tile2;
 	a2.ntiles = int(mp.tile2.size());
-	a2.grid   = h->m_grid;
+	a2.grid   = h->m_grid2;
+	a2.starts = h->m_starts2;
 	a2.error  = h->err_dev;
 	if ((e = tc_launch(a2, mp.bn, false, h->stream)))
 		return cuda_fail(h, e, "tensor-core pass 2 launch");
@@ -227,8 +229,13 @@ int build_mixed(dmrgpp_kron_handle h, const dmrgpp_kron_desc* d)
 	cudaError_t      e  = tc_init();
 	if (e != cudaSuccess)
 		return cuda_fail(h, e, "tensor-core kernel attributes");
-	if ((e = cudaDeviceGetAttribute(&h->m_grid, cudaDevAttrMultiProcessorCount, h->device)))
+	int sms = 0;
+	if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device)))
 		return cuda_fail(h, e, "SM count");
+	MixedPlan&       mpw = h->plan.mixed;
+	std::vector<int> starts1, starts2;
+	h->m_grid1 = balance_tiles(mpw.tile1, mpw.seg1, sms, starts1);
+	h->m_grid2 = balance_tiles(mpw.tile2, mpw.seg2, sms, starts2);
 	auto fbytes = [](long long n) { return size_t(n > 0 ? n : 1) * sizeof(float); };
 	if ((e = cudaMalloc(&h->m_ops_hi, fbytes(mp.ops_elems))) || (e = cudaMalloc(&h->m_ops_lo, fbytes(mp.ops_elems)))
 	    || (e = cudaMalloc(&h->m_xs_hi, fbytes(mp.xs_elems))) || (e = cudaMalloc(&h->m_xs_lo, fbytes(mp.xs_elems)))
@@ -260,6 +267,8 @@ int build_mixed(dmrgpp_kron_handle h, const dmrgpp_kron_desc* d)
 	add(mp.seg2.data(), mp.seg2.size() * sizeof(GemmSeg));
 	add(mp.tile1.data(), mp.tile1.size() * sizeof(GemmTile));
 	add(mp.tile2.data(), mp.tile2.size() * sizeof(GemmTile));
+	add(starts1.data(), starts1.size() * sizeof(int));
+	add(starts2.data(), starts2.size() * sizeof(int));
 	if ((e = cudaMalloc(&h->m_lists, lists.empty() ? 16 : lists.size())))
 		return cuda_fail(h, e, "cudaMalloc(mixed lists)");
 	auto at    = [&](int i) { return static_cast<unsigned char*>(h->m_lists) + offs[i]; };
@@ -267,6 +276,8 @@ int build_mixed(dmrgpp_kron_handle h, const dmrgpp_kron_desc* d)
 	h->m_seg2  = reinterpret_cast<GemmSeg*>(at(1));
 	h->m_tile1 = reinterpret_cast<GemmTile*>(at(2));
 	h->m_tile2 = reinterpret_cast<GemmTile*>(at(3));
+	h->m_starts1 = reinterpret_cast<int*>(at(4));
+	h->m_starts2 = reinterpret_cast<int*>(at(5));
 	if (!lists.empty()
 	    && (e = cudaMemcpy(h->m_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
 		return cuda_fail(h, e, "upload mixed lists");

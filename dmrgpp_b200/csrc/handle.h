@@ -50,7 +50,10 @@ struct dmrgpp_kron_s {
 	float*              m_bxs_hi = nullptr; // pass-1 result split
 	float*              m_bxs_lo = nullptr;
 	int*                m_xmap   = nullptr; // sector vector -> x split offsets
-	int                 m_grid   = 0;       // persistent CTAs of the tensor-core passes
+	int                 m_grid1  = 0;       // persistent CTAs of tensor-core pass 1 / 2
+	int                 m_grid2  = 0;
+	int*                m_starts1 = nullptr; // per-CTA tile runs of pass 1 / 2
+	int*                m_starts2 = nullptr;
 	void*               m_lists  = nullptr; // seg1, seg2, tile1, tile2
 	dmrgpp::GemmSeg*    m_seg1 = nullptr;
 	dmrgpp::GemmSeg*    m_seg2 = nullptr;

@@ -5,6 +5,7 @@
 #include <climits>
 #include <cstring>
 #include <numeric>
+#include <utility>
 
 namespace dmrgpp {
 
@@ -559,4 +560,50 @@ std::string build_mixed_plan(KronPlan&            plan,
 	return std::string();
 }
 
+int balance_tiles(std::vector<GemmTile>& tiles, const std::vector<GemmSeg>& segs, int bins,
+                  std::vector<int>& starts)
+{
+	const int n = int(tiles.size());
+	const int G = std::max(1, std::min(bins, n));
+	std::vector<long long> cost(size_t(n), 0);
+	for (int t = 0; t < n; ++t) {
+		long long c = 2;
+		for (int s = tiles[size_t(t)].seg_begin; s < tiles[size_t(t)].seg_end; ++s)
+			c += segs[size_t(s)].K / 32;
+		cost[size_t(t)] = c;
+	}
+	std::vector<int> order(static_cast<size_t>(n));
+	std::iota(order.begin(), order.end(), 0);
+	std::stable_sort(order.begin(), order.end(),
+	                 [&](int a, int b) { return cost[size_t(a)] > cost[size_t(b)]; });
+	// min-heap of (load, bin)
+	std::vector<std::pair<long long, int>> heap;
+	for (int b = 0; b < G; ++b)
+		heap.push_back({0, b});
+	auto cmp = [](const std::pair<long long, int>& x, const std::pair<long long, int>& y) {
+		return x.first != y.first ? x.first > y.first : x.second > y.second;
+	};
+	std::make_heap(heap.begin(), heap.end(), cmp);
+	std::vector<std::vector<int>> runs(static_cast<size_t>(G));
+	for (int t : order) {
+		std::pop_heap(heap.begin(), heap.end(), cmp);
+		auto& top = heap.back();
+		runs[size_t(top.second)].push_back(t);
+		top.first += cost[size_t(t)];
+		std::push_heap(heap.begin(), heap.end(), cmp);
+	}
+	std::vector<GemmTile> out;
+	out.reserve(size_t(n));
+	starts.assign(size_t(G) + 1, 0);
+	for (int b = 0; b < G; ++b) {
+		starts[size_t(b)] = int(out.size());
+		for (int t : runs[size_t(b)])
+			out.push_back(tiles[size_t(t)]);
+	}
+	starts[size_t(G)] = int(out.size());
+	tiles.swap(out);
+	return n == 0 ? 0 : G;
+}
+
 } // namespace dmrgpp
+

@@ -194,6 +194,14 @@ void split_tf32(double v, float* hi, float* lo);
 // sector for bm x bn output tiles.
 void build_tile_lists(KronPlan& plan, int bm, int bn);
 
+// Reorders the tiles of one tensor-core pass into per-CTA runs: CTA b of the
+// persistent launch processes tiles [starts[b], starts[b+1]).  Tiles go,
+// longest first, to the CTA with the least work so far (LPT; work of a tile =
+// its k-chunks + 2 for the epilogue); within a run the longest tile comes
+// first.  Returns the number of CTAs, min(bins, tiles.size()).
+int balance_tiles(std::vector<GemmTile>& tiles, const std::vector<GemmSeg>& segs, int bins,
+                  std::vector<int>& starts);
+
 // Most K-segments one work item may hold (they are staged in shared memory).
 constexpr int kMaxItemSegs = 32;
 

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -34,23 +35,15 @@ namespace {
 
 constexpr int kThreads   = 256;
 constexpr int kMaxBlocks = 1184; // 8 per SM of a B200
-constexpr int kDotBlocks = 296;  // grids of the basis projections (2 per SM)
-constexpr int kRowChunk  = 1024; // rows per block iteration of the basis GEMVs
+constexpr int kDotGrid   = 592;  // blocks of the basis projections (4 per SM)
+constexpr int kDotChunk  = 2048; // rows per block iteration of the basis projections
 constexpr int kMaxCols   = 1024; // stored Lanczos vectors per solve
 
-// blocks of the basis GEMVs: at least 256 rows each; the projections
-// (k_basis_dots, whose last block reduces kDotBlocks x columns partials) use
-// at most kDotBlocks, the row-parallel ones up to kMaxBlocks
+// blocks of the row-parallel basis kernels: at least 256 rows each
 int basis_blocks_for(size_t n)
 {
 	const size_t b = (n + 255) / 256;
 	return int(std::max<size_t>(1, std::min<size_t>(b, kMaxBlocks)));
-}
-
-int dots_blocks_for(size_t n)
-{
-	const size_t b = (n + 255) / 256;
-	return int(std::max<size_t>(1, std::min<size_t>(b, kDotBlocks)));
 }
 
 int blocks_for(size_t n)
@@ -170,23 +163,24 @@ __global__ void __launch_bounds__(kThreads) k_scale_inv(double* v, size_t n, con
 		v[i] *= a;
 }
 
-// r[c] = <V[:,c], v> for c < ncols.  Each warp owns columns warp, warp+8, ...;
-// the block walks its rows in chunks staged in shared memory.
-__global__ void __launch_bounds__(kThreads)
+// Per-block partial projections partial[b][c] = <V[rows of b, c], v[rows of b]>
+// for c < ncols.  Block b takes the kDotChunk-row chunks b, b + grid, ...;
+// each chunk of v is staged in shared memory and every warp streams whole
+// columns of it (warp w: columns w, w + 8, ...).  VEC: 16-byte loads (V, v
+// 16-byte aligned and ld even), 8 loads in flight per lane.  The order of
+// every sum is fixed, so results are bitwise reproducible.
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads, 4)
 k_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* __restrict__ v,
-             size_t n, double* r, double* partial, unsigned* ctr)
+             size_t n, double* __restrict__ partial)
 {
-	__shared__ double vs[kRowChunk];
+	__shared__ __align__(16) double vs[kDotChunk];
 	__shared__ double acc[kMaxCols];
-	__shared__ bool   last;
 	const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	for (int c = threadIdx.x; c < ncols; c += kThreads)
 		acc[c] = 0.0;
-	const size_t rows_per_block = (n + gridDim.x - 1) / gridDim.x;
-	const size_t r0             = size_t(blockIdx.x) * rows_per_block;
-	const size_t r1             = std::min(n, r0 + rows_per_block);
-	for (size_t base = r0; base < r1; base += kRowChunk) {
-		const int len = int(std::min<size_t>(kRowChunk, r1 - base));
+	for (size_t base = size_t(blockIdx.x) * kDotChunk; base < n; base += size_t(gridDim.x) * kDotChunk) {
+		const int len = int(std::min<size_t>(kDotChunk, n - base));
 		__syncthreads();
 		for (int i = threadIdx.x; i < len; i += kThreads)
 			vs[i] = v[base + i];
@@ -194,15 +188,30 @@ k_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* _
 		for (int c = warp; c < ncols; c += kThreads / 32) {
 			const double* col = V + size_t(c) * ld + base;
 			double        s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-			int           i  = lane;
-			for (; i + 96 < len; i += 128) {
-				s0 += col[i] * vs[i];
-				s1 += col[i + 32] * vs[i + 32];
-				s2 += col[i + 64] * vs[i + 64];
-				s3 += col[i + 96] * vs[i + 96];
+			if (VEC && len == kDotChunk) {
+				const double2* c2 = reinterpret_cast<const double2*>(col);
+				const double2* v2 = reinterpret_cast<const double2*>(vs);
+#pragma unroll 2
+				for (int q = lane; q < kDotChunk / 2; q += 128) {
+					const double2 a0 = __ldg(c2 + q), a1 = __ldg(c2 + q + 32);
+					const double2 a2 = __ldg(c2 + q + 64), a3 = __ldg(c2 + q + 96);
+					const double2 b0 = v2[q], b1 = v2[q + 32], b2 = v2[q + 64], b3 = v2[q + 96];
+					s0 += a0.x * b0.x + a0.y * b0.y;
+					s1 += a1.x * b1.x + a1.y * b1.y;
+					s2 += a2.x * b2.x + a2.y * b2.y;
+					s3 += a3.x * b3.x + a3.y * b3.y;
+				}
+			} else {
+				int i = lane;
+				for (; i + 96 < len; i += 128) {
+					s0 += col[i] * vs[i];
+					s1 += col[i + 32] * vs[i + 32];
+					s2 += col[i + 64] * vs[i + 64];
+					s3 += col[i + 96] * vs[i + 96];
+				}
+				for (; i < len; i += 32)
+					s0 += col[i] * vs[i];
 			}
-			for (; i < len; i += 32)
-				s0 += col[i] * vs[i];
 			double s = (s0 + s1) + (s2 + s3);
 			for (int o = 16; o > 0; o >>= 1)
 				s += __shfl_down_sync(0xffffffffu, s, o);
@@ -213,20 +222,27 @@ k_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* _
 	__syncthreads();
 	for (int c = threadIdx.x; c < ncols; c += kThreads)
 		partial[size_t(blockIdx.x) * kMaxCols + c] = acc[c];
-	__syncthreads();
-	if (threadIdx.x == 0)
-		last = last_block(ctr);
-	__syncthreads();
-	if (last)
-		for (int c = threadIdx.x; c < ncols; c += kThreads) {
-			double s = 0.0;
-			for (int b = 0; b < int(gridDim.x); ++b)
-				s += __ldcg(partial + size_t(b) * kMaxCols + c);
-			r[c] = s;
-		}
 }
 
-// v -= V[:, 0..ncols) r ; *nrm_out = |v|
+// r[c] = sum over blocks b < nblocks of partial[b][c], one block per column,
+// fixed order
+__global__ void __launch_bounds__(kThreads)
+k_reduce_cols(const double* __restrict__ partial, int nblocks, double* __restrict__ r)
+{
+	__shared__ double red[kThreads / 32];
+	const int         c = blockIdx.x;
+	double            s = 0.0;
+	for (int b = threadIdx.x; b < nblocks; b += kThreads)
+		s += partial[size_t(b) * kMaxCols + c];
+	s = block_sum(s, red);
+	if (threadIdx.x == 0)
+		r[c] = s;
+}
+
+// v -= V[:, 0..ncols) r ; *nrm_out = |v|.  VEC: each thread owns row pairs
+// (16-byte loads), 8 columns of loads issued before their updates; the
+// subtractions run in column order, as in the scalar form.
+template <bool VEC>
 __global__ void __launch_bounds__(kThreads)
 k_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t ld, int ncols,
                  const double* __restrict__ r, size_t n, double* nrm_out, double* partial,
@@ -237,20 +253,57 @@ k_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t ld
 	for (int c = threadIdx.x; c < ncols; c += kThreads)
 		rs[c] = r[c];
 	__syncthreads();
-	double s = 0.0;
-	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
-	     i += size_t(gridDim.x) * kThreads) {
-		double w = v[i];
-		for (int c = 0; c < ncols; ++c)
-			w -= V[size_t(c) * ld + i] * rs[c];
-		v[i] = w;
-		s += w * w;
+	double       s      = 0.0;
+	const size_t stride = size_t(gridDim.x) * kThreads;
+	const size_t first  = blockIdx.x * size_t(kThreads) + threadIdx.x;
+	if (VEC) {
+		double2*     v2  = reinterpret_cast<double2*>(v);
+		const size_t np2 = n / 2;
+		for (size_t p = first; p < np2; p += stride) {
+			double2 w = v2[p];
+			int     c = 0;
+			for (; c + 8 <= ncols; c += 8) {
+				double2 a[8];
+#pragma unroll
+				for (int u = 0; u < 8; ++u)
+					a[u] = __ldg(reinterpret_cast<const double2*>(V + size_t(c + u) * ld) + p);
+#pragma unroll
+				for (int u = 0; u < 8; ++u) {
+					w.x -= a[u].x * rs[c + u];
+					w.y -= a[u].y * rs[c + u];
+				}
+			}
+			for (; c < ncols; ++c) {
+				const double2 a = __ldg(reinterpret_cast<const double2*>(V + size_t(c) * ld) + p);
+				w.x -= a.x * rs[c];
+				w.y -= a.y * rs[c];
+			}
+			v2[p] = w;
+			s += w.x * w.x + w.y * w.y;
+		}
+		if ((n & 1) && first == 0) { // odd length: the last element
+			const size_t i = n - 1;
+			double       w = v[i];
+			for (int c = 0; c < ncols; ++c)
+				w -= V[size_t(c) * ld + i] * rs[c];
+			v[i] = w;
+			s += w * w;
+		}
+	} else {
+		for (size_t i = first; i < n; i += stride) {
+			double w = v[i];
+			for (int c = 0; c < ncols; ++c)
+				w -= V[size_t(c) * ld + i] * rs[c];
+			v[i] = w;
+			s += w * w;
+		}
 	}
 	s = block_sum(s, red);
 	grid_sum(s, partial, ctr, nrm_out, true, red);
 }
 
 // z = sum_c coef[c] V[:, c] (LanczosVectors::excitedVector, LanczosVectors.h:192-201)
+template <bool VEC>
 __global__ void __launch_bounds__(kThreads)
 k_basis_combine(double* __restrict__ z, const double* __restrict__ V, size_t ld, int ncols,
                 const double* __restrict__ coef, size_t n)
@@ -259,13 +312,88 @@ k_basis_combine(double* __restrict__ z, const double* __restrict__ V, size_t ld,
 	for (int c = threadIdx.x; c < ncols; c += kThreads)
 		cs[c] = coef[c];
 	__syncthreads();
-	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
-	     i += size_t(gridDim.x) * kThreads) {
-		double w = 0.0;
-		for (int c = 0; c < ncols; ++c)
-			w += cs[c] * V[size_t(c) * ld + i];
-		z[i] = w;
+	const size_t stride = size_t(gridDim.x) * kThreads;
+	const size_t first  = blockIdx.x * size_t(kThreads) + threadIdx.x;
+	if (VEC) {
+		const size_t np2 = n / 2;
+		for (size_t p = first; p < np2; p += stride) {
+			double2 w = make_double2(0.0, 0.0);
+			int     c = 0;
+			for (; c + 8 <= ncols; c += 8) {
+				double2 a[8];
+#pragma unroll
+				for (int u = 0; u < 8; ++u)
+					a[u] = __ldg(reinterpret_cast<const double2*>(V + size_t(c + u) * ld) + p);
+#pragma unroll
+				for (int u = 0; u < 8; ++u) {
+					w.x += cs[c + u] * a[u].x;
+					w.y += cs[c + u] * a[u].y;
+				}
+			}
+			for (; c < ncols; ++c) {
+				const double2 a = __ldg(reinterpret_cast<const double2*>(V + size_t(c) * ld) + p);
+				w.x += cs[c] * a.x;
+				w.y += cs[c] * a.y;
+			}
+			reinterpret_cast<double2*>(z)[p] = w;
+		}
+		if ((n & 1) && first == 0) {
+			const size_t i = n - 1;
+			double       w = 0.0;
+			for (int c = 0; c < ncols; ++c)
+				w += cs[c] * V[size_t(c) * ld + i];
+			z[i] = w;
+		}
+	} else {
+		for (size_t i = first; i < n; i += stride) {
+			double w = 0.0;
+			for (int c = 0; c < ncols; ++c)
+				w += cs[c] * V[size_t(c) * ld + i];
+			z[i] = w;
+		}
 	}
+}
+
+bool vec2_ok(const void* a, const void* b, size_t ld)
+{
+	return ld % 2 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0
+	    && (reinterpret_cast<uintptr_t>(b) & 15) == 0;
+}
+
+// r[c] = <V[:,c], v>, c < ncols (two launches: partials, per-column sums)
+void basis_dots(const double* V, size_t ld, int ncols, const double* v, size_t n, double* r,
+                double* partial, cudaStream_t st)
+{
+	if (ncols <= 0)
+		return;
+	const int grid = int(std::max<size_t>(1, std::min<size_t>((n + kDotChunk - 1) / kDotChunk, kDotGrid)));
+	if (vec2_ok(V, v, ld))
+		k_basis_dots<true><<<grid, kThreads, 0, st>>>(V, ld, ncols, v, n, partial);
+	else
+		k_basis_dots<false><<<grid, kThreads, 0, st>>>(V, ld, ncols, v, n, partial);
+	k_reduce_cols<<<ncols, kThreads, 0, st>>>(partial, grid, r);
+}
+
+// v -= V r, *nrm_out = |v|
+void basis_subtract(double* v, const double* V, size_t ld, int ncols, const double* r, size_t n,
+                    double* nrm_out, double* partial, unsigned* ctr, cudaStream_t st)
+{
+	const int grid = basis_blocks_for(n);
+	if (vec2_ok(V, v, ld))
+		k_basis_subtract<true><<<grid, kThreads, 0, st>>>(v, V, ld, ncols, r, n, nrm_out, partial, ctr);
+	else
+		k_basis_subtract<false><<<grid, kThreads, 0, st>>>(v, V, ld, ncols, r, n, nrm_out, partial, ctr);
+}
+
+// z = V coef
+void basis_combine(double* z, const double* V, size_t ld, int ncols, const double* coef, size_t n,
+                   cudaStream_t st)
+{
+	const int grid = basis_blocks_for(n);
+	if (vec2_ok(V, z, ld))
+		k_basis_combine<true><<<grid, kThreads, 0, st>>>(z, V, ld, ncols, coef, n);
+	else
+		k_basis_combine<false><<<grid, kThreads, 0, st>>>(z, V, ld, ncols, coef, n);
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -447,8 +575,6 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 	LanczosWork* w  = h->lanczos;
 	cudaStream_t st = h->stream;
 	const int    nb = blocks_for(D);
-	const int    nbb = basis_blocks_for(D);
-	const int    nbd = dots_blocks_for(D);
 	double*      V  = w->V;
 	double*      alpha = w->scal;
 	double*      beta  = w->scal + w->cols;
@@ -494,9 +620,8 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 			k_scale_inv<<<nb, kThreads, 0, st>>>(v2, D, beta + jj + 1);
 			if (p->reortho) { // reorthoIfNecessary (LanczosVectors.h:243-271)
 				const int nc = int(jj) + 1;
-				k_basis_dots<<<nbd, kThreads, 0, st>>>(V, D, nc, v2, D, w->r, w->partial, w->ctr + 3);
-				k_basis_subtract<<<nbb, kThreads, 0, st>>>(v2, V, D, nc, w->r, D, work + 1,
-				                                          w->partial, w->ctr + 4);
+				basis_dots(V, D, nc, v2, D, w->r, w->partial, st);
+				basis_subtract(v2, V, D, nc, w->r, D, work + 1, w->partial, w->ctr + 4, st);
 				k_scale_inv<<<nb, kThreads, 0, st>>>(v2, D, work + 1);
 			}
 		}
@@ -553,7 +678,7 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 	if ((e = cudaMemcpyAsync(w->r, zt.data(), n * sizeof(double), cudaMemcpyHostToDevice, st)))
 		return cuda_status(h, e, "upload Ritz coefficients");
 	double* zdst = on_device ? z : col(j_stop + 1); // that column is free after the solve
-	k_basis_combine<<<nb, kThreads, 0, st>>>(zdst, V, D, int(n), w->r, D);
+	basis_combine(zdst, V, D, int(n), w->r, D, st);
 	if (!on_device
 	    && (e = cudaMemcpyAsync(z, zdst, D * sizeof(double), cudaMemcpyDeviceToHost, st)))
 		return cuda_status(h, e, "copy Ritz vector");
@@ -741,8 +866,6 @@ int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
 	DavidsonWork* w   = h->davidson;
 	cudaStream_t  st  = h->stream;
 	const int     nb  = blocks_for(D);
-	const int     nbb = basis_blocks_for(D);
-	const int     nbd = dots_blocks_for(D);
 	cudaError_t   e;
 	auto          Vc  = [&](int c) { return w->V + size_t(c) * D; };
 	auto          Wc  = [&](int c) { return w->W + size_t(c) * D; };
@@ -774,9 +897,8 @@ int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
 		// orthonormalise the correction against the basis (two classical
 		// Gram-Schmidt passes) and append it
 		for (int pass = 0; pass < (k > 0 ? 2 : 0); ++pass) {
-			k_basis_dots<<<nbd, kThreads, 0, st>>>(w->V, D, k, w->t, D, w->coef, w->partial, w->ctr + 0);
-			k_basis_subtract<<<nbb, kThreads, 0, st>>>(w->t, w->V, D, k, w->coef, D, w->scal + 0,
-			                                          w->partial, w->ctr + 1);
+			basis_dots(w->V, D, k, w->t, D, w->coef, w->partial, st);
+			basis_subtract(w->t, w->V, D, k, w->coef, D, w->scal + 0, w->partial, w->ctr + 1, st);
 		}
 		k_dot<<<nb, kThreads, 0, st>>>(w->t, w->t, D, w->scal + 1, w->partial, w->ctr + 2);
 		k_scale_rsqrt<<<nb, kThreads, 0, st>>>(w->t, Vc(k), D, w->scal + 1);
@@ -787,7 +909,7 @@ int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
 		else
 			++s.fp64_matvecs;
 		// new column of the projected matrix G = V^T H V
-		k_basis_dots<<<nbd, kThreads, 0, st>>>(w->V, D, k + 1, Wc(k), D, w->coef, w->partial, w->ctr + 3);
+		basis_dots(w->V, D, k + 1, Wc(k), D, w->coef, w->partial, st);
 		if ((e = cudaMemcpyAsync(w->host, w->coef, size_t(k + 1) * sizeof(double),
 		                         cudaMemcpyDeviceToHost, st))
 		    || (e = cudaStreamSynchronize(st))) {
@@ -815,8 +937,8 @@ int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
 			rc = cuda_status(h, e, "Ritz coefficients");
 			break;
 		}
-		k_basis_combine<<<nbb, kThreads, 0, st>>>(w->u, w->V, D, k, w->coef, D);
-		k_basis_combine<<<nbb, kThreads, 0, st>>>(w->hu, w->W, D, k, w->coef, D);
+		basis_combine(w->u, w->V, D, k, w->coef, D, st);
+		basis_combine(w->hu, w->W, D, k, w->coef, D, st);
 		k_residual<<<nb, kThreads, 0, st>>>(w->hu, w->u, theta, w->r, D, w->scal + 2, w->partial,
 		                                    w->ctr + 4);
 		if ((e = cudaMemcpyAsync(w->host, w->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st))

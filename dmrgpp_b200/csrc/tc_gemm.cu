@@ -4,8 +4,9 @@
 // one tile accumulates a_hi*b_hi + a_hi*b_lo + a_lo*b_hi in FP32 in tensor
 // memory (the a_lo*b_lo term is below the FP32 accumulation error).
 //
-// Persistent, warp-specialised CTAs (one per SM), each walking the tile list
-// of one grouped pass (kron_plan.h, MixedPlan) with stride gridDim.x:
+// Persistent, warp-specialised CTAs (at most one per SM), each walking its
+// own run of the tile list of one grouped pass (kron_plan.h, MixedPlan;
+// runs balanced on the host by balance_tiles):
 //   warp 0, one thread: producer.  For every 32-wide k-chunk of every
 //     K-segment of its tiles it waits until the ring stage is free, arms the
 //     stage's mbarrier with the byte count and issues four bulk copies
@@ -196,7 +197,7 @@ __device__ void producer(const TcArgs& a, unsigned base, unsigned full0, unsigne
 	using L    = TcLayout<BN>;
 	unsigned g = 0; // chunks issued
 	bool     ok = true;
-	for (int ti = blockIdx.x; ti < a.ntiles && ok; ti += gridDim.x) {
+	for (int ti = a.starts[blockIdx.x]; ti < a.starts[blockIdx.x + 1] && ok; ++ti) {
 		const GemmTile t     = a.tiles[ti];
 		const int      rowsA = min(kBM, round8_dev(t.M) - t.m0);
 		const int      rowsB = min(BN, round8_dev(t.N) - t.n0);
@@ -244,7 +245,7 @@ __device__ void mma_issuer(const TcArgs& a, unsigned base, unsigned tmem, unsign
 	unsigned       tc     = 0; // tiles accumulated
 	bool           ok     = true;
 	bool           issued = false;
-	for (int ti = blockIdx.x; ti < a.ntiles && ok; ti += gridDim.x) {
+	for (int ti = a.starts[blockIdx.x]; ti < a.starts[blockIdx.x + 1] && ok; ++ti) {
 		const GemmTile t     = a.tiles[ti];
 		const int      total = tile_chunks(a, t);
 		if (total == 0)
@@ -339,7 +340,7 @@ __device__ void epilogue(const TcArgs& a, unsigned tmem, unsigned accf0, unsigne
 	const int row     = quarter * 32 + lane;
 	unsigned  tc      = 0;
 	bool      ok      = true;
-	for (int ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) {
+	for (int ti = a.starts[blockIdx.x]; ti < a.starts[blockIdx.x + 1]; ++ti) {
 		const GemmTile t     = a.tiles[ti];
 		const int      total = tile_chunks(a, t);
 		const int      grow  = t.m0 + row;
@@ -463,8 +464,7 @@ constexpr int kStages128 = 3; // 3 x 64 KB
 
 template <int BN, int STAGES, bool PASS1> void launch_one(const TcArgs& a, cudaStream_t stream)
 {
-	const int grid = a.grid < a.ntiles ? a.grid : a.ntiles;
-	tc_gemm_tf32x3_kernel<BN, STAGES, PASS1><<<grid, kTcThreads, tc_smem<BN, STAGES>(), stream>>>(a);
+	tc_gemm_tf32x3_kernel<BN, STAGES, PASS1><<<a.grid, kTcThreads, tc_smem<BN, STAGES>(), stream>>>(a);
 }
 
 } // namespace

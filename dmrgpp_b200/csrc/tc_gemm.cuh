@@ -16,9 +16,10 @@ struct TcArgs {
 	float*          C_lo;
 	double*         Cd;   // pass 2: FP64 column-major output
 	const GemmSeg*  segs;
-	const GemmTile* tiles;
+	const GemmTile* tiles;  // CTA b processes tiles [starts[b], starts[b+1])
+	const int*      starts; // grid + 1 entries (balance_tiles)
 	int             ntiles;
-	int             grid;  // persistent CTAs (one per SM); at most ntiles are launched
+	int             grid;   // persistent CTAs, at most one per SM
 	int*            error; // set to 2 when an mbarrier wait gave up
 };
 
@@ -26,7 +27,7 @@ struct TcArgs {
 cudaError_t tc_init();
 
 // One grouped pass over a.ntiles tiles of 128 x bn (bn = 64 or 128) by
-// min(a.grid, a.ntiles) persistent CTAs.
+// a.grid persistent CTAs.
 cudaError_t tc_launch(const TcArgs& a, int bn, bool pass1, cudaStream_t stream);
 
 // x (patch order, FP64) -> TF32 hi/lo parts at map[e].
