@@ -110,6 +110,13 @@ SIGNATURES.update({
 
 SIGNATURES.update({
     "dmrgpp_lanczos_params_init": (None, [ctypes.POINTER(LanczosParams)]),
+    "dmrgpp_kron_create_group": (ctypes.c_int, [ctypes.POINTER(KronDesc), _sz,
+                                                ctypes.POINTER(ctypes.c_void_p)]),
+    "dmrgpp_kron_group_sectors": (ctypes.c_int, [ctypes.c_void_p, _szp,
+                                                 ctypes.POINTER(ctypes.c_longlong)]),
+    "dmrgpp_lanczos_lowest_group": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LanczosParams),
+                                                   ctypes.c_void_p, ctypes.c_int, _dp,
+                                                   ctypes.c_void_p, _szp]),
     "dmrgpp_lanczos_lowest": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LanczosParams),
                                              ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_void_p,
                                              _szp]),

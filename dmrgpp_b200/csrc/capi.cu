@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <new>
 #include <string>
@@ -64,6 +65,7 @@ void release(dmrgpp_kron_handle h)
 		return;
 	dmrgpp::release_lanczos(h);
 	dmrgpp::release_davidson(h);
+	dmrgpp::release_group(h);
 	cudaFree(h->d_diag);
 	h->d_diag = nullptr;
 	cudaFree(h->m_ops_hi);
@@ -96,18 +98,23 @@ void release(dmrgpp_kron_handle h)
 }
 
 // Tile shape for a sector: small sectors need small tiles to fill the SMs.
-void pick_tile(const dmrgpp_kron_desc* d, int& bm, int& bn)
+void pick_tile_sizes(size_t np, const size_t* l, const size_t* r, int& bm, int& bn)
 {
 	size_t maxs = 0;
-	for (size_t p = 0; p < d->npatches; ++p) {
-		maxs = d->left_patch_size[p] > maxs ? d->left_patch_size[p] : maxs;
-		maxs = d->right_patch_size[p] > maxs ? d->right_patch_size[p] : maxs;
+	for (size_t p = 0; p < np; ++p) {
+		maxs = l[p] > maxs ? l[p] : maxs;
+		maxs = r[p] > maxs ? r[p] : maxs;
 	}
 	if (maxs <= 192) {
 		bm = bn = 32;
 	} else {
 		bm = bn = 64;
 	}
+}
+
+void pick_tile(const dmrgpp_kron_desc* d, int& bm, int& bn)
+{
+	pick_tile_sizes(d->npatches, d->left_patch_size, d->right_patch_size, bm, bn);
 }
 
 int check_desc(const dmrgpp_kron_desc* d)
@@ -213,7 +220,7 @@ int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 
 }
 
-int build_mixed(dmrgpp_kron_handle h, const dmrgpp_kron_desc* d)
+int build_mixed(dmrgpp_kron_handle h)
 {
 	std::vector<float> hi, lo;
 	std::vector<int>   xmap;
@@ -221,8 +228,7 @@ int build_mixed(dmrgpp_kron_handle h, const dmrgpp_kron_desc* d)
 	for (size_t p = 0; p < h->plan.np; ++p)
 		maxs = std::max<size_t>(maxs, size_t(std::max(h->plan.l[p], h->plan.r[p])));
 	const int   bn  = maxs > 96 ? 128 : 64;
-	std::string msg = build_mixed_plan(h->plan, d->Amatrix, d->ld_Amatrix, d->Bmatrix,
-	                                   d->ld_Bmatrix, bn, &hi, &lo, &xmap);
+	std::string msg = build_mixed_plan(h->plan, bn, &hi, &lo, &xmap);
 	if (!msg.empty())
 		return fail(h, DMRGPP_INVALID_ARG, msg);
 	const MixedPlan& mp = h->plan.mixed;
@@ -349,6 +355,87 @@ int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 
 } // namespace dmrgpp
 
+namespace {
+
+// Device side of a new handle whose plan (with host blocks) is built: device
+// buffers, persistent schedule, diagonal, and the TF32x3 form if requested.
+// Frees h on failure.
+int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm,
+                  const std::vector<double>& pack, dmrgpp_kron_handle* out)
+{
+	if (device >= 0) {
+		h->device = device;
+	} else if (cudaGetDevice(&h->device) != cudaSuccess) {
+		delete h;
+		return fail(nullptr, DMRGPP_CUDA_ERROR, "no CUDA device");
+	}
+	DeviceGuard g(h->device);
+	auto        bail = [&](cudaError_t e, const char* where) {
+                int rc = cuda_fail(nullptr, e, where);
+                release(h);
+                delete h;
+                return rc;
+	};
+	if (!g.ok)
+		return bail(cudaErrorInvalidDevice, "cudaSetDevice");
+
+	cudaError_t e = dmrgpp::init_grouped_dgemm();
+	if (e != cudaSuccess)
+		return bail(e, "kernel attributes");
+	// NULL is the CUDA default stream, as for cuBLAS handles
+	h->stream = static_cast<cudaStream_t>(stream);
+
+	const auto&  P   = h->plan;
+	const size_t dim = size_t(P.dim());
+	if ((e = cudaMalloc(&h->d_ops, size_t(P.op_elems ? P.op_elems : 1) * sizeof(double))))
+		return bail(e, "cudaMalloc(operators)");
+	if ((e = cudaMalloc(&h->d_bx, size_t(P.bx_elems ? P.bx_elems : 1) * sizeof(double))))
+		return bail(e, "cudaMalloc(BX)");
+	if ((e = cudaMalloc(&h->d_x, dim * sizeof(double))))
+		return bail(e, "cudaMalloc(x)");
+	if ((e = cudaMalloc(&h->d_y, dim * sizeof(double))))
+		return bail(e, "cudaMalloc(y)");
+
+	if ((e = cudaHostAlloc(reinterpret_cast<void**>(&h->err_host), sizeof(int), cudaHostAllocMapped)))
+		return bail(e, "cudaHostAlloc(error word)");
+	*h->err_host = 0;
+	if ((e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&h->err_dev), h->err_host, 0)))
+		return bail(e, "error word mapping");
+	if (int rc = dmrgpp::configure_schedule(h, bm == 32 ? 0 : 2, 2)) {
+		const std::string why = h->err;
+		release(h);
+		delete h;
+		return fail(nullptr, rc, why);
+	}
+	if (!pack.empty()
+	    && (e = cudaMemcpy(h->d_ops, pack.data(), pack.size() * sizeof(double), cudaMemcpyHostToDevice)))
+		return bail(e, "upload operators");
+	{
+		std::vector<double> diag;
+		dmrgpp::sector_diagonal(h->plan, diag);
+		if ((e = cudaMalloc(&h->d_diag, std::max<size_t>(diag.size(), 1) * sizeof(double))))
+			return bail(e, "cudaMalloc(diagonal)");
+		if (!diag.empty()
+		    && (e = cudaMemcpy(h->d_diag, diag.data(), diag.size() * sizeof(double), cudaMemcpyHostToDevice)))
+			return bail(e, "upload diagonal");
+	}
+	if (h->precision == DMRGPP_TF32X3) {
+		if (int rc = dmrgpp::build_mixed(h)) {
+			const std::string why = h->err;
+			release(h);
+			delete h;
+			return fail(nullptr, rc, why);
+		}
+	}
+	// the caller's host blocks are not referenced after create
+	h->plan.blocks.clear();
+	h->plan.blocks.shrink_to_fit();
+	*out = h;
+	return DMRGPP_OK;
+}
+
+} // namespace
+
 extern "C" {
 
 const char* dmrgpp_version(void) { return DMRGPP_VERSION_STRING; }
@@ -425,72 +512,92 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 		delete h;
 		return fail(nullptr, DMRGPP_INVALID_ARG, msg);
 	}
+	h->sector_start = { 0, h->plan.dim() };
+	return finish_create(h, d->device, d->stream, bm, pack, out);
+}
 
-	if (d->device >= 0) {
-		h->device = d->device;
-	} else if (cudaGetDevice(&h->device) != cudaSuccess) {
-		delete h;
-		return fail(nullptr, DMRGPP_CUDA_ERROR, "no CUDA device");
+int dmrgpp_kron_create_group(const dmrgpp_kron_desc* descs, size_t nsectors, dmrgpp_kron_handle* out)
+{
+	if (!out)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "null output handle");
+	*out = nullptr;
+	if (!descs || nsectors == 0)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "no sectors");
+	for (size_t s = 0; s < nsectors; ++s) {
+		if (int rc = check_desc(&descs[s]))
+			return rc;
+		if (descs[s].noperator == 0 || descs[s].npatches == 0)
+			return fail(nullptr, DMRGPP_INVALID_ARG,
+			            "sector " + std::to_string(s) + ": noperator and npatches must be >= 1");
+		if (!descs[s].Amatrix || !descs[s].ld_Amatrix || !descs[s].Bmatrix || !descs[s].ld_Bmatrix)
+			return fail(nullptr, DMRGPP_INVALID_ARG, "sector " + std::to_string(s) + ": null table");
+		if (descs[s].precision != descs[0].precision || descs[s].device != descs[0].device
+		    || descs[s].stream != descs[0].stream)
+			return fail(nullptr, DMRGPP_INVALID_ARG,
+			            "all sectors of a group need the same precision, device and stream");
 	}
-	DeviceGuard g(h->device);
-	auto        bail = [&](cudaError_t e, const char* where) {
-                int rc = cuda_fail(nullptr, e, where);
-                release(h);
-                delete h;
-                return rc;
-	};
-	if (!g.ok)
-		return bail(cudaErrorInvalidDevice, "cudaSetDevice");
+	if (descs[0].precision == DMRGPP_SPLIT_BF16)
+		return fail(nullptr, DMRGPP_NOT_SUPPORTED, "split-BF16 is not built into this library");
 
-	cudaError_t e = dmrgpp::init_grouped_dgemm();
-	if (e != cudaSuccess)
-		return bail(e, "kernel attributes");
-	// NULL is the CUDA default stream, as for cuBLAS handles
-	h->stream = static_cast<cudaStream_t>(d->stream);
-
-	const auto&  P   = h->plan;
-	const size_t dim = size_t(P.dim());
-	if ((e = cudaMalloc(&h->d_ops, size_t(P.op_elems ? P.op_elems : 1) * sizeof(double))))
-		return bail(e, "cudaMalloc(operators)");
-	if ((e = cudaMalloc(&h->d_bx, size_t(P.bx_elems ? P.bx_elems : 1) * sizeof(double))))
-		return bail(e, "cudaMalloc(BX)");
-	if ((e = cudaMalloc(&h->d_x, dim * sizeof(double))))
-		return bail(e, "cudaMalloc(x)");
-	if ((e = cudaMalloc(&h->d_y, dim * sizeof(double))))
-		return bail(e, "cudaMalloc(y)");
-
-	if ((e = cudaHostAlloc(reinterpret_cast<void**>(&h->err_host), sizeof(int), cudaHostAllocMapped)))
-		return bail(e, "cudaHostAlloc(error word)");
-	*h->err_host = 0;
-	if ((e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&h->err_dev), h->err_host, 0)))
-		return bail(e, "error word mapping");
-	if (int rc = dmrgpp::configure_schedule(h, bm == 32 ? 0 : 2, 2)) {
-		const std::string why = h->err;
-		release(h);
-		delete h;
-		return fail(nullptr, rc, why);
-	}
-	if (!pack.empty()
-	    && (e = cudaMemcpy(h->d_ops, pack.data(), pack.size() * sizeof(double), cudaMemcpyHostToDevice)))
-		return bail(e, "upload operators");
-	{
-		std::vector<double> diag;
-		dmrgpp::sector_diagonal(h->plan, d->Amatrix, d->ld_Amatrix, d->Bmatrix, d->ld_Bmatrix, diag);
-		if ((e = cudaMalloc(&h->d_diag, std::max<size_t>(diag.size(), 1) * sizeof(double))))
-			return bail(e, "cudaMalloc(diagonal)");
-		if (!diag.empty()
-		    && (e = cudaMemcpy(h->d_diag, diag.data(), diag.size() * sizeof(double), cudaMemcpyHostToDevice)))
-			return bail(e, "upload diagonal");
-	}
-	if (d->precision == DMRGPP_TF32X3) {
-		if (int rc = dmrgpp::build_mixed(h, d)) {
-			const std::string why = h->err;
-			release(h);
-			delete h;
-			return fail(nullptr, rc, why);
+	// the union: sector s's patches follow those of sectors 0..s-1; no block
+	// connects two sectors, so the union's H is block-diagonal
+	std::vector<size_t>           l, r;
+	std::vector<dmrgpp::Triple>   triples;
+	std::vector<dmrgpp::BlockRef> blocks;
+	std::vector<long long>        starts(1, 0);
+	double                        f_alg = 0.0;
+	size_t                        nop   = 0;
+	for (size_t s = 0; s < nsectors; ++s) {
+		const dmrgpp_kron_desc& d = descs[s];
+		for (size_t p = 0; p < d.npatches; ++p)
+			if (d.left_patch_size[p] < 1 || d.right_patch_size[p] < 1)
+				return fail(nullptr, DMRGPP_INVALID_ARG,
+				            "sector " + std::to_string(s) + " patch " + std::to_string(p)
+				                + " has an empty left or right group");
+		if (l.size() + d.npatches > size_t(INT_MAX))
+			return fail(nullptr, DMRGPP_INVALID_ARG, "too many patches in the group");
+		std::string msg = dmrgpp::collect_triples(d.noperator, d.npatches, d.left_patch_size,
+		                                          d.right_patch_size, d.Amatrix, d.ld_Amatrix,
+		                                          d.Bmatrix, d.ld_Bmatrix, int(l.size()), triples,
+		                                          blocks, f_alg);
+		if (!msg.empty())
+			return fail(nullptr, DMRGPP_INVALID_ARG, "sector " + std::to_string(s) + ": " + msg);
+		long long dim = 0;
+		for (size_t p = 0; p < d.npatches; ++p) {
+			l.push_back(d.left_patch_size[p]);
+			r.push_back(d.right_patch_size[p]);
+			dim += (long long)d.left_patch_size[p] * (long long)d.right_patch_size[p];
 		}
+		starts.push_back(starts.back() + dim);
+		nop = std::max(nop, d.noperator);
 	}
-	*out = h;
+
+	dmrgpp_kron_handle h = new (std::nothrow) dmrgpp_kron_s();
+	if (!h)
+		return fail(nullptr, DMRGPP_OOM, "host allocation failed");
+	h->precision = descs[0].precision;
+	int bm, bn;
+	pick_tile_sizes(l.size(), l.data(), r.data(), bm, bn);
+	std::vector<double> pack;
+	std::string msg = dmrgpp::build_kron_plan_triples(nop, l.size(), l.data(), r.data(),
+	                                                  std::move(triples), std::move(blocks), f_alg,
+	                                                  bm, bn, h->plan, &pack);
+	if (!msg.empty()) {
+		delete h;
+		return fail(nullptr, DMRGPP_INVALID_ARG, msg);
+	}
+	h->sector_start = std::move(starts);
+	return finish_create(h, descs[0].device, descs[0].stream, bm, pack, out);
+}
+
+int dmrgpp_kron_group_sectors(dmrgpp_kron_handle h, size_t* nsectors, long long* offsets)
+{
+	if (!h || !nsectors)
+		return fail(h, DMRGPP_INVALID_ARG, "null argument");
+	*nsectors = h->sector_start.size() - 1;
+	if (offsets)
+		for (size_t s = 0; s < h->sector_start.size(); ++s)
+			offsets[s] = h->sector_start[s];
 	return DMRGPP_OK;
 }
 

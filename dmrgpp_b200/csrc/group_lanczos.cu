@@ -1,0 +1,574 @@
+// Lanczos for every sector of a group handle at once (dmrgpp_kron_create_group):
+// all sectors advance in lockstep, one persistent launch applies H to all of
+// them per step, and every vector operation is segmented by sector.
+//
+// Per sector the recurrence is that of the single-sector solver (lanczos.cu,
+// following LanczosCore::decomposition, LanczosCore.h:147-272, and
+// LanczosVectors::oneStepDecomposition / reorthoIfNecessary,
+// LanczosVectors.h:203-271): normalise, V1 = H V0 - a0 V0, then
+// V2 = H V1 - a_j V1 - b_j V0, b_{j+1} = |V2|, V2 /= b_{j+1}, full
+// reorthogonalisation against the stored vectors (classical Gram-Schmidt)
+// and renormalisation.  The stopping test runs on the host every
+// check_every steps: a sector stops at the first test point where its lowest
+// eigs_for_stop Ritz values changed by less than the tolerance over the last
+// step (after min_steps steps), or when its Krylov space is exhausted.  A
+// stopped sector is masked out of every later vector operation (its matvec
+// still runs inside the group launch).  No counterpart in the reference.
+//
+// The sector vectors are cut into chunks of at most kChunk rows that never
+// cross a sector boundary; every kernel walks chunks, so each block knows its
+// sector, and every sum runs in a fixed order (bitwise reproducible).
+#include "dmrgpp_kron.h"
+#include "handle.h"
+#include "tridiag.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace dmrgpp {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kChunk   = 2048; // rows per chunk
+constexpr int kGrid    = 1184; // at most 8 blocks per SM
+
+struct Chunk {
+	long long begin;
+	int       len;
+	int       seg;
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red)
+{
+	for (int o = 16; o > 0; o >>= 1)
+		v += __shfl_down_sync(0xffffffffu, v, o);
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (lane == 0)
+		red[warp] = v;
+	__syncthreads();
+	double s = 0.0;
+	if (threadIdx.x == 0)
+		for (int w = 0; w < kThreads / 32; ++w)
+			s += red[w];
+	__syncthreads();
+	return s; // valid in thread 0
+}
+
+// partial[ch] = <x, y> over chunk ch (0 for stopped sectors)
+__global__ void __launch_bounds__(kThreads)
+k_g_dot(const double* __restrict__ x, const double* __restrict__ y, const Chunk* __restrict__ chunks,
+        int nch, const int* __restrict__ active, double* __restrict__ partial)
+{
+	__shared__ double red[kThreads / 32];
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk c = chunks[ch];
+		double      s = 0.0;
+		if (active[c.seg])
+			for (int i = threadIdx.x; i < c.len; i += kThreads)
+				s += x[c.begin + i] * y[c.begin + i];
+		s = block_sum(s, red);
+		if (threadIdx.x == 0)
+			partial[ch] = s;
+	}
+}
+
+// out[s] = sum of the sector's chunk partials (sqrt of it when root), for
+// active sectors; one block per sector
+__global__ void __launch_bounds__(kThreads)
+k_g_finish(const double* __restrict__ partial, const int* __restrict__ seg_chunk,
+           const int* __restrict__ active, double* __restrict__ out, int root)
+{
+	__shared__ double red[kThreads / 32];
+	const int         s = blockIdx.x;
+	if (!active[s])
+		return;
+	double t = 0.0;
+	for (int ch = seg_chunk[s] + threadIdx.x; ch < seg_chunk[s + 1]; ch += kThreads)
+		t += partial[ch];
+	t = block_sum(t, red);
+	if (threadIdx.x == 0)
+		out[s] = root ? sqrt(t) : t;
+}
+
+// y = x * f(scal[sector]): mode 0 f = 1/sqrt(v) (v a squared norm), mode 1
+// f = 1/v when v > 0 (else y = x); active sectors only
+__global__ void __launch_bounds__(kThreads)
+k_g_scale(const double* __restrict__ x, double* __restrict__ y, const double* __restrict__ scal,
+          int mode, const Chunk* __restrict__ chunks, int nch, const int* __restrict__ active)
+{
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk c = chunks[ch];
+		if (!active[c.seg])
+			continue;
+		const double v = scal[c.seg];
+		double       f = 1.0;
+		if (mode == 0)
+			f = 1.0 / sqrt(v);
+		else if (v > 0.0)
+			f = 1.0 / v;
+		for (int i = threadIdx.x; i < c.len; i += kThreads)
+			y[c.begin + i] = x[c.begin + i] * f;
+	}
+}
+
+// v2 -= alpha[s] v1 + beta[s] v0 (v0 may be null); partial[ch] = |v2|^2 over ch
+__global__ void __launch_bounds__(kThreads)
+k_g_update(double* __restrict__ v2, const double* __restrict__ v1, const double* __restrict__ v0,
+           const double* __restrict__ alpha, const double* __restrict__ beta,
+           const Chunk* __restrict__ chunks, int nch, const int* __restrict__ active,
+           double* __restrict__ partial)
+{
+	__shared__ double red[kThreads / 32];
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk c = chunks[ch];
+		double      s = 0.0;
+		if (active[c.seg]) {
+			const double a = alpha[c.seg], b = v0 ? beta[c.seg] : 0.0;
+			for (int i = threadIdx.x; i < c.len; i += kThreads) {
+				const long long q = c.begin + i;
+				double          w = v2[q] - a * v1[q];
+				if (v0)
+					w -= b * v0[q];
+				v2[q] = w;
+				s += w * w;
+			}
+		}
+		s = block_sum(s, red);
+		if (threadIdx.x == 0)
+			partial[ch] = s;
+	}
+}
+
+// partial[ch * ldp + c] = <V[:, c], v> over chunk ch, c < ncols (active sectors)
+__global__ void __launch_bounds__(kThreads)
+k_g_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* __restrict__ v,
+               const Chunk* __restrict__ chunks, int nch, const int* __restrict__ active,
+               double* __restrict__ partial, int ldp)
+{
+	__shared__ double vs[kChunk];
+	const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk c = chunks[ch];
+		if (!active[c.seg])
+			continue;
+		__syncthreads();
+		for (int i = threadIdx.x; i < c.len; i += kThreads)
+			vs[i] = v[c.begin + i];
+		__syncthreads();
+		for (int col = warp; col < ncols; col += kThreads / 32) {
+			const double* cp = V + size_t(col) * ld + c.begin;
+			double        s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+			int           i  = lane;
+			for (; i + 96 < c.len; i += 128) {
+				s0 += __ldg(cp + i) * vs[i];
+				s1 += __ldg(cp + i + 32) * vs[i + 32];
+				s2 += __ldg(cp + i + 64) * vs[i + 64];
+				s3 += __ldg(cp + i + 96) * vs[i + 96];
+			}
+			for (; i < c.len; i += 32)
+				s0 += __ldg(cp + i) * vs[i];
+			double s = (s0 + s1) + (s2 + s3);
+			for (int o = 16; o > 0; o >>= 1)
+				s += __shfl_down_sync(0xffffffffu, s, o);
+			if (lane == 0)
+				partial[size_t(ch) * ldp + col] = s;
+		}
+	}
+}
+
+// r[s * ldp + c] = sum over the sector's chunks of partial[ch * ldp + c]
+__global__ void __launch_bounds__(kThreads)
+k_g_basis_reduce(const double* __restrict__ partial, int ldp, int ncols,
+                 const int* __restrict__ seg_chunk, const int* __restrict__ active,
+                 double* __restrict__ r)
+{
+	const int s = blockIdx.x;
+	if (!active[s])
+		return;
+	for (int col = threadIdx.x; col < ncols; col += kThreads) {
+		double t = 0.0;
+		for (int ch = seg_chunk[s]; ch < seg_chunk[s + 1]; ++ch)
+			t += partial[size_t(ch) * ldp + col];
+		r[size_t(s) * ldp + col] = t;
+	}
+}
+
+// v -= V[:, 0..ncols) r[sector]; partial[ch] = |v|^2 over ch
+__global__ void __launch_bounds__(kThreads)
+k_g_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t ld, int ncols,
+                   const double* __restrict__ r, int ldp, const Chunk* __restrict__ chunks, int nch,
+                   const int* __restrict__ active, double* __restrict__ partial)
+{
+	__shared__ double rs[1024];
+	__shared__ double red[kThreads / 32];
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk c = chunks[ch];
+		double      s = 0.0;
+		if (active[c.seg]) {
+			__syncthreads();
+			for (int col = threadIdx.x; col < ncols; col += kThreads)
+				rs[col] = r[size_t(c.seg) * ldp + col];
+			__syncthreads();
+			for (int i = threadIdx.x; i < c.len; i += kThreads) {
+				const long long q = c.begin + i;
+				double          w = v[q];
+				int             col = 0;
+				for (; col + 4 <= ncols; col += 4) {
+					const double a0 = __ldg(V + size_t(col) * ld + q);
+					const double a1 = __ldg(V + size_t(col + 1) * ld + q);
+					const double a2 = __ldg(V + size_t(col + 2) * ld + q);
+					const double a3 = __ldg(V + size_t(col + 3) * ld + q);
+					w -= a0 * rs[col];
+					w -= a1 * rs[col + 1];
+					w -= a2 * rs[col + 2];
+					w -= a3 * rs[col + 3];
+				}
+				for (; col < ncols; ++col)
+					w -= __ldg(V + size_t(col) * ld + q) * rs[col];
+				v[q] = w;
+				s += w * w;
+			}
+		}
+		s = block_sum(s, red);
+		if (threadIdx.x == 0)
+			partial[ch] = s;
+	}
+}
+
+// z = V[:, 0..ncols[s]) coef[s] for every sector
+__global__ void __launch_bounds__(kThreads)
+k_g_basis_combine(double* __restrict__ z, const double* __restrict__ V, size_t ld,
+                  const int* __restrict__ ncols, const double* __restrict__ coef, int ldp,
+                  const Chunk* __restrict__ chunks, int nch)
+{
+	__shared__ double cs[1024];
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk c  = chunks[ch];
+		const int   nc = ncols[c.seg];
+		__syncthreads();
+		for (int col = threadIdx.x; col < nc; col += kThreads)
+			cs[col] = coef[size_t(c.seg) * ldp + col];
+		__syncthreads();
+		for (int i = threadIdx.x; i < c.len; i += kThreads) {
+			const long long q = c.begin + i;
+			double          w = 0.0;
+			for (int col = 0; col < nc; ++col)
+				w += cs[col] * __ldg(V + size_t(col) * ld + q);
+			z[q] = w;
+		}
+	}
+}
+
+int status(dmrgpp_kron_handle h, cudaError_t e, const char* where)
+{
+	return handle_fail(h, DMRGPP_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+} // namespace
+
+// Device buffers of the group solver of one handle.
+struct GroupWork {
+	size_t  dim = 0;
+	int     cols = 0, nseg = 0, nch = 0;
+	double* V       = nullptr; // dim x cols
+	double* z       = nullptr; // dim, Ritz vectors
+	double* alpha   = nullptr; // cols x nseg (step-major)
+	double* beta    = nullptr; // (cols + 1) x nseg
+	double* scal    = nullptr; // nseg x 4 scratch (norms)
+	double* partial = nullptr; // nch x cols
+	double* r       = nullptr; // nseg x cols (projections, Ritz coefficients)
+	Chunk*  chunks  = nullptr;
+	int*    seg_chunk = nullptr; // nseg + 1
+	int*    active  = nullptr;   // nseg
+	int*    ncols   = nullptr;   // nseg (Ritz vector lengths)
+	double* host    = nullptr;   // pinned: alpha, beta
+};
+
+void release_group(dmrgpp_kron_handle h)
+{
+	GroupWork* w = h->group;
+	if (!w)
+		return;
+	cudaFree(w->V);
+	cudaFree(w->z);
+	cudaFree(w->alpha);
+	cudaFree(w->beta);
+	cudaFree(w->scal);
+	cudaFree(w->partial);
+	cudaFree(w->r);
+	cudaFree(w->chunks);
+	cudaFree(w->seg_chunk);
+	cudaFree(w->active);
+	cudaFree(w->ncols);
+	if (w->host)
+		cudaFreeHost(w->host);
+	delete w;
+	h->group = nullptr;
+}
+
+namespace {
+
+int ensure_group_work(dmrgpp_kron_handle h, int cols)
+{
+	const size_t dim  = size_t(h->plan.dim());
+	const int    nseg = int(h->sector_start.size()) - 1;
+	GroupWork*   w    = h->group;
+	if (w && w->dim == dim && w->cols >= cols && w->nseg == nseg)
+		return DMRGPP_OK;
+	release_group(h);
+	w        = new GroupWork();
+	h->group = w;
+	w->dim   = dim;
+	w->cols  = cols;
+	w->nseg  = nseg;
+	std::vector<Chunk> ch;
+	std::vector<int>   sc(1, 0);
+	for (int s = 0; s < nseg; ++s) {
+		for (long long b = h->sector_start[size_t(s)]; b < h->sector_start[size_t(s) + 1]; b += kChunk)
+			ch.push_back({ b, int(std::min<long long>(kChunk, h->sector_start[size_t(s) + 1] - b)), s });
+		sc.push_back(int(ch.size()));
+	}
+	w->nch = int(ch.size());
+	cudaError_t e;
+	const size_t nsc = size_t(nseg) * size_t(cols);
+	if ((e = cudaMalloc(&w->V, dim * size_t(cols) * sizeof(double))) || (e = cudaMalloc(&w->z, dim * sizeof(double)))
+	    || (e = cudaMalloc(&w->alpha, nsc * sizeof(double)))
+	    || (e = cudaMalloc(&w->beta, (nsc + size_t(nseg)) * sizeof(double)))
+	    || (e = cudaMalloc(&w->scal, size_t(nseg) * 4 * sizeof(double)))
+	    || (e = cudaMalloc(&w->partial, std::max<size_t>(1, ch.size()) * size_t(cols) * sizeof(double)))
+	    || (e = cudaMalloc(&w->r, nsc * sizeof(double)))
+	    || (e = cudaMalloc(&w->chunks, std::max<size_t>(1, ch.size()) * sizeof(Chunk)))
+	    || (e = cudaMalloc(&w->seg_chunk, sc.size() * sizeof(int)))
+	    || (e = cudaMalloc(&w->active, size_t(nseg) * sizeof(int)))
+	    || (e = cudaMalloc(&w->ncols, size_t(nseg) * sizeof(int)))
+	    || (e = cudaHostAlloc(&w->host, (2 * nsc + size_t(nseg)) * sizeof(double), 0)))
+		return status(h, e, "group solver allocation");
+	if ((e = cudaMemcpy(w->chunks, ch.data(), ch.size() * sizeof(Chunk), cudaMemcpyHostToDevice))
+	    || (e = cudaMemcpy(w->seg_chunk, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice))
+	    || (e = cudaMemset(w->beta, 0, (nsc + size_t(nseg)) * sizeof(double)))
+	    || (e = cudaMemset(w->alpha, 0, nsc * sizeof(double))))
+		return status(h, e, "group solver set-up");
+	return DMRGPP_OK;
+}
+
+} // namespace
+
+} // namespace dmrgpp
+
+extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_lanczos_params* p,
+                                           const double* init, int on_device, double* energies,
+                                           double* z, size_t* steps_taken)
+{
+	using namespace dmrgpp;
+	if (!h)
+		return DMRGPP_INVALID_ARG;
+	if (!p || !init || !energies || !z)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "null argument");
+	if (p->steps < 1 || p->check_every < 1 || p->eigs_for_stop < 1)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "steps, check_every and eigs_for_stop must be >= 1");
+	const int    S = int(h->sector_start.size()) - 1;
+	const size_t D = size_t(h->plan.dim());
+	std::vector<size_t> maxn_s(static_cast<size_t>(S));
+	size_t              maxn = 1;
+	for (int s = 0; s < S; ++s) {
+		const size_t Ds = size_t(h->sector_start[size_t(s) + 1] - h->sector_start[size_t(s)]);
+		maxn_s[size_t(s)] = std::max<size_t>(1, std::min(p->steps, Ds)); // LanczosCore.h:177-178
+		maxn              = std::max(maxn, maxn_s[size_t(s)]);
+	}
+	if (maxn + 1 > 1024)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "at most 1023 Lanczos steps");
+
+	int prev = -1;
+	cudaGetDevice(&prev);
+	if (prev != h->device)
+		cudaSetDevice(h->device);
+	struct Restore {
+		int dev, prev;
+		~Restore()
+		{
+			if (dev != prev && prev >= 0)
+				cudaSetDevice(prev);
+		}
+	} restore { h->device, prev };
+
+	const int cols = int(maxn) + 1;
+	if (int rc = ensure_group_work(h, cols))
+		return rc;
+	GroupWork*         w   = h->group;
+	const cudaStream_t st  = h->stream;
+	const int          nch = w->nch;
+	const int          grid = std::max(1, std::min(nch, kGrid));
+	const int          ldp = w->cols;
+	auto               col = [&](size_t c) { return w->V + c * D; };
+	auto               al  = [&](size_t j) { return w->alpha + j * size_t(S); };
+	auto               be  = [&](size_t j) { return w->beta + j * size_t(S); };
+	double*            nrm = w->scal;
+	cudaError_t        e;
+
+	std::vector<int> act(size_t(S), 1);
+	if ((e = cudaMemcpyAsync(w->active, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st))
+	    || (e = cudaMemsetAsync(w->beta, 0, size_t(S) * sizeof(double), st))) // beta_0 = 0
+		return status(h, e, "group solver start");
+	if ((e = cudaMemcpyAsync(col(1), init, D * sizeof(double),
+	                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st)))
+		return status(h, e, "copy initial vectors");
+
+	// per-sector reductions: partial per chunk, then one sum per sector
+	auto dot = [&](const double* x, const double* y, double* out, int root) {
+		k_g_dot<<<grid, kThreads, 0, st>>>(x, y, w->chunks, nch, w->active, w->partial);
+		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, w->active, out, root);
+	};
+	// V0 = init / |init| per sector (LanczosCore.h:166-175)
+	dot(col(1), col(1), nrm, 0);
+	k_g_scale<<<grid, kThreads, 0, st>>>(col(1), col(0), nrm, 0, w->chunks, nch, w->active);
+	// first step (LanczosCore.h:186-208)
+	if (int rc = kron_apply_device(h, col(0), col(1)))
+		return rc;
+	dot(col(1), col(0), al(0), 0);
+	k_g_update<<<grid, kThreads, 0, st>>>(col(1), col(0), nullptr, al(0), be(0), w->chunks, nch,
+	                                      w->active, w->partial);
+	k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, w->active, be(1), 1);
+	k_g_scale<<<grid, kThreads, 0, st>>>(col(1), col(1), be(1), 1, w->chunks, nch, w->active);
+
+	std::vector<size_t> j_stop(size_t(S), 0);
+	int                 n_active = S;
+	for (int s = 0; s < S; ++s)
+		if (maxn_s[size_t(s)] == 1) { // nothing to iterate: the 1 x 1 tridiagonal
+			act[size_t(s)] = 0;
+			--n_active;
+		}
+	if (n_active < S
+	    && (e = cudaMemcpyAsync(w->active, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
+		return status(h, e, "update active sectors");
+	const size_t nsc = size_t(S) * size_t(cols);
+	std::vector<double> eold(size_t(S) * p->eigs_for_stop, 0.0);
+	size_t j = 1;
+	while (n_active > 0 && j < maxn) {
+		// no active sector runs past its own last step (its Krylov space)
+		size_t cap = maxn;
+		for (int s = 0; s < S; ++s)
+			if (act[size_t(s)])
+				cap = std::min(cap, maxn_s[size_t(s)]);
+		const size_t jend = std::min(cap, j + size_t(p->check_every));
+		for (size_t jj = j; jj < jend; ++jj) {
+			double* v0 = col(jj - 1);
+			double* v1 = col(jj);
+			double* v2 = col(jj + 1);
+			if (int rc = kron_apply_device(h, v1, v2))
+				return rc;
+			dot(v2, v1, al(jj), 0);
+			k_g_update<<<grid, kThreads, 0, st>>>(v2, v1, v0, al(jj), be(jj), w->chunks, nch,
+			                                      w->active, w->partial);
+			k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, w->active, be(jj + 1), 1);
+			k_g_scale<<<grid, kThreads, 0, st>>>(v2, v2, be(jj + 1), 1, w->chunks, nch, w->active);
+			if (p->reortho) { // reorthoIfNecessary (LanczosVectors.h:243-271)
+				const int nc = int(jj) + 1;
+				k_g_basis_dots<<<grid, kThreads, 0, st>>>(w->V, D, nc, v2, w->chunks, nch,
+				                                          w->active, w->partial, ldp);
+				k_g_basis_reduce<<<S, kThreads, 0, st>>>(w->partial, ldp, nc, w->seg_chunk,
+				                                         w->active, w->r);
+				k_g_basis_subtract<<<grid, kThreads, 0, st>>>(v2, w->V, D, nc, w->r, ldp, w->chunks,
+				                                              nch, w->active, w->partial);
+				k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, w->active, nrm, 1);
+				k_g_scale<<<grid, kThreads, 0, st>>>(v2, v2, nrm, 1, w->chunks, nch, w->active);
+			}
+		}
+		if ((e = cudaGetLastError()))
+			return status(h, e, "group Lanczos launch");
+		if ((e = cudaMemcpyAsync(w->host, w->alpha, nsc * sizeof(double), cudaMemcpyDeviceToHost, st))
+		    || (e = cudaMemcpyAsync(w->host + nsc, w->beta, (nsc + size_t(S)) * sizeof(double),
+		                            cudaMemcpyDeviceToHost, st))
+		    || (e = cudaStreamSynchronize(st)))
+			return status(h, e, "group Lanczos steps");
+		if (h->err_host && *reinterpret_cast<volatile int*>(h->err_host))
+			return handle_fail(h, DMRGPP_TIMEOUT, "H*x kernel wait gave up during the group Lanczos");
+		const double* ah = w->host;
+		const double* bh = w->host + nsc;
+		bool          changed = false;
+		std::vector<double> d, off;
+		for (int s = 0; s < S; ++s) {
+			if (!act[size_t(s)])
+				continue;
+			// steps up to jend - 1 are done; test at the last one
+			const size_t jj   = jend - 1;
+			const size_t n    = jj + 1;
+			const size_t ne   = std::min(p->eigs_for_stop, n);
+			double       dmax = 0.0;
+			for (size_t rep = 0; rep < 2; ++rep) { // Ritz values at steps jj - 1 and jj
+				const size_t nn = rep == 0 ? n - 1 : n;
+				if (nn == 0)
+					continue;
+				d.resize(nn);
+				off.resize(nn);
+				for (size_t q = 0; q < nn; ++q) {
+					d[q]   = ah[q * size_t(S) + size_t(s)];
+					off[q] = bh[(q + 1) * size_t(S) + size_t(s)];
+				}
+				for (size_t k = 0; k < std::min(ne, nn); ++k) {
+					const double th = tridiag_kth_lowest(int(nn), d.data(), off.data(), int(k) + 1);
+					if (rep == 1)
+						dmax = std::max(dmax, std::fabs(th - eold[size_t(s) * p->eigs_for_stop + k]));
+					eold[size_t(s) * p->eigs_for_stop + k] = th;
+				}
+			}
+			const bool last = jj == maxn_s[size_t(s)] - 1;
+			if ((dmax < p->tolerance && jj >= p->min_steps) || last) {
+				j_stop[size_t(s)] = jj;
+				act[size_t(s)]    = 0;
+				--n_active;
+				changed = true;
+			}
+		}
+		if (changed
+		    && (e = cudaMemcpyAsync(w->active, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
+			return status(h, e, "update active sectors");
+		j = jend;
+	}
+	if (n_active > 0 || maxn == 1) { // no test point read the scalars back yet
+		if ((e = cudaMemcpy(w->host, w->alpha, nsc * sizeof(double), cudaMemcpyDeviceToHost))
+		    || (e = cudaMemcpy(w->host + nsc, w->beta, (nsc + size_t(S)) * sizeof(double), cudaMemcpyDeviceToHost)))
+			return status(h, e, "read alpha/beta");
+		for (int s = 0; s < S; ++s)
+			if (act[size_t(s)])
+				j_stop[size_t(s)] = maxn_s[size_t(s)] - 1;
+	}
+	{
+	}
+
+	// Ritz pairs per sector (LanczosSolver.h:76-84): lowest eigenvalue of the
+	// (j_stop + 1)-dimensional tridiagonal and its eigenvector
+	const double*       ah = w->host;
+	const double*       bh = w->host + nsc;
+	std::vector<double> coef(nsc, 0.0), d, off;
+	std::vector<int>    ncols(static_cast<size_t>(S));
+	for (int s = 0; s < S; ++s) {
+		const size_t n = j_stop[size_t(s)] + 1;
+		d.resize(n);
+		off.resize(n);
+		for (size_t q = 0; q < n; ++q) {
+			d[q]   = ah[q * size_t(S) + size_t(s)];
+			off[q] = bh[(q + 1) * size_t(S) + size_t(s)];
+		}
+		energies[s] = tridiag_kth_lowest(int(n), d.data(), off.data(), 1);
+		tridiag_inverse_iteration(int(n), d.data(), off.data(), energies[s],
+		                          coef.data() + size_t(s) * size_t(ldp));
+		ncols[size_t(s)] = int(n);
+		if (steps_taken)
+			steps_taken[s] = j_stop[size_t(s)];
+	}
+	if ((e = cudaMemcpyAsync(w->r, coef.data(), nsc * sizeof(double), cudaMemcpyHostToDevice, st))
+	    || (e = cudaMemcpyAsync(w->ncols, ncols.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
+		return status(h, e, "upload Ritz coefficients");
+	k_g_basis_combine<<<grid, kThreads, 0, st>>>(w->z, w->V, D, w->ncols, w->r, ldp, w->chunks, nch);
+	if ((e = cudaMemcpyAsync(z, w->z, D * sizeof(double),
+	                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st))
+	    || (e = cudaStreamSynchronize(st)))
+		return status(h, e, "Ritz vectors");
+	return DMRGPP_OK;
+}

@@ -8,10 +8,12 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 namespace dmrgpp {
 struct LanczosWork;  // device buffers of the eigensolvers, created on first use
 struct DavidsonWork;
+struct GroupWork;
 }
 
 struct dmrgpp_kron_s {
@@ -19,6 +21,7 @@ struct dmrgpp_kron_s {
 	cudaStream_t        stream     = nullptr;
 	int                 precision  = DMRGPP_FP64;
 	dmrgpp::KronPlan    plan;
+	std::vector<long long> sector_start; // offsets of the group's sectors in x (one sector: {0, dim})
 	double*             d_ops   = nullptr; // packed Bstack_j and A^T blocks
 	double*             d_bx    = nullptr; // pass-1 output (scratch)
 	double*             d_x     = nullptr; // staging for host-pointer applies
@@ -62,6 +65,7 @@ struct dmrgpp_kron_s {
 	dmrgpp::LanczosWork* lanczos = nullptr;
 	double*             d_diag = nullptr; // diagonal of H (patch order)
 	dmrgpp::DavidsonWork* davidson = nullptr;
+	dmrgpp::GroupWork*  group = nullptr;   // group Lanczos buffers (group_lanczos.cu)
 	std::string         err;
 };
 
@@ -70,9 +74,9 @@ namespace dmrgpp {
 // Enqueues y = H x on h->stream (device pointers); no synchronisation.
 int kron_apply_device(dmrgpp_kron_handle h, const double* x, double* y);
 
-// Builds and uploads the TF32x3 tensor-core form of the sector (the desc's
-// host tables are read again).
-int build_mixed(dmrgpp_kron_handle h, const dmrgpp_kron_desc* d);
+// Builds and uploads the TF32x3 tensor-core form of the sector from the
+// plan's host blocks (create time only).
+int build_mixed(dmrgpp_kron_handle h);
 
 // (Re)builds and uploads the persistent schedule of h for tile configuration
 // cfg (0..kNumTileCfgs-1), aiming at items_per_cta work items per CTA.
@@ -84,5 +88,6 @@ int handle_fail(dmrgpp_kron_handle h, int status, const std::string& msg);
 // Releases the eigensolver buffers of a handle (lanczos.cu).
 void release_lanczos(dmrgpp_kron_handle h);
 void release_davidson(dmrgpp_kron_handle h);
+void release_group(dmrgpp_kron_handle h);
 
 } // namespace dmrgpp

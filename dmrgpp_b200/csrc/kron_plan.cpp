@@ -5,6 +5,7 @@
 #include <climits>
 #include <cstring>
 #include <numeric>
+#include <tuple>
 #include <utility>
 
 namespace dmrgpp {
@@ -119,6 +120,31 @@ void build_tile_lists(KronPlan& plan, int bm, int bn)
 	order_tiles(plan.tile2, plan.seg2);
 }
 
+std::string collect_triples(size_t noperator, size_t np, const size_t* lsz, const size_t* rsz,
+                            const double* const* A, const size_t* ldA, const double* const* B,
+                            const size_t* ldB, int patch_offset, std::vector<Triple>& triples,
+                            std::vector<BlockRef>& blocks, double& f_alg)
+{
+	const size_t np2 = np * np;
+	for (size_t i = 0; i < np; ++i)
+		for (size_t j = 0; j < np; ++j)
+			for (size_t k = 0; k < noperator; ++k) {
+				const size_t t = i + j * np + k * np2;
+				if (!A[t] || !B[t])
+					continue;
+				if (ldA[t] < lsz[i] || ldB[t] < rsz[i])
+					return "leading dimension smaller than the block's rows at table entry "
+					    + std::to_string(t);
+				if (!has_nonzero(A[t], ldA[t], lsz[i], lsz[j])
+				    || !has_nonzero(B[t], ldB[t], rsz[i], rsz[j]))
+					continue;
+				triples.push_back({ int(i) + patch_offset, int(j) + patch_offset, int(k) });
+				blocks.push_back({ A[t], ldA[t], B[t], ldB[t] });
+				f_alg += 2.0 * double(rsz[i]) * double(lsz[j]) * (double(rsz[j]) + double(lsz[i]));
+			}
+	return std::string();
+}
+
 std::string build_kron_plan(size_t               noperator,
                             size_t               npatches,
                             const size_t*        lsz,
@@ -136,18 +162,39 @@ std::string build_kron_plan(size_t               noperator,
 		return "noperator and npatches must be >= 1";
 	if (!lsz || !rsz || !A || !ldA || !B || !ldB)
 		return "null table or size array";
+	for (size_t p = 0; p < npatches; ++p)
+		if (lsz[p] < 1 || rsz[p] < 1) // the reference asserts 1 <= size (setup_sparse_batch.cpp:70-71)
+			return "patch " + std::to_string(p) + " has an empty left or right group";
+	std::vector<Triple>   triples;
+	std::vector<BlockRef> blocks;
+	double                f_alg = 0.0;
+	std::string msg = collect_triples(noperator, npatches, lsz, rsz, A, ldA, B, ldB, 0, triples,
+	                                  blocks, f_alg);
+	if (!msg.empty())
+		return msg;
+	return build_kron_plan_triples(noperator, npatches, lsz, rsz, std::move(triples),
+	                               std::move(blocks), f_alg, bm, bn, plan, pack_host);
+}
+
+std::string build_kron_plan_triples(size_t noperator, size_t npatches, const size_t* lsz,
+                                    const size_t* rsz, std::vector<Triple> triples,
+                                    std::vector<BlockRef> blocks, double f_alg, int bm, int bn,
+                                    KronPlan& plan, std::vector<double>* pack_host)
+{
+	if (noperator == 0 || npatches == 0)
+		return "noperator and npatches must be >= 1";
+	if (triples.size() != blocks.size())
+		return "triples and blocks differ in length";
 	const size_t np = npatches;
-	const size_t np2 = np * np;
-	plan     = KronPlan();
-	plan.np  = np;
-	plan.nop = noperator;
-	plan.bm  = bm;
-	plan.bn  = bn;
+	plan            = KronPlan();
+	plan.np         = np;
+	plan.nop        = noperator;
+	plan.bm         = bm;
+	plan.bn         = bn;
 	plan.l.resize(np);
 	plan.r.resize(np);
 	plan.xy_start.assign(np + 1, 0);
 	for (size_t p = 0; p < np; ++p) {
-		// the reference asserts 1 <= size (setup_sparse_batch.cpp:70-71)
 		if (lsz[p] < 1 || rsz[p] < 1)
 			return "patch " + std::to_string(p) + " has an empty left or right group";
 		if (lsz[p] > INT_MAX / 64 || rsz[p] > INT_MAX / 64)
@@ -156,25 +203,20 @@ std::string build_kron_plan(size_t               noperator,
 		plan.r[p]            = (long long)rsz[p];
 		plan.xy_start[p + 1] = plan.xy_start[p] + plan.l[p] * plan.r[p];
 	}
-
-	// contributing triples (setup_nC.cpp:43-121): both blocks present and
-	// each with at least one nonzero entry
-	for (size_t i = 0; i < np; ++i)
-		for (size_t j = 0; j < np; ++j)
-			for (size_t k = 0; k < noperator; ++k) {
-				const size_t t = i + j * np + k * np2;
-				if (!A[t] || !B[t])
-					continue;
-				if (ldA[t] < lsz[i] || ldB[t] < rsz[i])
-					return "leading dimension smaller than the block's rows at table entry "
-					    + std::to_string(t);
-				if (!has_nonzero(A[t], ldA[t], lsz[i], lsz[j])
-				    || !has_nonzero(B[t], ldB[t], rsz[i], rsz[j]))
-					continue;
-				plan.triples.push_back({ int(i), int(j), int(k) });
-				plan.f_alg += 2.0 * double(rsz[i]) * double(lsz[j])
-				    * (double(rsz[j]) + double(lsz[i]));
-			}
+	for (size_t t = 0; t < triples.size(); ++t) {
+		const Triple& tr = triples[t];
+		if (tr.i < 0 || tr.j < 0 || size_t(tr.i) >= np || size_t(tr.j) >= np || tr.k < 0
+		    || size_t(tr.k) >= noperator)
+			return "triple " + std::to_string(t) + " out of range";
+		if (t > 0) {
+			const Triple& q = triples[t - 1];
+			if (std::make_tuple(q.i, q.j, q.k) >= std::make_tuple(tr.i, tr.j, tr.k))
+				return "triples not in (i,j,k) order";
+		}
+	}
+	plan.triples = std::move(triples);
+	plan.blocks  = std::move(blocks);
+	plan.f_alg   = f_alg;
 
 	const size_t nt = plan.triples.size();
 	// pass-1 row layout: for each input patch j the rows of (i,k) stacked in
@@ -217,21 +259,21 @@ std::string build_kron_plan(size_t               noperator,
 		double* P = pack_host->data();
 		for (size_t t = 0; t < nt; ++t) {
 			const Triple& tr = plan.triples[t];
-			const size_t  ix = size_t(tr.i) + size_t(tr.j) * np + size_t(tr.k) * np2;
+			const BlockRef& bl = plan.blocks[t];
 			// B_k(i,j) (r_i x r_j) into rows [row_off, row_off + r_i) of Bstack_j
 			const long long Mj = plan.M[tr.j];
 			double*         bs = P + plan.bstack_off[tr.j] + plan.row_off[t];
-			const double*   b  = B[ix];
+			const double*   b  = bl.B;
 			for (long long c = 0; c < plan.r[tr.j]; ++c)
 				for (long long q = 0; q < plan.r[tr.i]; ++q)
-					bs[q + c * Mj] = b[q + c * (long long)ldB[ix]];
+					bs[q + c * Mj] = b[q + c * (long long)bl.ldB];
 			// A_k(i,j)^T (l_j x l_i), leading dimension l_j
 			double*         at = P + plan.at_off[t];
-			const double*   a  = A[ix];
+			const double*   a  = bl.A;
 			const long long lj = plan.l[tr.j];
 			for (long long c = 0; c < plan.l[tr.i]; ++c)
 				for (long long q = 0; q < lj; ++q)
-					at[q + c * lj] = a[c + q * (long long)ldA[ix]];
+					at[q + c * lj] = a[c + q * (long long)bl.ldA];
 		}
 	}
 
@@ -395,21 +437,20 @@ void add_tc_tiles(std::vector<GemmTile>& tiles, long long c_off, long long ldc, 
 
 } // namespace
 
-void sector_diagonal(const KronPlan& plan, const double* const* A, const size_t* ldA,
-                     const double* const* B, const size_t* ldB, std::vector<double>& diag)
+void sector_diagonal(const KronPlan& plan, std::vector<double>& diag)
 {
-	const size_t np = plan.np, np2 = np * np;
 	diag.assign(size_t(plan.dim()), 0.0);
-	for (const Triple& tr : plan.triples) {
+	for (size_t t = 0; t < plan.triples.size(); ++t) {
+		const Triple& tr = plan.triples[t];
 		if (tr.i != tr.j)
 			continue;
-		const size_t    ix = size_t(tr.i) + size_t(tr.i) * np + size_t(tr.k) * np2;
+		const BlockRef& bl = plan.blocks[t];
 		const long long li = plan.l[tr.i], ri = plan.r[tr.i];
 		double*         d  = diag.data() + plan.xy_start[tr.i];
 		for (long long il = 0; il < li; ++il) {
-			const double a = A[ix][il + il * (long long)ldA[ix]];
+			const double a = bl.A[il + il * (long long)bl.ldA];
 			for (long long ir = 0; ir < ri; ++ir)
-				d[ir + il * ri] += a * B[ix][ir + ir * (long long)ldB[ix]];
+				d[ir + il * ri] += a * bl.B[ir + ir * (long long)bl.ldB];
 		}
 	}
 }
@@ -421,20 +462,13 @@ void split_tf32(double v, float* hi, float* lo)
 	*lo           = tf32_round(float(v - double(h)));
 }
 
-std::string build_mixed_plan(KronPlan&            plan,
-                             const double* const* A,
-                             const size_t*        ldA,
-                             const double* const* B,
-                             const size_t*        ldB,
-                             int                  bn,
-                             std::vector<float>*  ops_hi,
-                             std::vector<float>*  ops_lo,
-                             std::vector<int>*    x_map)
+std::string build_mixed_plan(KronPlan& plan, int bn, std::vector<float>* ops_hi,
+                             std::vector<float>* ops_lo, std::vector<int>* x_map)
 {
 	MixedPlan& mp   = plan.mixed;
 	mp              = MixedPlan();
 	mp.bn           = bn;
-	const size_t np = plan.np, nt = plan.triples.size(), np2 = np * np;
+	const size_t np = plan.np, nt = plan.triples.size();
 	// (i,k) groups of Bstack_j / BX_j, in triple order, each padded to 8 rows
 	mp.Mp.assign(np, 0);
 	mp.group_row.assign(nt, 0);
@@ -478,25 +512,25 @@ std::string build_mixed_plan(KronPlan&            plan,
 		float* H = ops_hi->data();
 		float* L = ops_lo->data();
 		for (size_t t = 0; t < nt; ++t) {
-			const Triple& tr = plan.triples[t];
-			const size_t  ix = size_t(tr.i) + size_t(tr.j) * np + size_t(tr.k) * np2;
+			const Triple&   tr = plan.triples[t];
+			const BlockRef& bl = plan.blocks[t];
 			// Bstack_j row (group_row + q), K index c: B_k(i,j)(q, c)
-			const double*   b  = B[ix];
+			const double*   b  = bl.B;
 			const long long Mj = mp.Mp[tr.j];
 			for (long long q = 0; q < plan.r[tr.i]; ++q) {
 				const long long row = mp.group_row[t] + q;
 				for (long long c = 0; c < plan.r[tr.j]; ++c) {
 					const long long o = mp.bs_off[tr.j] + chunked_offset(Mj, row, c);
-					split_tf32(b[q + c * (long long)ldB[ix]], H + o, L + o);
+					split_tf32(b[q + c * (long long)bl.ldB], H + o, L + o);
 				}
 			}
 			// A^T row n (< l_i), K index k (< l_j): A_k(i,j)(n, k)
-			const double*   a  = A[ix];
+			const double*   a  = bl.A;
 			const long long Ri = round8(plan.l[tr.i]);
 			for (long long n = 0; n < plan.l[tr.i]; ++n)
 				for (long long k = 0; k < plan.l[tr.j]; ++k) {
 					const long long o = mp.at_off[t] + chunked_offset(Ri, n, k);
-					split_tf32(a[n + k * (long long)ldA[ix]], H + o, L + o);
+					split_tf32(a[n + k * (long long)bl.ldA], H + o, L + o);
 				}
 		}
 	}

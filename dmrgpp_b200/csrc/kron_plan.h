@@ -74,6 +74,16 @@ struct Triple {
 	int i, j, k;
 };
 
+// Host blocks of one contributing triple: A_k(i,j) (l_i x l_j) and B_k(i,j)
+// (r_i x r_j), column-major with leading dimensions ldA, ldB.  Only valid
+// while the caller's tables are (during create).
+struct BlockRef {
+	const double* A;
+	size_t        ldA;
+	const double* B;
+	size_t        ldB;
+};
+
 // Layout of the mixed-precision (tensor-core) form of a sector.  Every
 // operand is a "chunked K-major" matrix: rows padded to a multiple of 8 (Rp),
 // K padded to a multiple of 32 with zeros, stored chunk by chunk (32 K values
@@ -118,6 +128,7 @@ struct KronPlan {
 	std::vector<long long> l, r;        // patch sizes
 	std::vector<long long> xy_start;    // np+1 offsets into X / Y
 	std::vector<Triple>    triples;     // contributing (i,j,k), (i,j,k) order
+	std::vector<BlockRef>  blocks;      // per triple: host blocks (create time only)
 	double                 f_alg = 0.0; // sum 2 r_i l_j (r_j + l_i)
 
 	// packed operator buffer (doubles)
@@ -165,25 +176,33 @@ std::string build_kron_plan(size_t               noperator,
                             KronPlan&            plan,
                             std::vector<double>* pack_host);
 
-// Builds plan.mixed for bn-wide tensor-core tiles.  When ops_hi/ops_lo are
-// given, packs the operators (hi and lo TF32 parts stored as floats); x_map
-// (optional, dim entries) receives, for each element of the sector vector,
-// its offset in the x split buffer.
-std::string build_mixed_plan(KronPlan&            plan,
-                             const double* const* A,
-                             const size_t*        ldA,
-                             const double* const* B,
-                             const size_t*        ldB,
-                             int                  bn,
-                             std::vector<float>*  ops_hi,
-                             std::vector<float>*  ops_lo,
-                             std::vector<int>*    x_map);
+// Appends the contributing triples of one plugin table (np patches, patch
+// indices shifted by patch_offset) to triples/blocks, in (i,j,k) order:
+// both blocks present and each with a nonzero entry (setup_nC.cpp:43-121).
+// f_alg accumulates sum 2 r_i l_j (r_j + l_i).  Returns an error or "".
+std::string collect_triples(size_t noperator, size_t np, const size_t* lsz, const size_t* rsz,
+                            const double* const* A, const size_t* ldA, const double* const* B,
+                            const size_t* ldB, int patch_offset, std::vector<Triple>& triples,
+                            std::vector<BlockRef>& blocks, double& f_alg);
+
+// Builds the plan from patch sizes and a triple list in (i,j,k) order (the
+// union of independent sectors is such a list with shifted patch indices).
+std::string build_kron_plan_triples(size_t noperator, size_t npatches, const size_t* lsz,
+                                    const size_t* rsz, std::vector<Triple> triples,
+                                    std::vector<BlockRef> blocks, double f_alg, int bm, int bn,
+                                    KronPlan& plan, std::vector<double>* pack_host);
+
+// Builds plan.mixed for bn-wide tensor-core tiles from plan.blocks.  When
+// ops_hi/ops_lo are given, packs the operators (hi and lo TF32 parts stored
+// as floats); x_map (optional, dim entries) receives, for each element of the
+// sector vector, its offset in the x split buffer.
+std::string build_mixed_plan(KronPlan& plan, int bn, std::vector<float>* ops_hi,
+                             std::vector<float>* ops_lo, std::vector<int>* x_map);
 
 // Diagonal of the sector's H in patch order: element (iR, iL) of patch i is
 // sum_k A_k(i,i)(iL,iL) * B_k(i,i)(iR,iR) over the contributing diagonal
-// triples (the input of diagonal preconditioners).
-void sector_diagonal(const KronPlan& plan, const double* const* A, const size_t* ldA,
-                     const double* const* B, const size_t* ldB, std::vector<double>& diag);
+// triples (the input of diagonal preconditioners); reads plan.blocks.
+void sector_diagonal(const KronPlan& plan, std::vector<double>& diag);
 
 // Splits v into a TF32 high part and a TF32 remainder (host side of the
 // operator packing; round to nearest, ties away from zero, like the

@@ -164,3 +164,128 @@ bool sym_eigen(int n, const double* a, double* w, double* v)
 }
 
 } // namespace dmrgpp
+
+namespace dmrgpp {
+
+namespace {
+
+// number of eigenvalues of T below x
+int sturm_count(int n, const double* d, const double* off, double x, double tiny)
+{
+	int    count = 0;
+	double q     = d[0] - x;
+	for (int i = 0;; ++i) {
+		if (q == 0.0)
+			q = -tiny;
+		if (q < 0.0)
+			++count;
+		if (i + 1 == n)
+			break;
+		q = d[i + 1] - x - off[i] * off[i] / q;
+	}
+	return count;
+}
+
+} // namespace
+
+double tridiag_kth_lowest(int n, const double* d, const double* off, int k)
+{
+	if (n <= 0)
+		return 0.0;
+	double lo = d[0], hi = d[0], scale = 0.0;
+	for (int i = 0; i < n; ++i) { // Gershgorin bounds
+		const double r = (i > 0 ? std::fabs(off[i - 1]) : 0.0) + (i + 1 < n ? std::fabs(off[i]) : 0.0);
+		lo             = std::min(lo, d[i] - r);
+		hi             = std::max(hi, d[i] + r);
+		scale          = std::max(scale, std::fabs(d[i]) + r);
+	}
+	const double tiny = std::max(scale, 1.0) * 1e-300;
+	lo -= 1e-14 * std::max(scale, 1.0);
+	hi += 1e-14 * std::max(scale, 1.0);
+	for (int it = 0; it < 400; ++it) {
+		const double mid = 0.5 * (lo + hi);
+		if (mid <= lo || mid >= hi)
+			break;
+		if (sturm_count(n, d, off, mid, tiny) >= k)
+			hi = mid;
+		else
+			lo = mid;
+	}
+	return 0.5 * (lo + hi);
+}
+
+void tridiag_inverse_iteration(int n, const double* d, const double* off, double theta, double* z)
+{
+	if (n == 1) {
+		z[0] = 1.0;
+		return;
+	}
+	double scale = 0.0;
+	for (int i = 0; i < n; ++i)
+		scale = std::max(scale, std::fabs(d[i] - theta) + (i + 1 < n ? std::fabs(off[i]) : 0.0));
+	const double tiny = std::max(scale, 1e-300) * 1e-15;
+	// LU of T - theta I with row interchanges: U row i = (u0, u1, u2) at
+	// columns i, i+1, i+2; the multipliers and swaps replay on the rhs
+	std::vector<double> u0(static_cast<size_t>(n)), u1(static_cast<size_t>(n), 0.0), u2(static_cast<size_t>(n), 0.0), m(static_cast<size_t>(n), 0.0);
+	std::vector<char>   sw(size_t(n), 0);
+	double              a = d[0] - theta, b = off[0];
+	for (int i = 0; i + 1 < n; ++i) {
+		const double l = off[i], dd = d[i + 1] - theta, u = i + 2 < n ? off[i + 1] : 0.0;
+		if (std::fabs(a) >= std::fabs(l)) {
+			if (a == 0.0)
+				a = tiny;
+			u0[size_t(i)] = a;
+			u1[size_t(i)] = b;
+			m[size_t(i)]  = l / a;
+			a             = dd - m[size_t(i)] * b;
+			b             = u;
+		} else {
+			u0[size_t(i)] = l;
+			u1[size_t(i)] = dd;
+			u2[size_t(i)] = u;
+			m[size_t(i)]  = a / l;
+			sw[size_t(i)] = 1;
+			const double na = b - m[size_t(i)] * dd;
+			b               = -m[size_t(i)] * u;
+			a               = na;
+		}
+	}
+	u0[size_t(n - 1)] = a == 0.0 ? tiny : a;
+	for (int i = 0; i < n; ++i)
+		z[i] = 1.0 / std::sqrt(double(n));
+	for (int iter = 0; iter < 3; ++iter) {
+		// forward: apply the swaps and multipliers to the rhs
+		for (int i = 0; i + 1 < n; ++i) {
+			if (sw[size_t(i)]) {
+				const double t = z[i];
+				z[i]           = z[i + 1];
+				z[i + 1]       = t - m[size_t(i)] * z[i + 1];
+			} else {
+				z[i + 1] -= m[size_t(i)] * z[i];
+			}
+		}
+		// back substitution
+		for (int i = n - 1; i >= 0; --i) {
+			double s = z[i];
+			if (i + 1 < n)
+				s -= u1[size_t(i)] * z[i + 1];
+			if (i + 2 < n)
+				s -= u2[size_t(i)] * z[i + 2];
+			z[i] = s / u0[size_t(i)];
+		}
+		double nrm = 0.0, big = 0.0;
+		int    arg = 0;
+		for (int i = 0; i < n; ++i) {
+			nrm += z[i] * z[i];
+			if (std::fabs(z[i]) > big) {
+				big = std::fabs(z[i]);
+				arg = i;
+			}
+		}
+		const double f = (z[arg] < 0.0 ? -1.0 : 1.0) / std::sqrt(nrm);
+		for (int i = 0; i < n; ++i)
+			z[i] *= f;
+	}
+}
+
+} // namespace dmrgpp

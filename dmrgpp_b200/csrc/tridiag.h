@@ -18,3 +18,17 @@ namespace dmrgpp {
 bool sym_eigen(int n, const double* a, double* w, double* v);
 
 } // namespace dmrgpp
+
+namespace dmrgpp {
+
+// k-th lowest eigenvalue (k >= 1) of the symmetric tridiagonal matrix
+// (diagonal d[0..n-1], off-diagonal off[0..n-2]) by bisection on Sturm
+// counts (the number of negative pivots of T - x I), to the last bit.
+double tridiag_kth_lowest(int n, const double* d, const double* off, int k);
+
+// Unit eigenvector z[0..n-1] for the eigenvalue theta of the same matrix by
+// inverse iteration (Gaussian elimination with partial pivoting of
+// T - theta I); the component of largest magnitude is made positive.
+void tridiag_inverse_iteration(int n, const double* d, const double* off, double theta, double* z);
+
+} // namespace dmrgpp

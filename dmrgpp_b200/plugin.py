@@ -94,6 +94,75 @@ class BatchedGemm:
         A, ldA, B, ldB = prob.tables()
         return cls(prob.noperator, prob.npatches, prob.lsz, prob.rsz, A, ldA, B, ldB, **kw)
 
+    @classmethod
+    def from_problems(cls, probs, precision: int = FP64, stream: Optional[int] = None,
+                      device: int = -1) -> "BatchedGemm":
+        """Many independent sectors in one handle (dmrgpp_kron_create_group):
+        H is block-diagonal over the sectors, one apply runs them all in one
+        launch on the concatenated vector; sector_offsets() gives the layout."""
+        L = _capi.lib()
+        tabs = []
+        for prob in probs:
+            A, ldA, B, ldB = prob.tables()
+            tabs.append(_DescTables(prob.noperator, prob.npatches, prob.lsz, prob.rsz, A, ldA,
+                                    B, ldB, precision, stream, device))
+        descs = (_capi.KronDesc * len(tabs))(*[t.desc for t in tabs])
+        h = ctypes.c_void_p()
+        _capi.check(L.dmrgpp_kron_create_group(descs, len(tabs), ctypes.byref(h)))
+        self = cls.__new__(cls)
+        self._h, self._lib = h, L
+        d = ctypes.c_size_t()
+        _capi.check(L.dmrgpp_kron_dim(h, ctypes.byref(d)), h)
+        self.dim = int(d.value)
+        f = ctypes.c_double()
+        _capi.check(L.dmrgpp_kron_flops(h, ctypes.byref(f)), h)
+        self.f_alg = float(f.value)
+        return self
+
+    def sector_offsets(self) -> np.ndarray:
+        """Start offsets of the handle's sectors in x (nsectors + 1 entries)."""
+        n = ctypes.c_size_t()
+        _capi.check(self._lib.dmrgpp_kron_group_sectors(self._h, ctypes.byref(n), None), self._h)
+        offs = np.zeros(n.value + 1, dtype=np.int64)
+        _capi.check(self._lib.dmrgpp_kron_group_sectors(
+            self._h, ctypes.byref(n), offs.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))),
+            self._h)
+        return offs
+
+    def lanczos_lowest_group(self, init, steps: int = 200, min_steps: int = 4,
+                             tolerance: float = 1e-12, eigs_for_stop: int = 1,
+                             reortho: bool = True, check_every: int = 8):
+        """Lowest eigenpair of every sector of a group handle, all sectors in
+        lockstep (dmrgpp_lanczos_lowest_group).  Returns (energies array,
+        concatenated Ritz vectors, steps array); numpy or torch CUDA like
+        lanczos_lowest."""
+        L = self._lib
+        p = _capi.LanczosParams()
+        L.dmrgpp_lanczos_params_init(ctypes.byref(p))
+        p.steps, p.min_steps, p.tolerance = steps, min_steps, tolerance
+        p.eigs_for_stop, p.reortho, p.check_every = eigs_for_stop, int(reortho), check_every
+        nsec = len(self.sector_offsets()) - 1
+        e = np.zeros(nsec)
+        n = np.zeros(nsec, dtype=np.uint64)
+        dp = ctypes.POINTER(ctypes.c_double)
+        szp = ctypes.POINTER(ctypes.c_size_t)
+        if hasattr(init, "data_ptr"):
+            import torch
+            z = torch.empty_like(init)
+            self._pointers(init, z)
+            rc = L.dmrgpp_lanczos_lowest_group(self._h, ctypes.byref(p), init.data_ptr(), 1,
+                                               e.ctypes.data_as(dp), z.data_ptr(),
+                                               n.ctypes.data_as(szp))
+        else:
+            init = np.ascontiguousarray(init, dtype=np.float64)
+            z = np.empty(self.dim)
+            self._pointers(init, z)
+            rc = L.dmrgpp_lanczos_lowest_group(self._h, ctypes.byref(p), init.ctypes.data, 0,
+                                               e.ctypes.data_as(dp), z.ctypes.data,
+                                               n.ctypes.data_as(szp))
+        _capi.check(rc, self._h)
+        return e, z, n.astype(np.int64)
+
     @property
     def handle(self):
         return self._h

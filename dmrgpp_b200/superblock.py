@@ -231,7 +231,7 @@ def random_unit_vector(dim: int, seed: int = 1) -> np.ndarray:
 
 
 def ladder_problem(total_states: int = 16000, sigma: float = 2.5, seed: int = 20261203,
-                   min_group: int = 1, name: str = "") -> KronProblem:
+                   min_group: int = 1, name: str = "", legs: int = 2) -> KronProblem:
     """Sector shaped like a two-leg Hubbard ladder superblock at m ~ 4000
     (left and right blocks of `total_states` states each, 4 states per site).
     Left groups are (N_up, N_down) pairs whose sizes follow a 2-D discretised
@@ -242,7 +242,8 @@ def ladder_problem(total_states: int = 16000, sigma: float = 2.5, seed: int = 20
     directions), each moving one particle of one spin across the boundary,
     so it couples patches whose (nu, nd) differ by one.  Blocks are dense
     N(0,1) (H_L, H_R symmetrised; the two directions are transposes), the
-    synthetic stand-in for operators of a real sweep."""
+    synthetic stand-in for operators of a real sweep.  legs=1 gives the
+    Hubbard-chain shape (K = 6: 4 hopping terms)."""
     rng = np.random.default_rng(seed)
     R = int(np.ceil(4 * sigma))
     qs = [(a, b) for a in range(-R, R + 1) for b in range(-R, R + 1)]
@@ -263,7 +264,7 @@ def ladder_problem(total_states: int = 16000, sigma: float = 2.5, seed: int = 20
         B[(p, p, 1)] = _sym(rng, r[p])
     k = 2
     for spin in range(2):
-        for leg in range(2):
+        for leg in range(legs):
             for p, (a, b) in enumerate(qs):
                 q_to = (a + 1, b) if spin == 0 else (a, b + 1)
                 if q_to not in index:
@@ -276,6 +277,48 @@ def ladder_problem(total_states: int = 16000, sigma: float = 2.5, seed: int = 20
                 A[(p, q, k + 1)] = np.asfortranarray(cd.T)
                 B[(p, q, k + 1)] = np.asfortranarray(c.T)
             k += 2
-    return KronProblem(l, r, 10, A, B,
-                       name=name or f"hubbard-ladder-like-{total_states}x{total_states}-"
-                                    f"{len(qs)}sec-K10")
+    K = 2 + 4 * legs
+    shape = "ladder" if legs == 2 else ("chain" if legs == 1 else f"{legs}leg")
+    return KronProblem(l, r, K, A, B,
+                       name=name or f"hubbard-{shape}-like-{total_states}x{total_states}-"
+                                    f"{len(qs)}sec-K{K}")
+
+
+def serving_batch(nproblems: int = 256, seed: int = 20261203):
+    """Independent superblock sectors shaped like a serving-style batch of
+    ground-state problems: Heisenberg and Hubbard chains (half each, seeded
+    coin) with L uniform in [16, 48], U uniform in [0, 8] for Hubbard and m
+    drawn from {64, 128, 256, 512}.  Heisenberg: left and right blocks of 2m
+    states in 2 round(sqrt(L/2)) + 1 Sz groups (discretised Gaussian), K = 5
+    (spin_chain_like).  Hubbard: blocks of 4m states in (N_up, N_down)
+    groups of width 1 + L/32, K = 6 (ladder_problem with one leg), with U
+    times a seeded double-occupancy count added to the diagonal of H_L and
+    H_R.  Seeded N(0,1) blocks stand in for the operators of real sweeps.
+    Returns the list of KronProblem and a list of dicts describing them."""
+    rng = np.random.default_rng(seed)
+    probs, meta = [], []
+    for q in range(nproblems):
+        L = int(rng.integers(16, 49))
+        m = int(rng.choice([64, 128, 256, 512]))
+        sub = int(rng.integers(0, 2**31 - 1))
+        if rng.random() < 0.5:
+            nsec = 2 * int(round(np.sqrt(L / 2))) + 1
+            sizes = gaussian_sector_sizes(2 * m, nsec, nsec / 5.0)
+            sizes = sizes[sizes > 0]
+            p = spin_chain_like(sizes, seed=sub, name=f"heisenberg-L{L}-m{m}")
+            meta.append({"model": "heisenberg", "L": L, "m": m})
+        else:
+            U = float(rng.uniform(0.0, 8.0))
+            p = ladder_problem(total_states=4 * m, sigma=1.0 + L / 32.0, seed=sub, legs=1,
+                               name=f"hubbard-L{L}-m{m}-U{U:.2f}")
+            r2 = np.random.default_rng(sub + 1)
+            for pi in range(p.npatches):
+                a = p.A[(pi, pi, 0)]
+                p.A[(pi, pi, 0)] = np.asfortranarray(
+                    a + U * np.diag(r2.integers(0, max(2, L // 4), a.shape[0]).astype(float)))
+                b = p.B[(pi, pi, 1)]
+                p.B[(pi, pi, 1)] = np.asfortranarray(
+                    b + U * np.diag(r2.integers(0, max(2, L // 4), b.shape[0]).astype(float)))
+            meta.append({"model": "hubbard", "L": L, "m": m, "U": U})
+        probs.append(p)
+    return probs, meta

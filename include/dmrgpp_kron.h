@@ -85,6 +85,21 @@ typedef struct {
  * the device and builds the launch schedule. */
 int dmrgpp_kron_create(const dmrgpp_kron_desc* desc, dmrgpp_kron_handle* out);
 
+/* Many independent sectors in one handle (no counterpart in the reference,
+ * whose plugin holds one sector): sector s keeps its own tables (descs[s],
+ * all with the same precision, device and stream), its patches follow those
+ * of sectors 0..s-1, and no block connects two sectors, so the group's H is
+ * block-diagonal.  One dmrgpp_kron_apply then applies every sector in one
+ * persistent launch to the concatenated vector x = [x_0; x_1; ...]; the
+ * eigensolvers treat the group as one sector, dmrgpp_lanczos_lowest_group
+ * solves every sector separately. */
+int dmrgpp_kron_create_group(const dmrgpp_kron_desc* descs, size_t nsectors,
+                             dmrgpp_kron_handle* out);
+
+/* Number of sectors of a handle (1 unless made by dmrgpp_kron_create_group)
+ * and, if offsets is not NULL, their nsectors + 1 start offsets in x. */
+int dmrgpp_kron_group_sectors(dmrgpp_kron_handle h, size_t* nsectors, long long* offsets);
+
 /* Replaces BatchedGemm<T>::~BatchedGemm (dmrg/GPUPlugin/BatchedGemm.cpp:72-79). */
 int dmrgpp_kron_destroy(dmrgpp_kron_handle h);
 
@@ -200,6 +215,21 @@ void dmrgpp_lanczos_params_init(dmrgpp_lanczos_params* p);
 int dmrgpp_lanczos_lowest(dmrgpp_kron_handle h, const dmrgpp_lanczos_params* p,
                           const double* init, int on_device, double* energy, double* z,
                           size_t* steps_taken);
+
+/* Lowest eigenpair of every sector of a group handle (dmrgpp_kron_create_group)
+ * by Lanczos, all sectors in lockstep: each step applies H to all sectors in
+ * one persistent launch, and every vector operation is segmented by sector.
+ * init and z are the concatenated sector vectors (device pointers when
+ * on_device, else host); energies[s] and steps_taken[s] (may be NULL) per
+ * sector.  Same recurrence and parameters as dmrgpp_lanczos_lowest; the
+ * stopping test runs every check_every steps (a sector stops at the first
+ * test point where its lowest eigs_for_stop Ritz values changed by less than
+ * the tolerance over the last step, after min_steps, or when its Krylov space
+ * is exhausted) and stopped sectors drop out of the vector work.  No
+ * counterpart in the reference.  Synchronous. */
+int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_lanczos_params* p,
+                                const double* init, int on_device, double* energies, double* z,
+                                size_t* steps_taken);
 
 /* ---- Davidson with a preconditioned correction (no counterpart in the
  * reference, whose only eigensolver for this path is Lanczos) ---- */

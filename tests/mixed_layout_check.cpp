@@ -6,6 +6,7 @@
 //     multiple of 16 bytes and lies inside its operand buffer;
 //   * copies that start on a 128-row tile row 0 start on an 8-row swizzle
 //     group, so the pre-swizzled rows land where the descriptor expects them;
+//   * the per-CTA tile runs (balance_tiles) are a permutation of the tiles;
 //   * the epilogue's stores stay inside their buffers;
 //   * pass 1 + pass 2 computed from these buffers (hi*hi + hi*lo + lo*hi in
 //     double, stale rows included as NaN) reproduce the FP64 H*x.
@@ -13,11 +14,13 @@
 // Prints "ok <max relative error>" or "FAIL <reason>" (exit code 1).
 #include "kron_plan.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <limits>
 #include <random>
+#include <tuple>
 #include <vector>
 
 using namespace dmrgpp;
@@ -86,9 +89,32 @@ int main(int argc, char** argv)
 		return fail(msg.c_str());
 	std::vector<float> ohi, olo;
 	std::vector<int>   xmap;
-	msg = build_mixed_plan(plan, A.data(), ldA.data(), B.data(), ldB.data(), bn, &ohi, &olo, &xmap);
+	msg = build_mixed_plan(plan, bn, &ohi, &olo, &xmap);
 	if (!msg.empty())
 		return fail(msg.c_str());
+	// per-CTA runs (balance_tiles): a permutation of the tiles, runs cover all
+	for (int pass_no = 0; pass_no < 2; ++pass_no) {
+		std::vector<GemmTile>&       tl   = pass_no ? plan.mixed.tile2 : plan.mixed.tile1;
+		const std::vector<GemmSeg>&  sg   = pass_no ? plan.mixed.seg2 : plan.mixed.seg1;
+		auto key = [](const GemmTile& t) { return std::make_tuple(t.c_off, t.m0, t.n0, t.seg_begin); };
+		std::vector<std::tuple<long long, int, int, int>> before, after;
+		for (const GemmTile& t : tl)
+			before.push_back(key(t));
+		std::vector<int> starts;
+		const int        G = balance_tiles(tl, sg, 7, starts);
+		if (G != std::min<int>(7, int(tl.size())) || int(starts.size()) != std::max(G, 1) + 1
+		    || starts.front() != 0 || starts.back() != int(tl.size()))
+			return fail("tile runs do not cover the tiles", G, long(starts.size()));
+		for (size_t b = 0; b + 1 < starts.size(); ++b)
+			if (starts[b] > starts[b + 1])
+				return fail("tile runs not ordered", long(b), 0);
+		for (const GemmTile& t : tl)
+			after.push_back(key(t));
+		std::sort(before.begin(), before.end());
+		std::sort(after.begin(), after.end());
+		if (before != after)
+			return fail("tile runs are not a permutation", pass_no, 0);
+	}
 	const MixedPlan& mp = plan.mixed;
 	const long long  D  = plan.dim();
 

@@ -92,6 +92,40 @@ def test_invalid_inputs_are_rejected_with_status(cuda_lib):
         plugin.BatchedGemm(1, 2, [1, 1], [1, 1], [None], [0], [None], [0])
 
 
+def test_group_create_rejects_bad_sector_lists(cuda_lib):
+    """dmrgpp_kron_create_group validates every sector before any device work."""
+    from dmrgpp_b200 import _capi
+    a, b = _desc_for(sb.random_problem(3, 2, seed=2)), _desc_for(sb.random_problem(2, 1, seed=3))
+    h = ctypes.c_void_p()
+    descs = (_capi.KronDesc * 2)(a.desc, b.desc)
+    assert cuda_lib.dmrgpp_kron_create_group(descs, 0, ctypes.byref(h)) == _capi.INVALID_ARG
+    assert cuda_lib.dmrgpp_kron_create_group(None, 2, ctypes.byref(h)) == _capi.INVALID_ARG
+    assert cuda_lib.dmrgpp_kron_create_group(descs, 2, None) == _capi.INVALID_ARG
+    descs[1].precision = 2                       # precisions differ
+    assert cuda_lib.dmrgpp_kron_create_group(descs, 2, ctypes.byref(h)) == _capi.INVALID_ARG
+    assert b"same precision" in cuda_lib.dmrgpp_kron_last_error(None)
+    bad = sb.random_problem(2, 1, seed=3)
+    bad.lsz = bad.lsz.copy()
+    bad.lsz[0] = 0
+    c = _desc_for(bad)
+    descs = (_capi.KronDesc * 2)(a.desc, c.desc)
+    assert cuda_lib.dmrgpp_kron_create_group(descs, 2, ctypes.byref(h)) == _capi.INVALID_ARG
+    assert b"sector 1" in cuda_lib.dmrgpp_kron_last_error(None) and not h.value
+
+
+def test_tridiagonal_helpers_of_the_group_solver(tmp_path):
+    """Sturm bisection and inverse iteration (tridiag.cpp) against the QL
+    solver on random, graded and nearly degenerate tridiagonals."""
+    import subprocess
+    exe = str(tmp_path / "tridiag_check")
+    csrc = os.path.join(ROOT, "dmrgpp_b200", "csrc")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I" + csrc,
+                    os.path.join(ROOT, "tests", "tridiag_check.cpp"),
+                    os.path.join(csrc, "tridiag.cpp"), "-o", exe], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and out.stdout.startswith("ok"), out.stdout
+
+
 def test_missing_library_fails_loudly(monkeypatch):
     from dmrgpp_b200 import _capi
     monkeypatch.setattr(_capi, "LIB_PATH", "/nonexistent/libdmrgpp_kron.so")

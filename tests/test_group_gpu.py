@@ -1,0 +1,100 @@
+"""Many independent sectors in one handle (dmrgpp_kron_create_group) and the
+lockstep group Lanczos (dmrgpp_lanczos_lowest_group), through the C ABI.
+
+H*x of a group is checked sector by sector against the oracle (1e-12, the
+FP64 bar); group Lanczos energies against the single-sector device Lanczos
+and, for small sectors, dense diagonalisation."""
+import numpy as np
+import pytest
+
+from dmrgpp_b200 import superblock as sb
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-12
+
+
+def rel_err(y, ref):
+    return float(np.abs(y - ref).max() / max(np.abs(ref).max(), 1e-300))
+
+
+def mixed_sectors():
+    return [sb.random_problem(npatches=5, noperator=3, max_size=40, seed=1, symmetric=True),
+            sb.c2_problem(seed=5),
+            sb.random_problem(npatches=1, noperator=1, max_size=1, seed=2, symmetric=True),
+            sb.ladder_problem(total_states=600, sigma=1.5, seed=3, legs=1),
+            sb.random_problem(npatches=3, noperator=2, max_size=2, min_size=1, seed=4,
+                              symmetric=True),
+            sb.spin_chain_like(sb.gaussian_sector_sizes(128, 7, 1.4), seed=6)]
+
+
+def test_group_apply_matches_oracle_per_sector(cuda_lib, cuda_device, oracle_built):
+    from dmrgpp_b200 import plugin
+    probs = mixed_sectors()
+    bg = plugin.BatchedGemm.from_problems(probs)
+    offs = bg.sector_offsets()
+    assert len(offs) == len(probs) + 1 and offs[-1] == bg.dim
+    assert abs(bg.f_alg - sum(p.flops() for p in probs)) < 1e-6 * bg.f_alg
+    x = np.random.default_rng(0).standard_normal(bg.dim)
+    y = bg(x)
+    for s, p in enumerate(probs):
+        xs = x[offs[s]:offs[s + 1]]
+        assert rel_err(y[offs[s]:offs[s + 1]], oracle_built.kron_apply(p, xs)) < RTOL, s
+    assert np.array_equal(bg(x), y)            # bitwise reproducible
+    bg.close()
+
+
+def test_group_lanczos_matches_single_sector_solves(cuda_lib, cuda_device):
+    from dmrgpp_b200 import plugin
+    probs = mixed_sectors()
+    bg = plugin.BatchedGemm.from_problems(probs)
+    offs = bg.sector_offsets()
+    init = np.random.default_rng(11).standard_normal(bg.dim)
+    e, z, steps = bg.lanczos_lowest_group(init, steps=200, tolerance=1e-12)
+    for s, p in enumerate(probs):
+        xs = init[offs[s]:offs[s + 1]]
+        single = plugin.BatchedGemm.from_problem(p)
+        e1, z1, n1 = single.lanczos_lowest(xs, steps=200, tolerance=1e-12)
+        single.close()
+        assert abs(e[s] - e1) <= 1e-11 * max(1.0, abs(e1)), (s, e[s], e1)
+        zs = z[offs[s]:offs[s + 1]]
+        assert abs(np.linalg.norm(zs) - 1.0) < 1e-10
+        assert 1.0 - abs(float(zs @ z1)) < 1e-8, s
+        if p.dim <= 2000:
+            exact = np.linalg.eigvalsh(p.dense())[0]
+            assert abs(e[s] - exact) <= 1e-11 * max(1.0, abs(exact)), (s, e[s], exact)
+        assert 0 <= steps[s] < max(p.dim, 1) and steps[s] <= 200
+    bg.close()
+
+
+def test_group_lanczos_device_vectors_and_one_sector_group(cuda_lib, cuda_device):
+    import torch
+    from dmrgpp_b200 import plugin
+    p = sb.c2_problem(seed=8)
+    g = plugin.BatchedGemm.from_problems([p])
+    assert list(g.sector_offsets()) == [0, p.dim]
+    init = torch.from_numpy(np.random.default_rng(3).standard_normal(p.dim)).cuda()
+    e, z, steps = g.lanczos_lowest_group(init, steps=200)
+    single = plugin.BatchedGemm.from_problem(p)
+    e1, z1, n1 = single.lanczos_lowest(init, steps=200)
+    assert isinstance(z, torch.Tensor) and z.is_cuda
+    assert abs(e[0] - e1) <= 1e-11 * abs(e1)
+    assert 1.0 - abs(float(torch.dot(z, z1))) < 1e-9
+    g.close()
+    single.close()
+
+
+def test_serving_batch_subset(cuda_lib, cuda_device):
+    """Eight problems of the serving-style batch: group energies equal the
+    single-problem FP64 solves."""
+    from dmrgpp_b200 import plugin
+    probs, meta = sb.serving_batch(8, seed=77)
+    bg = plugin.BatchedGemm.from_problems(probs)
+    offs = bg.sector_offsets()
+    init = np.random.default_rng(5).standard_normal(bg.dim)
+    e, z, steps = bg.lanczos_lowest_group(init)
+    for s, p in enumerate(probs):
+        single = plugin.BatchedGemm.from_problem(p)
+        e1, _, _ = single.lanczos_lowest(init[offs[s]:offs[s + 1]])
+        single.close()
+        assert abs(e[s] - e1) <= 1e-11 * max(1.0, abs(e1)), (meta[s], e[s], e1)
+    bg.close()

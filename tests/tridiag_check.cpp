@@ -1,0 +1,63 @@
+// Host check of the tridiagonal helpers of the group Lanczos (tridiag.cpp):
+// the k-th lowest eigenvalue by Sturm bisection against the QL solver, and
+// the inverse-iteration eigenvector's residual, on seeded random and
+// Lanczos-like (graded, nearly degenerate) tridiagonals.
+// Prints "ok <worst eigenvalue error> <worst residual>" or "FAIL ...".
+#include "tridiag.h"
+
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+int main()
+{
+	std::mt19937_64                        rng(99);
+	std::uniform_real_distribution<double> u(-1.0, 1.0);
+	double                                 worst_e = 0.0, worst_r = 0.0;
+	for (int trial = 0; trial < 400; ++trial) {
+		const int           n = 1 + trial % 120;
+		std::vector<double> d(static_cast<size_t>(n)), e(static_cast<size_t>(n), 0.0);
+		const int           kind = trial % 3;
+		for (int i = 0; i < n; ++i) {
+			d[size_t(i)] = kind == 0 ? u(rng) * 10.0 : -50.0 + 0.01 * u(rng);
+			e[size_t(i)] = kind == 2 ? 1e-9 * u(rng) : u(rng);
+		}
+		std::vector<double> w(d);
+		if (!dmrgpp::tridiag_eigen(n, w.data(), e.data(), nullptr)) {
+			std::printf("FAIL ql %d\n", trial);
+			return 1;
+		}
+		double scale = 1.0;
+		for (double x : w)
+			scale = std::max(scale, std::fabs(x));
+		for (int k = 1; k <= std::min(n, 3); ++k) {
+			const double th = dmrgpp::tridiag_kth_lowest(n, d.data(), e.data(), k);
+			worst_e         = std::max(worst_e, std::fabs(th - w[size_t(k - 1)]) / scale);
+		}
+		const double        th = dmrgpp::tridiag_kth_lowest(n, d.data(), e.data(), 1);
+		std::vector<double> z(static_cast<size_t>(n));
+		dmrgpp::tridiag_inverse_iteration(n, d.data(), e.data(), th, z.data());
+		double res = 0.0, nz = 0.0;
+		for (int i = 0; i < n; ++i) {
+			double t = d[size_t(i)] * z[size_t(i)] - th * z[size_t(i)];
+			if (i > 0)
+				t += e[size_t(i - 1)] * z[size_t(i - 1)];
+			if (i + 1 < n)
+				t += e[size_t(i)] * z[size_t(i + 1)];
+			res = std::max(res, std::fabs(t));
+			nz += z[size_t(i)] * z[size_t(i)];
+		}
+		if (std::fabs(nz - 1.0) > 1e-12) {
+			std::printf("FAIL norm %d %g\n", trial, nz);
+			return 1;
+		}
+		worst_r = std::max(worst_r, res / scale);
+	}
+	if (worst_e > 1e-13 || worst_r > 1e-12) {
+		std::printf("FAIL %g %g\n", worst_e, worst_r);
+		return 1;
+	}
+	std::printf("ok %.3e %.3e\n", worst_e, worst_r);
+	return 0;
+}
