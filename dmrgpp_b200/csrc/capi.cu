@@ -211,6 +211,8 @@ int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 	pa.arrive        = h->d_ctr + 3 + P.np;
 	pa.test_extra_wait = h->test_stall;
 	pa.error         = h->err_dev;
+	pa.item_sector   = h->d_item_sector;
+	pa.sector_active = h->sector_active;
 	pa.n_items       = int(P.items.size());
 	pa.np            = int(P.np);
 	pa.n_split_tiles = P.n_split_tiles;
@@ -322,6 +324,20 @@ int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 	add(P.items.data(), P.items.size() * sizeof(KronItem));
 	add(P.pseg2.data(), P.pseg2.size() * sizeof(GemmSeg));
 	add(P.n1_of_j.data(), P.n1_of_j.size() * sizeof(int));
+	// sector of every item (a pass-1 item: its input patch; pass 2: its output)
+	std::vector<int> item_sector(P.items.size(), 0);
+	if (h->sector_start.size() > 2) {
+		auto sector_of = [&](long long off) {
+			return int(std::upper_bound(h->sector_start.begin(), h->sector_start.end(), off)
+			           - h->sector_start.begin())
+			    - 1;
+		};
+		for (size_t q = 0; q < P.items.size(); ++q) {
+			const KronItem& w = P.items[q];
+			item_sector[q]    = w.kind == 0 ? sector_of(P.xy_start[size_t(w.producer)]) : sector_of(w.c_off);
+		}
+	}
+	add(item_sector.data(), item_sector.size() * sizeof(int));
 	cudaFree(h->d_lists);
 	cudaFree(h->d_ctr);
 	cudaFree(h->d_part);
@@ -338,6 +354,7 @@ int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 	h->d_items = reinterpret_cast<KronItem*>(at(4));
 	h->d_pseg2 = reinterpret_cast<GemmSeg*>(at(5));
 	h->d_n1    = reinterpret_cast<int*>(at(6));
+	h->d_item_sector = reinterpret_cast<int*>(at(7));
 	if (!lists.empty()
 	    && (e = cudaMemcpy(h->d_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
 		return cuda_fail(h, e, "upload lists");

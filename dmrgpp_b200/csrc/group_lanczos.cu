@@ -12,8 +12,9 @@
 // check_every steps: a sector stops at the first test point where its lowest
 // eigs_for_stop Ritz values changed by less than the tolerance over the last
 // step (after min_steps steps), or when its Krylov space is exhausted.  A
-// stopped sector is masked out of every later vector operation (its matvec
-// still runs inside the group launch).  No counterpart in the reference.
+// stopped sector is masked out of every later vector operation and out of
+// the group H*x (the persistent kernel drops its items).  No counterpart in
+// the reference.
 //
 // The sector vectors are cut into chunks of at most kChunk rows that never
 // cross a sector boundary; every kernel walks chunks, so each block knows its
@@ -145,14 +146,15 @@ k_g_update(double* __restrict__ v2, const double* __restrict__ v1, const double*
 	}
 }
 
-// partial[ch * ldp + c] = <V[:, c], v> over chunk ch, c < ncols (active sectors)
+// partial[ch * ldp + c] = <V[:, c], v> over chunk ch, c < ncols (active
+// sectors).  Chunks that start on an even row use 16-byte loads (ld even).
 __global__ void __launch_bounds__(kThreads)
 k_g_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* __restrict__ v,
                const Chunk* __restrict__ chunks, int nch, const int* __restrict__ active,
                double* __restrict__ partial, int ldp)
 {
-	__shared__ double vs[kChunk];
-	const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	__shared__ __align__(16) double vs[kChunk];
+	const int                       lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
 		const Chunk c = chunks[ch];
 		if (!active[c.seg])
@@ -161,18 +163,41 @@ k_g_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double*
 		for (int i = threadIdx.x; i < c.len; i += kThreads)
 			vs[i] = v[c.begin + i];
 		__syncthreads();
+		const bool vec = ((c.begin | static_cast<long long>(ld)) & 1) == 0;
 		for (int col = warp; col < ncols; col += kThreads / 32) {
 			const double* cp = V + size_t(col) * ld + c.begin;
 			double        s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-			int           i  = lane;
-			for (; i + 96 < c.len; i += 128) {
-				s0 += __ldg(cp + i) * vs[i];
-				s1 += __ldg(cp + i + 32) * vs[i + 32];
-				s2 += __ldg(cp + i + 64) * vs[i + 64];
-				s3 += __ldg(cp + i + 96) * vs[i + 96];
+			if (vec) {
+				const double2* c2 = reinterpret_cast<const double2*>(cp);
+				const double2* v2 = reinterpret_cast<const double2*>(vs);
+				const int      np = c.len >> 1;
+				int            q  = lane;
+				for (; q + 96 < np; q += 128) {
+					const double2 a0 = __ldg(c2 + q), a1 = __ldg(c2 + q + 32);
+					const double2 a2 = __ldg(c2 + q + 64), a3 = __ldg(c2 + q + 96);
+					const double2 b0 = v2[q], b1 = v2[q + 32], b2 = v2[q + 64], b3 = v2[q + 96];
+					s0 += a0.x * b0.x + a0.y * b0.y;
+					s1 += a1.x * b1.x + a1.y * b1.y;
+					s2 += a2.x * b2.x + a2.y * b2.y;
+					s3 += a3.x * b3.x + a3.y * b3.y;
+				}
+				for (; q < np; q += 32) {
+					const double2 a0 = __ldg(c2 + q), b0 = v2[q];
+					s0 += a0.x * b0.x + a0.y * b0.y;
+				}
+				if ((c.len & 1) && lane == 0)
+					s1 += __ldg(cp + c.len - 1) * vs[c.len - 1];
+			} else {
+				int i = lane;
+				for (; i + 96 < c.len; i += 128) {
+					s0 += __ldg(cp + i) * vs[i];
+					s1 += __ldg(cp + i + 32) * vs[i + 32];
+					s2 += __ldg(cp + i + 64) * vs[i + 64];
+					s3 += __ldg(cp + i + 96) * vs[i + 96];
+				}
+				for (; i < c.len; i += 32)
+					s0 += __ldg(cp + i) * vs[i];
 			}
-			for (; i < c.len; i += 32)
-				s0 += __ldg(cp + i) * vs[i];
 			double s = (s0 + s1) + (s2 + s3);
 			for (int o = 16; o > 0; o >>= 1)
 				s += __shfl_down_sync(0xffffffffu, s, o);
@@ -199,7 +224,8 @@ k_g_basis_reduce(const double* __restrict__ partial, int ldp, int ncols,
 	}
 }
 
-// v -= V[:, 0..ncols) r[sector]; partial[ch] = |v|^2 over ch
+// v -= V[:, 0..ncols) r[sector]; partial[ch] = |v|^2 over ch.  Chunks that
+// start on an even row: row pairs, 16-byte loads, 8 columns in flight.
 __global__ void __launch_bounds__(kThreads)
 k_g_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t ld, int ncols,
                    const double* __restrict__ r, int ldp, const Chunk* __restrict__ chunks, int nch,
@@ -215,24 +241,49 @@ k_g_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t 
 			for (int col = threadIdx.x; col < ncols; col += kThreads)
 				rs[col] = r[size_t(c.seg) * ldp + col];
 			__syncthreads();
-			for (int i = threadIdx.x; i < c.len; i += kThreads) {
-				const long long q = c.begin + i;
-				double          w = v[q];
-				int             col = 0;
-				for (; col + 4 <= ncols; col += 4) {
-					const double a0 = __ldg(V + size_t(col) * ld + q);
-					const double a1 = __ldg(V + size_t(col + 1) * ld + q);
-					const double a2 = __ldg(V + size_t(col + 2) * ld + q);
-					const double a3 = __ldg(V + size_t(col + 3) * ld + q);
-					w -= a0 * rs[col];
-					w -= a1 * rs[col + 1];
-					w -= a2 * rs[col + 2];
-					w -= a3 * rs[col + 3];
+			const bool vec = ((c.begin | static_cast<long long>(ld)) & 1) == 0;
+			if (vec) {
+				const int np = c.len >> 1;
+				double2*  v2 = reinterpret_cast<double2*>(v + c.begin);
+				for (int p = threadIdx.x; p < np; p += kThreads) {
+					double2 w   = v2[p];
+					int     col = 0;
+					for (; col + 8 <= ncols; col += 8) {
+						double2 a[8];
+#pragma unroll
+						for (int u = 0; u < 8; ++u)
+							a[u] = __ldg(reinterpret_cast<const double2*>(V + size_t(col + u) * ld + c.begin) + p);
+#pragma unroll
+						for (int u = 0; u < 8; ++u) {
+							w.x -= a[u].x * rs[col + u];
+							w.y -= a[u].y * rs[col + u];
+						}
+					}
+					for (; col < ncols; ++col) {
+						const double2 a = __ldg(reinterpret_cast<const double2*>(V + size_t(col) * ld + c.begin) + p);
+						w.x -= a.x * rs[col];
+						w.y -= a.y * rs[col];
+					}
+					v2[p] = w;
+					s += w.x * w.x + w.y * w.y;
 				}
-				for (; col < ncols; ++col)
-					w -= __ldg(V + size_t(col) * ld + q) * rs[col];
-				v[q] = w;
-				s += w * w;
+				if ((c.len & 1) && threadIdx.x == 0) {
+					const long long q = c.begin + c.len - 1;
+					double          w = v[q];
+					for (int col = 0; col < ncols; ++col)
+						w -= __ldg(V + size_t(col) * ld + q) * rs[col];
+					v[q] = w;
+					s += w * w;
+				}
+			} else {
+				for (int i = threadIdx.x; i < c.len; i += kThreads) {
+					const long long q   = c.begin + i;
+					double          w   = v[q];
+					for (int col = 0; col < ncols; ++col)
+						w -= __ldg(V + size_t(col) * ld + q) * rs[col];
+					v[q] = w;
+					s += w * w;
+				}
 			}
 		}
 		s = block_sum(s, red);
@@ -330,8 +381,14 @@ int ensure_group_work(dmrgpp_kron_handle h, int cols)
 	std::vector<Chunk> ch;
 	std::vector<int>   sc(1, 0);
 	for (int s = 0; s < nseg; ++s) {
-		for (long long b = h->sector_start[size_t(s)]; b < h->sector_start[size_t(s) + 1]; b += kChunk)
-			ch.push_back({ b, int(std::min<long long>(kChunk, h->sector_start[size_t(s) + 1] - b)), s });
+		// chunk boundaries on even offsets (16-byte aligned rows) after the first
+		const long long end = h->sector_start[size_t(s) + 1];
+		long long       b   = h->sector_start[size_t(s)];
+		while (b < end) {
+			const long long e = std::min(end, ((b + kChunk) / 2) * 2);
+			ch.push_back({ b, int(e - b), s });
+			b = e;
+		}
 		sc.push_back(int(ch.size()));
 	}
 	w->nch = int(ch.size());
@@ -410,6 +467,13 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 	auto               be  = [&](size_t j) { return w->beta + j * size_t(S); };
 	double*            nrm = w->scal;
 	cudaError_t        e;
+
+	// the group H*x skips stopped sectors while this solve runs
+	h->sector_active = w->active;
+	struct MaskOff {
+		dmrgpp_kron_handle h;
+		~MaskOff() { h->sector_active = nullptr; }
+	} mask_off { h };
 
 	std::vector<int> act(size_t(S), 1);
 	if ((e = cudaMemcpyAsync(w->active, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st))

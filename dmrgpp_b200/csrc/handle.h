@@ -39,6 +39,8 @@ struct dmrgpp_kron_s {
 	dmrgpp::KronItem*   d_items = nullptr;
 	dmrgpp::GemmSeg*    d_pseg2 = nullptr;
 	int*                d_n1    = nullptr;
+	int*                d_item_sector = nullptr; // per persistent item: its sector
+	const int*          sector_active = nullptr; // set by the group solver: skip stopped sectors
 	unsigned*           d_ctr   = nullptr; // work counters, done[np], arrive[split tiles]
 	double*             d_part  = nullptr; // split-K partial tiles
 	int*                err_host = nullptr; // mapped pinned word written by the kernel

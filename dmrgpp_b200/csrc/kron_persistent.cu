@@ -17,6 +17,9 @@
 //
 // Counters are returned to zero by the last CTA to leave, so consecutive
 // launches (and CUDA-graph replays) need no memset.
+//
+// Group handles (independent sectors in one launch) may pass a per-sector
+// active mask: the items of stopped sectors are claimed and dropped.
 #include "kron_persistent.cuh"
 #include "tile_dmma.cuh"
 
@@ -85,6 +88,14 @@ __global__ void __launch_bounds__(C::THREADS) kron_persistent_kernel(PersistentA
 		const int it = s_next;
 		if (it >= a.n_items)
 			break;
+		if (a.sector_active && !a.sector_active[a.item_sector[it]]) {
+			// a stopped sector of a group: no work, no counters (its pass-2
+			// items, the only waiters on its pass-1 items, are skipped too)
+			__syncthreads();
+			if (tid == 0)
+				s_next = int(gridDim.x + atomicAdd(&a.work_counter[0], 1u));
+			continue;
+		}
 		if (tid < kItemVec)
 			reinterpret_cast<int4*>(&s_w[0])[tid] = reinterpret_cast<const int4*>(a.items + it)[tid];
 		__syncthreads();

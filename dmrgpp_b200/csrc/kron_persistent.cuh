@@ -21,6 +21,8 @@ struct PersistentArgs {
 	unsigned*       done;         // per input patch: finished pass-1 tiles
 	unsigned*       arrive;       // per split tile: finished parts
 	int*            error;        // set to nonzero when a wait gave up
+	const int*      item_sector;   // per item: its sector (group handles)
+	const int*      sector_active; // NULL, or per sector: 0 = skip its items (y left as is)
 	int             n_items;
 	int             np;
 	int             n_split_tiles;
