@@ -40,6 +40,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true",
                    help="skip the ladder-sector solve and mixed-precision measurements")
+    p.add_argument("--no-serving", action="store_true",
+                   help="skip the 256-problem serving-batch measurements")
     return p.parse_args()
 
 
@@ -216,6 +218,87 @@ def read_traffic(workload):
     return float(m.group(1)) if m else None
 
 
+def serving_measurements(torch, dev, stream, cpu_sample: bool = True):
+    """Serving-style batch: 256 independent ground-state problems (Heisenberg
+    and Hubbard chain-shaped sectors, L in [16, 48], m in {64, 128, 256, 512},
+    superblock.serving_batch) solved together by the group Lanczos (one
+    persistent launch per step for all sectors, FP64, full
+    reorthogonalisation) against one FP64 device Lanczos per problem, with
+    per-problem |dE| between the two; the reference's own LanczosSolver +
+    BatchedGemmCpu (oracle/_ref) timed on a sample of the batch."""
+    from dmrgpp_b200 import plugin
+    from dmrgpp_b200 import superblock as sb
+    probs, meta = sb.serving_batch(256)
+    bg = plugin.BatchedGemm.from_problems(probs, stream=stream.cuda_stream)
+    offs = bg.sector_offsets()
+    init = torch.from_numpy(np.random.default_rng(1).standard_normal(bg.dim)).to(dev)
+    out = {"workload": "serving-batch-256 (Heisenberg / Hubbard chain-shaped sectors, "
+                       "L 16-48, m 64-512, seeded N(0,1) blocks)",
+           "problems": len(probs), "total_dim": int(bg.dim), "f_alg_per_group_matvec": bg.f_alg}
+    x, y = init.clone(), torch.empty_like(init)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            bg.apply_Htarget(x, y)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(10):
+            bg.apply_Htarget(x, y)
+        b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b) / 10
+    out["group_matvec"] = {"ms": ms, "tflops_alg": bg.f_alg / (ms * 1e-3) / 1e12}
+    bg.lanczos_lowest_group(init)                      # warm-up (allocations)
+    ts = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e, z, steps = bg.lanczos_lowest_group(init)
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    tg = min(ts)
+    out["group_lanczos"] = {"seconds": tg, "problems_per_s": len(probs) / tg,
+                            "steps_max": int(steps.max()), "steps_mean": float(steps.mean())}
+    bg.close()
+    es, t_seq = [], 0.0
+    for s, p in enumerate(probs):
+        h = plugin.BatchedGemm.from_problem(p, stream=stream.cuda_stream)
+        xs = init[offs[s]:offs[s + 1]].contiguous()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e1, _, _ = h.lanczos_lowest(xs)
+        t_seq += time.perf_counter() - t0
+        es.append(e1)
+        h.close()
+    es = np.array(es)
+    out["single_problem_lanczos"] = {"seconds": t_seq, "problems_per_s": len(probs) / t_seq,
+                                     "note": "one FP64 device Lanczos per problem, handle "
+                                             "creation excluded"}
+    out["max_abs_dE_vs_single_fp64"] = float(np.abs(es - e).max())
+    out["max_rel_dE_vs_single_fp64"] = float((np.abs(es - e) / np.abs(es)).max())
+    out["speedup_group_vs_single"] = t_seq / tg
+    if cpu_sample:
+        import oracle
+        if oracle.ref_available():
+            pick = [s for s, p in enumerate(probs) if p.dim <= 40000][:6]
+            t_cpu, rel = 0.0, 0.0
+            for s in pick:
+                rk = oracle.RefKron(probs[s])
+                xs = init[offs[s]:offs[s + 1]].cpu().numpy()
+                t0 = time.perf_counter()
+                e_ref, _, _ = rk.lanczos(xs, steps=200, min_steps=4, tolerance=1e-12, reortho=True)
+                t_cpu += time.perf_counter() - t0
+                rel = max(rel, abs(e_ref - e[s]) / abs(e_ref))
+                del rk
+            cores = int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
+            out["cpu_reference"] = {
+                "problems_per_s": len(pick) / t_cpu, "cores": cores, "kind": "reference",
+                "max_rel_dE_group_vs_reference": rel,
+                "sample": f"problems {pick} of the batch (dims "
+                          f"{[int(probs[s].dim) for s in pick]}): PsimagLite::LanczosSolver "
+                          "with Dmrg::BatchedGemmCpu, compiled from the reference sources"}
+    return out
+
+
 def ladder_measurements(torch, dev, stream):
     """Ladder-shaped sector (16000 x 16000 states, 241 (N_up, N_down) patches,
     K = 10, D = 3.37e6): the H*x throughput in FP64 and TF32x3, and one
@@ -344,9 +427,11 @@ def run_ours(args):
 
     peak = measured_fp64_peak(torch, dev) if rank == 0 else None
     bg.close()
-    sweep_step = None
+    sweep_step = serving = None
     if rank == 0 and world == 1 and not args.no_sweep:
         sweep_step = ladder_measurements(torch, dev, stream)
+    if rank == 0 and world == 1 and not args.no_serving:
+        serving = serving_measurements(torch, dev, stream, cpu_sample=not args.no_cpu_baseline)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -378,6 +463,8 @@ def run_ours(args):
     }
     if sweep_step is not None:
         line["sweep_step"] = sweep_step
+    if serving is not None:
+        line["serving"] = serving
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(prob, f_alg)
     print(json.dumps(line))
