@@ -1,0 +1,84 @@
+"""Whole two-site DMRG runs (oracle/dmrg_driver.py) whose every superblock
+eigensolve goes through the CUDA library, against the reference's published
+energies, the same runs with the reference's own solver (golden fixture),
+exact values, and FP64 vs mixed precision (TF32x3 Lanczos + FP64 refinement:
+|dE/site| <= 1e-9).  Real superblock sectors from these runs are also H*x
+parity cases."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import dmrg_driver as dd
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def gpu_solver(mixed=False, tolerance=1e-10):
+    import torch
+    from dmrgpp_b200 import plugin
+
+    def solve(prob, init):
+        bg = plugin.BatchedGemm.from_problem(prob,
+                                             precision=plugin.TF32X3 if mixed else plugin.FP64)
+        try:
+            if not mixed:
+                return bg.lanczos_lowest(init, steps=200, tolerance=tolerance)
+            x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
+            e1, z, n = bg.lanczos_lowest(x, steps=100, tolerance=1e-4)
+            e, st = bg.refine_lowest(z, max_outer=8, tolerance=1e-10, inner_iterations=60,
+                                     inner_tolerance=1e-5, raise_on_no_convergence=False)
+            return e, z.cpu().numpy(), n
+        finally:
+            bg.close()
+    return solve
+
+
+def test_heisenberg_L32_m128_matches_reference(cuda_lib, cuda_device):
+    g = json.load(open(os.path.join(GOLDEN, "dmrg_heisenberg_L32_m128.json")))
+    d = dd.DMRG(dd.Heisenberg(), L=32, m=128, solver=gpu_solver())
+    e = d.run(sweeps=2)
+    # the reference's own test of this chain (dmrg/CMakeLists.txt:343-344)
+    assert abs(e - g["reference_test_energy"]) < g["reference_test_tolerance"]
+    # the same run with the reference's LanczosSolver + BatchedGemmCpu
+    assert len(d.energies) == len(g["energies"])
+    assert abs(e - g["energy"]) < 1e-8
+    assert np.abs(np.array(d.energies) - np.array(g["energies"])).max() < 1e-6
+
+
+def test_hubbard_L8_U0_matches_reference(cuda_lib, cuda_device):
+    d = dd.DMRG(dd.Hubbard(U=0.0), L=8, m=256, solver=gpu_solver())
+    e = d.run(sweeps=1)
+    assert abs(e - (-9.51754)) < 1e-5          # dmrg/CMakeLists.txt:180-181
+    assert abs(e - dd.free_fermion_energy(8, 4, 4)) < 1e-9
+
+
+@pytest.mark.parametrize("model,L,m", [("heisenberg", 32, 128), ("hubbard", 12, 128)])
+def test_mixed_precision_dmrg_matches_fp64(cuda_lib, cuda_device, model, L, m):
+    mk = (lambda: dd.Heisenberg()) if model == "heisenberg" else (lambda: dd.Hubbard(U=4.0))
+    d64 = dd.DMRG(mk(), L=L, m=m, solver=gpu_solver())
+    e64 = d64.run(sweeps=1)
+    dmx = dd.DMRG(mk(), L=L, m=m, solver=gpu_solver(mixed=True))
+    emx = dmx.run(sweeps=1)
+    assert abs(emx - e64) / L <= 1e-9, (emx, e64)
+
+
+def test_real_superblock_sectors_parity(cuda_lib, cuda_device, oracle_built):
+    """Sectors of a Hubbard L=8 run: H*x of the CUDA FP64 path within 1e-12 of
+    the oracle, TF32x3 within 2e-5."""
+    from dmrgpp_b200 import plugin
+    d = dd.DMRG(dd.Hubbard(U=4.0), L=8, m=64, solver=dd.dense_solver())
+    d.keep_sectors = True
+    d.run(sweeps=1)
+    probs = sorted(d.sectors, key=lambda p: -p.dim)[:4] + d.sectors[:2]
+    for p in probs:
+        x = np.random.default_rng(p.dim).standard_normal(p.dim)
+        ref = oracle_built.kron_apply(p, x)
+        scale = max(np.abs(ref).max(), 1e-300)
+        for prec, tol in ((plugin.FP64, 1e-12), (plugin.TF32X3, 2e-5)):
+            bg = plugin.BatchedGemm.from_problem(p, precision=prec)
+            y = bg(x)
+            bg.close()
+            assert np.abs(y - ref).max() / scale < tol, (p.name, prec)
