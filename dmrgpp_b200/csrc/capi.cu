@@ -152,11 +152,11 @@ int handle_fail(dmrgpp_kron_handle h, int status, const std::string& msg)
 	return fail(h, status, msg);
 }
 
-int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
+int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const StepIO* io)
 {
 	const MixedPlan& mp = h->plan.mixed;
 	cudaError_t      e;
-	if ((e = tc_split_x(X, h->m_xmap, h->m_xs_hi, h->m_xs_lo, h->plan.dim(), h->stream)))
+	if ((e = tc_split_x(X, h->m_xmap, h->m_xs_hi, h->m_xs_lo, h->plan.dim(), h->stream, io)))
 		return cuda_fail(h, e, "x split launch");
 	TcArgs a1 {};
 	a1.A_hi   = h->m_ops_hi;
@@ -179,6 +179,7 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 	a2.B_hi   = h->m_ops_hi;
 	a2.B_lo   = h->m_ops_lo;
 	a2.Cd     = Y;
+	a2.io     = io;
 	a2.segs   = h->m_seg2;
 	a2.tiles  = h->m_tile2;
 	a2.ntiles = int(mp.tile2.size());
@@ -190,10 +191,10 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 	return DMRGPP_OK;
 }
 
-int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
+int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const StepIO* io)
 {
 	if (h->precision == DMRGPP_TF32X3)
-		return mixed_apply_device(h, X, Y);
+		return mixed_apply_device(h, X, Y, io);
 	const auto& P = h->plan;
 	cudaError_t e;
 	dmrgpp::PersistentArgs pa {};
@@ -213,6 +214,7 @@ int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y)
 	pa.error         = h->err_dev;
 	pa.item_sector   = h->d_item_sector;
 	pa.sector_active = h->sector_active;
+	pa.io            = io;
 	pa.n_items       = int(P.items.size());
 	pa.np            = int(P.np);
 	pa.n_split_tiles = P.n_split_tiles;

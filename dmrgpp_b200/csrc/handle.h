@@ -73,8 +73,11 @@ struct dmrgpp_kron_s {
 
 namespace dmrgpp {
 
-// Enqueues y = H x on h->stream (device pointers); no synchronisation.
-int kron_apply_device(dmrgpp_kron_handle h, const double* x, double* y);
+// Enqueues y = H x on h->stream (device pointers); no synchronisation.  With
+// io, the kernels read x and y from io on the device instead (for captured,
+// replayed solver steps).
+int kron_apply_device(dmrgpp_kron_handle h, const double* x, double* y,
+                      const dmrgpp::StepIO* io = nullptr);
 
 // Builds and uploads the TF32x3 tensor-core form of the sector from the
 // plan's host blocks (create time only).

@@ -71,6 +71,8 @@ __global__ void __launch_bounds__(C::THREADS) kron_persistent_kernel(PersistentA
 	__shared__ int                    s_last;
 	const int                         tid = threadIdx.x;
 	tile::Acc<C>                      acc;
+	const double*                     X   = a.io ? a.io->x : a.x;
+	double*                           Y   = a.io ? a.io->y : a.y;
 	constexpr int                     kSegWords = int(sizeof(GemmSeg) / sizeof(int));
 	constexpr int                     kItemVec  = int(sizeof(KronItem) / 16);
 	static_assert(sizeof(KronItem) % 16 == 0, "descriptor copy");
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(C::THREADS) kron_persistent_kernel(PersistentA
 		__syncthreads();
 
 		if (w.kind == 0) {
-			tile::mma_tile<C>(acc, smem, a.ops, a.x, s_seg, 0, nseg, w.m0, w.n0, w.M, w.N);
+			tile::mma_tile<C>(acc, smem, a.ops, X, s_seg, 0, nseg, w.m0, w.n0, w.M, w.N);
 			store_tile<C>(acc, a.bx + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
 			__syncthreads();
 			if (tid == 0) {
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(C::THREADS) kron_persistent_kernel(PersistentA
 			__syncthreads();
 			tile::mma_tile<C>(acc, smem, a.bx, a.ops, s_seg, 0, nseg, w.m0, w.n0, w.M, w.N);
 			if (w.kind == 1) {
-				store_tile<C>(acc, a.y + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
+				store_tile<C>(acc, Y + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
 			} else {
 				// split part: partial tile to its slot, the last part reduces
 				constexpr int TE   = C::BM * C::BN;
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(C::THREADS) kron_persistent_kernel(PersistentA
 				__syncthreads();
 				if (s_last) {
 					const double* slots = a.partial + (long long)w.slot * TE;
-					double*       Cp    = a.y + w.c_off;
+					double*       Cp    = Y + w.c_off;
 #pragma unroll
 					for (int mi = 0; mi < C::MI; ++mi)
 #pragma unroll

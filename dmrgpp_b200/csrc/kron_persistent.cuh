@@ -23,6 +23,7 @@ struct PersistentArgs {
 	int*            error;        // set to nonzero when a wait gave up
 	const int*      item_sector;   // per item: its sector (group handles)
 	const int*      sector_active; // NULL, or per sector: 0 = skip its items (y left as is)
+	const StepIO*   io;            // NULL, or x and y to read on the device (replaces x, y)
 	int             n_items;
 	int             np;
 	int             n_split_tiles;

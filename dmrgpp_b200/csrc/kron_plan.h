@@ -74,6 +74,13 @@ struct Triple {
 	int i, j, k;
 };
 
+// Input and output vector of an H*x whose operands are chosen on the device
+// (graph-replayed solver steps): the kernels read x and y from here at start.
+struct StepIO {
+	const double* x;
+	double*       y;
+};
+
 // Host blocks of one contributing triple: A_k(i,j) (l_i x l_j) and B_k(i,j)
 // (r_i x r_j), column-major with leading dimensions ldA, ldB.  Only valid
 // while the caller's tables are (during create).

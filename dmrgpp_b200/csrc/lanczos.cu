@@ -106,9 +106,8 @@ __device__ __forceinline__ void grid_sum(double block_value, double* partial, un
 }
 
 // *out = <x, y>
-__global__ void __launch_bounds__(kThreads)
-k_dot(const double* __restrict__ x, const double* __restrict__ y, size_t n, double* out,
-      double* partial, unsigned* ctr)
+__device__ __forceinline__ void dot_body(const double* __restrict__ x, const double* __restrict__ y,
+                                         size_t n, double* out, double* partial, unsigned* ctr)
 {
 	__shared__ double red[kThreads / 32];
 	double            s = 0.0;
@@ -117,6 +116,13 @@ k_dot(const double* __restrict__ x, const double* __restrict__ y, size_t n, doub
 		s += x[i] * y[i];
 	s = block_sum(s, red);
 	grid_sum(s, partial, ctr, out, false, red);
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_dot(const double* __restrict__ x, const double* __restrict__ y, size_t n, double* out,
+      double* partial, unsigned* ctr)
+{
+	dot_body(x, y, n, out, partial, ctr);
 }
 
 // dst = src / sqrt(*nrm2) (nrm2 = <src,src> from k_dot)
@@ -130,10 +136,10 @@ k_scale_rsqrt(const double* src, double* dst, size_t n, const double* nrm2)
 }
 
 // v2 = v2 - alpha*v1 - beta*v0 (v0 may be null); *beta_out = |v2|
-__global__ void __launch_bounds__(kThreads)
-k_lanczos_update(double* __restrict__ v2, const double* __restrict__ v1,
-                 const double* __restrict__ v0, size_t n, const double* alpha,
-                 const double* beta, double* beta_out, double* partial, unsigned* ctr)
+__device__ __forceinline__ void update_body(double* __restrict__ v2, const double* __restrict__ v1,
+                                            const double* __restrict__ v0, size_t n,
+                                            const double* alpha, const double* beta,
+                                            double* beta_out, double* partial, unsigned* ctr)
 {
 	__shared__ double red[kThreads / 32];
 	const double      a = *alpha;
@@ -151,8 +157,16 @@ k_lanczos_update(double* __restrict__ v2, const double* __restrict__ v1,
 	grid_sum(s, partial, ctr, beta_out, true, red);
 }
 
+__global__ void __launch_bounds__(kThreads)
+k_lanczos_update(double* __restrict__ v2, const double* __restrict__ v1,
+                 const double* __restrict__ v0, size_t n, const double* alpha,
+                 const double* beta, double* beta_out, double* partial, unsigned* ctr)
+{
+	update_body(v2, v1, v0, n, alpha, beta, beta_out, partial, ctr);
+}
+
 // v *= 1 / *s when *s > 0 (LanczosVectors.h:233-237)
-__global__ void __launch_bounds__(kThreads) k_scale_inv(double* v, size_t n, const double* s)
+__device__ __forceinline__ void scale_inv_body(double* v, size_t n, const double* s)
 {
 	const double d = *s;
 	if (!(d > 0.0))
@@ -163,6 +177,11 @@ __global__ void __launch_bounds__(kThreads) k_scale_inv(double* v, size_t n, con
 		v[i] *= a;
 }
 
+__global__ void __launch_bounds__(kThreads) k_scale_inv(double* v, size_t n, const double* s)
+{
+	scale_inv_body(v, n, s);
+}
+
 // Per-block partial projections partial[b][c] = <V[rows of b, c], v[rows of b]>
 // for c < ncols.  Block b takes the kDotChunk-row chunks b, b + grid, ...;
 // each chunk of v is staged in shared memory and every warp streams whole
@@ -170,9 +189,9 @@ __global__ void __launch_bounds__(kThreads) k_scale_inv(double* v, size_t n, con
 // 16-byte aligned and ld even), 8 loads in flight per lane.  The order of
 // every sum is fixed, so results are bitwise reproducible.
 template <bool VEC>
-__global__ void __launch_bounds__(kThreads, 4)
-k_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* __restrict__ v,
-             size_t n, double* __restrict__ partial)
+__device__ __forceinline__ void basis_dots_body(const double* __restrict__ V, size_t ld, int ncols,
+                                                const double* __restrict__ v, size_t n,
+                                                double* __restrict__ partial)
 {
 	__shared__ __align__(16) double vs[kDotChunk];
 	__shared__ double acc[kMaxCols];
@@ -224,10 +243,18 @@ k_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* _
 		partial[size_t(blockIdx.x) * kMaxCols + c] = acc[c];
 }
 
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads, 4)
+k_basis_dots(const double* __restrict__ V, size_t ld, int ncols, const double* __restrict__ v,
+             size_t n, double* __restrict__ partial)
+{
+	basis_dots_body<VEC>(V, ld, ncols, v, n, partial);
+}
+
 // r[c] = sum over blocks b < nblocks of partial[b][c], one block per column,
 // fixed order
-__global__ void __launch_bounds__(kThreads)
-k_reduce_cols(const double* __restrict__ partial, int nblocks, double* __restrict__ r)
+__device__ __forceinline__ void reduce_cols_body(const double* __restrict__ partial, int nblocks,
+                                                 double* __restrict__ r)
 {
 	__shared__ double red[kThreads / 32];
 	const int         c = blockIdx.x;
@@ -239,14 +266,20 @@ k_reduce_cols(const double* __restrict__ partial, int nblocks, double* __restric
 		r[c] = s;
 }
 
+__global__ void __launch_bounds__(kThreads)
+k_reduce_cols(const double* __restrict__ partial, int nblocks, double* __restrict__ r)
+{
+	reduce_cols_body(partial, nblocks, r);
+}
+
 // v -= V[:, 0..ncols) r ; *nrm_out = |v|.  VEC: each thread owns row pairs
 // (16-byte loads), 8 columns of loads issued before their updates; the
 // subtractions run in column order, as in the scalar form.
 template <bool VEC>
-__global__ void __launch_bounds__(kThreads)
-k_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t ld, int ncols,
-                 const double* __restrict__ r, size_t n, double* nrm_out, double* partial,
-                 unsigned* ctr)
+__device__ __forceinline__ void basis_subtract_body(double* __restrict__ v, const double* __restrict__ V,
+                                                    size_t ld, int ncols, const double* __restrict__ r,
+                                                    size_t n, double* nrm_out, double* partial,
+                                                    unsigned* ctr)
 {
 	__shared__ double rs[kMaxCols];
 	__shared__ double red[kThreads / 32];
@@ -300,6 +333,94 @@ k_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t ld
 	}
 	s = block_sum(s, red);
 	grid_sum(s, partial, ctr, nrm_out, true, red);
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads)
+k_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t ld, int ncols,
+                 const double* __restrict__ r, size_t n, double* nrm_out, double* partial,
+                 unsigned* ctr)
+{
+	basis_subtract_body<VEC>(v, V, ld, ncols, r, n, nrm_out, partial, ctr);
+}
+
+// ---- one Lanczos step with its columns chosen on the device, so that a
+// captured CUDA graph of check_every steps is replayed unchanged for the
+// whole solve.  k_step_advance moves the step record to the next j before
+// every step (LanczosVectors::oneStepDecomposition, LanczosVectors.h:203-241).
+struct LanczosStep {
+	StepIO  io;      // the step's H*x: x = V_j, y = V_{j+1}
+	double* v0;      // V_{j-1}
+	double* v1;      // V_j
+	double* v2;      // V_{j+1}
+	double* alpha_j;
+	double* beta_j;
+	double* beta_j1;
+	int     ncols;   // j + 1 stored vectors (reorthogonalisation)
+	int     j;
+};
+
+__global__ void k_step_set(LanczosStep* sp, int j) { sp->j = j; }
+
+__global__ void k_step_advance(LanczosStep* sp, double* V, size_t D, double* alpha, double* beta)
+{
+	const int j = sp->j + 1;
+	sp->j       = j;
+	sp->v0      = V + size_t(j - 1) * D;
+	sp->v1      = V + size_t(j) * D;
+	sp->v2      = V + size_t(j + 1) * D;
+	sp->io.x    = sp->v1;
+	sp->io.y    = sp->v2;
+	sp->alpha_j = alpha + j;
+	sp->beta_j  = beta + j;
+	sp->beta_j1 = beta + j + 1;
+	sp->ncols   = j + 1;
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_dot_step(const LanczosStep* sp, size_t n, double* partial, unsigned* ctr)
+{
+	dot_body(sp->v2, sp->v1, n, sp->alpha_j, partial, ctr);
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_update_step(const LanczosStep* sp, size_t n, double* partial, unsigned* ctr)
+{
+	update_body(sp->v2, sp->v1, sp->v0, n, sp->alpha_j, sp->beta_j, sp->beta_j1, partial, ctr);
+}
+
+// v2 *= 1 / *s (s = beta_{j+1} when null)
+__global__ void __launch_bounds__(kThreads)
+k_scale_inv_step(const LanczosStep* sp, size_t n, const double* s)
+{
+	scale_inv_body(sp->v2, n, s ? s : sp->beta_j1);
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads, 4)
+k_basis_dots_step(const LanczosStep* sp, const double* __restrict__ V, size_t ld, size_t n,
+                  double* __restrict__ partial)
+{
+	basis_dots_body<VEC>(V, ld, sp->ncols, sp->v2, n, partial);
+}
+
+// launched with the largest column count; blocks past the step's ncols exit
+__global__ void __launch_bounds__(kThreads)
+k_reduce_cols_step(const LanczosStep* sp, const double* __restrict__ partial, int nblocks,
+                   double* __restrict__ r)
+{
+	if (int(blockIdx.x) >= sp->ncols)
+		return;
+	reduce_cols_body(partial, nblocks, r);
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads)
+k_basis_subtract_step(const LanczosStep* sp, const double* __restrict__ V, size_t ld,
+                      const double* __restrict__ r, size_t n, double* nrm_out, double* partial,
+                      unsigned* ctr)
+{
+	basis_subtract_body<VEC>(sp->v2, V, ld, sp->ncols, r, n, nrm_out, partial, ctr);
 }
 
 // z = sum_c coef[c] V[:, c] (LanczosVectors::excitedVector, LanczosVectors.h:192-201)
@@ -426,6 +547,7 @@ struct LanczosWork {
 	double*   r       = nullptr; // projection coefficients / Ritz coefficients
 	unsigned* ctr     = nullptr; // arrival counters (one per reduction kernel)
 	double*   host    = nullptr; // pinned mirror of alpha/beta
+	void*     step    = nullptr; // LanczosStep record of graph-replayed steps
 };
 
 void release_lanczos(dmrgpp_kron_handle h)
@@ -438,6 +560,7 @@ void release_lanczos(dmrgpp_kron_handle h)
 	cudaFree(w->partial);
 	cudaFree(w->r);
 	cudaFree(w->ctr);
+	cudaFree(w->step);
 	if (w->host)
 		cudaFreeHost(w->host);
 	delete w;
@@ -477,8 +600,10 @@ int ensure_work(dmrgpp_kron_handle h, size_t dim, int cols)
 		return cuda_status(h, e, "clear counters");
 	if ((e = cudaMemset(w->scal, 0, (2 * size_t(cols) + 16) * sizeof(double))))
 		return cuda_status(h, e, "clear scalars");
-	if ((e = cudaHostAlloc(&w->host, (2 * size_t(cols) + 16) * sizeof(double), 0)))
+	if ((e = cudaHostAlloc(&w->host, 2 * (2 * size_t(cols) + 16) * sizeof(double), 0)))
 		return cuda_status(h, e, "cudaHostAlloc(scalars)");
+	if ((e = cudaMalloc(&w->step, sizeof(LanczosStep))))
+		return cuda_status(h, e, "cudaMalloc(step record)");
 	return DMRGPP_OK;
 }
 
@@ -499,6 +624,7 @@ void dmrgpp_lanczos_params_init(dmrgpp_lanczos_params* p)
 	p->tolerance     = 1e-12; // ParametersForSolver.h:103
 	p->reortho       = 1;     // Options=reortho
 	p->check_every   = 8;
+	p->use_graph     = 1;
 }
 
 int dmrgpp_tridiag_eigen(size_t n, const double* diag, const double* offdiag, double* eigs,
@@ -601,13 +727,99 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 	                                          w->partial, w->ctr + 2);
 	k_scale_inv<<<nb, kThreads, 0, st>>>(col(1), D, beta + 1);
 
-	std::vector<double> a_host, b_host(1, 0.0), eold(p->eigs_for_stop, 0.0), eigs;
-	size_t              j_stop = 0;
-	bool                done   = false;
-	size_t              j      = 1;
-	while (!done && j < maxn) {
-		const size_t jend = std::min(maxn, j + size_t(p->check_every));
-		for (size_t jj = j; jj < jend; ++jj) {
+	// graph-replayed steps: every kernel of a step reads its columns from the
+	// step record, so one captured graph of check_every steps serves the
+	// whole solve (same kernels and grids as the launches below: bitwise
+	// identical results)
+	LanczosStep* sp       = static_cast<LanczosStep*>(w->step);
+	const bool   vec      = vec2_ok(V, V + D, D);
+	const int    dgrid    = int(std::max<size_t>(1, std::min<size_t>((D + kDotChunk - 1) / kDotChunk, kDotGrid)));
+	const int    sgrid    = basis_blocks_for(D);
+	const bool   use_graph = p->use_graph != 0;
+	auto         enqueue_step = [&](cudaStream_t s) -> int {
+		k_step_advance<<<1, 1, 0, s>>>(sp, V, D, alpha, beta);
+		if (int rc = kron_apply_device(h, nullptr, nullptr, &sp->io))
+			return rc;
+		k_dot_step<<<nb, kThreads, 0, s>>>(sp, D, w->partial, w->ctr + 1);
+		k_update_step<<<nb, kThreads, 0, s>>>(sp, D, w->partial, w->ctr + 2);
+		k_scale_inv_step<<<nb, kThreads, 0, s>>>(sp, D, nullptr);
+		if (p->reortho) {
+			if (vec) {
+				k_basis_dots_step<true><<<dgrid, kThreads, 0, s>>>(sp, V, D, D, w->partial);
+			} else {
+				k_basis_dots_step<false><<<dgrid, kThreads, 0, s>>>(sp, V, D, D, w->partial);
+			}
+			k_reduce_cols_step<<<w->cols, kThreads, 0, s>>>(sp, w->partial, dgrid, w->r);
+			if (vec) {
+				k_basis_subtract_step<true><<<sgrid, kThreads, 0, s>>>(sp, V, D, w->r, D, work + 1,
+				                                                      w->partial, w->ctr + 4);
+			} else {
+				k_basis_subtract_step<false><<<sgrid, kThreads, 0, s>>>(sp, V, D, w->r, D, work + 1,
+				                                                       w->partial, w->ctr + 4);
+			}
+			k_scale_inv_step<<<nb, kThreads, 0, s>>>(sp, D, work + 1);
+		}
+		return DMRGPP_OK;
+	};
+	struct Graph {
+		cudaGraph_t     g = nullptr;
+		cudaGraphExec_t x = nullptr;
+		~Graph()
+		{
+			if (x)
+				cudaGraphExecDestroy(x);
+			if (g)
+				cudaGraphDestroy(g);
+		}
+	} graph;
+	// capture check_every steps on a private stream (the handle's stream may
+	// be the legacy default stream, which cannot be captured)
+	auto capture = [&]() -> int {
+		cudaStream_t cs = nullptr;
+		if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)))
+			return cuda_status(h, e, "capture stream");
+		const cudaStream_t saved = h->stream;
+		h->stream                = cs;
+		int rc                   = DMRGPP_OK;
+		e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+		if (e == cudaSuccess) {
+			for (int q = 0; q < p->check_every && rc == DMRGPP_OK; ++q)
+				rc = enqueue_step(cs);
+			const cudaError_t e2 = cudaStreamEndCapture(cs, &graph.g);
+			if (rc == DMRGPP_OK && e2 != cudaSuccess)
+				rc = cuda_status(h, e2, "end of graph capture");
+		} else {
+			rc = cuda_status(h, e, "graph capture");
+		}
+		h->stream = saved;
+		cudaStreamDestroy(cs);
+		if (rc == DMRGPP_OK && (e = cudaGraphInstantiate(&graph.x, graph.g, 0)))
+			rc = cuda_status(h, e, "graph instantiation");
+		return rc;
+	};
+	if (use_graph)
+		k_step_set<<<1, 1, 0, st>>>(sp, 0); // the first step is j = 1
+
+	// Groups of check_every steps are enqueued one group ahead of the host's
+	// stopping test (two pinned copies of alpha/beta alternate), so the GPU
+	// runs the next group while the host tests the last one; steps past the
+	// stopping point are discarded, as in the one-group-at-a-time form.
+	auto enqueue_group = [&](size_t j0, size_t j1) -> int {
+		if (use_graph) {
+			if (j1 - j0 == size_t(p->check_every)) {
+				if (!graph.x)
+					if (int rc = capture())
+						return rc;
+				if ((e = cudaGraphLaunch(graph.x, st)))
+					return cuda_status(h, e, "graph launch");
+			} else {
+				for (size_t jj = j0; jj < j1; ++jj)
+					if (int rc = enqueue_step(st))
+						return rc;
+			}
+			return DMRGPP_OK;
+		}
+		for (size_t jj = j0; jj < j1; ++jj) {
 			// oneStepDecomposition (LanczosVectors.h:203-241), V2 lives in column jj+1
 			double* v0 = col(jj - 1);
 			double* v1 = col(jj);
@@ -625,29 +837,72 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 				k_scale_inv<<<nb, kThreads, 0, st>>>(v2, D, work + 1);
 			}
 		}
-		if ((e = cudaGetLastError()))
-			return cuda_status(h, e, "Lanczos step launch");
-		// alpha[0..jend) and beta[0..jend] back to the host
-		if ((e = cudaMemcpyAsync(w->host, w->scal, 2 * size_t(w->cols) * sizeof(double),
-		                         cudaMemcpyDeviceToHost, st)))
-			return cuda_status(h, e, "read alpha/beta");
-		if ((e = cudaStreamSynchronize(st)))
+		return DMRGPP_OK;
+	};
+	struct Events {
+		cudaEvent_t ev[2] = { nullptr, nullptr };
+		~Events()
+		{
+			for (cudaEvent_t x : ev)
+				if (x)
+					cudaEventDestroy(x);
+		}
+	} events;
+	for (int b = 0; b < 2; ++b)
+		if ((e = cudaEventCreateWithFlags(&events.ev[b], cudaEventDisableTiming)))
+			return cuda_status(h, e, "events");
+	const size_t host_stride = 2 * size_t(w->cols) + 16;
+	struct Group {
+		size_t j0, j1;
+		int    buf;
+	};
+	std::vector<Group> inflight;
+	std::vector<double> eold(p->eigs_for_stop, 0.0), dd, ee;
+	size_t              j_stop = 0;
+	bool                done   = false;
+	size_t              next   = 1;
+	int                 buf    = 0;
+	const double*       hb     = w->host; // alpha/beta of the last tested group
+	while (!done) {
+		while (inflight.size() < 2 && next < maxn) {
+			const size_t jend = std::min(maxn, next + size_t(p->check_every));
+			if (int rc = enqueue_group(next, jend))
+				return rc;
+			if ((e = cudaGetLastError()))
+				return cuda_status(h, e, "Lanczos step launch");
+			// alpha[0..jend) and beta[0..jend] back to the host
+			double* hbuf = w->host + size_t(buf) * host_stride;
+			if ((e = cudaMemcpyAsync(hbuf, w->scal, 2 * size_t(w->cols) * sizeof(double),
+			                         cudaMemcpyDeviceToHost, st))
+			    || (e = cudaEventRecord(events.ev[buf], st)))
+				return cuda_status(h, e, "read alpha/beta");
+			inflight.push_back({ next, jend, buf });
+			next = jend;
+			buf ^= 1;
+		}
+		if (inflight.empty())
+			break;
+		const Group g = inflight.front();
+		inflight.erase(inflight.begin());
+		if ((e = cudaEventSynchronize(events.ev[g.buf])))
 			return cuda_status(h, e, "Lanczos steps");
 		if (h->err_host && *reinterpret_cast<volatile int*>(h->err_host))
 			return handle_fail(h, DMRGPP_TIMEOUT, "H*x kernel wait gave up during Lanczos");
-		const double* ah = w->host;
-		const double* bh = w->host + w->cols;
-		// stopping test per step, in order (LanczosCore.h:215-240)
-		for (size_t jj = j; jj < jend; ++jj) {
+		hb               = w->host + size_t(g.buf) * host_stride;
+		const double* ah = hb;
+		const double* bh = hb + w->cols;
+		// stopping test per step, in order (LanczosCore.h:215-240); the
+		// lowest Ritz values by Sturm bisection of the step's tridiagonal
+		for (size_t jj = g.j0; jj < g.j1; ++jj) {
 			const size_t n = jj + 1;
-			std::vector<double> d(ah, ah + n), off(bh + 1, bh + n);
-			if (!tridiag_eigen(int(n), d.data(), off.data(), nullptr))
-				return handle_fail(h, DMRGPP_NOT_CONVERGED, "tridiagonal eigensolve failed");
+			dd.assign(ah, ah + n);
+			ee.assign(bh + 1, bh + n);
 			const size_t ne   = std::min(p->eigs_for_stop, n);
 			double       dmax = 0.0;
 			for (size_t k = 0; k < ne; ++k) {
-				dmax    = std::max(dmax, std::fabs(d[k] - eold[k]));
-				eold[k] = d[k];
+				const double th = tridiag_kth_lowest(int(n), dd.data(), ee.data(), int(k) + 1);
+				dmax            = std::max(dmax, std::fabs(th - eold[k]));
+				eold[k]         = th;
 			}
 			bool exit_flag = dmax < p->tolerance || jj == maxn - 1;
 			if ((exit_flag && D <= 4) || (exit_flag && jj >= p->min_steps)) {
@@ -656,7 +911,6 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 				break;
 			}
 		}
-		j = jend;
 	}
 	if (!done)
 		j_stop = maxn - 1;
@@ -665,8 +919,7 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 
 	// Ritz vector of the (j_stop+1)-dimensional tridiagonal (LanczosSolver.h:76-84)
 	const size_t        n = j_stop + 1;
-	std::vector<double> d(w->host, w->host + n), off(w->host + w->cols + 1, w->host + w->cols + n),
-	    zt(n * n);
+	std::vector<double> d(hb, hb + n), off(hb + w->cols + 1, hb + w->cols + n), zt(n * n);
 	if (maxn == 1) { // no loop ran: alpha[0] has not been read back yet
 		if ((e = cudaMemcpy(w->host, w->scal, sizeof(double), cudaMemcpyDeviceToHost)))
 			return cuda_status(h, e, "read alpha");

@@ -321,7 +321,7 @@ __device__ __forceinline__ void store_chunk(const TcArgs& a, const GemmTile& t, 
 			*reinterpret_cast<float4*>(lo + pos) = make_float4(lv[0], lv[1], lv[2], lv[3]);
 		}
 	} else {
-		double* y = a.Cd + t.c_off;
+		double* y = (a.io ? a.io->y : a.Cd) + t.c_off;
 #pragma unroll
 		for (int i = 0; i < 32; ++i) {
 			const int gcol = col0 + i;
@@ -435,9 +435,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_tf32x3_kernel(TcArgs a)
 
 // x (FP64, patch order) -> TF32 hi/lo parts in the chunked layout
 __global__ void __launch_bounds__(256)
-split_x_kernel(const double* __restrict__ x, const int* __restrict__ map, float* __restrict__ hi,
-               float* __restrict__ lo, long long n)
+split_x_kernel(const double* __restrict__ xin, const int* __restrict__ map, float* __restrict__ hi,
+               float* __restrict__ lo, long long n, const StepIO* io)
 {
+	const double* x = io ? io->x : xin;
 	for (long long e = blockIdx.x * 256LL + threadIdx.x; e < n; e += 256LL * gridDim.x) {
 		const double v = x[e];
 		const float  h = tf32_rna(float(v));
@@ -504,14 +505,14 @@ cudaError_t tc_launch(const TcArgs& a, int bn, bool pass1, cudaStream_t stream)
 }
 
 cudaError_t tc_split_x(const double* x, const int* map, float* hi, float* lo, long long n,
-                       cudaStream_t stream)
+                       cudaStream_t stream, const StepIO* io)
 {
 	if (n <= 0)
 		return cudaSuccess;
 	long long blocks = (n + 255) / 256;
 	if (blocks > 148 * 8)
 		blocks = 148 * 8;
-	split_x_kernel<<<int(blocks), 256, 0, stream>>>(x, map, hi, lo, n);
+	split_x_kernel<<<int(blocks), 256, 0, stream>>>(x, map, hi, lo, n, io);
 	return cudaGetLastError();
 }
 

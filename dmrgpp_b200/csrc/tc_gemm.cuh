@@ -21,6 +21,7 @@ struct TcArgs {
 	int             ntiles;
 	int             grid;   // persistent CTAs, at most one per SM
 	int*            error; // set to 2 when an mbarrier wait gave up
+	const StepIO*   io;    // NULL, or pass 2 writes io->y instead of Cd
 };
 
 // Kernel attributes on the current device; call once per device.
@@ -30,8 +31,8 @@ cudaError_t tc_init();
 // a.grid persistent CTAs.
 cudaError_t tc_launch(const TcArgs& a, int bn, bool pass1, cudaStream_t stream);
 
-// x (patch order, FP64) -> TF32 hi/lo parts at map[e].
+// x (patch order, FP64; io->x instead when io is given) -> TF32 hi/lo parts at map[e].
 cudaError_t tc_split_x(const double* x, const int* map, float* hi, float* lo, long long n,
-                       cudaStream_t stream);
+                       cudaStream_t stream, const StepIO* io = nullptr);
 
 } // namespace dmrgpp

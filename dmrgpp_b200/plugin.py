@@ -198,7 +198,7 @@ class BatchedGemm:
 
     def lanczos_lowest(self, init, steps: int = 200, min_steps: int = 4,
                        tolerance: float = 1e-12, eigs_for_stop: int = 1, reortho: bool = True,
-                       check_every: int = 8):
+                       check_every: int = 8, use_graph: bool = True):
         """Lowest eigenpair by the device Lanczos (the reference's
         LanczosSolver::computeAllStatesBelow for one state).  Returns
         (energy, ritz_vector, steps).  numpy init -> numpy vector; a torch
@@ -208,6 +208,7 @@ class BatchedGemm:
         L.dmrgpp_lanczos_params_init(ctypes.byref(p))
         p.steps, p.min_steps, p.tolerance = steps, min_steps, tolerance
         p.eigs_for_stop, p.reortho, p.check_every = eigs_for_stop, int(reortho), check_every
+        p.use_graph = int(use_graph)
         e = ctypes.c_double()
         n = ctypes.c_size_t()
         if hasattr(init, "data_ptr"):

@@ -202,6 +202,10 @@ typedef struct {
 	double tolerance;     /* LanczosEps: stop when they change by less (default 1e-12) */
 	int    reortho;       /* full reorthogonalisation, Options=reortho (default 1) */
 	int    check_every;   /* steps enqueued between stopping tests on the host (default 8) */
+	int    use_graph;     /* 1 (default): the steps between two tests run as one CUDA graph,
+	                         captured once per solve and replayed (the kernels choose their
+	                         Lanczos columns on the device); 0: launched one by one.  Results
+	                         are bitwise identical. */
 } dmrgpp_lanczos_params;
 
 /* Fills the reference's defaults (ParametersForSolver.h:93-120). */

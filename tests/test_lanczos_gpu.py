@@ -78,3 +78,22 @@ def test_gather_scatter_round_trip(cuda_lib, cuda_device):
     torch.cuda.synchronize()
     assert torch.equal(mid, src[idx])
     assert torch.equal(back, src)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "tf32x3"])
+def test_graph_replayed_steps_are_bitwise_identical(cuda_lib, cuda_device, prec):
+    """The CUDA-graph form of the solve (one captured graph of check_every
+    steps, replayed) gives exactly the launch-by-launch result, including a
+    final partial group of steps launched directly."""
+    import torch
+    from dmrgpp_b200 import plugin
+    prob = sb.c2_problem(seed=21)
+    bg = plugin.BatchedGemm.from_problem(
+        prob, precision=plugin.TF32X3 if prec == "tf32x3" else plugin.FP64)
+    init = torch.from_numpy(np.random.default_rng(4).standard_normal(prob.dim)).cuda()
+    for steps in (37, 200):
+        e0, z0, n0 = bg.lanczos_lowest(init, steps=steps, use_graph=False)
+        e1, z1, n1 = bg.lanczos_lowest(init, steps=steps, use_graph=True)
+        assert e0 == e1 and n0 == n1
+        assert torch.equal(z0, z1)
+    bg.close()
