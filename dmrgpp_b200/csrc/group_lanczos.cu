@@ -404,7 +404,7 @@ int ensure_group_work(dmrgpp_kron_handle h, int cols)
 	    || (e = cudaMalloc(&w->seg_chunk, sc.size() * sizeof(int)))
 	    || (e = cudaMalloc(&w->active, size_t(nseg) * sizeof(int)))
 	    || (e = cudaMalloc(&w->ncols, size_t(nseg) * sizeof(int)))
-	    || (e = cudaHostAlloc(&w->host, (2 * nsc + size_t(nseg)) * sizeof(double), 0)))
+	    || (e = cudaHostAlloc(&w->host, 2 * (2 * nsc + size_t(nseg)) * sizeof(double), 0)))
 		return status(h, e, "group solver allocation");
 	if ((e = cudaMemcpy(w->chunks, ch.data(), ch.size() * sizeof(Chunk), cudaMemcpyHostToDevice))
 	    || (e = cudaMemcpy(w->seg_chunk, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice))
@@ -512,15 +512,8 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 		return status(h, e, "update active sectors");
 	const size_t nsc = size_t(S) * size_t(cols);
 	std::vector<double> eold(size_t(S) * p->eigs_for_stop, 0.0);
-	size_t j = 1;
-	while (n_active > 0 && j < maxn) {
-		// no active sector runs past its own last step (its Krylov space)
-		size_t cap = maxn;
-		for (int s = 0; s < S; ++s)
-			if (act[size_t(s)])
-				cap = std::min(cap, maxn_s[size_t(s)]);
-		const size_t jend = std::min(cap, j + size_t(p->check_every));
-		for (size_t jj = j; jj < jend; ++jj) {
+	auto enqueue_group = [&](size_t j0, size_t j1) -> int {
+		for (size_t jj = j0; jj < j1; ++jj) {
 			double* v0 = col(jj - 1);
 			double* v1 = col(jj);
 			double* v2 = col(jj + 1);
@@ -543,24 +536,72 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 				k_g_scale<<<grid, kThreads, 0, st>>>(v2, v2, nrm, 1, w->chunks, nch, w->active);
 			}
 		}
-		if ((e = cudaGetLastError()))
-			return status(h, e, "group Lanczos launch");
-		if ((e = cudaMemcpyAsync(w->host, w->alpha, nsc * sizeof(double), cudaMemcpyDeviceToHost, st))
-		    || (e = cudaMemcpyAsync(w->host + nsc, w->beta, (nsc + size_t(S)) * sizeof(double),
-		                            cudaMemcpyDeviceToHost, st))
-		    || (e = cudaStreamSynchronize(st)))
+		return DMRGPP_OK;
+	};
+	// Groups of steps are enqueued one group ahead of the host's stopping test
+	// (two pinned copies of alpha/beta alternate), so the GPU runs the next
+	// group while the host tests the last one.  A group never passes the last
+	// step of a sector that is still active when it is enqueued.
+	struct Events {
+		cudaEvent_t ev[2] = { nullptr, nullptr };
+		~Events()
+		{
+			for (cudaEvent_t x : ev)
+				if (x)
+					cudaEventDestroy(x);
+		}
+	} events;
+	for (int b = 0; b < 2; ++b)
+		if ((e = cudaEventCreateWithFlags(&events.ev[b], cudaEventDisableTiming)))
+			return status(h, e, "events");
+	const size_t hstride = 2 * nsc + size_t(S);
+	struct Group {
+		size_t j0, j1;
+		int    buf;
+	};
+	std::vector<Group>  inflight;
+	std::vector<double> d, off;
+	size_t              next = 1;
+	int                 buf  = 0;
+	for (;;) {
+		while (inflight.size() < 2 && n_active > 0 && next < maxn) {
+			size_t cap = maxn;
+			for (int s = 0; s < S; ++s)
+				if (act[size_t(s)])
+					cap = std::min(cap, maxn_s[size_t(s)]);
+			if (cap <= next)
+				break; // a sector ends here: test before going on
+			const size_t jend = std::min(cap, next + size_t(p->check_every));
+			if (int rc = enqueue_group(next, jend))
+				return rc;
+			if ((e = cudaGetLastError()))
+				return status(h, e, "group Lanczos launch");
+			double* hb = w->host + size_t(buf) * hstride;
+			if ((e = cudaMemcpyAsync(hb, w->alpha, nsc * sizeof(double), cudaMemcpyDeviceToHost, st))
+			    || (e = cudaMemcpyAsync(hb + nsc, w->beta, (nsc + size_t(S)) * sizeof(double),
+			                            cudaMemcpyDeviceToHost, st))
+			    || (e = cudaEventRecord(events.ev[buf], st)))
+				return status(h, e, "read alpha/beta");
+			inflight.push_back({ next, jend, buf });
+			next = jend;
+			buf ^= 1;
+		}
+		if (inflight.empty())
+			break;
+		const Group g = inflight.front();
+		inflight.erase(inflight.begin());
+		if ((e = cudaEventSynchronize(events.ev[g.buf])))
 			return status(h, e, "group Lanczos steps");
 		if (h->err_host && *reinterpret_cast<volatile int*>(h->err_host))
 			return handle_fail(h, DMRGPP_TIMEOUT, "H*x kernel wait gave up during the group Lanczos");
-		const double* ah = w->host;
-		const double* bh = w->host + nsc;
+		const double* ah = w->host + size_t(g.buf) * hstride;
+		const double* bh = ah + nsc;
 		bool          changed = false;
-		std::vector<double> d, off;
 		for (int s = 0; s < S; ++s) {
 			if (!act[size_t(s)])
 				continue;
-			// steps up to jend - 1 are done; test at the last one
-			const size_t jj   = jend - 1;
+			// steps up to g.j1 - 1 are done; test at the last one
+			const size_t jj   = g.j1 - 1;
 			const size_t n    = jj + 1;
 			const size_t ne   = std::min(p->eigs_for_stop, n);
 			double       dmax = 0.0;
@@ -592,24 +633,21 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 		if (changed
 		    && (e = cudaMemcpyAsync(w->active, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
 			return status(h, e, "update active sectors");
-		j = jend;
 	}
-	if (n_active > 0 || maxn == 1) { // no test point read the scalars back yet
-		if ((e = cudaMemcpy(w->host, w->alpha, nsc * sizeof(double), cudaMemcpyDeviceToHost))
-		    || (e = cudaMemcpy(w->host + nsc, w->beta, (nsc + size_t(S)) * sizeof(double), cudaMemcpyDeviceToHost)))
-			return status(h, e, "read alpha/beta");
-		for (int s = 0; s < S; ++s)
-			if (act[size_t(s)])
-				j_stop[size_t(s)] = maxn_s[size_t(s)] - 1;
-	}
-	{
-	}
+	for (int s = 0; s < S; ++s)
+		if (act[size_t(s)])
+			j_stop[size_t(s)] = maxn_s[size_t(s)] - 1;
+	// final scalars: entries up to each sector's stopping step no longer change
+	if ((e = cudaStreamSynchronize(st))
+	    || (e = cudaMemcpy(w->host, w->alpha, nsc * sizeof(double), cudaMemcpyDeviceToHost))
+	    || (e = cudaMemcpy(w->host + nsc, w->beta, (nsc + size_t(S)) * sizeof(double), cudaMemcpyDeviceToHost)))
+		return status(h, e, "read alpha/beta");
 
 	// Ritz pairs per sector (LanczosSolver.h:76-84): lowest eigenvalue of the
 	// (j_stop + 1)-dimensional tridiagonal and its eigenvector
 	const double*       ah = w->host;
 	const double*       bh = w->host + nsc;
-	std::vector<double> coef(nsc, 0.0), d, off;
+	std::vector<double> coef(nsc, 0.0);
 	std::vector<int>    ncols(static_cast<size_t>(S));
 	for (int s = 0; s < S; ++s) {
 		const size_t n = j_stop[size_t(s)] + 1;
