@@ -61,7 +61,8 @@ NOALLOC_SCRATCH_BYTES = 16 << 20
 class LanczosParams(ctypes.Structure):
     _fields_ = [("steps", _sz), ("min_steps", _sz), ("eigs_for_stop", _sz),
                 ("tolerance", ctypes.c_double), ("reortho", ctypes.c_int),
-                ("check_every", ctypes.c_int), ("use_graph", ctypes.c_int)]
+                ("check_every", ctypes.c_int), ("use_graph", ctypes.c_int),
+                ("residual_gap_ratio", ctypes.c_double)]
 
 
 class DavidsonParams(ctypes.Structure):

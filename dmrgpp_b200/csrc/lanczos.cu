@@ -625,6 +625,7 @@ void dmrgpp_lanczos_params_init(dmrgpp_lanczos_params* p)
 	p->reortho       = 1;     // Options=reortho
 	p->check_every   = 8;
 	p->use_graph     = 1;
+	p->residual_gap_ratio = 0.0;
 }
 
 int dmrgpp_tridiag_eigen(size_t n, const double* diag, const double* offdiag, double* eigs,
@@ -857,7 +858,7 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 		int    buf;
 	};
 	std::vector<Group> inflight;
-	std::vector<double> eold(p->eigs_for_stop, 0.0), dd, ee;
+	std::vector<double> eold(p->eigs_for_stop, 0.0), dd, ee, rz;
 	size_t              j_stop = 0;
 	bool                done   = false;
 	size_t              next   = 1;
@@ -905,6 +906,14 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 				eold[k]         = th;
 			}
 			bool exit_flag = dmax < p->tolerance || jj == maxn - 1;
+			if (!exit_flag && p->residual_gap_ratio > 0.0 && n >= 2) {
+				// residual of the lowest Ritz pair: beta_{j+1} |last component|
+				const double th2 = tridiag_kth_lowest(int(n), dd.data(), ee.data(), 2);
+				rz.resize(n);
+				tridiag_inverse_iteration(int(n), dd.data(), ee.data(), eold[0], rz.data());
+				const double res = std::fabs(bh[n]) * std::fabs(rz[n - 1]);
+				exit_flag        = res <= p->residual_gap_ratio * (th2 - eold[0]);
+			}
 			if ((exit_flag && D <= 4) || (exit_flag && jj >= p->min_steps)) {
 				j_stop = jj;
 				done   = true;

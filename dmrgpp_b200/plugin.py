@@ -198,7 +198,8 @@ class BatchedGemm:
 
     def lanczos_lowest(self, init, steps: int = 200, min_steps: int = 4,
                        tolerance: float = 1e-12, eigs_for_stop: int = 1, reortho: bool = True,
-                       check_every: int = 8, use_graph: bool = True):
+                       check_every: int = 8, use_graph: bool = True,
+                       residual_gap_ratio: float = 0.0):
         """Lowest eigenpair by the device Lanczos (the reference's
         LanczosSolver::computeAllStatesBelow for one state).  Returns
         (energy, ritz_vector, steps).  numpy init -> numpy vector; a torch
@@ -209,6 +210,7 @@ class BatchedGemm:
         p.steps, p.min_steps, p.tolerance = steps, min_steps, tolerance
         p.eigs_for_stop, p.reortho, p.check_every = eigs_for_stop, int(reortho), check_every
         p.use_graph = int(use_graph)
+        p.residual_gap_ratio = residual_gap_ratio
         e = ctypes.c_double()
         n = ctypes.c_size_t()
         if hasattr(init, "data_ptr"):

@@ -206,6 +206,11 @@ typedef struct {
 	                         captured once per solve and replayed (the kernels choose their
 	                         Lanczos columns on the device); 0: launched one by one.  Results
 	                         are bitwise identical. */
+	double residual_gap_ratio; /* 0 (default): off.  > 0: also stop (after min_steps) once the
+	                         lowest Ritz pair's residual estimate beta_{j+1} |s_j| is below
+	                         this fraction of the gap to the second Ritz value -- the start
+	                         of a refinement that must converge to the lowest state.  No
+	                         counterpart in the reference. */
 } dmrgpp_lanczos_params;
 
 /* Fills the reference's defaults (ParametersForSolver.h:93-120). */

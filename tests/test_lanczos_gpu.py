@@ -97,3 +97,22 @@ def test_graph_replayed_steps_are_bitwise_identical(cuda_lib, cuda_device, prec)
         assert e0 == e1 and n0 == n1
         assert torch.equal(z0, z1)
     bg.close()
+
+
+def test_residual_gap_stop_ends_earlier_with_a_usable_start(cuda_lib, cuda_device):
+    """residual_gap_ratio > 0 stops once the lowest Ritz residual estimate is
+    below that fraction of the gap to the second Ritz value: fewer steps than
+    the eigenvalue-change test, and the FP64 refinement from there reaches the
+    same energy."""
+    import torch
+    from dmrgpp_b200 import plugin
+    prob = sb.c2_problem(seed=31)
+    bg = plugin.BatchedGemm.from_problem(prob)
+    init = torch.from_numpy(np.random.default_rng(6).standard_normal(prob.dim)).cuda()
+    e0, z0, n0 = bg.lanczos_lowest(init, steps=300, tolerance=1e-12)
+    e1, z1, n1 = bg.lanczos_lowest(init, steps=300, tolerance=1e-12, residual_gap_ratio=0.1)
+    assert n1 < n0
+    e2, st = bg.refine_lowest(z1, max_outer=10, tolerance=1e-11, inner_iterations=100,
+                              inner_tolerance=1e-6)
+    assert abs(e2 - e0) <= 1e-11 * abs(e0)
+    bg.close()
