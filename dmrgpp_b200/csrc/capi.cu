@@ -76,6 +76,10 @@ void release(dmrgpp_kron_handle h)
 	cudaFree(h->m_bxs_lo);
 	cudaFree(h->m_xmap);
 	cudaFree(h->m_lists);
+	cudaFree(h->m_partial);
+	cudaFree(h->m_arrive);
+	h->m_partial = nullptr;
+	h->m_arrive  = nullptr;
 	h->m_ops_hi = h->m_ops_lo = h->m_xs_hi = h->m_xs_lo = h->m_bxs_hi = h->m_bxs_lo = nullptr;
 	h->m_xmap   = nullptr;
 	h->m_lists  = nullptr;
@@ -139,6 +143,9 @@ int check_error_word(dmrgpp_kron_handle h)
 	*h->err_host      = 0;
 	const size_t nctr = 3 + h->plan.np + size_t(h->plan.n_split_tiles);
 	cudaMemsetAsync(h->d_ctr, 0, nctr * sizeof(unsigned), h->stream);
+	if (h->m_arrive)
+		cudaMemsetAsync(h->m_arrive, 0, size_t(std::max(h->plan.mixed.n_split_tiles, 1)) * sizeof(unsigned),
+		                h->stream);
 	cudaStreamSynchronize(h->stream);
 	return fail(h, DMRGPP_TIMEOUT, "a bounded wait in an H*x kernel gave up; result invalid");
 }
@@ -185,6 +192,8 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const S
 	a2.ntiles = int(mp.tile2.size());
 	a2.grid   = h->m_grid2;
 	a2.starts = h->m_starts2;
+	a2.partial = h->m_partial;
+	a2.arrive  = h->m_arrive;
 	a2.error  = h->err_dev;
 	if ((e = tc_launch(a2, mp.bn, false, h->stream)))
 		return cuda_fail(h, e, "tensor-core pass 2 launch");
@@ -232,16 +241,16 @@ int build_mixed(dmrgpp_kron_handle h)
 	for (size_t p = 0; p < h->plan.np; ++p)
 		maxs = std::max<size_t>(maxs, size_t(std::max(h->plan.l[p], h->plan.r[p])));
 	const int   bn  = maxs > 96 ? 128 : 64;
-	std::string msg = build_mixed_plan(h->plan, bn, &hi, &lo, &xmap);
+	int         sms = 0;
+	cudaError_t e   = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+	if (e != cudaSuccess)
+		return cuda_fail(h, e, "SM count");
+	std::string msg = build_mixed_plan(h->plan, bn, &hi, &lo, &xmap, sms);
 	if (!msg.empty())
 		return fail(h, DMRGPP_INVALID_ARG, msg);
 	const MixedPlan& mp = h->plan.mixed;
-	cudaError_t      e  = tc_init();
-	if (e != cudaSuccess)
+	if ((e = tc_init()) != cudaSuccess)
 		return cuda_fail(h, e, "tensor-core kernel attributes");
-	int sms = 0;
-	if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device)))
-		return cuda_fail(h, e, "SM count");
 	MixedPlan&       mpw = h->plan.mixed;
 	std::vector<int> starts1, starts2;
 	h->m_grid1 = balance_tiles(mpw.tile1, mpw.seg1, sms, starts1);
@@ -253,6 +262,11 @@ int build_mixed(dmrgpp_kron_handle h)
 	    || (e = cudaMalloc(&h->m_bxs_lo, fbytes(mp.bxs_elems)))
 	    || (e = cudaMalloc(&h->m_xmap, size_t(std::max<long long>(h->plan.dim(), 1)) * sizeof(int))))
 		return cuda_fail(h, e, "cudaMalloc(mixed-precision buffers)");
+	// K-split pass-2 tiles: FP32 partial slots and self-resetting counters
+	if ((e = cudaMalloc(&h->m_partial, fbytes(mp.split_slots * 128 * mp.bn)))
+	    || (e = cudaMalloc(&h->m_arrive, size_t(std::max(mp.n_split_tiles, 1)) * sizeof(unsigned)))
+	    || (e = cudaMemset(h->m_arrive, 0, size_t(std::max(mp.n_split_tiles, 1)) * sizeof(unsigned))))
+		return cuda_fail(h, e, "cudaMalloc(split-K partials)");
 	// K padding must read as zero
 	if ((e = cudaMemset(h->m_xs_hi, 0, fbytes(mp.xs_elems))) || (e = cudaMemset(h->m_xs_lo, 0, fbytes(mp.xs_elems)))
 	    || (e = cudaMemset(h->m_bxs_hi, 0, fbytes(mp.bxs_elems)))

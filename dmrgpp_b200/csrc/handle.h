@@ -59,6 +59,8 @@ struct dmrgpp_kron_s {
 	int                 m_grid2  = 0;
 	int*                m_starts1 = nullptr; // per-CTA tile runs of pass 1 / 2
 	int*                m_starts2 = nullptr;
+	float*              m_partial = nullptr; // split-K partial tiles of pass 2
+	unsigned*           m_arrive  = nullptr; // per split tile: parts done
 	void*               m_lists  = nullptr; // seg1, seg2, tile1, tile2
 	dmrgpp::GemmSeg*    m_seg1 = nullptr;
 	dmrgpp::GemmSeg*    m_seg2 = nullptr;

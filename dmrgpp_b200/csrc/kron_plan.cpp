@@ -463,7 +463,7 @@ void split_tf32(double v, float* hi, float* lo)
 }
 
 std::string build_mixed_plan(KronPlan& plan, int bn, std::vector<float>* ops_hi,
-                             std::vector<float>* ops_lo, std::vector<int>* x_map)
+                             std::vector<float>* ops_lo, std::vector<int>* x_map, int sms)
 {
 	MixedPlan& mp   = plan.mixed;
 	mp              = MixedPlan();
@@ -585,6 +585,52 @@ std::string build_mixed_plan(KronPlan& plan, int bn, std::vector<float>* ops_hi,
 			k += segs[s].K;
 		return k;
 	};
+	// split long pass-2 tiles along K (whole segments per part) so that the
+	// pass has about two parts per SM; a part keeps at least 16 k-chunks (the
+	// partial-tile round trip and the final reduction cost about that much)
+	{
+		long long total = 0;
+		for (const GemmTile& g : mp.tile2)
+			total += kcost(mp.seg2, g) / 32;
+		const long long target = std::max<long long>(16, total / (2LL * std::max(sms, 1)));
+		std::vector<GemmTile> out;
+		for (const GemmTile& g : mp.tile2) {
+			const long long c = kcost(mp.seg2, g) / 32;
+			if (c <= 2 * target || g.seg_end - g.seg_begin < 2) {
+				out.push_back(g);
+				continue;
+			}
+			std::vector<std::pair<int, int>> parts;
+			int       b   = g.seg_begin;
+			long long acc = 0;
+			for (int q = g.seg_begin; q < g.seg_end; ++q) {
+				acc += mp.seg2[size_t(q)].K / 32;
+				if (acc >= target && q + 1 < g.seg_end) {
+					parts.push_back({ b, q + 1 });
+					b   = q + 1;
+					acc = 0;
+				}
+			}
+			parts.push_back({ b, g.seg_end });
+			if (parts.size() < 2) {
+				out.push_back(g);
+				continue;
+			}
+			const int tile_id = mp.n_split_tiles++;
+			for (size_t q = 0; q < parts.size(); ++q) {
+				GemmTile part   = g;
+				part.seg_begin  = parts[q].first;
+				part.seg_end    = parts[q].second;
+				part.nsplit     = int(parts.size());
+				part.split_part = int(q);
+				part.split_tile = tile_id;
+				part.slot       = int(mp.split_slots);
+				out.push_back(part);
+			}
+			mp.split_slots += (long long)parts.size();
+		}
+		mp.tile2.swap(out);
+	}
 	std::stable_sort(mp.tile1.begin(), mp.tile1.end(), [&](const GemmTile& x, const GemmTile& y) {
 		return kcost(mp.seg1, x) > kcost(mp.seg1, y);
 	});

@@ -42,7 +42,13 @@ struct alignas(16) GemmTile {
 	int       n0;
 	int       seg_begin;
 	int       seg_end;
-	int       pad;
+	// tensor-core pass 2 only: nsplit >= 2 marks part split_part of output
+	// tile split_tile, cut along K at segment boundaries; its FP32 partial
+	// goes to slot + split_part, the last part to arrive sums the slots
+	int       nsplit;
+	int       split_part;
+	int       split_tile;
+	int       slot;
 };
 
 // One work item of the persistent launch (kron_persistent.cu).
@@ -128,6 +134,8 @@ struct MixedPlan {
 	std::vector<GemmSeg>   seg1, seg2;
 	std::vector<GemmTile>  tile1, tile2;
 	int                    bm = 128, bn = 64;
+	int                    n_split_tiles = 0; // pass-2 output tiles cut along K
+	long long              split_slots   = 0; // partial tiles of their parts
 };
 
 struct KronPlan {
@@ -202,9 +210,12 @@ std::string build_kron_plan_triples(size_t noperator, size_t npatches, const siz
 // Builds plan.mixed for bn-wide tensor-core tiles from plan.blocks.  When
 // ops_hi/ops_lo are given, packs the operators (hi and lo TF32 parts stored
 // as floats); x_map (optional, dim entries) receives, for each element of the
-// sector vector, its offset in the x split buffer.
+// sector vector, its offset in the x split buffer.  Pass-2 tiles much longer
+// than an even share of the work over `sms` SMs are cut along K at segment
+// boundaries (small sectors would otherwise leave most SMs idle).
 std::string build_mixed_plan(KronPlan& plan, int bn, std::vector<float>* ops_hi,
-                             std::vector<float>* ops_lo, std::vector<int>* x_map);
+                             std::vector<float>* ops_lo, std::vector<int>* x_map,
+                             int sms = 148);
 
 // Diagonal of the sector's H in patch order: element (iR, iL) of patch i is
 // sum_k A_k(i,i)(iL,iL) * B_k(i,i)(iR,iR) over the contributing diagonal

@@ -331,10 +331,76 @@ __device__ __forceinline__ void store_chunk(const TcArgs& a, const GemmTile& t, 
 	}
 }
 
+// the 4 epilogue warps only (named barrier 1)
+__device__ __forceinline__ void epilogue_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+
+// AND of a flag over the 4 epilogue warps (named barrier 1), so that every
+// epilogue thread takes the same branch after a bounded wait
+__device__ __forceinline__ bool epilogue_all(bool v)
+{
+	unsigned out;
+	asm volatile("{\n\t.reg .pred p, q;\n\t"
+	             "setp.ne.u32 p, %1, 0;\n\t"
+	             "bar.red.and.pred q, 1, 128, p;\n\t"
+	             "selp.u32 %0, 1, 0, q;\n\t}\n"
+	             : "=r"(out)
+	             : "r"(unsigned(v))
+	             : "memory");
+	return out != 0;
+}
+
+// part of a K-split pass-2 tile: this thread's row of one 32-column chunk
+// into the part's FP32 slot (row-major 128 x BN)
+template <int BN>
+__device__ __forceinline__ void store_partial(const TcArgs& a, const GemmTile& t, int row, int c0,
+                                              const float (&v)[32])
+{
+	float* dst = a.partial + (size_t(t.slot + t.split_part) * 128 + size_t(row)) * BN + c0;
+#pragma unroll
+	for (int q = 0; q < 8; ++q)
+		reinterpret_cast<float4*>(dst)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+// after every part of split tile t wrote its slot: sum the slots in part
+// order (deterministic) and write y
+template <int BN>
+__device__ __forceinline__ void reduce_split(const TcArgs& a, const GemmTile& t, int row)
+{
+	const int grow = t.m0 + row;
+	if (grow >= t.M)
+		return;
+	double* y = (a.io ? a.io->y : a.Cd) + t.c_off;
+	for (int c0 = 0; c0 < BN && t.n0 + c0 < t.N; c0 += 32) {
+		float s[32];
+#pragma unroll
+		for (int i = 0; i < 32; ++i)
+			s[i] = 0.f;
+		for (int p = 0; p < t.nsplit; ++p) {
+			const float4* src = reinterpret_cast<const float4*>(
+			    a.partial + (size_t(t.slot + p) * 128 + size_t(row)) * BN + c0);
+#pragma unroll
+			for (int q = 0; q < 8; ++q) {
+				const float4 f = __ldcg(src + q);
+				s[4 * q] += f.x;
+				s[4 * q + 1] += f.y;
+				s[4 * q + 2] += f.z;
+				s[4 * q + 3] += f.w;
+			}
+		}
+#pragma unroll
+		for (int i = 0; i < 32; ++i) {
+			const int gcol = t.n0 + c0 + i;
+			if (gcol < t.N)
+				y[(long long)gcol * t.ldc + grow] = double(s[i]);
+		}
+	}
+}
+
 template <int BN, bool PASS1>
 __device__ void epilogue(const TcArgs& a, unsigned tmem, unsigned accf0, unsigned acce0,
                          volatile int* abort)
 {
+	__shared__ int s_last;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int quarter = warp & 3; // TMEM lanes this warp may read
 	const int row     = quarter * 32 + lane;
@@ -354,20 +420,44 @@ __device__ void epilogue(const TcArgs& a, unsigned tmem, unsigned accf0, unsigne
 			continue;
 		}
 		const unsigned b = tc & 1;
-		if (!mbar_wait(accf0 + 8 * b, (tc >> 1) & 1, abort)) {
+		// uniform over the epilogue warps: a wait that gave up in any of them
+		// stops all (the split reduction below has unbounded named barriers)
+		if (!epilogue_all(mbar_wait(accf0 + 8 * b, (tc >> 1) & 1, abort))) {
 			ok = false;
 			break;
 		}
 		tc_fence_after();
+		const bool split = !PASS1 && t.nsplit >= 2;
 		for (int c0 = 0; c0 < BN; c0 += 32) {
 			tmem_ld32(tmem + (unsigned(quarter * 32) << 16) + b * unsigned(BN) + unsigned(c0), v);
-			store_chunk<BN, PASS1>(a, t, grow, c0, v);
+			if (split)
+				store_partial<BN>(a, t, row, c0, v);
+			else
+				store_chunk<BN, PASS1>(a, t, grow, c0, v);
 		}
 		tc_fence_before();
 		__syncwarp();
 		if (lane == 0)
 			mbar_arrive(acce0 + 8 * b);
 		++tc;
+		if (split) {
+			// the last part to finish sums every part's slot in order
+			__threadfence();
+			epilogue_sync();
+			if (threadIdx.x == 64) {
+				const unsigned old = atomicAdd(&a.arrive[t.split_tile], 1u);
+				s_last             = old == unsigned(t.nsplit - 1);
+				if (s_last)
+					__threadfence();
+			}
+			epilogue_sync();
+			if (s_last) {
+				reduce_split<BN>(a, t, row);
+				epilogue_sync();
+				if (threadIdx.x == 64)
+					a.arrive[t.split_tile] = 0u; // ready for the next launch
+			}
+		}
 	}
 	if (!ok && lane == 0)
 		give_up(abort, a.error);

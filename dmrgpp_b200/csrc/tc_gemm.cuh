@@ -22,6 +22,8 @@ struct TcArgs {
 	int             grid;   // persistent CTAs, at most one per SM
 	int*            error; // set to 2 when an mbarrier wait gave up
 	const StepIO*   io;    // NULL, or pass 2 writes io->y instead of Cd
+	float*          partial; // pass 2: 128 x BN FP32 partial tiles of split parts (slots)
+	unsigned*       arrive;  // pass 2: per split output tile, parts done (self-resetting)
 };
 
 // Kernel attributes on the current device; call once per device.

@@ -7,6 +7,8 @@
 //   * copies that start on a 128-row tile row 0 start on an 8-row swizzle
 //     group, so the pre-swizzled rows land where the descriptor expects them;
 //   * the per-CTA tile runs (balance_tiles) are a permutation of the tiles;
+//   * K-split pass-2 tiles: slots in range, every part present, the parts'
+//     sums are the tile's output;
 //   * the epilogue's stores stay inside their buffers;
 //   * pass 1 + pass 2 computed from these buffers (hi*hi + hi*lo + lo*hi in
 //     double, stale rows included as NaN) reproduce the FP64 H*x.
@@ -19,6 +21,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <limits>
+#include <map>
+#include <set>
 #include <random>
 #include <tuple>
 #include <vector>
@@ -149,6 +153,9 @@ int main(int argc, char** argv)
 	std::vector<double> y(size_t(D), std::numeric_limits<double>::quiet_NaN());
 
 	const int BM = mp.bm;
+	std::map<long long, double>      split_sum;
+	std::map<int, std::set<int>>     split_parts;
+	std::map<int, int>               split_n;
 	auto check_copy = [&](const Buf& b, long long off, long long rows) -> bool {
 		const long long bytes = rows * 128;
 		return off >= 0 && (off * 4) % 16 == 0 && bytes % 16 == 0 && bytes > 0
@@ -218,7 +225,16 @@ int main(int argc, char** argv)
 							const long long o = t.c_off + (long long)gcol * t.ldc + grow;
 							if (o < 0 || o >= D)
 								return fail("y store out of bounds", o, D);
-							y[size_t(o)] = v;
+							if (t.nsplit >= 2) { // part of a K-split tile: slot, summed later
+								if (t.slot < 0 || t.split_part < 0 || t.split_part >= t.nsplit
+								    || t.slot + t.nsplit > mp.split_slots)
+									return fail("split slot out of range", t.slot, t.split_part);
+								split_sum[o] = (split_sum.count(o) ? split_sum[o] : 0.0) + double(float(v));
+								split_parts[t.split_tile].insert(t.split_part);
+								split_n[t.split_tile] = t.nsplit;
+							} else {
+								y[size_t(o)] = v;
+							}
 						}
 					}
 				}
@@ -233,6 +249,14 @@ int main(int argc, char** argv)
 		return 1;
 	if (pass(mp.seg2, mp.tile2, bxb, ops, false))
 		return 1;
+	// every split tile got all of its parts, and their sums are its output
+	if (int(split_parts.size()) != mp.n_split_tiles)
+		return fail("split tiles without parts", long(split_parts.size()), mp.n_split_tiles);
+	for (const auto& kv : split_parts)
+		if (int(kv.second.size()) != split_n[kv.first])
+			return fail("split tile missing parts", kv.first, long(kv.second.size()));
+	for (const auto& kv : split_sum)
+		y[size_t(kv.first)] = kv.second;
 	double err = 0, ref = 0;
 	for (long long e = 0; e < D; ++e) {
 		if (!std::isfinite(y[size_t(e)]))
@@ -243,6 +267,6 @@ int main(int argc, char** argv)
 	const double rel = ref > 0 ? err / ref : err;
 	if (rel > 1e-5)
 		return fail("result differs from FP64", (long long)(rel * 1e9), 0);
-	std::printf("ok %.3e\n", rel);
+	std::printf("ok %.3e split_tiles %d\n", rel, mp.n_split_tiles);
 	return 0;
 }
