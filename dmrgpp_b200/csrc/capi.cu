@@ -176,6 +176,7 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const S
 	a1.tiles  = h->m_tile1;
 	a1.ntiles = int(mp.tile1.size());
 	a1.grid   = h->m_grid1;
+	a1.test_unarmed = h->test_stall;
 	a1.starts = h->m_starts1;
 	a1.error  = h->err_dev;
 	if ((e = tc_launch(a1, mp.bn, true, h->stream)))

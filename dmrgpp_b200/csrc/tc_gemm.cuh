@@ -24,6 +24,7 @@ struct TcArgs {
 	const StepIO*   io;    // NULL, or pass 2 writes io->y instead of Cd
 	float*          partial; // pass 2: 128 x BN FP32 partial tiles of split parts (slots)
 	unsigned*       arrive;  // pass 2: per split output tile, parts done (self-resetting)
+	int             test_unarmed; // test hook: CTA 0's producer leaves its first stage unarmed
 };
 
 // Kernel attributes on the current device; call once per device.

@@ -122,10 +122,13 @@ int dmrgpp_kron_set_precision(dmrgpp_kron_handle h, int precision);
 int dmrgpp_kron_synchronize(dmrgpp_kron_handle h);
 
 /* Test hook (no counterpart in the reference): with on != 0 every following
- * apply makes the kernel's dependency waits on input patch 0 unsatisfiable,
- * so they run into their time limit (about 0.2 s) and the apply reports
- * DMRGPP_TIMEOUT; the handle stays usable.  Used to test failure detection
- * without faulting the GPU. */
+ * apply makes a bounded wait inside the kernels unsatisfiable -- FP64: the
+ * dependency waits on input patch 0 (time limit about 0.2 s); TF32x3: the
+ * first pipeline stage of one CTA of pass 1 is never filled, so the MMA
+ * thread's mbarrier wait runs out (about 0.5 s), the CTA drains its copies,
+ * frees its tensor memory and exits.  The apply then reports DMRGPP_TIMEOUT
+ * and the handle stays usable.  Used to test failure detection without
+ * faulting the GPU. */
 int dmrgpp_kron_test_stall_dependency(dmrgpp_kron_handle h, int on);
 
 /* The diagonal of the sector's H (patch order) into diag (device pointer). */

@@ -10,11 +10,9 @@ them):  python tests/golden/make_golden.py
   expected Y = B X A^T is recomputed by the test's own loops and by the
   reference BatchedGemmCpu compiled from its sources.
 * kron_data31.npz -- the H*v dump TestSuite/inputs/kron_data31_0_ref.txt
-  (KronLogger format, dmrg/Engine/MatrixVectorKron/KronLogger.hh:112-174,
-  Heisenberg L=8) converted to plugin tables: records with
-  performTranspose=1 hold the stored lower block, so the table receives its
-  transpose (KronConnections.h:141-172).  The file has no output vector; y is
-  computed by the reference BatchedGemmCpu and stored with the fixture.
+  (KronLogger format, read by dmrgpp_b200.kronlog.read_kronlog; Heisenberg
+  L=8) as plugin tables.  The file has no output vector; y is computed by the
+  reference BatchedGemmCpu and stored with the fixture.
 """
 from __future__ import annotations
 
@@ -85,66 +83,22 @@ def batchedgemm_1patch():
     print("batchedgemm_1patch.json: max |ref - expected| =", np.abs(yref - expected).max())
 
 
-def _read_matrix(lines, pos):
-    """KronLogger block: either 'rows cols' + dense rows, or MatrixMarket."""
-    head = lines[pos].strip()
-    if head.startswith("%%MatrixMarket"):
-        rows, cols, nnz = map(int, lines[pos + 1].split())
-        m = np.zeros((rows, cols))
-        for t in range(nnz):
-            i, j, v = lines[pos + 2 + t].split()
-            m[int(i) - 1, int(j) - 1] = float(v)
-        return m, pos + 2 + nnz
-    rows, cols = map(int, head.split())
-    m = np.array([[float(x) for x in lines[pos + 1 + r].split()] for r in range(rows)])
-    return m.reshape(rows, cols), pos + 1 + rows
-
-
 def kron_data31():
+    from dmrgpp_b200.kronlog import read_kronlog
     path = os.path.join(REF, "TestSuite", "inputs", "kron_data31_0_ref.txt")
-    lines = open(path).read().splitlines()
-    pos = lines.index("Vector")
-    n = int(lines[pos + 1])
-    vin = np.array([float(lines[pos + 2 + i]) for i in range(n)])
-    pos = pos + 2 + n
-    recs = []
-    while pos < len(lines):
-        if lines[pos].startswith("# nc, total"):
-            f = [int(x) for x in lines[pos + 1].split()]
-            nc, total, outp, inp, ic, adj, tr, offx, offy = f
-            assert lines[pos + 2].startswith("## A:")
-            A, pos = _read_matrix(lines, pos + 3)
-            assert lines[pos].startswith("## B:")
-            B, pos = _read_matrix(lines, pos + 1)
-            if tr:  # stored lower block, applied transposed
-                A, B = A.T, B.T
-            recs.append((outp, inp, ic, offx, offy, A, B))
-        else:
-            pos += 1
-    nc, npatch = nc, total
-    lsz = np.zeros(npatch, dtype=np.int64)
-    rsz = np.zeros(npatch, dtype=np.int64)
-    offs = {}
-    Ad, Bd = {}, {}
-    for outp, inp, ic, offx, offy, A, B in recs:
-        lsz[outp], rsz[outp] = A.shape[0], B.shape[0]
-        lsz[inp], rsz[inp] = A.shape[1], B.shape[1]
-        offs[outp], offs[inp] = offx, offy
-        Ad[(outp, inp, ic)] = np.asfortranarray(A)
-        Bd[(outp, inp, ic)] = np.asfortranarray(B)
-    prob = KronProblem(lsz, rsz, nc, Ad, Bd, name="kron_data31")
-    assert prob.dim == n
-    assert all(prob.xy_start[p] == offs[p] for p in offs)
+    prob, vin = read_kronlog(path, name="kron_data31")
+    Ad, Bd = prob.A, prob.B
     y = oracle.RefKron(prob).apply(vin)
     rq = float(vin @ y / (vin @ vin))
     keys = sorted(Ad)
     np.savez_compressed(
-        os.path.join(HERE, "kron_data31.npz"), lsz=lsz, rsz=rsz, noperator=nc, vin=vin,
-        y_reference=y, rayleigh=rq, keys=np.array(keys, dtype=np.int64),
+        os.path.join(HERE, "kron_data31.npz"), lsz=prob.lsz, rsz=prob.rsz,
+        noperator=prob.noperator, vin=vin, y_reference=y, rayleigh=rq,
+        keys=np.array(keys, dtype=np.int64),
         A=np.concatenate([Ad[k].ravel(order="F") for k in keys]),
         B=np.concatenate([Bd[k].ravel(order="F") for k in keys]),
         source=np.array("TestSuite/inputs/kron_data31_0_ref.txt"))
-    print("kron_data31.npz: patches", npatch, "records", len(recs), "dim", n,
+    print("kron_data31.npz: patches", prob.npatches, "records", len(keys), "dim", prob.dim,
           "Rayleigh quotient", rq)
 
 
