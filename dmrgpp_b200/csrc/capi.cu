@@ -236,7 +236,6 @@ int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const St
 
 int build_mixed(dmrgpp_kron_handle h)
 {
-	std::vector<float> hi, lo;
 	std::vector<int>   xmap;
 	size_t             maxs = 0;
 	for (size_t p = 0; p < h->plan.np; ++p)
@@ -246,7 +245,8 @@ int build_mixed(dmrgpp_kron_handle h)
 	cudaError_t e   = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
 	if (e != cudaSuccess)
 		return cuda_fail(h, e, "SM count");
-	std::string msg = build_mixed_plan(h->plan, bn, &hi, &lo, &xmap, sms);
+	// operators: packed on the device from the FP64 copy already there
+	std::string msg = build_mixed_plan(h->plan, bn, nullptr, nullptr, &xmap, sms);
 	if (!msg.empty())
 		return fail(h, DMRGPP_INVALID_ARG, msg);
 	const MixedPlan& mp = h->plan.mixed;
@@ -273,10 +273,19 @@ int build_mixed(dmrgpp_kron_handle h)
 	    || (e = cudaMemset(h->m_bxs_hi, 0, fbytes(mp.bxs_elems)))
 	    || (e = cudaMemset(h->m_bxs_lo, 0, fbytes(mp.bxs_elems))))
 		return cuda_fail(h, e, "clear mixed-precision buffers");
-	if (!hi.empty()
-	    && ((e = cudaMemcpy(h->m_ops_hi, hi.data(), hi.size() * sizeof(float), cudaMemcpyHostToDevice))
-	        || (e = cudaMemcpy(h->m_ops_lo, lo.data(), lo.size() * sizeof(float), cudaMemcpyHostToDevice))))
-		return cuda_fail(h, e, "upload mixed-precision operators");
+	{
+		const std::vector<PackJob> jobs = mixed_pack_jobs(h->plan);
+		PackJob* d_jobs = nullptr;
+		if ((e = cudaMemset(h->m_ops_hi, 0, fbytes(mp.ops_elems))) || (e = cudaMemset(h->m_ops_lo, 0, fbytes(mp.ops_elems)))
+		    || (e = cudaMalloc(&d_jobs, std::max<size_t>(jobs.size(), 1) * sizeof(PackJob)))
+		    || (e = cudaMemcpy(d_jobs, jobs.data(), jobs.size() * sizeof(PackJob), cudaMemcpyHostToDevice))
+		    || (e = tc_pack_ops(h->d_ops, h->m_ops_hi, h->m_ops_lo, d_jobs, int(jobs.size()), h->stream))
+		    || (e = cudaStreamSynchronize(h->stream))) {
+			cudaFree(d_jobs);
+			return cuda_fail(h, e, "pack mixed-precision operators");
+		}
+		cudaFree(d_jobs);
+	}
 	if (!xmap.empty()
 	    && (e = cudaMemcpy(h->m_xmap, xmap.data(), xmap.size() * sizeof(int), cudaMemcpyHostToDevice)))
 		return cuda_fail(h, e, "upload x map");
@@ -395,7 +404,7 @@ namespace {
 // buffers, persistent schedule, diagonal, and the TF32x3 form if requested.
 // Frees h on failure.
 int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm,
-                  const std::vector<double>& pack, dmrgpp_kron_handle* out)
+                  const dmrgpp::PackBuffer& pack, dmrgpp_kron_handle* out)
 {
 	if (device >= 0) {
 		h->device = device;
@@ -529,7 +538,7 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 
 	int bm, bn;
 	pick_tile(d, bm, bn);
-	std::vector<double> pack;
+	dmrgpp::PackBuffer  pack;
 	std::string         msg = dmrgpp::build_kron_plan(d->noperator,
                                               d->npatches,
                                               d->left_patch_size,
@@ -612,7 +621,7 @@ int dmrgpp_kron_create_group(const dmrgpp_kron_desc* descs, size_t nsectors, dmr
 	h->precision = descs[0].precision;
 	int bm, bn;
 	pick_tile_sizes(l.size(), l.data(), r.data(), bm, bn);
-	std::vector<double> pack;
+	dmrgpp::PackBuffer  pack;
 	std::string msg = dmrgpp::build_kron_plan_triples(nop, l.size(), l.data(), r.data(),
 	                                                  std::move(triples), std::move(blocks), f_alg,
 	                                                  bm, bn, h->plan, &pack);

@@ -2,15 +2,43 @@
 #include "kron_plan.h"
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <tuple>
 #include <utility>
 
 namespace dmrgpp {
 
 namespace {
+
+// f(0..n-1) on the host's cores (dynamic assignment; every f(i) writes its
+// own disjoint output, so the result does not depend on the thread count)
+template <class F> void parallel_for(size_t n, F f)
+{
+	size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 32);
+	nt        = std::min(nt, n);
+	if (nt < 2) {
+		for (size_t i = 0; i < n; ++i)
+			f(i);
+		return;
+	}
+	std::atomic<size_t>      next { 0 };
+	std::vector<std::thread> pool;
+	for (size_t t = 0; t < nt; ++t)
+		pool.emplace_back([&] {
+			for (;;) {
+				const size_t i = next.fetch_add(1);
+				if (i >= n)
+					break;
+				f(i);
+			}
+		});
+	for (std::thread& th : pool)
+		th.join();
+}
 
 constexpr long long kAlign = 32; // doubles (256 bytes) between packed blocks
 
@@ -126,6 +154,8 @@ std::string collect_triples(size_t noperator, size_t np, const size_t* lsz, cons
                             std::vector<BlockRef>& blocks, double& f_alg)
 {
 	const size_t np2 = np * np;
+	// present entries in (i,j,k) order; leading dimensions checked in order
+	std::vector<size_t> cand;
 	for (size_t i = 0; i < np; ++i)
 		for (size_t j = 0; j < np; ++j)
 			for (size_t k = 0; k < noperator; ++k) {
@@ -135,13 +165,24 @@ std::string collect_triples(size_t noperator, size_t np, const size_t* lsz, cons
 				if (ldA[t] < lsz[i] || ldB[t] < rsz[i])
 					return "leading dimension smaller than the block's rows at table entry "
 					    + std::to_string(t);
-				if (!has_nonzero(A[t], ldA[t], lsz[i], lsz[j])
-				    || !has_nonzero(B[t], ldB[t], rsz[i], rsz[j]))
-					continue;
-				triples.push_back({ int(i) + patch_offset, int(j) + patch_offset, int(k) });
-				blocks.push_back({ A[t], ldA[t], B[t], ldB[t] });
-				f_alg += 2.0 * double(rsz[i]) * double(lsz[j]) * (double(rsz[j]) + double(lsz[i]));
+				cand.push_back(t);
 			}
+	// the all-zero test reads every block: on all host cores
+	std::vector<char> keep(cand.size(), 0);
+	parallel_for(cand.size(), [&](size_t q) {
+		const size_t t = cand[q];
+		const size_t i = t % np, j = (t / np) % np;
+		keep[q]        = has_nonzero(A[t], ldA[t], lsz[i], lsz[j]) && has_nonzero(B[t], ldB[t], rsz[i], rsz[j]);
+	});
+	for (size_t q = 0; q < cand.size(); ++q) {
+		if (!keep[q])
+			continue;
+		const size_t t = cand[q];
+		const size_t i = t % np, j = (t / np) % np, k = t / np2;
+		triples.push_back({ int(i) + patch_offset, int(j) + patch_offset, int(k) });
+		blocks.push_back({ A[t], ldA[t], B[t], ldB[t] });
+		f_alg += 2.0 * double(rsz[i]) * double(lsz[j]) * (double(rsz[j]) + double(lsz[i]));
+	}
 	return std::string();
 }
 
@@ -156,7 +197,7 @@ std::string build_kron_plan(size_t               noperator,
                             int                  bm,
                             int                  bn,
                             KronPlan&            plan,
-                            std::vector<double>* pack_host)
+                            PackBuffer*          pack_host)
 {
 	if (noperator == 0 || npatches == 0)
 		return "noperator and npatches must be >= 1";
@@ -179,7 +220,7 @@ std::string build_kron_plan(size_t               noperator,
 std::string build_kron_plan_triples(size_t noperator, size_t npatches, const size_t* lsz,
                                     const size_t* rsz, std::vector<Triple> triples,
                                     std::vector<BlockRef> blocks, double f_alg, int bm, int bn,
-                                    KronPlan& plan, std::vector<double>* pack_host)
+                                    KronPlan& plan, PackBuffer* pack_host)
 {
 	if (noperator == 0 || npatches == 0)
 		return "noperator and npatches must be >= 1";
@@ -255,9 +296,9 @@ std::string build_kron_plan_triples(size_t noperator, size_t npatches, const siz
 	plan.bx_elems = off;
 
 	if (pack_host) {
-		pack_host->assign(size_t(plan.op_elems), 0.0);
+		pack_host->resize(size_t(plan.op_elems)); // every element that is read gets written
 		double* P = pack_host->data();
-		for (size_t t = 0; t < nt; ++t) {
+		parallel_for(nt, [&](size_t t) {
 			const Triple& tr = plan.triples[t];
 			const BlockRef& bl = plan.blocks[t];
 			// B_k(i,j) (r_i x r_j) into rows [row_off, row_off + r_i) of Bstack_j
@@ -274,7 +315,7 @@ std::string build_kron_plan_triples(size_t noperator, size_t npatches, const siz
 			for (long long c = 0; c < plan.l[tr.i]; ++c)
 				for (long long q = 0; q < lj; ++q)
 					at[q + c * lj] = a[c + q * (long long)bl.ldA];
-		}
+		});
 	}
 
 	build_tile_lists(plan, bm, bn);
@@ -683,6 +724,24 @@ int balance_tiles(std::vector<GemmTile>& tiles, const std::vector<GemmSeg>& segs
 	starts[size_t(G)] = int(out.size());
 	tiles.swap(out);
 	return n == 0 ? 0 : G;
+}
+
+std::vector<PackJob> mixed_pack_jobs(const KronPlan& P)
+{
+	const MixedPlan&     mp = P.mixed;
+	std::vector<PackJob> jobs;
+	jobs.reserve(2 * P.triples.size());
+	for (size_t t = 0; t < P.triples.size(); ++t) {
+		const Triple& tr = P.triples[t];
+		const size_t  i = size_t(tr.i), j = size_t(tr.j);
+		// B_k(i,j): rows row_off of Bstack_j (M_j x r_j) -> rows group_row of the chunked Bstack_j
+		jobs.push_back({ P.bstack_off[j] + P.row_off[t], mp.bs_off[j], int(P.M[j]), int(P.r[i]),
+		                 int(P.r[j]), int(mp.Mp[j]), int(mp.group_row[t]), 0 });
+		// A_k(i,j)^T (l_j x l_i, ld l_j) -> rows l_i, K = l_j of the chunked A^T block
+		jobs.push_back({ P.at_off[t], mp.at_off[t], int(P.l[j]), int(P.l[j]), int(P.l[i]),
+		                 int(round8(P.l[i])), 0, 1 });
+	}
+	return jobs;
 }
 
 } // namespace dmrgpp

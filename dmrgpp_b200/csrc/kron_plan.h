@@ -16,6 +16,8 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <memory>
+#include <utility>
 #include <vector>
 
 namespace dmrgpp {
@@ -175,6 +177,23 @@ struct KronPlan {
 	long long dim() const { return xy_start.empty() ? 0 : xy_start.back(); }
 };
 
+// std::vector allocator that leaves elements uninitialised on resize (the
+// packed operator buffer is fully written where it is read; skipping the
+// zero fill of hundreds of MB halves the host side of create).
+template <class T> struct NoInitAllocator : std::allocator<T> {
+	template <class U> struct rebind {
+		using other = NoInitAllocator<U>;
+	};
+	NoInitAllocator() = default;
+	template <class U> NoInitAllocator(const NoInitAllocator<U>&) noexcept {}
+	template <class U> void construct(U* p) noexcept { ::new (static_cast<void*>(p)) U; }
+	template <class U, class... Args> void construct(U* p, Args&&... args)
+	{
+		::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+	}
+};
+using PackBuffer = std::vector<double, NoInitAllocator<double>>;
+
 // Validates the plugin tables and builds the plan.  Returns an empty string on
 // success, otherwise the reason.  pack_host (optional) receives the packed
 // operator buffer (op_elems doubles).
@@ -189,7 +208,7 @@ std::string build_kron_plan(size_t               noperator,
                             int                  bm,
                             int                  bn,
                             KronPlan&            plan,
-                            std::vector<double>* pack_host);
+                            PackBuffer*          pack_host);
 
 // Appends the contributing triples of one plugin table (np patches, patch
 // indices shifted by patch_offset) to triples/blocks, in (i,j,k) order:
@@ -205,7 +224,7 @@ std::string collect_triples(size_t noperator, size_t np, const size_t* lsz, cons
 std::string build_kron_plan_triples(size_t noperator, size_t npatches, const size_t* lsz,
                                     const size_t* rsz, std::vector<Triple> triples,
                                     std::vector<BlockRef> blocks, double f_alg, int bm, int bn,
-                                    KronPlan& plan, std::vector<double>* pack_host);
+                                    KronPlan& plan, PackBuffer* pack_host);
 
 // Builds plan.mixed for bn-wide tensor-core tiles from plan.blocks.  When
 // ops_hi/ops_lo are given, packs the operators (hi and lo TF32 parts stored
@@ -216,6 +235,26 @@ std::string build_kron_plan_triples(size_t noperator, size_t npatches, const siz
 std::string build_mixed_plan(KronPlan& plan, int bn, std::vector<float>* ops_hi,
                              std::vector<float>* ops_lo, std::vector<int>* x_map,
                              int sms = 148);
+
+// One block of the FP64 packed operators (column-major, leading dimension
+// ld, rows x cols at src) into the chunked TF32 hi/lo layout: element (q, c)
+// goes to row (swap ? c : row0 + q), K index (swap ? q : c) of the matrix
+// at dst with dst_rows padded rows.
+struct PackJob {
+	long long src;
+	long long dst;
+	int       ld;
+	int       rows;
+	int       cols;
+	int       dst_rows;
+	int       row0;
+	int       swap;
+};
+
+// The jobs that turn the FP64 packed operators of a planned sector (with
+// plan.mixed built) into its chunked TF32 layout: per triple, its B block
+// (rows of Bstack_j) and its A^T block.
+std::vector<PackJob> mixed_pack_jobs(const KronPlan& plan);
 
 // Diagonal of the sector's H in patch order: element (iR, iL) of patch i is
 // sum_k A_k(i,i)(iL,iL) * B_k(i,i)(iR,iR) over the contributing diagonal

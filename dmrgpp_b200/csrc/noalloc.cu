@@ -90,7 +90,7 @@ int dmrgpp_kron_apply_noalloc(const dmrgpp_kron_desc* d, const double* x, double
 	}
 	const int           tile = maxs <= 192 ? 32 : 64;
 	dmrgpp::KronPlan    plan;
-	std::vector<double> pack;
+	dmrgpp::PackBuffer  pack;
 	std::string         msg = dmrgpp::build_kron_plan(d->noperator,
                                               d->npatches,
                                               d->left_patch_size,

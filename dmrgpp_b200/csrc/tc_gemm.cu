@@ -545,6 +545,28 @@ split_x_kernel(const double* __restrict__ xin, const int* __restrict__ map, floa
 	}
 }
 
+// FP64 packed operators -> chunked TF32 hi/lo layout (one block per job);
+// the same rounding as the host's split_tf32
+__global__ void __launch_bounds__(256)
+pack_tf32_kernel(const double* __restrict__ ops, float* __restrict__ hi, float* __restrict__ lo,
+                 const PackJob* __restrict__ jobs)
+{
+	const PackJob   j = jobs[blockIdx.x];
+	const long long n = (long long)j.rows * j.cols;
+	for (long long e = threadIdx.x; e < n; e += 256) {
+		const int       q   = int(e % j.rows);
+		const int       c   = int(e / j.rows);
+		const double    v   = ops[j.src + q + (long long)c * j.ld];
+		const long long row = j.swap ? c : j.row0 + q;
+		const long long k   = j.swap ? q : c;
+		const long long d   = j.dst + (k >> 5) * (long long)j.dst_rows * 32 + row * 32
+		    + ((((k >> 2) & 7) ^ (row & 7)) << 2) + (k & 3);
+		const float h = tf32_rna(float(v));
+		hi[d]         = h;
+		lo[d]         = tf32_rna(float(v - double(h)));
+	}
+}
+
 template <int BN, int STAGES> constexpr size_t tc_smem()
 {
 	return size_t(STAGES) * TcLayout<BN>::STAGE_BYTES + 1024;
@@ -598,6 +620,15 @@ cudaError_t tc_launch(const TcArgs& a, int bn, bool pass1, cudaStream_t stream)
 	} else {
 		return cudaErrorInvalidValue;
 	}
+	return cudaGetLastError();
+}
+
+cudaError_t tc_pack_ops(const double* ops, float* hi, float* lo, const PackJob* jobs, int njobs,
+                        cudaStream_t stream)
+{
+	if (njobs <= 0)
+		return cudaSuccess;
+	pack_tf32_kernel<<<njobs, 256, 0, stream>>>(ops, hi, lo, jobs);
 	return cudaGetLastError();
 }
 

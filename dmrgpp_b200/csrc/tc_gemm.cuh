@@ -34,6 +34,10 @@ cudaError_t tc_init();
 // a.grid persistent CTAs.
 cudaError_t tc_launch(const TcArgs& a, int bn, bool pass1, cudaStream_t stream);
 
+// Runs the jobs (device array) on stream; hi/lo must be zeroed beforehand.
+cudaError_t tc_pack_ops(const double* ops, float* hi, float* lo, const PackJob* jobs, int njobs,
+                        cudaStream_t stream);
+
 // x (patch order, FP64; io->x instead when io is given) -> TF32 hi/lo parts at map[e].
 cudaError_t tc_split_x(const double* x, const int* map, float* hi, float* lo, long long n,
                        cudaStream_t stream, const StepIO* io = nullptr);

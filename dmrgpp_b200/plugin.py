@@ -10,6 +10,7 @@ raises ``DmrgppError`` instead of the reference's assert/printf.
 from __future__ import annotations
 
 import ctypes
+import time
 from typing import Optional, Sequence
 
 import numpy as np
@@ -79,7 +80,10 @@ class BatchedGemm:
         t = _DescTables(noperator, npatches, left_patch_size, right_patch_size, Amatrix,
                         ld_Amatrix, Bmatrix, ld_Bmatrix, precision, stream, device)
         h = ctypes.c_void_p()
-        _capi.check(L.dmrgpp_kron_create(ctypes.byref(t.desc), ctypes.byref(h)))
+        t0 = time.perf_counter()
+        rc = L.dmrgpp_kron_create(ctypes.byref(t.desc), ctypes.byref(h))
+        self.create_seconds = time.perf_counter() - t0   # the C create alone (synchronous)
+        _capi.check(rc)
         self._h = h
         self._lib = L
         d = ctypes.c_size_t()

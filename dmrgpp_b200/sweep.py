@@ -42,11 +42,20 @@ def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int 
                                 residual refinement with TF32x3 correction solves;
       mixed_davidson         -- TF32x3 Davidson with the learned (or Jacobi)
                                 correction, FP64 restart phase.
-    Seconds are device time around each whole solve (host work included)."""
+    Seconds are device time around each whole solve (host work included);
+    setup_seconds is the handle creation of each form (plan, packing and
+    upload: the plugin constructor a sweep step also pays), and
+    speedup_with_setup compares setup + solve of the two forms."""
     import torch
+    # handle set-up (the plugin constructor: plan, packing, upload) of each form
+    b64 = plugin.BatchedGemm.from_problem(prob, precision=plugin.FP64)
+    setup_fp64 = b64.create_seconds
+    b64.close()
     bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+    setup_mixed = bg.create_seconds
     init = torch.from_numpy(np.random.default_rng(seed).standard_normal(prob.dim)).cuda()
-    out = {"sector_dim": prob.dim, "f_alg_per_matvec": prob.flops(), "sites": sites}
+    out = {"sector_dim": prob.dim, "f_alg_per_matvec": prob.flops(), "sites": sites,
+           "setup_seconds": {"fp64": setup_fp64, "tf32x3": setup_mixed}}
 
     bg.set_precision(plugin.FP64)
     bg.autotune(None, reps=3)
@@ -79,6 +88,7 @@ def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int 
         refine_mixed_matvecs=st_r["inner_matvecs"], fp64_matvecs=st_r["fp64_matvecs"],
         converged=st_r["converged"], **compare(e_r, z_r))
     out["speedup_vs_fp64_lanczos"] = t_l / t_r
+    out["speedup_with_setup"] = (t_l + setup_fp64) / (t_r + setup_mixed)
 
     if with_davidson:
         pre = 2 if mlp is not None else 1

@@ -9,6 +9,8 @@
 //   * the per-CTA tile runs (balance_tiles) are a permutation of the tiles;
 //   * K-split pass-2 tiles: slots in range, every part present, the parts'
 //     sums are the tile's output;
+//   * the device-side operator packing (mixed_pack_jobs) reproduces the host
+//     packing bit for bit;
 //   * the epilogue's stores stay inside their buffers;
 //   * pass 1 + pass 2 computed from these buffers (hi*hi + hi*lo + lo*hi in
 //     double, stale rows included as NaN) reproduce the FP64 H*x.
@@ -86,13 +88,15 @@ int main(int argc, char** argv)
 				ldB[ix] = r[i];
 			}
 
-	KronPlan    plan;
-	std::string msg = build_kron_plan(size_t(nop), size_t(np), l.data(), r.data(), A.data(),
-	                                  ldA.data(), B.data(), ldB.data(), 64, 64, plan, nullptr);
+	KronPlan            plan;
+	std::string         msg;
+	std::vector<float>  ohi, olo;
+	std::vector<int>    xmap;
+	PackBuffer          pack64;
+	msg = build_kron_plan(size_t(nop), size_t(np), l.data(), r.data(), A.data(), ldA.data(),
+	                      B.data(), ldB.data(), 64, 64, plan, &pack64);
 	if (!msg.empty())
 		return fail(msg.c_str());
-	std::vector<float> ohi, olo;
-	std::vector<int>   xmap;
 	msg = build_mixed_plan(plan, bn, &ohi, &olo, &xmap);
 	if (!msg.empty())
 		return fail(msg.c_str());
@@ -121,6 +125,23 @@ int main(int argc, char** argv)
 	}
 	const MixedPlan& mp = plan.mixed;
 	const long long  D  = plan.dim();
+	// the device packing (mixed_pack_jobs over the FP64 packed operators,
+	// the arithmetic of pack_tf32_kernel) gives exactly the host packing
+	{
+		std::vector<float> dhi(size_t(mp.ops_elems), 0.f), dlo(size_t(mp.ops_elems), 0.f);
+		for (const PackJob& jb : mixed_pack_jobs(plan))
+			for (long long e = 0; e < (long long)jb.rows * jb.cols; ++e) {
+				const long long q = e % jb.rows, c = e / jb.rows;
+				const long long row = jb.swap ? c : jb.row0 + q, k = jb.swap ? q : c;
+				const long long d = jb.dst + chunked_offset(jb.dst_rows, row, k);
+				const long long sidx = jb.src + q + c * (long long)jb.ld;
+				if (d < 0 || d >= mp.ops_elems || sidx < 0 || sidx >= (long long)pack64.size())
+					return fail("pack job out of bounds", d, sidx);
+				split_tf32(pack64[size_t(sidx)], &dhi[size_t(d)], &dlo[size_t(d)]);
+			}
+		if (dhi != ohi || dlo != olo)
+			return fail("device-style packing differs from the host packing");
+	}
 
 	std::vector<double> x(static_cast<size_t>(D)), y_ref(static_cast<size_t>(D), 0.0);
 	for (double& v : x)

@@ -17,7 +17,7 @@ def checker(tmp_path_factory):
     exe = str(tmp_path_factory.mktemp("mixed") / "mixed_layout_check")
     subprocess.run(["g++", "-std=c++17", "-O2", "-I" + CSRC, "-I" + os.path.join(ROOT, "include"),
                     os.path.join(HERE, "mixed_layout_check.cpp"),
-                    os.path.join(CSRC, "kron_plan.cpp"), "-o", exe], check=True)
+                    os.path.join(CSRC, "kron_plan.cpp"), "-o", exe, "-lpthread"], check=True)
     return exe
 
 
