@@ -18,6 +18,10 @@
 // Counters are returned to zero by the last CTA to leave, so consecutive
 // launches (and CUDA-graph replays) need no memset.
 //
+// Per item the CTA pays a few global round trips (claim, descriptor,
+// segments, the release of a finished pass-1 tile); they are overlapped
+// with the previous item's stores (see the loop below).
+//
 // Group handles (independent sectors in one launch) may pass a per-sector
 // active mask: the items of stopped sectors are claimed and dropped.
 #include "kron_persistent.cuh"
@@ -65,135 +69,160 @@ template <class C>
 __global__ void __launch_bounds__(C::THREADS) kron_persistent_kernel(PersistentArgs a)
 {
 	extern __shared__ __align__(16) double smem[];
-	__shared__ __align__(16) KronItem s_w[1];
-	__shared__ __align__(16) GemmSeg  s_seg[kMaxItemSegs];
-	__shared__ int                    s_next;
+	__shared__ __align__(16) KronItem s_w[2];
+	__shared__ __align__(16) GemmSeg  s_seg[2][kMaxItemSegs];
+	__shared__ int                    s_it[2];
 	__shared__ int                    s_last;
-	const int                         tid = threadIdx.x;
+	const int                         tid  = threadIdx.x;
+	const int                         warp = tid >> 5, lane = tid & 31;
 	tile::Acc<C>                      acc;
 	const double*                     X   = a.io ? a.io->x : a.x;
 	double*                           Y   = a.io ? a.io->y : a.y;
 	constexpr int                     kSegWords = int(sizeof(GemmSeg) / sizeof(int));
 	constexpr int                     kItemVec  = int(sizeof(KronItem) / 16);
 	static_assert(sizeof(KronItem) % 16 == 0, "descriptor copy");
+	static_assert(kItemVec <= 32, "one warp loads a descriptor");
 
 	// Work distribution: the first item of every CTA is its block index;
-	// later items are claimed one at a time, when the previous one is done,
-	// from a counter offset by the grid size.  Claiming only when free keeps
-	// the pass-1 items (which pass-2 items wait on) from queueing behind
-	// long items.
-	const int cur = 0;
-	if (tid == 0)
-		s_next = int(blockIdx.x);
-	for (;;) {
-		__syncthreads();
-		const int it = s_next;
-		if (it >= a.n_items)
+	// later items are claimed one at a time from a counter offset by the grid
+	// size.  During a pass-1 item the next one is claimed only when its MMAs
+	// are done, which keeps the remaining pass-1 items (which pass-2 items
+	// wait on) from queueing behind busy CTAs; during a pass-2 item it is
+	// claimed at the start, so the claim and the loads of its descriptor and
+	// segments (by warp 0, into the other of two buffers) overlap the
+	// dependency wait and the MMAs.  Items of stopped sectors of a group are
+	// claimed and dropped here.
+	auto fetch = [&](int buf, int it) { // warp 0
+		for (;;) {
+			if (it < a.n_items && a.sector_active && !a.sector_active[a.item_sector[it]]) {
+				unsigned nx = 0;
+				if (lane == 0)
+					nx = atomicAdd(&a.work_counter[0], 1u);
+				it = int(gridDim.x + __shfl_sync(0xffffffffu, nx, 0));
+				continue;
+			}
 			break;
-		if (a.sector_active && !a.sector_active[a.item_sector[it]]) {
-			// a stopped sector of a group: no work, no counters (its pass-2
-			// items, the only waiters on its pass-1 items, are skipped too)
-			__syncthreads();
-			if (tid == 0)
-				s_next = int(gridDim.x + atomicAdd(&a.work_counter[0], 1u));
-			continue;
 		}
-		if (tid < kItemVec)
-			reinterpret_cast<int4*>(&s_w[0])[tid] = reinterpret_cast<const int4*>(a.items + it)[tid];
-		__syncthreads();
-		const KronItem& w    = s_w[cur];
+		if (lane == 0)
+			s_it[buf] = it;
+		if (it >= a.n_items)
+			return;
+		if (lane < kItemVec)
+			reinterpret_cast<int4*>(&s_w[buf])[lane] = reinterpret_cast<const int4*>(a.items + it)[lane];
+		__syncwarp();
+		const KronItem& w    = s_w[buf];
 		const int       nseg = w.seg_end - w.seg_begin;
 		if (nseg > 1) {
 			const GemmSeg* gseg = (w.kind == 0 ? a.seg1 : a.pseg2) + w.seg_begin;
-			for (int q = tid; q < nseg * kSegWords; q += C::THREADS)
-				reinterpret_cast<int*>(s_seg)[q] = reinterpret_cast<const int*>(gseg)[q];
-		} else if (tid < kSegWords) {
-			reinterpret_cast<int*>(s_seg)[tid] = reinterpret_cast<const int*>(&w.seg0)[tid];
+			for (int q = lane; q < nseg * kSegWords; q += 32)
+				reinterpret_cast<int*>(s_seg[buf])[q] = reinterpret_cast<const int*>(gseg)[q];
+		} else if (lane < kSegWords) {
+			reinterpret_cast<int*>(s_seg[buf])[lane] = reinterpret_cast<const int*>(&w.seg0)[lane];
 		}
-		__syncthreads();
+	};
+	auto claim_next = [&](int buf) { // warp 0
+		unsigned nx = 0;
+		if (lane == 0)
+			nx = atomicAdd(&a.work_counter[0], 1u);
+		fetch(buf, int(gridDim.x + __shfl_sync(0xffffffffu, nx, 0)));
+	};
+
+	if (warp == 0)
+		fetch(0, int(blockIdx.x));
+	__syncthreads();
+	for (int cur = 0;; cur ^= 1) {
+		const int it = s_it[cur];
+		if (it >= a.n_items)
+			break;
+		const KronItem& w    = s_w[cur];
+		const GemmSeg*  sg   = s_seg[cur];
+		const int       nseg = w.seg_end - w.seg_begin;
 
 		if (w.kind == 0) {
-			tile::mma_tile<C>(acc, smem, a.ops, X, s_seg, 0, nseg, w.m0, w.n0, w.M, w.N);
+			tile::mma_tile<C>(acc, smem, a.ops, X, sg, 0, nseg, w.m0, w.n0, w.M, w.N);
+			if (warp == 0)
+				claim_next(cur ^ 1);
 			store_tile<C>(acc, a.bx + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
-			__syncthreads();
+			__syncthreads(); // tile stored; next descriptor visible
 			if (tid == 0) {
 				__threadfence();
 				atomicAdd(&a.done[w.producer], 1u);
 			}
-		} else {
-			if (tid == 0) {
-				int last_dep = -1;
-				for (int s = 0; s < nseg; ++s) {
-					const int j = s_seg[s].dep;
-					if (j == last_dep)
-						continue;
-					last_dep = j;
-					const unsigned target =
-					    unsigned(a.n1_of_j[j] + (j == 0 ? a.test_extra_wait : 0));
-					const unsigned long long t0 = globaltimer_ns();
-					while (ld_acquire(&a.done[j]) < target) {
-						if (ld_acquire(&a.work_counter[2]) != 0u)
-							break; // another wait already gave up
-						if (globaltimer_ns() - t0 > kWaitLimitNs) {
-							atomicExch(&a.work_counter[2], 1u);
-							*reinterpret_cast<volatile int*>(a.error) = 1;
-							__threadfence_system();
-							break;
-						}
-						__nanosleep(128);
+			continue;
+		}
+		// a pass-2 item blocks no other item: claim and fetch the next one
+		// now, behind this item's dependency wait and MMAs
+		if (warp == 0)
+			claim_next(cur ^ 1);
+		if (tid == 0) {
+			int last_dep = -1;
+			for (int s = 0; s < nseg; ++s) {
+				const int j = sg[s].dep;
+				if (j == last_dep)
+					continue;
+				last_dep = j;
+				const unsigned target = unsigned(a.n1_of_j[j] + (j == 0 ? a.test_extra_wait : 0));
+				const unsigned long long t0 = globaltimer_ns();
+				while (ld_acquire(&a.done[j]) < target) {
+					if (ld_acquire(&a.work_counter[2]) != 0u)
+						break; // another wait already gave up
+					if (globaltimer_ns() - t0 > kWaitLimitNs) {
+						atomicExch(&a.work_counter[2], 1u);
+						*reinterpret_cast<volatile int*>(a.error) = 1;
+						__threadfence_system();
+						break;
 					}
-				}
-			}
-			__syncthreads();
-			tile::mma_tile<C>(acc, smem, a.bx, a.ops, s_seg, 0, nseg, w.m0, w.n0, w.M, w.N);
-			if (w.kind == 1) {
-				store_tile<C>(acc, Y + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
-			} else {
-				// split part: partial tile to its slot, the last part reduces
-				constexpr int TE   = C::BM * C::BN;
-				double*       part = a.partial + (long long)(w.slot + w.part) * TE;
-#pragma unroll
-				for (int mi = 0; mi < C::MI; ++mi)
-#pragma unroll
-					for (int ni = 0; ni < C::NI; ++ni)
-#pragma unroll
-						for (int h = 0; h < 2; ++h)
-							part[tile::acc_col<C>(ni, h) * C::BM + tile::acc_row<C>(mi)]
-							    = acc.v[mi][ni][h];
-				__syncthreads();
-				if (tid == 0) {
-					__threadfence();
-					const unsigned old = atomicAdd(&a.arrive[w.tile], 1u);
-					s_last             = (old == unsigned(w.nsplit - 1));
-					if (s_last)
-						__threadfence();
-				}
-				__syncthreads();
-				if (s_last) {
-					const double* slots = a.partial + (long long)w.slot * TE;
-					double*       Cp    = Y + w.c_off;
-#pragma unroll
-					for (int mi = 0; mi < C::MI; ++mi)
-#pragma unroll
-						for (int ni = 0; ni < C::NI; ++ni)
-#pragma unroll
-							for (int h = 0; h < 2; ++h) {
-								const int r   = tile::acc_row<C>(mi);
-								const int c   = tile::acc_col<C>(ni, h);
-								const int e   = c * C::BM + r;
-								double    sum = __ldcg(slots + e);
-								for (int p = 1; p < w.nsplit; ++p)
-									sum += __ldcg(slots + (long long)p * TE + e);
-								const int row = w.m0 + r, col = w.n0 + c;
-								if (row < w.M && col < w.N)
-									Cp[(long long)col * w.ldc + row] = sum;
-							}
+					__nanosleep(128);
 				}
 			}
 		}
-		__syncthreads(); // everyone is done with s_w and s_seg
-		if (tid == 0)
-			s_next = int(gridDim.x + atomicAdd(&a.work_counter[0], 1u));
+		__syncthreads();
+		tile::mma_tile<C>(acc, smem, a.bx, a.ops, sg, 0, nseg, w.m0, w.n0, w.M, w.N);
+		if (w.kind == 1) {
+			store_tile<C>(acc, Y + w.c_off, w.ldc, w.m0, w.n0, w.M, w.N);
+			__syncthreads(); // next descriptor visible
+			continue;
+		}
+		// split part: partial tile to its slot, the last part reduces
+		constexpr int TE   = C::BM * C::BN;
+		double*       part = a.partial + (long long)(w.slot + w.part) * TE;
+#pragma unroll
+		for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+			for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+				for (int h = 0; h < 2; ++h)
+					part[tile::acc_col<C>(ni, h) * C::BM + tile::acc_row<C>(mi)] = acc.v[mi][ni][h];
+		__syncthreads();
+		if (tid == 0) {
+			__threadfence();
+			const unsigned old = atomicAdd(&a.arrive[w.tile], 1u);
+			s_last             = (old == unsigned(w.nsplit - 1));
+			if (s_last)
+				__threadfence();
+		}
+		__syncthreads();
+		if (s_last) {
+			const double* slots = a.partial + (long long)w.slot * TE;
+			double*       Cp    = Y + w.c_off;
+#pragma unroll
+			for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+				for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+					for (int h = 0; h < 2; ++h) {
+						const int r   = tile::acc_row<C>(mi);
+						const int c   = tile::acc_col<C>(ni, h);
+						const int e   = c * C::BM + r;
+						double    sum = __ldcg(slots + e);
+						for (int p = 1; p < w.nsplit; ++p)
+							sum += __ldcg(slots + (long long)p * TE + e);
+						const int row = w.m0 + r, col = w.n0 + c;
+						if (row < w.M && col < w.N)
+							Cp[(long long)col * w.ldc + row] = sum;
+					}
+		}
+		__syncthreads(); // s_last read by everyone before the next part may set it
 	}
 
 	// the last CTA out returns every counter to zero for the next launch
