@@ -98,3 +98,36 @@ def test_serving_batch_subset(cuda_lib, cuda_device):
         single.close()
         assert abs(e[s] - e1) <= 1e-11 * max(1.0, abs(e1)), (meta[s], e[s], e1)
     bg.close()
+
+
+def test_group_apply_in_tf32x3(cuda_lib, cuda_device, oracle_built):
+    """A group created in TF32x3: the union's tensor-core plan applies every
+    sector within the mixed-precision bar (2e-5) of the oracle."""
+    from dmrgpp_b200 import plugin
+    probs = mixed_sectors()
+    bg = plugin.BatchedGemm.from_problems(probs, precision=plugin.TF32X3)
+    offs = bg.sector_offsets()
+    x = np.random.default_rng(3).standard_normal(bg.dim)
+    y = bg(x)
+    for s, p in enumerate(probs):
+        ref = oracle_built.kron_apply(p, x[offs[s]:offs[s + 1]])
+        assert rel_err(y[offs[s]:offs[s + 1]], ref) < 2e-5, s
+    bg.close()
+
+
+def test_group_handle_as_one_sector_with_graph_replay(cuda_lib, cuda_device):
+    """The single-sector Lanczos on a group handle treats the union as one
+    block-diagonal sector: its lowest energy is the lowest over the sectors,
+    and the CUDA-graph form is bitwise identical to launch by launch."""
+    import torch
+    from dmrgpp_b200 import plugin
+    probs = [sb.random_problem(npatches=4, noperator=2, max_size=20, seed=s, symmetric=True)
+             for s in (5, 6, 7)]
+    bg = plugin.BatchedGemm.from_problems(probs)
+    init = torch.from_numpy(np.random.default_rng(9).standard_normal(bg.dim)).cuda()
+    e0, z0, n0 = bg.lanczos_lowest(init, steps=300, use_graph=False)
+    e1, z1, n1 = bg.lanczos_lowest(init, steps=300, use_graph=True)
+    assert e0 == e1 and n0 == n1 and torch.equal(z0, z1)
+    exact = min(np.linalg.eigvalsh(p.dense())[0] for p in probs)
+    assert abs(e0 - exact) <= 1e-10 * abs(exact)
+    bg.close()
