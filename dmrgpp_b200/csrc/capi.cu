@@ -6,6 +6,8 @@
 #include "handle.h"
 #include "tc_gemm.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -121,6 +123,21 @@ void pick_tile(const dmrgpp_kron_desc* d, int& bm, int& bn)
 	pick_tile_sizes(d->npatches, d->left_patch_size, d->right_patch_size, bm, bn);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// direct libcuda dependency)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	if (!fn) {
+		void*                           p = nullptr;
+		cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess
+		    && q == cudaDriverEntryPointSuccess)
+			fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+	}
+	return fn;
+}
+
 int check_desc(const dmrgpp_kron_desc* d)
 {
 	if (!d)
@@ -166,10 +183,11 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const S
 	if ((e = tc_split_x(X, h->m_xmap, h->m_xs_hi, h->m_xs_lo, h->plan.dim(), h->stream, io)))
 		return cuda_fail(h, e, "x split launch");
 	TcArgs a1 {};
-	a1.A_hi   = h->m_ops_hi;
-	a1.A_lo   = h->m_ops_lo;
-	a1.B_hi   = h->m_xs_hi;
-	a1.B_lo   = h->m_xs_lo;
+	const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(h->m_tmap);
+	a1.A_hi   = tm[0];
+	a1.A_lo   = tm[1];
+	a1.B_hi   = tm[2];
+	a1.B_lo   = tm[3];
 	a1.C_hi   = h->m_bxs_hi;
 	a1.C_lo   = h->m_bxs_lo;
 	a1.segs   = h->m_seg1;
@@ -182,10 +200,10 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const S
 	if ((e = tc_launch(a1, mp.bn, true, h->stream)))
 		return cuda_fail(h, e, "tensor-core pass 1 launch");
 	TcArgs a2 {};
-	a2.A_hi   = h->m_bxs_hi;
-	a2.A_lo   = h->m_bxs_lo;
-	a2.B_hi   = h->m_ops_hi;
-	a2.B_lo   = h->m_ops_lo;
+	a2.A_hi   = tm[4];
+	a2.A_lo   = tm[5];
+	a2.B_hi   = tm[6];
+	a2.B_lo   = tm[7];
 	a2.Cd     = Y;
 	a2.io     = io;
 	a2.segs   = h->m_seg2;
@@ -285,6 +303,35 @@ int build_mixed(dmrgpp_kron_handle h)
 			return cuda_fail(h, e, "pack mixed-precision operators");
 		}
 		cudaFree(d_jobs);
+	}
+	{
+		// the operand buffers as 2-D tensors [row][32 floats], 128-byte
+		// swizzle: pass 1 A = operators (128-row boxes), B = x split (bn);
+		// pass 2 A = BX split (128), B = operators (bn); hi and lo each
+		PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+		if (!encode)
+			return fail(h, DMRGPP_NOT_SUPPORTED, "cuTensorMapEncodeTiled is not available");
+		CUtensorMap* tm = reinterpret_cast<CUtensorMap*>(h->m_tmap);
+		struct Spec {
+			float*    buf;
+			long long elems;
+			int       box;
+		} spec[8] = { { h->m_ops_hi, mp.ops_elems, mp.bm }, { h->m_ops_lo, mp.ops_elems, mp.bm },
+		              { h->m_xs_hi, mp.xs_elems, mp.bn },   { h->m_xs_lo, mp.xs_elems, mp.bn },
+		              { h->m_bxs_hi, mp.bxs_elems, mp.bm }, { h->m_bxs_lo, mp.bxs_elems, mp.bm },
+		              { h->m_ops_hi, mp.ops_elems, mp.bn }, { h->m_ops_lo, mp.ops_elems, mp.bn } };
+		for (int q = 0; q < 8; ++q) {
+			const cuuint64_t dims[2]    = { 32, cuuint64_t(std::max<long long>(spec[q].elems / 32, 1)) };
+			const cuuint64_t strides[1] = { 128 };
+			const cuuint32_t box[2]     = { 32, cuuint32_t(spec[q].box) };
+			const cuuint32_t es[2]      = { 1, 1 };
+			const CUresult   r = encode(&tm[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, spec[q].buf, dims, strides,
+                                          box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+			if (r != CUDA_SUCCESS)
+				return fail(h, DMRGPP_CUDA_ERROR,
+				            "tensor map " + std::to_string(q) + " rejected (code " + std::to_string(int(r)) + ")");
+		}
 	}
 	if (!xmap.empty()
 	    && (e = cudaMemcpy(h->m_xmap, xmap.data(), xmap.size() * sizeof(int), cudaMemcpyHostToDevice)))

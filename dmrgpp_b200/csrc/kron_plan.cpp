@@ -592,9 +592,9 @@ std::string build_mixed_plan(KronPlan& plan, int bn, std::vector<float>* ops_hi,
 		if (mp.Mp[j] == 0)
 			continue;
 		GemmSeg s {};
-		s.a_off = mp.bs_off[j];
+		s.a_off = mp.bs_off[j] / 32;
 		s.lda   = int(mp.Mp[j]);
-		s.b_off = mp.xs_off[j];
+		s.b_off = mp.xs_off[j] / 32;
 		s.ldb   = int(round8(plan.l[j]));
 		s.K     = int(round32(plan.r[j]));
 		s.dep   = int(j);
@@ -609,9 +609,9 @@ std::string build_mixed_plan(KronPlan& plan, int bn, std::vector<float>* ops_hi,
 		for (; t < nt && plan.triples[t].i == int(i); ++t) {
 			const Triple& tr = plan.triples[t];
 			GemmSeg       s {};
-			s.a_off = mp.bxs_off[tr.j] + mp.group_row[t] * 32;
+			s.a_off = mp.bxs_off[tr.j] / 32 + mp.group_row[t];
 			s.lda   = int(mp.Mp[tr.j]);
-			s.b_off = mp.at_off[t];
+			s.b_off = mp.at_off[t] / 32;
 			s.ldb   = int(round8(plan.l[i]));
 			s.K     = int(round32(plan.l[tr.j]));
 			s.dep   = tr.j;

@@ -102,12 +102,15 @@ struct BlockRef {
 // Layout of the mixed-precision (tensor-core) form of a sector.  Every
 // operand is a "chunked K-major" matrix: rows padded to a multiple of 8 (Rp),
 // K padded to a multiple of 32 with zeros, stored chunk by chunk (32 K values
-// = 128 bytes per row), each chunk Rp rows x 128 bytes with the 16-byte
-// pieces of row r at position (piece ^ (r % 8)) -- the 128-byte swizzle that
-// tcgen05.mma reads through a shared-memory descriptor.  A 128-row tile of
-// one chunk is therefore one contiguous block, copied to shared memory by
-// one bulk copy.  Element (row, k) sits at chunked_offset(Rp, row, k).  Every
-// operand has a hi and a lo TF32 part of identical layout; offsets are floats.
+// = 128 bytes per row, Rp rows per chunk): element (row, k) at
+// chunked_offset(Rp, row, k).  Each operand buffer (packed operators, x
+// split, BX split; hi and lo parts separately) is one 2-D tensor of the
+// Tensor Memory Accelerator, [row][32 values], so rows (row0 .. row0 + box)
+// of chunk c of a matrix are buffer rows (off/32 + c Rp + row0 ..): one
+// tiled TMA load, written into shared memory with the 128-byte swizzle
+// tcgen05.mma reads.  Rows of a tile past its matrix come from the next
+// data in the buffer (or zeros past the buffer's end) and only feed
+// discarded outputs.  Offsets are floats, multiples of 256.
 //   pass 1: A = Bstack_j (Mp_j rows: the (i,k) groups, each r_i rows padded
 //               to 8, at group_row[t]), K = r_j
 //           B = X_j split (Lp_j = round8(l_j) rows), K = r_j
@@ -115,14 +118,14 @@ struct BlockRef {
 //   pass 2: A = the (i,k) group of BX_j, K = l_j
 //           B = A_k(i,j)^T (round8(l_i) rows), K = l_j
 //           C = Y_i, FP64 column-major
-// GemmSeg of the mixed passes: a_off/b_off = float offset of the tile row 0
-// in chunk 0, lda/ldb = padded rows of the containing matrix (the chunk
-// stride is 32 times that), K = K padded to 32.  GemmTile: ldc = padded rows
-// of BX_j (pass 1) or r_i (pass 2).
+// GemmSeg of the mixed passes: a_off/b_off = buffer row of the matrix's
+// chunk 0, row of the tile's row 0; lda/ldb = Rp (rows from one chunk to the
+// next); K = K padded to 32.  GemmTile: ldc = padded rows of BX_j (pass 1)
+// or r_i (pass 2).
 inline long long round8(long long x) { return (x + 7) / 8 * 8; }
 inline long long chunked_offset(long long rows_pad, long long row, long long k)
 {
-	return (k >> 5) * rows_pad * 32 + row * 32 + ((((k >> 2) & 7) ^ (row & 7)) << 2) + (k & 3);
+	return (k >> 5) * rows_pad * 32 + row * 32 + (k & 31);
 }
 
 struct MixedPlan {

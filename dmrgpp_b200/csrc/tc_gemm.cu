@@ -9,12 +9,13 @@
 // runs balanced on the host by balance_tiles):
 //   warp 0, one thread: producer.  For every 32-wide k-chunk of every
 //     K-segment of its tiles it waits until the ring stage is free, arms the
-//     stage's mbarrier with the byte count and issues four bulk copies
-//     (cp.async.bulk, global -> shared, completion counted on the mbarrier):
-//     the hi and lo parts of the A tile (128 rows) and of the B tile (BN
-//     rows).  The operands are stored chunked and pre-swizzled
-//     (MixedPlan), so each copy is one contiguous block that lands in the
-//     128-byte-swizzled K-major layout tcgen05.mma reads.
+//     stage's mbarrier with the byte count and issues four tiled TMA loads
+//     (cp.async.bulk.tensor.3d, completion counted on the mbarrier): the hi
+//     and lo parts of the A tile (128 rows) and of the B tile (BN rows).
+//     Every operand buffer is a 2-D tensor [row][32 values] (kron_plan.h;
+//     the tensor maps are kernel parameters); the TMA unit writes the tile
+//     in the 128-byte-swizzled K-major layout tcgen05.mma reads.  The x
+//     coordinate is always 0.
 //   warp 1, one thread: MMA issuer.  Per chunk it waits for the stage's
 //     bytes, issues 3 x 4 MMAs (M = 128, N = BN, K = 8) into the tile's TMEM
 //     accumulator and commits them to the stage's "empty" mbarrier; after
@@ -97,13 +98,13 @@ __device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity, const 
 	}
 }
 
-// bulk copy global -> this CTA's shared memory, completion counted in bytes
-// on the mbarrier (16-byte aligned addresses, size a multiple of 16)
-__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned mbar)
+// tiled TMA load of box (0, row) of a 2-D tensor into this CTA's shared
+// memory, completion counted in bytes on the mbarrier
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int row, unsigned mbar)
 {
-	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-	                 dst),
-	             "l"(src), "r"(bytes), "r"(mbar)
+	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+	             "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+	             "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(row), "r"(mbar)
 	             : "memory");
 }
 
@@ -167,8 +168,6 @@ __device__ __forceinline__ float tf32_rna(float f)
 	return __uint_as_float(u);
 }
 
-__device__ __forceinline__ int round8_dev(int x) { return (x + 7) & ~7; }
-
 template <int BN> struct TcLayout {
 	static constexpr int A_BYTES     = kBM * 128;
 	static constexpr int B_BYTES     = BN * 128;
@@ -197,17 +196,15 @@ __device__ void producer(const TcArgs& a, unsigned base, unsigned full0, unsigne
 	using L    = TcLayout<BN>;
 	unsigned g = 0; // chunks issued
 	bool     ok = true;
+	// a tiled load moves its whole box (rows past the buffer arrive as 0)
+	constexpr unsigned kStageTx = 2u * unsigned(L::A_BYTES + L::B_BYTES);
 	for (int ti = a.starts[blockIdx.x]; ti < a.starts[blockIdx.x + 1] && ok; ++ti) {
-		const GemmTile t     = a.tiles[ti];
-		const int      rowsA = min(kBM, round8_dev(t.M) - t.m0);
-		const int      rowsB = min(BN, round8_dev(t.N) - t.n0);
-		const unsigned ba = unsigned(rowsA) * 128u, bb = unsigned(rowsB) * 128u;
+		const GemmTile t = a.tiles[ti];
 		for (int s = t.seg_begin; s < t.seg_end && ok; ++s) {
-			const GemmSeg   sg = a.segs[s];
-			const int       nk = sg.K / kBK;
-			const long long ao = sg.a_off + (long long)t.m0 * kBK;
-			const long long bo = sg.b_off + (long long)t.n0 * kBK;
-			const long long as = (long long)sg.lda * kBK, bs = (long long)sg.ldb * kBK;
+			const GemmSeg sg   = a.segs[s];
+			const int     nk   = sg.K / kBK;
+			const int     arow = int(sg.a_off) + t.m0; // buffer row of chunk 0
+			const int     brow = int(sg.b_off) + t.n0;
 			for (int c = 0; c < nk; ++c) {
 				const unsigned st = g % STAGES;
 				if (g >= STAGES && !mbar_wait(empty0 + 8 * st, ((g / STAGES) - 1) & 1, abort)) {
@@ -222,11 +219,12 @@ __device__ void producer(const TcArgs& a, unsigned base, unsigned full0, unsigne
 					++g;
 					continue;
 				}
-				mbar_expect_tx(fb, 2 * (ba + bb));
-				bulk_g2s(sa, a.A_hi + ao + c * as, ba, fb);
-				bulk_g2s(sa + L::A_BYTES, a.A_lo + ao + c * as, ba, fb);
-				bulk_g2s(sa + 2 * L::A_BYTES, a.B_hi + bo + c * bs, bb, fb);
-				bulk_g2s(sa + 2 * L::A_BYTES + L::B_BYTES, a.B_lo + bo + c * bs, bb, fb);
+				mbar_expect_tx(fb, kStageTx);
+				const int ya = arow + c * sg.lda, yb = brow + c * sg.ldb;
+				tma_load_2d(sa, &a.A_hi, ya, fb);
+				tma_load_2d(sa + L::A_BYTES, &a.A_lo, ya, fb);
+				tma_load_2d(sa + 2 * L::A_BYTES, &a.B_hi, yb, fb);
+				tma_load_2d(sa + 2 * L::A_BYTES + L::B_BYTES, &a.B_lo, yb, fb);
 				++g;
 			}
 		}
@@ -312,6 +310,7 @@ __device__ __forceinline__ void store_chunk(const TcArgs& a, const GemmTile& t, 
 		// one 128-byte row of chunk col0 / 32 of BX_j (hi and lo); columns
 		// past N are the K padding of pass 2 and must be zero
 		const long long o  = t.c_off + (long long)(col0 >> 5) * t.ldc * kBK + (long long)grow * kBK;
+		// rows of one chunk are 128 bytes apart: a warp stores 4 KB contiguously
 		float*          hi = a.C_hi + o;
 		float*          lo = a.C_lo + o;
 #pragma unroll
@@ -323,9 +322,8 @@ __device__ __forceinline__ void store_chunk(const TcArgs& a, const GemmTile& t, 
 				hv[e]         = tf32_rna(x);
 				lv[e]         = tf32_rna(x - hv[e]);
 			}
-			const int pos                          = (q ^ (grow & 7)) << 2;
-			*reinterpret_cast<float4*>(hi + pos) = make_float4(hv[0], hv[1], hv[2], hv[3]);
-			*reinterpret_cast<float4*>(lo + pos) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+			*reinterpret_cast<float4*>(hi + 4 * q) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+			*reinterpret_cast<float4*>(lo + 4 * q) = make_float4(lv[0], lv[1], lv[2], lv[3]);
 		}
 	} else {
 		double* y = (a.io ? a.io->y : a.Cd) + t.c_off;
@@ -471,7 +469,7 @@ __device__ void epilogue(const TcArgs& a, unsigned tmem, unsigned accf0, unsigne
 }
 
 template <int BN, int STAGES, bool PASS1>
-__global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_tf32x3_kernel(TcArgs a)
+__global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_tf32x3_kernel(const __grid_constant__ TcArgs a)
 {
 	extern __shared__ unsigned char smem_raw[];
 	__shared__ __align__(8) unsigned long long bars[2 * STAGES + 5];
@@ -559,8 +557,7 @@ pack_tf32_kernel(const double* __restrict__ ops, float* __restrict__ hi, float* 
 		const double    v   = ops[j.src + q + (long long)c * j.ld];
 		const long long row = j.swap ? c : j.row0 + q;
 		const long long k   = j.swap ? q : c;
-		const long long d   = j.dst + (k >> 5) * (long long)j.dst_rows * 32 + row * 32
-		    + ((((k >> 2) & 7) ^ (row & 7)) << 2) + (k & 3);
+		const long long d   = j.dst + (k >> 5) * (long long)j.dst_rows * 32 + row * 32 + (k & 31);
 		const float h = tf32_rna(float(v));
 		hi[d]         = h;
 		lo[d]         = tf32_rna(float(v - double(h)));

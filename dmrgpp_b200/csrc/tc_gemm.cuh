@@ -3,15 +3,15 @@
 
 #include "kron_plan.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace dmrgpp {
 
 struct TcArgs {
-	const float*    A_hi; // base of the pass's A operands (hi part)
-	const float*    A_lo;
-	const float*    B_hi;
-	const float*    B_lo;
+	// the pass's operand buffers as 2-D TMA tensors [row][32 floats]
+	// (kron_plan.h): A with 128-row boxes, B with BN-row boxes; hi and lo
+	CUtensorMap A_hi, A_lo, B_hi, B_lo;
 	float*          C_hi; // pass 1: K-major split output
 	float*          C_lo;
 	double*         Cd;   // pass 2: FP64 column-major output

@@ -1,11 +1,12 @@
 // Host emulation of the TF32x3 tensor-core passes over the chunked,
 // pre-swizzled operand layout that build_mixed_plan produces.  Checks, on
 // the CPU, what the kernel in tc_gemm.cu relies on:
-//   * every bulk copy the producer would issue (A and B tiles of every
-//     k-chunk of every segment) starts 16-byte aligned, has a size that is a
-//     multiple of 16 bytes and lies inside its operand buffer;
-//   * copies that start on a 128-row tile row 0 start on an 8-row swizzle
-//     group, so the pre-swizzled rows land where the descriptor expects them;
+//   * every operand buffer is a whole number of 128-byte rows (a 2-D TMA
+//     tensor); every tiled TMA load the producer would issue (A and B tiles
+//     of every k-chunk of every segment) starts inside its buffer at an int
+//     row, and the valid output rows and columns read rows of one chunk of
+//     their own matrix (rows past the buffer arrive as zeros, as the TMA unit
+//     fills them);
 //   * the per-CTA tile runs (balance_tiles) are a permutation of the tiles;
 //   * K-split pass-2 tiles: slots in range, every part present, the parts'
 //     sums are the tile's output;
@@ -13,12 +14,13 @@
 //     packing bit for bit;
 //   * the epilogue's stores stay inside their buffers;
 //   * pass 1 + pass 2 computed from these buffers (hi*hi + hi*lo + lo*hi in
-//     double, stale rows included as NaN) reproduce the FP64 H*x.
+//     double) reproduce the FP64 H*x.
 // Usage: mixed_layout_check seed npatches noperator max_size bn
 // Prints "ok <max relative error>" or "FAIL <reason>" (exit code 1).
 #include "kron_plan.h"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -177,47 +179,41 @@ int main(int argc, char** argv)
 	std::map<long long, double>      split_sum;
 	std::map<int, std::set<int>>     split_parts;
 	std::map<int, int>               split_n;
-	auto check_copy = [&](const Buf& b, long long off, long long rows) -> bool {
-		const long long bytes = rows * 128;
-		return off >= 0 && (off * 4) % 16 == 0 && bytes % 16 == 0 && bytes > 0
-		    && off + rows * 32 <= b.n;
-	};
-	// emulate one pass; returns 0 on success
+	// emulate one pass: every operand buffer is a 2-D TMA tensor
+	// [row][32 floats]; a load of `box` rows from buffer row y reads rows
+	// y .. y + box - 1 (zeros past the buffer's end).  Returns 0 on success.
 	auto pass = [&](const std::vector<GemmSeg>& segs, const std::vector<GemmTile>& tiles, Buf Ab,
 	                Buf Bb, bool pass1) -> int {
+		if (Ab.n % 32 != 0 || Bb.n % 32 != 0)
+			return fail("buffer not a whole number of rows", Ab.n, Bb.n);
+		const long long arows = Ab.n / 32, brows = Bb.n / 32;
 		std::vector<double> acc(size_t(BM) * bn);
 		for (const GemmTile& t : tiles) {
-			const int rowsA = std::min<int>(BM, int(round8(t.M)) - t.m0);
-			const int rowsB = std::min<int>(bn, int(round8(t.N)) - t.n0);
-			if (rowsA <= 0 || rowsB <= 0)
-				return fail("empty copy", rowsA, rowsB);
 			std::fill(acc.begin(), acc.end(), 0.0);
 			int chunks = 0;
 			for (int s = t.seg_begin; s < t.seg_end; ++s) {
 				const GemmSeg& g = segs[size_t(s)];
-				if (g.K % 32 != 0 || g.a_off % 8 != 0 || g.b_off % 8 != 0)
-					return fail("segment alignment", g.K, g.a_off);
+				if (g.K % 32 != 0 || g.lda <= 0 || g.ldb <= 0 || g.lda % 8 != 0 || g.ldb % 8 != 0)
+					return fail("segment fields", g.K, g.lda);
+				// the tile's valid rows stay inside one chunk of its matrix
+				if (t.m0 + std::min(BM, t.M - t.m0) > g.lda || t.n0 + std::min(bn, t.N - t.n0) > g.ldb)
+					return fail("valid rows past the matrix", g.lda, g.ldb);
 				for (int c = 0; c < g.K / 32; ++c, ++chunks) {
-					const long long ao = g.a_off + (long long)t.m0 * 32 + (long long)c * g.lda * 32;
-					const long long bo = g.b_off + (long long)t.n0 * 32 + (long long)c * g.ldb * 32;
-					if (!check_copy(Ab, ao, rowsA) || !check_copy(Bb, bo, rowsB))
-						return fail("copy out of bounds", ao, bo);
-					// shared-memory image: fresh rows, stale (NaN) rows beyond
+					const long long ya = g.a_off + t.m0 + (long long)c * g.lda;
+					const long long yb = g.b_off + t.n0 + (long long)c * g.ldb;
+					if (ya < 0 || yb < 0 || ya > INT_MAX || yb > INT_MAX || ya >= arows || yb >= brows)
+						return fail("tile row outside its buffer", ya, yb);
+					auto val = [&](const Buf& b, long long nrows, long long row, int k, bool hi) -> double {
+						if (row >= nrows)
+							return 0.0; // TMA out-of-bounds fill
+						return hi ? b.hi[row * 32 + k] : b.lo[row * 32 + k];
+					};
 					for (int m = 0; m < BM; ++m)
 						for (int n = 0; n < bn; ++n) {
-							if (m >= rowsA || n >= rowsB) {
-								if (m < t.M - t.m0 && n < t.N - t.n0)
-									return fail("valid output reads a stale row", m, n);
-								acc[size_t(m) * bn + n] = std::nan("");
-								continue;
-							}
 							double sum = 0;
 							for (int k = 0; k < 32; ++k) {
-								// swizzled position inside the copied block
-								const long long pa = ao + m * 32 + ((((k >> 2) ^ (m & 7)) << 2) | (k & 3));
-								const long long pb = bo + n * 32 + ((((k >> 2) ^ (n & 7)) << 2) | (k & 3));
-								const double    ah = Ab.hi[pa], al = Ab.lo[pa];
-								const double    bh = Bb.hi[pb], bl = Bb.lo[pb];
+								const double ah = val(Ab, arows, ya + m, k, true), al = val(Ab, arows, ya + m, k, false);
+								const double bh = val(Bb, brows, yb + n, k, true), bl = val(Bb, brows, yb + n, k, false);
 								sum += ah * bh + ah * bl + al * bh;
 							}
 							acc[size_t(m) * bn + n] += sum;
@@ -235,7 +231,7 @@ int main(int argc, char** argv)
 						const double v    = chunks ? acc[size_t(m) * bn + c0 + e] : 0.0;
 						if (pass1) {
 							const long long o = t.c_off + (long long)(col0 >> 5) * t.ldc * 32
-							    + (long long)grow * 32 + ((((e >> 2) ^ (grow & 7)) << 2) | (e & 3));
+							    + (long long)grow * 32 + e;
 							if (o < 0 || o >= mp.bxs_elems)
 								return fail("BX store out of bounds", o, mp.bxs_elems);
 							float h, lo;
