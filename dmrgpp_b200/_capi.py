@@ -48,6 +48,9 @@ SIGNATURES = {
     "dmrgpp_kron_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dmrgpp_kron_test_stall_dependency": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dmrgpp_kron_flops": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "dmrgpp_kron_setup_profile": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    "dmrgpp_release_cached_memory": (ctypes.c_int, [ctypes.c_int]),
+    "dmrgpp_cached_memory": (ctypes.c_int, [ctypes.c_int, _szp, _szp]),
     "dmrgpp_kron_plan_info_get": (ctypes.c_int, [ctypes.POINTER(KronDesc),
                                                  ctypes.POINTER(PlanInfo)]),
     "dmrgpp_kron_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),

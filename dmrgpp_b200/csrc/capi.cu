@@ -3,6 +3,7 @@
 #include "kron_gemm.cuh"
 #include "kron_persistent.cuh"
 #include "kron_plan.h"
+#include "devmem.h"
 #include "handle.h"
 #include "tc_gemm.cuh"
 
@@ -11,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cstring>
 #include <new>
@@ -68,31 +70,31 @@ void release(dmrgpp_kron_handle h)
 	dmrgpp::release_lanczos(h);
 	dmrgpp::release_davidson(h);
 	dmrgpp::release_group(h);
-	cudaFree(h->d_diag);
+	dmrgpp::dev_free(h->d_diag);
 	h->d_diag = nullptr;
-	cudaFree(h->m_ops_hi);
-	cudaFree(h->m_ops_lo);
-	cudaFree(h->m_xs_hi);
-	cudaFree(h->m_xs_lo);
-	cudaFree(h->m_bxs_hi);
-	cudaFree(h->m_bxs_lo);
-	cudaFree(h->m_xmap);
-	cudaFree(h->m_lists);
-	cudaFree(h->m_partial);
-	cudaFree(h->m_arrive);
+	dmrgpp::dev_free(h->m_ops_hi);
+	dmrgpp::dev_free(h->m_ops_lo);
+	dmrgpp::dev_free(h->m_xs_hi);
+	dmrgpp::dev_free(h->m_xs_lo);
+	dmrgpp::dev_free(h->m_bxs_hi);
+	dmrgpp::dev_free(h->m_bxs_lo);
+	dmrgpp::dev_free(h->m_xmap);
+	dmrgpp::dev_free(h->m_lists);
+	dmrgpp::dev_free(h->m_partial);
+	dmrgpp::dev_free(h->m_arrive);
 	h->m_partial = nullptr;
 	h->m_arrive  = nullptr;
 	h->m_ops_hi = h->m_ops_lo = h->m_xs_hi = h->m_xs_lo = h->m_bxs_hi = h->m_bxs_lo = nullptr;
 	h->m_xmap   = nullptr;
 	h->m_lists  = nullptr;
 	h->mixed_ready = false;
-	cudaFree(h->d_ops);
-	cudaFree(h->d_bx);
-	cudaFree(h->d_x);
-	cudaFree(h->d_y);
-	cudaFree(h->d_lists);
-	cudaFree(h->d_ctr);
-	cudaFree(h->d_part);
+	dmrgpp::dev_free(h->d_ops);
+	dmrgpp::dev_free(h->d_bx);
+	dmrgpp::dev_free(h->d_x);
+	dmrgpp::dev_free(h->d_y);
+	dmrgpp::dev_free(h->d_lists);
+	dmrgpp::dev_free(h->d_ctr);
+	dmrgpp::dev_free(h->d_part);
 	if (h->err_host)
 		cudaFreeHost(h->err_host);
 	h->err_host = h->err_dev = nullptr;
@@ -275,17 +277,17 @@ int build_mixed(dmrgpp_kron_handle h)
 	h->m_grid1 = balance_tiles(mpw.tile1, mpw.seg1, sms, starts1);
 	h->m_grid2 = balance_tiles(mpw.tile2, mpw.seg2, sms, starts2);
 	auto fbytes = [](long long n) { return size_t(n > 0 ? n : 1) * sizeof(float); };
-	if ((e = cudaMalloc(&h->m_ops_hi, fbytes(mp.ops_elems))) || (e = cudaMalloc(&h->m_ops_lo, fbytes(mp.ops_elems)))
-	    || (e = cudaMalloc(&h->m_xs_hi, fbytes(mp.xs_elems))) || (e = cudaMalloc(&h->m_xs_lo, fbytes(mp.xs_elems)))
-	    || (e = cudaMalloc(&h->m_bxs_hi, fbytes(mp.bxs_elems)))
-	    || (e = cudaMalloc(&h->m_bxs_lo, fbytes(mp.bxs_elems)))
-	    || (e = cudaMalloc(&h->m_xmap, size_t(std::max<long long>(h->plan.dim(), 1)) * sizeof(int))))
-		return cuda_fail(h, e, "cudaMalloc(mixed-precision buffers)");
+	if ((e = dmrgpp::dev_malloc(&h->m_ops_hi, fbytes(mp.ops_elems))) || (e = dmrgpp::dev_malloc(&h->m_ops_lo, fbytes(mp.ops_elems)))
+	    || (e = dmrgpp::dev_malloc(&h->m_xs_hi, fbytes(mp.xs_elems))) || (e = dmrgpp::dev_malloc(&h->m_xs_lo, fbytes(mp.xs_elems)))
+	    || (e = dmrgpp::dev_malloc(&h->m_bxs_hi, fbytes(mp.bxs_elems)))
+	    || (e = dmrgpp::dev_malloc(&h->m_bxs_lo, fbytes(mp.bxs_elems)))
+	    || (e = dmrgpp::dev_malloc(&h->m_xmap, size_t(std::max<long long>(h->plan.dim(), 1)) * sizeof(int))))
+		return cuda_fail(h, e, "device allocation (mixed-precision buffers)");
 	// K-split pass-2 tiles: FP32 partial slots and self-resetting counters
-	if ((e = cudaMalloc(&h->m_partial, fbytes(mp.split_slots * 128 * mp.bn)))
-	    || (e = cudaMalloc(&h->m_arrive, size_t(std::max(mp.n_split_tiles, 1)) * sizeof(unsigned)))
+	if ((e = dmrgpp::dev_malloc(&h->m_partial, fbytes(mp.split_slots * 128 * mp.bn)))
+	    || (e = dmrgpp::dev_malloc(&h->m_arrive, size_t(std::max(mp.n_split_tiles, 1)) * sizeof(unsigned)))
 	    || (e = cudaMemset(h->m_arrive, 0, size_t(std::max(mp.n_split_tiles, 1)) * sizeof(unsigned))))
-		return cuda_fail(h, e, "cudaMalloc(split-K partials)");
+		return cuda_fail(h, e, "device allocation (split-K partials)");
 	// K padding must read as zero
 	if ((e = cudaMemset(h->m_xs_hi, 0, fbytes(mp.xs_elems))) || (e = cudaMemset(h->m_xs_lo, 0, fbytes(mp.xs_elems)))
 	    || (e = cudaMemset(h->m_bxs_hi, 0, fbytes(mp.bxs_elems)))
@@ -295,14 +297,14 @@ int build_mixed(dmrgpp_kron_handle h)
 		const std::vector<PackJob> jobs = mixed_pack_jobs(h->plan);
 		PackJob* d_jobs = nullptr;
 		if ((e = cudaMemset(h->m_ops_hi, 0, fbytes(mp.ops_elems))) || (e = cudaMemset(h->m_ops_lo, 0, fbytes(mp.ops_elems)))
-		    || (e = cudaMalloc(&d_jobs, std::max<size_t>(jobs.size(), 1) * sizeof(PackJob)))
+		    || (e = dmrgpp::dev_malloc(&d_jobs, std::max<size_t>(jobs.size(), 1) * sizeof(PackJob)))
 		    || (e = cudaMemcpy(d_jobs, jobs.data(), jobs.size() * sizeof(PackJob), cudaMemcpyHostToDevice))
 		    || (e = tc_pack_ops(h->d_ops, h->m_ops_hi, h->m_ops_lo, d_jobs, int(jobs.size()), h->stream))
 		    || (e = cudaStreamSynchronize(h->stream))) {
-			cudaFree(d_jobs);
+			dmrgpp::dev_free(d_jobs);
 			return cuda_fail(h, e, "pack mixed-precision operators");
 		}
-		cudaFree(d_jobs);
+		dmrgpp::dev_free(d_jobs);
 	}
 	{
 		// the operand buffers as 2-D tensors [row][32 floats], 128-byte
@@ -350,8 +352,8 @@ int build_mixed(dmrgpp_kron_handle h)
 	add(mp.tile2.data(), mp.tile2.size() * sizeof(GemmTile));
 	add(starts1.data(), starts1.size() * sizeof(int));
 	add(starts2.data(), starts2.size() * sizeof(int));
-	if ((e = cudaMalloc(&h->m_lists, lists.empty() ? 16 : lists.size())))
-		return cuda_fail(h, e, "cudaMalloc(mixed lists)");
+	if ((e = dmrgpp::dev_malloc(&h->m_lists, lists.empty() ? 16 : lists.size())))
+		return cuda_fail(h, e, "device allocation (mixed lists)");
 	auto at    = [&](int i) { return static_cast<unsigned char*>(h->m_lists) + offs[i]; };
 	h->m_seg1  = reinterpret_cast<GemmSeg*>(at(0));
 	h->m_seg2  = reinterpret_cast<GemmSeg*>(at(1));
@@ -411,14 +413,14 @@ int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 		}
 	}
 	add(item_sector.data(), item_sector.size() * sizeof(int));
-	cudaFree(h->d_lists);
-	cudaFree(h->d_ctr);
-	cudaFree(h->d_part);
+	dmrgpp::dev_free(h->d_lists);
+	dmrgpp::dev_free(h->d_ctr);
+	dmrgpp::dev_free(h->d_part);
 	h->d_lists = nullptr;
 	h->d_ctr   = nullptr;
 	h->d_part  = nullptr;
-	if ((e = cudaMalloc(&h->d_lists, lists.empty() ? 16 : lists.size())))
-		return cuda_fail(h, e, "cudaMalloc(lists)");
+	if ((e = dmrgpp::dev_malloc(&h->d_lists, lists.empty() ? 16 : lists.size())))
+		return cuda_fail(h, e, "device allocation (lists)");
 	auto at    = [&](int i) { return static_cast<unsigned char*>(h->d_lists) + offs[i]; };
 	h->d_seg1  = reinterpret_cast<GemmSeg*>(at(0));
 	h->d_seg2  = reinterpret_cast<GemmSeg*>(at(1));
@@ -433,13 +435,13 @@ int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 		return cuda_fail(h, e, "upload lists");
 
 	const size_t nctr = 3 + P.np + size_t(P.n_split_tiles);
-	if ((e = cudaMalloc(&h->d_ctr, nctr * sizeof(unsigned))))
-		return cuda_fail(h, e, "cudaMalloc(counters)");
+	if ((e = dmrgpp::dev_malloc(&h->d_ctr, nctr * sizeof(unsigned))))
+		return cuda_fail(h, e, "device allocation (counters)");
 	if ((e = cudaMemset(h->d_ctr, 0, nctr * sizeof(unsigned))))
 		return cuda_fail(h, e, "clear counters");
 	const size_t part_elems = size_t(P.partial_slots) * size_t(tile) * size_t(tile);
-	if ((e = cudaMalloc(&h->d_part, (part_elems ? part_elems : 1) * sizeof(double))))
-		return cuda_fail(h, e, "cudaMalloc(partials)");
+	if ((e = dmrgpp::dev_malloc(&h->d_part, (part_elems ? part_elems : 1) * sizeof(double))))
+		return cuda_fail(h, e, "device allocation (partials)");
 	return DMRGPP_OK;
 }
 
@@ -450,8 +452,17 @@ namespace {
 // Device side of a new handle whose plan (with host blocks) is built: device
 // buffers, persistent schedule, diagonal, and the TF32x3 form if requested.
 // Frees h on failure.
-int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm,
-                  const dmrgpp::PackBuffer& pack, dmrgpp_kron_handle* out)
+using Clock = std::chrono::steady_clock;
+
+double seconds_since(Clock::time_point t0)
+{
+	return std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+// t0: when create started (before the plan); the plan's time is recorded by
+// the caller in h->setup_times[DMRGPP_SETUP_PLAN]
+int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm, Clock::time_point t0,
+                  dmrgpp_kron_handle* out)
 {
 	if (device >= 0) {
 		h->device = device;
@@ -475,16 +486,17 @@ int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm,
 	// NULL is the CUDA default stream, as for cuBLAS handles
 	h->stream = static_cast<cudaStream_t>(stream);
 
+	auto         tp  = Clock::now();
 	const auto&  P   = h->plan;
 	const size_t dim = size_t(P.dim());
-	if ((e = cudaMalloc(&h->d_ops, size_t(P.op_elems ? P.op_elems : 1) * sizeof(double))))
-		return bail(e, "cudaMalloc(operators)");
-	if ((e = cudaMalloc(&h->d_bx, size_t(P.bx_elems ? P.bx_elems : 1) * sizeof(double))))
-		return bail(e, "cudaMalloc(BX)");
-	if ((e = cudaMalloc(&h->d_x, dim * sizeof(double))))
-		return bail(e, "cudaMalloc(x)");
-	if ((e = cudaMalloc(&h->d_y, dim * sizeof(double))))
-		return bail(e, "cudaMalloc(y)");
+	if ((e = dmrgpp::dev_malloc(&h->d_ops, size_t(P.op_elems ? P.op_elems : 1) * sizeof(double))))
+		return bail(e, "device allocation (operators)");
+	if ((e = dmrgpp::dev_malloc(&h->d_bx, size_t(P.bx_elems ? P.bx_elems : 1) * sizeof(double))))
+		return bail(e, "device allocation (BX)");
+	if ((e = dmrgpp::dev_malloc(&h->d_x, dim * sizeof(double))))
+		return bail(e, "device allocation (x)");
+	if ((e = dmrgpp::dev_malloc(&h->d_y, dim * sizeof(double))))
+		return bail(e, "device allocation (y)");
 
 	if ((e = cudaHostAlloc(reinterpret_cast<void**>(&h->err_host), sizeof(int), cudaHostAllocMapped)))
 		return bail(e, "cudaHostAlloc(error word)");
@@ -497,18 +509,24 @@ int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm,
 		delete h;
 		return fail(nullptr, rc, why);
 	}
-	if (!pack.empty()
-	    && (e = cudaMemcpy(h->d_ops, pack.data(), pack.size() * sizeof(double), cudaMemcpyHostToDevice)))
-		return bail(e, "upload operators");
-	{
-		std::vector<double> diag;
-		dmrgpp::sector_diagonal(h->plan, diag);
-		if ((e = cudaMalloc(&h->d_diag, std::max<size_t>(diag.size(), 1) * sizeof(double))))
-			return bail(e, "cudaMalloc(diagonal)");
-		if (!diag.empty()
-		    && (e = cudaMemcpy(h->d_diag, diag.data(), diag.size() * sizeof(double), cudaMemcpyHostToDevice)))
-			return bail(e, "upload diagonal");
+	h->setup_times[DMRGPP_SETUP_ALLOC] = seconds_since(tp);
+	tp                                 = Clock::now();
+	if (int rc = dmrgpp::upload_operators(h, &h->setup_times[DMRGPP_SETUP_UPLOAD_FILL])) {
+		const std::string why = h->err;
+		release(h);
+		delete h;
+		return fail(nullptr, rc, why);
 	}
+	h->setup_times[DMRGPP_SETUP_UPLOAD] = seconds_since(tp);
+	tp                                  = Clock::now();
+	if (int rc = dmrgpp::upload_diagonal(h)) {
+		const std::string why = h->err;
+		release(h);
+		delete h;
+		return fail(nullptr, rc, why);
+	}
+	h->setup_times[DMRGPP_SETUP_DIAGONAL] = seconds_since(tp);
+	tp                                    = Clock::now();
 	if (h->precision == DMRGPP_TF32X3) {
 		if (int rc = dmrgpp::build_mixed(h)) {
 			const std::string why = h->err;
@@ -516,7 +534,9 @@ int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm,
 			delete h;
 			return fail(nullptr, rc, why);
 		}
+		h->setup_times[DMRGPP_SETUP_MIXED] = seconds_since(tp);
 	}
+	h->setup_times[DMRGPP_SETUP_TOTAL] = seconds_since(t0);
 	// the caller's host blocks are not referenced after create
 	h->plan.blocks.clear();
 	h->plan.blocks.shrink_to_fit();
@@ -533,6 +553,17 @@ const char* dmrgpp_version(void) { return DMRGPP_VERSION_STRING; }
 const char* dmrgpp_kron_last_error(dmrgpp_kron_handle h)
 {
 	return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int dmrgpp_kron_setup_profile(dmrgpp_kron_handle h, double* t, size_t n)
+{
+	if (!h || (!t && n))
+		return fail(h, DMRGPP_INVALID_ARG, "null argument");
+	if (n > DMRGPP_SETUP_NPHASES)
+		return fail(h, DMRGPP_INVALID_ARG, "at most DMRGPP_SETUP_NPHASES phases");
+	for (size_t q = 0; q < n; ++q)
+		t[q] = h->setup_times[q];
+	return DMRGPP_OK;
 }
 
 int dmrgpp_kron_plan_info_get(const dmrgpp_kron_desc* d, dmrgpp_kron_plan_info* info)
@@ -583,9 +614,9 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 		return fail(nullptr, DMRGPP_OOM, "host allocation failed");
 	h->precision = d->precision;
 
-	int bm, bn;
+	const auto t0 = Clock::now();
+	int        bm, bn;
 	pick_tile(d, bm, bn);
-	dmrgpp::PackBuffer  pack;
 	std::string         msg = dmrgpp::build_kron_plan(d->noperator,
                                               d->npatches,
                                               d->left_patch_size,
@@ -597,13 +628,14 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
                                               bm,
                                               bn,
                                               h->plan,
-                                              &pack);
+                                              nullptr);
 	if (!msg.empty()) {
 		delete h;
 		return fail(nullptr, DMRGPP_INVALID_ARG, msg);
 	}
-	h->sector_start = { 0, h->plan.dim() };
-	return finish_create(h, d->device, d->stream, bm, pack, out);
+	h->sector_start                   = { 0, h->plan.dim() };
+	h->setup_times[DMRGPP_SETUP_PLAN] = seconds_since(t0);
+	return finish_create(h, d->device, d->stream, bm, t0, out);
 }
 
 int dmrgpp_kron_create_group(const dmrgpp_kron_desc* descs, size_t nsectors, dmrgpp_kron_handle* out)
@@ -631,6 +663,7 @@ int dmrgpp_kron_create_group(const dmrgpp_kron_desc* descs, size_t nsectors, dmr
 
 	// the union: sector s's patches follow those of sectors 0..s-1; no block
 	// connects two sectors, so the union's H is block-diagonal
+	const auto                    t0 = Clock::now();
 	std::vector<size_t>           l, r;
 	std::vector<dmrgpp::Triple>   triples;
 	std::vector<dmrgpp::BlockRef> blocks;
@@ -668,16 +701,16 @@ int dmrgpp_kron_create_group(const dmrgpp_kron_desc* descs, size_t nsectors, dmr
 	h->precision = descs[0].precision;
 	int bm, bn;
 	pick_tile_sizes(l.size(), l.data(), r.data(), bm, bn);
-	dmrgpp::PackBuffer  pack;
 	std::string msg = dmrgpp::build_kron_plan_triples(nop, l.size(), l.data(), r.data(),
 	                                                  std::move(triples), std::move(blocks), f_alg,
-	                                                  bm, bn, h->plan, &pack);
+	                                                  bm, bn, h->plan, nullptr);
 	if (!msg.empty()) {
 		delete h;
 		return fail(nullptr, DMRGPP_INVALID_ARG, msg);
 	}
-	h->sector_start = std::move(starts);
-	return finish_create(h, descs[0].device, descs[0].stream, bm, pack, out);
+	h->sector_start                   = std::move(starts);
+	h->setup_times[DMRGPP_SETUP_PLAN] = seconds_since(t0);
+	return finish_create(h, descs[0].device, descs[0].stream, bm, t0, out);
 }
 
 int dmrgpp_kron_group_sectors(dmrgpp_kron_handle h, size_t* nsectors, long long* offsets)

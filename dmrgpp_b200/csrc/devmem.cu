@@ -1,0 +1,138 @@
+// Stream-ordered device memory pool of the library (devmem.h).
+#include "devmem.h"
+#include "dmrgpp_kron.h"
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+
+namespace dmrgpp {
+
+namespace {
+
+struct DevicePool {
+	cudaMemPool_t pool   = nullptr;
+	cudaStream_t  stream = nullptr; // allocations and frees are ordered on it
+};
+
+std::mutex& pools_mutex()
+{
+	static std::mutex mu;
+	return mu;
+}
+
+std::map<int, DevicePool>& pools() // never freed: outlive every handle
+{
+	static std::map<int, DevicePool>* p = new std::map<int, DevicePool>();
+	return *p;
+}
+
+cudaError_t pool_of(int device, DevicePool** out)
+{
+	std::lock_guard<std::mutex> g(pools_mutex());
+	DevicePool&                 d = pools()[device];
+	if (!d.pool) {
+		cudaMemPoolProps props {};
+		props.allocType     = cudaMemAllocationTypePinned;
+		props.handleTypes   = cudaMemHandleTypeNone;
+		props.location.type = cudaMemLocationTypeDevice;
+		props.location.id   = device;
+		cudaError_t e       = cudaMemPoolCreate(&d.pool, &props);
+		if (e != cudaSuccess) {
+			d.pool = nullptr;
+			return e;
+		}
+		uint64_t keep = UINT64_MAX;
+		int      prev = -1;
+		if ((e = cudaMemPoolSetAttribute(d.pool, cudaMemPoolAttrReleaseThreshold, &keep))
+		    || (e = cudaGetDevice(&prev)) || (e = cudaSetDevice(device))) {
+			cudaMemPoolDestroy(d.pool);
+			d.pool = nullptr;
+			return e;
+		}
+		// the pool's stream belongs to its device
+		e = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking);
+		cudaSetDevice(prev);
+		if (e != cudaSuccess) {
+			cudaMemPoolDestroy(d.pool);
+			d.pool = nullptr;
+			return e;
+		}
+	}
+	*out = &d;
+	return cudaSuccess;
+}
+
+} // namespace
+
+cudaError_t dev_malloc_bytes(void** p, size_t bytes)
+{
+	*p         = nullptr;
+	int         device;
+	cudaError_t e = cudaGetDevice(&device);
+	DevicePool* d = nullptr;
+	if (e || (e = pool_of(device, &d)))
+		return e;
+	if ((e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, d->pool, d->stream)))
+		return e;
+	return cudaStreamSynchronize(d->stream);
+}
+
+void dev_free(void* p)
+{
+	if (!p)
+		return;
+	int device;
+	if (cudaGetDevice(&device) != cudaSuccess)
+		return;
+	DevicePool* d = nullptr;
+	if (pool_of(device, &d) != cudaSuccess)
+		return;
+	cudaDeviceSynchronize();
+	cudaFreeAsync(p, d->stream);
+}
+
+} // namespace dmrgpp
+
+extern "C" {
+
+int dmrgpp_release_cached_memory(int device)
+{
+	int         prev = -1;
+	cudaError_t e    = cudaGetDevice(&prev);
+	if (e != cudaSuccess)
+		return DMRGPP_CUDA_ERROR;
+	const int dev = device >= 0 ? device : prev;
+	if (dev != prev && cudaSetDevice(dev) != cudaSuccess)
+		return DMRGPP_INVALID_ARG;
+	dmrgpp::DevicePool* d = nullptr;
+	int                 rc = DMRGPP_OK;
+	if (dmrgpp::pool_of(dev, &d) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess
+	    || cudaStreamSynchronize(d->stream) != cudaSuccess || cudaMemPoolTrimTo(d->pool, 0) != cudaSuccess)
+		rc = DMRGPP_CUDA_ERROR;
+	if (dev != prev)
+		cudaSetDevice(prev);
+	return rc;
+}
+
+int dmrgpp_cached_memory(int device, size_t* reserved_bytes, size_t* used_bytes)
+{
+	if (!reserved_bytes || !used_bytes)
+		return DMRGPP_INVALID_ARG;
+	int prev = -1;
+	if (cudaGetDevice(&prev) != cudaSuccess)
+		return DMRGPP_CUDA_ERROR;
+	const int           dev = device >= 0 ? device : prev;
+	dmrgpp::DevicePool* d   = nullptr;
+	if (dmrgpp::pool_of(dev, &d) != cudaSuccess)
+		return DMRGPP_CUDA_ERROR;
+	uint64_t res = 0, used = 0;
+	if (cudaMemPoolGetAttribute(d->pool, cudaMemPoolAttrReservedMemCurrent, &res) != cudaSuccess
+	    || cudaMemPoolGetAttribute(d->pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+		return DMRGPP_CUDA_ERROR;
+	*reserved_bytes = size_t(res);
+	*used_bytes     = size_t(used);
+	return DMRGPP_OK;
+}
+
+} // extern "C"

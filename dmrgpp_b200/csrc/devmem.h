@@ -1,0 +1,30 @@
+// Device memory of handles and solver workspaces.
+//
+// A DMRG sweep creates one sector handle per step and destroys the previous
+// one: the same few GB (packed operators, BX, the Lanczos basis) are freed
+// and allocated again every step.  cudaMalloc of fresh device memory costs up
+// to a few hundred ms per GB-sized buffer, so these buffers come from one
+// stream-ordered memory pool per device that keeps freed memory for reuse
+// (release threshold: unlimited) until dmrgpp_release_cached_memory trims it.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace dmrgpp {
+
+// bytes on the current device; the memory is ready for use on any stream
+// when the call returns
+cudaError_t dev_malloc_bytes(void** p, size_t bytes);
+
+// Returns p to the pool after waiting for all work on the device (the same
+// implicit synchronisation as cudaFree).  Null is ignored.
+void dev_free(void* p);
+
+template <class T> cudaError_t dev_malloc(T** p, size_t bytes)
+{
+	return dev_malloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
+
+} // namespace dmrgpp

@@ -20,6 +20,7 @@
 // cross a sector boundary; every kernel walks chunks, so each block knows its
 // sector, and every sum runs in a fixed order (bitwise reproducible).
 #include "dmrgpp_kron.h"
+#include "devmem.h"
 #include "handle.h"
 #include "tridiag.h"
 
@@ -346,17 +347,17 @@ void release_group(dmrgpp_kron_handle h)
 	GroupWork* w = h->group;
 	if (!w)
 		return;
-	cudaFree(w->V);
-	cudaFree(w->z);
-	cudaFree(w->alpha);
-	cudaFree(w->beta);
-	cudaFree(w->scal);
-	cudaFree(w->partial);
-	cudaFree(w->r);
-	cudaFree(w->chunks);
-	cudaFree(w->seg_chunk);
-	cudaFree(w->active);
-	cudaFree(w->ncols);
+	dmrgpp::dev_free(w->V);
+	dmrgpp::dev_free(w->z);
+	dmrgpp::dev_free(w->alpha);
+	dmrgpp::dev_free(w->beta);
+	dmrgpp::dev_free(w->scal);
+	dmrgpp::dev_free(w->partial);
+	dmrgpp::dev_free(w->r);
+	dmrgpp::dev_free(w->chunks);
+	dmrgpp::dev_free(w->seg_chunk);
+	dmrgpp::dev_free(w->active);
+	dmrgpp::dev_free(w->ncols);
 	if (w->host)
 		cudaFreeHost(w->host);
 	delete w;
@@ -394,16 +395,16 @@ int ensure_group_work(dmrgpp_kron_handle h, int cols)
 	w->nch = int(ch.size());
 	cudaError_t e;
 	const size_t nsc = size_t(nseg) * size_t(cols);
-	if ((e = cudaMalloc(&w->V, dim * size_t(cols) * sizeof(double))) || (e = cudaMalloc(&w->z, dim * sizeof(double)))
-	    || (e = cudaMalloc(&w->alpha, nsc * sizeof(double)))
-	    || (e = cudaMalloc(&w->beta, (nsc + size_t(nseg)) * sizeof(double)))
-	    || (e = cudaMalloc(&w->scal, size_t(nseg) * 4 * sizeof(double)))
-	    || (e = cudaMalloc(&w->partial, std::max<size_t>(1, ch.size()) * size_t(cols) * sizeof(double)))
-	    || (e = cudaMalloc(&w->r, nsc * sizeof(double)))
-	    || (e = cudaMalloc(&w->chunks, std::max<size_t>(1, ch.size()) * sizeof(Chunk)))
-	    || (e = cudaMalloc(&w->seg_chunk, sc.size() * sizeof(int)))
-	    || (e = cudaMalloc(&w->active, size_t(nseg) * sizeof(int)))
-	    || (e = cudaMalloc(&w->ncols, size_t(nseg) * sizeof(int)))
+	if ((e = dmrgpp::dev_malloc(&w->V, dim * size_t(cols) * sizeof(double))) || (e = dmrgpp::dev_malloc(&w->z, dim * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->alpha, nsc * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->beta, (nsc + size_t(nseg)) * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->scal, size_t(nseg) * 4 * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->partial, std::max<size_t>(1, ch.size()) * size_t(cols) * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->r, nsc * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->chunks, std::max<size_t>(1, ch.size()) * sizeof(Chunk)))
+	    || (e = dmrgpp::dev_malloc(&w->seg_chunk, sc.size() * sizeof(int)))
+	    || (e = dmrgpp::dev_malloc(&w->active, size_t(nseg) * sizeof(int)))
+	    || (e = dmrgpp::dev_malloc(&w->ncols, size_t(nseg) * sizeof(int)))
 	    || (e = cudaHostAlloc(&w->host, 2 * (2 * nsc + size_t(nseg)) * sizeof(double), 0)))
 		return status(h, e, "group solver allocation");
 	if ((e = cudaMemcpy(w->chunks, ch.data(), ch.size() * sizeof(Chunk), cudaMemcpyHostToDevice))

@@ -46,6 +46,7 @@ struct dmrgpp_kron_s {
 	int*                err_host = nullptr; // mapped pinned word written by the kernel
 	int*                err_dev  = nullptr;
 	int                 test_stall = 0;     // dmrgpp_kron_test_stall_dependency
+	double              setup_times[DMRGPP_SETUP_NPHASES] = {}; // dmrgpp_kron_setup_profile
 	// mixed-precision (TF32x3 tensor-core) form, built when requested
 	bool                mixed_ready = false;
 	float*              m_ops_hi = nullptr; // packed operators, TF32 hi / lo
@@ -83,6 +84,16 @@ namespace dmrgpp {
 // replayed solver steps).
 int kron_apply_device(dmrgpp_kron_handle h, const double* x, double* y,
                       const dmrgpp::StepIO* io = nullptr);
+
+// Copies the caller's blocks (h->plan.blocks) into the packed FP64 operators
+// h->d_ops through pinned staging buffers and a placement kernel, and waits
+// for it; seconds_fill (optional) receives the host time spent copying into
+// the staging buffers.
+int upload_operators(dmrgpp_kron_handle h, double* seconds_fill);
+
+// Allocates h->d_diag and computes the diagonal of H on the device from the
+// packed operators (after upload_operators); waits for it.
+int upload_diagonal(dmrgpp_kron_handle h);
 
 // Builds and uploads the TF32x3 tensor-core form of the sector from the
 // plan's host blocks (create time only).

@@ -478,6 +478,78 @@ void add_tc_tiles(std::vector<GemmTile>& tiles, long long c_off, long long ldc, 
 
 } // namespace
 
+UploadPlan build_upload_plan(const KronPlan& plan, long long chunk_elems, long long max_job_elems)
+{
+	UploadPlan up;
+	long long  longest = 1;
+	for (const Triple& tr : plan.triples)
+		longest = std::max({ longest, plan.r[tr.i], plan.l[tr.i] });
+	up.chunk_elems = std::max(chunk_elems, longest);
+	max_job_elems  = std::max<long long>(max_job_elems, 1);
+
+	long long fill = 0; // doubles used in the open chunk
+	up.chunk_begin.push_back(0);
+	auto close_chunk = [&] {
+		up.chunk_fill.push_back(fill);
+		up.chunk_begin.push_back(up.jobs.size());
+		fill = 0;
+	};
+	// the block rows x cols at src (leading dimension ld) in parts
+	auto add_block = [&](const double* src, long long ld, long long rows, long long cols,
+	                     long long dst, int ld_dst, int transpose) {
+		const long long job_cols = std::max<long long>(1, max_job_elems / rows);
+		for (long long c0 = 0; c0 < cols;) {
+			long long room = (up.chunk_elems - fill) / rows;
+			if (room < 1) {
+				close_chunk();
+				room = up.chunk_elems / rows;
+			}
+			const long long n = std::min({ cols - c0, job_cols, room });
+			UploadJob       j;
+			j.src       = fill;
+			j.dst       = dst + (transpose ? c0 : c0 * ld_dst);
+			j.rows      = int(rows);
+			j.cols      = int(n);
+			j.ld_dst    = ld_dst;
+			j.transpose = transpose;
+			up.jobs.push_back(j);
+			up.host_src.push_back(src + c0 * ld);
+			up.host_ld.push_back(ld);
+			fill += rows * n;
+			c0 += n;
+		}
+	};
+	for (size_t t = 0; t < plan.triples.size(); ++t) {
+		const Triple&   tr = plan.triples[t];
+		const BlockRef& bl = plan.blocks[t];
+		// B_k(i,j) (r_i x r_j) into rows [row_off, row_off + r_i) of Bstack_j
+		add_block(bl.B, (long long)bl.ldB, plan.r[tr.i], plan.r[tr.j],
+		          plan.bstack_off[tr.j] + plan.row_off[t], int(plan.M[tr.j]), 0);
+		// A_k(i,j) (l_i x l_j) transposed into A^T (l_j x l_i, leading dimension l_j)
+		add_block(bl.A, (long long)bl.ldA, plan.l[tr.i], plan.l[tr.j], plan.at_off[t],
+		          int(plan.l[tr.j]), 1);
+	}
+	if (fill > 0 || up.chunk_fill.empty())
+		close_chunk();
+	return up;
+}
+
+void fill_upload_chunk(const UploadPlan& up, size_t c, size_t first, size_t last, double* buf)
+{
+	for (size_t q = up.chunk_begin[c] + first; q < up.chunk_begin[c] + last; ++q) {
+		const UploadJob& j   = up.jobs[q];
+		const double*    src = up.host_src[q];
+		const long long  ld  = up.host_ld[q];
+		double*          dst = buf + j.src;
+		if (ld == j.rows) {
+			std::memcpy(dst, src, size_t(j.rows) * size_t(j.cols) * sizeof(double));
+		} else {
+			for (int c2 = 0; c2 < j.cols; ++c2)
+				std::memcpy(dst + (long long)c2 * j.rows, src + c2 * ld, size_t(j.rows) * sizeof(double));
+		}
+	}
+}
+
 void sector_diagonal(const KronPlan& plan, std::vector<double>& diag)
 {
 	diag.assign(size_t(plan.dim()), 0.0);

@@ -259,6 +259,41 @@ struct PackJob {
 // (rows of Bstack_j) and its A^T block.
 std::vector<PackJob> mixed_pack_jobs(const KronPlan& plan);
 
+// Staged upload of the FP64 packed operators at create time.  The caller's
+// blocks are copied, column range by column range and contiguous
+// (leading dimension = rows), into fixed-size chunks of pinned host memory;
+// each chunk goes to the device in one copy, where a kernel moves every part
+// to its place in the packed buffer (B blocks into Bstack_j, A blocks
+// transposed into A^T).  One part = columns [col0, col0 + cols) of one block.
+struct UploadJob {
+	long long src;       // offset of the part in its chunk (doubles)
+	long long dst;       // packed-buffer offset of element (0, col0) of the part
+	int       rows;      // rows of the block
+	int       cols;      // columns of the part
+	int       ld_dst;    // leading dimension at dst
+	int       transpose; // 0: (q, c) -> dst[q + c ld_dst]; 1: (q, c) -> dst[c + q ld_dst]
+};
+
+struct UploadPlan {
+	long long              chunk_elems = 0; // capacity of one chunk (doubles)
+	std::vector<UploadJob> jobs;            // in chunk order
+	std::vector<size_t>    chunk_begin;     // jobs of chunk c: [chunk_begin[c], chunk_begin[c+1])
+	std::vector<long long> chunk_fill;      // doubles used in chunk c
+	std::vector<const double*> host_src;    // per job: the part's first column in the caller's block
+	std::vector<long long> host_ld;         // per job: the caller's leading dimension
+	size_t chunks() const { return chunk_fill.size(); }
+};
+
+// Cuts the blocks of plan.blocks into parts of at most max_job_elems doubles
+// (at least one column) and fills chunks of chunk_elems doubles in triple
+// order (B then A of each triple); a chunk is at least as large as the
+// longest column.
+UploadPlan build_upload_plan(const KronPlan& plan, long long chunk_elems, long long max_job_elems);
+
+// Copies the parts of chunk c from the caller's blocks into buf (host side
+// of the staged upload; jobs [first, last) of the chunk).
+void fill_upload_chunk(const UploadPlan& up, size_t c, size_t first, size_t last, double* buf);
+
 // Diagonal of the sector's H in patch order: element (iR, iL) of patch i is
 // sum_k A_k(i,i)(iL,iL) * B_k(i,i)(iR,iR) over the contributing diagonal
 // triples (the input of diagonal preconditioners); reads plan.blocks.

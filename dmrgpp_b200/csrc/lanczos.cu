@@ -18,6 +18,7 @@
 // Reductions are deterministic: per-block partials in fixed-size grids, the
 // last block to finish (arrival counter) sums them in block order.
 #include "dmrgpp_kron.h"
+#include "devmem.h"
 #include "handle.h"
 #include "tridiag.h"
 
@@ -555,12 +556,12 @@ void release_lanczos(dmrgpp_kron_handle h)
 	LanczosWork* w = h->lanczos;
 	if (!w)
 		return;
-	cudaFree(w->V);
-	cudaFree(w->scal);
-	cudaFree(w->partial);
-	cudaFree(w->r);
-	cudaFree(w->ctr);
-	cudaFree(w->step);
+	dmrgpp::dev_free(w->V);
+	dmrgpp::dev_free(w->scal);
+	dmrgpp::dev_free(w->partial);
+	dmrgpp::dev_free(w->r);
+	dmrgpp::dev_free(w->ctr);
+	dmrgpp::dev_free(w->step);
 	if (w->host)
 		cudaFreeHost(w->host);
 	delete w;
@@ -586,24 +587,24 @@ int ensure_work(dmrgpp_kron_handle h, size_t dim, int cols)
 	w->dim      = dim;
 	w->cols     = cols;
 	cudaError_t e;
-	if ((e = cudaMalloc(&w->V, dim * size_t(cols) * sizeof(double))))
-		return cuda_status(h, e, "cudaMalloc(Lanczos basis)");
-	if ((e = cudaMalloc(&w->scal, (2 * size_t(cols) + 16) * sizeof(double))))
-		return cuda_status(h, e, "cudaMalloc(Lanczos scalars)");
-	if ((e = cudaMalloc(&w->partial, size_t(kMaxBlocks) * kMaxCols * sizeof(double))))
-		return cuda_status(h, e, "cudaMalloc(partials)");
-	if ((e = cudaMalloc(&w->r, size_t(kMaxCols) * sizeof(double))))
-		return cuda_status(h, e, "cudaMalloc(coefficients)");
-	if ((e = cudaMalloc(&w->ctr, 16 * sizeof(unsigned))))
-		return cuda_status(h, e, "cudaMalloc(counters)");
+	if ((e = dmrgpp::dev_malloc(&w->V, dim * size_t(cols) * sizeof(double))))
+		return cuda_status(h, e, "device allocation (Lanczos basis)");
+	if ((e = dmrgpp::dev_malloc(&w->scal, (2 * size_t(cols) + 16) * sizeof(double))))
+		return cuda_status(h, e, "device allocation (Lanczos scalars)");
+	if ((e = dmrgpp::dev_malloc(&w->partial, size_t(kMaxBlocks) * kMaxCols * sizeof(double))))
+		return cuda_status(h, e, "device allocation (partials)");
+	if ((e = dmrgpp::dev_malloc(&w->r, size_t(kMaxCols) * sizeof(double))))
+		return cuda_status(h, e, "device allocation (coefficients)");
+	if ((e = dmrgpp::dev_malloc(&w->ctr, 16 * sizeof(unsigned))))
+		return cuda_status(h, e, "device allocation (counters)");
 	if ((e = cudaMemset(w->ctr, 0, 16 * sizeof(unsigned))))
 		return cuda_status(h, e, "clear counters");
 	if ((e = cudaMemset(w->scal, 0, (2 * size_t(cols) + 16) * sizeof(double))))
 		return cuda_status(h, e, "clear scalars");
 	if ((e = cudaHostAlloc(&w->host, 2 * (2 * size_t(cols) + 16) * sizeof(double), 0)))
 		return cuda_status(h, e, "cudaHostAlloc(scalars)");
-	if ((e = cudaMalloc(&w->step, sizeof(LanczosStep))))
-		return cuda_status(h, e, "cudaMalloc(step record)");
+	if ((e = dmrgpp::dev_malloc(&w->step, sizeof(LanczosStep))))
+		return cuda_status(h, e, "device allocation (step record)");
 	return DMRGPP_OK;
 }
 
@@ -1031,13 +1032,13 @@ void release_davidson(dmrgpp_kron_handle h)
 	DavidsonWork* w = h->davidson;
 	if (!w)
 		return;
-	cudaFree(w->V);
-	cudaFree(w->W);
-	cudaFree(w->u);
-	cudaFree(w->coef);
-	cudaFree(w->scal);
-	cudaFree(w->partial);
-	cudaFree(w->ctr);
+	dmrgpp::dev_free(w->V);
+	dmrgpp::dev_free(w->W);
+	dmrgpp::dev_free(w->u);
+	dmrgpp::dev_free(w->coef);
+	dmrgpp::dev_free(w->scal);
+	dmrgpp::dev_free(w->partial);
+	dmrgpp::dev_free(w->ctr);
 	if (w->host)
 		cudaFreeHost(w->host);
 	delete w;
@@ -1057,13 +1058,13 @@ int ensure_davidson(dmrgpp_kron_handle h, size_t dim, int mmax)
 	w->dim      = dim;
 	w->mmax     = mmax;
 	cudaError_t e;
-	if ((e = cudaMalloc(&w->V, dim * size_t(mmax) * sizeof(double)))
-	    || (e = cudaMalloc(&w->W, dim * size_t(mmax) * sizeof(double)))
-	    || (e = cudaMalloc(&w->u, 4 * dim * sizeof(double)))
-	    || (e = cudaMalloc(&w->coef, size_t(kMaxCols) * sizeof(double)))
-	    || (e = cudaMalloc(&w->scal, 16 * sizeof(double)))
-	    || (e = cudaMalloc(&w->partial, size_t(kMaxBlocks) * kMaxCols * sizeof(double)))
-	    || (e = cudaMalloc(&w->ctr, 16 * sizeof(unsigned)))
+	if ((e = dmrgpp::dev_malloc(&w->V, dim * size_t(mmax) * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->W, dim * size_t(mmax) * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->u, 4 * dim * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->coef, size_t(kMaxCols) * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->scal, 16 * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->partial, size_t(kMaxBlocks) * kMaxCols * sizeof(double)))
+	    || (e = dmrgpp::dev_malloc(&w->ctr, 16 * sizeof(unsigned)))
 	    || (e = cudaMemset(w->ctr, 0, 16 * sizeof(unsigned)))
 	    || (e = cudaHostAlloc(&w->host, (size_t(kMaxCols) + 8) * sizeof(double), 0)))
 		return cuda_status(h, e, "Davidson buffers");

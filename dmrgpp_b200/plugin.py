@@ -64,6 +64,19 @@ class _DescTables:
             int(precision), stream, int(device))
 
 
+def cached_memory(device: int = -1):
+    """(reserved, in-use) bytes of the library's device memory pool."""
+    r, u = ctypes.c_size_t(), ctypes.c_size_t()
+    _capi.check(_capi.lib().dmrgpp_cached_memory(device, ctypes.byref(r), ctypes.byref(u)))
+    return int(r.value), int(u.value)
+
+
+def release_cached_memory(device: int = -1) -> None:
+    """Returns the pool's unused device memory (kept for the next handle
+    otherwise) to the device."""
+    _capi.check(_capi.lib().dmrgpp_release_cached_memory(device))
+
+
 class BatchedGemm:
     """y = H x for one superblock sector on the GPU.
 
@@ -122,6 +135,16 @@ class BatchedGemm:
         _capi.check(L.dmrgpp_kron_flops(h, ctypes.byref(f)), h)
         self.f_alg = float(f.value)
         return self
+
+    SETUP_PHASES = ("plan", "alloc", "upload", "upload_fill", "diagonal", "mixed", "total")
+
+    def setup_profile(self) -> dict:
+        """Seconds spent in each phase of this handle's create
+        (dmrgpp_kron_setup_profile)."""
+        n = len(self.SETUP_PHASES)
+        t = (ctypes.c_double * n)()
+        _capi.check(self._lib.dmrgpp_kron_setup_profile(self._h, t, n), self._h)
+        return {k: float(v) for k, v in zip(self.SETUP_PHASES, t)}
 
     def sector_offsets(self) -> np.ndarray:
         """Start offsets of the handle's sectors in x (nsectors + 1 entries)."""

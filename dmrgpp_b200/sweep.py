@@ -47,15 +47,25 @@ def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int 
     upload: the plugin constructor a sweep step also pays), and
     speedup_with_setup compares setup + solve of the two forms."""
     import torch
-    # handle set-up (the plugin constructor: plan, packing, upload) of each form
+    init = torch.from_numpy(np.random.default_rng(seed).standard_normal(prob.dim)).cuda()
+    # steady state of a sweep: the previous step's handle and solver buffers
+    # have gone back to the library's memory pool and the pinned staging
+    # buffers exist.  Stand-in: one untimed create of the same sector with a
+    # few Lanczos steps sized for lanczos_steps (the basis is allocated for
+    # the step limit), then destroyed.
+    warm = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+    warm.set_precision(plugin.FP64)
+    warm.lanczos_lowest(init, steps=lanczos_steps, min_steps=2, tolerance=1e300)
+    warm.close()
+    pool_before = plugin.cached_memory()[0]
     b64 = plugin.BatchedGemm.from_problem(prob, precision=plugin.FP64)
-    setup_fp64 = b64.create_seconds
+    setup_fp64, phases_fp64 = b64.create_seconds, b64.setup_profile()
     b64.close()
     bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
-    setup_mixed = bg.create_seconds
-    init = torch.from_numpy(np.random.default_rng(seed).standard_normal(prob.dim)).cuda()
+    setup_mixed, phases_mixed = bg.create_seconds, bg.setup_profile()
     out = {"sector_dim": prob.dim, "f_alg_per_matvec": prob.flops(), "sites": sites,
-           "setup_seconds": {"fp64": setup_fp64, "tf32x3": setup_mixed}}
+           "setup_seconds": {"fp64": setup_fp64, "tf32x3": setup_mixed},
+           "setup_phases": {"fp64": phases_fp64, "tf32x3": phases_mixed}}
 
     bg.set_precision(plugin.FP64)
     bg.autotune(None, reps=3)
@@ -89,6 +99,9 @@ def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int 
         converged=st_r["converged"], **compare(e_r, z_r))
     out["speedup_vs_fp64_lanczos"] = t_l / t_r
     out["speedup_with_setup"] = (t_l + setup_fp64) / (t_r + setup_mixed)
+    # growth of the memory pool during the timed creates and solves (0: every
+    # buffer came from memory the warm-up step had returned)
+    out["pool_growth_bytes"] = plugin.cached_memory()[0] - pool_before
 
     # warm start: the previous sweep step's state transformed to this
     # superblock is close to the answer; stand-in: the FP64 ground state plus

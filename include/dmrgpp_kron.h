@@ -142,6 +142,38 @@ int dmrgpp_kron_dim(dmrgpp_kron_handle h, size_t* dim);
  * summed as estimate_work.cpp:114-151). */
 int dmrgpp_kron_flops(dmrgpp_kron_handle h, double* f_alg);
 
+/* Wall-clock seconds of the phases of this handle's create (host clock,
+ * each phase waits for its device work): the plugin constructor's work
+ * (BatchedGemm.cpp:8-79, setup_sparse_batch.cpp:14-379) split into
+ *   PLAN         all-zero block scan, triple list, offsets, tile lists
+ *   ALLOC        device allocations and the persistent schedule
+ *   UPLOAD       the staged copy of the blocks into the packed operators
+ *   UPLOAD_FILL  of which host time copying blocks into pinned staging
+ *   DIAGONAL     the diagonal of H (preconditioners)
+ *   MIXED        the TF32x3 form (0 for FP64 handles)
+ *   TOTAL        the whole create
+ * n (<= DMRGPP_SETUP_NPHASES) values are written to t. */
+enum {
+	DMRGPP_SETUP_PLAN        = 0,
+	DMRGPP_SETUP_ALLOC       = 1,
+	DMRGPP_SETUP_UPLOAD      = 2,
+	DMRGPP_SETUP_UPLOAD_FILL = 3,
+	DMRGPP_SETUP_DIAGONAL    = 4,
+	DMRGPP_SETUP_MIXED       = 5,
+	DMRGPP_SETUP_TOTAL       = 6,
+	DMRGPP_SETUP_NPHASES     = 7
+};
+int dmrgpp_kron_setup_profile(dmrgpp_kron_handle h, double* t, size_t n);
+
+/* Device memory of handles and solver workspaces comes from one
+ * stream-ordered pool per device that keeps freed memory for the next handle
+ * (a sweep destroys and creates a handle of similar size every step).
+ * dmrgpp_release_cached_memory returns the unused part to the device
+ * (device < 0: the current device); dmrgpp_cached_memory reports the pool's
+ * reserved and in-use bytes. */
+int dmrgpp_release_cached_memory(int device);
+int dmrgpp_cached_memory(int device, size_t* reserved_bytes, size_t* used_bytes);
+
 /* Host-only planning statistics (no device work; usable without a GPU):
  * number of contributing triples, F_alg, packed operator bytes and the
  * bytes of the intermediate BX buffer. */

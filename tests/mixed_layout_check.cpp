@@ -12,6 +12,10 @@
 //     sums are the tile's output;
 //   * the device-side operator packing (mixed_pack_jobs) reproduces the host
 //     packing bit for bit;
+//   * the staged FP64 upload (build_upload_plan, fill_upload_chunk and the
+//     placement of upload_place_kernel) writes every packed position once,
+//     with the host packing's value, also for blocks whose leading dimension
+//     exceeds their rows;
 //   * the epilogue's stores stay inside their buffers;
 //   * pass 1 + pass 2 computed from these buffers (hi*hi + hi*lo + lo*hi in
 //     double) reproduce the FP64 H*x.
@@ -78,16 +82,17 @@ int main(int argc, char** argv)
 				if (coin(rng) < 0.35)
 					continue;
 				const size_t ix = size_t(i) + size_t(j) * np + size_t(k) * np * np;
-				Ast[ix].resize(l[i] * l[j]);
-				Bst[ix].resize(r[i] * r[j]);
+				// some blocks sit in larger arrays (leading dimension > rows)
+				ldA[ix] = l[i] + (coin(rng) < 0.3 ? 3 : 0);
+				ldB[ix] = r[i] + (coin(rng) < 0.3 ? 5 : 0);
+				Ast[ix].resize(ldA[ix] * l[j]);
+				Bst[ix].resize(ldB[ix] * r[j]);
 				for (double& v : Ast[ix])
 					v = val(rng);
 				for (double& v : Bst[ix])
 					v = val(rng);
 				A[ix]   = Ast[ix].data();
 				B[ix]   = Bst[ix].data();
-				ldA[ix] = l[i];
-				ldB[ix] = r[i];
 			}
 
 	KronPlan            plan;
@@ -125,6 +130,53 @@ int main(int argc, char** argv)
 		if (before != after)
 			return fail("tile runs are not a permutation", pass_no, 0);
 	}
+	// the staged upload (build_upload_plan + fill_upload_chunk on the host,
+	// the placement of upload_place_kernel emulated here) writes exactly the
+	// packed FP64 operators: every position once, with the host packing's value
+	{
+		const long long chunk = 700 + 37 * (long long)(seed % 11), job = 150 + 13 * (long long)(seed % 7);
+		const UploadPlan up   = build_upload_plan(plan, chunk, job);
+		std::vector<double> out(pack64.size(), std::numeric_limits<double>::quiet_NaN());
+		std::vector<char>   hit(pack64.size(), 0);
+		long long           written = 0, expect = 0;
+		for (size_t t = 0; t < plan.triples.size(); ++t) {
+			const Triple& tr = plan.triples[t];
+			expect += plan.r[tr.i] * plan.r[tr.j] + plan.l[tr.i] * plan.l[tr.j];
+		}
+		if (up.chunk_begin.size() != up.chunks() + 1 || up.chunk_begin.back() != up.jobs.size())
+			return fail("upload chunks do not cover the jobs", long(up.chunks()), long(up.jobs.size()));
+		for (size_t c = 0; c < up.chunks(); ++c) {
+			if (up.chunk_fill[c] > up.chunk_elems)
+				return fail("upload chunk overfilled", up.chunk_fill[c], up.chunk_elems);
+			std::vector<double> buf(size_t(up.chunk_elems), 0.0);
+			const size_t        n = up.chunk_begin[c + 1] - up.chunk_begin[c];
+			fill_upload_chunk(up, c, 0, n / 2, buf.data()); // two calls, as two threads would
+			fill_upload_chunk(up, c, n / 2, n, buf.data());
+			for (size_t q = up.chunk_begin[c]; q < up.chunk_begin[c + 1]; ++q) {
+				const UploadJob& j = up.jobs[q];
+				if (j.src < 0 || j.src + (long long)j.rows * j.cols > up.chunk_fill[c])
+					return fail("upload part outside its chunk", j.src, up.chunk_fill[c]);
+				if ((long long)j.rows * j.cols > std::max<long long>(job, j.rows))
+					return fail("upload part too large", j.rows, j.cols);
+				for (int cc = 0; cc < j.cols; ++cc)
+					for (int qq = 0; qq < j.rows; ++qq) {
+						const long long d = j.transpose ? j.dst + cc + (long long)qq * j.ld_dst
+						                                : j.dst + qq + (long long)cc * j.ld_dst;
+						if (d < 0 || d >= (long long)out.size())
+							return fail("upload placement out of bounds", d, (long long)out.size());
+						if (hit[size_t(d)]++)
+							return fail("upload writes a position twice", d, 0);
+						out[size_t(d)] = buf[size_t(j.src + qq + (long long)cc * j.rows)];
+						++written;
+					}
+			}
+		}
+		if (written != expect)
+			return fail("upload writes the wrong number of elements", written, expect);
+		for (size_t e = 0; e < out.size(); ++e)
+			if (hit[e] && out[e] != pack64[e])
+				return fail("upload differs from the host packing", (long long)e, 0);
+	}
 	const MixedPlan& mp = plan.mixed;
 	const long long  D  = plan.dim();
 	// the device packing (mixed_pack_jobs over the FP64 packed operators,
@@ -157,8 +209,8 @@ int main(int argc, char** argv)
 				double s = 0;
 				for (long long c = 0; c < rj; ++c)
 					for (long long d = 0; d < lj; ++d)
-						s += B[ix][a + c * ri] * x[size_t(plan.xy_start[t.j] + c + d * rj)]
-						    * A[ix][b + d * li];
+						s += B[ix][a + c * (long long)ldB[ix]] * x[size_t(plan.xy_start[t.j] + c + d * rj)]
+						    * A[ix][b + d * (long long)ldA[ix]];
 				y_ref[size_t(plan.xy_start[t.i] + a + b * ri)] += s;
 			}
 	}

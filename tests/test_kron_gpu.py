@@ -201,3 +201,85 @@ def test_ladder_shaped_sector(cuda_lib, cuda_device, oracle_built):
     x = np.random.default_rng(5).standard_normal(prob.dim)
     y = gpu_apply(prob, x)
     assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL
+
+
+def test_blocks_in_larger_arrays(cuda_lib, cuda_device, oracle_built):
+    """Blocks whose leading dimension exceeds their rows (ld = rows + 3) go
+    through the staged upload column by column."""
+    from dmrgpp_b200 import plugin
+    prob = sb.random_problem(npatches=5, noperator=3, max_size=60, seed=21, zero_block_rate=0.2)
+    A, ldA, B, ldB = prob.tables()
+    keep = []
+
+    def embed(tab, ld):
+        out, lds = [], list(ld)
+        for q, m in enumerate(tab):
+            if m is None:
+                out.append(None)
+                continue
+            m = np.asfortranarray(m)
+            big = np.zeros((m.shape[0] + 3, m.shape[1]), order="F")
+            big[:m.shape[0], :] = m
+            keep.append(big)
+            out.append(big.ctypes.data)
+            lds[q] = m.shape[0] + 3
+        return out, lds
+    Ap, ldAp = embed(A, ldA)
+    Bp, ldBp = embed(B, ldB)
+    bg = plugin.BatchedGemm(prob.noperator, prob.npatches, prob.lsz, prob.rsz, Ap, ldAp, Bp, ldBp)
+    try:
+        x = np.random.default_rng(4).standard_normal(prob.dim)
+        assert rel_err(bg(x), oracle_built.kron_apply(prob, x)) < RTOL
+    finally:
+        bg.close()
+
+
+def test_operators_spanning_several_upload_chunks(cuda_lib, cuda_device, oracle_built):
+    """36 MB of packed operators: more than one 32 MB staging chunk, so the
+    pinned buffers are refilled while earlier chunks are in flight."""
+    from dmrgpp_b200 import plugin
+    prob = sb.ladder_problem(total_states=4000, sigma=2.5, seed=9)
+    bg = plugin.BatchedGemm.from_problem(prob)
+    try:
+        ph = bg.setup_profile()
+        assert ph["total"] >= ph["upload"] >= ph["upload_fill"] > 0.0 and ph["plan"] > 0.0
+        assert ph["mixed"] == 0.0
+        x = np.random.default_rng(8).standard_normal(prob.dim)
+        assert rel_err(bg(x), oracle_built.kron_apply(prob, x)) < RTOL
+    finally:
+        bg.close()
+
+
+@pytest.mark.parametrize("seed,np_,K,maxs", [(31, 4, 3, 30), (32, 7, 5, 12), (33, 1, 1, 1)])
+def test_device_diagonal_matches_dense_h(cuda_lib, cuda_device, seed, np_, K, maxs):
+    """The create-time diagonal (Jacobi and learned preconditioners) equals
+    diag(H) of the explicit sector matrix."""
+    import torch
+    from dmrgpp_b200 import plugin
+    prob = sb.random_problem(npatches=np_, noperator=K, max_size=maxs, seed=seed,
+                             zero_block_rate=0.2)
+    bg = plugin.BatchedGemm.from_problem(prob)
+    try:
+        d = bg.diagonal()
+        torch.cuda.synchronize()
+        ref = np.diag(prob.dense())
+        np.testing.assert_allclose(d.cpu().numpy(), ref, rtol=1e-13, atol=1e-13 * np.abs(ref).max())
+    finally:
+        bg.close()
+
+
+def test_memory_pool_reuses_freed_handles(cuda_lib, cuda_device):
+    """A destroyed handle's device memory stays in the library's pool and
+    serves the next create of the same size; releasing the cache returns it."""
+    from dmrgpp_b200 import plugin
+    prob = sb.ladder_problem(total_states=1500, sigma=2.0, seed=3)
+    plugin.BatchedGemm.from_problem(prob).close()
+    r1, u1 = plugin.cached_memory()
+    assert r1 > 0
+    bg = plugin.BatchedGemm.from_problem(prob)
+    r2, u2 = plugin.cached_memory()
+    bg.close()
+    assert r2 <= r1 and u2 > u1
+    plugin.release_cached_memory()
+    r3, u3 = plugin.cached_memory()
+    assert u3 <= r3 < r1
