@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <thread>
 #include <climits>
 #include <cstring>
 #include <new>
@@ -67,6 +68,8 @@ void release(dmrgpp_kron_handle h)
 {
 	if (!h)
 		return;
+	// nothing of the handle may still run: its memory and error word are reused
+	cudaDeviceSynchronize();
 	dmrgpp::release_lanczos(h);
 	dmrgpp::release_davidson(h);
 	dmrgpp::release_group(h);
@@ -95,8 +98,7 @@ void release(dmrgpp_kron_handle h)
 	dmrgpp::dev_free(h->d_lists);
 	dmrgpp::dev_free(h->d_ctr);
 	dmrgpp::dev_free(h->d_part);
-	if (h->err_host)
-		cudaFreeHost(h->err_host);
+	dmrgpp::error_word_free(h->err_host);
 	h->err_host = h->err_dev = nullptr;
 	h->d_ctr                 = nullptr;
 	h->d_part                = nullptr;
@@ -254,28 +256,36 @@ int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const St
 
 }
 
-int build_mixed(dmrgpp_kron_handle h)
+void mixed_host_plan(dmrgpp_kron_handle h, int sms, MixedHost& out)
 {
-	std::vector<int>   xmap;
-	size_t             maxs = 0;
+	size_t maxs = 0;
 	for (size_t p = 0; p < h->plan.np; ++p)
 		maxs = std::max<size_t>(maxs, size_t(std::max(h->plan.l[p], h->plan.r[p])));
-	const int   bn  = maxs > 96 ? 128 : 64;
-	int         sms = 0;
-	cudaError_t e   = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-	if (e != cudaSuccess)
-		return cuda_fail(h, e, "SM count");
-	// operators: packed on the device from the FP64 copy already there
-	std::string msg = build_mixed_plan(h->plan, bn, nullptr, nullptr, &xmap, sms);
-	if (!msg.empty())
-		return fail(h, DMRGPP_INVALID_ARG, msg);
+	const int bn = maxs > 96 ? 128 : 64;
+	// operators: packed on the device from the FP64 copy (mixed_pack_jobs)
+	out.msg = build_mixed_plan(h->plan, bn, nullptr, nullptr, &out.xmap, sms);
+	if (!out.msg.empty())
+		return;
+	MixedPlan& mp = h->plan.mixed;
+	out.grid1     = balance_tiles(mp.tile1, mp.seg1, sms, out.starts1);
+	out.grid2     = balance_tiles(mp.tile2, mp.seg2, sms, out.starts2);
+	out.jobs      = mixed_pack_jobs(h->plan);
+	out.ready     = true;
+}
+
+int build_mixed(dmrgpp_kron_handle h, MixedHost& host)
+{
+	if (!host.ready)
+		return fail(h, DMRGPP_INVALID_ARG, host.msg);
+	cudaError_t      e;
 	const MixedPlan& mp = h->plan.mixed;
 	if ((e = tc_init()) != cudaSuccess)
 		return cuda_fail(h, e, "tensor-core kernel attributes");
-	MixedPlan&       mpw = h->plan.mixed;
-	std::vector<int> starts1, starts2;
-	h->m_grid1 = balance_tiles(mpw.tile1, mpw.seg1, sms, starts1);
-	h->m_grid2 = balance_tiles(mpw.tile2, mpw.seg2, sms, starts2);
+	const std::vector<int>& xmap    = host.xmap;
+	const std::vector<int>& starts1 = host.starts1;
+	const std::vector<int>& starts2 = host.starts2;
+	h->m_grid1                      = host.grid1;
+	h->m_grid2                      = host.grid2;
 	auto fbytes = [](long long n) { return size_t(n > 0 ? n : 1) * sizeof(float); };
 	if ((e = dmrgpp::dev_malloc(&h->m_ops_hi, fbytes(mp.ops_elems))) || (e = dmrgpp::dev_malloc(&h->m_ops_lo, fbytes(mp.ops_elems)))
 	    || (e = dmrgpp::dev_malloc(&h->m_xs_hi, fbytes(mp.xs_elems))) || (e = dmrgpp::dev_malloc(&h->m_xs_lo, fbytes(mp.xs_elems)))
@@ -294,8 +304,8 @@ int build_mixed(dmrgpp_kron_handle h)
 	    || (e = cudaMemset(h->m_bxs_lo, 0, fbytes(mp.bxs_elems))))
 		return cuda_fail(h, e, "clear mixed-precision buffers");
 	{
-		const std::vector<PackJob> jobs = mixed_pack_jobs(h->plan);
-		PackJob* d_jobs = nullptr;
+		const std::vector<PackJob>& jobs   = host.jobs;
+		PackJob*                    d_jobs = nullptr;
 		if ((e = cudaMemset(h->m_ops_hi, 0, fbytes(mp.ops_elems))) || (e = cudaMemset(h->m_ops_lo, 0, fbytes(mp.ops_elems)))
 		    || (e = dmrgpp::dev_malloc(&d_jobs, std::max<size_t>(jobs.size(), 1) * sizeof(PackJob)))
 		    || (e = cudaMemcpy(d_jobs, jobs.data(), jobs.size() * sizeof(PackJob), cudaMemcpyHostToDevice))
@@ -498,42 +508,49 @@ int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm, Clock:
 	if ((e = dmrgpp::dev_malloc(&h->d_y, dim * sizeof(double))))
 		return bail(e, "device allocation (y)");
 
-	if ((e = cudaHostAlloc(reinterpret_cast<void**>(&h->err_host), sizeof(int), cudaHostAllocMapped)))
-		return bail(e, "cudaHostAlloc(error word)");
-	*h->err_host = 0;
-	if ((e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&h->err_dev), h->err_host, 0)))
-		return bail(e, "error word mapping");
+	if ((e = dmrgpp::error_word_alloc(&h->err_host, &h->err_dev)))
+		return bail(e, "error word");
 	if (int rc = dmrgpp::configure_schedule(h, bm == 32 ? 0 : 2, 2)) {
 		const std::string why = h->err;
 		release(h);
 		delete h;
 		return fail(nullptr, rc, why);
 	}
+	// the TF32x3 form's host planning (reads the plan, writes plan.mixed)
+	// runs on its own thread while the operators are uploaded
+	dmrgpp::MixedHost mixed_host;
+	std::thread       mixed_thread;
+	if (h->precision == DMRGPP_TF32X3) {
+		int sms = 0;
+		if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device)))
+			return bail(e, "SM count");
+		mixed_thread = std::thread([h, sms, &mixed_host] { dmrgpp::mixed_host_plan(h, sms, mixed_host); });
+	}
+	auto join_mixed = [&] {
+		if (mixed_thread.joinable())
+			mixed_thread.join();
+	};
+	auto abandon = [&](int rc) { // the thread reads h: join it before h goes
+		join_mixed();
+		const std::string why = h->err;
+		release(h);
+		delete h;
+		return fail(nullptr, rc, why);
+	};
 	h->setup_times[DMRGPP_SETUP_ALLOC] = seconds_since(tp);
 	tp                                 = Clock::now();
-	if (int rc = dmrgpp::upload_operators(h, &h->setup_times[DMRGPP_SETUP_UPLOAD_FILL])) {
-		const std::string why = h->err;
-		release(h);
-		delete h;
-		return fail(nullptr, rc, why);
-	}
+	if (int rc = dmrgpp::upload_operators(h, &h->setup_times[DMRGPP_SETUP_UPLOAD_FILL]))
+		return abandon(rc);
 	h->setup_times[DMRGPP_SETUP_UPLOAD] = seconds_since(tp);
 	tp                                  = Clock::now();
-	if (int rc = dmrgpp::upload_diagonal(h)) {
-		const std::string why = h->err;
-		release(h);
-		delete h;
-		return fail(nullptr, rc, why);
-	}
+	if (int rc = dmrgpp::upload_diagonal(h))
+		return abandon(rc);
 	h->setup_times[DMRGPP_SETUP_DIAGONAL] = seconds_since(tp);
 	tp                                    = Clock::now();
 	if (h->precision == DMRGPP_TF32X3) {
-		if (int rc = dmrgpp::build_mixed(h)) {
-			const std::string why = h->err;
-			release(h);
-			delete h;
-			return fail(nullptr, rc, why);
-		}
+		join_mixed();
+		if (int rc = dmrgpp::build_mixed(h, mixed_host))
+			return abandon(rc);
 		h->setup_times[DMRGPP_SETUP_MIXED] = seconds_since(tp);
 	}
 	h->setup_times[DMRGPP_SETUP_TOTAL] = seconds_since(t0);

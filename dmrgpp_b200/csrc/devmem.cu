@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <map>
 #include <mutex>
+#include <vector>
 
 namespace dmrgpp {
 
@@ -63,7 +64,56 @@ cudaError_t pool_of(int device, DevicePool** out)
 	return cudaSuccess;
 }
 
+// error words: one per 64-byte line, 1024 per slab, slabs never freed
+constexpr int kWordStride = 16; // ints
+constexpr int kSlabWords  = 1024;
+
+struct WordSlabs {
+	std::mutex        mu;
+	std::vector<int*> free_words;
+};
+
+WordSlabs& word_slabs()
+{
+	static WordSlabs* w = new WordSlabs();
+	return *w;
+}
+
 } // namespace
+
+cudaError_t error_word_alloc(int** host, int** dev)
+{
+	WordSlabs&                  w = word_slabs();
+	std::lock_guard<std::mutex> g(w.mu);
+	if (w.free_words.empty()) {
+		int*        slab = nullptr;
+		cudaError_t e    = cudaHostAlloc(reinterpret_cast<void**>(&slab),
+                                          size_t(kSlabWords) * kWordStride * sizeof(int),
+                                          cudaHostAllocMapped | cudaHostAllocPortable);
+		if (e != cudaSuccess)
+			return e;
+		for (int q = kSlabWords - 1; q >= 0; --q)
+			w.free_words.push_back(slab + size_t(q) * kWordStride);
+	}
+	int* word = w.free_words.back();
+	int* d    = nullptr;
+	if (cudaError_t e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&d), word, 0))
+		return e;
+	w.free_words.pop_back();
+	*word = 0;
+	*host = word;
+	*dev  = d;
+	return cudaSuccess;
+}
+
+void error_word_free(int* host)
+{
+	if (!host)
+		return;
+	WordSlabs&                  w = word_slabs();
+	std::lock_guard<std::mutex> g(w.mu);
+	w.free_words.push_back(host);
+}
 
 cudaError_t dev_malloc_bytes(void** p, size_t bytes)
 {

@@ -22,6 +22,12 @@ cudaError_t dev_malloc_bytes(void** p, size_t bytes);
 // implicit synchronisation as cudaFree).  Null is ignored.
 void dev_free(void* p);
 
+// A mapped pinned int (zeroed) for a kernel-to-host error word, from slabs
+// shared by all handles of the process (a cudaHostAlloc per handle costs
+// milliseconds).  *dev is the device view of *host.
+cudaError_t error_word_alloc(int** host, int** dev);
+void        error_word_free(int* host);
+
 template <class T> cudaError_t dev_malloc(T** p, size_t bytes)
 {
 	return dev_malloc_bytes(reinterpret_cast<void**>(p), bytes);

@@ -95,9 +95,22 @@ int upload_operators(dmrgpp_kron_handle h, double* seconds_fill);
 // packed operators (after upload_operators); waits for it.
 int upload_diagonal(dmrgpp_kron_handle h);
 
-// Builds and uploads the TF32x3 tensor-core form of the sector from the
-// plan's host blocks (create time only).
-int build_mixed(dmrgpp_kron_handle h);
+// Host planning of the TF32x3 tensor-core form: plan.mixed, the per-CTA
+// tile runs, the x map and the device packing jobs.  Reads h->plan and
+// writes only h->plan.mixed and out, so it may run on another thread while
+// the FP64 operators are uploaded.
+struct MixedHost {
+	bool                 ready = false;
+	std::string          msg;
+	std::vector<int>     xmap, starts1, starts2;
+	int                  grid1 = 0, grid2 = 0;
+	std::vector<PackJob> jobs;
+};
+void mixed_host_plan(dmrgpp_kron_handle h, int sms, MixedHost& out);
+
+// Uploads the TF32x3 form planned in host (create time only, after the FP64
+// operators are on the device).
+int build_mixed(dmrgpp_kron_handle h, MixedHost& host);
 
 // (Re)builds and uploads the persistent schedule of h for tile configuration
 // cfg (0..kNumTileCfgs-1), aiming at items_per_cta work items per CTA.
