@@ -107,6 +107,7 @@ SIGNATURES.update({
     "dmrgpp_mlp_forward": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp]),
     "dmrgpp_mlp_backward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _dp, _vp]),
     "dmrgpp_mlp_adam_step": (ctypes.c_int, [_vp, ctypes.c_float, _vp]),
+    "dmrgpp_mlp_set_inference": (ctypes.c_int, [_vp, ctypes.c_int]),
     "dmrgpp_mlp_precondition": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp,
                                                _sz, _vp]),
     "dmrgpp_mlp_last_error": (ctypes.c_char_p, [_vp]),

@@ -11,12 +11,26 @@
 // linear function of the inputs).  Training minimises the mean squared error
 // between o and the scaled exact correction t*_e * s / rms.
 //
-// Parameters are kept in FP32 (master copy, Adam state); inference runs
-// with BF16 copies of the weights and FP32 accumulation.  Contractions use
-// one tiled FP32 GEMM kernel whose reduction order is fixed, so training is
-// bitwise reproducible.
+// Parameters are kept in FP32 (master copy, Adam state).  Training runs its
+// contractions in one tiled FP32 GEMM kernel whose reduction order is fixed,
+// so it is bitwise reproducible.  Inference (the preconditioner applied in
+// a solve) uses BF16 copies of the weights with FP32 accumulation, by
+// default in one fused tcgen05 kernel (mlp_infer_tc_kernel):
+//   per tile of 128 elements, 4 warps compute the features and layer 1 on
+//   the CUDA cores and write h1 as BF16 into a ring of 64-unit chunks in the
+//   128-byte-swizzled K-major layout; one thread issues the layer-2 MMAs
+//   (kind::f16, BF16 x BF16 -> FP32, M = 128, N = 256, K = 16) against W2
+//   kept in shared memory for the whole launch, into one of two TMEM
+//   accumulators (2 x 256 columns); 4 epilogue warps read the accumulator
+//   row by row (tcgen05.ld), apply bias and tanh and reduce with w3.
+// The per-element work is 2 x 256 tanh and 66k MACs, so the fused kernel is
+// bound by the tanh (SFU) throughput, not by the tensor cores or HBM.
+// The earlier CUDA-core inference (BF16 weights widened to FP32, h1 kept in
+// FP32) stays selectable (dmrgpp_mlp_set_inference).
+#include "devmem.h"
 #include "dmrgpp_kron.h"
 #include "mlp.h"
+#include "tc_common.cuh"
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -68,6 +82,9 @@ struct dmrgpp_mlp_s {
 	double*        partial = nullptr;
 	unsigned*      ctr     = nullptr;
 	int            last_rows = 0;
+	int            inference = DMRGPP_MLP_TENSOR_CORES;
+	int*           err_host  = nullptr; // mapped word: a tensor-core launch gave up
+	int*           err_dev   = nullptr;
 	std::string    err;
 };
 
@@ -301,6 +318,253 @@ __global__ void k_scale_out(const float* __restrict__ o, double scale, double* _
 		t[e] = double(o[e]) * scale;
 }
 
+// ------------------------------------------------ tensor-core inference
+constexpr int kTcRows    = 128;                 // elements per tile = TMEM lanes
+constexpr int kTcSlots   = 4;                   // ring of h1 chunks (64 units each)
+constexpr int kTcThreads = 288;                 // layer-1 warps 0-3, epilogue 4-7, MMA 8
+constexpr int kW2Bytes   = H * H * 2;           // BF16 W2, 128 KB
+constexpr int kSlotBytes = kTcRows * 128;       // 128 rows x 64 BF16
+constexpr int kTcSmem    = kW2Bytes + kTcSlots * kSlotBytes + 1024;
+
+struct MlpTcArgs {
+	const double*        diag;
+	const double*        r;
+	double*              t;
+	long long            n;
+	int                  ntiles;
+	double               theta, s, rms, scale; // scale = rms / s
+	const float*         p;  // parameters: BF16 values widened to FP32
+	const __nv_bfloat16* w2; // BF16 W2 (row j = hidden unit j of layer 2)
+	int*                 error;
+};
+
+// kind::f16: D = F32, A = B = BF16, both K-major, M = 128, N = 256
+__device__ __forceinline__ unsigned idesc_bf16_128x256()
+{
+	return (1u << 4) | (1u << 7) | (1u << 10) | (unsigned(256 >> 3) << 17) | (unsigned(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(unsigned d, uint64_t a, uint64_t b, unsigned idesc, unsigned acc)
+{
+	asm volatile("{\n\t.reg .pred p;\n\t"
+	             "setp.ne.b32 p, %4, 0;\n\t"
+	             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+	             "l"(a), "l"(b), "r"(idesc), "r"(acc)
+	             : "memory");
+}
+
+__device__ __forceinline__ float tanh_sfu(float x)
+{
+	float y;
+	asm("tanh.approx.f32 %0, %1;\n" : "=f"(y) : "f"(x));
+	return y;
+}
+
+// generic-proxy shared-memory writes -> visible to the tensor cores
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// byte offset of 16-byte unit u (0..7) of a 128-byte row in the
+// 128-byte-swizzled K-major layout (8-row atoms of 1024 bytes)
+__device__ __forceinline__ unsigned swz(int row, int u)
+{
+	return unsigned(row) * 128u + unsigned((u ^ (row & 7)) * 16);
+}
+
+__device__ __forceinline__ unsigned bf16x2(float lo, float hi)
+{
+	const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+	return *reinterpret_cast<const unsigned*>(&v);
+}
+
+__device__ __forceinline__ void mlp_give_up(volatile int* abort, int* error)
+{
+	*abort = 1;
+	atomicExch(error, 2);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) mlp_infer_tc_kernel(const __grid_constant__ MlpTcArgs a)
+{
+	using namespace tc;
+	extern __shared__ unsigned char smem_raw[];
+	__shared__ float                           sW1[H * F], sb1[H], sb2[H], sw3[H];
+	__shared__ float                           sb3;
+	__shared__ __align__(8) unsigned long long bars[2 * kTcSlots + 5];
+	__shared__ unsigned                        tmem_slot;
+	__shared__ volatile int                    abort_flag;
+
+	const unsigned raw   = smem_addr(smem_raw);
+	const unsigned base  = (raw + 1023u) & ~1023u; // W2, then the ring
+	unsigned char* basep = smem_raw + (base - raw);
+	const unsigned full0 = smem_addr(&bars[0]), empty0 = smem_addr(&bars[kTcSlots]);
+	const unsigned accf0 = smem_addr(&bars[2 * kTcSlots]), acce0 = smem_addr(&bars[2 * kTcSlots + 2]);
+	const unsigned drain = smem_addr(&bars[2 * kTcSlots + 4]);
+	const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+	for (int i = threadIdx.x; i < H * F; i += kTcThreads)
+		sW1[i] = a.p[kW1 + i];
+	for (int i = threadIdx.x; i < H; i += kTcThreads) {
+		sb1[i] = a.p[kB1 + i];
+		sb2[i] = a.p[kB2 + i];
+		sw3[i] = a.p[kW3 + i];
+	}
+	if (threadIdx.x == 0)
+		sb3 = a.p[kB3];
+	// W2 as the B operand (N = 256 rows j, K = 256): K-chunk c holds units
+	// 64c .. 64c+63 of every row, 32 KB per chunk
+	const uint4* w2g = reinterpret_cast<const uint4*>(a.w2);
+	for (int u = threadIdx.x; u < H * H / 8; u += kTcThreads) {
+		const int j = u >> 5, q = u & 31;
+		*reinterpret_cast<uint4*>(basep + (q >> 3) * (H * 128) + swz(j, q & 7)) = w2g[u];
+	}
+	fence_async_smem();
+	if (warp == 8) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+		                 smem_addr(&tmem_slot)),
+		             "r"(512u)
+		             : "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+	}
+	if (threadIdx.x == 0) {
+		abort_flag = 0;
+		for (int q = 0; q < kTcSlots; ++q) {
+			mbar_init(full0 + 8 * q, 4); // one arrival per layer-1 warp
+			mbar_init(empty0 + 8 * q, 1);
+		}
+		for (int b = 0; b < 2; ++b) {
+			mbar_init(accf0 + 8 * b, 1);
+			mbar_init(acce0 + 8 * b, 4); // one arrival per epilogue warp
+		}
+		mbar_init(drain, 1);
+		asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const unsigned tmem = tmem_slot;
+	const unsigned ring = base + kW2Bytes;
+
+	if (warp < 4) {
+		// layer 1: thread = element row of the tile
+		const int row = threadIdx.x;
+		unsigned  g   = 0;
+		bool      ok  = true;
+		for (int tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x) {
+			const long long e    = (long long)tile * kTcRows + row;
+			float           x[F] = { 0.f, 0.f, 0.f, 0.f };
+			if (e < a.n)
+				features(a.diag[e], a.r[e], a.theta, a.s, a.rms, x);
+			for (int c = 0; c < H / 64; ++c) {
+				const unsigned slot = g % kTcSlots;
+				if (g >= kTcSlots)
+					ok = __all_sync(0xffffffffu, mbar_wait(empty0 + 8 * slot, ((g / kTcSlots) - 1) & 1, &abort_flag));
+				if (!ok)
+					break;
+				unsigned char* dst = basep + kW2Bytes + slot * kSlotBytes;
+#pragma unroll
+				for (int u = 0; u < 8; ++u) {
+					unsigned w[4];
+#pragma unroll
+					for (int q = 0; q < 4; ++q) {
+						const int j0 = c * 64 + u * 8 + 2 * q;
+						float     h[2];
+#pragma unroll
+						for (int k = 0; k < 2; ++k) {
+							const float* wr = sW1 + (j0 + k) * F;
+							h[k] = tanh_sfu(fmaf(wr[3], x[3], fmaf(wr[2], x[2], fmaf(wr[1], x[1], fmaf(wr[0], x[0], sb1[j0 + k])))));
+						}
+						w[q] = bf16x2(h[0], h[1]);
+					}
+					*reinterpret_cast<uint4*>(dst + swz(row, u)) = make_uint4(w[0], w[1], w[2], w[3]);
+				}
+				fence_async_smem();
+				__syncwarp();
+				if (lane == 0)
+					mbar_arrive(full0 + 8 * slot);
+				++g;
+			}
+		}
+		if (!ok && lane == 0)
+			mlp_give_up(&abort_flag, a.error);
+	} else if (warp < 8) {
+		// epilogue: TMEM lanes 32 (warp % 4) ..
+		const int quarter = warp & 3, row = quarter * 32 + lane;
+		unsigned  tcount  = 0;
+		bool      ok      = true;
+		for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+			const unsigned b = tcount & 1;
+			ok               = __all_sync(0xffffffffu, mbar_wait(accf0 + 8 * b, (tcount >> 1) & 1, &abort_flag));
+			if (!ok)
+				break;
+			tc_fence_after();
+			float o = 0.f;
+			for (int c0 = 0; c0 < H; c0 += 32) {
+				float v[32];
+				tmem_ld32(tmem + (unsigned(quarter * 32) << 16) + b * 256u + unsigned(c0), v);
+#pragma unroll
+				for (int i = 0; i < 32; ++i)
+					o = fmaf(sw3[c0 + i], tanh_sfu(v[i] + sb2[c0 + i]), o);
+			}
+			tc_fence_before();
+			__syncwarp();
+			if (lane == 0)
+				mbar_arrive(acce0 + 8 * b);
+			const long long e = (long long)tile * kTcRows + row;
+			if (e < a.n)
+				a.t[e] = double(o + sb3) * a.scale;
+			++tcount;
+		}
+		if (!ok && lane == 0)
+			mlp_give_up(&abort_flag, a.error);
+	} else if (lane == 0) {
+		// layer-2 MMAs
+		const unsigned idesc  = idesc_bf16_128x256();
+		unsigned       g      = 0, tcount = 0;
+		bool           ok     = true, issued = false;
+		for (int tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x) {
+			const unsigned b = tcount & 1;
+			if (tcount >= 2 && !mbar_wait(acce0 + 8 * b, ((tcount >> 1) - 1) & 1, &abort_flag)) {
+				ok = false;
+				break;
+			}
+			tc_fence_after();
+			const unsigned d = tmem + b * 256u;
+			for (int c = 0; c < H / 64; ++c) {
+				const unsigned slot = g % kTcSlots;
+				if (!mbar_wait(full0 + 8 * slot, (g / kTcSlots) & 1, &abort_flag)) {
+					ok = false;
+					break;
+				}
+				tc_fence_after();
+#pragma unroll
+				for (int ks = 0; ks < 4; ++ks) // K = 16 BF16 = 32 bytes per MMA
+					mma_bf16(d, smem_desc(ring + slot * kSlotBytes + ks * 32),
+					         smem_desc(base + c * (H * 128) + ks * 32), idesc, (c | ks) != 0);
+				mma_commit(empty0 + 8 * slot);
+				issued = true;
+				++g;
+			}
+			if (!ok)
+				break;
+			mma_commit(accf0 + 8 * b);
+			++tcount;
+		}
+		if (!ok)
+			mlp_give_up(&abort_flag, a.error);
+		if (issued) {
+			mma_commit(drain);
+			if (!mbar_wait(drain, 0, nullptr))
+				mlp_give_up(&abort_flag, a.error);
+		}
+	}
+	__syncwarp();
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	if (warp == 8)
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512u)
+		             : "memory");
+}
+
 int grid_for(size_t n, int threads = 256)
 {
 	size_t b = (n + threads - 1) / threads;
@@ -358,6 +622,42 @@ int mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, d
 	// inference weights: BF16 values widened to FP32 (the network as it ships)
 	k_from_bf16<<<grid_for(kNumParams), 256, 0, st>>>(m->wbf, m->pinf, kNumParams);
 	const float* pinf = m->pinf;
+	if (m->inference == DMRGPP_MLP_TENSOR_CORES) {
+		if (*reinterpret_cast<volatile int*>(m->err_host)) {
+			*m->err_host = 0;
+			return mlp_fail(m, DMRGPP_TIMEOUT, "an earlier tensor-core MLP launch gave up waiting");
+		}
+		if (n == 0)
+			return DMRGPP_OK;
+		static thread_local int attr_device = -1;
+		int                     dev = 0, sms = 0;
+		cudaError_t             e   = cudaGetDevice(&dev);
+		if (!e && attr_device != dev) {
+			e = cudaFuncSetAttribute(mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+			if (!e)
+				attr_device = dev;
+		}
+		if (!e)
+			e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+		if (e)
+			return mlp_cuda(m, e, "MLP tensor-core kernel attributes");
+		MlpTcArgs a;
+		a.diag   = diag;
+		a.r      = r;
+		a.t      = t;
+		a.n      = (long long)n;
+		a.ntiles = int((n + kTcRows - 1) / kTcRows);
+		a.theta  = theta;
+		a.s      = s;
+		a.rms    = rms;
+		a.scale  = rms / s;
+		a.p      = pinf;
+		a.w2     = m->wbf + kW2;
+		a.error  = m->err_dev;
+		mlp_infer_tc_kernel<<<unsigned(std::min(a.ntiles, sms)), kTcThreads, kTcSmem, st>>>(a);
+		e = cudaGetLastError();
+		return e == cudaSuccess ? DMRGPP_OK : mlp_cuda(m, e, "MLP tensor-core inference");
+	}
 	const int chunk = 1 << 16;
 	if (int rc = ensure_rows(m, int(std::min<size_t>(n, chunk))))
 		return rc;
@@ -412,7 +712,8 @@ int dmrgpp_mlp_create(unsigned long long seed, dmrgpp_mlp_handle* out)
 	    || (e = cudaMalloc(&m->ctr, sizeof(unsigned))) || (e = cudaMemset(m->ctr, 0, sizeof(unsigned)))
 	    || (e = cudaMemset(m->adam_m, 0, kNumParams * sizeof(float)))
 	    || (e = cudaMemset(m->adam_v, 0, kNumParams * sizeof(float)))
-	    || (e = cudaMemcpy(m->params, p.data(), kNumParams * sizeof(float), cudaMemcpyHostToDevice))) {
+	    || (e = cudaMemcpy(m->params, p.data(), kNumParams * sizeof(float), cudaMemcpyHostToDevice))
+	    || (e = error_word_alloc(&m->err_host, &m->err_dev))) {
 		const int rc = mlp_cuda(nullptr, e, "MLP create");
 		dmrgpp_mlp_destroy(m);
 		return rc;
@@ -442,7 +743,18 @@ int dmrgpp_mlp_destroy(dmrgpp_mlp_handle m)
 	cudaFree(m->gout);
 	cudaFree(m->dz);
 	cudaFree(m->dz1);
+	dmrgpp::error_word_free(m->err_host);
 	delete m;
+	return DMRGPP_OK;
+}
+
+int dmrgpp_mlp_set_inference(dmrgpp_mlp_handle m, int mode)
+{
+	if (!m)
+		return dmrgpp::mlp_fail(nullptr, DMRGPP_INVALID_ARG, "null handle");
+	if (mode != DMRGPP_MLP_TENSOR_CORES && mode != DMRGPP_MLP_CUDA_CORES)
+		return dmrgpp::mlp_fail(m, DMRGPP_INVALID_ARG, "unknown inference mode");
+	m->inference = mode;
 	return DMRGPP_OK;
 }
 

@@ -100,6 +100,13 @@ class MLPPreconditioner:
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         self._check(self._lib.dmrgpp_mlp_adam_step(self._h, lr, s))
 
+    TENSOR_CORES, CUDA_CORES = 0, 1
+
+    def set_inference(self, mode: int) -> None:
+        """TENSOR_CORES (default): fused tcgen05 kernel, first hidden layer
+        in BF16; CUDA_CORES: the FP32 GEMM kernels of training."""
+        self._check(self._lib.dmrgpp_mlp_set_inference(self._h, int(mode)))
+
     def precondition(self, diag, r, theta: float, rnorm: float, stream=None):
         import torch
         t = torch.empty_like(r)

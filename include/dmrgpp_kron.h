@@ -365,7 +365,16 @@ int         dmrgpp_mlp_forward(dmrgpp_mlp_handle m, const float* x, int rows, fl
 int         dmrgpp_mlp_backward(dmrgpp_mlp_handle m, const float* x, const float* y,
                                 const float* weight, double* loss, void* stream);
 int         dmrgpp_mlp_adam_step(dmrgpp_mlp_handle m, float lr, void* stream);
-/* t = learned correction of residual r (what the Davidson solver applies) */
+/* t = learned correction of residual r (what the Davidson solver applies).
+ * Inference uses the BF16 copy of the weights with FP32 accumulation:
+ * DMRGPP_MLP_TENSOR_CORES (default) runs one fused tcgen05 kernel (layer 1
+ * and both tanh on the CUDA cores, h1 rounded to BF16, layer 2 as BF16 MMAs
+ * into FP32 tensor memory); DMRGPP_MLP_CUDA_CORES runs the FP32 GEMM kernels
+ * of training with the BF16 weights widened to FP32 (h1 kept in FP32).  A
+ * tensor-core launch whose bounded wait gave up is reported as
+ * DMRGPP_TIMEOUT by the next precondition call. */
+enum { DMRGPP_MLP_TENSOR_CORES = 0, DMRGPP_MLP_CUDA_CORES = 1 };
+int         dmrgpp_mlp_set_inference(dmrgpp_mlp_handle m, int mode);
 int         dmrgpp_mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r,
                                     double theta, double rnorm, double* t, size_t n, void* stream);
 const char* dmrgpp_mlp_last_error(dmrgpp_mlp_handle m);

@@ -33,9 +33,21 @@ def features(d, r, theta, rnorm):
     return x
 
 
-def forward(flat, x):
+def to_bf16(a):
+    """Round to the nearest BF16 value (ties to even), returned as float64."""
+    u = np.asarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def forward(flat, x, bf16_hidden=False):
+    """Network output; bf16_hidden rounds the first hidden layer to BF16
+    before the second layer (the operand format of the tensor-core
+    inference, mlp.cu)."""
     p = unpack(flat)
     h1 = np.tanh(x @ p["W1"].T + p["b1"])
+    if bf16_hidden:
+        h1 = to_bf16(h1)
     h2 = np.tanh(h1 @ p["W2"].T + p["b2"])
     o = h2 @ p["w3"] + p["b3"][0]
     return o, (h1, h2)

@@ -89,6 +89,7 @@ def test_mlp_inference_uses_bf16_weights(cuda_lib, cuda_device):
     from oracle import mlp_oracle
     rng = np.random.default_rng(1)
     m = MLPPreconditioner(seed=5)
+    m.set_inference(MLPPreconditioner.CUDA_CORES)
     p = m.get_params()
     pb = torch.tensor(p).to(torch.bfloat16).to(torch.float64).numpy()
     n = 5000
@@ -101,6 +102,39 @@ def test_mlp_inference_uses_bf16_weights(cuda_lib, cuda_device):
     o, _ = mlp_oracle.forward(pb, x.astype(np.float32).astype(np.float64))
     t_ref = o * (rn / np.sqrt(n)) / max(1.0, abs(theta))
     assert np.abs(t.cpu().numpy() - t_ref).max() < 2e-4 * np.abs(t_ref).max()
+    m.close()
+
+
+@pytest.mark.parametrize("n", [5000, 128 * 37 + 1, 1, 300_000])
+def test_mlp_tensor_core_inference(cuda_lib, cuda_device, n):
+    """The fused tcgen05 inference (BF16 weights and first hidden layer,
+    BF16 MMAs with FP32 accumulation in tensor memory, SFU tanh) against the
+    FP64 oracle with the same BF16 roundings, and against the CUDA-core path;
+    ragged last tiles and more tiles than SMs included; reproducible."""
+    import torch
+    from dmrgpp_b200.mlp import MLPPreconditioner
+    from oracle import mlp_oracle
+    rng = np.random.default_rng(n)
+    m = MLPPreconditioner(seed=7)
+    p = m.get_params()
+    p[:] = p * 1.5 + rng.normal(0.0, 0.1, p.shape)   # biases away from zero too
+    m.set_params(p.astype(np.float32))
+    pb = mlp_oracle.to_bf16(m.get_params())
+    d = torch.tensor(rng.standard_normal(n) * 3, dtype=torch.float64, device="cuda")
+    r = torch.tensor(rng.standard_normal(n), dtype=torch.float64, device="cuda")
+    theta, rn = -1.7, float(torch.linalg.vector_norm(r))
+    t1 = m.precondition(d, r, theta, rn)
+    t2 = m.precondition(d, r, theta, rn)
+    m.set_inference(MLPPreconditioner.CUDA_CORES)
+    tc = m.precondition(d, r, theta, rn)
+    torch.cuda.synchronize()
+    assert torch.equal(t1, t2)
+    x = m.features(d, r, theta, rn).double().cpu().numpy()
+    o, _ = mlp_oracle.forward(pb, x, bf16_hidden=True)
+    t_ref = o * (rn / np.sqrt(n)) / max(1.0, abs(theta))
+    scale = np.abs(t_ref).max()
+    assert np.abs(t1.cpu().numpy() - t_ref).max() < 1e-2 * scale
+    assert np.abs(t1.cpu().numpy() - tc.cpu().numpy()).max() < 2e-2 * scale
     m.close()
 
 
