@@ -6,10 +6,13 @@ only the kernels of that workload.
                                           [--config C --ipc I]
     python -m dmrgpp_b200.profile_case ladder --states 4000 --precision tf32x3
     python -m dmrgpp_b200.profile_case ladder --states 4000 --solve lanczos
+    python -m dmrgpp_b200.profile_case mlp --elements 300000 [--inference cuda_cores]
 
 Workloads: c2 = the 1024 x 1024-state, 21-group, K=5 microbench sector;
 ladder = the ladder-shaped (N_up, N_down) sector with `--states` left and
-right states (K = 10).  Prints one line "ok <dim> <F_alg> <|y|>" at the end.
+right states (K = 10); mlp = learned-preconditioner applications (seeded
+network, seeded diagonal and residual of `--elements` entries).  Prints one
+line "ok ..." at the end.
 """
 from __future__ import annotations
 
@@ -19,7 +22,9 @@ import sys
 
 def main(argv=None) -> int:
     p = argparse.ArgumentParser()
-    p.add_argument("workload", choices=["c2", "ladder"])
+    p.add_argument("workload", choices=["c2", "ladder", "mlp"])
+    p.add_argument("--elements", type=int, default=300000, help="mlp: vector length")
+    p.add_argument("--inference", default="tensor_cores", choices=["tensor_cores", "cuda_cores"])
     p.add_argument("--states", type=int, default=4000, help="ladder: left = right states")
     p.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"])
     p.add_argument("--applies", type=int, default=6)
@@ -33,6 +38,22 @@ def main(argv=None) -> int:
     import torch
     from . import plugin
     from . import superblock as sb
+
+    if a.workload == "mlp":
+        import numpy as np
+        from .mlp import MLPPreconditioner
+        m = MLPPreconditioner(seed=7)
+        m.set_inference(m.TENSOR_CORES if a.inference == "tensor_cores" else m.CUDA_CORES)
+        rng = np.random.default_rng(0)
+        d = torch.tensor(rng.standard_normal(a.elements) * 3, dtype=torch.float64, device="cuda")
+        r = torch.tensor(rng.standard_normal(a.elements), dtype=torch.float64, device="cuda")
+        rn = float(torch.linalg.vector_norm(r))
+        for _ in range(a.applies):
+            t = m.precondition(d, r, -1.7, rn)
+        torch.cuda.synchronize()
+        print("ok", a.elements, float(t.abs().max()))
+        m.close()
+        return 0
 
     prob = (sb.c2_problem() if a.workload == "c2"
             else sb.ladder_problem(total_states=a.states, sigma=2.5, seed=9))
