@@ -363,7 +363,8 @@ def ladder_measurements(torch, dev, stream):
         out[f"matvec_{name}"] = {"ms": t * 1e3, "tflops_alg": f / t / 1e12}
     bg.close()
     out["matvec_speedup_tf32x3_vs_fp64"] = out["matvec_fp64"]["ms"] / out["matvec_tf32x3"]["ms"]
-    out["solve"] = sweep.sector_solves(prob, sites=64, mixed_steps=100, refine_inner=60,
+    out["solve"] = sweep.sector_solves(prob, sites=64, mixed_steps=60, refine_inner=80,
+                                       refine_inner_tolerance=1e-2,
                                        with_davidson=False)
     return out
 

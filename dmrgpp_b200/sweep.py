@@ -30,8 +30,9 @@ def _timed(fn):
 
 
 def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int = 300,
-                  tolerance: float = 1e-9, mixed_steps: int = 100,
-                  refine_inner: int = 60, with_davidson: bool = True) -> Dict:
+                  tolerance: float = 1e-9, mixed_steps: int = 60,
+                  refine_inner: int = 80, refine_inner_tolerance: float = 1e-2,
+                  with_davidson: bool = True) -> Dict:
     """Lowest state of one sector by
       fp64_lanczos           -- the plain method: FP64 Lanczos, full reorthogonalisation,
                                 eigenvalue-change tolerance 1e-12 (reference defaults);
@@ -89,7 +90,8 @@ def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int 
     def mixed_refined():
         e1, z1, n1 = bg.lanczos_lowest(init, steps=mixed_steps, tolerance=1e-4)
         e2, st = bg.refine_lowest(z1, max_outer=8, tolerance=tolerance,
-                                  inner_iterations=refine_inner, inner_tolerance=1e-5,
+                                  inner_iterations=refine_inner,
+                                  inner_tolerance=refine_inner_tolerance,
                                   raise_on_no_convergence=False)
         return e2, z1, n1, st
     (e_r, z_r, n_r, st_r), t_r, _ = _timed(mixed_refined)
@@ -119,7 +121,8 @@ def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int 
     def warm_refined():
         psi = warm.clone()
         e2, st = bg.refine_lowest(psi, max_outer=12, tolerance=tolerance,
-                                  inner_iterations=refine_inner, inner_tolerance=1e-5,
+                                  inner_iterations=refine_inner,
+                                  inner_tolerance=refine_inner_tolerance,
                                   raise_on_no_convergence=False)
         return e2, psi, st
     (e_wr, z_wr, st_wr), t_wr, _ = _timed(warm_refined)
