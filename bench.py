@@ -366,7 +366,51 @@ def ladder_measurements(torch, dev, stream):
     out["solve"] = sweep.sector_solves(prob, sites=64, mixed_steps=60, refine_inner=80,
                                        refine_inner_tolerance=1e-2,
                                        with_davidson=False)
+    out["wft"] = wft_measurement(torch, prob, stream, flush)
     return out
+
+
+def wft_measurement(torch, prob, stream, flush):
+    """Wave-function transformation of the ladder sector's vector (the step
+    before each sweep-step solve: every patch block multiplied on both sides
+    by its groups' transformation blocks, here square N(0,1)/sqrt(n) blocks),
+    FP64 on the device against the oracle's per-patch numpy products on the
+    host cores (the reference's BlockDiagWf::transform does the same GEMMs)."""
+    from dmrgpp_b200.wft import WaveFunctionTransform
+    from oracle import wft_oracle
+    rng = np.random.default_rng(17)
+    l, r = prob.lsz, prob.rsz
+    src = list(range(prob.npatches))
+    WL = [rng.standard_normal((int(n), int(n))) / np.sqrt(n) for n in l]
+    WR = [rng.standard_normal((int(n), int(n))) / np.sqrt(n) for n in r]
+    w = WaveFunctionTransform(l, r, l, r, src, WL, WR, stream=stream.cuda_stream)
+    xh = rng.standard_normal(w.dim_in)
+    x = torch.from_numpy(xh).cuda()
+    y = torch.empty(w.dim_out, dtype=torch.float64, device=x.device)
+    for _ in range(3):
+        w(x, y)
+    ts = []
+    for _ in range(10):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        w(x, y)
+        b.record(stream)
+        ts.append((a, b))
+    torch.cuda.synchronize()
+    t = statistics.median(a.elapsed_time(b) for a, b in ts) / 1e3
+    ref = wft_oracle.transform(xh, l, r, l, r, src, WL, WR)
+    err = float(np.abs(y.cpu().numpy() - ref).max() / np.abs(ref).max())
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        wft_oracle.transform(xh, l, r, l, r, src, WL, WR)
+    t_cpu = (time.perf_counter() - t0) / reps
+    w.close()
+    return {"flops": w.flops, "ms": t * 1e3, "tflops": w.flops / t / 1e12,
+            "rel_err_vs_oracle": err,
+            "cpu_oracle": {"ms": t_cpu * 1e3, "tflops": w.flops / t_cpu / 1e12,
+                           "cores": os.cpu_count(), "kind": "port (numpy per-patch GEMMs)"}}
 
 
 def run_ours(args):

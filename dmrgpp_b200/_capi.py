@@ -30,6 +30,14 @@ class KronDesc(ctypes.Structure):
                 ("stream", ctypes.c_void_p), ("device", ctypes.c_int)]
 
 
+class WftDesc(ctypes.Structure):
+    _fields_ = [("np_in", _sz), ("l_in", _szp), ("r_in", _szp), ("np_out", _sz),
+                ("l_out", _szp), ("r_out", _szp), ("src", ctypes.POINTER(ctypes.c_longlong)),
+                ("WL", _vpp), ("ld_WL", _szp), ("WR", _vpp), ("ld_WR", _szp),
+                ("trans_WL", ctypes.c_int), ("trans_WR", ctypes.c_int),
+                ("stream", ctypes.c_void_p), ("device", ctypes.c_int)]
+
+
 class PlanInfo(ctypes.Structure):
     _fields_ = [("ntriples", _sz), ("dim", _sz), ("f_alg", ctypes.c_double),
                 ("operator_bytes", _sz), ("bx_bytes", _sz), ("pass1_tiles", _sz),
@@ -50,6 +58,12 @@ SIGNATURES = {
     "dmrgpp_kron_flops": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "dmrgpp_kron_setup_profile": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     "dmrgpp_release_cached_memory": (ctypes.c_int, [ctypes.c_int]),
+    "dmrgpp_wft_create": (ctypes.c_int, [ctypes.POINTER(WftDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "dmrgpp_wft_apply": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "dmrgpp_wft_dims": (ctypes.c_int, [ctypes.c_void_p, _szp, _szp]),
+    "dmrgpp_wft_flops": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "dmrgpp_wft_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dmrgpp_wft_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "dmrgpp_cached_memory": (ctypes.c_int, [ctypes.c_int, _szp, _szp]),
     "dmrgpp_kron_plan_info_get": (ctypes.c_int, [ctypes.POINTER(KronDesc),
                                                  ctypes.POINTER(PlanInfo)]),

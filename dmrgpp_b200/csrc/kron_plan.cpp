@@ -14,32 +14,6 @@ namespace dmrgpp {
 
 namespace {
 
-// f(0..n-1) on the host's cores (dynamic assignment; every f(i) writes its
-// own disjoint output, so the result does not depend on the thread count)
-template <class F> void parallel_for(size_t n, F f)
-{
-	size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 32);
-	nt        = std::min(nt, n);
-	if (nt < 2) {
-		for (size_t i = 0; i < n; ++i)
-			f(i);
-		return;
-	}
-	std::atomic<size_t>      next { 0 };
-	std::vector<std::thread> pool;
-	for (size_t t = 0; t < nt; ++t)
-		pool.emplace_back([&] {
-			for (;;) {
-				const size_t i = next.fetch_add(1);
-				if (i >= n)
-					break;
-				f(i);
-			}
-		});
-	for (std::thread& th : pool)
-		th.join();
-}
-
 constexpr long long kAlign = 32; // doubles (256 bytes) between packed blocks
 
 long long align_up(long long x) { return (x + kAlign - 1) / kAlign * kAlign; }

@@ -13,6 +13,9 @@
 // passes read their B operand K-contiguous.
 #pragma once
 
+#include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -21,6 +24,32 @@
 #include <vector>
 
 namespace dmrgpp {
+
+// f(0..n-1) on the host's cores (dynamic assignment; every f(i) writes its
+// own disjoint output, so the result does not depend on the thread count)
+template <class F> void parallel_for(size_t n, F f)
+{
+	size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 32);
+	nt        = std::min(nt, n);
+	if (nt < 2) {
+		for (size_t i = 0; i < n; ++i)
+			f(i);
+		return;
+	}
+	std::atomic<size_t>      next { 0 };
+	std::vector<std::thread> pool;
+	for (size_t t = 0; t < nt; ++t)
+		pool.emplace_back([&] {
+			for (;;) {
+				const size_t i = next.fetch_add(1);
+				if (i >= n)
+					break;
+				f(i);
+			}
+		});
+	for (std::thread& th : pool)
+		th.join();
+}
 
 // One K-segment of an output tile: C += A(M x K) * B(K x N), column-major,
 // offsets relative to the pass's A and B base pointers.

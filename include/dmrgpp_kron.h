@@ -392,6 +392,54 @@ int dmrgpp_tridiag_eigen(size_t n, const double* diag, const double* offdiag, do
 int dmrgpp_gather(const double* src, const int64_t* idx, double* dst, size_t n, void* stream);
 int dmrgpp_scatter(const double* src, const int64_t* idx, double* dst, size_t n, void* stream);
 
+/* ---- Wave-function transformation between two patch layouts ----
+ * The GEMM core of the reference's patch-wise WFT (Wft/WftAccelPatches.h:
+ * 43-66, BlockDiagWf.h:131-260 ParallelBlockTransform::doTask): per patch,
+ * Ynew = opL(W_L) * Yold * opR(W_R) with the block-diagonal transformations
+ * of the system and environment.  In the sector layout of this library a
+ * patch block is r x l column-major (right index fastest), so for every
+ * output patch q with source patch p = src[q] >= 0:
+ *     Y_q = WR_q * X_p * WL_q^T,
+ * WR_q applied to the right index (r_out[q] x r_in[p]) and WL_q to the left
+ * index (l_out[q] x l_in[p]); in the reference's terms WL = opL(W_L) and
+ * WR = opR(W_R)^T.  trans_WL / trans_WR = 1: the given block is stored
+ * transposed (l_in[p] x l_out[q] / r_in[p] x r_out[q]), which covers the
+ * reference's 'C' / 'T' / 'N' choices for real blocks.  Output patches
+ * without a source (src[q] < 0) are zero.  The re-indexing of the
+ * transformed patches into the new superblock's order
+ * (BlockDiagWf::toVectorWithOffsets) is a permutation: dmrgpp_gather.
+ * Both contractions run as FP64 grouped GEMMs on the FP64 tensor pipe. */
+typedef struct {
+	size_t               np_in;
+	const size_t*        l_in;
+	const size_t*        r_in;
+	size_t               np_out;
+	const size_t*        l_out;
+	const size_t*        r_out;
+	const long long*     src;   /* np_out entries: source input patch or -1 */
+	const double* const* WL;    /* np_out blocks (NULL where src < 0) */
+	const size_t*        ld_WL;
+	const double* const* WR;
+	const size_t*        ld_WR;
+	int                  trans_WL;
+	int                  trans_WR;
+	void*                stream; /* cudaStream_t, NULL = default stream */
+	int                  device; /* -1 = current device */
+} dmrgpp_wft_desc;
+
+typedef struct dmrgpp_wft_s* dmrgpp_wft_handle;
+
+int dmrgpp_wft_create(const dmrgpp_wft_desc* desc, dmrgpp_wft_handle* out);
+/* y (output layout) = transform of x (input layout); host pointers are copied
+ * through device staging, device pointers (on_device = 1) are used in place
+ * and the call only enqueues. */
+int dmrgpp_wft_apply(dmrgpp_wft_handle h, const double* x, double* y, int on_device);
+int dmrgpp_wft_dims(dmrgpp_wft_handle h, size_t* dim_in, size_t* dim_out);
+/* sum over transformed patches of 2 r_out r_in l_in + 2 r_out l_in l_out */
+int dmrgpp_wft_flops(dmrgpp_wft_handle h, double* flops);
+int dmrgpp_wft_destroy(dmrgpp_wft_handle h);
+const char* dmrgpp_wft_last_error(dmrgpp_wft_handle h);
+
 /* Last error message of a handle, or of the calling thread's last failed
  * create when h is NULL.  Never returns NULL. */
 const char* dmrgpp_kron_last_error(dmrgpp_kron_handle h);

@@ -168,3 +168,23 @@ def test_cpp_dropin_header_compiles_links_and_throws(cuda_lib, tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "caught: dmrgpp-b200:" in r.stdout and "empty" in r.stdout
+
+
+def test_wft_create_rejects_bad_descriptors(cuda_lib):
+    """Descriptor checks of the wave-function transformation happen before
+    any device work, with the reason in dmrgpp_wft_last_error(NULL)."""
+    from dmrgpp_b200 import _capi
+    from dmrgpp_b200 import wft as wft_mod
+    ok = dict(l_in=[2, 3], r_in=[3, 1], l_out=[2], r_out=[2], src=[1],
+              WL=[np.ones((2, 3))], WR=[np.ones((2, 1))])
+    for change, words in [({"src": [2]}, "out of range"),
+                          ({"WL": [None]}, "null transformation block"),
+                          ({"l_in": [2, 0]}, "empty"),
+                          ({"WR": [np.ones((1, 1))]}, "leading dimension")]:
+        kw = dict(ok, **change)
+        with pytest.raises(_capi.DmrgppError) as e:
+            wft_mod.WaveFunctionTransform(**kw)
+        assert e.value.status == _capi.INVALID_ARG and words in str(e.value), str(e.value)
+    h = ctypes.c_void_p()
+    assert cuda_lib.dmrgpp_wft_create(None, ctypes.byref(h)) == _capi.INVALID_ARG
+    assert cuda_lib.dmrgpp_wft_destroy(None) == _capi.OK
