@@ -58,6 +58,8 @@ SIGNATURES = {
     "dmrgpp_kron_flops": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "dmrgpp_kron_setup_profile": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     "dmrgpp_release_cached_memory": (ctypes.c_int, [ctypes.c_int]),
+    "dmrgpp_kron_create_complex": (ctypes.c_int, [ctypes.POINTER(KronDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    "dmrgpp_kron_is_complex": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "dmrgpp_wft_create": (ctypes.c_int, [ctypes.POINTER(WftDesc), ctypes.POINTER(ctypes.c_void_p)]),
     "dmrgpp_wft_apply": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "dmrgpp_wft_dims": (ctypes.c_int, [ctypes.c_void_p, _szp, _szp]),

@@ -75,6 +75,8 @@ void release(dmrgpp_kron_handle h)
 	dmrgpp::release_group(h);
 	dmrgpp::dev_free(h->d_diag);
 	h->d_diag = nullptr;
+	dmrgpp::dev_free(h->d_cx);
+	h->d_cx = nullptr;
 	dmrgpp::dev_free(h->m_ops_hi);
 	dmrgpp::dev_free(h->m_ops_lo);
 	dmrgpp::dev_free(h->m_xs_hi);
@@ -655,6 +657,105 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 	return finish_create(h, d->device, d->stream, bm, t0, out);
 }
 
+int dmrgpp_kron_create_complex(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
+{
+	if (!out)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "null output handle");
+	*out = nullptr;
+	if (int rc = check_desc(d))
+		return rc;
+	if (d->precision == DMRGPP_SPLIT_BF16)
+		return fail(nullptr, DMRGPP_NOT_SUPPORTED, "split-BF16 is not built into this library");
+	if (d->noperator == 0 || d->npatches == 0)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "noperator and npatches must be >= 1");
+	const size_t np = d->npatches, K = d->noperator, np2 = 2 * np, K2 = 2 * K;
+	if (np2 > size_t(INT_MAX))
+		return fail(nullptr, DMRGPP_INVALID_ARG, "too many patches");
+	// real embedding: patch p holds Re x_p, patch p + np holds Im x_p; with
+	// A = Ar + i Ai and B = Br + i Bi, A (x) B = (Ar(x)Br - Ai(x)Bi) + i (Ar(x)Bi + Ai(x)Br):
+	//   (i, j), (i+np, j+np):  Ar(x)Br, (-Ai)(x)Bi
+	//   (i, j+np):             (-Ar)(x)Bi, (-Ai)(x)Br
+	//   (i+np, j):             Ar(x)Bi, Ai(x)Br
+	// each complex term k becomes real terms 2k and 2k+1 of every quadrant
+	std::vector<size_t>        l2(np2), r2(np2);
+	std::vector<const double*> A2(np2 * np2 * K2, nullptr), B2(np2 * np2 * K2, nullptr);
+	std::vector<size_t>        ldA2(np2 * np2 * K2, 0), ldB2(np2 * np2 * K2, 0);
+	for (size_t p = 0; p < np; ++p) {
+		l2[p] = l2[p + np] = d->left_patch_size[p];
+		r2[p] = r2[p + np] = d->right_patch_size[p];
+	}
+	std::vector<std::vector<double>> store;
+	auto part = [&](const double* z, size_t ld, size_t rows, size_t cols, int im, double sign) {
+		store.emplace_back(rows * cols);
+		double* m = store.back().data();
+		for (size_t c = 0; c < cols; ++c)
+			for (size_t q = 0; q < rows; ++q)
+				m[q + c * rows] = sign * z[2 * (q + c * ld) + size_t(im)];
+		return static_cast<const double*>(m);
+	};
+	for (size_t k = 0; k < K; ++k)
+		for (size_t j = 0; j < np; ++j)
+			for (size_t i = 0; i < np; ++i) {
+				const size_t t = i + j * np + k * np * np;
+				if (!d->Amatrix[t] || !d->Bmatrix[t])
+					continue;
+				if (d->ld_Amatrix[t] < l2[i] || d->ld_Bmatrix[t] < r2[i])
+					return fail(nullptr, DMRGPP_INVALID_ARG,
+					            "leading dimension smaller than the block's rows at table entry "
+					                + std::to_string(t));
+				const size_t  li = l2[i], lj = l2[j], ri = r2[i], rj = r2[j];
+				const double* Ar  = part(d->Amatrix[t], d->ld_Amatrix[t], li, lj, 0, 1.0);
+				const double* Ai  = part(d->Amatrix[t], d->ld_Amatrix[t], li, lj, 1, 1.0);
+				const double* nAr = part(d->Amatrix[t], d->ld_Amatrix[t], li, lj, 0, -1.0);
+				const double* nAi = part(d->Amatrix[t], d->ld_Amatrix[t], li, lj, 1, -1.0);
+				const double* Br  = part(d->Bmatrix[t], d->ld_Bmatrix[t], ri, rj, 0, 1.0);
+				const double* Bi  = part(d->Bmatrix[t], d->ld_Bmatrix[t], ri, rj, 1, 1.0);
+				auto set = [&](size_t I, size_t J, size_t kk, const double* a, const double* b) {
+					const size_t u = I + J * np2 + kk * np2 * np2;
+					A2[u]          = a;
+					B2[u]          = b;
+					ldA2[u]        = l2[I];
+					ldB2[u]        = r2[I];
+				};
+				set(i, j, 2 * k, Ar, Br);
+				set(i, j, 2 * k + 1, nAi, Bi);
+				set(i + np, j + np, 2 * k, Ar, Br);
+				set(i + np, j + np, 2 * k + 1, nAi, Bi);
+				set(i, j + np, 2 * k, nAr, Bi);
+				set(i, j + np, 2 * k + 1, nAi, Br);
+				set(i + np, j, 2 * k, Ar, Bi);
+				set(i + np, j, 2 * k + 1, Ai, Br);
+			}
+	dmrgpp_kron_desc e = *d;
+	e.noperator        = K2;
+	e.npatches         = np2;
+	e.left_patch_size  = l2.data();
+	e.right_patch_size = r2.data();
+	e.Amatrix          = A2.data();
+	e.ld_Amatrix       = ldA2.data();
+	e.Bmatrix          = B2.data();
+	e.ld_Bmatrix       = ldB2.data();
+	dmrgpp_kron_handle h = nullptr;
+	if (int rc = dmrgpp_kron_create(&e, &h))
+		return rc;
+	h->complex_sector = true;
+	DeviceGuard       g(h->device);
+	if (cudaError_t err = dmrgpp::dev_malloc(&h->d_cx, size_t(std::max<long long>(h->plan.dim(), 1)) * sizeof(double))) {
+		dmrgpp_kron_destroy(h);
+		return cuda_fail(nullptr, err, "device allocation (complex staging)");
+	}
+	*out = h;
+	return DMRGPP_OK;
+}
+
+int dmrgpp_kron_is_complex(dmrgpp_kron_handle h, int* is_complex)
+{
+	if (!h || !is_complex)
+		return fail(h, DMRGPP_INVALID_ARG, "null argument");
+	*is_complex = h->complex_sector ? 1 : 0;
+	return DMRGPP_OK;
+}
+
 int dmrgpp_kron_create_group(const dmrgpp_kron_desc* descs, size_t nsectors, dmrgpp_kron_handle* out)
 {
 	if (!out)
@@ -756,7 +857,7 @@ int dmrgpp_kron_dim(dmrgpp_kron_handle h, size_t* dim)
 {
 	if (!h || !dim)
 		return fail(h, DMRGPP_INVALID_ARG, "null argument");
-	*dim = size_t(h->plan.dim());
+	*dim = size_t(h->plan.dim()) / (h->complex_sector ? 2 : 1);
 	return DMRGPP_OK;
 }
 
@@ -777,6 +878,26 @@ int dmrgpp_kron_apply(dmrgpp_kron_handle h, const double* x, double* y, int on_d
 	DeviceGuard g(h->device);
 	if (!g.ok)
 		return cuda_fail(h, cudaErrorInvalidDevice, "cudaSetDevice");
+	if (h->complex_sector) {
+		// interleaved complex x -> [Re; Im] -> real embedding -> interleaved y
+		const size_t n = size_t(h->plan.dim()) / 2;
+		cudaError_t  e;
+		if (!on_device
+		    && (e = cudaMemcpyAsync(h->d_cx, x, 2 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream)))
+			return cuda_fail(h, e, "copy x to device");
+		if ((e = dmrgpp::complex_split(on_device ? x : h->d_cx, h->d_x, n, h->stream)))
+			return cuda_fail(h, e, "complex split");
+		if (int rc = dmrgpp::kron_apply_device(h, h->d_x, h->d_y))
+			return rc;
+		if ((e = dmrgpp::complex_join(h->d_y, on_device ? y : h->d_cx, n, h->stream)))
+			return cuda_fail(h, e, "complex join");
+		if (on_device)
+			return DMRGPP_OK;
+		if ((e = cudaMemcpyAsync(y, h->d_cx, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream))
+		    || (e = cudaStreamSynchronize(h->stream)))
+			return cuda_fail(h, e, "copy y to host");
+		return check_error_word(h);
+	}
 	const auto&   P   = h->plan;
 	const size_t  dim = size_t(P.dim());
 	const double* X   = on_device ? x : h->d_x;

@@ -423,6 +423,8 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
                                            const double* init, int on_device, double* energies,
                                            double* z, size_t* steps_taken)
 {
+	if (h && h->complex_sector)
+		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
 	if (!h)
 		return DMRGPP_INVALID_ARG;

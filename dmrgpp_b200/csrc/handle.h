@@ -47,6 +47,11 @@ struct dmrgpp_kron_s {
 	int*                err_dev  = nullptr;
 	int                 test_stall = 0;     // dmrgpp_kron_test_stall_dependency
 	double              setup_times[DMRGPP_SETUP_NPHASES] = {}; // dmrgpp_kron_setup_profile
+	// complex sector (dmrgpp_kron_create_complex): the plan is its real
+	// embedding with 2 np patches (real parts, then imaginary parts); user
+	// vectors are interleaved complex of plan.dim() / 2 entries
+	bool                complex_sector = false;
+	double*             d_cx = nullptr;     // interleaved staging for host-pointer applies
 	// mixed-precision (TF32x3 tensor-core) form, built when requested
 	bool                mixed_ready = false;
 	float*              m_ops_hi = nullptr; // packed operators, TF32 hi / lo
@@ -118,6 +123,11 @@ int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta);
 
 // Records msg as the handle's last error and returns status.
 int handle_fail(dmrgpp_kron_handle h, int status, const std::string& msg);
+
+// Interleaved complex (re, im pairs) <-> real embedding [re parts; im parts]
+// of n complex values, enqueued on stream (complex.cu).
+cudaError_t complex_split(const double* interleaved, double* split, size_t n, cudaStream_t stream);
+cudaError_t complex_join(const double* split, double* interleaved, size_t n, cudaStream_t stream);
 
 // Releases the eigensolver buffers of a handle (lanczos.cu).
 void release_lanczos(dmrgpp_kron_handle h);

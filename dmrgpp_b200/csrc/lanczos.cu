@@ -673,6 +673,8 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
                           double*                     z,
                           size_t*                     steps_taken)
 {
+	if (h && h->complex_sector)
+		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
 	if (!h)
 		return DMRGPP_INVALID_ARG;
@@ -1100,6 +1102,8 @@ int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
                            double*                       z,
                            dmrgpp_davidson_stats*        stats)
 {
+	if (h && h->complex_sector)
+		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
 	if (!h)
 		return DMRGPP_INVALID_ARG;
@@ -1349,6 +1353,8 @@ extern "C" {
 
 int dmrgpp_kron_diagonal(dmrgpp_kron_handle h, double* diag)
 {
+	if (h && h->complex_sector)
+		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	if (!h || !diag)
 		return DMRGPP_INVALID_ARG;
 	const size_t D = size_t(h->plan.dim());
@@ -1362,6 +1368,8 @@ int dmrgpp_correction_solve(dmrgpp_kron_handle h, const double* u, double theta,
                             double* t, int max_iterations, double rel_tolerance, int* iterations,
                             double* rel_residual)
 {
+	if (h && h->complex_sector)
+		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
 	if (!h || !u || !r || !t || max_iterations < 1)
 		return DMRGPP_INVALID_ARG;
@@ -1447,6 +1455,8 @@ int dmrgpp_refine_lowest(dmrgpp_kron_handle h, double* psi, int max_outer, doubl
                          int inner_iterations, double inner_tolerance, double* energy,
                          dmrgpp_refine_stats* stats)
 {
+	if (h && h->complex_sector)
+		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
 	if (!h || !psi || !energy || max_outer < 0 || inner_iterations < 1)
 		return DMRGPP_INVALID_ARG;

@@ -27,7 +27,7 @@ class _DescTables:
     """Keeps the ctypes descriptor and everything it points to alive."""
 
     def __init__(self, noperator, npatches, left_patch_size, right_patch_size, Amatrix,
-                 ld_Amatrix, Bmatrix, ld_Bmatrix, precision, stream, device):
+                 ld_Amatrix, Bmatrix, ld_Bmatrix, precision, stream, device, complex_blocks=False):
         tot = npatches * npatches * noperator
         if len(Amatrix) != tot or len(Bmatrix) != tot:
             raise ValueError(f"tables must have npatches^2*noperator = {tot} entries")
@@ -43,8 +43,8 @@ class _DescTables:
             if isinstance(m, int):
                 return m
             a = np.asarray(m)
-            if a.dtype != np.float64:
-                raise TypeError("blocks must be float64")
+            if a.dtype != (np.complex128 if complex_blocks else np.float64):
+                raise TypeError("blocks must be complex128" if complex_blocks else "blocks must be float64")
             if a.ndim == 2 and not a.flags.f_contiguous:
                 a = np.asfortranarray(a)
             self.keep.append(a)
@@ -90,11 +90,19 @@ class BatchedGemm:
                  right_patch_size: Sequence[int], Amatrix, ld_Amatrix, Bmatrix, ld_Bmatrix,
                  precision: int = FP64, stream: Optional[int] = None, device: int = -1):
         L = _capi.lib()
+        # complex blocks (std::complex<double>): dmrgpp_kron_create_complex
+        self.is_complex = any(m is not None and not isinstance(m, int) and np.iscomplexobj(m)
+                              for m in list(Amatrix) + list(Bmatrix))
+        if self.is_complex:
+            cast = lambda tab: [None if m is None else np.asarray(m, dtype=np.complex128) for m in tab]
+            Amatrix, Bmatrix = cast(Amatrix), cast(Bmatrix)
         t = _DescTables(noperator, npatches, left_patch_size, right_patch_size, Amatrix,
-                        ld_Amatrix, Bmatrix, ld_Bmatrix, precision, stream, device)
+                        ld_Amatrix, Bmatrix, ld_Bmatrix, precision, stream, device,
+                        complex_blocks=self.is_complex)
         h = ctypes.c_void_p()
         t0 = time.perf_counter()
-        rc = L.dmrgpp_kron_create(ctypes.byref(t.desc), ctypes.byref(h))
+        create = L.dmrgpp_kron_create_complex if self.is_complex else L.dmrgpp_kron_create
+        rc = create(ctypes.byref(t.desc), ctypes.byref(h))
         self.create_seconds = time.perf_counter() - t0   # the C create alone (synchronous)
         _capi.check(rc)
         self._h = h
@@ -205,22 +213,27 @@ class BatchedGemm:
             import torch
             y = torch.empty_like(x)
         else:
-            y = np.empty(self.dim)
+            y = np.empty(self.dim, dtype=np.complex128 if getattr(self, "is_complex", False)
+                         else np.float64)
         self.apply_Htarget(x, y)
         return y
 
     def _pointers(self, vin, vout):
+        cplx = getattr(self, "is_complex", False)
         if hasattr(vin, "data_ptr"):
+            want = "torch.complex128" if cplx else "torch.float64"
             for v in (vin, vout):
-                if not (v.is_cuda and v.is_contiguous() and str(v.dtype) == "torch.float64"
+                if not (v.is_cuda and v.is_contiguous() and str(v.dtype) == want
                         and v.numel() == self.dim):
-                    raise ValueError("device vectors must be contiguous float64 CUDA tensors "
+                    raise ValueError(f"device vectors must be contiguous {want[6:]} CUDA tensors "
                                      f"of length {self.dim}")
             return 1, vin.data_ptr(), vout.data_ptr()
+        want = np.complex128 if cplx else np.float64
         for v in (vin, vout):
-            if not (isinstance(v, np.ndarray) and v.dtype == np.float64 and v.flags.c_contiguous
+            if not (isinstance(v, np.ndarray) and v.dtype == want and v.flags.c_contiguous
                     and v.size == self.dim):
-                raise ValueError(f"host vectors must be contiguous float64 of length {self.dim}")
+                raise ValueError(f"host vectors must be contiguous {np.dtype(want).name} of "
+                                 f"length {self.dim}")
         return 0, vin.ctypes.data, vout.ctypes.data
 
     def lanczos_lowest(self, init, steps: int = 200, min_steps: int = 4,

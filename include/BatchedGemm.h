@@ -13,13 +13,15 @@
 //     that keep vectors resident on the GPU.
 //   * errors throw std::runtime_error carrying the library's message instead
 //     of assert/printf (dmrg_malloc_cuda.cpp:24-29).
-//   * only T = double is implemented; the complex<double> instantiation of the
-//     reference (BatchedGemm.cpp:119) is declared but rejected at compile time.
+//   * T = double and T = std::complex<double>, the two instantiations of the
+//     reference (BatchedGemm.cpp:117-119); complex handles come from
+//     dmrgpp_kron_create_complex (the real embedding of the complex sector).
 #ifndef DMRGPP_B200_BATCHEDGEMM_H
 #define DMRGPP_B200_BATCHEDGEMM_H
 
 #include "dmrgpp_kron.h"
 
+#include <complex>
 #include <cstddef>
 #include <stdexcept>
 #include <string>
@@ -28,8 +30,9 @@
 
 template <typename T> class BatchedGemm {
 
-	static_assert(std::is_same<T, double>::value,
-	              "the B200 library implements BatchedGemm<double> only");
+	static_assert(std::is_same<T, double>::value || std::is_same<T, std::complex<double>>::value,
+	              "the B200 library implements BatchedGemm<double> and BatchedGemm<std::complex<double>>");
+	static constexpr bool kComplex = std::is_same<T, std::complex<double>>::value;
 
 public:
 
@@ -54,27 +57,33 @@ public:
 		d.npatches         = npatches;
 		d.left_patch_size  = left_patch_size.data();
 		d.right_patch_size = right_patch_size.data();
-		d.Amatrix          = const_cast<const double* const*>(Amatrix.data());
+		// std::complex<double> is two doubles (real, imaginary)
+		d.Amatrix          = reinterpret_cast<const double* const*>(Amatrix.data());
 		d.ld_Amatrix       = ld_Amatrix.data();
-		d.Bmatrix          = const_cast<const double* const*>(Bmatrix.data());
+		d.Bmatrix          = reinterpret_cast<const double* const*>(Bmatrix.data());
 		d.ld_Bmatrix       = ld_Bmatrix.data();
 		d.precision        = precision;
 		d.stream           = stream;
 		d.device           = -1;
-		check(dmrgpp_kron_create(&d, &handle_), nullptr);
+		check(kComplex ? dmrgpp_kron_create_complex(&d, &handle_) : dmrgpp_kron_create(&d, &handle_),
+		      nullptr);
 		check(dmrgpp_kron_dim(handle_, &dim_), handle_);
 	}
 
 	// vout = H vin, both host vectors in patch order (BatchedGemm.cpp:81-115).
 	void apply_Htarget(const T* vin, T* vout) const
 	{
-		check(dmrgpp_kron_apply(handle_, vin, vout, 0), handle_);
+		check(dmrgpp_kron_apply(handle_, reinterpret_cast<const double*>(vin),
+		                        reinterpret_cast<double*>(vout), 0),
+		      handle_);
 	}
 
 	// vout = H vin with device-resident vectors; enqueued on the handle's stream.
 	void apply_Htarget_device(const T* vin_dev, T* vout_dev) const
 	{
-		check(dmrgpp_kron_apply(handle_, vin_dev, vout_dev, 1), handle_);
+		check(dmrgpp_kron_apply(handle_, reinterpret_cast<const double*>(vin_dev),
+		                        reinterpret_cast<double*>(vout_dev), 1),
+		      handle_);
 	}
 
 	SizeType size() const { return dim_; }

@@ -137,6 +137,20 @@ int dmrgpp_kron_diagonal(dmrgpp_kron_handle h, double* diag);
 /* Sector dimension D = sum_p l_p r_p (xy_patch_start, setup_sparse_batch.cpp:98-103). */
 int dmrgpp_kron_dim(dmrgpp_kron_handle h, size_t* dim);
 
+/* Complex sectors (the reference's BatchedGemm<std::complex<double>>,
+ * BatchedGemm.cpp:117-119): the descriptor's blocks are std::complex<double>
+ * (interleaved real and imaginary parts, passed as const double*), column-
+ * major with leading dimensions in complex elements.  dmrgpp_kron_apply then
+ * takes interleaved complex x and y of dmrgpp_kron_dim(h) complex entries
+ * (y = H x, H = sum_k A_k (x) B_k without conjugation).  The handle runs the
+ * real embedding: patches of Re x and of Im x, and for every complex term the
+ * real terms Ar(x)Br, -Ai(x)Bi (diagonal quadrants), Ar(x)Bi, Ai(x)Br
+ * (Im from Re) and -Ar(x)Bi, -Ai(x)Br (Re from Im), so dmrgpp_kron_flops
+ * reports the real flops executed.  The device eigensolvers return
+ * DMRGPP_NOT_SUPPORTED on complex handles. */
+int dmrgpp_kron_create_complex(const dmrgpp_kron_desc* desc, dmrgpp_kron_handle* out);
+int dmrgpp_kron_is_complex(dmrgpp_kron_handle h, int* is_complex);
+
 /* Algorithmic flops of one apply: sum over contributing triples of
  * 2 r_i l_j (r_j + l_i) (dmrg/GPUPlugin/cal_kron_flops.cpp:27-33 method 1,
  * summed as estimate_work.cpp:114-151). */

@@ -136,19 +136,27 @@ def test_missing_library_fails_loudly(monkeypatch):
 
 CPP_SHIM_PROGRAM = r"""
 #include "BatchedGemm.h"
+#include <complex>
 #include <cstdio>
 #include <vector>
 int main() {
   std::vector<std::size_t> l = {2, 0}, r = {3, 1}, ld(8, 0);   // patch 1 has an empty left group
   std::vector<double*> A(8, nullptr), B(8, nullptr);
+  std::vector<std::complex<double>*> Ac(8, nullptr), Bc(8, nullptr);
+  int caught = 0;
   try {
     BatchedGemm<double> bg(2, 2, l, r, A, ld, B, ld);
-    std::printf("constructed\n");
-    return 1;
   } catch (const std::runtime_error& e) {
     std::printf("caught: %s\n", e.what());
-    return 0;
+    ++caught;
   }
+  try {   // the reference's second instantiation
+    BatchedGemm<std::complex<double>> bg(2, 2, l, r, Ac, ld, Bc, ld);
+  } catch (const std::runtime_error& e) {
+    std::printf("caught complex: %s\n", e.what());
+    ++caught;
+  }
+  return caught == 2 ? 0 : 1;
 }
 """
 
@@ -168,6 +176,7 @@ def test_cpp_dropin_header_compiles_links_and_throws(cuda_lib, tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "caught: dmrgpp-b200:" in r.stdout and "empty" in r.stdout
+    assert "caught complex: dmrgpp-b200:" in r.stdout
 
 
 def test_wft_create_rejects_bad_descriptors(cuda_lib):
