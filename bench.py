@@ -413,6 +413,23 @@ def wft_measurement(torch, prob, stream, flush):
                            "cores": os.cpu_count(), "kind": "port (numpy per-patch GEMMs)"}}
 
 
+def rank_barrier(dist, world):
+    """Every rank waits for the others (no-op on one rank)."""
+    if world > 1:
+        dist.barrier()
+
+
+def reduce_max(dist, world, v, device):
+    """The largest of the ranks' values (each rank passes its own time); every
+    rank takes part, in the same order on every rank."""
+    if world == 1:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -442,16 +459,11 @@ def run_ours(args):
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        rank_barrier(dist, world)
         torch.cuda.synchronize(dev)
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(dist, world, v, dev)
 
     # ---- device-resident timing: events around each matvec, L2 flushed
     # between steps (outside the events)
