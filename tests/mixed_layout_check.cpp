@@ -134,8 +134,16 @@ int main(int argc, char** argv)
 	// the placement of upload_place_kernel emulated here) writes exactly the
 	// packed FP64 operators: every position once, with the host packing's value
 	{
-		const long long chunk = 700 + 37 * (long long)(seed % 11), job = 150 + 13 * (long long)(seed % 7);
+		// chunks smaller than the longest column (seeds 1-3) take the
+		// longest column as their size
+		const long long chunk = (seed % 4 == 1 ? 20 : 700) + 37 * (long long)(seed % 11);
+		const long long job   = 150 + 13 * (long long)(seed % 7);
 		const UploadPlan up   = build_upload_plan(plan, chunk, job);
+		long long        longest = 1;
+		for (const Triple& tr : plan.triples)
+			longest = std::max({ longest, plan.r[tr.i], plan.l[tr.i] });
+		if (up.chunk_elems != std::max(chunk, longest))
+			return fail("upload chunk size", up.chunk_elems, std::max(chunk, longest));
 		std::vector<double> out(pack64.size(), std::numeric_limits<double>::quiet_NaN());
 		std::vector<char>   hit(pack64.size(), 0);
 		long long           written = 0, expect = 0;
