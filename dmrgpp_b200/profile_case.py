@@ -7,11 +7,14 @@ only the kernels of that workload.
     python -m dmrgpp_b200.profile_case ladder --states 4000 --precision tf32x3
     python -m dmrgpp_b200.profile_case ladder --states 4000 --solve lanczos
     python -m dmrgpp_b200.profile_case mlp --elements 300000 [--inference cuda_cores]
+    python -m dmrgpp_b200.profile_case wft --states 4000
 
 Workloads: c2 = the 1024 x 1024-state, 21-group, K=5 microbench sector;
 ladder = the ladder-shaped (N_up, N_down) sector with `--states` left and
 right states (K = 10); mlp = learned-preconditioner applications (seeded
-network, seeded diagonal and residual of `--elements` entries).  Prints one
+network, seeded diagonal and residual of `--elements` entries); wft = the
+wave-function transformation of the ladder-shaped layout with seeded square
+N(0,1)/sqrt(n) blocks.  Prints one
 line "ok ..." at the end.
 """
 from __future__ import annotations
@@ -22,7 +25,7 @@ import sys
 
 def main(argv=None) -> int:
     p = argparse.ArgumentParser()
-    p.add_argument("workload", choices=["c2", "ladder", "mlp"])
+    p.add_argument("workload", choices=["c2", "ladder", "mlp", "wft"])
     p.add_argument("--elements", type=int, default=300000, help="mlp: vector length")
     p.add_argument("--inference", default="tensor_cores", choices=["tensor_cores", "cuda_cores"])
     p.add_argument("--states", type=int, default=4000, help="ladder: left = right states")
@@ -53,6 +56,24 @@ def main(argv=None) -> int:
         torch.cuda.synchronize()
         print("ok", a.elements, float(t.abs().max()))
         m.close()
+        return 0
+
+    if a.workload == "wft":
+        import numpy as np
+        from .wft import WaveFunctionTransform
+        prob = sb.ladder_problem(total_states=a.states, sigma=2.5, seed=9)
+        rng = np.random.default_rng(17)
+        l, r = prob.lsz, prob.rsz
+        WL = [rng.standard_normal((int(n), int(n))) / np.sqrt(n) for n in l]
+        WR = [rng.standard_normal((int(n), int(n))) / np.sqrt(n) for n in r]
+        w = WaveFunctionTransform(l, r, l, r, list(range(prob.npatches)), WL, WR)
+        x = torch.from_numpy(rng.standard_normal(w.dim_in)).cuda()
+        y = torch.empty(w.dim_out, dtype=torch.float64, device="cuda")
+        for _ in range(a.applies):
+            w(x, y)
+        torch.cuda.synchronize()
+        print("ok", w.dim_in, w.flops, float(y.norm()))
+        w.close()
         return 0
 
     prob = (sb.c2_problem() if a.workload == "c2"
