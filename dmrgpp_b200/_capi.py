@@ -113,6 +113,10 @@ SIGNATURES.update({
     "dmrgpp_kron_diagonal": (ctypes.c_int, [_vp, _vp]),
     "dmrgpp_refine_lowest": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                             ctypes.c_double, _dp, ctypes.POINTER(RefineStats)]),
+    "dmrgpp_refine_lowest_group": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.c_int, ctypes.c_double, _dp,
+                                                  ctypes.POINTER(ctypes.c_int),
+                                                  ctypes.POINTER(RefineStats)]),
     "dmrgpp_mlp_num_params": (_sz, []),
     "dmrgpp_mlp_create": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_void_p)]),
     "dmrgpp_mlp_destroy": (ctypes.c_int, [_vp]),

@@ -92,6 +92,7 @@ void release(dmrgpp_kron_handle h)
 	h->m_ops_hi = h->m_ops_lo = h->m_xs_hi = h->m_xs_lo = h->m_bxs_hi = h->m_bxs_lo = nullptr;
 	h->m_xmap   = nullptr;
 	h->m_lists  = nullptr;
+	h->m_tsec1 = h->m_tsec2 = nullptr;
 	h->mixed_ready = false;
 	dmrgpp::dev_free(h->d_ops);
 	dmrgpp::dev_free(h->d_bx);
@@ -203,6 +204,8 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const S
 	a1.test_unarmed = h->test_stall;
 	a1.starts = h->m_starts1;
 	a1.error  = h->err_dev;
+	a1.tile_sector   = h->m_tsec1;
+	a1.sector_active = h->m_tsec1 ? h->sector_active : nullptr;
 	if ((e = tc_launch(a1, mp.bn, true, h->stream)))
 		return cuda_fail(h, e, "tensor-core pass 1 launch");
 	TcArgs a2 {};
@@ -217,6 +220,8 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const S
 	a2.ntiles = int(mp.tile2.size());
 	a2.grid   = h->m_grid2;
 	a2.starts = h->m_starts2;
+	a2.tile_sector   = h->m_tsec2;
+	a2.sector_active = h->m_tsec2 ? h->sector_active : nullptr;
 	a2.partial = h->m_partial;
 	a2.arrive  = h->m_arrive;
 	a2.error  = h->err_dev;
@@ -364,6 +369,23 @@ int build_mixed(dmrgpp_kron_handle h, MixedHost& host)
 	add(mp.tile2.data(), mp.tile2.size() * sizeof(GemmTile));
 	add(starts1.data(), starts1.size() * sizeof(int));
 	add(starts2.data(), starts2.size() * sizeof(int));
+	// group handles: the sector of every tile (pass 1: its input patch; pass
+	// 2: its output patch), so that stopped sectors' tiles can be skipped
+	const bool group = h->sector_start.size() > 2;
+	if (group) {
+		auto sector_of = [&](long long off) {
+			return int(std::upper_bound(h->sector_start.begin(), h->sector_start.end(), off)
+			           - h->sector_start.begin())
+			    - 1;
+		};
+		std::vector<int> t1(mp.tile1.size()), t2(mp.tile2.size());
+		for (size_t q = 0; q < t1.size(); ++q)
+			t1[q] = sector_of(h->plan.xy_start[size_t(mp.seg1[size_t(mp.tile1[q].seg_begin)].dep)]);
+		for (size_t q = 0; q < t2.size(); ++q)
+			t2[q] = sector_of(mp.tile2[q].c_off);
+		add(t1.data(), t1.size() * sizeof(int));
+		add(t2.data(), t2.size() * sizeof(int));
+	}
 	if ((e = dmrgpp::dev_malloc(&h->m_lists, lists.empty() ? 16 : lists.size())))
 		return cuda_fail(h, e, "device allocation (mixed lists)");
 	auto at    = [&](int i) { return static_cast<unsigned char*>(h->m_lists) + offs[i]; };
@@ -373,6 +395,8 @@ int build_mixed(dmrgpp_kron_handle h, MixedHost& host)
 	h->m_tile2 = reinterpret_cast<GemmTile*>(at(3));
 	h->m_starts1 = reinterpret_cast<int*>(at(4));
 	h->m_starts2 = reinterpret_cast<int*>(at(5));
+	h->m_tsec1   = group ? reinterpret_cast<int*>(at(6)) : nullptr;
+	h->m_tsec2   = group ? reinterpret_cast<int*>(at(7)) : nullptr;
 	if (!lists.empty()
 	    && (e = cudaMemcpy(h->m_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
 		return cuda_fail(h, e, "upload mixed lists");

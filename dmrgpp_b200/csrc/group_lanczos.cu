@@ -317,6 +317,115 @@ k_g_basis_combine(double* __restrict__ z, const double* __restrict__ V, size_t l
 	}
 }
 
+// ---- segmented kernels of the group refinement (dmrgpp_refine_lowest_group)
+
+// y += sgn * c[sector] * x (c null: coefficient 1), active sectors
+__global__ void __launch_bounds__(kThreads)
+k_g_axpy(double* __restrict__ y, const double* __restrict__ x, const double* __restrict__ c, double sgn,
+         const Chunk* __restrict__ chunks, int nch, const int* __restrict__ active)
+{
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk k = chunks[ch];
+		if (!active[k.seg])
+			continue;
+		const double f = sgn * (c ? c[k.seg] : 1.0);
+		for (int i = threadIdx.x; i < k.len; i += kThreads)
+			y[k.begin + i] += f * x[k.begin + i];
+	}
+}
+
+// r = hu - theta[sector] u; partial[ch] = |r|^2 over ch
+__global__ void __launch_bounds__(kThreads)
+k_g_residual(const double* __restrict__ hu, const double* __restrict__ u, const double* __restrict__ theta,
+             double* __restrict__ r, const Chunk* __restrict__ chunks, int nch,
+             const int* __restrict__ active, double* __restrict__ partial)
+{
+	__shared__ double red[kThreads / 32];
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk k = chunks[ch];
+		double      s = 0.0;
+		if (active[k.seg]) {
+			const double th = theta[k.seg];
+			for (int i = threadIdx.x; i < k.len; i += kThreads) {
+				const long long q = k.begin + i;
+				const double    w = hu[q] - th * u[q];
+				r[q]              = w;
+				s += w * w;
+			}
+		}
+		s = block_sum(s, red);
+		if (threadIdx.x == 0)
+			partial[ch] = s;
+	}
+}
+
+// CG step of every active sector: alpha = rr / pAp (0 when pAp <= 0: the
+// check below then stops the sector), t += alpha p, res -= alpha Aq;
+// partial[ch] = |res|^2 over ch
+__global__ void __launch_bounds__(kThreads)
+k_g_cg_update(double* __restrict__ t, double* __restrict__ res, const double* __restrict__ p,
+              const double* __restrict__ Aq, const double* __restrict__ rr, const double* __restrict__ pAp,
+              const Chunk* __restrict__ chunks, int nch, const int* __restrict__ active,
+              double* __restrict__ partial)
+{
+	__shared__ double red[kThreads / 32];
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk k = chunks[ch];
+		double      s = 0.0;
+		if (active[k.seg]) {
+			const double d     = pAp[k.seg];
+			const double alpha = d > 0.0 ? rr[k.seg] / d : 0.0;
+			for (int i = threadIdx.x; i < k.len; i += kThreads) {
+				const long long q = k.begin + i;
+				t[q] += alpha * p[q];
+				const double w = res[q] - alpha * Aq[q];
+				res[q]         = w;
+				s += w * w;
+			}
+		}
+		s = block_sum(s, red);
+		if (threadIdx.x == 0)
+			partial[ch] = s;
+	}
+}
+
+// one thread per sector: stop the sector's CG on a non-positive pAp or once
+// |res| <= tol * b0
+__global__ void k_g_cg_check(const double* __restrict__ pAp, const double* __restrict__ rr_next,
+                             const double* __restrict__ b0, double tol, int* __restrict__ active, int nseg)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= nseg || !active[s])
+		return;
+	if (!(pAp[s] > 0.0) || sqrt(rr_next[s]) <= tol * b0[s])
+		active[s] = 0;
+}
+
+// one thread per sector: the CG runs for outer-active sectors with b0 > 0
+__global__ void k_g_cg_start(const double* __restrict__ b0, const int* __restrict__ outer,
+                             int* __restrict__ active, int nseg)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s < nseg)
+		active[s] = outer[s] && b0[s] > 0.0 ? 1 : 0;
+}
+
+// p = res + (rr_next / rr) p, active sectors
+__global__ void __launch_bounds__(kThreads)
+k_g_cg_direction(double* __restrict__ p, const double* __restrict__ res, const double* __restrict__ rr_next,
+                 const double* __restrict__ rr, const Chunk* __restrict__ chunks, int nch,
+                 const int* __restrict__ active)
+{
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk k = chunks[ch];
+		if (!active[k.seg])
+			continue;
+		const double beta = rr[k.seg] > 0.0 ? rr_next[k.seg] / rr[k.seg] : 0.0;
+		for (int i = threadIdx.x; i < k.len; i += kThreads)
+			p[k.begin + i] = res[k.begin + i] + beta * p[k.begin + i];
+	}
+}
+
 int status(dmrgpp_kron_handle h, cudaError_t e, const char* where)
 {
 	return handle_fail(h, DMRGPP_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorString(e));
@@ -340,6 +449,11 @@ struct GroupWork {
 	int*    active  = nullptr;   // nseg
 	int*    ncols   = nullptr;   // nseg (Ritz vector lengths)
 	double* host    = nullptr;   // pinned: alpha, beta
+	// refinement (dmrgpp_refine_lowest_group), allocated on first use
+	double* rv    = nullptr; // 6 x dim: H psi, r, t, res, p, Aq
+	double* rsc   = nullptr; // 8 x nseg scalars
+	int*    rint  = nullptr; // 2 x nseg: outer active, CG active
+	double* rhost = nullptr; // pinned: theta, |r| (2 x nseg), then 2 x nseg ints
 };
 
 void release_group(dmrgpp_kron_handle h)
@@ -360,6 +474,11 @@ void release_group(dmrgpp_kron_handle h)
 	dmrgpp::dev_free(w->ncols);
 	if (w->host)
 		cudaFreeHost(w->host);
+	dmrgpp::dev_free(w->rv);
+	dmrgpp::dev_free(w->rsc);
+	dmrgpp::dev_free(w->rint);
+	if (w->rhost)
+		cudaFreeHost(w->rhost);
 	delete w;
 	h->group = nullptr;
 }
@@ -650,7 +769,10 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 	// (j_stop + 1)-dimensional tridiagonal and its eigenvector
 	const double*       ah = w->host;
 	const double*       bh = w->host + nsc;
-	std::vector<double> coef(nsc, 0.0);
+	// sector s's coefficients at s * ldp: the layout of w->r, whose row length
+	// is that of the (possibly larger) work buffers kept from an earlier solve
+	const size_t        ncoef = size_t(S) * size_t(ldp);
+	std::vector<double> coef(ncoef, 0.0);
 	std::vector<int>    ncols(static_cast<size_t>(S));
 	for (int s = 0; s < S; ++s) {
 		const size_t n = j_stop[size_t(s)] + 1;
@@ -667,7 +789,7 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 		if (steps_taken)
 			steps_taken[s] = j_stop[size_t(s)];
 	}
-	if ((e = cudaMemcpyAsync(w->r, coef.data(), nsc * sizeof(double), cudaMemcpyHostToDevice, st))
+	if ((e = cudaMemcpyAsync(w->r, coef.data(), ncoef * sizeof(double), cudaMemcpyHostToDevice, st))
 	    || (e = cudaMemcpyAsync(w->ncols, ncols.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
 		return status(h, e, "upload Ritz coefficients");
 	k_g_basis_combine<<<grid, kThreads, 0, st>>>(w->z, w->V, D, w->ncols, w->r, ldp, w->chunks, nch);
@@ -676,4 +798,205 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 	    || (e = cudaStreamSynchronize(st)))
 		return status(h, e, "Ritz vectors");
 	return DMRGPP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 refinement of every sector of a group handle: the outer iteration of
+// dmrgpp_refine_lowest (lanczos.cu) per sector, all sectors in lockstep.  Each
+// outer step normalises psi, forms the FP64 Rayleigh quotients and residuals
+// with one FP64 group H*x, and solves every unconverged sector's projected
+// correction equation (I - psi psi^T)(H - theta)(I - psi psi^T) t = -r by
+// conjugate gradients whose matvecs are the handle's (mixed) group launches;
+// the per-sector CG scalars live on the device and a sector's CG stops on the
+// device (converged, or a non-positive pAp), so the host reads one flag array
+// per burst of 8 iterations.  No counterpart in the reference.
+// ---------------------------------------------------------------------------
+extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int max_outer,
+                                          double tolerance, int inner_iterations,
+                                          double inner_tolerance, double* energies, int* converged,
+                                          dmrgpp_refine_stats* stats)
+{
+	if (h && h->complex_sector)
+		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
+	using namespace dmrgpp;
+	if (!h)
+		return DMRGPP_INVALID_ARG;
+	if (!psi || !energies)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "null argument");
+	if (max_outer < 0 || inner_iterations < 1)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "max_outer must be >= 0 and inner_iterations >= 1");
+	const int    S = int(h->sector_start.size()) - 1;
+	const size_t D = size_t(h->plan.dim());
+
+	int prev = -1;
+	cudaGetDevice(&prev);
+	if (prev != h->device)
+		cudaSetDevice(h->device);
+	struct Restore {
+		int dev, prev;
+		~Restore()
+		{
+			if (dev != prev && prev >= 0)
+				cudaSetDevice(prev);
+		}
+	} restore { h->device, prev };
+
+	if (int rc = ensure_group_work(h, 1))
+		return rc;
+	GroupWork*         w  = h->group;
+	const cudaStream_t st = h->stream;
+	cudaError_t        e;
+	if (!w->rv) {
+		if ((e = dmrgpp::dev_malloc(&w->rv, 6 * D * sizeof(double)))
+		    || (e = dmrgpp::dev_malloc(&w->rsc, 8 * size_t(S) * sizeof(double)))
+		    || (e = dmrgpp::dev_malloc(&w->rint, 2 * size_t(S) * sizeof(int)))
+		    || (e = cudaHostAlloc(&w->rhost, 2 * size_t(S) * (sizeof(double) + sizeof(int)), 0)))
+			return status(h, e, "group refinement allocation");
+	}
+	const int nch   = w->nch;
+	const int grid  = std::max(1, std::min(nch, kGrid));
+	const int sgrid = (S + kThreads - 1) / kThreads;
+	double*   hpsi  = w->rv;
+	double*   r     = w->rv + D;
+	double*   t     = w->rv + 2 * D;
+	double*   res   = w->rv + 3 * D;
+	double*   pv    = w->rv + 4 * D;
+	double*   Aq    = w->rv + 5 * D;
+	double*   theta = w->rsc;
+	double*   rnorm = w->rsc + S;
+	double*   nrm   = w->rsc + 2 * S;
+	double*   ua    = w->rsc + 3 * S;
+	double*   pAp   = w->rsc + 4 * S;
+	double*   rr[2] = { w->rsc + 5 * S, w->rsc + 6 * S };
+	double*   b0    = w->rsc + 7 * S;
+	int*      outer = w->rint;
+	int*      cg    = w->rint + S;
+	double*   th_h  = w->rhost;
+	double*   rn_h  = w->rhost + S;
+	int*      cg_h  = reinterpret_cast<int*>(w->rhost + 2 * S);
+
+	auto dot = [&](const double* x, const double* y, double* out, const int* act, int root) {
+		k_g_dot<<<grid, kThreads, 0, st>>>(x, y, w->chunks, nch, act, w->partial);
+		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, act, out, root);
+	};
+	// the FP64 group H*x skips converged sectors while this runs
+	struct MaskOff {
+		dmrgpp_kron_handle h;
+		int                user;
+		~MaskOff()
+		{
+			h->sector_active = nullptr;
+			h->precision     = user;
+		}
+	} mask_off { h, h->precision };
+
+	std::vector<int> act(size_t(S), 1), done(size_t(S), 0);
+	std::vector<double> th(size_t(S), 0.0), rn(size_t(S), 0.0);
+	if ((e = cudaMemcpyAsync(outer, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
+		return status(h, e, "group refinement start");
+	dmrgpp_refine_stats s {};
+	int                 n_active = S;
+	for (int it = 0; it <= max_outer && n_active > 0; ++it) {
+		// normalise, FP64 Rayleigh quotients and residuals of the active sectors
+		dot(psi, psi, nrm, outer, 0);
+		k_g_scale<<<grid, kThreads, 0, st>>>(psi, psi, nrm, 0, w->chunks, nch, outer);
+		h->precision     = DMRGPP_FP64;
+		h->sector_active = outer;
+		int rc           = kron_apply_device(h, psi, hpsi);
+		h->precision     = mask_off.user;
+		h->sector_active = nullptr;
+		if (rc)
+			return rc;
+		++s.fp64_matvecs;
+		dot(psi, hpsi, theta, outer, 0);
+		k_g_residual<<<grid, kThreads, 0, st>>>(hpsi, psi, theta, r, w->chunks, nch, outer, w->partial);
+		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, outer, rnorm, 1);
+		if ((e = cudaMemcpyAsync(th_h, theta, 2 * size_t(S) * sizeof(double), cudaMemcpyDeviceToHost, st))
+		    || (e = cudaStreamSynchronize(st)))
+			return status(h, e, "group refinement Rayleigh quotients");
+		if (h->err_host && *reinterpret_cast<volatile int*>(h->err_host))
+			return handle_fail(h, DMRGPP_TIMEOUT, "H*x kernel wait gave up during the group refinement");
+		bool changed = false;
+		for (int q = 0; q < S; ++q) {
+			if (!act[size_t(q)])
+				continue;
+			th[size_t(q)] = th_h[q];
+			rn[size_t(q)] = rn_h[q];
+			if (rn_h[q] <= tolerance * std::max(1.0, std::fabs(th_h[q]))) {
+				act[size_t(q)]  = 0;
+				done[size_t(q)] = 1;
+				--n_active;
+				changed = true;
+			}
+		}
+		s.outer_iterations = size_t(it);
+		if (n_active == 0 || it == max_outer)
+			break;
+		if (changed
+		    && (e = cudaMemcpyAsync(outer, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
+			return status(h, e, "group refinement update");
+		// correction solves: t = 0, res = -(I - psi psi^T) r, p = res
+		if ((e = cudaMemsetAsync(t, 0, D * sizeof(double), st))
+		    || (e = cudaMemsetAsync(res, 0, D * sizeof(double), st)))
+			return status(h, e, "group refinement clear");
+		k_g_axpy<<<grid, kThreads, 0, st>>>(res, r, nullptr, -1.0, w->chunks, nch, outer);
+		dot(psi, res, ua, outer, 0);
+		k_g_axpy<<<grid, kThreads, 0, st>>>(res, psi, ua, -1.0, w->chunks, nch, outer);
+		if ((e = cudaMemcpyAsync(pv, res, D * sizeof(double), cudaMemcpyDeviceToDevice, st)))
+			return status(h, e, "group refinement copy");
+		k_g_dot<<<grid, kThreads, 0, st>>>(res, res, w->chunks, nch, outer, w->partial);
+		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, outer, rr[0], 0);
+		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, outer, b0, 1);
+		k_g_cg_start<<<sgrid, kThreads, 0, st>>>(b0, outer, cg, S);
+		int cur = 0, inner = 0;
+		while (inner < inner_iterations) {
+			const int burst = std::min(8, inner_iterations - inner);
+			for (int q = 0; q < burst; ++q, ++inner) {
+				// Aq = P (H - theta) p
+				h->sector_active = cg;
+				rc               = kron_apply_device(h, pv, Aq);
+				h->sector_active = nullptr;
+				if (rc)
+					return rc;
+				++s.inner_matvecs;
+				k_g_axpy<<<grid, kThreads, 0, st>>>(Aq, pv, theta, -1.0, w->chunks, nch, cg);
+				dot(psi, Aq, ua, cg, 0);
+				k_g_axpy<<<grid, kThreads, 0, st>>>(Aq, psi, ua, -1.0, w->chunks, nch, cg);
+				dot(pv, Aq, pAp, cg, 0);
+				k_g_cg_update<<<grid, kThreads, 0, st>>>(t, res, pv, Aq, rr[cur], pAp, w->chunks, nch, cg,
+				                                         w->partial);
+				k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, cg, rr[cur ^ 1], 0);
+				k_g_cg_check<<<sgrid, kThreads, 0, st>>>(pAp, rr[cur ^ 1], b0, inner_tolerance, cg, S);
+				k_g_cg_direction<<<grid, kThreads, 0, st>>>(pv, res, rr[cur ^ 1], rr[cur], w->chunks, nch, cg);
+				cur ^= 1;
+			}
+			if ((e = cudaGetLastError()))
+				return status(h, e, "group refinement launch");
+			if ((e = cudaMemcpyAsync(cg_h, cg, size_t(S) * sizeof(int), cudaMemcpyDeviceToHost, st))
+			    || (e = cudaStreamSynchronize(st)))
+				return status(h, e, "group refinement correction solves");
+			bool any = false;
+			for (int q = 0; q < S && !any; ++q)
+				any = cg_h[q] != 0;
+			if (!any)
+				break;
+		}
+		// psi += t (t = 0 outside the active sectors)
+		k_g_axpy<<<grid, kThreads, 0, st>>>(psi, t, nullptr, 1.0, w->chunks, nch, outer);
+	}
+	if ((e = cudaStreamSynchronize(st)))
+		return status(h, e, "group refinement");
+	s.converged = 1;
+	for (int q = 0; q < S; ++q) {
+		energies[q] = th[size_t(q)];
+		if (converged)
+			converged[q] = done[size_t(q)];
+		s.residual_norm = std::max(s.residual_norm, rn[size_t(q)]);
+		if (!done[size_t(q)])
+			s.converged = 0;
+	}
+	if (stats)
+		*stats = s;
+	return s.converged ? DMRGPP_OK
+	                   : handle_fail(h, DMRGPP_NOT_CONVERGED, "group refinement: a sector did not converge");
 }

@@ -65,6 +65,8 @@ struct dmrgpp_kron_s {
 	int                 m_grid2  = 0;
 	int*                m_starts1 = nullptr; // per-CTA tile runs of pass 1 / 2
 	int*                m_starts2 = nullptr;
+	int*                m_tsec1 = nullptr;   // group handles: per tile of pass 1 / 2 its sector
+	int*                m_tsec2 = nullptr;
 	float*              m_partial = nullptr; // split-K partial tiles of pass 2
 	unsigned*           m_arrive  = nullptr; // per split tile: parts done
 	// CUtensorMap (128 bytes) of the operand buffers: pass 1 A hi/lo, B hi/lo,

@@ -97,6 +97,14 @@ __device__ __forceinline__ void give_up(volatile int* abort, int* error)
 	atomicExch(error, 2);
 }
 
+// Tiles of a stopped sector are skipped by all three roles alike (the flags
+// do not change during a launch), so the stage and accumulator phases stay
+// in step; a pass-2 tile and all its K-split parts share one sector.
+__device__ __forceinline__ bool skip_tile(const TcArgs& a, int ti)
+{
+	return a.sector_active && !a.sector_active[a.tile_sector[ti]];
+}
+
 // ---------------------------------------------------------------- producer
 template <int BN, int STAGES>
 __device__ void producer(const TcArgs& a, unsigned base, unsigned full0, unsigned empty0,
@@ -108,6 +116,8 @@ __device__ void producer(const TcArgs& a, unsigned base, unsigned full0, unsigne
 	// a tiled load moves its whole box (rows past the buffer arrive as 0)
 	constexpr unsigned kStageTx = 2u * unsigned(L::A_BYTES + L::B_BYTES);
 	for (int ti = a.starts[blockIdx.x]; ti < a.starts[blockIdx.x + 1] && ok; ++ti) {
+		if (skip_tile(a, ti))
+			continue;
 		const GemmTile t = a.tiles[ti];
 		for (int s = t.seg_begin; s < t.seg_end && ok; ++s) {
 			const GemmSeg sg   = a.segs[s];
@@ -160,6 +170,8 @@ __device__ void mma_issuer(const TcArgs& a, unsigned base, unsigned tmem, unsign
 	bool           ok     = true;
 	bool           issued = false;
 	for (int ti = a.starts[blockIdx.x]; ti < a.starts[blockIdx.x + 1] && ok; ++ti) {
+		if (skip_tile(a, ti))
+			continue;
 		const GemmTile t     = a.tiles[ti];
 		const int      total = tile_chunks(a, t);
 		if (total == 0)
@@ -321,6 +333,8 @@ __device__ void epilogue(const TcArgs& a, unsigned tmem, unsigned accf0, unsigne
 	unsigned  tc      = 0;
 	bool      ok      = true;
 	for (int ti = a.starts[blockIdx.x]; ti < a.starts[blockIdx.x + 1]; ++ti) {
+		if (skip_tile(a, ti))
+			continue;
 		const GemmTile t     = a.tiles[ti];
 		const int      total = tile_chunks(a, t);
 		const int      grow  = t.m0 + row;

@@ -25,6 +25,8 @@ struct TcArgs {
 	float*          partial; // pass 2: 128 x BN FP32 partial tiles of split parts (slots)
 	unsigned*       arrive;  // pass 2: per split output tile, parts done (self-resetting)
 	int             test_unarmed; // test hook: CTA 0's producer leaves its first stage unarmed
+	const int*      tile_sector;   // group handles: per tile its sector (else NULL)
+	const int*      sector_active; // NULL, or per sector: 0 = skip its tiles (C left as is)
 };
 
 // Kernel attributes on the current device; call once per device.

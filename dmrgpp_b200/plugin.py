@@ -317,6 +317,26 @@ class BatchedGemm:
             _capi.check(rc, self._h)
         return e.value, {f: getattr(st, f) for f, _ in _capi.RefineStats._fields_}
 
+    def refine_lowest_group(self, psi, max_outer: int = 6, tolerance: float = 1e-9,
+                            inner_iterations: int = 200, inner_tolerance: float = 1e-4,
+                            raise_on_no_convergence: bool = True):
+        """FP64 refinement of every sector of a group handle at once
+        (dmrgpp_refine_lowest_group); psi is the concatenated sector vectors
+        (torch CUDA tensor, updated in place).  Returns (energies array,
+        converged array, stats dict)."""
+        nsec = len(self.sector_offsets()) - 1
+        e = np.zeros(nsec)
+        conv = np.zeros(nsec, dtype=np.int32)
+        st = _capi.RefineStats()
+        self._pointers(psi, psi)
+        rc = self._lib.dmrgpp_refine_lowest_group(
+            self._h, psi.data_ptr(), max_outer, tolerance, inner_iterations, inner_tolerance,
+            e.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            conv.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(st))
+        if rc != _capi.NOT_CONVERGED or raise_on_no_convergence:
+            _capi.check(rc, self._h)
+        return e, conv.astype(bool), {f: getattr(st, f) for f, _ in _capi.RefineStats._fields_}
+
     def diagonal(self):
         """Diagonal of H (torch CUDA tensor, patch order)."""
         import torch

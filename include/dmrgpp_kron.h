@@ -359,6 +359,26 @@ int dmrgpp_refine_lowest(dmrgpp_kron_handle h, double* psi, int max_outer, doubl
                          int inner_iterations, double inner_tolerance, double* energy,
                          dmrgpp_refine_stats* stats);
 
+/* The same refinement for every sector of a group handle
+ * (dmrgpp_kron_create_group) at once: each sector runs the iteration of
+ * dmrgpp_refine_lowest with its own Rayleigh quotient, residual and
+ * conjugate-gradient scalars, and one launch per step applies H to all
+ * sectors (FP64 for the Rayleigh quotients, the handle's precision in the
+ * correction solves).  A sector leaves the outer iteration once
+ * |r| <= tolerance * max(1, |theta|), and the conjugate gradients once its
+ * residual is below inner_tolerance times its initial one or its projected
+ * operator is not positive definite.  psi: the concatenated sector vectors
+ * (device, updated in place); energies[s]: sector s's final FP64 Rayleigh
+ * quotient; converged (may be NULL): per sector 1 when it met the tolerance.
+ * stats (may be NULL): outer_iterations = most outer steps of any sector,
+ * inner_matvecs and fp64_matvecs = group launches, residual_norm = largest
+ * final sector residual, converged = every sector converged.  Returns
+ * DMRGPP_NOT_CONVERGED when a sector did not converge (energies are still
+ * written).  No counterpart in the reference.  Synchronous. */
+int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int max_outer, double tolerance,
+                               int inner_iterations, double inner_tolerance, double* energies,
+                               int* converged, dmrgpp_refine_stats* stats);
+
 /* ---- Learned preconditioner: per-element MLP 4 -> 256 -> 256 -> 1 ----
  * Trained on the GPU by these kernels (FP32 master weights, Adam); inference
  * uses BF16 weights with FP32 accumulation.  All arrays are device pointers

@@ -131,3 +131,83 @@ def test_group_handle_as_one_sector_with_graph_replay(cuda_lib, cuda_device):
     exact = min(np.linalg.eigvalsh(p.dense())[0] for p in probs)
     assert abs(e0 - exact) <= 1e-10 * abs(exact)
     bg.close()
+
+
+@pytest.mark.parametrize("precision", ["tf32x3", "fp64"])
+def test_group_refinement_matches_single_fp64_solves(cuda_lib, cuda_device, precision):
+    """Serving-style problems in one group handle: a loose lockstep group
+    Lanczos (the handle's matvecs: tensor-core TF32x3 or FP64), then the
+    lockstep FP64 refinement (dmrgpp_refine_lowest_group).  Every sector
+    converges; its energy is within 1e-9 per site (and 1e-10 relative) of its
+    single-problem FP64 Lanczos, its vector has unit norm and overlaps the
+    FP64 Ritz vector to 1e-8."""
+    import torch
+    from dmrgpp_b200 import plugin
+    probs, meta = sb.serving_batch(8, seed=77)
+    prec = plugin.TF32X3 if precision == "tf32x3" else plugin.FP64
+    bg = plugin.BatchedGemm.from_problems(probs, precision=prec)
+    offs = bg.sector_offsets()
+    init = torch.from_numpy(np.random.default_rng(5).standard_normal(bg.dim)).cuda()
+    _, z, _ = bg.lanczos_lowest_group(init, steps=100, tolerance=1e-4)
+    e, conv, st = bg.refine_lowest_group(z, max_outer=8, tolerance=1e-10, inner_iterations=80,
+                                         inner_tolerance=1e-2)
+    assert conv.all() and st["converged"] == 1 and st["fp64_matvecs"] >= 1
+    for s, p in enumerate(probs):
+        single = plugin.BatchedGemm.from_problem(p)
+        e1, z1, _ = single.lanczos_lowest(init[offs[s]:offs[s + 1]].contiguous(), tolerance=1e-12)
+        single.close()
+        assert abs(e[s] - e1) / meta[s]["L"] <= 1e-9, (meta[s], e[s], e1)
+        assert abs(e[s] - e1) <= 1e-10 * abs(e1), (meta[s], e[s], e1)
+        zs = z[offs[s]:offs[s + 1]]
+        assert abs(float(torch.linalg.norm(zs)) - 1.0) < 1e-12
+        assert 1.0 - abs(float(torch.dot(zs, z1))) < 1e-8, s
+    bg.close()
+
+
+def test_group_refinement_edge_sectors(cuda_lib, cuda_device):
+    """Uneven sectors (one of dimension 1, tiny ones, C2) refined from random
+    vectors in a TF32x3 group: the 1-state sector converges at once, the
+    others reach the dense-diagonalisation energies; with max_outer = 0 only
+    the Rayleigh quotients are formed and unconverged sectors are reported."""
+    import torch
+    from dmrgpp_b200 import plugin
+    probs = mixed_sectors()
+    bg = plugin.BatchedGemm.from_problems(probs, precision=plugin.TF32X3)
+    offs = bg.sector_offsets()
+    x = torch.from_numpy(np.random.default_rng(21).standard_normal(bg.dim)).cuda()
+    e0, conv0, st0 = bg.refine_lowest_group(x.clone(), max_outer=0, raise_on_no_convergence=False)
+    assert st0["inner_matvecs"] == 0 and st0["fp64_matvecs"] == 1
+    assert conv0[2] and not conv0.all()
+    for s, p in enumerate(probs):
+        xs = x[offs[s]:offs[s + 1]].cpu().numpy()
+        rq = float(xs @ (p.dense() @ xs) / (xs @ xs)) if p.dim <= 2000 else None
+        if rq is not None:
+            assert abs(e0[s] - rq) <= 1e-12 * max(1.0, abs(rq)), s
+    _, z, _ = bg.lanczos_lowest_group(x, steps=150, tolerance=1e-5)
+    e, conv, st = bg.refine_lowest_group(z, max_outer=12, tolerance=1e-10, inner_iterations=150,
+                                         inner_tolerance=1e-3)
+    assert conv.all()
+    for s, p in enumerate(probs):
+        if p.dim <= 2000:
+            exact = np.linalg.eigvalsh(p.dense())[0]
+            assert abs(e[s] - exact) <= 1e-10 * max(1.0, abs(exact)), (s, e[s], exact)
+    bg.close()
+
+
+def test_group_lanczos_reuses_larger_work_buffers(cuda_lib, cuda_device):
+    """A group solve with fewer steps after one with more reuses the larger
+    work buffers: same energies and Ritz vectors (bitwise) as on a fresh
+    handle."""
+    import torch
+    from dmrgpp_b200 import plugin
+    probs, _ = sb.serving_batch(6, seed=13)
+    bg = plugin.BatchedGemm.from_problems(probs)
+    init = torch.from_numpy(np.random.default_rng(2).standard_normal(bg.dim)).cuda()
+    bg.lanczos_lowest_group(init, steps=200)
+    e1, z1, n1 = bg.lanczos_lowest_group(init, steps=40)
+    bg.close()
+    fresh = plugin.BatchedGemm.from_problems(probs)
+    e2, z2, n2 = fresh.lanczos_lowest_group(init, steps=40)
+    fresh.close()
+    assert np.array_equal(e1, e2) and np.array_equal(n1, n2)
+    assert torch.equal(z1, z2)
