@@ -250,6 +250,55 @@ def mixed_matvec_measurement(torch, dev, stream, prob, xh, y64, f_alg):
 SERVING_MIXED_TOLERANCE = 1e-5
 
 
+def learned_ablation(torch, bgm, init, stream):
+    """The serving batch through the lockstep group Davidson (TF32x3 group
+    matvecs, residual 1e-5, subspace 32) with no, the Jacobi and the learned
+    correction (weights/serving_mlp.npz, trained by train_serving_mlp), each
+    followed by the group FP64 refinement; plus the cost of one learned
+    correction of the whole batch."""
+    from dmrgpp_b200.mlp import MLPPreconditioner
+    from dmrgpp_b200.train_serving_mlp import SERVING_WEIGHTS
+    mlp = MLPPreconditioner.load(SERVING_WEIGHTS)
+    bgm.davidson_lowest_group(init, max_iterations=2, raise_on_no_convergence=False)  # buffers
+    runs = {}
+    for name, pre in (("none", 0), ("jacobi", 1), ("learned", 2)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, zd, _, sd = bgm.davidson_lowest_group(init, preconditioner=pre,
+                                                 mlp=mlp if pre == 2 else None, tolerance=1e-5,
+                                                 max_iterations=600, max_subspace=32,
+                                                 raise_on_no_convergence=False)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        ed, cr, _ = bgm.refine_lowest_group(zd, max_outer=10, tolerance=1e-10, inner_iterations=80,
+                                            inner_tolerance=1e-2, raise_on_no_convergence=False)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        runs[name] = {"seconds": t2 - t0, "davidson_seconds": t1 - t0,
+                      "iterations": int(sd["iterations"]),
+                      "ms_per_iteration": (t1 - t0) * 1e3 / max(1, sd["iterations"]),
+                      "converged": int(cr.sum()), "energies": ed}
+    diag = bgm.diagonal()
+    r = torch.from_numpy(np.random.default_rng(4).standard_normal(bgm.dim)).to(diag.device)
+    offs = torch.tensor(bgm.sector_offsets(), device=diag.device)
+    nsec = offs.numel() - 1
+    theta = torch.full((nsec,), -10.0, dtype=torch.float64, device=diag.device)
+    rn = torch.ones(nsec, dtype=torch.float64, device=diag.device)
+    with torch.cuda.stream(stream):
+        mlp.precondition_group(diag, r, offs, theta, rn, stream=stream.cuda_stream)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(3):
+            mlp.precondition_group(diag, r, offs, theta, rn, stream=stream.cuda_stream)
+        b.record(stream)
+    b.synchronize()
+    mlp.close()
+    return {"runs": runs, "learned_correction_ms": a.elapsed_time(b) / 3,
+            "note": "group Davidson (dmrgpp_davidson_lowest_group) + dmrgpp_refine_lowest_group; "
+                    "learned_correction_ms = one tensor-core MLP inference over every element "
+                    "of the batch"}
+
+
 def serving_measurements(torch, dev, stream, cpu_sample: bool = True):
     """Serving-style batch: 256 independent ground-state problems (Heisenberg
     and Hubbard chain-shaped sectors, L in [16, 48], m in {64, 128, 256, 512},
@@ -328,6 +377,7 @@ def serving_measurements(torch, dev, stream, cpu_sample: bool = True):
         runs.append(mixed_solve())
     em, conv, st, zm, steps_m, split = min(runs, key=lambda r: sum(r[5]))
     tm = sum(split)
+    dav = learned_ablation(torch, bgm, init, stream)
     bgm.close()
     es, t_seq, ovl = [], 0.0, []
     for s, p in enumerate(probs):
@@ -353,6 +403,9 @@ def serving_measurements(torch, dev, stream, cpu_sample: bool = True):
         "note": f"TF32x3 group Lanczos to a Ritz-value change of {SERVING_MIXED_TOLERANCE:g}, then "
                 "dmrgpp_refine_lowest_group (FP64 Rayleigh quotients and residuals, |r| <= "
                 "1e-10 max(1, |E|)), handle creation excluded"}
+    for v in dav["runs"].values():
+        v["max_abs_dE_per_site_vs_single_fp64"] = float((np.abs(v.pop("energies") - es) / sites).max())
+    out["group_davidson"] = dav
     out["single_problem_lanczos"] = {"seconds": t_seq, "problems_per_s": len(probs) / t_seq,
                                      "note": "one FP64 device Lanczos per problem, handle "
                                              "creation excluded"}

@@ -130,6 +130,12 @@ SIGNATURES.update({
     "dmrgpp_mlp_set_inference": (ctypes.c_int, [_vp, ctypes.c_int]),
     "dmrgpp_mlp_precondition": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp,
                                                _sz, _vp]),
+    "dmrgpp_mlp_precondition_group": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int,
+                                                     _vp, _sz, _vp]),
+    "dmrgpp_davidson_lowest_group": (ctypes.c_int, [_vp, ctypes.POINTER(DavidsonParams), _vp,
+                                                    ctypes.c_int, _dp, _vp,
+                                                    ctypes.POINTER(ctypes.c_int),
+                                                    ctypes.POINTER(DavidsonStats)]),
     "dmrgpp_mlp_last_error": (ctypes.c_char_p, [_vp]),
 })
 

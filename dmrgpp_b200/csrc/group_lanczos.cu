@@ -22,6 +22,7 @@
 #include "dmrgpp_kron.h"
 #include "devmem.h"
 #include "handle.h"
+#include "mlp.h"
 #include "tridiag.h"
 
 #include <cuda_runtime.h>
@@ -293,15 +294,18 @@ k_g_basis_subtract(double* __restrict__ v, const double* __restrict__ V, size_t 
 	}
 }
 
-// z = V[:, 0..ncols[s]) coef[s] for every sector
+// z = V[:, 0..ncols[s]) coef[s] for every sector (active ones when active
+// is not NULL)
 __global__ void __launch_bounds__(kThreads)
 k_g_basis_combine(double* __restrict__ z, const double* __restrict__ V, size_t ld,
                   const int* __restrict__ ncols, const double* __restrict__ coef, int ldp,
-                  const Chunk* __restrict__ chunks, int nch)
+                  const Chunk* __restrict__ chunks, int nch, const int* __restrict__ active)
 {
 	__shared__ double cs[1024];
 	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
 		const Chunk c  = chunks[ch];
+		if (active && !active[c.seg])
+			continue;
 		const int   nc = ncols[c.seg];
 		__syncthreads();
 		for (int col = threadIdx.x; col < nc; col += kThreads)
@@ -426,6 +430,29 @@ k_g_cg_direction(double* __restrict__ p, const double* __restrict__ res, const d
 	}
 }
 
+// Jacobi correction of every active sector: t = r / (theta[s] - d), the
+// denominator kept at least floor_rel * max(1, |theta[s]|) in magnitude
+__global__ void __launch_bounds__(kThreads)
+k_g_jacobi(const double* __restrict__ r, const double* __restrict__ d, const double* __restrict__ theta,
+           double floor_rel, double* __restrict__ t, const Chunk* __restrict__ chunks, int nch,
+           const int* __restrict__ active)
+{
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk k = chunks[ch];
+		if (!active[k.seg])
+			continue;
+		const double th = theta[k.seg];
+		const double fl = floor_rel * fmax(1.0, fabs(th));
+		for (int i = threadIdx.x; i < k.len; i += kThreads) {
+			const long long q   = k.begin + i;
+			double          den = th - d[q];
+			if (fabs(den) < fl)
+				den = den < 0 ? -fl : fl;
+			t[q] = r[q] / den;
+		}
+	}
+}
+
 int status(dmrgpp_kron_handle h, cudaError_t e, const char* where)
 {
 	return handle_fail(h, DMRGPP_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorString(e));
@@ -454,6 +481,14 @@ struct GroupWork {
 	double* rsc   = nullptr; // 8 x nseg scalars
 	int*    rint  = nullptr; // 2 x nseg: outer active, CG active
 	double* rhost = nullptr; // pinned: theta, |r| (2 x nseg), then 2 x nseg ints
+	long long* sec_start = nullptr; // nseg + 1 sector offsets
+	// Davidson (dmrgpp_davidson_lowest_group), allocated on first use
+	int     dmax   = 0;       // basis columns of dV / dW
+	double* dV     = nullptr; // dim x dmax, per-sector orthonormal bases
+	double* dW     = nullptr; // dim x dmax, H V
+	double* dvec   = nullptr; // 4 x dim: Ritz vectors, H u, residuals, corrections
+	double* dsc    = nullptr; // 3 x nseg: theta, |r|, norms
+	double* dcoef  = nullptr; // nseg x cols: Ritz coefficients
 };
 
 void release_group(dmrgpp_kron_handle h)
@@ -479,6 +514,12 @@ void release_group(dmrgpp_kron_handle h)
 	dmrgpp::dev_free(w->rint);
 	if (w->rhost)
 		cudaFreeHost(w->rhost);
+	dmrgpp::dev_free(w->sec_start);
+	dmrgpp::dev_free(w->dV);
+	dmrgpp::dev_free(w->dW);
+	dmrgpp::dev_free(w->dvec);
+	dmrgpp::dev_free(w->dsc);
+	dmrgpp::dev_free(w->dcoef);
 	delete w;
 	h->group = nullptr;
 }
@@ -524,10 +565,13 @@ int ensure_group_work(dmrgpp_kron_handle h, int cols)
 	    || (e = dmrgpp::dev_malloc(&w->seg_chunk, sc.size() * sizeof(int)))
 	    || (e = dmrgpp::dev_malloc(&w->active, size_t(nseg) * sizeof(int)))
 	    || (e = dmrgpp::dev_malloc(&w->ncols, size_t(nseg) * sizeof(int)))
+	    || (e = dmrgpp::dev_malloc(&w->sec_start, (size_t(nseg) + 1) * sizeof(long long)))
 	    || (e = cudaHostAlloc(&w->host, 2 * (2 * nsc + size_t(nseg)) * sizeof(double), 0)))
 		return status(h, e, "group solver allocation");
 	if ((e = cudaMemcpy(w->chunks, ch.data(), ch.size() * sizeof(Chunk), cudaMemcpyHostToDevice))
 	    || (e = cudaMemcpy(w->seg_chunk, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice))
+	    || (e = cudaMemcpy(w->sec_start, h->sector_start.data(), (size_t(nseg) + 1) * sizeof(long long),
+	                       cudaMemcpyHostToDevice))
 	    || (e = cudaMemset(w->beta, 0, (nsc + size_t(nseg)) * sizeof(double)))
 	    || (e = cudaMemset(w->alpha, 0, nsc * sizeof(double))))
 		return status(h, e, "group solver set-up");
@@ -792,7 +836,8 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 	if ((e = cudaMemcpyAsync(w->r, coef.data(), ncoef * sizeof(double), cudaMemcpyHostToDevice, st))
 	    || (e = cudaMemcpyAsync(w->ncols, ncols.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
 		return status(h, e, "upload Ritz coefficients");
-	k_g_basis_combine<<<grid, kThreads, 0, st>>>(w->z, w->V, D, w->ncols, w->r, ldp, w->chunks, nch);
+	k_g_basis_combine<<<grid, kThreads, 0, st>>>(w->z, w->V, D, w->ncols, w->r, ldp, w->chunks, nch,
+	                                             nullptr);
 	if ((e = cudaMemcpyAsync(z, w->z, D * sizeof(double),
 	                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st))
 	    || (e = cudaStreamSynchronize(st)))
@@ -999,4 +1044,244 @@ extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int
 		*stats = s;
 	return s.converged ? DMRGPP_OK
 	                   : handle_fail(h, DMRGPP_NOT_CONVERGED, "group refinement: a sector did not converge");
+}
+
+// ---------------------------------------------------------------------------
+// Davidson for every sector of a group handle, all sectors in lockstep: the
+// iteration of dmrgpp_davidson_lowest (lanczos.cu) per sector with the
+// handle's matvecs.  Every iteration orthonormalises each active sector's
+// correction against its basis (two classical Gram-Schmidt passes), applies H
+// to the new columns of all sectors in one group launch, adds a column to
+// each sector's projected matrix (read to the host), takes the lowest Ritz
+// pair of every sector on the host, forms the Ritz vectors, residuals and
+// their norms on the device, stops the sectors whose residual met the
+// tolerance, and forms the next corrections (none, Jacobi, or the learned
+// one with each sector's own Ritz value and residual norm).  Since every
+// active sector adds one column per iteration, all restart together.  No
+// counterpart in the reference.
+// ---------------------------------------------------------------------------
+extern "C" int dmrgpp_davidson_lowest_group(dmrgpp_kron_handle h, const dmrgpp_davidson_params* p,
+                                            const double* init, int on_device, double* energies,
+                                            double* z, int* converged, dmrgpp_davidson_stats* stats)
+{
+	if (h && h->complex_sector)
+		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
+	using namespace dmrgpp;
+	if (!h)
+		return DMRGPP_INVALID_ARG;
+	if (!p || !init || !energies || !z)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "null argument");
+	if (p->max_subspace < 2 || p->max_subspace > 128 || p->max_iterations < 1)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "max_subspace must be in [2, 128] for a group");
+	if (p->preconditioner == DMRGPP_PRECOND_MLP && !p->mlp)
+		return handle_fail(h, DMRGPP_INVALID_ARG, "learned preconditioner selected without a network");
+	const int    S    = int(h->sector_start.size()) - 1;
+	const size_t D    = size_t(h->plan.dim());
+	const int    mmax = int(p->max_subspace);
+
+	int prev = -1;
+	cudaGetDevice(&prev);
+	if (prev != h->device)
+		cudaSetDevice(h->device);
+	struct Restore {
+		int dev, prev;
+		~Restore()
+		{
+			if (dev != prev && prev >= 0)
+				cudaSetDevice(prev);
+		}
+	} restore { h->device, prev };
+
+	if (int rc = ensure_group_work(h, mmax))
+		return rc;
+	GroupWork*         w  = h->group;
+	const cudaStream_t st = h->stream;
+	cudaError_t        e;
+	const int          ldp = w->cols;
+	if (w->dmax < mmax) {
+		dmrgpp::dev_free(w->dV);
+		dmrgpp::dev_free(w->dW);
+		w->dV = w->dW = nullptr;
+		w->dmax       = 0;
+		if ((e = dmrgpp::dev_malloc(&w->dV, D * size_t(mmax) * sizeof(double)))
+		    || (e = dmrgpp::dev_malloc(&w->dW, D * size_t(mmax) * sizeof(double))))
+			return status(h, e, "group Davidson basis allocation");
+		w->dmax = mmax;
+	}
+	if (!w->dvec
+	    && ((e = dmrgpp::dev_malloc(&w->dvec, 4 * D * sizeof(double)))
+	        || (e = dmrgpp::dev_malloc(&w->dsc, 3 * size_t(S) * sizeof(double)))
+	        || (e = dmrgpp::dev_malloc(&w->dcoef, size_t(S) * size_t(ldp) * sizeof(double)))))
+		return status(h, e, "group Davidson allocation");
+	const int nch  = w->nch;
+	const int grid = std::max(1, std::min(nch, kGrid));
+	auto      Vc   = [&](int c) { return w->dV + size_t(c) * D; };
+	auto      Wc   = [&](int c) { return w->dW + size_t(c) * D; };
+	double*   u    = w->dvec;
+	double*   hu   = w->dvec + D;
+	double*   r    = w->dvec + 2 * D;
+	double*   t    = w->dvec + 3 * D;
+	double*   th_d = w->dsc;
+	double*   rn_d = w->dsc + S;
+	double*   nrm  = w->dsc + 2 * S;
+	double*   hbuf = w->host; // pinned, at least 2 * nseg * cols doubles
+
+	// the group H*x skips converged sectors while this runs
+	h->sector_active = w->active;
+	struct MaskOff {
+		dmrgpp_kron_handle h;
+		~MaskOff() { h->sector_active = nullptr; }
+	} mask_off { h };
+
+	std::vector<int> act(size_t(S), 1), done(size_t(S), 0);
+	std::vector<long long> dim_s(static_cast<size_t>(S));
+	for (int q = 0; q < S; ++q)
+		dim_s[size_t(q)] = h->sector_start[size_t(q) + 1] - h->sector_start[size_t(q)];
+	if ((e = cudaMemcpyAsync(w->active, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st))
+	    || (e = cudaMemcpyAsync(t, init, D * sizeof(double),
+	                            on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st)))
+		return status(h, e, "group Davidson start");
+
+	const size_t        mm = size_t(mmax);
+	std::vector<double> G(size_t(S) * mm * mm, 0.0);
+	std::vector<double> th(size_t(S), 0.0), rn(size_t(S), 0.0), coef(size_t(S) * size_t(ldp), 0.0);
+	std::vector<int>    ncols(size_t(S), 0);
+	dmrgpp_davidson_stats s {};
+	const bool          mixed    = h->precision != DMRGPP_FP64;
+	int                 n_active = S;
+	int                 k        = 0;
+	auto dot = [&](const double* x, const double* y, double* out) {
+		k_g_dot<<<grid, kThreads, 0, st>>>(x, y, w->chunks, nch, w->active, w->partial);
+		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, w->active, out, 0);
+	};
+	for (size_t it = 0; it < p->max_iterations && n_active > 0; ++it) {
+		// orthonormalise the corrections against the bases and append them
+		for (int pass = 0; pass < (k > 0 ? 2 : 0); ++pass) {
+			k_g_basis_dots<<<grid, kThreads, 0, st>>>(w->dV, D, k, t, w->chunks, nch, w->active,
+			                                          w->partial, ldp);
+			k_g_basis_reduce<<<S, kThreads, 0, st>>>(w->partial, ldp, k, w->seg_chunk, w->active, w->r);
+			k_g_basis_subtract<<<grid, kThreads, 0, st>>>(t, w->dV, D, k, w->r, ldp, w->chunks, nch,
+			                                              w->active, w->partial);
+		}
+		if (k == 0)
+			dot(t, t, nrm);
+		else
+			k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, w->active, nrm, 0);
+		k_g_scale<<<grid, kThreads, 0, st>>>(t, Vc(k), nrm, 0, w->chunks, nch, w->active);
+		if (int rc = kron_apply_device(h, Vc(k), Wc(k)))
+			return rc;
+		if (mixed)
+			++s.mixed_matvecs;
+		else
+			++s.fp64_matvecs;
+		// new column of every sector's projected matrix
+		k_g_basis_dots<<<grid, kThreads, 0, st>>>(w->dV, D, k + 1, Wc(k), w->chunks, nch, w->active,
+		                                          w->partial, ldp);
+		k_g_basis_reduce<<<S, kThreads, 0, st>>>(w->partial, ldp, k + 1, w->seg_chunk, w->active, w->r);
+		if ((e = cudaMemcpyAsync(hbuf, w->r, size_t(S) * size_t(ldp) * sizeof(double),
+		                         cudaMemcpyDeviceToHost, st))
+		    || (e = cudaStreamSynchronize(st)))
+			return status(h, e, "group Davidson projection");
+		if (h->err_host && *reinterpret_cast<volatile int*>(h->err_host))
+			return handle_fail(h, DMRGPP_TIMEOUT, "H*x kernel wait gave up during the group Davidson");
+		// Rayleigh-Ritz per active sector
+		for (int q = 0; q < S; ++q) {
+			if (!act[size_t(q)])
+				continue;
+			double*       Gq  = G.data() + size_t(q) * mm * mm;
+			const double* col = hbuf + size_t(q) * size_t(ldp);
+			for (int i = 0; i <= k; ++i) {
+				Gq[size_t(i) + size_t(k) * mm] = col[i];
+				Gq[size_t(k) + size_t(i) * mm] = col[i];
+			}
+		}
+		++k;
+		// lowest pair of every active sector's k x k projected matrix, on the
+		// host's cores (each sector writes only its own entries)
+		parallel_for(size_t(S), [&](size_t q) {
+			if (!act[q])
+				return;
+			const double*       Gq = G.data() + q * mm * mm;
+			std::vector<double> Gk(size_t(k) * size_t(k));
+			for (int j = 0; j < k; ++j)
+				for (int i = 0; i < k; ++i)
+					Gk[size_t(i) + size_t(j) * size_t(k)] = Gq[size_t(i) + size_t(j) * mm];
+			sym_lowest(k, Gk.data(), &th[q], coef.data() + q * size_t(ldp));
+			ncols[q] = k;
+		});
+		if ((e = cudaMemcpyAsync(w->dcoef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, st))
+		    || (e = cudaMemcpyAsync(th_d, th.data(), size_t(S) * sizeof(double), cudaMemcpyHostToDevice, st))
+		    || (e = cudaMemcpyAsync(w->ncols, ncols.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
+			return status(h, e, "group Davidson Ritz coefficients");
+		k_g_basis_combine<<<grid, kThreads, 0, st>>>(u, w->dV, D, w->ncols, w->dcoef, ldp, w->chunks, nch,
+		                                             w->active);
+		k_g_basis_combine<<<grid, kThreads, 0, st>>>(hu, w->dW, D, w->ncols, w->dcoef, ldp, w->chunks, nch,
+		                                             w->active);
+		k_g_residual<<<grid, kThreads, 0, st>>>(hu, u, th_d, r, w->chunks, nch, w->active, w->partial);
+		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, w->active, rn_d, 1);
+		if ((e = cudaMemcpyAsync(hbuf, rn_d, size_t(S) * sizeof(double), cudaMemcpyDeviceToHost, st))
+		    || (e = cudaStreamSynchronize(st)))
+			return status(h, e, "group Davidson residuals");
+		++s.iterations;
+		bool changed = false;
+		for (int q = 0; q < S; ++q) {
+			if (!act[size_t(q)])
+				continue;
+			rn[size_t(q)] = hbuf[q];
+			// converged, or the basis spans the whole sector (the pair is exact)
+			if (hbuf[q] <= p->tolerance * std::max(1.0, std::fabs(th[size_t(q)])) || k >= dim_s[size_t(q)]) {
+				act[size_t(q)]  = 0;
+				done[size_t(q)] = 1;
+				--n_active;
+				changed = true;
+			}
+		}
+		if (n_active == 0)
+			break;
+		if (changed
+		    && (e = cudaMemcpyAsync(w->active, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
+			return status(h, e, "group Davidson update");
+		if (k == mmax) {
+			// restart every active sector from its Ritz pair: V = [u], W = [H u]
+			dot(u, u, nrm);
+			k_g_scale<<<grid, kThreads, 0, st>>>(u, Vc(0), nrm, 0, w->chunks, nch, w->active);
+			k_g_scale<<<grid, kThreads, 0, st>>>(hu, Wc(0), nrm, 0, w->chunks, nch, w->active);
+			for (int q = 0; q < S; ++q)
+				if (act[size_t(q)])
+					G[size_t(q) * mm * mm] = th[size_t(q)];
+			k = 1;
+			++s.restarts;
+		}
+		// corrections
+		if (p->preconditioner == DMRGPP_PRECOND_JACOBI) {
+			k_g_jacobi<<<grid, kThreads, 0, st>>>(r, h->d_diag, th_d, p->denominator_floor, t, w->chunks, nch,
+			                                      w->active);
+		} else if (p->preconditioner == DMRGPP_PRECOND_MLP) {
+			if (int rc = mlp_precondition_group(static_cast<dmrgpp_mlp_handle>(p->mlp), h->d_diag, r,
+			                                    w->sec_start, th_d, rn_d, S, t, D, st))
+				return handle_fail(h, rc, "learned preconditioner failed");
+		} else if ((e = cudaMemcpyAsync(t, r, D * sizeof(double), cudaMemcpyDeviceToDevice, st))) {
+			return status(h, e, "group Davidson correction");
+		}
+		if ((e = cudaGetLastError()))
+			return status(h, e, "group Davidson launch");
+	}
+	// the Ritz vectors are normalised by construction (orthonormal bases, unit coefficients)
+	if ((e = cudaMemcpyAsync(z, u, D * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+	                         st))
+	    || (e = cudaStreamSynchronize(st)))
+		return status(h, e, "group Davidson Ritz vectors");
+	s.converged = 1;
+	for (int q = 0; q < S; ++q) {
+		energies[q] = th[size_t(q)];
+		if (converged)
+			converged[q] = done[size_t(q)];
+		s.residual_norm = std::max(s.residual_norm, rn[size_t(q)]);
+		if (!done[size_t(q)])
+			s.converged = 0;
+	}
+	if (stats)
+		*stats = s;
+	return s.converged ? DMRGPP_OK
+	                   : handle_fail(h, DMRGPP_NOT_CONVERGED, "group Davidson: a sector did not converge");
 }

@@ -128,6 +128,56 @@ __global__ void k_features(const double* __restrict__ d, const double* __restric
 		features(d[e], r[e], theta, s, rms, x + e * F);
 }
 
+// Per-sector Ritz values and residual norms of a group of sectors (device
+// arrays; start has nsec + 1 entries).  start == NULL: one sector, the
+// scalars passed beside it.
+struct SectorScalars {
+	const long long* start;
+	const double*    theta;
+	const double*    rnorm;
+	int              nsec;
+};
+
+struct RowScalars {
+	double theta, s, rms, scale;
+};
+
+// The scalars of element e: the single-sector ones, or those of the sector
+// holding e (binary search over the sector starts), formed as the host
+// forms them for one sector: s = max(1, |theta|), rms = |r| / sqrt(n_s).
+__device__ __forceinline__ RowScalars row_scalars(const SectorScalars& g, const RowScalars& one, long long e)
+{
+	if (!g.start)
+		return one;
+	int lo = 0, hi = g.nsec;
+	while (hi - lo > 1) {
+		const int mid = (lo + hi) >> 1;
+		if (g.start[mid] <= e)
+			lo = mid;
+		else
+			hi = mid;
+	}
+	RowScalars      v;
+	const long long n = g.start[lo + 1] - g.start[lo];
+	v.theta           = g.theta[lo];
+	v.s               = fmax(1.0, fabs(v.theta));
+	v.rms             = g.rnorm[lo] / sqrt(double(n > 0 ? n : 1));
+	v.scale           = v.rms / v.s;
+	return v;
+}
+
+// features of rows e0 .. e0 + n of a group
+__global__ void k_features_group(const double* __restrict__ d, const double* __restrict__ r,
+                                 SectorScalars g, long long e0, size_t n, float* __restrict__ x)
+{
+	const RowScalars none {};
+	for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n;
+	     e += size_t(gridDim.x) * blockDim.x) {
+		const RowScalars v = row_scalars(g, none, e0 + (long long)e);
+		features(d[e], r[e], v.theta, v.s, v.rms, x + e * F);
+	}
+}
+
 // C (M x N, row-major, ldc) = op(A) * op(B) (+ C if accumulate); op(A) is
 // M x K, op(B) is K x N.  TA: A stored K x M (row-major) instead of M x K.
 // TB: B stored N x K instead of K x N.  64 x 64 tiles, k-steps of 16, each
@@ -318,6 +368,15 @@ __global__ void k_scale_out(const float* __restrict__ o, double scale, double* _
 		t[e] = double(o[e]) * scale;
 }
 
+__global__ void k_scale_out_group(const float* __restrict__ o, SectorScalars g, long long e0,
+                                  double* __restrict__ t, size_t n)
+{
+	const RowScalars none {};
+	for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n;
+	     e += size_t(gridDim.x) * blockDim.x)
+		t[e] = double(o[e]) * row_scalars(g, none, e0 + (long long)e).scale;
+}
+
 // ------------------------------------------------ tensor-core inference
 constexpr int kTcRows    = 128;                 // elements per tile = TMEM lanes
 constexpr int kTcSlots   = 4;                   // ring of h1 chunks (64 units each)
@@ -332,7 +391,8 @@ struct MlpTcArgs {
 	double*              t;
 	long long            n;
 	int                  ntiles;
-	double               theta, s, rms, scale; // scale = rms / s
+	RowScalars           one; // one sector: theta, s, rms, scale = rms / s
+	SectorScalars        g;   // a group of sectors (g.start != NULL): per-row scalars
 	const float*         p;  // parameters: BF16 values widened to FP32
 	const __nv_bfloat16* w2; // BF16 W2 (row j = hidden unit j of layer 2)
 	int*                 error;
@@ -451,8 +511,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) mlp_infer_tc_kernel(const __gri
 		for (int tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x) {
 			const long long e    = (long long)tile * kTcRows + row;
 			float           x[F] = { 0.f, 0.f, 0.f, 0.f };
-			if (e < a.n)
-				features(a.diag[e], a.r[e], a.theta, a.s, a.rms, x);
+			if (e < a.n) {
+				const RowScalars v = row_scalars(a.g, a.one, e);
+				features(a.diag[e], a.r[e], v.theta, v.s, v.rms, x);
+			}
 			for (int c = 0; c < H / 64; ++c) {
 				const unsigned slot = g % kTcSlots;
 				if (g >= kTcSlots)
@@ -510,7 +572,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) mlp_infer_tc_kernel(const __gri
 				mbar_arrive(acce0 + 8 * b);
 			const long long e = (long long)tile * kTcRows + row;
 			if (e < a.n)
-				a.t[e] = double(o + sb3) * a.scale;
+				a.t[e] = double(o + sb3) * row_scalars(a.g, a.one, e).scale;
 			++tcount;
 		}
 		if (!ok && lane == 0)
@@ -608,13 +670,20 @@ void forward(dmrgpp_mlp_handle m, const float* P, const float* x, int rows, cuda
 
 } // namespace
 
-int mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, double theta,
-                     double rnorm, double* t, size_t n, cudaStream_t st)
+namespace {
+
+// t = learned correction of r; one sector (g.start == NULL: theta, rnorm) or
+// a group of sectors (per-sector scalars in g)
+int precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, double theta, double rnorm,
+                 const SectorScalars& g, double* t, size_t n, cudaStream_t st)
 {
 	if (!m)
 		return DMRGPP_INVALID_ARG;
-	const double s   = std::max(1.0, std::fabs(theta));
-	const double rms = rnorm / std::sqrt(double(n > 0 ? n : 1));
+	RowScalars one;
+	one.theta = theta;
+	one.s     = std::max(1.0, std::fabs(theta));
+	one.rms   = rnorm / std::sqrt(double(n > 0 ? n : 1));
+	one.scale = one.rms / one.s;
 	if (m->bf_dirty) {
 		k_to_bf16<<<grid_for(kNumParams), 256, 0, st>>>(m->params, m->wbf, kNumParams);
 		m->bf_dirty = false;
@@ -647,10 +716,8 @@ int mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, d
 		a.t      = t;
 		a.n      = (long long)n;
 		a.ntiles = int((n + kTcRows - 1) / kTcRows);
-		a.theta  = theta;
-		a.s      = s;
-		a.rms    = rms;
-		a.scale  = rms / s;
+		a.one    = one;
+		a.g      = g;
 		a.p      = pinf;
 		a.w2     = m->wbf + kW2;
 		a.error  = m->err_dev;
@@ -663,13 +730,39 @@ int mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, d
 		return rc;
 	for (size_t e0 = 0; e0 < n; e0 += chunk) {
 		const int rows = int(std::min<size_t>(chunk, n - e0));
-		k_features<<<grid_for(size_t(rows)), 256, 0, st>>>(diag + e0, r + e0, theta, s, rms,
-		                                                  size_t(rows), m->x);
+		if (g.start)
+			k_features_group<<<grid_for(size_t(rows)), 256, 0, st>>>(diag + e0, r + e0, g, (long long)e0,
+			                                                        size_t(rows), m->x);
+		else
+			k_features<<<grid_for(size_t(rows)), 256, 0, st>>>(diag + e0, r + e0, one.theta, one.s,
+			                                                  one.rms, size_t(rows), m->x);
 		forward(m, pinf, m->x, rows, st);
-		k_scale_out<<<grid_for(size_t(rows)), 256, 0, st>>>(m->out, rms / s, t + e0, size_t(rows));
+		if (g.start)
+			k_scale_out_group<<<grid_for(size_t(rows)), 256, 0, st>>>(m->out, g, (long long)e0, t + e0,
+			                                                         size_t(rows));
+		else
+			k_scale_out<<<grid_for(size_t(rows)), 256, 0, st>>>(m->out, one.scale, t + e0, size_t(rows));
 	}
 	cudaError_t e = cudaGetLastError();
 	return e == cudaSuccess ? DMRGPP_OK : mlp_cuda(m, e, "MLP inference");
+}
+
+} // namespace
+
+int mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, double theta,
+                     double rnorm, double* t, size_t n, cudaStream_t st)
+{
+	return precondition(m, diag, r, theta, rnorm, SectorScalars {}, t, n, st);
+}
+
+int mlp_precondition_group(dmrgpp_mlp_handle m, const double* diag, const double* r,
+                           const long long* sector_start, const double* theta, const double* rnorm,
+                           int nsec, double* t, size_t n, cudaStream_t st)
+{
+	if (nsec < 1 || !sector_start || !theta || !rnorm)
+		return mlp_fail(m, DMRGPP_INVALID_ARG, "group preconditioner: null sector arrays");
+	const SectorScalars g { sector_start, theta, rnorm, nsec };
+	return precondition(m, diag, r, 0.0, 0.0, g, t, n, st);
 }
 
 } // namespace dmrgpp
@@ -865,6 +958,14 @@ int dmrgpp_mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const doubl
                             double rnorm, double* t, size_t n, void* stream)
 {
 	return dmrgpp::mlp_precondition(m, diag, r, theta, rnorm, t, n, static_cast<cudaStream_t>(stream));
+}
+
+int dmrgpp_mlp_precondition_group(dmrgpp_mlp_handle m, const double* diag, const double* r,
+                                  const long long* sector_start, const double* theta,
+                                  const double* rnorm, int nsectors, double* t, size_t n, void* stream)
+{
+	return dmrgpp::mlp_precondition_group(m, diag, r, sector_start, theta, rnorm, nsectors, t, n,
+	                                      static_cast<cudaStream_t>(stream));
 }
 
 } // extern "C"

@@ -17,4 +17,11 @@ constexpr int kMlpWidth    = 256;
 int mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, double theta,
                      double rnorm, double* t, size_t n, cudaStream_t stream);
 
+// The same for the concatenated vectors of nsec sectors (device arrays:
+// sector_start has nsec + 1 offsets, theta and rnorm one value per sector);
+// every element sees its own sector's scalars.
+int mlp_precondition_group(dmrgpp_mlp_handle m, const double* diag, const double* r,
+                           const long long* sector_start, const double* theta, const double* rnorm,
+                           int nsec, double* t, size_t n, cudaStream_t stream);
+
 } // namespace dmrgpp

@@ -289,3 +289,80 @@ void tridiag_inverse_iteration(int n, const double* d, const double* off, double
 }
 
 } // namespace dmrgpp
+
+namespace dmrgpp {
+
+bool sym_lowest(int n, const double* a, double* w, double* v)
+{
+	if (n <= 0)
+		return false;
+	if (n == 1) {
+		*w   = a[0];
+		v[0] = 1.0;
+		return true;
+	}
+	// Householder reduction T = Q^T A Q, Q = P_0 P_1 ... P_{n-3}; P_k acts on
+	// rows / columns k+1..n-1 with P_k = I - beta_k h_k h_k^T, h_k(0) = 1
+	// (Golub and Van Loan, algorithms 5.1.1 and 8.3.1)
+	const size_t        N = size_t(n);
+	std::vector<double> m(a, a + N * N), d(N), off(N - 1), hv(N * N, 0.0), beta(N, 0.0), p(N), q(N);
+	auto                M = [&](int i, int j) -> double& { return m[size_t(i) + size_t(j) * N]; };
+	for (int k = 0; k + 2 < n; ++k) {
+		const int len   = n - k - 1;
+		double*   h     = hv.data() + size_t(k) * N; // h[0..len)
+		double    sigma = 0.0;
+		for (int i = 1; i < len; ++i)
+			sigma += M(k + 1 + i, k) * M(k + 1 + i, k);
+		const double x0 = M(k + 1, k);
+		d[size_t(k)]    = M(k, k);
+		if (sigma == 0.0) { // already tridiagonal in this column
+			off[size_t(k)] = x0;
+			continue;
+		}
+		const double mu = std::sqrt(x0 * x0 + sigma);
+		const double h0 = x0 <= 0.0 ? x0 - mu : -sigma / (x0 + mu);
+		beta[size_t(k)] = 2.0 * h0 * h0 / (sigma + h0 * h0);
+		h[0]            = 1.0;
+		for (int i = 1; i < len; ++i)
+			h[i] = M(k + 1 + i, k) / h0;
+		off[size_t(k)] = mu;
+		// trailing block A22 <- P A22 P = A22 - h w^T - w h^T with
+		// p = beta A22 h, w = p - (beta / 2)(p^T h) h
+		const double b = beta[size_t(k)];
+		for (int i = 0; i < len; ++i) {
+			double s = 0.0;
+			for (int j = 0; j < len; ++j)
+				s += M(k + 1 + i, k + 1 + j) * h[j];
+			p[size_t(i)] = b * s;
+		}
+		double ph = 0.0;
+		for (int i = 0; i < len; ++i)
+			ph += p[size_t(i)] * h[i];
+		for (int i = 0; i < len; ++i)
+			q[size_t(i)] = p[size_t(i)] - 0.5 * b * ph * h[i];
+		for (int j = 0; j < len; ++j)
+			for (int i = 0; i < len; ++i)
+				M(k + 1 + i, k + 1 + j) -= h[i] * q[size_t(j)] + q[size_t(i)] * h[j];
+	}
+	d[N - 2]   = M(n - 2, n - 2);
+	d[N - 1]   = M(n - 1, n - 1);
+	off[N - 2] = M(n - 1, n - 2);
+	// lowest eigenpair of T, then v = Q z
+	*w = tridiag_kth_lowest(n, d.data(), off.data(), 1);
+	tridiag_inverse_iteration(n, d.data(), off.data(), *w, v);
+	for (int k = n - 3; k >= 0; --k) {
+		if (beta[size_t(k)] == 0.0)
+			continue;
+		const double* h   = hv.data() + size_t(k) * N;
+		const int     len = n - k - 1;
+		double        s   = 0.0;
+		for (int i = 0; i < len; ++i)
+			s += h[i] * v[k + 1 + i];
+		s *= beta[size_t(k)];
+		for (int i = 0; i < len; ++i)
+			v[k + 1 + i] -= s * h[i];
+	}
+	return true;
+}
+
+} // namespace dmrgpp

@@ -17,6 +17,13 @@ namespace dmrgpp {
 // dense symmetric matrix a (n x n column-major) by cyclic Jacobi rotations.
 bool sym_eigen(int n, const double* a, double* w, double* v);
 
+// Lowest eigenvalue w and its unit eigenvector v (n entries) of the dense
+// symmetric matrix a (n x n column-major): Householder reduction to
+// tridiagonal form, bisection for the eigenvalue, inverse iteration for the
+// tridiagonal eigenvector, transformed back.  About (4/3) n^3 flops, against
+// some 20 n^3 for the full Jacobi solve above.
+bool sym_lowest(int n, const double* a, double* w, double* v);
+
 } // namespace dmrgpp
 
 namespace dmrgpp {

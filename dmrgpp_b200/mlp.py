@@ -115,6 +115,18 @@ class MLPPreconditioner:
                                                       theta, rnorm, t.data_ptr(), r.numel(), s))
         return t
 
+    def precondition_group(self, diag, r, sector_start, theta, rnorm, stream=None):
+        """Learned correction of the concatenated residuals of several sectors
+        (dmrgpp_mlp_precondition_group): sector_start (int64, nsectors + 1),
+        theta and rnorm (float64, one per sector) are torch CUDA tensors."""
+        import torch
+        t = torch.empty_like(r)
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        self._check(self._lib.dmrgpp_mlp_precondition_group(
+            self._h, diag.data_ptr(), r.data_ptr(), sector_start.data_ptr(), theta.data_ptr(),
+            rnorm.data_ptr(), int(theta.numel()), t.data_ptr(), r.numel(), s))
+        return t
+
     def save(self, path: str) -> None:
         np.savez_compressed(path, params=self.get_params())
 

@@ -301,6 +301,47 @@ class BatchedGemm:
         stats = {f: getattr(st, f) for f, _ in _capi.DavidsonStats._fields_}
         return e.value, z, stats
 
+    def davidson_lowest_group(self, init, preconditioner: int = 1, mlp=None,
+                              tolerance: float = 1e-8, max_iterations: int = 500,
+                              max_subspace: int = 32, denominator_floor: float = 1e-3,
+                              raise_on_no_convergence: bool = True):
+        """Lowest eigenpair of every sector of a group handle by the lockstep
+        group Davidson (dmrgpp_davidson_lowest_group), in the handle's
+        precision.  Returns (energies array, concatenated Ritz vectors,
+        converged array, stats dict); numpy or torch CUDA like
+        davidson_lowest."""
+        L = self._lib
+        p = _capi.DavidsonParams()
+        L.dmrgpp_davidson_params_init(ctypes.byref(p))
+        p.max_iterations, p.max_subspace, p.tolerance = max_iterations, max_subspace, tolerance
+        p.preconditioner = preconditioner
+        p.mlp = mlp.handle if mlp is not None else None
+        p.denominator_floor = denominator_floor
+        nsec = len(self.sector_offsets()) - 1
+        e = np.zeros(nsec)
+        conv = np.zeros(nsec, dtype=np.int32)
+        st = _capi.DavidsonStats()
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        if hasattr(init, "data_ptr"):
+            import torch
+            z = torch.empty_like(init)
+            self._pointers(init, z)
+            rc = L.dmrgpp_davidson_lowest_group(self._h, ctypes.byref(p), init.data_ptr(), 1,
+                                                e.ctypes.data_as(dp), z.data_ptr(),
+                                                conv.ctypes.data_as(ip), ctypes.byref(st))
+        else:
+            init = np.ascontiguousarray(init, dtype=np.float64)
+            z = np.empty(self.dim)
+            self._pointers(init, z)
+            rc = L.dmrgpp_davidson_lowest_group(self._h, ctypes.byref(p), init.ctypes.data, 0,
+                                                e.ctypes.data_as(dp), z.ctypes.data,
+                                                conv.ctypes.data_as(ip), ctypes.byref(st))
+        if rc != _capi.NOT_CONVERGED or raise_on_no_convergence:
+            _capi.check(rc, self._h)
+        stats = {f: getattr(st, f) for f, _ in _capi.DavidsonStats._fields_}
+        return e, z, conv.astype(bool), stats
+
     def refine_lowest(self, psi, max_outer: int = 6, tolerance: float = 1e-9,
                       inner_iterations: int = 200, inner_tolerance: float = 1e-4,
                       raise_on_no_convergence: bool = True):

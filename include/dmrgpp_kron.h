@@ -379,6 +379,28 @@ int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int max_outer,
                                int inner_iterations, double inner_tolerance, double* energies,
                                int* converged, dmrgpp_refine_stats* stats);
 
+/* Lowest eigenpair of every sector of a group handle (dmrgpp_kron_create_group)
+ * by Davidson, all sectors in lockstep: per sector the iteration of
+ * dmrgpp_davidson_lowest, with one group launch per iteration applying H to
+ * every sector's new basis vector in the handle's precision (no FP64 phase:
+ * on a mixed handle follow with dmrgpp_refine_lowest_group), each sector's
+ * own projected matrix and lowest Ritz pair, and its own correction (none,
+ * Jacobi, or the learned one with the sector's Ritz value and residual norm,
+ * dmrgpp_mlp_precondition_group).  A sector stops once its residual
+ * |r| <= tolerance * max(1, |theta|) (or its basis spans the sector) and then
+ * drops out of the vector work and of the group H*x; all sectors restart
+ * together when the basis reaches max_subspace (at most 128 here).
+ * energies[s], z (the concatenated Ritz vectors: device when on_device),
+ * converged (may be NULL: per sector 1 when its residual met the tolerance
+ * or its basis spans the sector);
+ * stats (may be NULL): iterations (lockstep), mixed_matvecs / fp64_matvecs
+ * (group launches), restarts, residual_norm (largest sector residual),
+ * converged (every sector).  Returns DMRGPP_NOT_CONVERGED with the last
+ * pairs after max_iterations.  No counterpart in the reference. */
+int dmrgpp_davidson_lowest_group(dmrgpp_kron_handle h, const dmrgpp_davidson_params* p,
+                                 const double* init, int on_device, double* energies, double* z,
+                                 int* converged, dmrgpp_davidson_stats* stats);
+
 /* ---- Learned preconditioner: per-element MLP 4 -> 256 -> 256 -> 1 ----
  * Trained on the GPU by these kernels (FP32 master weights, Adam); inference
  * uses BF16 weights with FP32 accumulation.  All arrays are device pointers
@@ -411,6 +433,15 @@ enum { DMRGPP_MLP_TENSOR_CORES = 0, DMRGPP_MLP_CUDA_CORES = 1 };
 int         dmrgpp_mlp_set_inference(dmrgpp_mlp_handle m, int mode);
 int         dmrgpp_mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r,
                                     double theta, double rnorm, double* t, size_t n, void* stream);
+/* The learned correction of the concatenated residuals of nsectors sectors
+ * (a group handle's layout): element e of sector s is corrected with that
+ * sector's Ritz value theta[s] and residual norm rnorm[s], bitwise as
+ * dmrgpp_mlp_precondition on the sector alone.  sector_start (nsectors + 1
+ * offsets), theta and rnorm are device arrays. */
+int         dmrgpp_mlp_precondition_group(dmrgpp_mlp_handle m, const double* diag, const double* r,
+                                          const long long* sector_start, const double* theta,
+                                          const double* rnorm, int nsectors, double* t, size_t n,
+                                          void* stream);
 const char* dmrgpp_mlp_last_error(dmrgpp_mlp_handle m);
 
 /* Host helper: eigenvalues (ascending) and, when vectors != NULL, eigenvectors

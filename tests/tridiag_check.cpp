@@ -1,7 +1,8 @@
 // Host check of the tridiagonal helpers of the group Lanczos (tridiag.cpp):
 // the k-th lowest eigenvalue by Sturm bisection against the QL solver, and
 // the inverse-iteration eigenvector's residual, on seeded random and
-// Lanczos-like (graded, nearly degenerate) tridiagonals.
+// Lanczos-like (graded, nearly degenerate) tridiagonals; and the lowest pair
+// of dense symmetric matrices by sym_lowest against the Jacobi solver.
 // Prints "ok <worst eigenvalue error> <worst residual>" or "FAIL ...".
 #include "tridiag.h"
 
@@ -52,6 +53,40 @@ int main()
 			std::printf("FAIL norm %d %g\n", trial, nz);
 			return 1;
 		}
+		worst_r = std::max(worst_r, res / scale);
+	}
+	// lowest pair of dense symmetric matrices (sym_lowest) against the Jacobi
+	// solver (sym_eigen): eigenvalue and residual of the eigenvector; random
+	// matrices and Davidson-like ones (graded diagonal, small couplings)
+	for (int trial = 0; trial < 300; ++trial) {
+		const int           n = 1 + trial % 48;
+		const size_t        N = size_t(n);
+		std::vector<double> A(N * N), ev(N), V(N * N), z(N);
+		for (int j = 0; j < n; ++j)
+			for (int i = 0; i <= j; ++i) {
+				double x = u(rng);
+				if (trial % 2)
+					x = i == j ? -10.0 + 0.5 * i + 1e-3 * x : 1e-2 * x;
+				A[size_t(i) + size_t(j) * N] = A[size_t(j) + size_t(i) * N] = x;
+			}
+		dmrgpp::sym_eigen(n, A.data(), ev.data(), V.data());
+		double th = 0.0;
+		dmrgpp::sym_lowest(n, A.data(), &th, z.data());
+		double scale = 1.0, res = 0.0, nz = 0.0;
+		for (double x : ev)
+			scale = std::max(scale, std::fabs(x));
+		for (int i = 0; i < n; ++i) {
+			double t = -th * z[size_t(i)];
+			for (int j = 0; j < n; ++j)
+				t += A[size_t(i) + size_t(j) * N] * z[size_t(j)];
+			res = std::max(res, std::fabs(t));
+			nz += z[size_t(i)] * z[size_t(i)];
+		}
+		if (std::fabs(th - ev[0]) > 1e-13 * scale || res > 1e-12 * scale || std::fabs(nz - 1.0) > 1e-12) {
+			std::printf("FAIL dense %d %g %g %g\n", trial, th - ev[0], res, nz);
+			return 1;
+		}
+		worst_e = std::max(worst_e, std::fabs(th - ev[0]) / scale);
 		worst_r = std::max(worst_r, res / scale);
 	}
 	if (worst_e > 1e-13 || worst_r > 1e-12) {
