@@ -38,6 +38,14 @@ class WftDesc(ctypes.Structure):
                 ("stream", ctypes.c_void_p), ("device", ctypes.c_int)]
 
 
+class DensityDesc(ctypes.Structure):
+    _fields_ = [("npatches", _sz), ("left_patch_size", _szp), ("right_patch_size", _szp),
+                ("patch_group", _szp), ("ngroups", _sz), ("group_size", _szp),
+                ("side", ctypes.c_int), ("ntargets", _sz), ("psi", ctypes.c_void_p),
+                ("weights", ctypes.POINTER(ctypes.c_double)), ("stream", ctypes.c_void_p),
+                ("device", ctypes.c_int)]
+
+
 class PlanInfo(ctypes.Structure):
     _fields_ = [("ntriples", _sz), ("dim", _sz), ("f_alg", ctypes.c_double),
                 ("operator_bytes", _sz), ("bx_bytes", _sz), ("pass1_tiles", _sz),
@@ -137,6 +145,8 @@ SIGNATURES.update({
                                                     ctypes.POINTER(ctypes.c_int),
                                                     ctypes.POINTER(DavidsonStats)]),
     "dmrgpp_mlp_last_error": (ctypes.c_char_p, [_vp]),
+    "dmrgpp_density_truncate": (ctypes.c_int, [ctypes.POINTER(DensityDesc), _sz, ctypes.c_double,
+                                               _sz, _dp, _dp, _szp, _szp, _dp]),
 })
 
 SIGNATURES.update({

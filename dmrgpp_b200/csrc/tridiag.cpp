@@ -12,23 +12,41 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdint>
 #include <numeric>
+#include <random>
 #include <vector>
 
 namespace dmrgpp {
 
-bool tridiag_eigen(int n, double* d, const double* off, double* z)
+namespace {
+
+// The implicit QL iteration on (d, off); every plane rotation is passed to
+// rot(i, c, s) in the order applied (it maps columns i, i+1 of the
+// eigenvector matrix: z_{i+1} <- s z_i + c z_{i+1}, z_i <- c z_i - s z_{i+1}).
+// d ends as the eigenvalues, unsorted.  Kept as a template so that the
+// eigenvalue-only solve skips the vector update entirely.
+// sqrt(a^2 + b^2), through std::hypot only where the squares could over- or
+// underflow
+inline double safe_hypot(double a, double b)
 {
-	if (n <= 0)
-		return true;
+	const double s = a * a + b * b;
+	return (s > 1e-280 && s < 1e280) ? std::sqrt(s) : std::hypot(a, b);
+}
+
+template <class Rot> bool ql_iterate(int n, double* d, const double* off, Rot rot)
+{
 	std::vector<double> e(size_t(n), 0.0);
 	for (int i = 0; i + 1 < n; ++i)
 		e[size_t(i)] = off[i];
-	if (z) {
-		std::fill(z, z + size_t(n) * size_t(n), 0.0);
-		for (int i = 0; i < n; ++i)
-			z[size_t(i) + size_t(i) * size_t(n)] = 1.0;
-	}
+	// an off-diagonal element is negligible against its two diagonal
+	// neighbours or against the norm of the whole matrix (the norm-based test
+	// of the EISPACK tql2 routine): eigenvalues far below the norm, as in a
+	// density matrix of low rank, carry rounding noise of the order of
+	// eps * norm and a purely local test would never accept them
+	double anorm = 0.0;
+	for (int i = 0; i < n; ++i)
+		anorm = std::max(anorm, std::fabs(d[i]) + std::fabs(e[size_t(i)]));
 	for (int l = 0; l < n; ++l) {
 		int iter = 0;
 		for (;;) {
@@ -36,7 +54,8 @@ bool tridiag_eigen(int n, double* d, const double* off, double* z)
 			int m = l;
 			for (; m + 1 < n; ++m) {
 				const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
-				if (std::fabs(e[size_t(m)]) <= DBL_EPSILON * dd)
+				const double em = std::fabs(e[size_t(m)]);
+				if (em <= DBL_EPSILON * dd || em <= DBL_EPSILON * anorm)
 					break;
 			}
 			if (m == l)
@@ -45,14 +64,14 @@ bool tridiag_eigen(int n, double* d, const double* off, double* z)
 				return false;
 			// shift: eigenvalue of the leading 2x2 block closer to d[l]
 			double g = (d[l + 1] - d[l]) / (2.0 * e[size_t(l)]);
-			double r = std::hypot(g, 1.0);
+			double r = safe_hypot(g, 1.0);
 			g        = d[m] - d[l] + e[size_t(l)] / (g + std::copysign(r, g));
 			double s = 1.0, c = 1.0, p = 0.0;
 			bool   split = false;
 			for (int i = m - 1; i >= l; --i) {
 				const double f = s * e[size_t(i)];
 				const double b = c * e[size_t(i)];
-				r              = std::hypot(f, g);
+				r              = safe_hypot(f, g);
 				e[size_t(i) + 1] = r;
 				if (r == 0.0) { // underflow: the block splits, restart on it
 					d[i + 1] -= p;
@@ -67,15 +86,7 @@ bool tridiag_eigen(int n, double* d, const double* off, double* z)
 				p        = s * r;
 				d[i + 1] = g + p;
 				g        = c * r - b;
-				if (z) {
-					double* zi  = z + size_t(i) * size_t(n);
-					double* zi1 = zi + size_t(n);
-					for (int k = 0; k < n; ++k) {
-						const double t = zi1[k];
-						zi1[k]         = s * zi[k] + c * t;
-						zi[k]          = c * zi[k] - s * t;
-					}
-				}
+				rot(i, c, s);
 			}
 			if (split)
 				continue;
@@ -84,6 +95,33 @@ bool tridiag_eigen(int n, double* d, const double* off, double* z)
 			e[size_t(m)] = 0.0;
 		}
 	}
+	return true;
+}
+
+} // namespace
+
+bool tridiag_eigen(int n, double* d, const double* off, double* z)
+{
+	if (n <= 0)
+		return true;
+	if (z) {
+		std::fill(z, z + size_t(n) * size_t(n), 0.0);
+		for (int i = 0; i < n; ++i)
+			z[size_t(i) + size_t(i) * size_t(n)] = 1.0;
+	}
+	const bool ok = ql_iterate(n, d, off, [&](int i, double c, double s) {
+		if (!z)
+			return;
+		double* zi  = z + size_t(i) * size_t(n);
+		double* zi1 = zi + size_t(n);
+		for (int k = 0; k < n; ++k) {
+			const double t = zi1[k];
+			zi1[k]         = s * zi[k] + c * t;
+			zi[k]          = c * zi[k] - s * t;
+		}
+	});
+	if (!ok)
+		return false;
 	// ascending order, vectors follow their values
 	std::vector<int> order(static_cast<size_t>(n));
 	std::iota(order.begin(), order.end(), 0);
@@ -292,6 +330,122 @@ void tridiag_inverse_iteration(int n, const double* d, const double* off, double
 
 namespace dmrgpp {
 
+// Householder reduction T = Q^T A Q of the dense symmetric n x n matrix a
+// (column-major), Q = P_0 P_1 ... P_{n-3}, P_k = I - beta_k h_k h_k^T acting
+// on rows / columns k+1..n-1 with h_k(0) = 1 (Golub and Van Loan, algorithms
+// 5.1.1 and 8.3.1): diagonal d, off-diagonal off (n - 1), reflectors hv
+// (column k holds h_k) and beta.  n >= 2.
+void householder_tridiag(int n, const double* a, std::vector<double>& d, std::vector<double>& off,
+                         std::vector<double>& hv, std::vector<double>& beta)
+{
+	// Only the lower triangle of the (symmetric) trailing block is kept, and
+	// the rank-2 update of step k - 1 is applied in the same pass over it
+	// that forms step k's product p = beta A22 h: one read and one write of
+	// the lower triangle per step.
+	const size_t        N = size_t(n);
+	std::vector<double> m(a, a + N * N), p(N), q(N), qprev(N), hprev(N);
+	d.assign(N, 0.0);
+	off.assign(N - 1, 0.0);
+	hv.assign(N * N, 0.0);
+	beta.assign(N, 0.0);
+	auto M       = [&](int i, int j) -> double& { return m[size_t(i) + size_t(j) * N]; };
+	bool pending = false; // update A <- A - h' q'^T - q' h'^T on rows / columns >= k
+	for (int k = 0; k + 2 < n; ++k) {
+		const int len = n - k - 1;
+		// bring column k (rows >= k) up to date; h', q' index 0 is row k
+		if (pending) {
+			const double hk = hprev[0], qk = qprev[0];
+			for (int i = 0; i <= len; ++i)
+				M(k + i, k) -= hprev[size_t(i)] * qk + qprev[size_t(i)] * hk;
+		}
+		double* h     = hv.data() + size_t(k) * N; // h[0..len)
+		double  sigma = 0.0;
+		for (int i = 1; i < len; ++i)
+			sigma += M(k + 1 + i, k) * M(k + 1 + i, k);
+		const double x0 = M(k + 1, k);
+		d[size_t(k)]    = M(k, k);
+		double b        = 0.0;
+		if (sigma == 0.0) { // already tridiagonal in this column
+			off[size_t(k)] = x0;
+		} else {
+			const double mu = std::sqrt(x0 * x0 + sigma);
+			const double h0 = x0 <= 0.0 ? x0 - mu : -sigma / (x0 + mu);
+			b               = 2.0 * h0 * h0 / (sigma + h0 * h0);
+			beta[size_t(k)] = b;
+			h[0]            = 1.0;
+			for (int i = 1; i < len; ++i)
+				h[i] = M(k + 1 + i, k) / h0;
+			off[size_t(k)] = mu;
+		}
+		// one pass over the lower triangle of A22 (rows / columns >= k+1):
+		// the pending update, then p += A22 h with the updated entries
+		for (int i = 0; i < len; ++i)
+			p[size_t(i)] = 0.0;
+		const double* hp = hprev.data() + 1; // h', q' from row k+1 on
+		const double* qp = qprev.data() + 1;
+		for (int j = 0; j < len; ++j) {
+			double* col = &M(k + 1, k + 1 + j); // col[i], i >= j: A22(i, j)
+			if (pending) {
+				const double hj = hp[j], qj = qp[j];
+				for (int i = j; i < len; ++i)
+					col[i] -= hp[i] * qj + qp[i] * hj;
+			}
+			if (b != 0.0) {
+				const double hj = h[j];
+				double       pj = col[j] * hj;
+				for (int i = j + 1; i < len; ++i) {
+					pj += col[i] * h[i];
+					p[size_t(i)] += col[i] * hj;
+				}
+				p[size_t(j)] += pj;
+			}
+		}
+		pending = b != 0.0;
+		if (!pending)
+			continue;
+		// p = beta A22 h, w = p - (beta / 2)(p^T h) h: the update of this step
+		double ph = 0.0;
+		for (int i = 0; i < len; ++i) {
+			p[size_t(i)] *= b;
+			ph += p[size_t(i)] * h[i];
+		}
+		for (int i = 0; i < len; ++i) {
+			qprev[size_t(i)] = p[size_t(i)] - 0.5 * b * ph * h[i];
+			hprev[size_t(i)] = h[i];
+		}
+	}
+	if (pending) { // the last update reaches the trailing 2 x 2 block
+		const int k0 = n - 2; // hprev index 0 is row n - 2
+		for (int j = 0; j < 2; ++j)
+			for (int i = j; i < 2; ++i)
+				M(k0 + i, k0 + j) -= hprev[size_t(i)] * qprev[size_t(j)] + qprev[size_t(i)] * hprev[size_t(j)];
+	}
+	d[N - 2]   = M(n - 2, n - 2);
+	d[N - 1]   = M(n - 1, n - 1);
+	off[N - 2] = M(n - 1, n - 2);
+}
+
+// v (n x ncols, column-major) <- Q v
+void apply_q(int n, const std::vector<double>& hv, const std::vector<double>& beta, double* v, int ncols)
+{
+	const size_t N = size_t(n);
+	for (int k = n - 3; k >= 0; --k) {
+		if (beta[size_t(k)] == 0.0)
+			continue;
+		const double* h   = hv.data() + size_t(k) * N;
+		const int     len = n - k - 1;
+		for (int c = 0; c < ncols; ++c) {
+			double* x = v + size_t(c) * N + size_t(k) + 1;
+			double  s = 0.0;
+			for (int i = 0; i < len; ++i)
+				s += h[i] * x[i];
+			s *= beta[size_t(k)];
+			for (int i = 0; i < len; ++i)
+				x[i] -= s * h[i];
+		}
+	}
+}
+
 bool sym_lowest(int n, const double* a, double* w, double* v)
 {
 	if (n <= 0)
@@ -301,68 +455,152 @@ bool sym_lowest(int n, const double* a, double* w, double* v)
 		v[0] = 1.0;
 		return true;
 	}
-	// Householder reduction T = Q^T A Q, Q = P_0 P_1 ... P_{n-3}; P_k acts on
-	// rows / columns k+1..n-1 with P_k = I - beta_k h_k h_k^T, h_k(0) = 1
-	// (Golub and Van Loan, algorithms 5.1.1 and 8.3.1)
-	const size_t        N = size_t(n);
-	std::vector<double> m(a, a + N * N), d(N), off(N - 1), hv(N * N, 0.0), beta(N, 0.0), p(N), q(N);
-	auto                M = [&](int i, int j) -> double& { return m[size_t(i) + size_t(j) * N]; };
-	for (int k = 0; k + 2 < n; ++k) {
-		const int len   = n - k - 1;
-		double*   h     = hv.data() + size_t(k) * N; // h[0..len)
-		double    sigma = 0.0;
-		for (int i = 1; i < len; ++i)
-			sigma += M(k + 1 + i, k) * M(k + 1 + i, k);
-		const double x0 = M(k + 1, k);
-		d[size_t(k)]    = M(k, k);
-		if (sigma == 0.0) { // already tridiagonal in this column
-			off[size_t(k)] = x0;
-			continue;
-		}
-		const double mu = std::sqrt(x0 * x0 + sigma);
-		const double h0 = x0 <= 0.0 ? x0 - mu : -sigma / (x0 + mu);
-		beta[size_t(k)] = 2.0 * h0 * h0 / (sigma + h0 * h0);
-		h[0]            = 1.0;
-		for (int i = 1; i < len; ++i)
-			h[i] = M(k + 1 + i, k) / h0;
-		off[size_t(k)] = mu;
-		// trailing block A22 <- P A22 P = A22 - h w^T - w h^T with
-		// p = beta A22 h, w = p - (beta / 2)(p^T h) h
-		const double b = beta[size_t(k)];
-		for (int i = 0; i < len; ++i) {
-			double s = 0.0;
-			for (int j = 0; j < len; ++j)
-				s += M(k + 1 + i, k + 1 + j) * h[j];
-			p[size_t(i)] = b * s;
-		}
-		double ph = 0.0;
-		for (int i = 0; i < len; ++i)
-			ph += p[size_t(i)] * h[i];
-		for (int i = 0; i < len; ++i)
-			q[size_t(i)] = p[size_t(i)] - 0.5 * b * ph * h[i];
-		for (int j = 0; j < len; ++j)
-			for (int i = 0; i < len; ++i)
-				M(k + 1 + i, k + 1 + j) -= h[i] * q[size_t(j)] + q[size_t(i)] * h[j];
-	}
-	d[N - 2]   = M(n - 2, n - 2);
-	d[N - 1]   = M(n - 1, n - 1);
-	off[N - 2] = M(n - 1, n - 2);
+	std::vector<double> d, off, hv, beta;
+	householder_tridiag(n, a, d, off, hv, beta);
 	// lowest eigenpair of T, then v = Q z
 	*w = tridiag_kth_lowest(n, d.data(), off.data(), 1);
 	tridiag_inverse_iteration(n, d.data(), off.data(), *w, v);
-	for (int k = n - 3; k >= 0; --k) {
-		if (beta[size_t(k)] == 0.0)
-			continue;
-		const double* h   = hv.data() + size_t(k) * N;
-		const int     len = n - k - 1;
-		double        s   = 0.0;
-		for (int i = 0; i < len; ++i)
-			s += h[i] * v[k + 1 + i];
-		s *= beta[size_t(k)];
-		for (int i = 0; i < len; ++i)
-			v[k + 1 + i] -= s * h[i];
-	}
+	apply_q(n, hv, beta, v, 1);
 	return true;
+}
+
+bool sym_eigen_full(int n, const double* a, double* w, double* v)
+{
+	if (n <= 0)
+		return true;
+	if (n == 1) {
+		w[0] = a[0];
+		if (v)
+			v[0] = 1.0;
+		return true;
+	}
+	std::vector<double> d, off, hv, beta;
+	householder_tridiag(n, a, d, off, hv, beta);
+	if (!tridiag_eigen(n, d.data(), off.data(), v))
+		return false;
+	std::copy(d.begin(), d.end(), w);
+	if (v)
+		apply_q(n, hv, beta, v, n);
+	return true;
+}
+
+} // namespace dmrgpp
+
+namespace dmrgpp {
+
+void tridiag_eigenvectors(int n, const double* d, const double* off, const double* w, int k, double* z)
+{
+	if (n <= 0 || k <= 0)
+		return;
+	const size_t N = size_t(n);
+	if (n == 1) {
+		for (int j = 0; j < k; ++j)
+			z[j] = 1.0;
+		return;
+	}
+	double norm = 0.0;
+	for (int i = 0; i < n; ++i)
+		norm = std::max(norm, std::fabs(d[i]) + (i > 0 ? std::fabs(off[i - 1]) : 0.0)
+		                         + (i + 1 < n ? std::fabs(off[i]) : 0.0));
+	if (!(norm > 0.0)) { // the zero matrix: any orthonormal set
+		std::fill(z, z + N * size_t(k), 0.0);
+		for (int j = 0; j < k; ++j)
+			z[size_t(j) * N + size_t(j % n)] = 1.0;
+		return;
+	}
+	const double ortol = 1e-3 * norm;
+	const double tiny  = norm * 1e-15;
+	std::vector<double> u0(N), u1(N), u2(N), m(N);
+	std::vector<char>   sw(N);
+	int                 cluster = 0; // first vector of the current cluster
+	for (int j = 0; j < k; ++j) {
+		if (j > 0 && w[j] - w[j - 1] > ortol)
+			cluster = j;
+		// LU of T - w_j I with row interchanges (as tridiag_inverse_iteration)
+		std::fill(u1.begin(), u1.end(), 0.0);
+		std::fill(u2.begin(), u2.end(), 0.0);
+		std::fill(m.begin(), m.end(), 0.0);
+		std::fill(sw.begin(), sw.end(), 0);
+		double a = d[0] - w[j], b = off[0];
+		for (int i = 0; i + 1 < n; ++i) {
+			const double l = off[i], dd = d[i + 1] - w[j], uu = i + 2 < n ? off[i + 1] : 0.0;
+			if (std::fabs(a) >= std::fabs(l)) {
+				if (a == 0.0)
+					a = tiny;
+				u0[size_t(i)] = a;
+				u1[size_t(i)] = b;
+				m[size_t(i)]  = l / a;
+				a             = dd - m[size_t(i)] * b;
+				b             = uu;
+			} else {
+				u0[size_t(i)] = l;
+				u1[size_t(i)] = dd;
+				u2[size_t(i)] = uu;
+				m[size_t(i)]  = a / l;
+				sw[size_t(i)] = 1;
+				const double na = b - m[size_t(i)] * dd;
+				b               = -m[size_t(i)] * uu;
+				a               = na;
+			}
+		}
+		u0[N - 1] = a == 0.0 ? tiny : a;
+		// seeded start vector, three solves, each followed by Gram-Schmidt
+		// against the earlier vectors of the cluster (the grouping of LAPACK's
+		// dstein: eigenvalues closer than 1e-3 |T|)
+		double*                                x = z + size_t(j) * N;
+		std::mt19937_64                        rng(0x9e3779b97f4a7c15ULL + uint64_t(j));
+		std::uniform_real_distribution<double> uni(-1.0, 1.0);
+		for (int i = 0; i < n; ++i)
+			x[i] = uni(rng);
+		for (int iter = 0; iter < 3; ++iter) {
+			for (int i = 0; i + 1 < n; ++i) {
+				if (sw[size_t(i)]) {
+					const double t = x[i];
+					x[i]           = x[i + 1];
+					x[i + 1]       = t - m[size_t(i)] * x[i + 1];
+				} else {
+					x[i + 1] -= m[size_t(i)] * x[i];
+				}
+			}
+			for (int i = n - 1; i >= 0; --i) {
+				double s = x[i];
+				if (i + 1 < n)
+					s -= u1[size_t(i)] * x[i + 1];
+				if (i + 2 < n)
+					s -= u2[size_t(i)] * x[i + 2];
+				x[i] = s / u0[size_t(i)];
+			}
+			for (int q = cluster; q < j; ++q) {
+				const double* y = z + size_t(q) * N;
+				double        p = 0.0;
+				for (int i = 0; i < n; ++i)
+					p += y[i] * x[i];
+				for (int i = 0; i < n; ++i)
+					x[i] -= p * y[i];
+			}
+			double nrm = 0.0;
+			for (int i = 0; i < n; ++i)
+				nrm += x[i] * x[i];
+			nrm = std::sqrt(nrm);
+			if (!(nrm > 0.0) || !std::isfinite(nrm)) { // start again from a unit vector
+				std::fill(x, x + N, 0.0);
+				x[j % n] = 1.0;
+				continue;
+			}
+			for (int i = 0; i < n; ++i)
+				x[i] /= nrm;
+		}
+		double big = 0.0;
+		int    arg = 0;
+		for (int i = 0; i < n; ++i)
+			if (std::fabs(x[i]) > big) {
+				big = std::fabs(x[i]);
+				arg = i;
+			}
+		if (x[arg] < 0.0)
+			for (int i = 0; i < n; ++i)
+				x[i] = -x[i];
+	}
 }
 
 } // namespace dmrgpp

@@ -1,6 +1,8 @@
 // Symmetric tridiagonal eigensolver (tridiag.cpp).
 #pragma once
 
+#include <vector>
+
 namespace dmrgpp {
 
 // Eigenvalues (ascending, into d) and optionally eigenvectors (z: n x n
@@ -8,6 +10,24 @@ namespace dmrgpp {
 // matrix with diagonal d[0..n-1] and off-diagonal off[0..n-2].  Returns false
 // if the iteration fails to converge.
 bool tridiag_eigen(int n, double* d, const double* off, double* z);
+
+// Unit eigenvectors z (n x k, column-major) of the symmetric tridiagonal
+// matrix (d, off) for its eigenvalues w[0..k) (ascending, as computed by
+// tridiag_eigen) by inverse iteration: for each, three solves with the LU of
+// T - w_j I from a seeded start vector, each followed by Gram-Schmidt against
+// the earlier vectors of its cluster (eigenvalues closer than 1e-3 |T|, the
+// grouping of LAPACK's dstein); the largest component is made positive.
+void tridiag_eigenvectors(int n, const double* d, const double* off, const double* w, int k, double* z);
+
+// Householder reduction T = Q^T A Q of the dense symmetric n x n matrix a
+// (column-major, n >= 2), Q = P_0 ... P_{n-3}, P_k = I - beta_k h_k h_k^T
+// acting on entries k+1..n-1 with h_k(0) = 1: diagonal d (n), off-diagonal
+// off (n - 1), reflectors hv (n x n, column k holds h_k) and beta (n).
+void householder_tridiag(int n, const double* a, std::vector<double>& d, std::vector<double>& off,
+                         std::vector<double>& hv, std::vector<double>& beta);
+
+// v (n x ncols, column-major) <- Q v for the reflectors of householder_tridiag.
+void apply_q(int n, const std::vector<double>& hv, const std::vector<double>& beta, double* v, int ncols);
 
 } // namespace dmrgpp
 
@@ -23,6 +43,12 @@ bool sym_eigen(int n, const double* a, double* w, double* v);
 // tridiagonal eigenvector, transformed back.  About (4/3) n^3 flops, against
 // some 20 n^3 for the full Jacobi solve above.
 bool sym_lowest(int n, const double* a, double* w, double* v);
+
+// All eigenvalues (ascending, w) and, when v != NULL, the eigenvectors (v:
+// n x n column-major, column i belongs to w[i]) of the dense symmetric matrix
+// a by Householder reduction and the implicit QL iteration of tridiag_eigen;
+// about 6 n^3 flops.  Returns false if the QL iteration fails to converge.
+bool sym_eigen_full(int n, const double* a, double* w, double* v);
 
 } // namespace dmrgpp
 

@@ -505,6 +505,57 @@ int dmrgpp_wft_flops(dmrgpp_wft_handle h, double* flops);
 int dmrgpp_wft_destroy(dmrgpp_wft_handle h);
 const char* dmrgpp_wft_last_error(dmrgpp_wft_handle h);
 
+/* ---- Density-matrix truncation after a sector solve ----
+ * The reference's per-patch SVD route (DensityMatrixSvd.h:285-410,
+ * Truncation.h:218-285 changeBasis, 373-519 updateKeptStates /
+ * computeKeptStates).  The block being truncated (the system block when
+ * side = 0, the environment when side = 1) has ngroups quantum-number groups
+ * of group_size[g] states; patch p of the sector (left group of l_p, right
+ * group of r_p states; block X_p is r_p x l_p column-major) belongs to group
+ * patch_group[p] of that block.  For ntargets sector vectors (psi: device,
+ * ntargets x D, target-major, patch order) with weights w_t:
+ *     side 0:  rho_g = sum_t w_t sum_{p in g} X_{t,p}^T X_{t,p}   (l_p x l_p)
+ *     side 1:  rho_g = sum_t w_t sum_{p in g} X_{t,p} X_{t,p}^T   (r_p x r_p)
+ * which is M_g M_g^T of the reference's stacked per-group matrix M_g, so its
+ * eigenvalues are the squared singular values the reference takes from
+ * svd('A', M_g).  The rho_g are formed by grouped DGEMMs on the FP64 tensor
+ * pipe; their tridiagonal reductions (Householder) and eigenvalues (implicit
+ * QL) are computed on the host cores, the kept eigenvectors by inverse
+ * iteration there and transformed back on the device; groups without
+ * patches have rho_g = 0.  All states are ranked by eigenvalue
+ * (ascending; ties by group, then by index), the kept number K follows
+ * computeKeptStates (tolerance < 0: K = m; else the fewest states, not below
+ * m_min, whose removal keeps the discarded weight within the tolerance, never
+ * more than m), and the N - K lowest are removed. */
+typedef struct {
+	size_t        npatches;
+	const size_t* left_patch_size;
+	const size_t* right_patch_size;
+	const size_t* patch_group; /* per patch: its group in the block being truncated */
+	size_t        ngroups;
+	const size_t* group_size;  /* states per group; l_p (side 0) or r_p (side 1) of its patches */
+	int           side;        /* 0: system (left) block, 1: environment (right) block */
+	size_t        ntargets;
+	const double* psi;         /* device, ntargets x D */
+	const double* weights;     /* host, ntargets; NULL: every weight 1 */
+	void*         stream;
+	int           device;      /* -1: current */
+} dmrgpp_density_desc;
+
+/* Host outputs: eigenvalues (sum_g group_size[g] entries): each group's
+ * eigenvalues ascending, group after group; kept[g]: states kept in group g
+ * (its kept[g] largest eigenvalues); vectors (may be NULL; room for
+ * sum_g group_size[g]^2 doubles): the kept eigenvectors, group after group,
+ * group g's as a group_size[g] x kept[g] column-major block whose columns
+ * follow its last kept[g] eigenvalues (ascending) -- the truncated
+ * transformation of the reference's changeBasis; *kept_total = K;
+ * *discarded = the sum of the removed eigenvalues' magnitudes (the
+ * reference's "Discarded weight").  Synchronous.  Errors: the calling
+ * thread's message, dmrgpp_kron_last_error(NULL). */
+int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, double tolerance, size_t m_min,
+                            double* eigenvalues, double* vectors, size_t* kept, size_t* kept_total,
+                            double* discarded);
+
 /* Last error message of a handle, or of the calling thread's last failed
  * create when h is NULL.  Never returns NULL. */
 const char* dmrgpp_kron_last_error(dmrgpp_kron_handle h);

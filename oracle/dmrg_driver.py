@@ -27,13 +27,18 @@ Operators are block-sparse by quantum number: {(out_group, in_group): dense}.
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import Callable, Dict, List, Tuple
+from typing import Callable, Dict, List, Optional, Tuple
 
 import numpy as np
 
 from dmrgpp_b200.superblock import KronProblem
 
 BlockOp = Dict[Tuple[int, int], np.ndarray]
+
+
+class KeptBasis(dict):
+    """{group: U_g (group size x kept)}: the kept eigenvectors of a block's
+    reduced density matrix chosen outside the driver (DMRG.truncator)."""
 
 
 @dataclass
@@ -214,6 +219,10 @@ class DMRG:
         self.energies: List[float] = []
         self.sectors: List[KronProblem] = []
         self.keep_sectors = False
+        # optional (prob, patches, psi, side, enlarged block, m) -> KeptBasis
+        # (side 0: the left block, 1: the right block) in place of the
+        # driver's own density-matrix truncation
+        self.truncator: Optional[Callable] = None
 
     # enlarge a left block by one site on its right
     def grow_left(self, b: Block) -> Block:
@@ -276,20 +285,24 @@ class DMRG:
                            name=f"dmrg-superblock-{left.length}+{right.length}")
         return prob, patches
 
-    def truncate(self, blk: Block, rho: Dict[int, np.ndarray]) -> Block:
+    def truncate(self, blk: Block, rho) -> Block:
         """Keep the m largest-weight eigenvectors of the block-diagonal
-        reduced density matrix (DensityMatrixSvd.h:285-391)."""
-        evals, evecs = [], {}
-        for g, r in rho.items():
-            w, v = np.linalg.eigh(0.5 * (r + r.T))
-            evecs[g] = (w, v)
-            evals += [(wi, g, i) for i, wi in enumerate(w)]
-        evals.sort(key=lambda t: -t[0])
-        kept: Dict[int, List[int]] = {}
-        for wi, g, i in evals[:self.m]:
-            kept.setdefault(g, []).append(i)
-        groups = sorted(kept)
-        U = {g: evecs[g][1][:, sorted(kept[g])] for g in groups}
+        reduced density matrix (DensityMatrixSvd.h:285-391); rho is either
+        {group: rho_g} or a KeptBasis chosen by an external truncation."""
+        if isinstance(rho, KeptBasis):
+            U = {g: u for g, u in rho.items() if u.shape[1] > 0}
+        else:
+            evals, evecs = [], {}
+            for g, r in rho.items():
+                w, v = np.linalg.eigh(0.5 * (r + r.T))
+                evecs[g] = (w, v)
+                evals += [(wi, g, i) for i, wi in enumerate(w)]
+            evals.sort(key=lambda t: -t[0])
+            kept: Dict[int, List[int]] = {}
+            for wi, g, i in evals[:self.m]:
+                kept.setdefault(g, []).append(i)
+            U = {g: evecs[g][1][:, sorted(kept[g])] for g in sorted(kept)}
+        groups = sorted(U)
         newi = {g: n for n, g in enumerate(groups)}
         ops = {}
         for name, op in blk.ops.items():
@@ -313,6 +326,9 @@ class DMRG:
         self.energies.append(float(e))
         if self.keep_sectors:
             self.sectors.append(prob)
+        if self.truncator is not None:
+            return (float(e), lp, rp, self.truncator(prob, patches, psi, 0, lp, self.m),
+                    self.truncator(prob, patches, psi, 1, rp, self.m))
         rho_l, rho_r = {}, {}
         xs = prob.xy_start
         for p, (gl, gr) in enumerate(patches):

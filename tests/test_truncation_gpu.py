@@ -1,0 +1,133 @@
+"""dmrgpp_density_truncate through the C ABI against the numpy oracle
+(oracle/truncation_oracle.py): density-matrix eigenvalues, eigenvectors, the
+kept states per group and the discarded weight, for the system and the
+environment block, one and two weighted targets, groups shared by several
+patches and groups without patches; and whole DMRG runs whose every
+truncation goes through the library."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import truncation_oracle as to
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _layout(seed, side):
+    """Patches whose block-side groups are shared in pairs, plus one empty
+    group at the end."""
+    rng = np.random.default_rng(seed)
+    ng = 5
+    gsize = rng.integers(1, 90, ng)
+    lsz, rsz, pg = [], [], []
+    for g in range(ng):
+        for _ in range(int(rng.integers(1, 3))):
+            other = int(rng.integers(1, 120))
+            lsz.append(int(gsize[g]) if side == 0 else other)
+            rsz.append(other if side == 0 else int(gsize[g]))
+            pg.append(g)
+    return lsz, rsz, pg, [int(x) for x in gsize] + [7]
+
+
+@pytest.mark.parametrize("side", [0, 1])
+@pytest.mark.parametrize("targets", [1, 2])
+def test_truncation_matches_oracle(cuda_lib, cuda_device, side, targets):
+    import torch
+    from dmrgpp_b200.truncation import density_truncate
+    lsz, rsz, pg, gs = _layout(10 * side + targets, side)
+    D = int(np.dot(lsz, rsz))
+    rng = np.random.default_rng(targets)
+    psis = [rng.standard_normal(D) for _ in range(targets)]
+    psis = [p / np.linalg.norm(p) for p in psis]
+    w = [1.0] if targets == 1 else [0.7, 0.3]
+    N = sum(gs)
+    for m, tol, mmin in ((N // 3, -1.0, 0), (N // 2, 1e-3, 5), (N + 10, -1.0, 0)):
+        ref = to.truncate(lsz, rsz, pg, gs, side, psis, m, tol, mmin, weights=w)
+        psi_d = torch.tensor(np.concatenate(psis), device="cuda")
+        out = density_truncate(lsz, rsz, pg, gs, side, psi_d, m, tol, mmin,
+                               weights=w if targets > 1 else None)
+        assert out["kept_total"] == ref["kept_total"]
+        assert np.array_equal(out["kept"], ref["kept"])
+        assert abs(out["discarded"] - ref["discarded"]) <= 1e-13
+        for g in range(len(gs)):
+            we, wr = out["eigenvalues"][g], ref["eigenvalues"][g]
+            assert np.abs(we - wr).max(initial=0.0) <= 1e-14, g
+            V = out["vectors"][g]
+            n, k = gs[g], int(out["kept"][g])
+            assert V.shape == (n, k)
+            assert np.abs(V.T @ V - np.eye(k)).max(initial=0.0) < 1e-12
+            # eigenvectors of the oracle's density matrix for the kept eigenvalues
+            assert np.abs(ref["rho"][g] @ V - V * we[n - k:]).max(initial=0.0) < 1e-13
+            if 0 < k < n and wr[n - k] - wr[n - k - 1] > 1e-9:
+                P = V @ V.T
+                Pr = ref["vectors"][g][:, n - k:] @ ref["vectors"][g][:, n - k:].T
+                assert np.abs(P - Pr).max() < 1e-8, g
+        assert np.abs(out["eigenvalues"][-1]).max() == 0.0    # the group without patches
+        if targets == 1:
+            assert abs(sum(x.sum() for x in out["eigenvalues"]) - 1.0) < 1e-12
+
+
+def test_truncation_argument_checks(cuda_lib, cuda_device):
+    import torch
+    from dmrgpp_b200 import _capi
+    from dmrgpp_b200.truncation import density_truncate
+    psi = torch.zeros(6, dtype=torch.float64, device="cuda")
+    with pytest.raises(_capi.DmrgppError):       # group size differs from the patch's
+        density_truncate([2], [3], [0], [3], 0, psi, 2)
+    with pytest.raises(_capi.DmrgppError):       # group out of range
+        density_truncate([2], [3], [1], [2], 0, psi, 2)
+    with pytest.raises(_capi.DmrgppError):       # m_min above m
+        density_truncate([2], [3], [0], [2], 0, psi, 1, 1e-3, 2)
+
+
+def gpu_solver(prob, init):
+    """FP64 device Lanczos of one superblock sector."""
+    from dmrgpp_b200 import plugin
+    bg = plugin.BatchedGemm.from_problem(prob)
+    try:
+        return bg.lanczos_lowest(init, steps=200, tolerance=1e-10)
+    finally:
+        bg.close()
+
+
+def gpu_truncator(prob, patches, psi, side, blk, m):
+    """The driver's truncation through dmrgpp_density_truncate (groups of the
+    enlarged block that appear in the sector, as the driver's own does)."""
+    import torch
+    from oracle.dmrg_driver import KeptBasis
+    from dmrgpp_b200.truncation import density_truncate
+    groups = sorted({p[side] for p in patches})
+    index = {g: q for q, g in enumerate(groups)}
+    pg = [index[p[side]] for p in patches]
+    gs = [blk.sizes[g] for g in groups]
+    out = density_truncate(prob.lsz, prob.rsz, pg, gs, side,
+                           torch.tensor(np.asarray(psi), device="cuda"), m)
+    kb = KeptBasis()
+    for q, g in enumerate(groups):
+        kb[g] = out["vectors"][q]
+    return kb
+
+
+def test_dmrg_with_device_truncation_matches_reference(cuda_lib, cuda_device):
+    """Heisenberg L=32, m=128, every solve and every truncation on the device:
+    the reference's own test energy (dmrg/CMakeLists.txt:343-344) and the
+    run with the driver's host truncation."""
+    from oracle import dmrg_driver as dd
+    g = json.load(open(os.path.join(GOLDEN, "dmrg_heisenberg_L32_m128.json")))
+    d = dd.DMRG(dd.Heisenberg(), L=32, m=128, solver=gpu_solver)
+    d.truncator = gpu_truncator
+    e = d.run(sweeps=2)
+    assert abs(e - g["reference_test_energy"]) < g["reference_test_tolerance"]
+    assert abs(e - g["energy"]) < 1e-6, (e, g["energy"])
+
+
+def test_hubbard_with_device_truncation_is_exact_at_u0(cuda_lib, cuda_device):
+    from oracle import dmrg_driver as dd
+    d = dd.DMRG(dd.Hubbard(U=0.0), L=8, m=256, solver=gpu_solver)
+    d.truncator = gpu_truncator
+    e = d.run(sweeps=1)
+    assert abs(e - (-9.51754)) < 1e-5          # dmrg/CMakeLists.txt:180-181
+    assert abs(e - dd.free_fermion_energy(8, 4, 4)) < 1e-9

@@ -2,7 +2,8 @@
 // the k-th lowest eigenvalue by Sturm bisection against the QL solver, and
 // the inverse-iteration eigenvector's residual, on seeded random and
 // Lanczos-like (graded, nearly degenerate) tridiagonals; and the lowest pair
-// of dense symmetric matrices by sym_lowest against the Jacobi solver.
+// of dense symmetric matrices by sym_lowest, and all pairs by sym_eigen_full,
+// against the Jacobi solver.
 // Prints "ok <worst eigenvalue error> <worst residual>" or "FAIL ...".
 #include "tridiag.h"
 
@@ -87,6 +88,117 @@ int main()
 			return 1;
 		}
 		worst_e = std::max(worst_e, std::fabs(th - ev[0]) / scale);
+		worst_r = std::max(worst_r, res / scale);
+	}
+	// all pairs of dense symmetric matrices (sym_eigen_full): eigenvalues
+	// against the Jacobi solver, residuals and orthonormality of the vectors;
+	// random, graded, and density-matrix-like (Gram matrices, eigenvalues down
+	// to round-off) cases
+	for (int trial = 0; trial < 240; ++trial) {
+		const int           n = 1 + (trial * 7) % 90;
+		const size_t        N = size_t(n);
+		std::vector<double> A(N * N, 0.0), ev(N), V(N * N), w(N), Z(N * N);
+		if (trial % 3 == 2) { // X^T X with X n/2 x n: rank deficient
+			const int           r = std::max(1, n / 2);
+			std::vector<double> X(size_t(r) * N);
+			for (size_t q = 0; q < X.size(); ++q) // rows of X decay like a DMRG spectrum in half the cases
+				X[q] = trial % 2 ? u(rng) * std::exp(-0.7 * double(q % size_t(r)))
+				                 : u(rng) * std::exp(-4.0 * std::fabs(u(rng)));
+			for (int j = 0; j < n; ++j)
+				for (int i = 0; i < n; ++i) {
+					double s = 0.0;
+					for (int k = 0; k < r; ++k)
+						s += X[size_t(k) + size_t(i) * size_t(r)] * X[size_t(k) + size_t(j) * size_t(r)];
+					A[size_t(i) + size_t(j) * N] = s;
+				}
+		} else {
+			for (int j = 0; j < n; ++j)
+				for (int i = 0; i <= j; ++i) {
+					double x = u(rng);
+					if (trial % 3 == 1)
+						x = i == j ? -10.0 + 0.5 * i + 1e-3 * x : 1e-2 * x;
+					A[size_t(i) + size_t(j) * N] = A[size_t(j) + size_t(i) * N] = x;
+				}
+		}
+		dmrgpp::sym_eigen(n, A.data(), ev.data(), V.data());
+		if (!dmrgpp::sym_eigen_full(n, A.data(), w.data(), Z.data())) {
+			std::printf("FAIL full %d\n", trial);
+			return 1;
+		}
+		double scale = 1.0, de = 0.0, res = 0.0, orth = 0.0;
+		for (double x : ev)
+			scale = std::max(scale, std::fabs(x));
+		for (int c = 0; c < n; ++c) {
+			de = std::max(de, std::fabs(w[size_t(c)] - ev[size_t(c)]));
+			for (int i = 0; i < n; ++i) {
+				double t = -w[size_t(c)] * Z[size_t(i) + size_t(c) * N];
+				for (int j = 0; j < n; ++j)
+					t += A[size_t(i) + size_t(j) * N] * Z[size_t(j) + size_t(c) * N];
+				res = std::max(res, std::fabs(t));
+			}
+			for (int c2 = 0; c2 <= c; ++c2) {
+				double s = 0.0;
+				for (int i = 0; i < n; ++i)
+					s += Z[size_t(i) + size_t(c) * N] * Z[size_t(i) + size_t(c2) * N];
+				orth = std::max(orth, std::fabs(s - (c == c2 ? 1.0 : 0.0)));
+			}
+		}
+		if (de > 1e-13 * scale || res > 1e-12 * scale || orth > 1e-12) {
+			std::printf("FAIL full %d %g %g %g\n", trial, de, res, orth);
+			return 1;
+		}
+		worst_e = std::max(worst_e, de / scale);
+		worst_r = std::max(worst_r, res / scale);
+	}
+	// the top k eigenvectors by inverse iteration (tridiag_eigenvectors):
+	// residuals and orthonormality, on random, graded and clustered
+	// tridiagonals (exactly repeated diagonal blocks give repeated eigenvalues)
+	for (int trial = 0; trial < 150; ++trial) {
+		const int           n = 1 + (trial * 5) % 70;
+		const size_t        N = size_t(n);
+		std::vector<double> d(N), e(N, 0.0), w;
+		for (int i = 0; i < n; ++i) {
+			d[size_t(i)] = trial % 3 == 1 ? std::exp(-0.5 * i) * u(rng) : u(rng);
+			e[size_t(i)] = trial % 3 == 1 ? 1e-3 * std::exp(-0.5 * i) * u(rng) : u(rng);
+		}
+		if (trial % 10 == 9) // the zero matrix (a density-matrix group without patches)
+			std::fill(d.begin(), d.end(), 0.0), std::fill(e.begin(), e.end(), 0.0);
+		else if (trial % 3 == 2 && n >= 4) // two decoupled copies of one block
+			for (int i = 0; i < n / 2; ++i) {
+				d[size_t(n / 2 + i)] = d[size_t(i)];
+				e[size_t(n / 2 + i)] = i + 1 < n / 2 ? e[size_t(i)] : 0.0;
+				if (i + 1 == n / 2)
+					e[size_t(i)] = 0.0;
+			}
+		w = d;
+		dmrgpp::tridiag_eigen(n, w.data(), e.data(), nullptr);
+		const int           k = std::max(1, n / 3);
+		std::vector<double> Z(N * size_t(k));
+		dmrgpp::tridiag_eigenvectors(n, d.data(), e.data(), w.data() + (n - k), k, Z.data());
+		double scale = 1.0, res = 0.0, orth = 0.0;
+		for (double x : w)
+			scale = std::max(scale, std::fabs(x));
+		for (int c = 0; c < k; ++c) {
+			const double th = w[size_t(n - k + c)];
+			for (int i = 0; i < n; ++i) {
+				double t = (d[size_t(i)] - th) * Z[size_t(i) + size_t(c) * N];
+				if (i > 0)
+					t += e[size_t(i - 1)] * Z[size_t(i - 1) + size_t(c) * N];
+				if (i + 1 < n)
+					t += e[size_t(i)] * Z[size_t(i + 1) + size_t(c) * N];
+				res = std::max(res, std::fabs(t));
+			}
+			for (int c2 = 0; c2 <= c; ++c2) {
+				double s = 0.0;
+				for (int i = 0; i < n; ++i)
+					s += Z[size_t(i) + size_t(c) * N] * Z[size_t(i) + size_t(c2) * N];
+				orth = std::max(orth, std::fabs(s - (c == c2 ? 1.0 : 0.0)));
+			}
+		}
+		if (res > 1e-12 * scale || orth > 1e-12) {
+			std::printf("FAIL vectors %d %g %g\n", trial, res, orth);
+			return 1;
+		}
 		worst_r = std::max(worst_r, res / scale);
 	}
 	if (worst_e > 1e-13 || worst_r > 1e-12) {
