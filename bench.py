@@ -475,6 +475,15 @@ def ladder_measurements(torch, dev, stream):
                                        with_davidson=False)
     out["wft"] = wft_measurement(torch, prob, stream, flush)
     out["truncation"] = truncation_measurement(torch, prob, stream)
+    # one whole sweep step of the sector: wave-function transformation (the
+    # initial guess), the eigensolve, the truncation of the grown block
+    sv = out["solve"]
+    rest = out["wft"]["ms"] * 1e-3 + out["truncation"]["seconds"]
+    fp64 = sv["fp64_lanczos"]["seconds"] + rest
+    mixed = sv["mixed_lanczos_refined"]["seconds"] + rest
+    out["step"] = {"fp64_seconds": fp64, "mixed_seconds": mixed, "speedup": fp64 / mixed,
+                   "parts": "wft + solve + truncation (m = 4000 of 16000 states); the WFT and "
+                            "truncation run in FP64 in both"}
     return out
 
 
@@ -493,19 +502,20 @@ def truncation_measurement(torch, prob, stream, m: int = 4000):
     psi = torch.from_numpy(psi_h).cuda()
     pg = list(range(prob.npatches))
     density_truncate(l, r, pg, l, 0, psi, m, stream=stream.cuda_stream)   # warm-up
-    ts = []
+    from dmrgpp_b200.truncation import truncation_profile
+    runs = []
     for _ in range(3):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         out = density_truncate(l, r, pg, l, 0, psi, m, stream=stream.cuda_stream)
-        ts.append(time.perf_counter() - t0)
-    t = min(ts)
+        runs.append((time.perf_counter() - t0, truncation_profile()))
+    t, phases = min(runs, key=lambda x: x[0])
     t0 = time.perf_counter()
     ref = truncation_oracle.truncate(l, r, pg, l, 0, [psi_h], m)
     t_cpu = time.perf_counter() - t0
     dw = max(float(np.abs(a - b).max()) for a, b in zip(out["eigenvalues"], ref["eigenvalues"]))
     return {"states": int(np.sum(l)), "groups": int(prob.npatches), "kept": out["kept_total"],
-            "seconds": t, "discarded": out["discarded"],
+            "seconds": t, "phases": phases, "discarded": out["discarded"],
             "same_kept_per_group_as_oracle": bool(np.array_equal(out["kept"], ref["kept"])),
             "max_abs_eigenvalue_diff_vs_oracle": dw,
             "cpu_oracle": {"seconds": t_cpu, "cores": os.cpu_count(),

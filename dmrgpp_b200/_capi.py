@@ -147,6 +147,7 @@ SIGNATURES.update({
     "dmrgpp_mlp_last_error": (ctypes.c_char_p, [_vp]),
     "dmrgpp_density_truncate": (ctypes.c_int, [ctypes.POINTER(DensityDesc), _sz, ctypes.c_double,
                                                _sz, _dp, _dp, _szp, _szp, _dp]),
+    "dmrgpp_density_profile": (ctypes.c_int, [_dp, ctypes.c_int]),
 })
 
 SIGNATURES.update({

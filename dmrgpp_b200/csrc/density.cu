@@ -23,7 +23,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
+#include <memory>
 #include <cmath>
 #include <numeric>
 #include <string>
@@ -142,6 +144,41 @@ size_t compute_kept(size_t kept_states, double tolerance, size_t m_min, const st
 
 int fail(int status, const std::string& msg) { return handle_fail(nullptr, status, msg); }
 
+using Clock = std::chrono::steady_clock;
+thread_local double g_trunc_times[DMRGPP_TRUNC_NPHASES] = {};
+
+// Page-locked host buffers of the calling thread, kept between calls (the
+// density matrices, reflectors and vectors cross PCIe every call; pageable
+// copies and first-touch page faults would cost more than the transfers).
+struct PinnedSlot {
+	void*  p   = nullptr;
+	size_t cap = 0;
+	~PinnedSlot()
+	{
+		if (p)
+			cudaFreeHost(p);
+	}
+};
+thread_local PinnedSlot g_pinned[4];
+
+template <class T> T* pinned(int slot, size_t n)
+{
+	PinnedSlot& s     = g_pinned[slot];
+	const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+	if (s.cap < bytes) {
+		if (s.p)
+			cudaFreeHost(s.p);
+		s.p   = nullptr;
+		s.cap = 0;
+		if (cudaHostAlloc(&s.p, bytes, cudaHostAllocDefault) != cudaSuccess)
+			return nullptr;
+		s.cap = bytes;
+	}
+	return static_cast<T*>(s.p);
+}
+
+double seconds_since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
 int cuda_fail(cudaError_t e, const char* where)
 {
 	return fail(e == cudaErrorMemoryAllocation ? DMRGPP_OOM : DMRGPP_CUDA_ERROR,
@@ -165,6 +202,9 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 	if (d->side != 0 && d->side != 1)
 		return fail(DMRGPP_INVALID_ARG, "side must be 0 (system) or 1 (environment)");
 	const size_t np = d->npatches, ng = d->ngroups, nt = d->ntargets;
+	const auto   t_start = Clock::now();
+	for (double& x : g_trunc_times)
+		x = 0.0;
 	// sector layout, group membership and sizes
 	std::vector<long long> xy(np + 1, 0);
 	for (size_t p = 0; p < np; ++p) {
@@ -310,11 +350,15 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 		if ((e = launch_grouped_dgemm(ga, bm, bm, st)))
 			return cuda_fail(e, "density-matrix GEMM launch");
 	}
-	std::vector<double> h_rho(rho_elems);
-	if ((e = cudaGetLastError()) || (e = cudaMemcpyAsync(h_rho.data(), rho, rho_elems * sizeof(double), cudaMemcpyDeviceToHost, st))
+	double* h_rho = pinned<double>(0, rho_elems);
+	if (!h_rho)
+		return fail(DMRGPP_OOM, "page-locked host buffer for the density matrices");
+	if ((e = cudaGetLastError()) || (e = cudaMemcpyAsync(h_rho, rho, rho_elems * sizeof(double), cudaMemcpyDeviceToHost, st))
 	    || (e = cudaStreamSynchronize(st)))
 		return cuda_fail(e, "density matrices");
 
+	g_trunc_times[DMRGPP_TRUNC_RHO] = seconds_since(t_start);
+	auto tp                         = Clock::now();
 	// eigenvalues of every group on the host cores (Householder reduction,
 	// QL without vectors)
 	std::vector<long long> eoff(ng + 1, 0);
@@ -336,7 +380,7 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 		if (n == 0)
 			return;
 		GroupEig& G = ge[g];
-		double*   a = h_rho.data() + goff[g];
+		double*   a = h_rho + goff[g];
 		for (int j = 0; j < n; ++j) // symmetrise the round-off of the two triangles
 			for (int i = 0; i < j; ++i) {
 				const double s = 0.5 * (a[i + (long long)j * n] + a[j + (long long)i * n]);
@@ -356,6 +400,8 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 		if (!ge[g].ok)
 			return fail(DMRGPP_NOT_CONVERGED, "eigensolver of group " + std::to_string(g) + " did not converge");
 
+	g_trunc_times[DMRGPP_TRUNC_EIGENVALUES] = seconds_since(tp);
+	tp                                      = Clock::now();
 	// rank every state (ascending eigenvalue, then group, then index) and keep K
 	std::vector<long long> order(N);
 	std::iota(order.begin(), order.end(), 0LL);
@@ -377,6 +423,8 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 		disc += std::fabs(sorted[q]);
 		--kept[group_of[size_t(order[q])]];
 	}
+	g_trunc_times[DMRGPP_TRUNC_SELECT] = seconds_since(tp);
+	tp                                 = Clock::now();
 	if (vectors) {
 		// the kept eigenvectors: inverse iteration on each tridiagonal (host
 		// cores), then V = Q Z on the device
@@ -384,7 +432,14 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 		for (size_t g = 0; g < ng; ++g)
 			koff[g + 1] = koff[g] + (long long)(d->group_size[g] * kept[g]);
 		const size_t        kelems = size_t(std::max<long long>(koff[ng], 1));
-		std::vector<double> zk(kelems), hv(rho_elems, 0.0), bt(size_t(std::max<long long>(eoff[ng], 1)), 0.0);
+		// the packed reflectors: every group with kept states copies its whole
+		// n x n block; the rest is never read
+		double* hv = pinned<double>(1, rho_elems);
+		double* zk = pinned<double>(2, kelems);
+		double* vo = pinned<double>(3, kelems);
+		if (!hv || !zk || !vo)
+			return fail(DMRGPP_OOM, "page-locked host buffers for the eigenvectors");
+		std::vector<double> bt(size_t(std::max<long long>(eoff[ng], 1)), 0.0);
 		parallel_for(ng, [&](size_t t) {
 			const size_t g = by_size[t];
 			const int    n = int(d->group_size[g]), k = int(kept[g]);
@@ -392,10 +447,12 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 				return;
 			const GroupEig& G = ge[g];
 			tridiag_eigenvectors(n, G.d.data(), G.off.data(), eigenvalues + eoff[g] + (n - k), k,
-			                     zk.data() + koff[g]);
-			std::copy(G.hv.begin(), G.hv.end(), hv.begin() + goff[g]);
+			                     zk + koff[g]);
+			std::copy(G.hv.begin(), G.hv.end(), hv + goff[g]);
 			std::copy(G.beta.begin(), G.beta.end(), bt.begin() + eoff[g]);
 		});
+		g_trunc_times[DMRGPP_TRUNC_VECTORS_HOST] = seconds_since(tp);
+		tp                                       = Clock::now();
 		std::vector<ColumnJob> cj;
 		for (size_t g = 0; g < ng; ++g)
 			for (int j = 0; j < int(kept[g]); ++j)
@@ -417,20 +474,33 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 			    || (e = dev_malloc(&d_hv, rho_elems * sizeof(double))) || (e = dev_malloc(&d_bt, bt.size() * sizeof(double)))
 			    || (e = dev_malloc(&d_cj, cj.size() * sizeof(ColumnJob))))
 				return cuda_fail(e, "eigenvector allocation");
-			if ((e = cudaMemcpyAsync(z, zk.data(), kelems * sizeof(double), cudaMemcpyHostToDevice, st))
-			    || (e = cudaMemcpyAsync(d_hv, hv.data(), rho_elems * sizeof(double), cudaMemcpyHostToDevice, st))
+			if ((e = cudaMemcpyAsync(z, zk, kelems * sizeof(double), cudaMemcpyHostToDevice, st))
+			    || (e = cudaMemcpyAsync(d_hv, hv, rho_elems * sizeof(double), cudaMemcpyHostToDevice, st))
 			    || (e = cudaMemcpyAsync(d_bt, bt.data(), bt.size() * sizeof(double), cudaMemcpyHostToDevice, st))
 			    || (e = cudaMemcpyAsync(d_cj, cj.data(), cj.size() * sizeof(ColumnJob), cudaMemcpyHostToDevice, st)))
 				return cuda_fail(e, "eigenvector set-up");
 			const int cgrid = int(std::min<size_t>((cj.size() + 7) / 8, 148 * 8));
 			k_back_transform<<<std::max(cgrid, 1), 256, 0, st>>>(z, v, d_hv, d_bt, d_cj, int(cj.size()));
 			if ((e = cudaGetLastError())
-			    || (e = cudaMemcpyAsync(vectors, v, size_t(koff[ng]) * sizeof(double), cudaMemcpyDeviceToHost, st))
+			    || (e = cudaMemcpyAsync(vo, v, size_t(koff[ng]) * sizeof(double), cudaMemcpyDeviceToHost, st))
 			    || (e = cudaStreamSynchronize(st)))
 				return cuda_fail(e, "eigenvectors");
+			std::copy(vo, vo + koff[ng], vectors);
 		}
 	}
-	*kept_total = K;
-	*discarded  = disc;
+	if (vectors)
+		g_trunc_times[DMRGPP_TRUNC_VECTORS_DEVICE] = seconds_since(tp);
+	g_trunc_times[DMRGPP_TRUNC_TOTAL] = seconds_since(t_start);
+	*kept_total                       = K;
+	*discarded                        = disc;
+	return DMRGPP_OK;
+}
+
+extern "C" int dmrgpp_density_profile(double* t, int n)
+{
+	if (!t || n < 0 || n > DMRGPP_TRUNC_NPHASES)
+		return dmrgpp::fail(DMRGPP_INVALID_ARG, "need 0 <= n <= DMRGPP_TRUNC_NPHASES and a buffer");
+	for (int i = 0; i < n; ++i)
+		t[i] = dmrgpp::g_trunc_times[i];
 	return DMRGPP_OK;
 }

@@ -67,3 +67,15 @@ def density_truncate(lsz: Sequence[int], rsz: Sequence[int], patch_group: Sequen
     return {"eigenvalues": evals, "vectors": evecs if vectors else None,
             "kept": kept.astype(np.int64), "kept_total": int(kt.value),
             "discarded": float(disc.value)}
+
+
+TRUNCATION_PHASES = ("rho", "eigenvalues", "select", "vectors_host", "vectors_device", "total")
+
+
+def truncation_profile() -> dict:
+    """Seconds of the phases of this thread's last density_truncate
+    (dmrgpp_density_profile)."""
+    n = len(TRUNCATION_PHASES)
+    t = (ctypes.c_double * n)()
+    _capi.check(_capi.lib().dmrgpp_density_profile(t, n))
+    return {k: float(v) for k, v in zip(TRUNCATION_PHASES, t)}

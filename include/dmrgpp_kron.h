@@ -556,6 +556,24 @@ int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, double toler
                             double* eigenvalues, double* vectors, size_t* kept, size_t* kept_total,
                             double* discarded);
 
+/* Wall-clock seconds of the phases of the calling thread's last
+ * dmrgpp_density_truncate (host clock, each phase waiting for its device
+ * work): RHO the density matrices (device, to the host), EIGENVALUES the
+ * tridiagonal reductions and eigenvalues (host cores), SELECT the ranking,
+ * VECTORS_HOST the inverse iterations and packing, VECTORS_DEVICE the
+ * back-transformation and copy out, TOTAL the whole call.  n (<=
+ * DMRGPP_TRUNC_NPHASES) values are written to t. */
+enum {
+	DMRGPP_TRUNC_RHO            = 0,
+	DMRGPP_TRUNC_EIGENVALUES    = 1,
+	DMRGPP_TRUNC_SELECT         = 2,
+	DMRGPP_TRUNC_VECTORS_HOST   = 3,
+	DMRGPP_TRUNC_VECTORS_DEVICE = 4,
+	DMRGPP_TRUNC_TOTAL          = 5,
+	DMRGPP_TRUNC_NPHASES        = 6
+};
+int dmrgpp_density_profile(double* t, int n);
+
 /* Last error message of a handle, or of the calling thread's last failed
  * create when h is NULL.  Never returns NULL. */
 const char* dmrgpp_kron_last_error(dmrgpp_kron_handle h);
