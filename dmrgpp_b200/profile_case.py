@@ -8,14 +8,17 @@ only the kernels of that workload.
     python -m dmrgpp_b200.profile_case ladder --states 4000 --solve lanczos
     python -m dmrgpp_b200.profile_case mlp --elements 300000 [--inference cuda_cores]
     python -m dmrgpp_b200.profile_case wft --states 4000
+    python -m dmrgpp_b200.profile_case truncation --states 16000
 
 Workloads: c2 = the 1024 x 1024-state, 21-group, K=5 microbench sector;
 ladder = the ladder-shaped (N_up, N_down) sector with `--states` left and
 right states (K = 10); mlp = learned-preconditioner applications (seeded
 network, seeded diagonal and residual of `--elements` entries); wft = the
 wave-function transformation of the ladder-shaped layout with seeded square
-N(0,1)/sqrt(n) blocks.  Prints one
-line "ok ..." at the end.
+N(0,1)/sqrt(n) blocks; truncation = the density-matrix truncation of the
+ladder-shaped layout's system block (one group per patch) for a seeded unit
+sector vector, a quarter of the states kept.  Prints one line "ok ..." at the
+end.
 """
 from __future__ import annotations
 
@@ -25,7 +28,7 @@ import sys
 
 def main(argv=None) -> int:
     p = argparse.ArgumentParser()
-    p.add_argument("workload", choices=["c2", "ladder", "mlp", "wft"])
+    p.add_argument("workload", choices=["c2", "ladder", "mlp", "wft", "truncation"])
     p.add_argument("--elements", type=int, default=300000, help="mlp: vector length")
     p.add_argument("--inference", default="tensor_cores", choices=["tensor_cores", "cuda_cores"])
     p.add_argument("--states", type=int, default=4000, help="ladder: left = right states")
@@ -74,6 +77,18 @@ def main(argv=None) -> int:
         torch.cuda.synchronize()
         print("ok", w.dim_in, w.flops, float(y.norm()))
         w.close()
+        return 0
+
+    if a.workload == "truncation":
+        import numpy as np
+        from .truncation import density_truncate
+        prob = sb.ladder_problem(total_states=a.states, sigma=2.5, seed=9)
+        l, r = prob.lsz, prob.rsz
+        psi = torch.from_numpy(sb.random_unit_vector(prob.dim)).cuda()
+        for _ in range(a.applies):
+            out = density_truncate(l, r, list(range(prob.npatches)), l, 0, psi, a.states // 4)
+        torch.cuda.synchronize()
+        print("ok", prob.dim, out["kept_total"], out["discarded"])
         return 0
 
     prob = (sb.c2_problem() if a.workload == "c2"
