@@ -46,6 +46,20 @@ class DensityDesc(ctypes.Structure):
                 ("device", ctypes.c_int)]
 
 
+class Crs(ctypes.Structure):
+    _fields_ = [("rows", _sz), ("rowptr", ctypes.POINTER(ctypes.c_int)),
+                ("colind", ctypes.POINTER(ctypes.c_int)), ("values", ctypes.POINTER(ctypes.c_double))]
+
+
+class KronCrsDesc(ctypes.Structure):
+    _fields_ = [("noperator", _sz), ("npatches", _sz), ("left_offset", _szp),
+                ("left_patch_size", _szp), ("right_offset", _szp), ("right_patch_size", _szp),
+                ("A", ctypes.POINTER(Crs)), ("B", ctypes.POINTER(Crs)),
+                ("value", ctypes.POINTER(ctypes.c_double)), ("fermion", ctypes.POINTER(ctypes.c_int)),
+                ("left_parity", ctypes.POINTER(ctypes.c_ubyte)), ("precision", ctypes.c_int),
+                ("stream", ctypes.c_void_p), ("device", ctypes.c_int)]
+
+
 class PlanInfo(ctypes.Structure):
     _fields_ = [("ntriples", _sz), ("dim", _sz), ("f_alg", ctypes.c_double),
                 ("operator_bytes", _sz), ("bx_bytes", _sz), ("pass1_tiles", _sz),
@@ -145,6 +159,8 @@ SIGNATURES.update({
                                                     ctypes.POINTER(ctypes.c_int),
                                                     ctypes.POINTER(DavidsonStats)]),
     "dmrgpp_mlp_last_error": (ctypes.c_char_p, [_vp]),
+    "dmrgpp_kron_create_crs": (ctypes.c_int, [ctypes.POINTER(KronCrsDesc),
+                                              ctypes.POINTER(ctypes.c_void_p)]),
     "dmrgpp_density_truncate": (ctypes.c_int, [ctypes.POINTER(DensityDesc), _sz, ctypes.c_double,
                                                _sz, _dp, _dp, _szp, _szp, _dp]),
     "dmrgpp_density_profile": (ctypes.c_int, [_dp, ctypes.c_int]),

@@ -500,6 +500,7 @@ double seconds_since(Clock::time_point t0)
 int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm, Clock::time_point t0,
                   dmrgpp_kron_handle* out)
 {
+	// (h->crs, when set, points at the caller's CRS operators until the upload)
 	if (device >= 0) {
 		h->device = device;
 	} else if (cudaGetDevice(&h->device) != cudaSuccess) {
@@ -565,8 +566,10 @@ int finish_create(dmrgpp_kron_handle h, int device, void* stream, int bm, Clock:
 	};
 	h->setup_times[DMRGPP_SETUP_ALLOC] = seconds_since(tp);
 	tp                                 = Clock::now();
-	if (int rc = dmrgpp::upload_operators(h, &h->setup_times[DMRGPP_SETUP_UPLOAD_FILL]))
+	if (int rc = h->crs ? dmrgpp::upload_operators_crs(h)
+	                    : dmrgpp::upload_operators(h, &h->setup_times[DMRGPP_SETUP_UPLOAD_FILL]))
 		return abandon(rc);
+	h->crs = nullptr;
 	h->setup_times[DMRGPP_SETUP_UPLOAD] = seconds_since(tp);
 	tp                                  = Clock::now();
 	if (int rc = dmrgpp::upload_diagonal(h))
@@ -678,6 +681,44 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 	}
 	h->sector_start                   = { 0, h->plan.dim() };
 	h->setup_times[DMRGPP_SETUP_PLAN] = seconds_since(t0);
+	return finish_create(h, d->device, d->stream, bm, t0, out);
+}
+
+int dmrgpp_kron_create_crs(const dmrgpp_kron_crs_desc* d, dmrgpp_kron_handle* out)
+{
+	if (!out)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "null output handle");
+	*out = nullptr;
+	if (!d)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "null descriptor");
+	if (d->precision != DMRGPP_FP64 && d->precision != DMRGPP_SPLIT_BF16 && d->precision != DMRGPP_TF32X3)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "unknown precision mode");
+	if (d->precision == DMRGPP_SPLIT_BF16)
+		return fail(nullptr, DMRGPP_NOT_SUPPORTED, "split-BF16 is not built into this library");
+	const auto                    t0 = Clock::now();
+	dmrgpp::CrsSource             src;
+	std::vector<dmrgpp::Triple>   triples;
+	std::vector<dmrgpp::BlockRef> blocks;
+	double                        f_alg = 0.0;
+	std::string                   msg   = dmrgpp::crs_triples(d, src, triples, blocks, f_alg);
+	if (!msg.empty())
+		return fail(nullptr, DMRGPP_INVALID_ARG, msg);
+	dmrgpp_kron_handle h = new (std::nothrow) dmrgpp_kron_s();
+	if (!h)
+		return fail(nullptr, DMRGPP_OOM, "host allocation failed");
+	h->precision = d->precision;
+	int bm, bn;
+	pick_tile_sizes(d->npatches, d->left_patch_size, d->right_patch_size, bm, bn);
+	msg = dmrgpp::build_kron_plan_triples(d->noperator, d->npatches, d->left_patch_size, d->right_patch_size,
+	                                      std::move(triples), std::move(blocks), f_alg, bm, bn, h->plan,
+	                                      nullptr);
+	if (!msg.empty()) {
+		delete h;
+		return fail(nullptr, DMRGPP_INVALID_ARG, msg);
+	}
+	h->sector_start                   = { 0, h->plan.dim() };
+	h->setup_times[DMRGPP_SETUP_PLAN] = seconds_since(t0);
+	h->crs                            = &src; // read by finish_create's upload only
 	return finish_create(h, d->device, d->stream, bm, t0, out);
 }
 

@@ -14,6 +14,21 @@ namespace dmrgpp {
 struct LanczosWork;  // device buffers of the eigensolvers, created on first use
 struct DavidsonWork;
 struct GroupWork;
+// The caller's CRS operators during dmrgpp_kron_create_crs (crs.cu), with the
+// host-side maps the device scatter needs.
+struct CrsSource {
+	const dmrgpp_kron_crs_desc* desc = nullptr;
+	std::vector<int> lpatch, lloc; // per left state: its patch (-1: none) and index in the group
+	std::vector<int> rpatch, rloc; // per right state
+	std::vector<int> tri_ptr;      // per (k, i) (k * np + i): range of tri_j / tri_t
+	std::vector<int> tri_j, tri_t; // contributing input patches j (ascending) and their triples
+};
+
+// Block-presence scan of the CRS operators: validates d, fills src and the
+// contributing (i, j, k) triples in (i, j, k) order with their algorithmic
+// flops, as collect_triples does for dense tables.  Returns "" or the reason.
+std::string crs_triples(const dmrgpp_kron_crs_desc* d, CrsSource& src, std::vector<Triple>& triples,
+                        std::vector<BlockRef>& blocks, double& f_alg);
 }
 
 struct dmrgpp_kron_s {
@@ -81,6 +96,7 @@ struct dmrgpp_kron_s {
 	double*             d_diag = nullptr; // diagonal of H (patch order)
 	dmrgpp::DavidsonWork* davidson = nullptr;
 	dmrgpp::GroupWork*  group = nullptr;   // group Lanczos buffers (group_lanczos.cu)
+	const dmrgpp::CrsSource* crs = nullptr; // create time only: build the blocks from CRS operators
 	std::string         err;
 };
 
@@ -118,6 +134,10 @@ void mixed_host_plan(dmrgpp_kron_handle h, int sms, MixedHost& out);
 // Uploads the TF32x3 form planned in host (create time only, after the FP64
 // operators are on the device).
 int build_mixed(dmrgpp_kron_handle h, MixedHost& host);
+
+// Writes the packed operators of a handle made by dmrgpp_kron_create_crs from
+// h->crs (crs.cu), in place of upload_operators.
+int upload_operators_crs(dmrgpp_kron_handle h);
 
 // (Re)builds and uploads the persistent schedule of h for tile configuration
 // cfg (0..kNumTileCfgs-1), aiming at items_per_cta work items per CTA.

@@ -120,6 +120,70 @@ class BatchedGemm:
         return cls(prob.noperator, prob.npatches, prob.lsz, prob.rsz, A, ldA, B, ldB, **kw)
 
     @classmethod
+    def from_crs(cls, left_offset, left_size, right_offset, right_size, A, B, value=None,
+                 fermion=None, left_parity=None, precision: int = FP64,
+                 stream: Optional[int] = None, device: int = -1) -> "BatchedGemm":
+        """A sector built on the device from its CRS operators
+        (dmrgpp_kron_create_crs): A and B are lists (one per term) of
+        scipy.sparse CSR matrices or (indptr, indices, data) triples over the
+        left and right bases; value (per-term factor on A), fermion (per-term
+        flag) and left_parity (per left state) as in calculateAhat."""
+        L = _capi.lib()
+        keep = []
+
+        def crs(m):
+            if hasattr(m, "indptr"):
+                ip, ix, dv, rows = m.indptr, m.indices, m.data, m.shape[0]
+            else:
+                ip, ix, dv = m
+                rows = len(ip) - 1
+            ip = np.ascontiguousarray(ip, dtype=np.int32)
+            ix = np.ascontiguousarray(ix, dtype=np.int32)
+            dv = np.ascontiguousarray(dv, dtype=np.float64)
+            keep.extend([ip, ix, dv])
+            return _capi.Crs(rows, ip.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                             ix.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                             dv.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+
+        K = len(A)
+        Ac = (_capi.Crs * K)(*[crs(m) for m in A])
+        Bc = (_capi.Crs * K)(*[crs(m) for m in B])
+        arrs = [_size_array(x) for x in (left_offset, left_size, right_offset, right_size)]
+        d = _capi.KronCrsDesc()
+        szp = ctypes.POINTER(ctypes.c_size_t)
+        d.noperator, d.npatches = K, len(arrs[1])
+        d.left_offset, d.left_patch_size, d.right_offset, d.right_patch_size = \
+            [a.ctypes.data_as(szp) for a in arrs]
+        d.A, d.B = Ac, Bc
+        vals = fer = par = None
+        if value is not None:
+            vals = np.ascontiguousarray(value, dtype=np.float64)
+            d.value = vals.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        if fermion is not None:
+            fer = np.ascontiguousarray(fermion, dtype=np.int32)
+            d.fermion = fer.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        if left_parity is not None:
+            par = np.ascontiguousarray(left_parity, dtype=np.uint8)
+            d.left_parity = par.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte))
+        d.precision, d.stream, d.device = precision, stream, device
+        h = ctypes.c_void_p()
+        t0 = time.perf_counter()
+        rc = L.dmrgpp_kron_create_crs(ctypes.byref(d), ctypes.byref(h))
+        create_seconds = time.perf_counter() - t0
+        _capi.check(rc)
+        self = cls.__new__(cls)
+        self._h, self._lib = h, L
+        self.is_complex = False
+        self.create_seconds = create_seconds
+        n = ctypes.c_size_t()
+        _capi.check(L.dmrgpp_kron_dim(h, ctypes.byref(n)), h)
+        self.dim = int(n.value)
+        f = ctypes.c_double()
+        _capi.check(L.dmrgpp_kron_flops(h, ctypes.byref(f)), h)
+        self.f_alg = float(f.value)
+        return self
+
+    @classmethod
     def from_problems(cls, probs, precision: int = FP64, stream: Optional[int] = None,
                       device: int = -1) -> "BatchedGemm":
         """Many independent sectors in one handle (dmrgpp_kron_create_group):

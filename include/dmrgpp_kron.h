@@ -85,6 +85,47 @@ typedef struct {
  * the device and builds the launch schedule. */
 int dmrgpp_kron_create(const dmrgpp_kron_desc* desc, dmrgpp_kron_handle* out);
 
+/* ---- Building the block tables on the device from the CRS operators ----
+ * The reference's InitKron set-up: each connection's left operator A and
+ * right operator B are CRS matrices over the left and right block bases
+ * (PsimagLite::CrsMatrix, 0-based rowptr / colind / values);
+ * InitKronBase::calculateAhat (InitKronBase.h:393-413) forms
+ * Ahat(a,:) = A(a,:) * sign * value with sign = -1 for a fermionic term on a
+ * left state of odd parity, and ArrayOfMatStruct (ArrayOfMatStruct.h:105-448)
+ * slices Ahat and B into the per-patch blocks A_k(i,j) (rows of patch i's
+ * left group, columns of patch j's) and B_k(i,j) (right groups), which the
+ * batched path densifies (BatchedGemmKokkos.h:354-370).  Here the CRS arrays
+ * go to the device as they are and a scatter kernel writes every entry into
+ * the handle's packed blocks; only the block-presence scan (which blocks hold
+ * a nonzero) runs on the host.  The handle is the one dmrgpp_kron_create
+ * builds from the same blocks as dense tables, bit for bit. */
+typedef struct {
+	size_t        rows;   /* square operator: rows x rows */
+	const int*    rowptr; /* rows + 1, rowptr[0] = 0 */
+	const int*    colind; /* rowptr[rows] entries, each in [0, rows), no repeats within a row */
+	const double* values;
+} dmrgpp_crs;
+
+typedef struct {
+	size_t               noperator;        /* Kronecker terms k */
+	size_t               npatches;
+	const size_t*        left_offset;      /* per patch: first state of its left group in the left basis */
+	const size_t*        left_patch_size;
+	const size_t*        right_offset;     /* per patch: first state of its right group */
+	const size_t*        right_patch_size;
+	const dmrgpp_crs*    A;                /* noperator left-basis operators (all the same rows) */
+	const dmrgpp_crs*    B;                /* noperator right-basis operators */
+	const double*        value;            /* per term: the factor on A (NULL: 1) */
+	const int*           fermion;          /* per term: 1 = sign by the left state's parity (NULL: none) */
+	const unsigned char* left_parity;      /* per left state: 1 = odd (needed when a term is fermionic) */
+	int                  precision;
+	void*                stream;
+	int                  device;
+} dmrgpp_kron_crs_desc;
+
+/* The patches' left groups (and right groups) must not overlap. */
+int dmrgpp_kron_create_crs(const dmrgpp_kron_crs_desc* desc, dmrgpp_kron_handle* out);
+
 /* Many independent sectors in one handle (no counterpart in the reference,
  * whose plugin holds one sector): sector s keeps its own tables (descs[s],
  * all with the same precision, device and stream), its patches follow those
