@@ -138,6 +138,64 @@ __global__ void __launch_bounds__(256) k_scatter_crs(const ScatterArgs s)
 	}
 }
 
+// Host arrays to the device through two page-locked buffers of the calling
+// thread (kept between creates): the host cores copy one buffer's worth while
+// the other crosses PCIe, so the copies run at the page-locked transfer rate
+// instead of the pageable one.
+struct Stager {
+	static constexpr size_t kBytes = size_t(32) << 20;
+	unsigned char*          buf[2] = {};
+	cudaEvent_t             ev[2]  = {};
+	bool                    used[2] = {};
+	int                     slot   = 0;
+	~Stager()
+	{
+		for (int s = 0; s < 2; ++s) {
+			if (buf[s])
+				cudaFreeHost(buf[s]);
+			if (ev[s])
+				cudaEventDestroy(ev[s]);
+		}
+	}
+	cudaError_t ready()
+	{
+		cudaError_t e = cudaSuccess;
+		for (int s = 0; s < 2 && !e; ++s) {
+			if (!buf[s])
+				e = cudaHostAlloc(reinterpret_cast<void**>(&buf[s]), kBytes, cudaHostAllocDefault);
+			if (!e && !ev[s])
+				e = cudaEventCreateWithFlags(&ev[s], cudaEventDisableTiming);
+		}
+		return e;
+	}
+	cudaError_t copy(void* dst, const void* src, size_t bytes, cudaStream_t st)
+	{
+		// small arrays: one pageable copy costs less than a staging round
+		if (bytes < (size_t(8) << 20))
+			return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+		cudaError_t e;
+		for (size_t o = 0; o < bytes; o += kBytes) {
+			const size_t n = std::min(kBytes, bytes - o);
+			if (used[slot] && (e = cudaEventSynchronize(ev[slot])))
+				return e;
+			const size_t piece = size_t(1) << 20;
+			unsigned char* b   = buf[slot];
+			const unsigned char* s = static_cast<const unsigned char*>(src) + o;
+			parallel_for((n + piece - 1) / piece, [&](size_t q) {
+				std::memcpy(b + q * piece, s + q * piece, std::min(piece, n - q * piece));
+			});
+			if ((e = cudaMemcpyAsync(static_cast<unsigned char*>(dst) + o, b, n, cudaMemcpyHostToDevice, st))
+			    || (e = cudaEventRecord(ev[slot], st)))
+				return e;
+			used[slot] = true;
+			slot ^= 1;
+		}
+		return cudaSuccess;
+	}
+};
+
+thread_local Stager g_stager;
+
 } // namespace
 
 std::string crs_triples(const dmrgpp_kron_crs_desc* d, CrsSource& src, std::vector<Triple>& triples,
@@ -224,17 +282,25 @@ int upload_operators_crs(dmrgpp_kron_handle h)
 		ld_b[t]          = int(P.M[size_t(tr.j)]);
 	}
 	const size_t K = d->noperator, nL = src.lpatch.size(), nR = src.rpatch.size();
-	size_t       max_nnz = 1, max_rows = 1;
-	for (size_t k = 0; k < K; ++k) {
-		max_nnz  = std::max({ max_nnz, size_t(d->A[k].rowptr[nL]), size_t(d->B[k].rowptr[nR]) });
-		max_rows = std::max({ max_rows, nL + 1, nR + 1 });
-	}
-	// one device buffer for the maps and lists, one for a term's CRS arrays
+	// every term's CRS arrays in one device buffer (16-byte aligned pieces)
+	auto al = [](size_t b) { return (b + 15) / 16 * 16; };
+	std::vector<size_t> crs_off(6 * K + 1, 0);
+	for (size_t k = 0; k < K; ++k)
+		for (int side = 0; side < 2; ++side) {
+			const dmrgpp_crs& m    = side == 0 ? d->A[k] : d->B[k];
+			const size_t      rows = side == 0 ? nL : nR;
+			const size_t      nnz  = size_t(m.rowptr[rows]);
+			const size_t      q    = 6 * k + 3 * size_t(side);
+			crs_off[q + 1]         = crs_off[q] + al((rows + 1) * sizeof(int));
+			crs_off[q + 2]         = crs_off[q + 1] + al(nnz * sizeof(int));
+			crs_off[q + 3]         = crs_off[q + 2] + al(nnz * sizeof(double));
+		}
+	// one device buffer for the maps and lists
 	std::vector<unsigned char> blob;
 	std::vector<size_t>        offs;
 	auto add = [&](const void* p, size_t bytes) {
 		offs.push_back(blob.size());
-		blob.resize(blob.size() + (bytes + 15) / 16 * 16);
+		blob.resize(blob.size() + al(bytes));
 		if (bytes)
 			std::memcpy(blob.data() + offs.back(), p, bytes);
 	};
@@ -261,29 +327,29 @@ int upload_operators_crs(dmrgpp_kron_handle h)
 			dev_free(*b);
 		}
 	} release { &d_blob, &d_crs };
-	const size_t crs_bytes = (max_rows * sizeof(int) + 15) / 16 * 16 + (max_nnz * sizeof(int) + 15) / 16 * 16
-	    + max_nnz * sizeof(double);
 	cudaError_t e;
-	if ((e = dev_malloc(&d_blob, std::max<size_t>(blob.size(), 16))) || (e = dev_malloc(&d_crs, crs_bytes)))
-		return fail_cuda(e, "device allocation (CRS set-up)");
+	if ((e = dev_malloc(&d_blob, std::max<size_t>(blob.size(), 16)))
+	    || (e = dev_malloc(&d_crs, std::max<size_t>(crs_off[6 * K], 16))) || (e = g_stager.ready()))
+		return fail_cuda(e, "allocation (CRS set-up)");
 	if ((e = cudaMemsetAsync(h->d_ops, 0, size_t(std::max<long long>(P.op_elems, 1)) * sizeof(double), st))
 	    || (e = cudaMemcpyAsync(d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, st)))
 		return fail_cuda(e, "CRS set-up copies");
+	if (P.triples.empty())
+		return cudaStreamSynchronize(st) == cudaSuccess ? DMRGPP_OK
+		                                                : handle_fail(h, DMRGPP_CUDA_ERROR, "CRS set-up");
 	auto at = [&](int q) { return d_blob + offs[size_t(q)]; };
-	int*    d_rowptr = reinterpret_cast<int*>(d_crs);
-	int*    d_col    = reinterpret_cast<int*>(d_crs + (max_rows * sizeof(int) + 15) / 16 * 16);
-	double* d_val    = reinterpret_cast<double*>(d_crs + (max_rows * sizeof(int) + 15) / 16 * 16
-	                                             + (max_nnz * sizeof(int) + 15) / 16 * 16);
 	for (size_t k = 0; k < K; ++k)
 		for (int side = 0; side < 2; ++side) {
 			const dmrgpp_crs& m    = side == 0 ? d->A[k] : d->B[k];
 			const size_t      rows = side == 0 ? nL : nR;
 			const size_t      nnz  = size_t(m.rowptr[rows]);
-			if (P.triples.empty())
-				continue;
-			if ((e = cudaMemcpyAsync(d_rowptr, m.rowptr, (rows + 1) * sizeof(int), cudaMemcpyHostToDevice, st))
-			    || (nnz && (e = cudaMemcpyAsync(d_col, m.colind, nnz * sizeof(int), cudaMemcpyHostToDevice, st)))
-			    || (nnz && (e = cudaMemcpyAsync(d_val, m.values, nnz * sizeof(double), cudaMemcpyHostToDevice, st))))
+			const size_t      q    = 6 * k + 3 * size_t(side);
+			int*              d_rowptr = reinterpret_cast<int*>(d_crs + crs_off[q]);
+			int*              d_col    = reinterpret_cast<int*>(d_crs + crs_off[q + 1]);
+			double*           d_val    = reinterpret_cast<double*>(d_crs + crs_off[q + 2]);
+			if ((e = g_stager.copy(d_rowptr, m.rowptr, (rows + 1) * sizeof(int), st))
+			    || (nnz && (e = g_stager.copy(d_col, m.colind, nnz * sizeof(int), st)))
+			    || (nnz && (e = g_stager.copy(d_val, m.values, nnz * sizeof(double), st))))
 				return fail_cuda(e, "CRS copy");
 			ScatterArgs s {};
 			s.rowptr    = d_rowptr;
@@ -306,7 +372,6 @@ int upload_operators_crs(dmrgpp_kron_handle h)
 			s.ops       = h->d_ops;
 			const int grid = int(std::min<size_t>((rows + 7) / 8, 148 * 16));
 			k_scatter_crs<<<std::max(grid, 1), 256, 0, st>>>(s);
-			// the next term's copies into the same buffers follow in stream order
 			if ((e = cudaGetLastError()))
 				return fail_cuda(e, "CRS scatter launch");
 		}
