@@ -374,9 +374,8 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 	std::iota(by_size.begin(), by_size.end(), size_t(0));
 	std::stable_sort(by_size.begin(), by_size.end(),
 	                 [&](size_t x, size_t y) { return d->group_size[x] > d->group_size[y]; });
-	parallel_for(ng, [&](size_t t) {
-		const size_t g = by_size[t];
-		const int    n = int(d->group_size[g]);
+	auto eig_group = [&](size_t g, int threads) {
+		const int n = int(d->group_size[g]);
 		if (n == 0)
 			return;
 		GroupEig& G = ge[g];
@@ -390,12 +389,20 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 			G.d.assign(1, a[0]);
 			G.off.assign(1, 0.0);
 		} else {
-			householder_tridiag(n, a, G.d, G.off, G.hv, G.beta);
+			householder_tridiag_parallel(n, a, G.d, G.off, G.hv, G.beta, threads);
 		}
 		double* w = eigenvalues + eoff[g];
 		std::copy(G.d.begin(), G.d.end(), w);
 		G.ok = tridiag_eigen(n, w, G.off.data(), nullptr); // ascending
-	});
+	};
+	// the largest group, when big, first on all host cores (a team sharing
+	// each Householder step), then the others one per core; running the team
+	// beside the others oversubscribed the cores and was slower
+	const int    hw    = int(std::max(2u, std::thread::hardware_concurrency()));
+	const size_t first = d->group_size[by_size[0]] >= 256 ? 1 : 0;
+	if (first)
+		eig_group(by_size[0], hw);
+	parallel_for(ng - first, [&](size_t t) { eig_group(by_size[t + first], 1); });
 	for (size_t g = 0; g < ng; ++g)
 		if (!ge[g].ok)
 			return fail(DMRGPP_NOT_CONVERGED, "eigensolver of group " + std::to_string(g) + " did not converge");

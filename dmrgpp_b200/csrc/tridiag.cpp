@@ -15,6 +15,8 @@
 #include <cstdint>
 #include <numeric>
 #include <random>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 namespace dmrgpp {
@@ -416,6 +418,179 @@ void householder_tridiag(int n, const double* a, std::vector<double>& d, std::ve
 	}
 	if (pending) { // the last update reaches the trailing 2 x 2 block
 		const int k0 = n - 2; // hprev index 0 is row n - 2
+		for (int j = 0; j < 2; ++j)
+			for (int i = j; i < 2; ++i)
+				M(k0 + i, k0 + j) -= hprev[size_t(i)] * qprev[size_t(j)] + qprev[size_t(i)] * hprev[size_t(j)];
+	}
+	d[N - 2]   = M(n - 2, n - 2);
+	d[N - 1]   = M(n - 1, n - 1);
+	off[N - 2] = M(n - 1, n - 2);
+}
+
+namespace {
+
+// A sense-reversing spin barrier for a fixed team of threads (the parallel
+// reduction below synchronises three times per Householder step, too often
+// for a condition variable).
+class SpinBarrier {
+public:
+	explicit SpinBarrier(int n)
+	    : n_(n)
+	{
+	}
+	void wait()
+	{
+		const int gen = gen_.load(std::memory_order_acquire);
+		if (count_.fetch_add(1, std::memory_order_acq_rel) == n_ - 1) {
+			count_.store(0, std::memory_order_relaxed);
+			gen_.store(gen + 1, std::memory_order_release);
+			return;
+		}
+		while (gen_.load(std::memory_order_acquire) == gen)
+			std::this_thread::yield();
+	}
+
+private:
+	const int        n_;
+	std::atomic<int> count_ { 0 };
+	std::atomic<int> gen_ { 0 };
+};
+
+} // namespace
+
+void householder_tridiag_parallel(int n, const double* a, std::vector<double>& d, std::vector<double>& off,
+                                  std::vector<double>& hv, std::vector<double>& beta, int threads)
+{
+	if (threads < 2 || n < 64) {
+		householder_tridiag(n, a, d, off, hv, beta);
+		return;
+	}
+	// householder_tridiag's one-pass scheme with the pass over the lower
+	// triangle split by columns into equal areas; each thread accumulates its
+	// own part of p, and the parts are summed in thread order
+	const size_t                     N = size_t(n);
+	const int                        T = threads;
+	std::vector<double>              m(a, a + N * N), p(N), hprev(N), qprev(N);
+	std::vector<std::vector<double>> part(static_cast<size_t>(T), std::vector<double>(N));
+	d.assign(N, 0.0);
+	off.assign(N - 1, 0.0);
+	hv.assign(N * N, 0.0);
+	beta.assign(N, 0.0);
+	auto        M       = [&](int i, int j) -> double& { return m[size_t(i) + size_t(j) * N]; };
+	bool        pending = false;
+	double      b       = 0.0;
+	SpinBarrier bar(T);
+	// thread 0, between passes: the end of step k - 1 (its update vectors)
+	// and the start of step k (column k brought up to date, reflector k)
+	auto serial = [&](int k) {
+		const int len = n - k - 1;
+		if (pending) {
+			const double hk = hprev[0], qk = qprev[0];
+			for (int i = 0; i <= len; ++i)
+				M(k + i, k) -= hprev[size_t(i)] * qk + qprev[size_t(i)] * hk;
+		}
+		double* h     = hv.data() + size_t(k) * N;
+		double  sigma = 0.0;
+		for (int i = 1; i < len; ++i)
+			sigma += M(k + 1 + i, k) * M(k + 1 + i, k);
+		const double x0 = M(k + 1, k);
+		d[size_t(k)]    = M(k, k);
+		b               = 0.0;
+		if (sigma == 0.0) {
+			off[size_t(k)] = x0;
+		} else {
+			const double mu = std::sqrt(x0 * x0 + sigma);
+			const double h0 = x0 <= 0.0 ? x0 - mu : -sigma / (x0 + mu);
+			b               = 2.0 * h0 * h0 / (sigma + h0 * h0);
+			beta[size_t(k)] = b;
+			h[0]            = 1.0;
+			for (int i = 1; i < len; ++i)
+				h[i] = M(k + 1 + i, k) / h0;
+			off[size_t(k)] = mu;
+		}
+	};
+	auto finish_step = [&](int k) { // thread 0, after the reduction of p
+		const int     len = n - k - 1;
+		const double* h   = hv.data() + size_t(k) * N;
+		const bool    had = pending;
+		pending           = b != 0.0;
+		if (!pending)
+			return had;
+		double ph = 0.0;
+		for (int i = 0; i < len; ++i) {
+			p[size_t(i)] *= b;
+			ph += p[size_t(i)] * h[i];
+		}
+		for (int i = 0; i < len; ++i) {
+			qprev[size_t(i)] = p[size_t(i)] - 0.5 * b * ph * h[i];
+			hprev[size_t(i)] = h[i];
+		}
+		return had;
+	};
+	auto worker = [&](int t) {
+		for (int k = 0; k + 2 < n; ++k) {
+			if (t == 0)
+				serial(k);
+			bar.wait();
+			const int     len = n - k - 1;
+			const double* h   = hv.data() + size_t(k) * N;
+			const double* hp  = hprev.data() + 1;
+			const double* qp  = qprev.data() + 1;
+			// columns [c0, c1) of the trailing block: equal shares of its
+			// lower-triangle area len (len + 1) / 2
+			auto col_of = [&](int share) {
+				if (share <= 0)
+					return 0;
+				if (share >= T)
+					return len;
+				const double target = double(share) / T * 0.5 * double(len) * double(len + 1);
+				// area of columns [0, c) is c * len - c (c - 1) / 2
+				const double L  = double(len) + 0.5;
+				const double c  = L - std::sqrt(std::max(0.0, L * L - 2.0 * target));
+				return std::min(len, std::max(0, int(c)));
+			};
+			const int c0 = col_of(t), c1 = col_of(t + 1);
+			double*   pt = part[size_t(t)].data();
+			std::fill(pt, pt + len, 0.0);
+			for (int j = c0; j < c1; ++j) {
+				double* col = &M(k + 1, k + 1 + j);
+				if (pending) {
+					const double hj = hp[j], qj = qp[j];
+					for (int i = j; i < len; ++i)
+						col[i] -= hp[i] * qj + qp[i] * hj;
+				}
+				if (b != 0.0) {
+					const double hj = h[j];
+					double       pj = col[j] * hj;
+					for (int i = j + 1; i < len; ++i) {
+						pj += col[i] * h[i];
+						pt[i] += col[i] * hj;
+					}
+					pt[j] += pj;
+				}
+			}
+			bar.wait();
+			// p = sum of the parts, rows split among the threads
+			const int r0 = int((long long)len * t / T), r1 = int((long long)len * (t + 1) / T);
+			for (int i = r0; i < r1; ++i) {
+				double sum = 0.0;
+				for (int q = 0; q < T; ++q)
+					sum += part[size_t(q)][size_t(i)];
+				p[size_t(i)] = sum;
+			}
+			bar.wait();
+			if (t == 0)
+				finish_step(k);
+		}
+	};
+	std::vector<std::thread> team;
+	for (int t = 1; t < T; ++t)
+		team.emplace_back(worker, t);
+	worker(0);
+	for (std::thread& th : team)
+		th.join();
+	if (pending) { // the last update reaches the trailing 2 x 2 block
+		const int k0 = n - 2;
 		for (int j = 0; j < 2; ++j)
 			for (int i = j; i < 2; ++i)
 				M(k0 + i, k0 + j) -= hprev[size_t(i)] * qprev[size_t(j)] + qprev[size_t(i)] * hprev[size_t(j)];

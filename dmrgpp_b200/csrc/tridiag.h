@@ -26,6 +26,12 @@ void tridiag_eigenvectors(int n, const double* d, const double* off, const doubl
 void householder_tridiag(int n, const double* a, std::vector<double>& d, std::vector<double>& off,
                          std::vector<double>& hv, std::vector<double>& beta);
 
+// The same reduction by a team of `threads` host threads (the caller's
+// thread included; below 64 rows or 2 threads, householder_tridiag).  The
+// sums of the threads' parts make its rounding depend on the thread count.
+void householder_tridiag_parallel(int n, const double* a, std::vector<double>& d, std::vector<double>& off,
+                                  std::vector<double>& hv, std::vector<double>& beta, int threads);
+
 // v (n x ncols, column-major) <- Q v for the reflectors of householder_tridiag.
 void apply_q(int n, const std::vector<double>& hv, const std::vector<double>& beta, double* v, int ncols);
 

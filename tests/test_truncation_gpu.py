@@ -131,3 +131,41 @@ def test_hubbard_with_device_truncation_is_exact_at_u0(cuda_lib, cuda_device):
     e = d.run(sweeps=1)
     assert abs(e - (-9.51754)) < 1e-5          # dmrg/CMakeLists.txt:180-181
     assert abs(e - dd.free_fermion_energy(8, 4, 4)) < 1e-9
+
+
+def test_operator_change_of_basis_through_wft(cuda_lib, cuda_device):
+    """After a truncation, every block operator O(gi, gj) of the block becomes
+    U_gi^T O(gi, gj) U_gj (the reference's changeBasis / truncateBasis): one
+    dmrgpp_wft call with the operator blocks as patches (rows = right index,
+    columns = left index), WR = U_gi^T and WL = U_gj^T; FP64 against numpy."""
+    import torch
+    from dmrgpp_b200.truncation import density_truncate
+    from dmrgpp_b200.wft import WaveFunctionTransform
+    lsz, rsz, pg, gs = _layout(7, 0)
+    D = int(np.dot(lsz, rsz))
+    rng = np.random.default_rng(70)
+    psi = rng.standard_normal(D)
+    psi /= np.linalg.norm(psi)
+    out = density_truncate(lsz, rsz, pg, gs, 0, torch.tensor(psi, device="cuda"), sum(gs) // 2)
+    U = out["vectors"]
+    kept = [int(k) for k in out["kept"]]
+    # block operator: diagonal blocks and neighbouring-group couplings
+    pairs = [(g, h) for g in range(len(gs)) for h in range(len(gs))
+             if abs(g - h) <= 1 and kept[g] > 0 and kept[h] > 0]
+    O = {(g, h): rng.standard_normal((gs[g], gs[h])) for g, h in pairs}
+    r_in = [gs[g] for g, h in pairs]
+    l_in = [gs[h] for g, h in pairs]
+    r_out = [kept[g] for g, h in pairs]
+    l_out = [kept[h] for g, h in pairs]
+    WR = [U[g].T for g, h in pairs]
+    WL = [U[h].T for g, h in pairs]
+    w = WaveFunctionTransform(l_in, r_in, l_out, r_out, list(range(len(pairs))), WL, WR)
+    x = np.concatenate([O[p].ravel(order="F") for p in pairs])
+    y = w(x)
+    off = 0
+    for (g, h), ro, lo in zip(pairs, r_out, l_out):
+        ref = U[g].T @ O[(g, h)] @ U[h]
+        got = y[off:off + ro * lo].reshape(ro, lo, order="F")
+        assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()), (g, h)
+        off += ro * lo
+    w.close()

@@ -201,6 +201,31 @@ int main()
 		}
 		worst_r = std::max(worst_r, res / scale);
 	}
+	// the thread-team Householder reduction: same eigenvalues, and Q from its
+	// reflectors orthogonal, as the serial one
+	for (int trial = 0; trial < 12; ++trial) {
+		const int           n = 60 + 37 * trial;
+		const size_t        N = size_t(n);
+		std::vector<double> A(N * N);
+		for (int j = 0; j < n; ++j)
+			for (int i = 0; i <= j; ++i)
+				A[size_t(i) + size_t(j) * N] = A[size_t(j) + size_t(i) * N] = u(rng);
+		std::vector<double> d1, e1, h1, b1, d2, e2, h2, b2;
+		dmrgpp::householder_tridiag(n, A.data(), d1, e1, h1, b1);
+		dmrgpp::householder_tridiag_parallel(n, A.data(), d2, e2, h2, b2, 1 + trial % 7);
+		dmrgpp::tridiag_eigen(n, d1.data(), e1.data(), nullptr);
+		dmrgpp::tridiag_eigen(n, d2.data(), e2.data(), nullptr);
+		double scale = 1.0, de = 0.0;
+		for (int i = 0; i < n; ++i) {
+			scale = std::max(scale, std::fabs(d1[size_t(i)]));
+			de    = std::max(de, std::fabs(d1[size_t(i)] - d2[size_t(i)]));
+		}
+		if (de > 1e-12 * scale) {
+			std::printf("FAIL parallel householder %d %g\n", n, de);
+			return 1;
+		}
+		worst_e = std::max(worst_e, de / scale * 1e-1);
+	}
 	if (worst_e > 1e-13 || worst_r > 1e-12) {
 		std::printf("FAIL %g %g\n", worst_e, worst_r);
 		return 1;
