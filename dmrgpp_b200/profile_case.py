@@ -9,6 +9,7 @@ only the kernels of that workload.
     python -m dmrgpp_b200.profile_case mlp --elements 300000 [--inference cuda_cores]
     python -m dmrgpp_b200.profile_case wft --states 4000
     python -m dmrgpp_b200.profile_case truncation --states 16000
+    python -m dmrgpp_b200.profile_case serving --problems 256
 
 Workloads: c2 = the 1024 x 1024-state, 21-group, K=5 microbench sector;
 ladder = the ladder-shaped (N_up, N_down) sector with `--states` left and
@@ -18,7 +19,9 @@ wave-function transformation of the ladder-shaped layout with seeded square
 N(0,1)/sqrt(n) blocks; truncation = the density-matrix truncation of the
 ladder-shaped layout's system block (one group per patch) for a seeded unit
 sector vector, a quarter of the states kept.  Prints one line "ok ..." at the
-end.
+end.  serving = the serving-style batch (superblock.serving_batch) in one TF32x3
+group handle, solved once as the bench does: group Lanczos to a Ritz-value
+change of 1e-5, then the lockstep FP64 group refinement.
 """
 from __future__ import annotations
 
@@ -28,7 +31,8 @@ import sys
 
 def main(argv=None) -> int:
     p = argparse.ArgumentParser()
-    p.add_argument("workload", choices=["c2", "ladder", "mlp", "wft", "truncation"])
+    p.add_argument("workload", choices=["c2", "ladder", "mlp", "wft", "truncation", "serving"])
+    p.add_argument("--problems", type=int, default=256, help="serving: problems in the batch")
     p.add_argument("--elements", type=int, default=300000, help="mlp: vector length")
     p.add_argument("--inference", default="tensor_cores", choices=["tensor_cores", "cuda_cores"])
     p.add_argument("--states", type=int, default=4000, help="ladder: left = right states")
@@ -77,6 +81,19 @@ def main(argv=None) -> int:
         torch.cuda.synchronize()
         print("ok", w.dim_in, w.flops, float(y.norm()))
         w.close()
+        return 0
+
+    if a.workload == "serving":
+        import numpy as np
+        probs, _ = sb.serving_batch(a.problems)
+        bg = plugin.BatchedGemm.from_problems(probs, precision=plugin.TF32X3)
+        init = torch.from_numpy(np.random.default_rng(1).standard_normal(bg.dim)).cuda()
+        _, z, steps = bg.lanczos_lowest_group(init, steps=200, tolerance=1e-5)
+        e, conv, st = bg.refine_lowest_group(z, max_outer=10, tolerance=1e-10, inner_iterations=80,
+                                             inner_tolerance=1e-2, raise_on_no_convergence=False)
+        torch.cuda.synchronize()
+        print("ok", bg.dim, int(steps.max()), int(conv.sum()), st["inner_matvecs"])
+        bg.close()
         return 0
 
     if a.workload == "truncation":
