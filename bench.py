@@ -361,7 +361,8 @@ def serving_measurements(torch, dev, stream, cpu_sample: bool = True):
     def mixed_solve():
         t0 = time.perf_counter()
         _, zm, steps_m = bgm.lanczos_lowest_group(init, steps=200,
-                                                  tolerance=SERVING_MIXED_TOLERANCE)
+                                                  tolerance=SERVING_MIXED_TOLERANCE,
+                                                  reortho=False)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         em, conv, st = bgm.refine_lowest_group(zm, max_outer=10, tolerance=1e-10,
@@ -400,7 +401,8 @@ def serving_measurements(torch, dev, stream, cpu_sample: bool = True):
         "tf32x3_group_matvecs_in_refinement": int(st["inner_matvecs"]),
         "max_abs_dE_per_site_vs_single_fp64": float((np.abs(em - es) / sites).max()),
         "max_one_minus_overlap_vs_single_fp64": float(max(ovl)),
-        "note": f"TF32x3 group Lanczos to a Ritz-value change of {SERVING_MIXED_TOLERANCE:g}, then "
+        "note": f"TF32x3 group Lanczos (no reorthogonalisation: it only supplies the start "
+                f"vectors) to a Ritz-value change of {SERVING_MIXED_TOLERANCE:g}, then "
                 "dmrgpp_refine_lowest_group (FP64 Rayleigh quotients and residuals, |r| <= "
                 "1e-10 max(1, |E|)), handle creation excluded"}
     for v in dav["runs"].values():

@@ -32,15 +32,16 @@ def _timed(fn):
 def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int = 300,
                   tolerance: float = 1e-9, mixed_steps: int = 60,
                   refine_inner: int = 80, refine_inner_tolerance: float = 1e-2,
-                  with_davidson: bool = True) -> Dict:
+                  with_davidson: bool = True, mixed_reortho: bool = False) -> Dict:
     """Lowest state of one sector by
       fp64_lanczos           -- the plain method: FP64 Lanczos, full reorthogonalisation,
                                 eigenvalue-change tolerance 1e-12 (reference defaults);
       fp64_davidson          -- FP64 Davidson, Jacobi correction, |r| <= tolerance |E|
                                 (the converged FP64 pair the others are compared with);
-      mixed_lanczos_refined  -- TF32x3 Lanczos (FP64 recurrence and reorthogonalisation)
-                                for mixed_steps steps, then FP64 Rayleigh-quotient and
-                                residual refinement with TF32x3 correction solves;
+      mixed_lanczos_refined  -- TF32x3 Lanczos (FP64 recurrence; reorthogonalisation only
+                                with mixed_reortho: this phase only supplies the start
+                                vector) for mixed_steps steps, then FP64 Rayleigh-quotient
+                                and residual refinement with TF32x3 correction solves;
       mixed_davidson         -- TF32x3 Davidson with the learned (or Jacobi)
                                 correction, FP64 restart phase.
     Seconds are device time around each whole solve (host work included);
@@ -88,7 +89,8 @@ def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int 
     bg.set_precision(plugin.TF32X3)
 
     def mixed_refined():
-        e1, z1, n1 = bg.lanczos_lowest(init, steps=mixed_steps, tolerance=1e-4)
+        e1, z1, n1 = bg.lanczos_lowest(init, steps=mixed_steps, tolerance=1e-4,
+                                       reortho=mixed_reortho)
         e2, st = bg.refine_lowest(z1, max_outer=8, tolerance=tolerance,
                                   inner_iterations=refine_inner,
                                   inner_tolerance=refine_inner_tolerance,
