@@ -133,10 +133,11 @@ def test_group_handle_as_one_sector_with_graph_replay(cuda_lib, cuda_device):
     bg.close()
 
 
-@pytest.mark.parametrize("precision", ["tf32x3", "fp64"])
-def test_group_refinement_matches_single_fp64_solves(cuda_lib, cuda_device, precision):
+@pytest.mark.parametrize("precision,reortho", [("tf32x3", True), ("tf32x3", False), ("fp64", True)])
+def test_group_refinement_matches_single_fp64_solves(cuda_lib, cuda_device, precision, reortho):
     """Serving-style problems in one group handle: a loose lockstep group
-    Lanczos (the handle's matvecs: tensor-core TF32x3 or FP64), then the
+    Lanczos (the handle's matvecs: tensor-core TF32x3 or FP64; with or without
+    reorthogonalisation, as the start vectors only), then the
     lockstep FP64 refinement (dmrgpp_refine_lowest_group).  Every sector
     converges; its energy is within 1e-9 per site (and 1e-10 relative) of its
     single-problem FP64 Lanczos, its vector has unit norm and overlaps the
@@ -148,7 +149,7 @@ def test_group_refinement_matches_single_fp64_solves(cuda_lib, cuda_device, prec
     bg = plugin.BatchedGemm.from_problems(probs, precision=prec)
     offs = bg.sector_offsets()
     init = torch.from_numpy(np.random.default_rng(5).standard_normal(bg.dim)).cuda()
-    _, z, _ = bg.lanczos_lowest_group(init, steps=100, tolerance=1e-4)
+    _, z, _ = bg.lanczos_lowest_group(init, steps=100, tolerance=1e-4, reortho=reortho)
     e, conv, st = bg.refine_lowest_group(z, max_outer=8, tolerance=1e-10, inner_iterations=80,
                                          inner_tolerance=1e-2)
     assert conv.all() and st["converged"] == 1 and st["fp64_matvecs"] >= 1
