@@ -9,6 +9,7 @@
 // in later sweep steps or runs skip the timing.
 #include "dmrgpp_kron.h"
 #include "handle.h"
+#include "kron_fused.cuh"
 #include "kron_persistent.cuh"
 
 #include <cuda_runtime.h>
@@ -63,7 +64,8 @@ bool cache_lookup(const char* path, const std::string& sig, int* cfg, int* ipc, 
 		std::string        s;
 		int                c = -1, i = 0;
 		double             t = 0;
-		if (in >> s >> c >> i >> t && s == sig && c >= 0 && c < dmrgpp::kNumTileCfgs && i > 0) {
+		if (in >> s >> c >> i >> t && s == sig && c >= 0 && c < dmrgpp::kNumTileCfgs + dmrgpp::kNumFusedCfgs
+		    && i > 0) {
 			*cfg  = c;
 			*ipc  = i;
 			*us   = t;
@@ -98,7 +100,8 @@ int dmrgpp_kron_set_config(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 {
 	if (!h)
 		return DMRGPP_INVALID_ARG;
-	if (cfg < 0 || cfg >= dmrgpp::kNumTileCfgs || items_per_cta < 1 || items_per_cta > 64)
+	if (cfg < 0 || cfg >= dmrgpp::kNumTileCfgs + dmrgpp::kNumFusedCfgs || items_per_cta < 1
+	    || items_per_cta > 64)
 		return dmrgpp::handle_fail(h, DMRGPP_INVALID_ARG, "unknown tile configuration");
 	int prev = -1;
 	cudaGetDevice(&prev);
@@ -154,7 +157,18 @@ int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps,
 	const int ipcs[] = { 1, 2, 4 };
 	double    best   = -1.0;
 	int       bcfg = h->cfg, bipc = h->items_per_cta;
+	// fused configurations where the output patches fit in at most two column
+	// tiles (wider ones repeat the first product per column tile)
+	long long max_l = 0;
+	for (size_t p = 0; p < h->plan.np; ++p)
+		max_l = std::max(max_l, h->plan.l[p]);
+	std::vector<int> cands;
 	for (int c = 0; c < kNumTileCfgs; ++c)
+		cands.push_back(c);
+	for (int f = 0; f < kNumFusedCfgs; ++f)
+		if (max_l <= 2LL * fused_shape(f).bn)
+			cands.push_back(kNumTileCfgs + f);
+	for (int c : cands)
 		for (int i : ipcs) {
 			if (configure_schedule(h, c, i) != DMRGPP_OK)
 				continue;

@@ -1,6 +1,7 @@
 // C ABI of the Kronecker H*x engine (include/dmrgpp_kron.h).
 #include "dmrgpp_kron.h"
 #include "kron_gemm.cuh"
+#include "kron_fused.cuh"
 #include "kron_persistent.cuh"
 #include "kron_plan.h"
 #include "devmem.h"
@@ -101,6 +102,10 @@ void release(dmrgpp_kron_handle h)
 	dmrgpp::dev_free(h->d_lists);
 	dmrgpp::dev_free(h->d_ctr);
 	dmrgpp::dev_free(h->d_part);
+	dmrgpp::dev_free(h->d_flists);
+	h->d_flists = nullptr;
+	h->d_fitems = nullptr;
+	h->d_funits = nullptr;
 	dmrgpp::error_word_free(h->err_host);
 	h->err_host = h->err_dev = nullptr;
 	h->d_ctr                 = nullptr;
@@ -236,6 +241,21 @@ int kron_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const St
 		return mixed_apply_device(h, X, Y, io);
 	const auto& P = h->plan;
 	cudaError_t e;
+	if (h->cfg >= kNumTileCfgs) {
+		dmrgpp::FusedArgs fa {};
+		fa.ops           = h->d_ops;
+		fa.x             = X;
+		fa.y             = Y;
+		fa.items         = h->d_fitems;
+		fa.units         = h->d_funits;
+		fa.sector_active = h->sector_active;
+		fa.io            = io;
+		fa.n_items       = int(P.fitems.size());
+		fa.max_clusters  = h->fused_clusters;
+		if ((e = dmrgpp::launch_fused(fa, h->cfg - kNumTileCfgs, h->stream)))
+			return cuda_fail(h, e, "fused H*x launch");
+		return DMRGPP_OK;
+	}
 	dmrgpp::PersistentArgs pa {};
 	pa.ops           = h->d_ops;
 	pa.x             = X;
@@ -404,8 +424,51 @@ int build_mixed(dmrgpp_kron_handle h, MixedHost& host)
 	return DMRGPP_OK;
 }
 
+// Fused form: schedule for configuration fcfg, its tiles' work cut into about
+// parts_per_sm rounds of parts for every co-resident CTA.
+int configure_fused(dmrgpp_kron_handle h, int fcfg, int parts_per_sm)
+{
+	cudaError_t e = fused_init(fcfg, &h->fused_clusters);
+	if (e == cudaSuccess && h->fused_clusters < 1)
+		e = cudaErrorInvalidConfiguration;
+	if (e != cudaSuccess)
+		return cuda_fail(h, e, "fused kernel attributes");
+	KronPlan&        P = h->plan;
+	const FusedShape s = fused_shape(fcfg);
+	std::vector<int> sector_of_patch;
+	if (h->sector_start.size() > 2) {
+		sector_of_patch.resize(P.np);
+		for (size_t i = 0; i < P.np; ++i)
+			sector_of_patch[i] = int(std::upper_bound(h->sector_start.begin(), h->sector_start.end(),
+			                                          P.xy_start[i])
+			                         - h->sector_start.begin())
+			    - 1;
+	}
+	build_fused_schedule(P, s.bm, s.bn, s.cw, s.cluster, parts_per_sm, h->fused_clusters * s.cluster,
+	                     sector_of_patch.empty() ? nullptr : &sector_of_patch);
+	if (P.fitems.size() > size_t(INT_MAX) || P.funits.size() > size_t(INT_MAX))
+		return fail(h, DMRGPP_INVALID_ARG, "sector too large for the fused form");
+	const size_t ib = P.fitems.size() * sizeof(FusedItem), ub = P.funits.size() * sizeof(FusedUnit);
+	dmrgpp::dev_free(h->d_flists);
+	h->d_flists = nullptr;
+	h->d_fitems = nullptr;
+	h->d_funits = nullptr;
+	if ((e = dmrgpp::dev_malloc(&h->d_flists, std::max<size_t>(ib + ub, 16))))
+		return cuda_fail(h, e, "device allocation (fused lists)");
+	h->d_fitems = static_cast<FusedItem*>(h->d_flists);
+	h->d_funits = reinterpret_cast<FusedUnit*>(static_cast<unsigned char*>(h->d_flists) + ib);
+	if ((ib && (e = cudaMemcpy(h->d_fitems, P.fitems.data(), ib, cudaMemcpyHostToDevice)))
+	    || (ub && (e = cudaMemcpy(h->d_funits, P.funits.data(), ub, cudaMemcpyHostToDevice))))
+		return cuda_fail(h, e, "upload fused lists");
+	h->cfg           = kNumTileCfgs + fcfg;
+	h->items_per_cta = parts_per_sm;
+	return DMRGPP_OK;
+}
+
 int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 {
+	if (cfg >= kNumTileCfgs)
+		return configure_fused(h, cfg - kNumTileCfgs, items_per_cta);
 	int         grid = 0, tile = 0, bk = 0;
 	cudaError_t e    = persistent_config(cfg, &grid, &tile, &bk);
 	if (e != cudaSuccess)

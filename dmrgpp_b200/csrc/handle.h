@@ -58,6 +58,11 @@ struct dmrgpp_kron_s {
 	const int*          sector_active = nullptr; // set by the group solver: skip stopped sectors
 	unsigned*           d_ctr   = nullptr; // work counters, done[np], arrive[split tiles]
 	double*             d_part  = nullptr; // split-K partial tiles
+	// fused form (cfg >= kNumTileCfgs, kron_fused.cu): items and units
+	void*               d_flists = nullptr;
+	dmrgpp::FusedItem*  d_fitems = nullptr;
+	dmrgpp::FusedUnit*  d_funits = nullptr;
+	int                 fused_clusters = 0; // co-resident clusters of the fused configuration
 	int*                err_host = nullptr; // mapped pinned word written by the kernel
 	int*                err_dev  = nullptr;
 	int                 test_stall = 0;     // dmrgpp_kron_test_stall_dependency
@@ -139,8 +144,10 @@ int build_mixed(dmrgpp_kron_handle h, MixedHost& host);
 // h->crs (crs.cu), in place of upload_operators.
 int upload_operators_crs(dmrgpp_kron_handle h);
 
-// (Re)builds and uploads the persistent schedule of h for tile configuration
-// cfg (0..kNumTileCfgs-1), aiming at items_per_cta work items per CTA.
+// (Re)builds and uploads the schedule of h for configuration cfg: the
+// persistent two-pass form for cfg in 0..kNumTileCfgs-1 (items_per_cta work
+// items per CTA), the fused form (kron_fused.cuh) for kNumTileCfgs + f
+// (items_per_cta parts per SM).
 int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta);
 
 // Records msg as the handle's last error and returns status.

@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <numeric>
 #include <thread>
@@ -410,6 +412,174 @@ void build_persistent_schedule(KronPlan& plan, int bk, int grid, int items_per_c
 		const std::vector<GemmSeg>& segs = w.kind == 0 ? plan.seg1 : plan.pseg2;
 		if (w.seg_end > w.seg_begin)
 			w.seg0 = segs[size_t(w.seg_begin)];
+	}
+}
+
+void build_fused_schedule(KronPlan& plan, int bm, int bn, int cw, int cluster, int rounds,
+                          int ctas, const std::vector<int>* sector_of_patch)
+{
+	plan.fitems.clear();
+	plan.funits.clear();
+	plan.f_max_part = 0.0;
+	const size_t np = plan.np, nt = plan.triples.size();
+	// contributing triples of output patch i: [tri_begin[i], tri_begin[i+1])
+	std::vector<size_t> tri_begin(np + 1, nt);
+	for (size_t t = nt; t-- > 0;)
+		tri_begin[size_t(plan.triples[t].i)] = t;
+	for (size_t i = np; i-- > 0;)
+		if (tri_begin[i] > tri_begin[i + 1])
+			tri_begin[i] = tri_begin[i + 1];
+
+	auto up = [](long long x, long long q) { return (x + q - 1) / q * q; };
+	struct Tile {
+		int       i, m0, n0;
+		size_t    u_begin, u_end; // in plan.funits
+		double    work;
+		int       parts;
+		std::vector<size_t> cut; // parts + 1 unit boundaries
+	};
+	std::vector<Tile>   tiles;
+	std::vector<double> uwork; // per unit: modelled flops
+	// modelled cost of one k-step (16 of the contraction) apart from its flops
+	const double step_cost = 2.0 * 32 * 32 * 16;
+	double total = 0.0;
+	for (size_t i = 0; i < np; ++i) {
+		const long long M = plan.r[i], N = plan.l[i];
+		for (long long m0 = 0; m0 < M; m0 += bm)
+			for (long long n0 = 0; n0 < N; n0 += bn) {
+				Tile tl {};
+				tl.i       = int(i);
+				tl.m0      = int(m0);
+				tl.n0      = int(n0);
+				tl.u_begin = plan.funits.size();
+				const double bme = double(up(std::min<long long>(bm, M - m0), 8));
+				const double bne = double(up(std::min<long long>(bn, N - n0), 8));
+				for (size_t t = tri_begin[i]; t < tri_begin[i + 1]; ++t) {
+					const Triple&   tr = plan.triples[t];
+					const long long rj = plan.r[tr.j], lj = plan.l[tr.j];
+					for (long long c0 = 0; c0 < lj; c0 += cw) {
+						FusedUnit u {};
+						u.cw     = int(std::min<long long>(cw, lj - c0));
+						u.b_off  = plan.bstack_off[tr.j] + plan.row_off[t];
+						u.ldb    = int(plan.M[tr.j]);
+						u.rj     = int(rj);
+						u.x_off  = plan.xy_start[tr.j] + c0 * rj;
+						u.at_off = plan.at_off[t] + c0;
+						u.lj     = int(lj);
+						plan.funits.push_back(u);
+						const double k1 = double(up(rj, 16)), k2 = double(up(u.cw, 16));
+						const double w  = 2.0 * bme * double(up(u.cw, 8)) * k1 + 2.0 * bme * bne * k2
+						    + step_cost * (k1 + k2) / 16.0;
+						uwork.push_back(w);
+						tl.work += w;
+					}
+				}
+				tl.u_end = plan.funits.size();
+				total += tl.work;
+				tiles.push_back(std::move(tl));
+			}
+	}
+	const double target = total / double(std::max(1, rounds * ctas));
+	for (Tile& tl : tiles) {
+		const size_t nu = tl.u_end - tl.u_begin;
+		int          p  = target > 0.0 ? int(std::ceil(tl.work / target - 1e-9)) : 1;
+		p               = std::max(1, std::min<int>(p, cluster));
+		p               = int(std::min<size_t>(size_t(p), std::max<size_t>(nu, 1)));
+		tl.parts        = p;
+		// cut where the running work crosses q / p of the tile's work (the
+		// nearer unit boundary), keeping every part non-empty
+		tl.cut.assign(size_t(p) + 1, tl.u_begin);
+		tl.cut[size_t(p)] = tl.u_end;
+		double acc  = 0.0;
+		size_t u    = tl.u_begin;
+		for (int q = 1; q < p; ++q) {
+			const double goal = tl.work * q / p;
+			while (u < tl.u_end - size_t(p - q) && acc + uwork[u] * 0.5 < goal) {
+				acc += uwork[u];
+				++u;
+			}
+			if (u <= tl.cut[size_t(q - 1)]) { // at least one unit per part
+				acc += uwork[u];
+				++u;
+			}
+			tl.cut[size_t(q)] = u;
+		}
+		for (int q = 0; q < p; ++q) {
+			double w = 0.0;
+			for (size_t v = tl.cut[size_t(q)]; v < tl.cut[size_t(q) + 1]; ++v)
+				w += uwork[v];
+			plan.f_max_part = std::max(plan.f_max_part, w);
+		}
+	}
+	// whole tiles into clusters: largest part count first, best fit
+	std::vector<size_t> order(tiles.size());
+	for (size_t q = 0; q < order.size(); ++q)
+		order[q] = q;
+	std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+		if (tiles[a].parts != tiles[b].parts)
+			return tiles[a].parts > tiles[b].parts;
+		return tiles[a].work > tiles[b].work;
+	});
+	struct Cl {
+		int                 used = 0;
+		double              heaviest = 0.0;
+		std::vector<size_t> tiles;
+	};
+	std::vector<Cl>                  cls;
+	std::vector<std::vector<size_t>> by_free(size_t(cluster) + 1); // clusters by free slots
+	for (size_t q : order) {
+		const Tile& tl   = tiles[q];
+		size_t      cidx = SIZE_MAX;
+		for (int f = tl.parts; f < cluster && cidx == SIZE_MAX; ++f)
+			if (!by_free[size_t(f)].empty()) {
+				cidx = by_free[size_t(f)].back();
+				by_free[size_t(f)].pop_back();
+			}
+		if (cidx == SIZE_MAX) {
+			cidx = cls.size();
+			cls.emplace_back();
+		}
+		Cl& c = cls[cidx];
+		c.used += tl.parts;
+		c.heaviest = std::max(c.heaviest, tl.work / tl.parts);
+		c.tiles.push_back(q);
+		const int free = cluster - c.used;
+		if (free > 0)
+			by_free[size_t(free)].push_back(cidx);
+	}
+	std::vector<size_t> corder(cls.size());
+	for (size_t q = 0; q < corder.size(); ++q)
+		corder[q] = q;
+	std::stable_sort(corder.begin(), corder.end(),
+	                 [&](size_t a, size_t b) { return cls[a].heaviest > cls[b].heaviest; });
+	plan.fitems.reserve(cls.size() * size_t(cluster));
+	for (size_t c : corder) {
+		int rank = 0;
+		for (size_t q : cls[c].tiles) {
+			const Tile& tl = tiles[q];
+			const int   i  = tl.i;
+			for (int p = 0; p < tl.parts; ++p) {
+				FusedItem it {};
+				it.y_off   = plan.xy_start[size_t(i)];
+				it.M       = int(plan.r[size_t(i)]);
+				it.N       = int(plan.l[size_t(i)]);
+				it.m0      = tl.m0;
+				it.n0      = tl.n0;
+				it.u_begin = int(tl.cut[size_t(p)]);
+				it.u_end   = int(tl.cut[size_t(p) + 1]);
+				it.part    = p;
+				it.nparts  = tl.parts;
+				it.rank0   = rank;
+				it.sector  = sector_of_patch ? (*sector_of_patch)[size_t(i)] : 0;
+				plan.fitems.push_back(it);
+			}
+			rank += tl.parts;
+		}
+		for (; rank < cluster; ++rank) {
+			FusedItem it {};
+			it.nparts = 0;
+			plan.fitems.push_back(it);
+		}
 	}
 }
 

@@ -107,6 +107,40 @@ struct alignas(16) KronItem {
 	int       pad;
 };
 
+// Fused form (kron_fused.cu): one unit = one contributing triple (i,j,k)
+// restricted to input columns [c0, c0 + cw) of X_j:
+//     T  (rows x cw)  = B_k(i,j)[rows, :] * X_j[:, c0 .. c0+cw)
+//     Y_i[rows, cols] += T * A_k(i,j)[cols, c0 .. c0+cw)^T
+// Offsets point at element (row 0 of the (i,k) group, column 0) of
+// Bstack_j, at X_j[0, c0], and at A^T_k(i,j)[c0, 0].
+struct alignas(16) FusedUnit {
+	long long b_off;
+	long long x_off;
+	long long at_off;
+	int       ldb; // M_j (leading dimension of Bstack_j)
+	int       rj;  // contraction of the first product (rows of X_j)
+	int       lj;  // leading dimension of A^T_k(i,j) (= l_j)
+	int       cw;  // columns of the unit (<= the configuration's unit width)
+};
+
+// One CTA of the fused launch: part `part` of `nparts` of the output tile
+// [m0, m0+BM) x [n0, n0+BN) of Y_i (M = r_i rows, N = l_i columns, at y_off),
+// summing units [u_begin, u_end).  The parts of one tile sit in one cluster
+// at ranks rank0 .. rank0 + nparts - 1; nparts = 0 marks an empty slot.
+struct alignas(16) FusedItem {
+	long long y_off;
+	int       M;
+	int       N;
+	int       m0;
+	int       n0;
+	int       u_begin;
+	int       u_end;
+	int       part;
+	int       nparts;
+	int       rank0;
+	int       sector;
+};
+
 struct Triple {
 	int i, j, k;
 };
@@ -205,6 +239,11 @@ struct KronPlan {
 	long long             partial_slots = 0;
 
 	MixedPlan mixed;
+
+	// fused form: items cluster by cluster, and their units
+	std::vector<FusedItem> fitems;
+	std::vector<FusedUnit> funits;
+	double                 f_max_part = 0.0; // modelled flops of the largest part
 
 	long long dim() const { return xy_start.empty() ? 0 : xy_start.back(); }
 };
@@ -352,5 +391,15 @@ constexpr int kMaxItemSegs = 32;
 // CTAs: pass-2 output tiles are cut into K-slices (multiples of bk, on any
 // k boundary) when there are fewer than items_per_cta tiles per CTA.
 void build_persistent_schedule(KronPlan& plan, int bk, int grid, int items_per_cta = 2);
+
+// Builds plan.fitems / funits for the fused launch: output tiles of bm rows
+// and bn columns (columns past bn repeat the first product per column tile),
+// units cw input columns wide, each tile's units cut into at most `cluster`
+// parts of about equal modelled work (the target is the total over
+// rounds x ctas parts, ctas = the CTAs resident at once), tiles packed whole
+// into clusters of `cluster` CTAs (best fit, largest first).  sector_of_patch
+// (optional, np entries) gives each output patch's sector for group handles.
+void build_fused_schedule(KronPlan& plan, int bm, int bn, int cw, int cluster, int rounds,
+                          int ctas, const std::vector<int>* sector_of_patch = nullptr);
 
 } // namespace dmrgpp

@@ -267,10 +267,16 @@ const char* dmrgpp_kron_noalloc_last_error(void);
 
 /* ---- Launch tuning (no counterpart in the reference, whose GPU tiling is a
  * set of fixed constants, BatchedGemmKokkos.h:110-130) ----
- * Tile configurations of the H*x kernel: 0: 32x32 tiles, k-chunk 16;
- * 1: 32x32, k32; 2: 64x64, k16; 3: 64x64, k32; 4: 32x32, k32, deeper
- * pipeline; 5: 32x32, k64.  items_per_cta: pass-2 work
- * items per resident CTA below which output tiles are split along K. */
+ * Tile configurations of the H*x kernel.  Two-pass persistent form:
+ * 0: 32x32 tiles, k-chunk 16; 1: 32x32, k32; 2: 64x64, k16; 3: 64x64, k32;
+ * 4: 32x32, k32, deeper pipeline; 5: 32x32, k64; items_per_cta: pass-2
+ * work items per resident CTA below which output tiles are split along K.
+ * Fused form (both passes of an output tile in one CTA, parts of a tile
+ * summed inside a thread-block cluster; for sectors of small patches):
+ * 6: 32x128 output tiles, 64-column units, clusters of 8; 7: the same with
+ * clusters of 16;
+ * items_per_cta: rounds of parts per resident CTA the tiles' work is cut
+ * into. */
 int dmrgpp_kron_get_config(dmrgpp_kron_handle h, int* cfg, int* items_per_cta);
 int dmrgpp_kron_set_config(dmrgpp_kron_handle h, int cfg, int items_per_cta);
 

@@ -184,7 +184,7 @@ def test_autotune_then_cache_hit(cuda_lib, cuda_device, oracle_built, tmp_path):
     cache = str(tmp_path / "tune.txt")
     bg = plugin.BatchedGemm.from_problem(prob)
     cfg, us = bg.autotune(cache, reps=3)
-    assert 0 <= cfg <= 5 and us > 0
+    assert 0 <= cfg < 8 and us > 0
     assert rel_err(bg(x), oracle_built.kron_apply(prob, x)) < RTOL
     bg.close()
     lines = open(cache).read().split("\n")
