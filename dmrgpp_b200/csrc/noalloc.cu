@@ -133,13 +133,25 @@ int dmrgpp_kron_apply_noalloc(const dmrgpp_kron_desc* d, const double* x, double
 		return rc;
 	};
 
-	double*     base = nullptr;
-	cudaError_t e    = setup_device(dev, &base);
+	// The operator and list uploads read host memory that this call frees
+	// before it returns; a capture would record copies from freed memory.
+	cudaStream_t                stream = static_cast<cudaStream_t>(d->stream);
+	cudaStreamCaptureStatus     cap    = cudaStreamCaptureStatusNone;
+	cudaError_t                 e      = cudaStreamIsCapturing(stream, &cap);
+	if (e != cudaSuccess)
+		return restore(noalloc_fail(DMRGPP_CUDA_ERROR,
+		                            std::string("stream query: ") + cudaGetErrorString(e)));
+	if (cap != cudaStreamCaptureStatusNone)
+		return restore(noalloc_fail(DMRGPP_NOT_SUPPORTED,
+		                            "the stream is being captured: this call uploads from host "
+		                            "memory that it frees before returning"));
+
+	double* base = nullptr;
+	e            = setup_device(dev, &base);
 	if (e != cudaSuccess)
 		return restore(noalloc_fail(DMRGPP_CUDA_ERROR,
 		                            std::string("scratch set-up: ") + cudaGetErrorString(e)));
 
-	cudaStream_t stream = static_cast<cudaStream_t>(d->stream);
 	double*      ops    = base;
 	double*      bx     = base + plan.op_elems;
 	auto*        segs   = reinterpret_cast<dmrgpp::GemmSeg*>(bx + plan.bx_elems);

@@ -27,31 +27,77 @@ def _rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
+def _sparse_second_sector():
+    """A sector smaller than the microbench one, with all-zero blocks and an
+    output patch that no term reaches (its part of y must come out 0)."""
+    prob = sb.random_problem(npatches=7, noperator=4, max_size=90, seed=21, zero_block_rate=0.3)
+    for key in [k for k in prob.A if k[0] == 3]:
+        del prob.A[key]
+        del prob.B[key]
+    some = sorted(prob.A)[:3]
+    for key in some:                       # present but all zero: not a term
+        prob.A[key] = np.zeros_like(prob.A[key], order="F")
+    return prob
+
+
+def _noalloc_apply(cuda_lib, cuda_device, prob, x, stream):
+    import torch
+    from dmrgpp_b200 import _capi
+    t = _desc(prob, stream)
+    xd = torch.from_numpy(x).to(cuda_device)
+    yd = torch.full_like(xd, float("nan"))
+    rc = cuda_lib.dmrgpp_kron_apply_noalloc(ctypes.byref(t.desc), ctypes.c_void_p(xd.data_ptr()),
+                                            ctypes.c_void_p(yd.data_ptr()))
+    assert rc == _capi.OK, cuda_lib.dmrgpp_kron_noalloc_last_error()
+    torch.cuda.synchronize()
+    return yd.cpu().numpy()
+
+
 @pytest.mark.gpu
 def test_noalloc_matches_allocating_entry_point_twice(cuda_lib, cuda_device):
+    """Two calls in a row: the microbench sector, then a smaller sector with
+    all-zero blocks and an output patch without terms, which starts from the
+    scratch the larger call left behind (y prefilled with NaN each time)."""
     import torch
-    from dmrgpp_b200 import _capi, plugin
+    from dmrgpp_b200 import plugin
 
     stream = torch.cuda.current_stream().cuda_stream
-    first = sb.c2_problem(seed=3)
-    second = sb.random_problem(npatches=7, noperator=4, max_size=90, seed=21,
-                               zero_block_rate=0.0)
-    for prob, seed in ((first, 1), (second, 2)):
+    second = _sparse_second_sector()
+    for prob, seed in ((sb.c2_problem(seed=3), 1), (second, 2)):
         x = sb.random_unit_vector(prob.dim, seed=seed)
         bg = plugin.BatchedGemm.from_problem(prob, stream=stream)
         y_alloc = bg(x)
         bg.close()
-
-        t = _desc(prob, stream)
-        xd = torch.from_numpy(x).to(cuda_device)
-        yd = torch.full_like(xd, float("nan"))
-        rc = cuda_lib.dmrgpp_kron_apply_noalloc(ctypes.byref(t.desc), ctypes.c_void_p(xd.data_ptr()),
-                                                ctypes.c_void_p(yd.data_ptr()))
-        assert rc == _capi.OK, cuda_lib.dmrgpp_kron_noalloc_last_error()
-        torch.cuda.synchronize()
-        y_noalloc = yd.cpu().numpy()
+        y_noalloc = _noalloc_apply(cuda_lib, cuda_device, prob, x, stream)
         assert np.isfinite(y_noalloc).all()
         assert _rel(y_noalloc, y_alloc) < RTOL
+    s3 = second.xy_start
+    assert np.all(y_noalloc[s3[3]:s3[4]] == 0.0)
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_a_capturing_stream(cuda_lib, cuda_device):
+    """Its uploads read host memory freed when the call returns, so a call on
+    a stream under capture is refused before any device work; the capture
+    itself stays valid."""
+    import torch
+    from dmrgpp_b200 import _capi
+    prob = sb.c2_problem(seed=3)
+    x = torch.from_numpy(sb.random_unit_vector(prob.dim, seed=1)).to(cuda_device)
+    y = torch.zeros_like(x)
+    side = torch.cuda.Stream(cuda_device)
+    t = _desc(prob, side.cuda_stream)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side):
+        y.add_(x)
+        rc = cuda_lib.dmrgpp_kron_apply_noalloc(ctypes.byref(t.desc), ctypes.c_void_p(x.data_ptr()),
+                                                ctypes.c_void_p(y.data_ptr()))
+    assert rc == _capi.NOT_SUPPORTED
+    assert "captured" in cuda_lib.dmrgpp_kron_noalloc_last_error().decode()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(y, x)
+    del g
 
 
 def test_noalloc_rejects_sectors_beyond_its_scratch(cuda_lib):
