@@ -5,8 +5,31 @@ sector) on B200, against the reference's CPU batched path.
                     [--workload c2|ladder] [--precision fp64]
 
 Prints one JSON line on rank 0.  Multi-GPU runs (torchrun, one rank per GPU)
-are independent replicas of the sector (the path is single-GPU; see the
-design notes), timed on the device as the max over ranks.
+are independent replicas of the sector (the path is single-GPU), timed on the
+device as the max over ranks.
+
+    python bench.py --profile-case c2 [--precision fp64|tf32x3] [--applies N]
+                                      [--config C --ipc I]
+    python bench.py --profile-case ladder --states 4000 --precision tf32x3
+    python bench.py --profile-case ladder --states 4000 --solve lanczos
+    python bench.py --profile-case mlp --elements 300000 [--inference cuda_cores]
+    python bench.py --profile-case wft --states 4000
+    python bench.py --profile-case truncation --states 16000
+    python bench.py --profile-case serving --problems 256
+
+runs one fixed workload on cuda:0 and nothing else, so that a profiler's
+launch list and captures see only its kernels: c2 = the 1024 x 1024-state,
+21-group, K=5 microbench sector; ladder = the ladder-shaped (N_up, N_down)
+sector with `--states` left and right states (K = 10); mlp = learned-
+preconditioner applications (seeded network, seeded diagonal and residual of
+`--elements` entries); wft = the wave-function transformation of the
+ladder-shaped layout with seeded square N(0,1)/sqrt(n) blocks; truncation =
+the density-matrix truncation of the ladder-shaped layout's system block (one
+group per patch) for a seeded unit sector vector, a quarter of the states
+kept; serving = the serving-style batch (superblock.serving_batch) in one
+TF32x3 group handle, solved once as the bench does: group Lanczos to a
+Ritz-value change of 1e-5, then the lockstep FP64 group refinement.  Prints
+one line "ok ..." at the end.
 """
 from __future__ import annotations
 
@@ -207,11 +230,11 @@ def measured_fp64_peak(torch, dev):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def read_traffic(workload):
-    """dram__bytes_read.sum + dram__bytes_write.sum of one kron_persistent
-    launch on this workload, from the committed ncu summary (a line
-    `traffic_bytes_per_launch: N`)."""
-    path = os.path.join(ROOT, "profiles", f"kron_persistent_{workload}.md")
+def read_traffic(workload, family="kron_persistent"):
+    """dram__bytes_read.sum + dram__bytes_write.sum of one launch of the
+    kernel family on this workload, from the committed ncu summary (a line
+    `traffic_bytes_per_launch: N` in profiles/<family>_<workload>.md)."""
+    path = os.path.join(ROOT, "profiles", f"{family}_{workload}.md")
     if not os.path.exists(path):
         return None
     m = re.search(r"^traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read(), re.M)
@@ -475,17 +498,20 @@ def ladder_measurements(torch, dev, stream):
     out["solve"] = sweep.sector_solves(prob, sites=64, mixed_steps=60, refine_inner=80,
                                        refine_inner_tolerance=1e-2,
                                        with_davidson=False)
+    out["attribution"] = sweep.step_attribution(prob, sites=64, repeats=5)
     out["wft"] = wft_measurement(torch, prob, stream, flush)
     out["truncation"] = truncation_measurement(torch, prob, stream)
     # one whole sweep step of the sector: wave-function transformation (the
     # initial guess), the eigensolve, the truncation of the grown block
-    sv = out["solve"]
+    at = out["attribution"]
     rest = out["wft"]["ms"] * 1e-3 + out["truncation"]["seconds"]
-    fp64 = sv["fp64_lanczos"]["seconds"] + rest
-    mixed = sv["mixed_lanczos_refined"]["seconds"] + rest
+    fp64 = at["fp64_lanczos"]["median_seconds"] + rest
+    mixed = at["mixed_refined"]["median_seconds"] + rest
     out["step"] = {"fp64_seconds": fp64, "mixed_seconds": mixed, "speedup": fp64 / mixed,
+                   "solve_medians_of": at["repeats"],
+                   "abs_dE_per_site": at["mixed_refined"]["abs_dE_per_site_vs_fp64_lanczos"],
                    "parts": "wft + solve + truncation (m = 4000 of 16000 states); the WFT and "
-                            "truncation run in FP64 in both"}
+                            "truncation run in FP64 in both; solves: medians of the repeats"}
     return out
 
 
@@ -681,10 +707,25 @@ def run_ours(args):
     if rank != 0:
         return 0
     achieved = f_alg / per_launch_s / 1e12
+    # the sweep-step and serving results as short keys near the start of the
+    # line (the full records follow at its end)
+    short = {}
+    if sweep_step is not None:
+        short.update(sweep_step_speedup=sweep_step["step"]["speedup"],
+                     sweep_step_solve_speedup=sweep_step["attribution"]["total_gain"],
+                     sweep_step_precision_gain=sweep_step["attribution"]["precision_gain"],
+                     sweep_step_abs_dE_per_site=sweep_step["step"]["abs_dE_per_site"])
+    if serving is not None:
+        short.update(serving_problems_per_s=serving["group_mixed"]["problems_per_s"],
+                     serving_problems_per_s_fp64=serving["group_lanczos"]["problems_per_s"])
+    kernel = ("kron_fused_kernel (both passes per output tile, cluster reduction; one launch)"
+              if tuned_cfg >= 6 else
+              "kron_persistent_kernel (both passes of one matvec in one launch)")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        **short,
         "data": "synthetic (seeded N(0,1) sector blocks)",
         "config": dict(workload_config(prob, args.workload),
                        precision=args.precision,
@@ -696,8 +737,9 @@ def run_ours(args):
                 "path": "dmrgpp_kron_apply(host x, host y) through the C ABI, pinned buffers"},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": UNIT,
                      "frac": achieved / peak if peak else None,
-                     "traffic": read_traffic(args.workload),
-                     "kernel": "kron_persistent_kernel (both passes of one matvec in one launch)",
+                     "traffic": read_traffic(args.workload,
+                                             "kron_fused" if tuned_cfg >= 6 else "kron_persistent"),
+                     "kernel": kernel,
                      "peak_source": "measured live: cuBLAS DGEMM 8192^3 FP64 (no FP64 entry "
                                     "in MEASURED_PEAKS.json)"},
         "gpu_launches": args.steps,
@@ -723,5 +765,111 @@ def main():
     return run_ours(args)
 
 
+def profile_case(argv) -> int:
+    """The workloads of the ncu summaries under profiles/ (see the module
+    docstring): a fixed number of applies or one solve, nothing else."""
+    p = argparse.ArgumentParser(prog="bench.py --profile-case")
+    p.add_argument("workload", choices=["c2", "ladder", "mlp", "wft", "truncation", "serving"])
+    p.add_argument("--problems", type=int, default=256, help="serving: problems in the batch")
+    p.add_argument("--elements", type=int, default=300000, help="mlp: vector length")
+    p.add_argument("--inference", default="tensor_cores", choices=["tensor_cores", "cuda_cores"])
+    p.add_argument("--states", type=int, default=4000, help="ladder: left = right states")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"])
+    p.add_argument("--applies", type=int, default=6)
+    p.add_argument("--config", type=int, default=None, help="FP64 tile configuration")
+    p.add_argument("--ipc", type=int, default=2, help="FP64 items per CTA")
+    p.add_argument("--solve", default=None, choices=["lanczos"],
+                   help="run one FP64 Lanczos solve instead of bare applies")
+    p.add_argument("--steps", type=int, default=60)
+    a = p.parse_args(argv)
+
+    import torch
+    from dmrgpp_b200 import plugin
+    from dmrgpp_b200 import superblock as sb
+
+    if a.workload == "mlp":
+        import numpy as np
+        from dmrgpp_b200.mlp import MLPPreconditioner
+        m = MLPPreconditioner(seed=7)
+        m.set_inference(m.TENSOR_CORES if a.inference == "tensor_cores" else m.CUDA_CORES)
+        rng = np.random.default_rng(0)
+        d = torch.tensor(rng.standard_normal(a.elements) * 3, dtype=torch.float64, device="cuda")
+        r = torch.tensor(rng.standard_normal(a.elements), dtype=torch.float64, device="cuda")
+        rn = float(torch.linalg.vector_norm(r))
+        for _ in range(a.applies):
+            t = m.precondition(d, r, -1.7, rn)
+        torch.cuda.synchronize()
+        print("ok", a.elements, float(t.abs().max()))
+        m.close()
+        return 0
+
+    if a.workload == "wft":
+        import numpy as np
+        from dmrgpp_b200.wft import WaveFunctionTransform
+        prob = sb.ladder_problem(total_states=a.states, sigma=2.5, seed=9)
+        rng = np.random.default_rng(17)
+        l, r = prob.lsz, prob.rsz
+        WL = [rng.standard_normal((int(n), int(n))) / np.sqrt(n) for n in l]
+        WR = [rng.standard_normal((int(n), int(n))) / np.sqrt(n) for n in r]
+        w = WaveFunctionTransform(l, r, l, r, list(range(prob.npatches)), WL, WR)
+        x = torch.from_numpy(rng.standard_normal(w.dim_in)).cuda()
+        y = torch.empty(w.dim_out, dtype=torch.float64, device="cuda")
+        for _ in range(a.applies):
+            w(x, y)
+        torch.cuda.synchronize()
+        print("ok", w.dim_in, w.flops, float(y.norm()))
+        w.close()
+        return 0
+
+    if a.workload == "serving":
+        import numpy as np
+        probs, _ = sb.serving_batch(a.problems)
+        bg = plugin.BatchedGemm.from_problems(probs, precision=plugin.TF32X3)
+        init = torch.from_numpy(np.random.default_rng(1).standard_normal(bg.dim)).cuda()
+        _, z, steps = bg.lanczos_lowest_group(init, steps=200, tolerance=1e-5)
+        e, conv, st = bg.refine_lowest_group(z, max_outer=10, tolerance=1e-10, inner_iterations=80,
+                                             inner_tolerance=1e-2, raise_on_no_convergence=False)
+        torch.cuda.synchronize()
+        print("ok", bg.dim, int(steps.max()), int(conv.sum()), st["inner_matvecs"])
+        bg.close()
+        return 0
+
+    if a.workload == "truncation":
+        import numpy as np
+        from dmrgpp_b200.truncation import density_truncate
+        prob = sb.ladder_problem(total_states=a.states, sigma=2.5, seed=9)
+        l, r = prob.lsz, prob.rsz
+        psi = torch.from_numpy(sb.random_unit_vector(prob.dim)).cuda()
+        for _ in range(a.applies):
+            out = density_truncate(l, r, list(range(prob.npatches)), l, 0, psi, a.states // 4)
+        torch.cuda.synchronize()
+        print("ok", prob.dim, out["kept_total"], out["discarded"])
+        return 0
+
+    prob = (sb.c2_problem() if a.workload == "c2"
+            else sb.ladder_problem(total_states=a.states, sigma=2.5, seed=9))
+    prec = plugin.TF32X3 if a.precision == "tf32x3" else plugin.FP64
+    s = torch.cuda.Stream()
+    torch.cuda.set_stream(s)
+    bg = plugin.BatchedGemm.from_problem(prob, stream=s.cuda_stream, precision=prec)
+    if prec == plugin.FP64 and a.config is not None:
+        bg.set_config(a.config, a.ipc)
+    x = torch.from_numpy(sb.random_unit_vector(prob.dim)).cuda()
+    y = torch.empty_like(x)
+    if a.solve == "lanczos":
+        e, z, n = bg.lanczos_lowest(x, steps=a.steps, tolerance=1e-12)
+        y = z
+        print("E", e, "steps", n)
+    else:
+        for _ in range(a.applies):
+            bg.apply_Htarget(x, y)
+    torch.cuda.synchronize()
+    print("ok", prob.dim, prob.flops(), float(y.norm()))
+    bg.close()
+    return 0
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "--profile-case":
+        sys.exit(profile_case(sys.argv[2:]))
     sys.exit(main())

@@ -60,6 +60,13 @@ class KronCrsDesc(ctypes.Structure):
                 ("stream", ctypes.c_void_p), ("device", ctypes.c_int)]
 
 
+class GatherIndexDesc(ctypes.Structure):
+    _fields_ = [("npatches", _sz), ("patch_left", _szp), ("patch_right", _szp),
+                ("left_groups", _sz), ("left_partition", _szp), ("right_groups", _sz),
+                ("right_partition", _szp), ("perm_inverse", _szp), ("offset", _sz),
+                ("sector_size", _sz)]
+
+
 class PlanInfo(ctypes.Structure):
     _fields_ = [("ntriples", _sz), ("dim", _sz), ("f_alg", ctypes.c_double),
                 ("operator_bytes", _sz), ("bx_bytes", _sz), ("pass1_tiles", _sz),
@@ -188,6 +195,8 @@ SIGNATURES.update({
                                             ctypes.POINTER(ctypes.c_int), _dp]),
     "dmrgpp_scatter": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _sz,
                                       ctypes.c_void_p]),
+    "dmrgpp_kron_gather_index": (ctypes.c_int, [ctypes.POINTER(GatherIndexDesc),
+                                                ctypes.POINTER(ctypes.c_int64)]),
 })
 
 

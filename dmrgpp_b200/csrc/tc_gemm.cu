@@ -10,7 +10,7 @@
 //   warp 0, one thread: producer.  For every 32-wide k-chunk of every
 //     K-segment of its tiles it waits until the ring stage is free, arms the
 //     stage's mbarrier with the byte count and issues four tiled TMA loads
-//     (cp.async.bulk.tensor.3d, completion counted on the mbarrier): the hi
+//     (cp.async.bulk.tensor.2d, completion counted on the mbarrier): the hi
 //     and lo parts of the A tile (128 rows) and of the B tile (BN rows).
 //     Every operand buffer is a 2-D tensor [row][32 values] (kron_plan.h;
 //     the tensor maps are kernel parameters); the TMA unit writes the tile

@@ -522,3 +522,29 @@ def plan_info(prob, precision: int = FP64) -> dict:
     info = _capi.PlanInfo()
     _capi.check(_capi.lib().dmrgpp_kron_plan_info_get(ctypes.byref(t.desc), ctypes.byref(info)))
     return {f: getattr(info, f) for f, _ in _capi.PlanInfo._fields_}
+
+
+def sector_gather_index(patch_left, patch_right, left_partition, right_partition, perm_inverse,
+                        offset: int, sector_size: int) -> np.ndarray:
+    """The sector's copyIn / copyOut index (dmrgpp_kron_gather_index, host
+    only): patch_left / patch_right are the patches' left and right groups
+    (GenIjPatch), left_partition / right_partition the blocks' group offsets
+    (Basis::partition, groups + 1 entries), perm_inverse the superblock's
+    permutationInverse (nl x nr), offset and sector_size the target sector in
+    super-basis order.  Returns int64 idx with yin = vin[idx] (dmrgpp_gather)
+    and vout[idx] = xout (dmrgpp_scatter)."""
+    pl, pr = _size_array(patch_left), _size_array(patch_right)
+    lp, rp = _size_array(left_partition), _size_array(right_partition)
+    perm = _size_array(perm_inverse)
+    d = _capi.GatherIndexDesc()
+    szp = ctypes.POINTER(ctypes.c_size_t)
+    d.npatches = len(pl)
+    d.patch_left, d.patch_right = pl.ctypes.data_as(szp), pr.ctypes.data_as(szp)
+    d.left_groups, d.right_groups = len(lp) - 1, len(rp) - 1
+    d.left_partition, d.right_partition = lp.ctypes.data_as(szp), rp.ctypes.data_as(szp)
+    d.perm_inverse = perm.ctypes.data_as(szp)
+    d.offset, d.sector_size = int(offset), int(sector_size)
+    idx = np.empty(int(sector_size), dtype=np.int64)
+    _capi.check(_capi.lib().dmrgpp_kron_gather_index(
+        ctypes.byref(d), idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+    return idx

@@ -155,3 +155,72 @@ def load_ladder_mlp():
     if os.path.exists(LADDER_WEIGHTS):
         return MLPPreconditioner.load(LADDER_WEIGHTS)
     return None
+
+
+def step_attribution(prob, sites: int, repeats: int = 5, seed: int = 7,
+                     lanczos_steps: int = 300, mixed_steps: int = 60,
+                     tolerance: float = 1e-9) -> Dict:
+    """Separates the mixed solve's gain over the plain method into its causes,
+    each arm on its own handle, every arm repeated `repeats` times in
+    interleaved order (median, min, max seconds of device time):
+      fp64_lanczos        -- the plain method: FP64 handle, FP64 Lanczos with
+                             full reorthogonalisation, eigenvalue change 1e-12;
+      fp64_refined        -- the mixed solve's scheme in FP64: mixed_steps
+                             Lanczos steps without reorthogonalisation (1e-4
+                             Ritz-value change), then the FP64 refinement
+                             whose correction solves also run in FP64;
+      mixed_refined       -- the same scheme with TF32x3 matvecs in the Lanczos
+                             phase and the correction solves (TF32X3 handle).
+    scheme_gain = fp64_lanczos / fp64_refined, precision_gain = fp64_refined /
+    mixed_refined; their product is the total.  Before timing, every arm runs
+    once untimed, so the library's memory pool already holds what the timed
+    solves need (pool_growth_bytes reports any growth during the timing)."""
+    import torch
+    init = torch.from_numpy(np.random.default_rng(seed).standard_normal(prob.dim)).cuda()
+    b64 = plugin.BatchedGemm.from_problem(prob, precision=plugin.FP64)
+    bmx = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+    for b in (b64, bmx):
+        b.set_precision(plugin.FP64)
+        b.autotune(None, reps=3)
+    bmx.set_precision(plugin.TF32X3)
+
+    def refined(bg):
+        e1, z1, n1 = bg.lanczos_lowest(init, steps=mixed_steps, tolerance=1e-4, reortho=False)
+        e2, st = bg.refine_lowest(z1, max_outer=8, tolerance=tolerance, inner_iterations=80,
+                                  inner_tolerance=1e-2, raise_on_no_convergence=False)
+        return e2, z1, st
+
+    arms = {"fp64_lanczos": lambda: b64.lanczos_lowest(init, steps=lanczos_steps, tolerance=1e-12),
+            "fp64_refined": lambda: refined(b64),
+            "mixed_refined": lambda: refined(bmx)}
+    for fn in arms.values():             # untimed: sizes the memory pool
+        fn()
+    pool_before = plugin.cached_memory()[0]
+    times = {k: [] for k in arms}
+    results = {}
+    for _ in range(repeats):
+        for k, fn in arms.items():
+            results[k], t, _ = _timed(fn)
+            times[k].append(t)
+    pool_growth = plugin.cached_memory()[0] - pool_before
+    b64.close()
+    bmx.close()
+    e_ref, z_ref, n_ref = results["fp64_lanczos"]
+    out = {"sector_dim": prob.dim, "repeats": repeats, "pool_growth_bytes": pool_growth}
+    for k in arms:
+        ts = sorted(times[k])
+        rec = {"median_seconds": ts[len(ts) // 2], "min_seconds": ts[0], "max_seconds": ts[-1]}
+        if k == "fp64_lanczos":
+            rec.update(energy=e_ref, matvecs=n_ref + 1)
+        else:
+            e, z, st = results[k]
+            rec.update(energy=e, converged=st["converged"], refine_inner_matvecs=st["inner_matvecs"],
+                       refine_fp64_matvecs=st["fp64_matvecs"],
+                       abs_dE_per_site_vs_fp64_lanczos=abs(e - e_ref) / sites,
+                       one_minus_overlap_vs_fp64_lanczos=1.0 - abs(float(torch.dot(z, z_ref))))
+        out[k] = rec
+    med = {k: out[k]["median_seconds"] for k in arms}
+    out["scheme_gain"] = med["fp64_lanczos"] / med["fp64_refined"]
+    out["precision_gain"] = med["fp64_refined"] / med["mixed_refined"]
+    out["total_gain"] = med["fp64_lanczos"] / med["mixed_refined"]
+    return out

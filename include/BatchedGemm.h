@@ -23,6 +23,7 @@
 
 #include <complex>
 #include <cstddef>
+#include <cstdint>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -36,7 +37,13 @@ template <typename T> class BatchedGemm {
 
 public:
 
-	using SizeType       = std::size_t; // PsimagLite SizeType (AllocatorCpu.h:44)
+	// PsimagLite's SizeType (AllocatorCpu.h:43-47): 32-bit with USE_SHORT, so
+	// that the caller's VectorSizeType& arguments bind either way
+#ifdef USE_SHORT
+	using SizeType = std::uint32_t;
+#else
+	using SizeType = long unsigned int;
+#endif
 	using VectorSizeType = std::vector<SizeType>;
 
 	BatchedGemm(SizeType         noperator,
@@ -52,22 +59,29 @@ public:
 	    : handle_(nullptr)
 	    , dim_(0)
 	{
-		dmrgpp_kron_desc d {};
+		// the C ABI takes size_t arrays
+		const std::vector<std::size_t> l(left_patch_size.begin(), left_patch_size.end());
+		const std::vector<std::size_t> r(right_patch_size.begin(), right_patch_size.end());
+		const std::vector<std::size_t> lda(ld_Amatrix.begin(), ld_Amatrix.end());
+		const std::vector<std::size_t> ldb(ld_Bmatrix.begin(), ld_Bmatrix.end());
+		dmrgpp_kron_desc               d {};
 		d.noperator        = noperator;
 		d.npatches         = npatches;
-		d.left_patch_size  = left_patch_size.data();
-		d.right_patch_size = right_patch_size.data();
+		d.left_patch_size  = l.data();
+		d.right_patch_size = r.data();
 		// std::complex<double> is two doubles (real, imaginary)
 		d.Amatrix          = reinterpret_cast<const double* const*>(Amatrix.data());
-		d.ld_Amatrix       = ld_Amatrix.data();
+		d.ld_Amatrix       = lda.data();
 		d.Bmatrix          = reinterpret_cast<const double* const*>(Bmatrix.data());
-		d.ld_Bmatrix       = ld_Bmatrix.data();
+		d.ld_Bmatrix       = ldb.data();
 		d.precision        = precision;
 		d.stream           = stream;
 		d.device           = -1;
 		check(kComplex ? dmrgpp_kron_create_complex(&d, &handle_) : dmrgpp_kron_create(&d, &handle_),
 		      nullptr);
-		check(dmrgpp_kron_dim(handle_, &dim_), handle_);
+		std::size_t dim = 0;
+		check(dmrgpp_kron_dim(handle_, &dim), handle_);
+		dim_ = SizeType(dim);
 	}
 
 	// vout = H vin, both host vectors in patch order (BatchedGemm.cpp:81-115).

@@ -256,7 +256,9 @@ int dmrgpp_kron_plan_info_get(const dmrgpp_kron_desc* desc, dmrgpp_kron_plan_inf
  * which loads the library holds until the process exits; a sector needing
  * more is rejected with DMRGPP_INVALID_ARG.  The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress) and sets kernel
- * attributes, so make that first call before any stream capture.  Every call
+ * attributes, so make that first call before any stream capture.  A call
+ * made on a stream that is being captured returns DMRGPP_NOT_SUPPORTED: its
+ * uploads read host memory that the call frees before returning.  Every call
  * shares the one array: calls that may overlap on the GPU (other streams,
  * other host threads) race and must be serialised by the caller.  Each call
  * rewrites every scratch byte it reads, so no clearing is needed between
@@ -503,6 +505,36 @@ int dmrgpp_tridiag_eigen(size_t n, const double* diag, const double* offdiag, do
  * positions in super-basis order; enqueued on stream (cudaStream_t). */
 int dmrgpp_gather(const double* src, const int64_t* idx, double* dst, size_t n, void* stream);
 int dmrgpp_scatter(const double* src, const int64_t* idx, double* dst, size_t n, void* stream);
+
+/* The index those two apply, built on the host cores from the superblock
+ * basis as the reference's copyIn / copyOut read it
+ * (InitKronHamiltonian.h:158-221, InitKronBase.h:315-360):
+ *   idx[vstart[p] + iR + iL * r_p] = perm_inverse[(iL + Loff) + (iR + Roff) * nl] - offset
+ * for patch p = (left group patch_left[p], right group patch_right[p]), its
+ * l_p and r_p states starting at Loff = left_partition[patch_left[p]] and
+ * Roff = right_partition[patch_right[p]], nl = left_partition[left_groups],
+ * vstart the prefix sums of l_p r_p (InitKronBase.h:277-310).  The arrays are
+ * the reference's GenIjPatch patches (GenIjPatch.h:104-118), Basis::partition
+ * of the left and right blocks (left_groups + 1 and right_groups + 1
+ * offsets), super().permutationInverse() (nl x nr entries) and the sector's
+ * offset and size.  Every entry is checked as the reference asserts
+ * (offset <= perm_inverse[.] < offset + sector_size) and the map must be a
+ * permutation of the sector; otherwise DMRGPP_INVALID_ARG with the reason in
+ * dmrgpp_kron_last_error(NULL).  idx: sector_size host entries. */
+typedef struct {
+	size_t        npatches;
+	const size_t* patch_left;      /* per patch: its left group */
+	const size_t* patch_right;     /* per patch: its right group */
+	size_t        left_groups;
+	const size_t* left_partition;  /* left_groups + 1 state offsets */
+	size_t        right_groups;
+	const size_t* right_partition; /* right_groups + 1 state offsets */
+	const size_t* perm_inverse;    /* nl x nr super-basis positions */
+	size_t        offset;          /* first super-basis position of the sector */
+	size_t        sector_size;
+} dmrgpp_gather_index_desc;
+
+int dmrgpp_kron_gather_index(const dmrgpp_gather_index_desc* desc, int64_t* idx);
 
 /* ---- Wave-function transformation between two patch layouts ----
  * The GEMM core of the reference's patch-wise WFT (Wft/WftAccelPatches.h:

@@ -26,7 +26,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle_kron.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_kron.so")
-REFERENCE_TREE = "/root/reference"
+# the reference source tree (read-only); only the build recipe reads it
+REFERENCE_TREE = os.environ.get("DMRGPP_REFERENCE_TREE", "/root/reference")
 
 _sz = ctypes.c_size_t
 _szp = ctypes.POINTER(ctypes.c_size_t)

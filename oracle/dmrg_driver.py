@@ -133,6 +133,53 @@ class Hubbard:
         return (nu, nd)
 
 
+class HubbardLadder(Hubbard):
+    """Two-leg Fermi-Hubbard ladder, H = -t_leg sum_leg - t_rung sum_rung
+    sum_s (c+_i,s c_j,s + h.c.) + U sum_i n_i,up n_i,down, open boundaries,
+    in the reference's site order (PsimagLite/src/PsimagLite/Geometry/
+    Ladder.h:87-292, LadderLeg=2): site i sits on rung i // 2 and leg i % 2;
+    sites on one rung (i, i+1 with i even) and on one leg two apart (i, i+2)
+    are connected.  Blocks grow one site at a time along that order, so each
+    block carries the operators of its last two sites (depth 2).  Quantum
+    number (N_up, N_down); the target of an N-site stage is the full
+    system's filling scaled to N sites (rounded)."""
+
+    depth = 2
+
+    def __init__(self, Lx: int, t_leg: float = 1.0, t_rung: float = 1.0, U: float = 0.0,
+                 n_up: int = None, n_dn: int = None):
+        super().__init__(t=t_leg, U=U, n_up=n_up, n_dn=n_dn)
+        self.Lx, self.t_leg, self.t_rung = Lx, t_leg, t_rung
+
+    @staticmethod
+    def connected(i: int, j: int) -> bool:
+        ci, cj, ri, rj = i // 2, j // 2, i % 2, j % 2
+        if ci == cj:
+            return abs(ri - rj) == 1
+        return ri == rj and abs(ci - cj) == 1
+
+    def link_terms(self, left_edge, right_edge, left_parity, i: int, j: int):
+        t = self.t_rung if i // 2 == j // 2 else self.t_leg
+        out = []
+        for name in ("Cu", "Cd"):
+            cl, cr = left_edge[name], right_edge[name]
+            out.append((-t, matmul(transpose(cl), left_parity), cr))
+            out.append((-t, matmul(left_parity, cl), transpose(cr)))
+        return out
+
+    def bonds(self):
+        """(i, j, t) of every connected pair, i < j (for exact checks)."""
+        L = 2 * self.Lx
+        return [(i, j, self.t_rung if i // 2 == j // 2 else self.t_leg)
+                for i in range(L) for j in range(i + 1, L) if self.connected(i, j)]
+
+    def target(self, N: int):
+        L = 2 * self.Lx
+        nu = self.n_up if self.n_up is not None else L // 2
+        nd = self.n_dn if self.n_dn is not None else L // 2
+        return (int(np.floor(nu * N / L + 0.5)), int(np.floor(nd * N / L + 0.5)))
+
+
 # ---------------------------------------------------- block-sparse algebra
 def transpose(a: BlockOp) -> BlockOp:
     return {(j, i): m.T.copy() for (i, j), m in a.items()}
@@ -224,41 +271,74 @@ class DMRG:
         # driver's own density-matrix truncation
         self.truncator: Optional[Callable] = None
 
-    # enlarge a left block by one site on its right
+    # boundary sites: chains couple nearest neighbours only (one boundary site
+    # per block); the two-leg ladder also couples sites two apart, so its
+    # blocks carry the operators of their last two sites (slot 0: the
+    # outermost site, slot 1: the one before it, names suffixed "~1")
+    def _depth(self) -> int:
+        return getattr(self.model, "depth", 1)
+
+    def _connected(self, i: int, j: int) -> bool:
+        f = getattr(self.model, "connected", None)
+        return f(i, j) if f is not None else abs(i - j) == 1
+
+    def _link_terms(self, lops, rops, parity, i: int, j: int):
+        f = getattr(self.model, "link_terms", None)
+        return f(lops, rops, parity, i, j) if f is not None else self.model.links(lops, rops, parity)
+
+    def _slot(self, blk: Block, d: int):
+        if d == 0:
+            return blk.ops
+        return {n: blk.ops[f"{n}~{d}"] for n in self.model.edge_names()}
+
+    # enlarge a left block (sites 0 .. k-1) by site k on its right
     def grow_left(self, b: Block) -> Block:
         s = self.site
+        k = b.length
         qns, sizes, layout = product_basis(b, s)
         H = kron_op(b.ops["H"], identity(s), qns, sizes, layout)
         add_into(H, kron_op(identity(b), s.ops["H"], qns, sizes, layout))
         parity = b.ops.get("P")
-        for c, lo, ro in self.model.links(b.ops, s.ops, parity):
-            add_into(H, kron_op(lo, ro, qns, sizes, layout), c)
+        for d in range(min(self._depth(), b.length)):
+            if self._connected(k - 1 - d, k):
+                for c, lo, ro in self._link_terms(self._slot(b, d), s.ops, parity, k - 1 - d, k):
+                    add_into(H, kron_op(lo, ro, qns, sizes, layout), c)
         ops = {"H": H}
         for name in self.model.edge_names():   # the new site is the edge
             left = parity if parity is not None else identity(b)
             ops[name] = kron_op(left, s.ops[name], qns, sizes, layout)
+            for d in range(1, min(self._depth(), b.length + 1)):
+                ops[f"{name}~{d}"] = kron_op(self._slot(b, d - 1)[name], identity(s), qns, sizes,
+                                             layout)
         if parity is not None:
             ops["P"] = kron_op(parity, s.ops["P"], qns, sizes, layout)
         return Block(qns, sizes, ops, b.length + 1)
 
-    # enlarge a right block by one site on its left
-    def grow_right(self, b: Block) -> Block:
+    # enlarge a right block (the last sites of an N-site system) by the site
+    # on its left
+    def grow_right(self, b: Block, N: int = 0) -> Block:
         s = self.site
+        k = N - b.length - 1                    # the new site's index
         qns, sizes, layout = product_basis(s, b)
         H = kron_op(identity(s), b.ops["H"], qns, sizes, layout)
         add_into(H, kron_op(s.ops["H"], identity(b), qns, sizes, layout))
         sp = s.ops.get("P")
-        for c, lo, ro in self.model.links(s.ops, b.ops, sp):
-            add_into(H, kron_op(lo, ro, qns, sizes, layout), c)
+        for d in range(min(self._depth(), b.length)):
+            if self._connected(k, k + 1 + d):
+                for c, lo, ro in self._link_terms(s.ops, self._slot(b, d), sp, k, k + 1 + d):
+                    add_into(H, kron_op(lo, ro, qns, sizes, layout), c)
         ops = {"H": H}
         for name in self.model.edge_names():   # the new site is the edge
             ops[name] = kron_op(s.ops[name], identity(b), qns, sizes, layout)
+            for d in range(1, min(self._depth(), b.length + 1)):
+                left = sp if sp is not None else identity(s)
+                ops[f"{name}~{d}"] = kron_op(left, self._slot(b, d - 1)[name], qns, sizes, layout)
         if sp is not None:
             ops["P"] = kron_op(sp, b.ops["P"], qns, sizes, layout)
         return Block(qns, sizes, ops, b.length + 1)
 
-    def superblock(self, left: Block, right: Block, target) -> Tuple[KronProblem, list]:
-        """Sector `target` of left (x) right as plugin tables."""
+    def superblock(self, left: Block, right: Block, target, N: int = 0) -> Tuple[KronProblem, list]:
+        """Sector `target` of left (x) right (an N-site system) as plugin tables."""
         ridx = right.index()
         patches = []
         for gl, ql in enumerate(left.qns):
@@ -269,7 +349,13 @@ class DMRG:
         lsz = np.array([left.sizes[gl] for gl, _ in patches], dtype=np.int64)
         rsz = np.array([right.sizes[gr] for _, gr in patches], dtype=np.int64)
         terms = [(1.0, left.ops["H"], identity(right)), (1.0, identity(left), right.ops["H"])]
-        terms += self.model.links(left.ops, right.ops, left.ops.get("P"))
+        N = N or (left.length + right.length)
+        for d in range(min(self._depth(), left.length)):
+            for e in range(min(self._depth(), right.length)):
+                i, j = left.length - 1 - d, N - right.length + e
+                if self._connected(i, j):
+                    terms += self._link_terms(self._slot(left, d), self._slot(right, e),
+                                              left.ops.get("P"), i, j)
         A, B = {}, {}
         for k, (c, lo, ro) in enumerate(terms):
             for (gi, gj), a in lo.items():
@@ -317,9 +403,9 @@ class DMRG:
     def step(self, left: Block, right: Block, sites: int):
         """One superblock solve: enlarge both, solve the target sector,
         return (energy, enlarged left, enlarged right, rho_L, rho_R)."""
-        lp, rp = self.grow_left(left), self.grow_right(right)
+        lp, rp = self.grow_left(left), self.grow_right(right, sites)
         target = self.model.target(sites)
-        prob, patches = self.superblock(lp, rp, target)
+        prob, patches = self.superblock(lp, rp, target, sites)
         init = self.rng.standard_normal(prob.dim)
         e, psi, _ = self.solver(prob, init)
         psi = np.asarray(psi)
@@ -394,8 +480,9 @@ def free_fermion_energy(L: int, n_up: int, n_dn: int, t: float = 1.0) -> float:
     return float(lev[:n_up].sum() + lev[:n_dn].sum())
 
 
-def hubbard_ed(L: int, U: float, n_up: int, n_dn: int, t: float = 1.0) -> float:
-    """Lowest energy of the open Hubbard chain by diagonalising H in the
+def hubbard_ed(L: int, U: float, n_up: int, n_dn: int, t: float = 1.0, bonds=None) -> float:
+    """Lowest energy of the open Hubbard chain (or of the lattice given by
+    bonds, (i, j, t) per connected pair) by diagonalising H in the
     fixed-(N_up, N_down) Fock space built directly from creation and
     annihilation operators (modes site-major, up before down), independent
     of the block construction above (small L only)."""
@@ -421,11 +508,11 @@ def hubbard_ed(L: int, U: float, n_up: int, n_dn: int, t: float = 1.0) -> float:
         for site in range(L):
             if (s >> (2 * site)) & 1 and (s >> (2 * site + 1)) & 1:
                 H[idx[s], idx[s]] += U
-        for site in range(L - 1):
+        for si, sj, tb in (bonds if bonds is not None else [(q, q + 1, t) for q in range(L - 1)]):
             for sp in range(2):
-                a, b = 2 * site + sp, 2 * (site + 1) + sp
+                a, b = 2 * si + sp, 2 * sj + sp
                 for i, j in ((a, b), (b, a)):
                     s2, sg = hop(s, i, j)
                     if s2 is not None:
-                        H[idx[s2], idx[s]] += -t * sg
+                        H[idx[s2], idx[s]] += -tb * sg
     return float(np.linalg.eigvalsh(H)[0])

@@ -1,0 +1,355 @@
+"""Whole DMRG runs of the configurations the benchmark names, with every
+sector eigensolve on the GPU (test infrastructure: the sweep engine is the
+oracle's two-site driver, oracle/dmrg_driver.py).
+
+    python tests/dmrg_runs.py c3 [--L 64 --m 1000 --sweeps 6] [--out run.json]
+    python tests/dmrg_runs.py ladder [--Lx 32 --m-inf 1000 --m 4000 --steps 2] [--mlp w.npz]
+                                    [--out run.json]
+    python tests/dmrg_runs.py ladder-mlp --mlp w.npz [--out run.json]
+
+c3: Fermi-Hubbard chain, t=1, U=4, open BC, half filling, m states kept, the
+    given finite sweeps.  The trajectory follows the mixed-precision solve
+    (TF32x3 Lanczos without reorthogonalisation, then the FP64 residual
+    refinement with TF32x3 correction solves); at every step the same sector
+    is also solved from the same start vector by the plain FP64 Lanczos (full
+    reorthogonalisation, eigenvalue-change tolerance 1e-10), and |dE|/site and
+    1 - |<psi|psi_FP64>| are recorded.  A second run along the FP64 trajectory
+    gives the final-energy comparison of the two runs.
+ladder: two-leg Hubbard ladder Lx x 2, t_leg = t_rung = 1, U=8, 56 electrons
+    (Sz=0) on 64 sites; infinite growth at m_inf states, then finite steps at
+    m states.  Each finite step's sector is solved by the plain FP64 Lanczos
+    (its own FP64 handle), by TF32x3 Lanczos + FP64 refinement, by the FP64
+    Jacobi-preconditioned Davidson and by the mixed Davidson with the learned
+    correction (weights trained on this ladder at m <= 1000); seconds (device
+    time of the whole solve, handle set-up separate), iterations and energies
+    per site are recorded.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from oracle import dmrg_driver as dd  # noqa: E402
+
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _timed(fn):
+    import torch
+    torch.cuda.synchronize()
+    a, b = _events()
+    a.record()
+    out = fn()
+    b.record()
+    b.synchronize()
+    return out, a.elapsed_time(b) / 1e3
+
+
+def mixed_solve(bg, init, sites, tolerance=1e-10):
+    """TF32x3 Lanczos (no reorthogonalisation, 60 steps or a 1e-4 Ritz-value
+    change) then the FP64 refinement to |r| <= tolerance |E|."""
+    from dmrgpp_b200 import plugin
+    bg.set_precision(plugin.TF32X3)
+    e1, z, n1 = bg.lanczos_lowest(init, steps=60, tolerance=1e-4, reortho=False)
+    e, st = bg.refine_lowest(z, max_outer=12, tolerance=tolerance, inner_iterations=80,
+                             inner_tolerance=1e-2, raise_on_no_convergence=False)
+    return e, z, n1, st
+
+
+def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print):
+    import torch
+    from dmrgpp_b200 import plugin
+    steps = []
+
+    def solve(prob, init):
+        x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
+        bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+        try:
+            (e, z, n1, st), t_mx = _timed(lambda: mixed_solve(bg, x, L))
+            bg.set_precision(plugin.FP64)
+            (e64, z64, n64), t_64 = _timed(lambda: bg.lanczos_lowest(x, steps=400, tolerance=1e-10))
+        finally:
+            bg.close()
+        rec = dict(dim=prob.dim, f_alg=prob.flops(), e_mixed=e, e_fp64=e64,
+                   abs_dE_per_site=abs(e - e64) / L,
+                   one_minus_overlap=1.0 - abs(float(torch.dot(z, z64))),
+                   mixed_seconds=t_mx, fp64_seconds=t_64, fp64_lanczos_steps=n64,
+                   refine_converged=int(st["converged"]))
+        steps.append(rec)
+        if len(steps) % 20 == 0:
+            log(f"step {len(steps)} dim {prob.dim} E {e:.12f} dE/site {rec['abs_dE_per_site']:.2e}")
+        return e, z.cpu().numpy(), n1
+
+    t0 = time.time()
+    d = dd.DMRG(dd.Hubbard(U=U, n_up=L // 2, n_dn=L // 2), L=L, m=m, solver=solve)
+    e_mixed = d.run(sweeps=sweeps)
+    out = dict(config=f"Hubbard chain L={L} U={U} half filling m={m} {sweeps} finite sweeps",
+               steps=len(steps), final_energy_mixed_run=e_mixed,
+               max_abs_dE_per_site_same_input=max(s["abs_dE_per_site"] for s in steps),
+               max_one_minus_overlap=max(s["one_minus_overlap"] for s in steps),
+               all_refinements_converged=all(s["refine_converged"] for s in steps),
+               max_dim=max(s["dim"] for s in steps),
+               solve_seconds_mixed=sum(s["mixed_seconds"] for s in steps),
+               solve_seconds_fp64=sum(s["fp64_seconds"] for s in steps),
+               wall_seconds_mixed_run=time.time() - t0, per_step=steps)
+    if fp64_run:
+        t1 = time.time()
+        n64 = []
+
+        def solve64(prob, init):
+            bg = plugin.BatchedGemm.from_problem(prob)
+            try:
+                e, z, n = bg.lanczos_lowest(init, steps=400, tolerance=1e-10)
+            finally:
+                bg.close()
+            n64.append(n)
+            return e, z, n
+        d64 = dd.DMRG(dd.Hubbard(U=U, n_up=L // 2, n_dn=L // 2), L=L, m=m, solver=solve64)
+        e64 = d64.run(sweeps=sweeps)
+        out.update(final_energy_fp64_run=e64, final_abs_dE_per_site=abs(e_mixed - e64) / L,
+                   wall_seconds_fp64_run=time.time() - t1)
+    return out
+
+
+def ladder_model(Lx=32, U=8.0, electrons=56):
+    return dd.HubbardLadder(Lx, t_leg=1.0, t_rung=1.0, U=U, n_up=electrons // 2,
+                            n_dn=electrons // 2)
+
+
+def ladder_sectors(Lx=32, U=8.0, electrons=56, m_inf=1000, m=4000, finite_steps=2,
+                   on_sector=None, log=print):
+    """Runs the ladder's infinite growth at m_inf (mixed solves), then
+    finite_steps left-to-right steps from the middle at m states; calls
+    on_sector(prob, init, step_index) for each finite step's sector, which
+    returns the (energy, state) the run continues with."""
+    import torch
+    from dmrgpp_b200 import plugin
+    L = 2 * Lx
+
+    def solve(prob, init):
+        x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
+        bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+        try:
+            e, z, n, st = mixed_solve(bg, x, L)
+        finally:
+            bg.close()
+        return e, z.cpu().numpy(), n
+
+    d = dd.DMRG(ladder_model(Lx, U, electrons), L=L, m=m_inf, solver=solve)
+    b_l = b_r = d.site
+    left, right = {1: b_l}, {1: b_r}
+    n = 1
+    while 2 * (n + 1) <= L:
+        t0 = time.time()
+        e, lp, rp, rl, rr = d.step(b_l, b_r, 2 * (n + 1))
+        b_l, b_r = d.truncate(lp, rl), d.truncate(rp, rr)
+        n += 1
+        left[n], right[n] = b_l, b_r
+        log(f"infinite {n}: E {e:.10f} left states {sum(lp.sizes)} ({time.time() - t0:.1f} s)")
+    d.m = m
+    records = []
+    for q, nl in enumerate(range(L // 2, L // 2 + finite_steps)):
+        lp, rp = d.grow_left(left[nl]), d.grow_right(right[L - nl - 2], L)
+        target = d.model.target(L)
+        prob, patches = d.superblock(lp, rp, target, L)
+        init = d.rng.standard_normal(prob.dim)
+        e, psi, rec = on_sector(prob, init, q)
+        records.append(rec)
+        rho_l = {}
+        xs = prob.xy_start
+        for p, (gl, gr) in enumerate(patches):
+            X = psi[xs[p]:xs[p + 1]].reshape(int(prob.lsz[p]), int(prob.rsz[p])).T
+            rho_l[gl] = rho_l.get(gl, 0.0) + X.T @ X
+        left[nl + 1] = d.truncate(lp, rho_l)
+        log(f"finite step {q}: E {e:.10f} dim {prob.dim} left states {sum(lp.sizes)}")
+    return records
+
+
+def ladder_step_measurement(prob, init, sites, mlp=None, lanczos_steps=400):
+    """One ladder sector solved every way (see the module docstring)."""
+    import torch
+    from dmrgpp_b200 import plugin
+    x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
+    rec = dict(dim=prob.dim, npatches=prob.npatches, noperator=prob.noperator,
+               f_alg=prob.flops())
+    # plain FP64 on its own FP64 handle; a warm create first (the previous
+    # step's buffers back in the pool, as in a sweep)
+    warm = plugin.BatchedGemm.from_problem(prob)
+    warm.lanczos_lowest(x, steps=lanczos_steps, min_steps=2, tolerance=1e300)
+    warm.close()
+    b64, t_set64 = _timed(lambda: plugin.BatchedGemm.from_problem(prob))
+    b64.autotune(None, reps=3)
+    (e64, z64, n64), t64 = _timed(lambda: b64.lanczos_lowest(x, steps=lanczos_steps,
+                                                             tolerance=1e-10))
+    (ej, zj, sj), tj = _timed(lambda: b64.davidson_lowest(x, preconditioner=1, tolerance=1e-9,
+                                                          max_iterations=4000,
+                                                          raise_on_no_convergence=False))
+    b64.close()
+    rec["fp64_lanczos"] = dict(energy=e64, seconds=t64, setup_seconds=t_set64, matvecs=n64 + 1)
+    rec["fp64_jacobi_davidson"] = dict(energy=ej, seconds=tj, iterations=sj["iterations"],
+                                       converged=sj["converged"])
+    bmx, t_setmx = _timed(lambda: plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3))
+    bmx.set_precision(plugin.FP64)
+    bmx.autotune(None, reps=3)
+    (e, z, n1, st), tmx = _timed(lambda: mixed_solve(bmx, x, sites, tolerance=1e-9))
+    rec["mixed_lanczos_refined"] = dict(
+        energy=e, seconds=tmx, setup_seconds=t_setmx, lanczos_steps=n1 + 1,
+        refine_mixed_matvecs=st["inner_matvecs"], fp64_matvecs=st["fp64_matvecs"],
+        converged=st["converged"], abs_dE_per_site=abs(e - e64) / sites,
+        one_minus_overlap=1.0 - abs(float(torch.dot(z, z64))))
+    for name, pre, m in (("mixed_davidson_none", 0, None), ("mixed_davidson_jacobi", 1, None),
+                         ("mixed_davidson_learned", 2, mlp)):
+        if pre == 2 and mlp is None:
+            continue
+        bmx.set_precision(plugin.TF32X3)
+        (ed, zd, sd), td = _timed(lambda: bmx.davidson_lowest(
+            x, preconditioner=pre, mlp=m, tolerance=1e-9, max_iterations=4000,
+            raise_on_no_convergence=False))
+        rec[name] = dict(energy=ed, seconds=td, iterations=sd["iterations"],
+                         converged=sd["converged"], abs_dE_per_site=abs(ed - e64) / sites)
+    bmx.close()
+    rec["speedup_mixed_vs_fp64"] = t64 / tmx
+    rec["speedup_with_setup"] = (t64 + t_set64) / (tmx + t_setmx)
+    return e, z.cpu().numpy(), rec
+
+
+def ladder_mlp(train_specs=((12, 400), (16, 600)), test_specs=((16, 1000),), sectors_per_run=3,
+               out_path=None, log=print):
+    """The learned correction trained on real ladder superblocks: two-leg
+    Hubbard ladders (U=8, filling 0.875) of Lx rungs run at m states (mixed
+    solves); the last sectors_per_run finite-step sectors of each training
+    run give solver-generated (features, exact correction) pairs
+    (dmrgpp_b200.mlp.correction_pairs), the 3 x 256 network is trained by the
+    library's kernels, and on the test runs' sectors Davidson runs to
+    |r| <= 1e-9 |E| with no correction, the Jacobi correction and the learned
+    one (TF32x3 matvecs, FP64 restart phase) are counted and timed.  Returns
+    the summary; writes the weights to out_path."""
+    import torch
+    from dmrgpp_b200 import plugin
+    from dmrgpp_b200.mlp import MLPPreconditioner, correction_pairs, train
+
+    def sectors(Lx, m):
+        kept = []
+
+        def on_sector(prob, init, q):
+            x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
+            bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+            try:
+                e, z, n, st = mixed_solve(bg, x, 2 * Lx)
+            finally:
+                bg.close()
+            kept.append((prob, init))
+            return e, z.cpu().numpy(), None
+        # electrons scaled to 0.875 filling, Sz = 0
+        ne = int(round(0.875 * 2 * Lx / 2)) * 2
+        ladder_sectors(Lx=Lx, electrons=ne, m_inf=m, m=m, finite_steps=sectors_per_run,
+                       on_sector=on_sector, log=lambda *a: None)
+        return kept
+
+    t0 = time.time()
+    Xs, Ys, infos = [], [], []
+    for Lx, m in train_specs:
+        for prob, init in sectors(Lx, m):
+            bg = plugin.BatchedGemm.from_problem(prob)
+            x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
+            for xx, yy, info in correction_pairs(bg, x):
+                Xs.append(xx)
+                Ys.append(yy)
+                infos.append(info)
+            bg.close()
+        log(f"training data: Lx={Lx} m={m}: {sum(x.shape[0] for x in Xs)} rows "
+            f"({time.time() - t0:.0f} s)")
+    X = torch.cat(Xs)
+    Y = torch.cat(Ys).clamp(-20, 20)
+    mlp = MLPPreconditioner(seed=2026)
+    losses = train(mlp, X, Y, steps=800, batch=8192, lr=2e-3)
+    if out_path:
+        mlp.save(out_path)
+    summary = dict(rows=int(X.shape[0]), loss_first=float(np.mean(losses[:20])),
+                   loss_last=float(np.mean(losses[-20:])),
+                   cos_exact_vs_jacobi=float(np.mean([i["cos_jacobi"] for i in infos])),
+                   cos_exact_vs_residual=float(np.mean([i["cos_residual"] for i in infos])),
+                   train_seconds=time.time() - t0, held_out=[])
+    for Lx, m in test_specs:
+        for prob, init in sectors(Lx, m):
+            bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+            x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
+            rec = dict(Lx=Lx, m=m, dim=prob.dim)
+            for name, pre, mm in (("none", 0, None), ("jacobi", 1, None), ("learned", 2, mlp)):
+                (e, z, st), t = _timed(lambda: bg.davidson_lowest(
+                    x, preconditioner=pre, mlp=mm, tolerance=1e-9, max_iterations=4000,
+                    raise_on_no_convergence=False))
+                rec[name] = dict(energy=e, seconds=t, iterations=st["iterations"],
+                                 converged=st["converged"])
+            bg.set_precision(plugin.FP64)
+            (e, z, st), t = _timed(lambda: bg.davidson_lowest(
+                x, preconditioner=1, tolerance=1e-9, max_iterations=4000,
+                raise_on_no_convergence=False))
+            rec["fp64_jacobi"] = dict(energy=e, seconds=t, iterations=st["iterations"],
+                                      converged=st["converged"])
+            bg.close()
+            summary["held_out"].append(rec)
+            log(json.dumps(rec, default=float))
+    mlp.close()
+    return summary
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("what", choices=["c3", "ladder", "ladder-mlp"])
+    p.add_argument("--L", type=int, default=64)
+    p.add_argument("--m", type=int, default=None)
+    p.add_argument("--sweeps", type=int, default=6)
+    p.add_argument("--Lx", type=int, default=32)
+    p.add_argument("--m-inf", type=int, default=1000)
+    p.add_argument("--steps", type=int, default=2)
+    p.add_argument("--no-fp64-run", action="store_true")
+    p.add_argument("--mlp", default=None, help="learned-correction weights (.npz)")
+    p.add_argument("--out", default=None)
+    a = p.parse_args(argv)
+    if a.what == "ladder-mlp":
+        out = ladder_mlp(out_path=a.mlp)
+        print(json.dumps({k: v for k, v in out.items() if k != "held_out"}, default=float))
+        for r in out["held_out"]:
+            print(json.dumps(r, default=float))
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(out, f, indent=1, default=float)
+        return
+    if a.what == "c3":
+        out = c3(L=a.L, m=a.m or 1000, sweeps=a.sweeps, fp64_run=not a.no_fp64_run)
+    else:
+        from dmrgpp_b200.mlp import MLPPreconditioner
+        mlp = MLPPreconditioner.load(a.mlp) if a.mlp else None
+        L = 2 * a.Lx
+        recs = ladder_sectors(Lx=a.Lx, m_inf=a.m_inf, m=a.m or 4000, finite_steps=a.steps,
+                              on_sector=lambda prob, init, q: ladder_step_measurement(
+                                  prob, init, L, mlp=mlp))
+        out = dict(config=f"Hubbard ladder {a.Lx}x2 U=8 56 electrons, m_inf={a.m_inf}, "
+                          f"m={a.m or 4000}, {a.steps} finite steps", steps=recs)
+    text = json.dumps(out, indent=1, default=float)
+    if a.out:
+        with open(a.out, "w") as f:
+            f.write(text)
+    summary = {k: v for k, v in out.items() if k not in ("per_step", "steps")}
+    print(json.dumps(summary, default=float))
+    if a.what == "ladder":
+        for r in out["steps"]:
+            print(json.dumps({k: v for k, v in r.items()}, default=float))
+
+
+if __name__ == "__main__":
+    main()

@@ -11,7 +11,8 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = "/root/reference/dmrg/Engine/tests/test_KronConnections.cpp"
+SRC = os.path.join(os.environ.get("DMRGPP_REFERENCE_TREE", "/root/reference"),
+                   "dmrg", "Engine", "tests", "test_KronConnections.cpp")
 CPLX = r"ComplexType\(\s*([-0-9.]+)\s*,\s*([-0-9.]+)\s*\)"
 
 

@@ -26,7 +26,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+REF = os.environ.get("DMRGPP_REFERENCE_TREE", "/root/reference")  # read-only source tree
 sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402

@@ -39,3 +39,21 @@ def test_heisenberg_L32_golden_is_the_reference_value():
     g = json.load(open(os.path.join(GOLDEN, "dmrg_heisenberg_L32_m128.json")))
     assert abs(g["energy"] - g["reference_test_energy"]) < g["reference_test_tolerance"]
     assert len(g["energies"]) == 131
+
+
+@pytest.mark.parametrize("Lx,U,n", [(2, 4.0, 2), (3, 8.0, 3), (4, 8.0, 3)])
+def test_hubbard_ladder_matches_exact_diagonalisation(Lx, U, n):
+    """Two-leg ladder in the reference's site order (Ladder.h:87-292: rungs
+    (2c, 2c+1), legs (i, i+2)): blocks carry their last two sites'
+    operators; with every state kept the DMRG energy is the Fock-space exact
+    energy of the same bond list."""
+    mdl = dd.HubbardLadder(Lx, U=U, n_up=n, n_dn=n)
+    exact = dd.hubbard_ed(2 * Lx, U, n, n, bonds=mdl.bonds())
+    d = dd.DMRG(mdl, L=2 * Lx, m=400, solver=dd.dense_solver())
+    assert abs(d.run(sweeps=1) - exact) < 1e-11
+
+
+def test_ladder_bonds_follow_the_reference_geometry():
+    mdl = dd.HubbardLadder(3)
+    assert mdl.bonds() == [(0, 1, 1.0), (0, 2, 1.0), (1, 3, 1.0), (2, 3, 1.0), (2, 4, 1.0),
+                           (3, 5, 1.0), (4, 5, 1.0)]

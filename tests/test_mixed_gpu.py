@@ -117,3 +117,27 @@ def test_k_split_pass2_on_a_small_sector(cuda_lib, cuda_device, oracle_built):
     for _ in range(3):
         assert np.array_equal(bg(x), y)
     bg.close()
+
+
+def test_refinement_from_a_start_without_reorthogonalisation(cuda_lib, cuda_device):
+    """The shipped single-sector mixed solve: TF32x3 Lanczos without
+    reorthogonalisation to a 1e-4 Ritz-value change, then the FP64 residual
+    refinement (TF32x3 correction solves).  On a ladder-shaped sector it
+    converges and agrees with the plain FP64 Lanczos (full
+    reorthogonalisation) to 1e-9 per site (64 sites)."""
+    import torch
+    from dmrgpp_b200 import plugin
+    prob = sb.ladder_problem(total_states=2000, sigma=2.0, seed=4)
+    init = torch.from_numpy(np.random.default_rng(9).standard_normal(prob.dim)).cuda()
+    ref = plugin.BatchedGemm.from_problem(prob)
+    e_ref, z_ref, _ = ref.lanczos_lowest(init, steps=400, tolerance=1e-12)
+    ref.close()
+    bg = mixed(prob)
+    e1, z1, n1 = bg.lanczos_lowest(init, steps=60, tolerance=1e-4, reortho=False)
+    e2, st = bg.refine_lowest(z1, max_outer=12, tolerance=1e-10, inner_iterations=80,
+                              inner_tolerance=1e-2)
+    bg.close()
+    assert st["converged"]
+    assert abs(e2 - e_ref) / 64 <= 1e-9, (e2, e_ref)
+    overlap = abs(float(torch.dot(z1, z_ref)))
+    assert 1.0 - overlap < 1e-8

@@ -5,6 +5,8 @@ import json
 import os
 
 import numpy as np
+
+import oracle
 import pytest
 
 from dmrgpp_b200 import superblock as sb
@@ -66,7 +68,7 @@ def test_zero_and_missing_blocks_do_not_contribute(oracle_built):
     np.testing.assert_allclose(y, prob.dense() @ x, rtol=1e-13)
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference") and
+@pytest.mark.skipif(not os.path.isdir(oracle.REFERENCE_TREE) and
                     not os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle",
                                                     "_ref", "libref_kron.so")),
                     reason="reference harness not built")
@@ -80,7 +82,7 @@ def test_oracle_vs_reference_batched_gemm_cpu(oracle_built, seed):
     np.testing.assert_allclose(y, y_ref, rtol=1e-12, atol=1e-13)
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference") and
+@pytest.mark.skipif(not os.path.isdir(oracle.REFERENCE_TREE) and
                     not os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle",
                                                     "_ref", "libref_kron.so")),
                     reason="reference harness not built")
