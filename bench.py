@@ -155,10 +155,12 @@ def cpu_baseline(prob, f_alg, calls=30):
             ts.append(time.perf_counter() - t0)
         t = statistics.median(ts)
         cores = int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
-        return {"value": f_alg / t / 1e12, "unit": UNIT, "cores": cores, "kind": "reference",
-                "sample": f"median of {calls} full matvecs of the same sector by "
-                          "Dmrg::BatchedGemmCpu::matrixVector (OpenBLAS dgemm)",
-                "s_per_matvec": t}
+        out = {"value": f_alg / t / 1e12, "unit": UNIT, "cores": cores, "kind": "reference",
+               "sample": f"median of {calls} full matvecs of the same sector by "
+                         "Dmrg::BatchedGemmCpu::matrixVector (OpenBLAS dgemm)",
+               "s_per_matvec": t}
+        out["nonbatched"] = nonbatched_cpu(prob, f_alg, calls)
+        return out
     oracle.build()
     calls = 3
     oracle.kron_apply(prob, x)
@@ -171,6 +173,29 @@ def cpu_baseline(prob, f_alg, calls=30):
     return {"value": f_alg / t / 1e12, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"median of {calls} full matvecs by the scalar C restatement",
             "s_per_matvec": t}
+
+
+def nonbatched_cpu(prob, f_alg, calls=30):
+    """The reference's default non-batched CPU H*x (KronConnections::doTask
+    with den_kron_mult per block, compiled from its sources into oracle/_ref)
+    with one task thread per host core and one BLAS thread each; median of
+    `calls` matvecs after one warm-up."""
+    import oracle
+    x = np.random.default_rng(7).standard_normal(prob.dim)
+    kc = oracle.RefKronConn(prob)
+    cores = os.cpu_count() or 1
+    kc.apply(x, threads=cores)
+    ts = []
+    for _ in range(calls):
+        t0 = time.perf_counter()
+        kc.apply(x, threads=cores)
+        ts.append(time.perf_counter() - t0)
+    kc.close()
+    t = statistics.median(ts)
+    return {"value": f_alg / t / 1e12, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"median of {calls} full matvecs by KronConnections::doTask over the "
+                      "output patches with den_kron_mult per block (the reference's default "
+                      "path)", "s_per_matvec": t}
 
 
 def run_reference(args):
@@ -322,7 +347,8 @@ def learned_ablation(torch, bgm, init, stream):
                     "of the batch"}
 
 
-def serving_measurements(torch, dev, stream, cpu_sample: bool = True):
+def serving_measurements(torch, dev, stream, cpu_sample: bool = True, probs=None, meta=None,
+                         workload=None):
     """Serving-style batch: 256 independent ground-state problems (Heisenberg
     and Hubbard chain-shaped sectors, L in [16, 48], m in {64, 128, 256, 512},
     superblock.serving_batch) solved together by the group Lanczos (one
@@ -332,15 +358,18 @@ def serving_measurements(torch, dev, stream, cpu_sample: bool = True):
     (TF32x3 group Lanczos + lockstep FP64 group refinement) with |dE| per site
     and 1 - |<psi|psi_FP64>| against the single-problem FP64 solves; the
     reference's own LanczosSolver + BatchedGemmCpu (oracle/_ref) timed on a
-    sample of the batch."""
+    sample of the batch.  probs / meta (with "L" per problem) replace the
+    synthetic batch when given (the physical batch of real superblocks)."""
     from dmrgpp_b200 import plugin
     from dmrgpp_b200 import superblock as sb
-    probs, meta = sb.serving_batch(256)
+    if probs is None:
+        probs, meta = sb.serving_batch(256)
+        workload = ("serving-batch-256 (Heisenberg / Hubbard chain-shaped sectors, "
+                    "L 16-48, m 64-512, seeded N(0,1) blocks)")
     bg = plugin.BatchedGemm.from_problems(probs, stream=stream.cuda_stream)
     offs = bg.sector_offsets()
     init = torch.from_numpy(np.random.default_rng(1).standard_normal(bg.dim)).to(dev)
-    out = {"workload": "serving-batch-256 (Heisenberg / Hubbard chain-shaped sectors, "
-                       "L 16-48, m 64-512, seeded N(0,1) blocks)",
+    out = {"workload": workload,
            "problems": len(probs), "total_dim": int(bg.dim), "f_alg_per_group_matvec": bg.f_alg}
     x, y = init.clone(), torch.empty_like(init)
     with torch.cuda.stream(stream):
@@ -495,6 +524,9 @@ def ladder_measurements(torch, dev, stream):
         out[f"matvec_{name}"] = {"ms": t * 1e3, "tflops_alg": f / t / 1e12}
     bg.close()
     out["matvec_speedup_tf32x3_vs_fp64"] = out["matvec_fp64"]["ms"] / out["matvec_tf32x3"]["ms"]
+    # the reference's default CPU path on this sector (its batched path's
+    # dense nL x (nL K) slabs would need ~20 GB here)
+    out["cpu_nonbatched_matvec"] = nonbatched_cpu(prob, f, calls=3)
     out["solve"] = sweep.sector_solves(prob, sites=64, mixed_steps=60, refine_inner=80,
                                        refine_inner_tolerance=1e-2,
                                        with_davidson=False)

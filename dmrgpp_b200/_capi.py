@@ -197,6 +197,10 @@ SIGNATURES.update({
                                       ctypes.c_void_p]),
     "dmrgpp_kron_gather_index": (ctypes.c_int, [ctypes.POINTER(GatherIndexDesc),
                                                 ctypes.POINTER(ctypes.c_int64)]),
+    "dmrgpp_kron_patch_list": (ctypes.c_int, [_sz, ctypes.POINTER(ctypes.c_int64), _sz,
+                                              ctypes.POINTER(ctypes.c_int64), _sz,
+                                              ctypes.POINTER(ctypes.c_int64), _sz, _szp, _szp,
+                                              _szp]),
 })
 
 

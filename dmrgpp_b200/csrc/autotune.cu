@@ -1,12 +1,13 @@
-// Autotuner of the persistent H*x launch.
+// Autotuner of the FP64 H*x launch.
 //
 // The reference hard-codes its GPU tiling ("tuned" constants for one GH200
 // input, BatchedGemmKokkos.h:110-130).  Here each sector is timed under every
-// tile configuration (kron_persistent.cuh) and work split (pass-2 items per
-// CTA), the fastest is kept, and the choice is cached in a text file keyed
-// by a signature of the sector-size histogram (patch sizes, Kronecker terms,
-// contributing triples) and the GPU name, so that sectors of the same shape
-// in later sweep steps or runs skip the timing.
+// configuration (the persistent two-pass form's tiles and work splits, the
+// fused form's where its patches are narrow enough), the fastest is kept,
+// and the choice is cached in a text file keyed by a bucketed histogram of
+// the sector's shape (patch sizes, contributing triples, Kronecker terms)
+// and the GPU name, so that sectors of similar shape in later sweep steps or
+// runs skip the timing.
 #include "dmrgpp_kron.h"
 #include "handle.h"
 #include "kron_fused.cuh"
@@ -15,6 +16,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
+#include <map>
+#include <utility>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -26,9 +30,27 @@ namespace {
 
 using dmrgpp::KronPlan;
 
-// FNV-1a over the sector's shape
+// FNV-1a over a bucketed histogram of the sector's shape: patches counted
+// by (l, r) in buckets of a quarter octave each, contributing triples
+// counted by (l_i, l_j) the same way, the number of terms, and the GPU name.
+// Consecutive sweep steps change patch sizes by a few states, which mostly
+// stays inside the buckets, so their sectors share a tuning entry.
+int size_bucket(long long n)
+{
+	if (n <= 8)
+		return int(n);
+	// 4 buckets per factor of two above 8
+	const double b = 4.0 * std::log2(double(n) / 8.0);
+	return 8 + int(b);
+}
+
 std::string sector_signature(const KronPlan& P, const char* gpu)
 {
+	std::map<std::pair<int, int>, long long> patches, triples;
+	for (size_t p = 0; p < P.np; ++p)
+		patches[{ size_bucket(P.l[p]), size_bucket(P.r[p]) }]++;
+	for (const auto& t : P.triples)
+		triples[{ size_bucket(P.l[size_t(t.i)]), size_bucket(P.l[size_t(t.j)]) }]++;
 	unsigned long long h   = 1469598103934665603ull;
 	auto               mix = [&](unsigned long long v) {
                 for (int b = 0; b < 8; ++b) {
@@ -36,15 +58,18 @@ std::string sector_signature(const KronPlan& P, const char* gpu)
                         h *= 1099511628211ull;
                 }
 	};
-	mix(P.np);
+	// counts bucketed too (a quarter octave), so a patch more or less in a
+	// populated bucket keeps the key
 	mix(P.nop);
-	for (size_t p = 0; p < P.np; ++p) {
-		mix((unsigned long long)P.l[p]);
-		mix((unsigned long long)P.r[p]);
+	for (const auto& kv : patches) {
+		mix((unsigned long long)kv.first.first << 32 | (unsigned)kv.first.second);
+		mix((unsigned long long)size_bucket(kv.second));
 	}
-	mix(P.triples.size());
-	for (const auto& t : P.triples)
-		mix((unsigned long long)(t.i * 65536 + t.j));
+	mix(0xfffffffffull);
+	for (const auto& kv : triples) {
+		mix((unsigned long long)kv.first.first << 32 | (unsigned)kv.first.second);
+		mix((unsigned long long)size_bucket(kv.second));
+	}
 	for (const char* c = gpu; *c; ++c)
 		mix((unsigned long long)(unsigned char)*c);
 	char buf[32];

@@ -15,6 +15,7 @@
 #include "kron_plan.h"
 
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -79,5 +80,46 @@ extern "C" int dmrgpp_kron_gather_index(const dmrgpp_gather_index_desc* d, int64
 			                   "two patch-order elements map to sector position " + std::to_string(idx[q]));
 		seen[size_t(idx[q])] = 1;
 	}
+	return DMRGPP_OK;
+}
+
+// GenIjPatch::GenIjPatch (dmrg/Engine/MatrixVectorKron/GenIjPatch.h:104-118):
+// every (left group i, right group j), i outer and j inner, whose quantum
+// numbers combine to the target.  The quantum numbers are additive vectors
+// of qn_len integers per group (Sz, particle numbers, ...); the right groups
+// are indexed by quantum number, so the search is linear in the groups.
+extern "C" int dmrgpp_kron_patch_list(size_t left_groups, const int64_t* left_qn, size_t right_groups,
+                                      const int64_t* right_qn, size_t qn_len, const int64_t* target,
+                                      size_t capacity, size_t* patch_left, size_t* patch_right,
+                                      size_t* npatches)
+{
+	using dmrgpp::handle_fail;
+	if (!npatches || (left_groups && !left_qn) || (right_groups && !right_qn) || (qn_len && !target)
+	    || (capacity && (!patch_left || !patch_right)))
+		return handle_fail(nullptr, DMRGPP_INVALID_ARG, "null array in the patch-list arguments");
+	std::map<std::vector<int64_t>, std::vector<size_t>> by_qn;
+	for (size_t j = 0; j < right_groups; ++j)
+		by_qn[std::vector<int64_t>(right_qn + j * qn_len, right_qn + (j + 1) * qn_len)].push_back(j);
+	size_t              n = 0;
+	std::vector<int64_t> need(qn_len);
+	for (size_t i = 0; i < left_groups; ++i) {
+		for (size_t c = 0; c < qn_len; ++c)
+			need[c] = target[c] - left_qn[i * qn_len + c];
+		auto f = by_qn.find(need);
+		if (f == by_qn.end())
+			continue;
+		for (size_t j : f->second) {
+			if (n < capacity) {
+				patch_left[n]  = i;
+				patch_right[n] = j;
+			}
+			++n;
+		}
+	}
+	*npatches = n;
+	if (n > capacity)
+		return handle_fail(nullptr, DMRGPP_INVALID_ARG,
+		                   "the sector has " + std::to_string(n) + " patches, more than the capacity "
+		                       + std::to_string(capacity));
 	return DMRGPP_OK;
 }

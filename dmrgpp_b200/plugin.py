@@ -548,3 +548,24 @@ def sector_gather_index(patch_left, patch_right, left_partition, right_partition
     _capi.check(_capi.lib().dmrgpp_kron_gather_index(
         ctypes.byref(d), idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
     return idx
+
+
+def sector_patches(left_qns, right_qns, target):
+    """The sector's patches (dmrgpp_kron_patch_list, host only): left_qns and
+    right_qns are the blocks' group quantum numbers (tuples of additive
+    integers, one per group), target the sector's.  Returns (patch_left,
+    patch_right) arrays, left group outer, right group inner."""
+    q = len(target)
+    lq = np.ascontiguousarray(np.asarray(left_qns, dtype=np.int64).reshape(-1, q))
+    rq = np.ascontiguousarray(np.asarray(right_qns, dtype=np.int64).reshape(-1, q))
+    t = np.ascontiguousarray(np.asarray(target, dtype=np.int64))
+    cap = len(lq) * max(len(rq), 1)
+    pl = np.empty(max(cap, 1), dtype=np.uint64)
+    pr = np.empty(max(cap, 1), dtype=np.uint64)
+    n = ctypes.c_size_t()
+    i64 = ctypes.POINTER(ctypes.c_int64)
+    szp = ctypes.POINTER(ctypes.c_size_t)
+    _capi.check(_capi.lib().dmrgpp_kron_patch_list(
+        len(lq), lq.ctypes.data_as(i64), len(rq), rq.ctypes.data_as(i64), q, t.ctypes.data_as(i64),
+        cap, pl.ctypes.data_as(szp), pr.ctypes.data_as(szp), ctypes.byref(n)))
+    return pl[:n.value].astype(np.int64), pr[:n.value].astype(np.int64)

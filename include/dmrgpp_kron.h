@@ -536,6 +536,17 @@ typedef struct {
 
 int dmrgpp_kron_gather_index(const dmrgpp_gather_index_desc* desc, int64_t* idx);
 
+/* The sector's patches (GenIjPatch::GenIjPatch, GenIjPatch.h:104-118): every
+ * (left group i, right group j), i outer and j inner, whose quantum numbers
+ * add up to the target.  left_qn / right_qn: qn_len integers per group
+ * (additive components: 2 Sz, N_up, N_down, ...), target: qn_len integers.
+ * Writes up to capacity pairs, the count to *npatches; DMRGPP_INVALID_ARG if
+ * there are more.  Host only. */
+int dmrgpp_kron_patch_list(size_t left_groups, const int64_t* left_qn, size_t right_groups,
+                           const int64_t* right_qn, size_t qn_len, const int64_t* target,
+                           size_t capacity, size_t* patch_left, size_t* patch_right,
+                           size_t* npatches);
+
 /* ---- Wave-function transformation between two patch layouts ----
  * The GEMM core of the reference's patch-wise WFT (Wft/WftAccelPatches.h:
  * 43-66, BlockDiagWf.h:131-260 ParallelBlockTransform::doTask): per patch,

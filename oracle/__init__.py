@@ -9,6 +9,9 @@ CPU checkers for the Kronecker H*psi path:
   ``Dmrg::BatchedGemmCpu`` and ``PsimagLite::LanczosSolver`` compiled from
   the reference sources (built here only when the reference tree exists; the
   built file travels with the repository snapshot).
+* ``_ref/libref_kronconn.so`` (``kronconn_harness.cpp``): the reference's
+  default non-batched H*x, ``KronConnections::doTask`` over the output
+  patches with the reference's ``den_kron_mult`` per block.
 * ``lanczos_oracle``: a numpy restatement of PsimagLite's Lanczos.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
@@ -26,6 +29,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle_kron.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_kron.so")
+REF_KC_SO = os.path.join(HERE, "_ref", "libref_kronconn.so")
 # the reference source tree (read-only); only the build recipe reads it
 REFERENCE_TREE = os.environ.get("DMRGPP_REFERENCE_TREE", "/root/reference")
 
@@ -40,7 +44,8 @@ def build(force: bool = False) -> None:
     the reference harness."""
     if force or not os.path.exists(ORACLE_SO):
         subprocess.run(["make", "-s", "-C", HERE, "liboracle_kron.so"], check=True)
-    if os.path.isdir(REFERENCE_TREE) and (force or not os.path.exists(REF_SO)):
+    if os.path.isdir(REFERENCE_TREE) and (force or not os.path.exists(REF_SO)
+                                          or not os.path.exists(REF_KC_SO)):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + REFERENCE_TREE], check=True)
 
 
@@ -154,6 +159,54 @@ def gather_index(npatches, left_part, right_part, patch_left, patch_right, nl, p
         idx.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
     assert n == dim
     return idx
+
+
+_ref_kc = None
+
+
+def ref_kronconn_lib():
+    global _ref_kc
+    if _ref_kc is None:
+        ref_lib()          # loads the BLAS's Fortran runtime first
+        lib = _load(REF_KC_SO)
+        lib.ref_kronconn_create.argtypes = [_sz, _sz, _szp, _szp, _vpp, _szp, _vpp, _szp]
+        lib.ref_kronconn_create.restype = ctypes.c_void_p
+        lib.ref_kronconn_apply.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int]
+        lib.ref_kronconn_apply.restype = None
+        lib.ref_kronconn_destroy.argtypes = [ctypes.c_void_p]
+        _ref_kc = lib
+    return _ref_kc
+
+
+class RefKronConn:
+    """The reference's default non-batched H*x for one sector
+    (KronConnections::doTask with den_kron_mult per block, oracle/_ref);
+    fits sectors whose BatchedGemmCpu slabs would not."""
+
+    def __init__(self, prob):
+        t = _Tables(prob)
+        self.dim = prob.dim
+        self.lib = ref_kronconn_lib()
+        self.h = self.lib.ref_kronconn_create(*t.args())   # copies the blocks
+
+    def apply(self, x: np.ndarray, threads: int = 1, y: Optional[np.ndarray] = None) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if y is None:
+            y = np.empty(self.dim)
+        self.lib.ref_kronconn_apply(self.h, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp),
+                                    int(threads))
+        return y
+
+    def close(self):
+        if self.h:
+            self.lib.ref_kronconn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class RefKron:

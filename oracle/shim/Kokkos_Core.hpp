@@ -1,8 +1,10 @@
-// Host-only stand-in for the three Kokkos names that the reference's CPU
-// batched-GEMM path and PsimagLite's Lanczos solver mention when compiled
-// without Kokkos.  Test infrastructure for the oracle build only.
+// Host-only stand-in for the Kokkos names that the reference's CPU paths
+// mention when compiled without Kokkos (the batched-GEMM path, PsimagLite's
+// Lanczos solver, and PsimagLite's thread pool with one host execution
+// space per thread).  Test infrastructure for the oracle build only.
 #pragma once
 #include <complex>
+#include <vector>
 namespace Kokkos {
 struct DefaultExecutionSpace {};
 template <class T> using complex = std::complex<T>;
@@ -11,4 +13,11 @@ inline void finalize() {}
 struct ScopeGuard {
 	ScopeGuard(int&, char**) {}
 };
+namespace Experimental {
+template <class Space>
+std::vector<Space> partition_space(const Space&, const std::vector<int>& weights)
+{
+	return std::vector<Space>(weights.size());
+}
+} // namespace Experimental
 } // namespace Kokkos

@@ -3,9 +3,10 @@ sector eigensolve on the GPU (test infrastructure: the sweep engine is the
 oracle's two-site driver, oracle/dmrg_driver.py).
 
     python tests/dmrg_runs.py c3 [--L 64 --m 1000 --sweeps 6] [--out run.json]
-    python tests/dmrg_runs.py ladder [--Lx 32 --m-inf 1000 --m 4000 --steps 2] [--mlp w.npz]
+    python tests/dmrg_runs.py ladder [--Lx 32 --m-inf 4000 --m 4000 --steps 1] [--mlp w.npz]
                                     [--out run.json]
     python tests/dmrg_runs.py ladder-mlp --mlp w.npz [--out run.json]
+    python tests/dmrg_runs.py serving [--out run.json]
 
 c3: Fermi-Hubbard chain, t=1, U=4, open BC, half filling, m states kept, the
     given finite sweeps.  The trajectory follows the mixed-precision solve
@@ -17,7 +18,8 @@ c3: Fermi-Hubbard chain, t=1, U=4, open BC, half filling, m states kept, the
     gives the final-energy comparison of the two runs.
 ladder: two-leg Hubbard ladder Lx x 2, t_leg = t_rung = 1, U=8, 56 electrons
     (Sz=0) on 64 sites; infinite growth at m_inf states, then finite steps at
-    m states.  Each finite step's sector is solved by the plain FP64 Lanczos
+    m states (or, with m_inf = m, the last infinite-growth steps measured:
+    their blocks hold ~4 m states each, as in a sweep at m).  Each finite step's sector is solved by the plain FP64 Lanczos
     (its own FP64 handle), by TF32x3 Lanczos + FP64 refinement, by the FP64
     Jacobi-preconditioned Davidson and by the mixed Davidson with the learned
     correction (weights trained on this ladder at m <= 1000); seconds (device
@@ -94,7 +96,8 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print):
         return e, z.cpu().numpy(), n1
 
     t0 = time.time()
-    d = dd.DMRG(dd.Hubbard(U=U, n_up=L // 2, n_dn=L // 2), L=L, m=m, solver=solve)
+    # half filling at every stage (the model scales the target with the sites)
+    d = dd.DMRG(dd.Hubbard(U=U), L=L, m=m, solver=solve)
     e_mixed = d.run(sweeps=sweeps)
     out = dict(config=f"Hubbard chain L={L} U={U} half filling m={m} {sweeps} finite sweeps",
                steps=len(steps), final_energy_mixed_run=e_mixed,
@@ -117,19 +120,24 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print):
                 bg.close()
             n64.append(n)
             return e, z, n
-        d64 = dd.DMRG(dd.Hubbard(U=U, n_up=L // 2, n_dn=L // 2), L=L, m=m, solver=solve64)
+        d64 = dd.DMRG(dd.Hubbard(U=U), L=L, m=m, solver=solve64)
         e64 = d64.run(sweeps=sweeps)
         out.update(final_energy_fp64_run=e64, final_abs_dE_per_site=abs(e_mixed - e64) / L,
                    wall_seconds_fp64_run=time.time() - t1)
     return out
 
 
-def ladder_model(Lx=32, U=8.0, electrons=56):
-    return dd.HubbardLadder(Lx, t_leg=1.0, t_rung=1.0, U=U, n_up=electrons // 2,
-                            n_dn=electrons // 2)
+def ladder_electrons(Lx):
+    """Filling 0.875 with Sz = 0 (56 electrons on 32 x 2 sites)."""
+    return int(round(0.875 * 2 * Lx / 2)) * 2
 
 
-def ladder_sectors(Lx=32, U=8.0, electrons=56, m_inf=1000, m=4000, finite_steps=2,
+def ladder_model(Lx=32, U=8.0, electrons=None):
+    ne = electrons if electrons is not None else ladder_electrons(Lx)
+    return dd.HubbardLadder(Lx, t_leg=1.0, t_rung=1.0, U=U, n_up=ne // 2, n_dn=ne // 2)
+
+
+def ladder_sectors(Lx=32, U=8.0, electrons=None, m_inf=1000, m=4000, finite_steps=2,
                    on_sector=None, log=print):
     """Runs the ladder's infinite growth at m_inf (mixed solves), then
     finite_steps left-to-right steps from the middle at m states; calls
@@ -175,6 +183,47 @@ def ladder_sectors(Lx=32, U=8.0, electrons=56, m_inf=1000, m=4000, finite_steps=
             rho_l[gl] = rho_l.get(gl, 0.0) + X.T @ X
         left[nl + 1] = d.truncate(lp, rho_l)
         log(f"finite step {q}: E {e:.10f} dim {prob.dim} left states {sum(lp.sizes)}")
+    return records
+
+
+def ladder_infinite(Lx=32, U=8.0, m=4000, measure_last=1, on_sector=None, log=print):
+    """Infinite growth of the ladder at m states to 2 Lx sites (mixed solves);
+    the last measure_last steps (blocks of ~4 m states each once m is
+    reached: the superblocks of a sweep at m) go to on_sector(prob, init, q),
+    which returns (energy, state, record)."""
+    import torch
+    from dmrgpp_b200 import plugin
+    L = 2 * Lx
+
+    def solve(prob, init):
+        x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
+        bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+        try:
+            e, z, n, st = mixed_solve(bg, x, L)
+        finally:
+            bg.close()
+        return e, z.cpu().numpy(), n
+
+    records = []
+    d = dd.DMRG(ladder_model(Lx, U), L=L, m=m, solver=solve)
+    b_l = b_r = d.site
+    nsteps = L // 2 - 1
+    for n in range(1, nsteps + 1):
+        t0 = time.time()
+        q = n - (nsteps - measure_last) - 1
+        if q >= 0:
+            def measured(prob, init, q=q):
+                e, z, rec = on_sector(prob, init, q)
+                rec["sites"] = 2 * (n + 1)
+                records.append(rec)
+                return e, z, 0
+            d.solver = measured
+        e, lp, rp, rl, rr = d.step(b_l, b_r, 2 * (n + 1))
+        d.solver = solve
+        if n < nsteps:
+            b_l, b_r = d.truncate(lp, rl), d.truncate(rp, rr)
+        log(f"infinite {n}: N {2 * (n + 1)} E {e:.10f} left states {sum(lp.sizes)} "
+            f"({time.time() - t0:.1f} s)")
     return records
 
 
@@ -253,9 +302,7 @@ def ladder_mlp(train_specs=((12, 400), (16, 600)), test_specs=((16, 1000),), sec
                 bg.close()
             kept.append((prob, init))
             return e, z.cpu().numpy(), None
-        # electrons scaled to 0.875 filling, Sz = 0
-        ne = int(round(0.875 * 2 * Lx / 2)) * 2
-        ladder_sectors(Lx=Lx, electrons=ne, m_inf=m, m=m, finite_steps=sectors_per_run,
+        ladder_sectors(Lx=Lx, m_inf=m, m=m, finite_steps=sectors_per_run,
                        on_sector=on_sector, log=lambda *a: None)
         return kept
 
@@ -307,9 +354,88 @@ def ladder_mlp(train_specs=((12, 400), (16, 600)), test_specs=((16, 1000),), sec
     return summary
 
 
+def serving_problems(n=256, seed=20261203, log=print):
+    """The serving-style batch built from real DMRG superblocks: n problems,
+    each a Heisenberg (J=1) or Hubbard (t=1, U uniform in [0, 8]) chain
+    (seeded coin) with L uniform in [16, 48] (rounded down to even) and m from
+    {64, 128, 256, 512}; its sector is the last infinite-growth superblock
+    (N = L sites, Sz = 0 or half filling) of a driver run at m states (mixed
+    solves along the way).  Heisenberg problems of one m share one run to
+    their largest L.  Returns (probs, meta)."""
+    import torch
+    from dmrgpp_b200 import plugin
+    rng = np.random.default_rng(seed)
+    specs = []
+    for q in range(n):
+        L = int(rng.integers(16, 49)) // 2 * 2
+        m = int(rng.choice([64, 128, 256, 512]))
+        if rng.random() < 0.5:
+            specs.append(("heisenberg", L, 0.0, m))
+        else:
+            specs.append(("hubbard", L, float(rng.uniform(0.0, 8.0)), m))
+
+    def solve(prob, init):
+        x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
+        bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
+        try:
+            e, z, nn, st = mixed_solve(bg, x, 1)
+        finally:
+            bg.close()
+        return e, z.cpu().numpy(), nn
+
+    def run(model, Lmax, m, wanted):
+        d = dd.DMRG(model, L=Lmax, m=m, solver=solve)
+        got = {}
+        b_l = b_r = d.site
+        n_ = 1
+        while 2 * (n_ + 1) <= Lmax:
+            N = 2 * (n_ + 1)
+            if N in wanted:
+                d.keep_sectors = True
+            e, lp, rp, rl, rr = d.step(b_l, b_r, N)
+            if d.keep_sectors:
+                got[N] = d.sectors.pop()
+                d.keep_sectors = False
+            b_l, b_r = d.truncate(lp, rl), d.truncate(rp, rr)
+            n_ += 1
+        return got
+
+    t0 = time.time()
+    sectors = {}
+    for m in sorted({s[3] for s in specs if s[0] == "heisenberg"}):
+        Ls = {s[1] for s in specs if s[0] == "heisenberg" and s[3] == m}
+        for L, p in run(dd.Heisenberg(), max(Ls), m, Ls).items():
+            sectors[("heisenberg", L, 0.0, m)] = p
+    for q, s in enumerate(specs):
+        if s[0] == "hubbard":
+            sectors[s] = run(dd.Hubbard(U=s[2]), s[1], s[3], {s[1]})[s[1]]
+        if q % 32 == 31:
+            log(f"serving batch: {q + 1} problems ({time.time() - t0:.0f} s)")
+    probs = [sectors[s] for s in specs]
+    meta = [{"model": s[0], "L": s[1], "U": s[2], "m": s[3]} for s in specs]
+    return probs, meta
+
+
+def serving(n=256, log=print):
+    """bench.py's serving measurements on the batch of real superblocks."""
+    import torch
+    sys.path.insert(0, ROOT)
+    import bench
+    probs, meta = serving_problems(n, log=log)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    out = bench.serving_measurements(
+        torch, dev, stream, cpu_sample=True, probs=probs, meta=meta,
+        workload=f"serving-batch-{n} of real DMRG superblocks (Heisenberg / Hubbard chains, "
+                 "L 16-48, U 0-8, m 64-512, last infinite-growth sector)")
+    out["dims"] = {"min": int(min(p.dim for p in probs)), "max": int(max(p.dim for p in probs))}
+    return out
+
+
 def main(argv=None):
     p = argparse.ArgumentParser()
-    p.add_argument("what", choices=["c3", "ladder", "ladder-mlp"])
+    p.add_argument("what", choices=["c3", "ladder", "ladder-mlp", "serving"])
     p.add_argument("--L", type=int, default=64)
     p.add_argument("--m", type=int, default=None)
     p.add_argument("--sweeps", type=int, default=6)
@@ -320,6 +446,15 @@ def main(argv=None):
     p.add_argument("--mlp", default=None, help="learned-correction weights (.npz)")
     p.add_argument("--out", default=None)
     a = p.parse_args(argv)
+    if a.what == "serving":
+        out = serving()
+        text = json.dumps(out, indent=1, default=float)
+        if a.out:
+            with open(a.out, "w") as f:
+                f.write(text)
+        print(json.dumps({k: v for k, v in out.items() if k not in ("group_davidson",)},
+                         default=float))
+        return
     if a.what == "ladder-mlp":
         out = ladder_mlp(out_path=a.mlp)
         print(json.dumps({k: v for k, v in out.items() if k != "held_out"}, default=float))
@@ -335,11 +470,16 @@ def main(argv=None):
         from dmrgpp_b200.mlp import MLPPreconditioner
         mlp = MLPPreconditioner.load(a.mlp) if a.mlp else None
         L = 2 * a.Lx
-        recs = ladder_sectors(Lx=a.Lx, m_inf=a.m_inf, m=a.m or 4000, finite_steps=a.steps,
-                              on_sector=lambda prob, init, q: ladder_step_measurement(
-                                  prob, init, L, mlp=mlp))
-        out = dict(config=f"Hubbard ladder {a.Lx}x2 U=8 56 electrons, m_inf={a.m_inf}, "
-                          f"m={a.m or 4000}, {a.steps} finite steps", steps=recs)
+        measure = lambda prob, init, q: ladder_step_measurement(prob, init, L, mlp=mlp)
+        if a.m_inf == (a.m or 4000):
+            recs = ladder_infinite(Lx=a.Lx, m=a.m_inf, measure_last=a.steps, on_sector=measure)
+            how = f"infinite growth at m={a.m_inf}, the last {a.steps} steps measured"
+        else:
+            recs = ladder_sectors(Lx=a.Lx, m_inf=a.m_inf, m=a.m or 4000, finite_steps=a.steps,
+                                  on_sector=measure)
+            how = f"m_inf={a.m_inf}, then {a.steps} finite steps at m={a.m or 4000}"
+        out = dict(config=f"Hubbard ladder {a.Lx}x2, t_leg = t_rung = 1, U=8, "
+                          f"{ladder_electrons(a.Lx)} electrons (Sz=0); {how}", steps=recs)
     text = json.dumps(out, indent=1, default=float)
     if a.out:
         with open(a.out, "w") as f:

@@ -28,7 +28,8 @@ def sector_case(model: str, L: int, m: int, steps: int):
     perm, sectors = superbasis.product_permutation(lp.qns, lp.sizes, rp.qns, rp.sizes)
     offset, size = sectors[target]
     assert size == prob.dim
-    return dict(prob=prob, patch_left=[gl for gl, _ in patches],
+    return dict(prob=prob, left_qns=lp.qns, right_qns=rp.qns, target=target,
+                patch_left=[gl for gl, _ in patches],
                 patch_right=[gr for _, gr in patches],
                 left_partition=np.concatenate([[0], np.cumsum(lp.sizes)]).astype(np.uint64),
                 right_partition=np.concatenate([[0], np.cumsum(rp.sizes)]).astype(np.uint64),

@@ -75,3 +75,31 @@ def test_reference_assertions_become_errors():
     with pytest.raises(_capi.DmrgppError) as e:
         _product(bad)
     assert "patches hold" in str(e.value)
+
+
+@pytest.mark.parametrize("model,L,m,steps", CASES)
+def test_patch_list_matches_the_drivers_genijpatch(model, L, m, steps):
+    """dmrgpp_kron_patch_list against the DMRG driver's restatement of
+    GenIjPatch (GenIjPatch.h:104-118) on real superblocks: same pairs, same
+    order."""
+    c = sector_case(model, L, m, steps)
+    pl, pr = plugin.sector_patches(c["left_qns"], c["right_qns"], c["target"])
+    assert list(pl) == list(c["patch_left"]) and list(pr) == list(c["patch_right"])
+
+
+def test_patch_list_capacity_and_multi_component_numbers():
+    lq = [(0, 0), (1, 0), (0, 1), (1, 1)]
+    rq = [(1, 1), (0, 1), (1, 0), (0, 0), (1, 1)]     # a repeated right number too
+    pl, pr = plugin.sector_patches(lq, rq, (1, 1))
+    direct = [(i, j) for i, a in enumerate(lq) for j, b in enumerate(rq)
+              if (a[0] + b[0], a[1] + b[1]) == (1, 1)]
+    assert list(zip(pl, pr)) == direct
+    import ctypes
+    n = ctypes.c_size_t()
+    i64 = ctypes.POINTER(ctypes.c_int64)
+    a = np.array(lq, dtype=np.int64)
+    b = np.array(rq, dtype=np.int64)
+    t = np.array([1, 1], dtype=np.int64)
+    rc = _capi.lib().dmrgpp_kron_patch_list(4, a.ctypes.data_as(i64), 5, b.ctypes.data_as(i64), 2,
+                                            t.ctypes.data_as(i64), 0, None, None, ctypes.byref(n))
+    assert rc == _capi.INVALID_ARG and n.value == len(direct)

@@ -315,3 +315,28 @@ def test_page_locked_host_vectors(cuda_lib, cuda_device, oracle_built, which):
             assert rel_err(ref, oracle_built.kron_apply(prob, x)) < RTOL
     finally:
         bg.close()
+
+
+def test_tuning_cache_hits_across_similar_sectors(cuda_lib, cuda_device, oracle_built, tmp_path):
+    """The tuning cache key is a bucketed histogram of the sector's shape:
+    a sector whose patches differ by a state or two (as between consecutive
+    sweep steps) reuses the first sector's entry; a sector of another shape
+    does not."""
+    from dmrgpp_b200 import plugin
+    sizes = sb.gaussian_sector_sizes(1024, 13, 2.5)
+    nearby = sizes.copy()
+    nearby[len(sizes) // 2] += 1
+    nearby[len(sizes) // 2 + 1] -= 1
+    other = sb.gaussian_sector_sizes(4096, 21, 4.0)
+    cache = str(tmp_path / "tune.txt")
+
+    def lines():
+        return [ln for ln in open(cache).read().split("\n") if ln.strip()]
+    for n, (sz, seed) in enumerate(((sizes, 1), (nearby, 2), (other, 3))):
+        prob = sb.spin_chain_like(sz, seed=seed)
+        bg = plugin.BatchedGemm.from_problem(prob)
+        cfg, us = bg.autotune(cache, reps=2)
+        x = np.random.default_rng(seed).standard_normal(prob.dim)
+        assert rel_err(bg(x), oracle_built.kron_apply(prob, x)) < RTOL
+        bg.close()
+        assert len(lines()) == (1 if n < 2 else 2), n

@@ -133,3 +133,19 @@ def test_gather_index_restates_copy_in(oracle_built):
                 assert yin[q + ir + il * sr] == vin[r - offset]
         q += sl * sr
     assert sorted(idx.tolist()) == list(range(dim))
+
+
+@pytest.mark.skipif(not os.path.isdir(oracle.REFERENCE_TREE) and
+                    not os.path.exists(oracle.REF_KC_SO), reason="reference harness not built")
+@pytest.mark.parametrize("threads", [1, 4])
+def test_reference_nonbatched_path_matches_restatement(oracle_built, threads):
+    """The reference's default CPU H*x (KronConnections::doTask with
+    den_kron_mult per block, compiled from its sources) against the
+    restatement, on a ragged sector with absent and all-zero blocks and on
+    the microbench sector."""
+    for prob in (sb.random_problem(npatches=6, noperator=3, max_size=40, seed=3,
+                                   zero_block_rate=0.2), sb.c2_problem()):
+        x = np.random.default_rng(1).standard_normal(prob.dim)
+        y = oracle_built.RefKronConn(prob).apply(x, threads=threads)
+        ref = oracle_built.kron_apply(prob, x)
+        assert np.abs(y - ref).max() <= 1e-12 * np.abs(ref).max()
