@@ -83,6 +83,7 @@ SIGNATURES = {
     "dmrgpp_kron_dim": (ctypes.c_int, [ctypes.c_void_p, _szp]),
     "dmrgpp_kron_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "dmrgpp_kron_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "dmrgpp_kron_get_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "dmrgpp_kron_test_stall_dependency": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dmrgpp_kron_flops": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "dmrgpp_kron_setup_profile": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
@@ -197,6 +198,7 @@ SIGNATURES.update({
                                       ctypes.c_void_p]),
     "dmrgpp_kron_gather_index": (ctypes.c_int, [ctypes.POINTER(GatherIndexDesc),
                                                 ctypes.POINTER(ctypes.c_int64)]),
+    "dmrgpp_kron_tuned_times": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
     "dmrgpp_kron_patch_list": (ctypes.c_int, [_sz, ctypes.POINTER(ctypes.c_int64), _sz,
                                               ctypes.POINTER(ctypes.c_int64), _sz,
                                               ctypes.POINTER(ctypes.c_int64), _sz, _szp, _szp,

@@ -77,7 +77,11 @@ std::string sector_signature(const KronPlan& P, const char* gpu)
 	return buf;
 }
 
-bool cache_lookup(const char* path, const std::string& sig, int* cfg, int* ipc, double* us)
+// One line per entry: signature, configuration, items per CTA, the FP64
+// apply's microseconds and (optional fifth field) the TF32x3 apply's, -1
+// when no TF32x3 form was timed.
+bool cache_lookup(const char* path, const std::string& sig, int* cfg, int* ipc, double* us,
+                  double* us_tf32x3)
 {
 	if (!path)
 		return false;
@@ -88,24 +92,27 @@ bool cache_lookup(const char* path, const std::string& sig, int* cfg, int* ipc, 
 		std::istringstream in(line);
 		std::string        s;
 		int                c = -1, i = 0;
-		double             t = 0;
+		double             t = 0, t32 = -1.0;
 		if (in >> s >> c >> i >> t && s == sig && c >= 0 && c < dmrgpp::kNumTileCfgs + dmrgpp::kNumFusedCfgs
 		    && i > 0) {
-			*cfg  = c;
-			*ipc  = i;
-			*us   = t;
-			found = true; // the last entry wins
+			if (!(in >> t32))
+				t32 = -1.0;
+			*cfg       = c;
+			*ipc       = i;
+			*us        = t;
+			*us_tf32x3 = t32;
+			found      = true; // the last entry wins
 		}
 	}
 	return found;
 }
 
-void cache_store(const char* path, const std::string& sig, int cfg, int ipc, double us)
+void cache_store(const char* path, const std::string& sig, int cfg, int ipc, double us, double us_tf32x3)
 {
 	if (!path)
 		return;
 	std::ofstream f(path, std::ios::app);
-	f << sig << ' ' << cfg << ' ' << ipc << ' ' << us << '\n';
+	f << sig << ' ' << cfg << ' ' << ipc << ' ' << us << ' ' << us_tf32x3 << '\n';
 }
 
 } // namespace
@@ -165,9 +172,65 @@ int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps,
 	const std::string sig = sector_signature(h->plan, prop.name);
 	int               cfg = 0, ipc = 2;
 	double            us  = 0.0;
-	if (cache_lookup(cache_path, sig, &cfg, &ipc, &us)) {
+	cudaEvent_t       e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	// minimum over reps of one apply in the handle's current form (or -1)
+	auto time_apply = [&]() {
+		bool ok = true;
+		for (int w = 0; w < 2 && ok; ++w)
+			ok = kron_apply_device(h, h->d_x, h->d_y) == DMRGPP_OK;
+		double tmin = 1e30;
+		for (int r = 0; r < reps && ok; ++r) {
+			cudaEventRecord(e0, h->stream);
+			ok = kron_apply_device(h, h->d_x, h->d_y) == DMRGPP_OK;
+			cudaEventRecord(e1, h->stream);
+			cudaEventSynchronize(e1);
+			float ms = 0.f;
+			cudaEventElapsedTime(&ms, e0, e1);
+			tmin = std::min(tmin, double(ms) * 1e3);
+		}
+		ok = ok && cudaStreamSynchronize(h->stream) == cudaSuccess && h->err_host
+		    && *reinterpret_cast<volatile int*>(h->err_host) == 0;
+		return ok ? tmin : -1.0;
+	};
+	// the TF32x3 form (when the handle has one) against the chosen FP64 one,
+	// so that a mixed-precision solve can use the faster arithmetic per sector
+	auto time_mixed = [&](double fp64_us) {
+		h->tuned_fp64_us   = fp64_us;
+		h->tuned_tf32x3_us = -1.0;
+		if (!h->mixed_ready)
+			return;
+		const int prec = h->precision;
+		h->precision   = DMRGPP_TF32X3;
+		h->tuned_tf32x3_us = time_apply();
+		h->precision   = prec;
+	};
+	struct Events {
+		cudaEvent_t a, b;
+		~Events()
+		{
+			cudaEventDestroy(a);
+			cudaEventDestroy(b);
+		}
+	} events { e0, e1 };
+	const int prec_in = h->precision;
+	h->precision      = DMRGPP_FP64; // the configurations are the FP64 forms'
+	struct RestorePrecision {
+		dmrgpp_kron_handle h;
+		int                p;
+		~RestorePrecision() { h->precision = p; }
+	} restore_prec { h, prec_in };
+	double us32 = -1.0;
+	if (cache_lookup(cache_path, sig, &cfg, &ipc, &us, &us32)) {
 		if (int rc = configure_schedule(h, cfg, ipc))
 			return rc;
+		h->tuned_fp64_us   = us;
+		h->tuned_tf32x3_us = h->mixed_ready ? us32 : -1.0;
+		if (h->mixed_ready && us32 < 0) { // an entry made by an FP64 handle
+			time_mixed(us);
+			cache_store(cache_path, sig, cfg, ipc, us, h->tuned_tf32x3_us);
+		}
 		if (cfg_out)
 			*cfg_out = cfg;
 		if (us_out)
@@ -175,9 +238,6 @@ int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps,
 		return DMRGPP_OK;
 	}
 
-	cudaEvent_t e0, e1;
-	cudaEventCreate(&e0);
-	cudaEventCreate(&e1);
 	cudaStreamSynchronize(h->stream);
 	const int ipcs[] = { 1, 2, 4 };
 	double    best   = -1.0;
@@ -197,38 +257,32 @@ int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps,
 		for (int i : ipcs) {
 			if (configure_schedule(h, c, i) != DMRGPP_OK)
 				continue;
-			bool ok = true;
-			for (int w = 0; w < 2 && ok; ++w)
-				ok = kron_apply_device(h, h->d_x, h->d_y) == DMRGPP_OK;
-			double tmin = 1e30;
-			for (int r = 0; r < reps && ok; ++r) {
-				cudaEventRecord(e0, h->stream);
-				ok = kron_apply_device(h, h->d_x, h->d_y) == DMRGPP_OK;
-				cudaEventRecord(e1, h->stream);
-				cudaEventSynchronize(e1);
-				float ms = 0.f;
-				cudaEventElapsedTime(&ms, e0, e1);
-				tmin = std::min(tmin, double(ms) * 1e3);
-			}
-			if (ok && cudaStreamSynchronize(h->stream) == cudaSuccess && h->err_host
-			    && *reinterpret_cast<volatile int*>(h->err_host) == 0
-			    && (best < 0 || tmin < best)) {
+			const double tmin = time_apply();
+			if (tmin >= 0 && (best < 0 || tmin < best)) {
 				best = tmin;
 				bcfg = c;
 				bipc = i;
 			}
 		}
-	cudaEventDestroy(e0);
-	cudaEventDestroy(e1);
 	if (best < 0)
 		return handle_fail(h, DMRGPP_CUDA_ERROR, "autotune: no configuration ran");
 	if (int rc = configure_schedule(h, bcfg, bipc))
 		return rc;
-	cache_store(cache_path, sig, bcfg, bipc, best);
+	time_mixed(best);
+	cache_store(cache_path, sig, bcfg, bipc, best, h->tuned_tf32x3_us);
 	if (cfg_out)
 		*cfg_out = bcfg;
 	if (us_out)
 		*us_out = best;
+	return DMRGPP_OK;
+}
+
+int dmrgpp_kron_tuned_times(dmrgpp_kron_handle h, double* fp64_us, double* tf32x3_us)
+{
+	if (!h || !fp64_us || !tf32x3_us)
+		return DMRGPP_INVALID_ARG;
+	*fp64_us   = h->tuned_fp64_us;
+	*tf32x3_us = h->tuned_tf32x3_us;
 	return DMRGPP_OK;
 }
 

@@ -1068,6 +1068,14 @@ int dmrgpp_kron_set_precision(dmrgpp_kron_handle h, int precision)
 	            "precision not available on this handle (create it with that precision)");
 }
 
+int dmrgpp_kron_get_precision(dmrgpp_kron_handle h, int* precision)
+{
+	if (!h || !precision)
+		return fail(nullptr, DMRGPP_INVALID_ARG, "null handle or output");
+	*precision = h->precision;
+	return DMRGPP_OK;
+}
+
 int dmrgpp_kron_synchronize(dmrgpp_kron_handle h)
 {
 	if (!h)

@@ -63,6 +63,8 @@ struct dmrgpp_kron_s {
 	dmrgpp::FusedItem*  d_fitems = nullptr;
 	dmrgpp::FusedUnit*  d_funits = nullptr;
 	int                 fused_clusters = 0; // co-resident clusters of the fused configuration
+	double              tuned_fp64_us   = -1.0; // last autotune: best FP64 apply (microseconds)
+	double              tuned_tf32x3_us = -1.0; // and the TF32x3 apply (handles with that form)
 	int*                err_host = nullptr; // mapped pinned word written by the kernel
 	int*                err_dev  = nullptr;
 	int                 test_stall = 0;     // dmrgpp_kron_test_stall_dependency

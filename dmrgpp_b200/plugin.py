@@ -422,6 +422,59 @@ class BatchedGemm:
             _capi.check(rc, self._h)
         return e.value, {f: getattr(st, f) for f, _ in _capi.RefineStats._fields_}
 
+    def solve_lowest(self, init, tolerance: float = 1e-10, method: str = "auto",
+                     mixed_steps: int = 150, mixed_tolerance: float = 1e-7,
+                     fp64_steps: int = 400, tf32x3_gain: float = 1.5):
+        """Lowest eigenpair of a real sector (init: torch CUDA tensor) by
+          "fp64"  -- FP64 Lanczos, full reorthogonalisation, eigenvalue-change
+                     tolerance `tolerance` (the reference's method);
+          "mixed" -- Lanczos in the handle's TF32x3 form without
+                     reorthogonalisation (it only supplies a start vector; up
+                     to mixed_steps steps or a mixed_tolerance Ritz-value
+                     change), then the FP64 refinement to |r| <= tolerance
+                     max(1, |E|); if the refinement reports no convergence (a
+                     start above the first excitation of a nearly gapless
+                     sector), FP64 Lanczos finishes from the refined state;
+          "auto"  -- "mixed" on a TF32x3 handle unless the last autotune timed
+                     its TF32x3 H*x less than tf32x3_gain times faster than the
+                     tuned FP64 one (sectors of small patches), else "fp64".
+        Returns (energy, vector, stats dict; stats["method"] is the one used).
+        The handle's precision is left as it was."""
+        if method not in ("auto", "fp64", "mixed"):
+            raise ValueError(f"unknown method {method!r}")
+        t64, t32 = self.tuned_times()
+        user = self.get_precision()
+        if method == "auto":
+            has_mixed = user == TF32X3 or t32 > 0
+            slow = t32 > 0 and t64 > 0 and t64 < tf32x3_gain * t32
+            method = "mixed" if has_mixed and not slow else "fp64"
+        clock = time.perf_counter   # each phase ends in a host read of its result
+        try:
+            if method == "fp64":
+                self.set_precision(FP64)
+                t0 = clock()
+                e, z, n = self.lanczos_lowest(init, steps=fp64_steps, tolerance=tolerance)
+                return e, z, dict(method="fp64", fp64_lanczos_steps=n, converged=1,
+                                  fp64_lanczos_seconds=clock() - t0)
+            self.set_precision(TF32X3)
+            t0 = clock()
+            e1, z, n1 = self.lanczos_lowest(init, steps=mixed_steps, tolerance=mixed_tolerance,
+                                            reortho=False)
+            t1 = clock()
+            e, st = self.refine_lowest(z, max_outer=12, tolerance=tolerance, inner_iterations=80,
+                                       inner_tolerance=1e-2, raise_on_no_convergence=False)
+            st = dict(st, method="mixed", mixed_lanczos_steps=n1, fallback=0,
+                      mixed_lanczos_seconds=t1 - t0, refine_seconds=clock() - t1)
+            if not st["converged"]:
+                self.set_precision(FP64)
+                t0 = clock()
+                e, z, n2 = self.lanczos_lowest(z, steps=fp64_steps, tolerance=tolerance)
+                st.update(fallback=1, converged=1, fp64_lanczos_steps=n2,
+                          fp64_lanczos_seconds=clock() - t0)
+            return e, z, st
+        finally:
+            self.set_precision(user)
+
     def refine_lowest_group(self, psi, max_outer: int = 6, tolerance: float = 1e-9,
                             inner_iterations: int = 200, inner_tolerance: float = 1e-4,
                             raise_on_no_convergence: bool = True):
@@ -471,6 +524,19 @@ class BatchedGemm:
         _capi.check(self._lib.dmrgpp_kron_autotune(self._h, path, reps, ctypes.byref(cfg),
                                                    ctypes.byref(us)), self._h)
         return cfg.value, us.value
+
+    def tuned_times(self):
+        """(FP64 apply, TF32x3 apply) microseconds of the last autotune (-1
+        when not measured)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _capi.check(self._lib.dmrgpp_kron_tuned_times(self._h, ctypes.byref(a), ctypes.byref(b)),
+                    self._h)
+        return a.value, b.value
+
+    def get_precision(self) -> int:
+        v = ctypes.c_int()
+        _capi.check(self._lib.dmrgpp_kron_get_precision(self._h, ctypes.byref(v)), self._h)
+        return v.value
 
     def set_precision(self, precision: int) -> None:
         """FP64 or the mixed mode the handle was created with."""

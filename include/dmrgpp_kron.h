@@ -156,6 +156,10 @@ int dmrgpp_kron_apply(dmrgpp_kron_handle h, const double* x, double* y, int on_d
  * available.  No counterpart in the reference. */
 int dmrgpp_kron_set_precision(dmrgpp_kron_handle h, int precision);
 
+/* The precision that H*x launches of the handle currently use (DMRGPP_FP64
+ * or the mixed mode it was created with). */
+int dmrgpp_kron_get_precision(dmrgpp_kron_handle h, int* precision);
+
 /* Waits for the handle's stream and reports errors of work enqueued by
  * device-pointer applies (DMRGPP_TIMEOUT if a dependency wait inside the
  * kernel gave up, DMRGPP_CUDA_ERROR for a CUDA failure).  No counterpart in
@@ -289,6 +293,14 @@ int dmrgpp_kron_set_config(dmrgpp_kron_handle h, int cfg, int items_per_cta);
  * timing, a miss appends the new choice. */
 int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps, int* cfg,
                          double* us);
+
+/* The last autotune's best FP64 apply time and, for a handle created with
+ * DMRGPP_TF32X3, its TF32x3 apply time on the same sector (microseconds; -1
+ * when not measured), so that a mixed-precision solve can pick the faster
+ * arithmetic per sector (the TF32x3 form pays on large patches, not on
+ * sectors of small ones).  Both times are kept in the tuning cache beside
+ * the configuration. */
+int dmrgpp_kron_tuned_times(dmrgpp_kron_handle h, double* fp64_us, double* tf32x3_us);
 
 /* ---- Eigensolver on the device (replaces PsimagLite::LanczosSolver for one
  * sector, PsimagLite/src/PsimagLite/LanczosSolver.h:68-88 with

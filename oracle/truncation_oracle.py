@@ -5,9 +5,10 @@ dmrgpp_density_truncate.  It restates the reference's per-patch SVD route:
 for every group g of the block being truncated, the stacked matrix M_g of the
 sector-vector entries of the patches of g (DensityMatrixSvd.h:285-340,
 ParallelPsiSplit::doTask; one column block per patch and target, scaled by
-sqrt(weight)) and its singular values (DensityMatrixSvd.h:355-410,
-ParallelSvd::doTask: eigs = s^2), here as the eigenvalues of
-rho_g = M_g M_g^T; then the kept number of Truncation::computeKeptStates
+sqrt(weight)) and its singular values and left singular vectors
+(DensityMatrixSvd.h:355-410, ParallelSvd::doTask: eigs = s^2, LAPACK SVD of
+M_g); rho_g = M_g M_g^T is also returned; then the kept number of
+Truncation::computeKeptStates
 (Truncation.h:476-512) and the discarded weight of updateKeptStates
 (Truncation.h:373-419, sumUpTo).
 """
@@ -31,6 +32,23 @@ def density_blocks(lsz, rsz, patch_group, group_size, side, psis, weights=None):
             g = int(patch_group[p])
             rho[g] += w[t] * (X.T @ X if side == 0 else X @ X.T)
     return rho
+
+
+def stacked_blocks(lsz, rsz, patch_group, group_size, side, psis, weights=None):
+    """M_g for every group (DensityMatrixSvd.h:285-340, ParallelPsiSplit): the
+    columns of every patch of g and every target, scaled by sqrt(weight); side
+    0 stacks X_p^T (l x r_p), side 1 X_p (r x l_p)."""
+    lsz = np.asarray(lsz, dtype=np.int64)
+    rsz = np.asarray(rsz, dtype=np.int64)
+    xs = np.concatenate([[0], np.cumsum(lsz * rsz)])
+    psis = [np.asarray(p, dtype=np.float64) for p in psis]
+    w = np.ones(len(psis)) if weights is None else np.asarray(weights, dtype=np.float64)
+    cols = [[] for _ in group_size]
+    for t, psi in enumerate(psis):
+        for p in range(len(lsz)):
+            X = psi[xs[p]:xs[p + 1]].reshape(int(lsz[p]), int(rsz[p])).T   # r x l
+            cols[int(patch_group[p])].append(np.sqrt(w[t]) * (X.T if side == 0 else X))
+    return [np.hstack(c) if c else np.zeros((int(n), 0)) for c, n in zip(cols, group_size)]
 
 
 def compute_kept_states(kept_states, tolerance, m_min, eigs):
@@ -61,14 +79,19 @@ def truncate(lsz, rsz, patch_group, group_size, side, psis, m, tolerance=-1.0, m
     group then index (the reference's std::sort leaves ties unspecified)."""
     rho = density_blocks(lsz, rsz, patch_group, group_size, side, psis, weights)
     evals, evecs = [], []
-    for r in rho:
-        if r.shape[0] == 0:
+    # the reference's route: svd('A', M_g) (DensityMatrixSvd.h:355-410), the
+    # density-matrix eigenvalues the squared singular values, ascending
+    for Mg in stacked_blocks(lsz, rsz, patch_group, group_size, side, psis, weights):
+        n = Mg.shape[0]
+        if n == 0:
             evals.append(np.zeros(0))
             evecs.append(np.zeros((0, 0)))
             continue
-        w, v = np.linalg.eigh(0.5 * (r + r.T))
-        evals.append(w)
-        evecs.append(v)
+        U, sv, _ = np.linalg.svd(Mg, full_matrices=True)
+        w = np.zeros(n)
+        w[:len(sv)] = sv ** 2
+        evals.append(w[::-1].copy())
+        evecs.append(U[:, ::-1].copy())
     flat = [(float(w), g, i) for g, ws in enumerate(evals) for i, w in enumerate(ws)]
     order = sorted(range(len(flat)), key=lambda q: (flat[q][0], q))
     eigs = np.array([flat[q][0] for q in order])

@@ -61,35 +61,54 @@ def _timed(fn):
 
 
 def mixed_solve(bg, init, sites, tolerance=1e-10):
-    """TF32x3 Lanczos (no reorthogonalisation, 60 steps or a 1e-4 Ritz-value
-    change) then the FP64 refinement to |r| <= tolerance |E|."""
-    from dmrgpp_b200 import plugin
-    bg.set_precision(plugin.TF32X3)
-    e1, z, n1 = bg.lanczos_lowest(init, steps=60, tolerance=1e-4, reortho=False)
-    e, st = bg.refine_lowest(z, max_outer=12, tolerance=tolerance, inner_iterations=80,
-                             inner_tolerance=1e-2, raise_on_no_convergence=False)
-    return e, z, n1, st
+    """The library's mixed sector solve (BatchedGemm.solve_lowest, method
+    "mixed"): TF32x3 Lanczos without reorthogonalisation (up to 150 steps or
+    a 1e-7 Ritz-value change), then the FP64 refinement to |r| <= tolerance
+    |E|, and FP64 Lanczos from the refined state when the refinement reports
+    no convergence (counted as a fallback in the returned stats)."""
+    e, z, st = bg.solve_lowest(init, tolerance=tolerance, method="mixed")
+    return e, z, st["mixed_lanczos_steps"], st
 
 
-def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print):
+def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", tune=True):
+    """method: the library's solve_lowest method of the measured arm
+    ("mixed", or "auto": mixed only where the tuned TF32x3 H*x is at least
+    1.5x the tuned FP64 one).  tune: autotune every sector's FP64
+    configuration through one tuning cache for the run (its bucketed keys let
+    later steps reuse earlier timings; the tuning seconds are recorded)."""
+    import tempfile
     import torch
     from dmrgpp_b200 import plugin
     steps = []
+    cache = os.path.join(tempfile.mkdtemp(prefix="dmrgpp_tune_"), "tune.txt") if tune else None
 
     def solve(prob, init):
         x = torch.from_numpy(np.ascontiguousarray(init)).cuda()
         bg = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
         try:
-            (e, z, n1, st), t_mx = _timed(lambda: mixed_solve(bg, x, L))
+            t_tune, t64_us, t32_us = 0.0, -1.0, -1.0
+            if tune:
+                t0 = time.perf_counter()
+                bg.autotune(cache, reps=5)
+                t_tune = time.perf_counter() - t0
+                t64_us, t32_us = bg.tuned_times()
+            (e, z, st), t_mx = _timed(lambda: bg.solve_lowest(x, tolerance=1e-10, method=method))
             bg.set_precision(plugin.FP64)
             (e64, z64, n64), t_64 = _timed(lambda: bg.lanczos_lowest(x, steps=400, tolerance=1e-10))
         finally:
             bg.close()
+        n1 = st.get("mixed_lanczos_steps", st.get("fp64_lanczos_steps", 0))
         rec = dict(dim=prob.dim, f_alg=prob.flops(), e_mixed=e, e_fp64=e64,
                    abs_dE_per_site=abs(e - e64) / L,
                    one_minus_overlap=1.0 - abs(float(torch.dot(z, z64))),
                    mixed_seconds=t_mx, fp64_seconds=t_64, fp64_lanczos_steps=n64,
-                   refine_converged=int(st["converged"]))
+                   method=st["method"], mixed_lanczos_steps=n1, fallback=int(st.get("fallback", 0)),
+                   refine_converged=int(st["converged"]),
+                   mixed_lanczos_seconds=st.get("mixed_lanczos_seconds", 0.0),
+                   refine_seconds=st.get("refine_seconds", 0.0),
+                   refine_outer=int(st.get("outer_iterations", -1)),
+                   refine_inner_matvecs=int(st.get("inner_matvecs", -1)),
+                   tune_seconds=t_tune, tuned_fp64_us=t64_us, tuned_tf32x3_us=t32_us)
         steps.append(rec)
         if len(steps) % 20 == 0:
             log(f"step {len(steps)} dim {prob.dim} E {e:.12f} dE/site {rec['abs_dE_per_site']:.2e}")
@@ -103,10 +122,13 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print):
                steps=len(steps), final_energy_mixed_run=e_mixed,
                max_abs_dE_per_site_same_input=max(s["abs_dE_per_site"] for s in steps),
                max_one_minus_overlap=max(s["one_minus_overlap"] for s in steps),
-               all_refinements_converged=all(s["refine_converged"] for s in steps),
+               all_converged=all(s["refine_converged"] for s in steps),
+               fallbacks=sum(s["fallback"] for s in steps),
                max_dim=max(s["dim"] for s in steps),
                solve_seconds_mixed=sum(s["mixed_seconds"] for s in steps),
                solve_seconds_fp64=sum(s["fp64_seconds"] for s in steps),
+               tune_seconds=sum(s["tune_seconds"] for s in steps), method=method,
+               steps_solved_mixed=sum(s["method"] == "mixed" for s in steps),
                wall_seconds_mixed_run=time.time() - t0, per_step=steps)
     if fp64_run:
         t1 = time.time()
@@ -115,6 +137,8 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print):
         def solve64(prob, init):
             bg = plugin.BatchedGemm.from_problem(prob)
             try:
+                if tune:
+                    bg.autotune(cache, reps=5)
                 e, z, n = bg.lanczos_lowest(init, steps=400, tolerance=1e-10)
             finally:
                 bg.close()
@@ -257,7 +281,7 @@ def ladder_step_measurement(prob, init, sites, mlp=None, lanczos_steps=400):
     rec["mixed_lanczos_refined"] = dict(
         energy=e, seconds=tmx, setup_seconds=t_setmx, lanczos_steps=n1 + 1,
         refine_mixed_matvecs=st["inner_matvecs"], fp64_matvecs=st["fp64_matvecs"],
-        converged=st["converged"], abs_dE_per_site=abs(e - e64) / sites,
+        converged=st["converged"], fallback=st["fallback"], abs_dE_per_site=abs(e - e64) / sites,
         one_minus_overlap=1.0 - abs(float(torch.dot(z, z64))))
     for name, pre, m in (("mixed_davidson_none", 0, None), ("mixed_davidson_jacobi", 1, None),
                          ("mixed_davidson_learned", 2, mlp)):
@@ -443,6 +467,8 @@ def main(argv=None):
     p.add_argument("--m-inf", type=int, default=1000)
     p.add_argument("--steps", type=int, default=2)
     p.add_argument("--no-fp64-run", action="store_true")
+    p.add_argument("--method", default="mixed", choices=["mixed", "auto"])
+    p.add_argument("--no-tune", action="store_true")
     p.add_argument("--mlp", default=None, help="learned-correction weights (.npz)")
     p.add_argument("--out", default=None)
     a = p.parse_args(argv)
@@ -465,7 +491,8 @@ def main(argv=None):
                 json.dump(out, f, indent=1, default=float)
         return
     if a.what == "c3":
-        out = c3(L=a.L, m=a.m or 1000, sweeps=a.sweeps, fp64_run=not a.no_fp64_run)
+        out = c3(L=a.L, m=a.m or 1000, sweeps=a.sweeps, fp64_run=not a.no_fp64_run,
+                 method=a.method, tune=not a.no_tune)
     else:
         from dmrgpp_b200.mlp import MLPPreconditioner
         mlp = MLPPreconditioner.load(a.mlp) if a.mlp else None

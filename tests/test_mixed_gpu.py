@@ -141,3 +141,50 @@ def test_refinement_from_a_start_without_reorthogonalisation(cuda_lib, cuda_devi
     assert abs(e2 - e_ref) / 64 <= 1e-9, (e2, e_ref)
     overlap = abs(float(torch.dot(z1, z_ref)))
     assert 1.0 - overlap < 1e-8
+
+
+def test_autotune_times_both_arithmetics(cuda_lib, cuda_device, oracle_built, tmp_path):
+    """The tuner picks among the FP64 forms even on a TF32x3 handle, keeps the
+    handle's precision, and reports the TF32x3 apply beside the best FP64 one
+    (an FP64 handle reports -1 for TF32x3)."""
+    from dmrgpp_b200 import plugin
+    prob = sb.c2_problem()
+    x = sb.random_unit_vector(prob.dim, seed=4)
+    ref = oracle_built.kron_apply(prob, x)
+    bg = mixed(prob)
+    cfg, us = bg.autotune(str(tmp_path / "tune.txt"), reps=3)
+    t64, t32 = bg.tuned_times()
+    assert t64 == pytest.approx(us) and t32 > 0
+    assert rel_err(bg(x), ref) < RTOL_MIXED          # still the TF32x3 form
+    bg.set_precision(plugin.FP64)
+    assert rel_err(bg(x), ref) < 1e-12               # the tuned FP64 configuration
+    bg.close()
+    bg = plugin.BatchedGemm.from_problem(prob)
+    bg.autotune(str(tmp_path / "tune.txt"), reps=3)  # cache hit
+    t64b, t32b = bg.tuned_times()
+    assert t64b == pytest.approx(us) and t32b == -1.0
+    bg.close()
+
+
+@pytest.mark.parametrize("which,expect", [("c2", "fp64"), ("ladder8000", "mixed")])
+def test_solve_lowest_auto_follows_the_tuned_times(cuda_lib, cuda_device, which, expect):
+    """solve_lowest("auto") runs the mixed solve where the tuned TF32x3 H*x is
+    at least 1.5x the FP64 one (the 8000-state ladder sector: ~2.6x) and FP64
+    Lanczos where it is not (the microbench sector's small patches: ~0.9x);
+    either way the energy is the FP64 one and the handle keeps its precision."""
+    import torch
+    from dmrgpp_b200 import plugin
+    prob = sb.c2_problem() if which == "c2" else sb.ladder_problem(total_states=8000, seed=3)
+    x = torch.from_numpy(sb.random_unit_vector(prob.dim, seed=5)).cuda()
+    bg = mixed(prob)
+    bg.autotune(None, reps=3)
+    t64, t32 = bg.tuned_times()
+    assert t64 > 0 and t32 > 0
+    e, z, st = bg.solve_lowest(x, tolerance=1e-10, method="auto")
+    assert st["method"] == expect, (t64, t32)
+    assert bg.get_precision() == plugin.TF32X3
+    bg.set_precision(plugin.FP64)
+    e64, z64, _ = bg.lanczos_lowest(x, steps=400, tolerance=1e-12)
+    bg.close()
+    assert abs(e - e64) <= 1e-9 * abs(e64)
+    assert 1.0 - abs(float(torch.dot(z, z64))) <= 1e-6

@@ -70,6 +70,50 @@ def test_truncation_matches_oracle(cuda_lib, cuda_device, side, targets):
             assert abs(sum(x.sum() for x in out["eigenvalues"]) - 1.0) < 1e-12
 
 
+def test_low_rank_group_keeps_the_states_of_an_svd(cuda_lib, cuda_device):
+    """A group whose stacked matrix M_g has singular values 1, 1e-3, 1e-5,
+    1e-7, 1e-8 and zeros (weights down to 1e-16), beside a group of full rank,
+    with a discarded-weight tolerance of 1e-12: the library (eigenpairs of
+    rho_g = M_g M_g^T) keeps the same states per group as the reference's SVD
+    of M_g (the oracle), the kept weights agree to 1e-5 relative, and the kept
+    subspace agrees with the SVD's to 1e-5.  (rho_g's eigenvalues carry an
+    absolute error of about eps ||rho_g||: weights below ~1e-12 ||rho_g|| lose
+    relative accuracy, which only a tolerance below that would see.)"""
+    import torch
+    from dmrgpp_b200.truncation import density_truncate
+    rng = np.random.default_rng(5)
+    n0, cols0 = 40, (30, 50)
+    U, _ = np.linalg.qr(rng.standard_normal((n0, n0)))
+    V, _ = np.linalg.qr(rng.standard_normal((sum(cols0), n0)))
+    sv = np.zeros(n0)
+    sv[:5] = [1.0, 1e-3, 1e-5, 1e-7, 1e-8]
+    M0 = U @ np.diag(sv) @ V.T                      # 40 x 80, rank 5
+    n1, cols1 = 25, (20,)
+    M1 = 0.3 * rng.standard_normal((n1, sum(cols1)))
+    lsz, rsz, pg, psi = [], [], [], []
+    for g, (M, cols) in enumerate(((M0, cols0), (M1, cols1))):
+        c0 = 0
+        for c in cols:              # side 0: patch p contributes X_p^T = M[:, c0:c0+c]
+            X = M[:, c0:c0 + c].T   # r_p x l_p
+            lsz.append(M.shape[0])
+            rsz.append(c)
+            pg.append(g)
+            psi.append(X.flatten(order="F"))
+            c0 += c
+    psi = np.concatenate(psi)
+    gs = [n0, n1]
+    ref = to.truncate(lsz, rsz, pg, gs, 0, [psi], m=n0 + n1, tolerance=1e-12, m_min=0)
+    out = density_truncate(lsz, rsz, pg, gs, 0, torch.tensor(psi, device="cuda"), n0 + n1, 1e-12, 0)
+    assert np.array_equal(out["kept"], ref["kept"]) and out["kept_total"] == ref["kept_total"]
+    assert int(out["kept"][0]) == 3                  # weights 1, 1e-6, 1e-10
+    for g in range(2):
+        k = int(out["kept"][g])
+        we, wr = out["eigenvalues"][g][-k:], ref["eigenvalues"][g][-k:]
+        assert np.all(np.abs(we - wr) <= 1e-5 * wr), g
+        V_l, V_r = out["vectors"][g], ref["vectors"][g][:, -k:]
+        assert np.abs(V_l @ V_l.T - V_r @ V_r.T).max() < 1e-5, g
+
+
 def test_truncation_argument_checks(cuda_lib, cuda_device):
     import torch
     from dmrgpp_b200 import _capi
