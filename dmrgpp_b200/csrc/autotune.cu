@@ -4,10 +4,10 @@
 // input, BatchedGemmKokkos.h:110-130).  Here each sector is timed under every
 // configuration (the persistent two-pass form's tiles and work splits, the
 // fused form's where its patches are narrow enough), the fastest is kept,
-// and the choice is cached in a text file keyed by a bucketed histogram of
-// the sector's shape (patch sizes, contributing triples, Kronecker terms)
-// and the GPU name, so that sectors of similar shape in later sweep steps or
-// runs skip the timing.
+// and the choice is cached in a text file keyed by a coarse summary of the
+// sector's size histogram (work quartiles of the patch dimensions, total
+// work, Kronecker terms) and the GPU name, so that sectors of similar shape
+// in later sweep steps or runs skip the timing.
 #include "dmrgpp_kron.h"
 #include "handle.h"
 #include "kron_fused.cuh"
@@ -30,27 +30,38 @@ namespace {
 
 using dmrgpp::KronPlan;
 
-// FNV-1a over a bucketed histogram of the sector's shape: patches counted
-// by (l, r) in buckets of a quarter octave each, contributing triples
-// counted by (l_i, l_j) the same way, the number of terms, and the GPU name.
-// Consecutive sweep steps change patch sizes by a few states, which mostly
-// stays inside the buckets, so their sectors share a tuning entry.
-int size_bucket(long long n)
-{
-	if (n <= 8)
-		return int(n);
-	// 4 buckets per factor of two above 8
-	const double b = 4.0 * std::log2(double(n) / 8.0);
-	return 8 + int(b);
-}
+int octave(double x) { return x >= 1.0 ? int(std::floor(std::log2(x))) : 0; }
 
+// FNV-1a over a coarse summary of the sector's size histogram: the patch
+// dimension (max(l_i, r_i) of the output patch) at the quartiles and the
+// maximum of the work-weighted distribution, one bucket per octave; the
+// total work in half-octave buckets; the number of terms; the GPU name.
+// These set what the configurations trade off (tile padding against
+// tiles per SM), and they move little between consecutive sweep steps,
+// whose patch sizes change by a few states, so those sectors share an
+// entry.
 std::string sector_signature(const KronPlan& P, const char* gpu)
 {
-	std::map<std::pair<int, int>, long long> patches, triples;
-	for (size_t p = 0; p < P.np; ++p)
-		patches[{ size_bucket(P.l[p]), size_bucket(P.r[p]) }]++;
-	for (const auto& t : P.triples)
-		triples[{ size_bucket(P.l[size_t(t.i)]), size_bucket(P.l[size_t(t.j)]) }]++;
+	std::vector<std::pair<long long, double>> w; // (patch dimension, work)
+	double                                    total = 0.0;
+	long long                                 dmax  = 0;
+	for (const auto& t : P.triples) {
+		const long long d = std::max(P.l[size_t(t.i)], P.r[size_t(t.i)]);
+		const double    f = 2.0 * double(P.r[size_t(t.i)]) * double(P.l[size_t(t.j)])
+		    * double(P.r[size_t(t.j)] + P.l[size_t(t.i)]);
+		w.push_back({ d, f });
+		total += f;
+		dmax = std::max(dmax, d);
+	}
+	std::sort(w.begin(), w.end());
+	long long q[3] = { 0, 0, 0 };
+	double    acc  = 0.0;
+	int       k    = 0;
+	for (const auto& e : w) {
+		acc += e.second;
+		while (k < 3 && acc >= total * 0.25 * (k + 1))
+			q[k++] = e.first;
+	}
 	unsigned long long h   = 1469598103934665603ull;
 	auto               mix = [&](unsigned long long v) {
                 for (int b = 0; b < 8; ++b) {
@@ -58,18 +69,11 @@ std::string sector_signature(const KronPlan& P, const char* gpu)
                         h *= 1099511628211ull;
                 }
 	};
-	// counts bucketed too (a quarter octave), so a patch more or less in a
-	// populated bucket keeps the key
 	mix(P.nop);
-	for (const auto& kv : patches) {
-		mix((unsigned long long)kv.first.first << 32 | (unsigned)kv.first.second);
-		mix((unsigned long long)size_bucket(kv.second));
-	}
-	mix(0xfffffffffull);
-	for (const auto& kv : triples) {
-		mix((unsigned long long)kv.first.first << 32 | (unsigned)kv.first.second);
-		mix((unsigned long long)size_bucket(kv.second));
-	}
+	for (long long v : q)
+		mix((unsigned long long)octave(double(v)));
+	mix((unsigned long long)octave(double(dmax)));
+	mix((unsigned long long)(total > 1.0 ? int(std::floor(2.0 * std::log2(total))) : 0));
 	for (const char* c = gpu; *c; ++c)
 		mix((unsigned long long)(unsigned char)*c);
 	char buf[32];

@@ -200,6 +200,8 @@ int mixed_apply_device(dmrgpp_kron_handle h, const double* X, double* Y, const S
 	a1.A_lo   = tm[1];
 	a1.B_hi   = tm[2];
 	a1.B_lo   = tm[3];
+	a1.C_hi_map = tm[8];
+	a1.C_lo_map = tm[9];
 	a1.C_hi   = h->m_bxs_hi;
 	a1.C_lo   = h->m_bxs_lo;
 	a1.segs   = h->m_seg1;
@@ -323,19 +325,19 @@ int build_mixed(dmrgpp_kron_handle h, MixedHost& host)
 	// K-split pass-2 tiles: FP32 partial slots and self-resetting counters
 	if ((e = dmrgpp::dev_malloc(&h->m_partial, fbytes(mp.split_slots * 128 * mp.bn)))
 	    || (e = dmrgpp::dev_malloc(&h->m_arrive, size_t(std::max(mp.n_split_tiles, 1)) * sizeof(unsigned)))
-	    || (e = cudaMemset(h->m_arrive, 0, size_t(std::max(mp.n_split_tiles, 1)) * sizeof(unsigned))))
+	    || (e = dmrgpp::clear_async(h->m_arrive, size_t(std::max(mp.n_split_tiles, 1)) * sizeof(unsigned), h->stream)))
 		return cuda_fail(h, e, "device allocation (split-K partials)");
 	// K padding must read as zero
-	if ((e = cudaMemset(h->m_xs_hi, 0, fbytes(mp.xs_elems))) || (e = cudaMemset(h->m_xs_lo, 0, fbytes(mp.xs_elems)))
-	    || (e = cudaMemset(h->m_bxs_hi, 0, fbytes(mp.bxs_elems)))
-	    || (e = cudaMemset(h->m_bxs_lo, 0, fbytes(mp.bxs_elems))))
+	if ((e = dmrgpp::clear_async(h->m_xs_hi, fbytes(mp.xs_elems), h->stream)) || (e = dmrgpp::clear_async(h->m_xs_lo, fbytes(mp.xs_elems), h->stream))
+	    || (e = dmrgpp::clear_async(h->m_bxs_hi, fbytes(mp.bxs_elems), h->stream))
+	    || (e = dmrgpp::clear_async(h->m_bxs_lo, fbytes(mp.bxs_elems), h->stream)))
 		return cuda_fail(h, e, "clear mixed-precision buffers");
 	{
 		const std::vector<PackJob>& jobs   = host.jobs;
 		PackJob*                    d_jobs = nullptr;
-		if ((e = cudaMemset(h->m_ops_hi, 0, fbytes(mp.ops_elems))) || (e = cudaMemset(h->m_ops_lo, 0, fbytes(mp.ops_elems)))
+		if ((e = dmrgpp::clear_async(h->m_ops_hi, fbytes(mp.ops_elems), h->stream)) || (e = dmrgpp::clear_async(h->m_ops_lo, fbytes(mp.ops_elems), h->stream))
 		    || (e = dmrgpp::dev_malloc(&d_jobs, std::max<size_t>(jobs.size(), 1) * sizeof(PackJob)))
-		    || (e = cudaMemcpy(d_jobs, jobs.data(), jobs.size() * sizeof(PackJob), cudaMemcpyHostToDevice))
+		    || (e = dmrgpp::upload_sync(d_jobs, jobs.data(), jobs.size() * sizeof(PackJob), h->stream))
 		    || (e = tc_pack_ops(h->d_ops, h->m_ops_hi, h->m_ops_lo, d_jobs, int(jobs.size()), h->stream))
 		    || (e = cudaStreamSynchronize(h->stream))) {
 			dmrgpp::dev_free(d_jobs);
@@ -346,7 +348,8 @@ int build_mixed(dmrgpp_kron_handle h, MixedHost& host)
 	{
 		// the operand buffers as 2-D tensors [row][32 floats], 128-byte
 		// swizzle: pass 1 A = operators (128-row boxes), B = x split (bn);
-		// pass 2 A = BX split (128), B = operators (bn); hi and lo each
+		// pass 2 A = BX split (128), B = operators (bn); hi and lo each;
+		// then the BX split with 32-row boxes for pass 1's stores
 		PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
 		if (!encode)
 			return fail(h, DMRGPP_NOT_SUPPORTED, "cuTensorMapEncodeTiled is not available");
@@ -355,11 +358,12 @@ int build_mixed(dmrgpp_kron_handle h, MixedHost& host)
 			float*    buf;
 			long long elems;
 			int       box;
-		} spec[8] = { { h->m_ops_hi, mp.ops_elems, mp.bm }, { h->m_ops_lo, mp.ops_elems, mp.bm },
-		              { h->m_xs_hi, mp.xs_elems, mp.bn },   { h->m_xs_lo, mp.xs_elems, mp.bn },
-		              { h->m_bxs_hi, mp.bxs_elems, mp.bm }, { h->m_bxs_lo, mp.bxs_elems, mp.bm },
-		              { h->m_ops_hi, mp.ops_elems, mp.bn }, { h->m_ops_lo, mp.ops_elems, mp.bn } };
-		for (int q = 0; q < 8; ++q) {
+		} spec[10] = { { h->m_ops_hi, mp.ops_elems, mp.bm }, { h->m_ops_lo, mp.ops_elems, mp.bm },
+		               { h->m_xs_hi, mp.xs_elems, mp.bn },   { h->m_xs_lo, mp.xs_elems, mp.bn },
+		               { h->m_bxs_hi, mp.bxs_elems, mp.bm }, { h->m_bxs_lo, mp.bxs_elems, mp.bm },
+		               { h->m_ops_hi, mp.ops_elems, mp.bn }, { h->m_ops_lo, mp.ops_elems, mp.bn },
+		               { h->m_bxs_hi, mp.bxs_elems, 32 },    { h->m_bxs_lo, mp.bxs_elems, 32 } };
+		for (int q = 0; q < 10; ++q) {
 			const cuuint64_t dims[2]    = { 32, cuuint64_t(std::max<long long>(spec[q].elems / 32, 1)) };
 			const cuuint64_t strides[1] = { 128 };
 			const cuuint32_t box[2]     = { 32, cuuint32_t(spec[q].box) };
@@ -373,7 +377,7 @@ int build_mixed(dmrgpp_kron_handle h, MixedHost& host)
 		}
 	}
 	if (!xmap.empty()
-	    && (e = cudaMemcpy(h->m_xmap, xmap.data(), xmap.size() * sizeof(int), cudaMemcpyHostToDevice)))
+	    && (e = dmrgpp::upload_sync(h->m_xmap, xmap.data(), xmap.size() * sizeof(int), h->stream)))
 		return cuda_fail(h, e, "upload x map");
 	std::vector<unsigned char> lists;
 	std::vector<size_t>        offs;
@@ -418,7 +422,7 @@ int build_mixed(dmrgpp_kron_handle h, MixedHost& host)
 	h->m_tsec1   = group ? reinterpret_cast<int*>(at(6)) : nullptr;
 	h->m_tsec2   = group ? reinterpret_cast<int*>(at(7)) : nullptr;
 	if (!lists.empty()
-	    && (e = cudaMemcpy(h->m_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
+	    && (e = dmrgpp::upload_sync(h->m_lists, lists.data(), lists.size(), h->stream)))
 		return cuda_fail(h, e, "upload mixed lists");
 	h->mixed_ready = true;
 	return DMRGPP_OK;
@@ -457,8 +461,8 @@ int configure_fused(dmrgpp_kron_handle h, int fcfg, int parts_per_sm)
 		return cuda_fail(h, e, "device allocation (fused lists)");
 	h->d_fitems = static_cast<FusedItem*>(h->d_flists);
 	h->d_funits = reinterpret_cast<FusedUnit*>(static_cast<unsigned char*>(h->d_flists) + ib);
-	if ((ib && (e = cudaMemcpy(h->d_fitems, P.fitems.data(), ib, cudaMemcpyHostToDevice)))
-	    || (ub && (e = cudaMemcpy(h->d_funits, P.funits.data(), ub, cudaMemcpyHostToDevice))))
+	if ((ib && (e = dmrgpp::upload_sync(h->d_fitems, P.fitems.data(), ib, h->stream)))
+	    || (ub && (e = dmrgpp::upload_sync(h->d_funits, P.funits.data(), ub, h->stream))))
 		return cuda_fail(h, e, "upload fused lists");
 	h->cfg           = kNumTileCfgs + fcfg;
 	h->items_per_cta = parts_per_sm;
@@ -530,13 +534,13 @@ int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 	h->d_n1    = reinterpret_cast<int*>(at(6));
 	h->d_item_sector = reinterpret_cast<int*>(at(7));
 	if (!lists.empty()
-	    && (e = cudaMemcpy(h->d_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
+	    && (e = dmrgpp::upload_sync(h->d_lists, lists.data(), lists.size(), h->stream)))
 		return cuda_fail(h, e, "upload lists");
 
 	const size_t nctr = 3 + P.np + size_t(P.n_split_tiles);
 	if ((e = dmrgpp::dev_malloc(&h->d_ctr, nctr * sizeof(unsigned))))
 		return cuda_fail(h, e, "device allocation (counters)");
-	if ((e = cudaMemset(h->d_ctr, 0, nctr * sizeof(unsigned))))
+	if ((e = dmrgpp::clear_async(h->d_ctr, nctr * sizeof(unsigned), h->stream)))
 		return cuda_fail(h, e, "clear counters");
 	const size_t part_elems = size_t(P.partial_slots) * size_t(tile) * size_t(tile);
 	if ((e = dmrgpp::dev_malloc(&h->d_part, (part_elems ? part_elems : 1) * sizeof(double))))

@@ -115,8 +115,24 @@ void error_word_free(int* host)
 	w.free_words.push_back(host);
 }
 
+// Requests of 64 MB and more are rounded up to size classes (eight per
+// factor of two, at most 12.5% more), so that the buffers of consecutive
+// sweep steps, whose sizes differ by a few percent, fit blocks the pool
+// already holds instead of making it map new memory.
+size_t size_class(size_t bytes)
+{
+	if (bytes < (size_t(64) << 20))
+		return bytes;
+	int lg = 63;
+	while (!(bytes >> lg))
+		--lg;
+	const size_t q = size_t(1) << (lg - 3);
+	return (bytes + q - 1) / q * q;
+}
+
 cudaError_t dev_malloc_bytes(void** p, size_t bytes)
 {
+	bytes      = size_class(bytes);
 	*p         = nullptr;
 	int         device;
 	cudaError_t e = cudaGetDevice(&device);
@@ -126,6 +142,27 @@ cudaError_t dev_malloc_bytes(void** p, size_t bytes)
 	if ((e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, d->pool, d->stream)))
 		return e;
 	return cudaStreamSynchronize(d->stream);
+}
+
+cudaError_t upload_sync(void* dst, const void* src, size_t bytes, cudaStream_t st)
+{
+	if (!bytes)
+		return cudaSuccess;
+	const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+	return e ? e : cudaStreamSynchronize(st);
+}
+
+cudaError_t download_sync(void* dst, const void* src, size_t bytes, cudaStream_t st)
+{
+	if (!bytes)
+		return cudaSuccess;
+	const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+	return e ? e : cudaStreamSynchronize(st);
+}
+
+cudaError_t clear_async(void* dst, size_t bytes, cudaStream_t st)
+{
+	return bytes ? cudaMemsetAsync(dst, 0, bytes, st) : cudaSuccess;
 }
 
 void dev_free(void* p)

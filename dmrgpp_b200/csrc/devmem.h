@@ -28,6 +28,15 @@ void dev_free(void* p);
 cudaError_t error_word_alloc(int** host, int** dev);
 void        error_word_free(int* host);
 
+// Copies and clears ordered on the handle's stream st.  A caller's stream
+// may be non-blocking (torch's streams are), and such a stream is not
+// ordered with the legacy default stream that cudaMemcpy / cudaMemset use:
+// a clear there could land after a kernel on st has written the buffer.
+// upload_sync / download_sync return once the bytes have arrived.
+cudaError_t upload_sync(void* dst, const void* src, size_t bytes, cudaStream_t st);
+cudaError_t download_sync(void* dst, const void* src, size_t bytes, cudaStream_t st);
+cudaError_t clear_async(void* dst, size_t bytes, cudaStream_t st);
+
 template <class T> cudaError_t dev_malloc(T** p, size_t bytes)
 {
 	return dev_malloc_bytes(reinterpret_cast<void**>(p), bytes);

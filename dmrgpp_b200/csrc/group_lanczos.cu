@@ -568,12 +568,12 @@ int ensure_group_work(dmrgpp_kron_handle h, int cols)
 	    || (e = dmrgpp::dev_malloc(&w->sec_start, (size_t(nseg) + 1) * sizeof(long long)))
 	    || (e = cudaHostAlloc(&w->host, 2 * (2 * nsc + size_t(nseg)) * sizeof(double), 0)))
 		return status(h, e, "group solver allocation");
-	if ((e = cudaMemcpy(w->chunks, ch.data(), ch.size() * sizeof(Chunk), cudaMemcpyHostToDevice))
-	    || (e = cudaMemcpy(w->seg_chunk, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice))
-	    || (e = cudaMemcpy(w->sec_start, h->sector_start.data(), (size_t(nseg) + 1) * sizeof(long long),
-	                       cudaMemcpyHostToDevice))
-	    || (e = cudaMemset(w->beta, 0, (nsc + size_t(nseg)) * sizeof(double)))
-	    || (e = cudaMemset(w->alpha, 0, nsc * sizeof(double))))
+	if ((e = dmrgpp::upload_sync(w->chunks, ch.data(), ch.size() * sizeof(Chunk), h->stream))
+	    || (e = dmrgpp::upload_sync(w->seg_chunk, sc.data(), sc.size() * sizeof(int), h->stream))
+	    || (e = dmrgpp::upload_sync(w->sec_start, h->sector_start.data(), (size_t(nseg) + 1) * sizeof(long long),
+	                                h->stream))
+	    || (e = dmrgpp::clear_async(w->beta, (nsc + size_t(nseg)) * sizeof(double), h->stream))
+	    || (e = dmrgpp::clear_async(w->alpha, nsc * sizeof(double), h->stream)))
 		return status(h, e, "group solver set-up");
 	return DMRGPP_OK;
 }
@@ -805,8 +805,8 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 			j_stop[size_t(s)] = maxn_s[size_t(s)] - 1;
 	// final scalars: entries up to each sector's stopping step no longer change
 	if ((e = cudaStreamSynchronize(st))
-	    || (e = cudaMemcpy(w->host, w->alpha, nsc * sizeof(double), cudaMemcpyDeviceToHost))
-	    || (e = cudaMemcpy(w->host + nsc, w->beta, (nsc + size_t(S)) * sizeof(double), cudaMemcpyDeviceToHost)))
+	    || (e = dmrgpp::download_sync(w->host, w->alpha, nsc * sizeof(double), h->stream))
+	    || (e = dmrgpp::download_sync(w->host + nsc, w->beta, (nsc + size_t(S)) * sizeof(double), h->stream)))
 		return status(h, e, "read alpha/beta");
 
 	// Ritz pairs per sector (LanczosSolver.h:76-84): lowest eigenvalue of the

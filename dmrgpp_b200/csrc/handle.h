@@ -92,8 +92,9 @@ struct dmrgpp_kron_s {
 	float*              m_partial = nullptr; // split-K partial tiles of pass 2
 	unsigned*           m_arrive  = nullptr; // per split tile: parts done
 	// CUtensorMap (128 bytes) of the operand buffers: pass 1 A hi/lo, B hi/lo,
-	// pass 2 A hi/lo, B hi/lo; passed to the kernels by value
-	alignas(64) unsigned char m_tmap[8][128] = {};
+	// pass 2 A hi/lo, B hi/lo, then the BX split hi/lo with 32-row boxes
+	// (pass 1's stores); passed to the kernels by value
+	alignas(64) unsigned char m_tmap[10][128] = {};
 	void*               m_lists  = nullptr; // seg1, seg2, tile1, tile2
 	dmrgpp::GemmSeg*    m_seg1 = nullptr;
 	dmrgpp::GemmSeg*    m_seg2 = nullptr;

@@ -597,9 +597,9 @@ int ensure_work(dmrgpp_kron_handle h, size_t dim, int cols)
 		return cuda_status(h, e, "device allocation (coefficients)");
 	if ((e = dmrgpp::dev_malloc(&w->ctr, 16 * sizeof(unsigned))))
 		return cuda_status(h, e, "device allocation (counters)");
-	if ((e = cudaMemset(w->ctr, 0, 16 * sizeof(unsigned))))
+	if ((e = dmrgpp::clear_async(w->ctr, 16 * sizeof(unsigned), h->stream)))
 		return cuda_status(h, e, "clear counters");
-	if ((e = cudaMemset(w->scal, 0, (2 * size_t(cols) + 16) * sizeof(double))))
+	if ((e = dmrgpp::clear_async(w->scal, (2 * size_t(cols) + 16) * sizeof(double), h->stream)))
 		return cuda_status(h, e, "clear scalars");
 	if ((e = cudaHostAlloc(&w->host, 2 * (2 * size_t(cols) + 16) * sizeof(double), 0)))
 		return cuda_status(h, e, "cudaHostAlloc(scalars)");
@@ -933,7 +933,7 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 	const size_t        n = j_stop + 1;
 	std::vector<double> d(hb, hb + n), off(hb + w->cols + 1, hb + w->cols + n), zt(n * n);
 	if (maxn == 1) { // no loop ran: alpha[0] has not been read back yet
-		if ((e = cudaMemcpy(w->host, w->scal, sizeof(double), cudaMemcpyDeviceToHost)))
+		if ((e = dmrgpp::download_sync(w->host, w->scal, sizeof(double), h->stream)))
 			return cuda_status(h, e, "read alpha");
 		d[0] = w->host[0];
 	}
@@ -1067,7 +1067,7 @@ int ensure_davidson(dmrgpp_kron_handle h, size_t dim, int mmax)
 	    || (e = dmrgpp::dev_malloc(&w->scal, 16 * sizeof(double)))
 	    || (e = dmrgpp::dev_malloc(&w->partial, size_t(kMaxBlocks) * kMaxCols * sizeof(double)))
 	    || (e = dmrgpp::dev_malloc(&w->ctr, 16 * sizeof(unsigned)))
-	    || (e = cudaMemset(w->ctr, 0, 16 * sizeof(unsigned)))
+	    || (e = dmrgpp::clear_async(w->ctr, 16 * sizeof(unsigned), h->stream))
 	    || (e = cudaHostAlloc(&w->host, (size_t(kMaxCols) + 8) * sizeof(double), 0)))
 		return cuda_status(h, e, "Davidson buffers");
 	w->hu = w->u + dim;

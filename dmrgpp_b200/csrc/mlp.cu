@@ -806,6 +806,9 @@ int dmrgpp_mlp_create(unsigned long long seed, dmrgpp_mlp_handle* out)
 	    || (e = cudaMemset(m->adam_m, 0, kNumParams * sizeof(float)))
 	    || (e = cudaMemset(m->adam_v, 0, kNumParams * sizeof(float)))
 	    || (e = cudaMemcpy(m->params, p.data(), kNumParams * sizeof(float), cudaMemcpyHostToDevice))
+	    // the MLP's kernels run on callers' streams, which may be non-blocking
+	    // (not ordered with these legacy-stream writes): finish them here
+	    || (e = cudaDeviceSynchronize())
 	    || (e = error_word_alloc(&m->err_host, &m->err_dev))) {
 		const int rc = mlp_cuda(nullptr, e, "MLP create");
 		dmrgpp_mlp_destroy(m);
@@ -855,7 +858,9 @@ int dmrgpp_mlp_get_params(dmrgpp_mlp_handle m, float* host, size_t n)
 {
 	if (!m || !host || n != dmrgpp::kNumParams)
 		return DMRGPP_INVALID_ARG;
-	return cudaMemcpy(host, m->params, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess
+	// kernels on callers' (possibly non-blocking) streams finish first
+	return cudaDeviceSynchronize() == cudaSuccess
+	        && cudaMemcpy(host, m->params, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess
 	    ? DMRGPP_OK
 	    : DMRGPP_CUDA_ERROR;
 }
@@ -866,9 +871,14 @@ int dmrgpp_mlp_set_params(dmrgpp_mlp_handle m, const float* host, size_t n)
 		return DMRGPP_INVALID_ARG;
 	m->bf_dirty = true;
 	m->adam_t   = 0;
+	// no kernel on a caller's stream may still use the old values, and the
+	// next one must see the new ones
+	if (cudaDeviceSynchronize() != cudaSuccess)
+		return DMRGPP_CUDA_ERROR;
 	cudaMemset(m->adam_m, 0, n * sizeof(float));
 	cudaMemset(m->adam_v, 0, n * sizeof(float));
 	return cudaMemcpy(m->params, host, n * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess
+	        && cudaDeviceSynchronize() == cudaSuccess
 	    ? DMRGPP_OK
 	    : DMRGPP_CUDA_ERROR;
 }
@@ -877,7 +887,8 @@ int dmrgpp_mlp_get_grads(dmrgpp_mlp_handle m, float* host, size_t n)
 {
 	if (!m || !host || n != dmrgpp::kNumParams)
 		return DMRGPP_INVALID_ARG;
-	return cudaMemcpy(host, m->grads, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess
+	return cudaDeviceSynchronize() == cudaSuccess
+	        && cudaMemcpy(host, m->grads, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess
 	    ? DMRGPP_OK
 	    : DMRGPP_CUDA_ERROR;
 }

@@ -25,7 +25,12 @@
 //   warps 2-5: epilogue.  Warp w reads TMEM lanes 32(w % 4) .. +31 (tile
 //     rows) with tcgen05.ld and either splits the result into the hi/lo
 //     chunked layout of the next pass (pass 1: BX, the A operand of pass 2)
-//     or widens it to FP64 (pass 2: y), then frees the accumulator.
+//     or widens it to FP64 (pass 2: y), then frees the accumulator.  In
+//     pass 1 a thread's 32 values of one chunk are one 128-byte row of BX;
+//     the warp writes its 32 rows into its own shared-memory staging tile
+//     in the 128-byte-swizzled layout (no bank conflicts) and one lane
+//     stores the tile with a tiled TMA store (a row-per-lane global store
+//     would touch 32 lines per instruction).
 //
 // Every mbarrier wait is bounded in time and also ends when another role
 // has given up (shared abort flag); a wait that gives up sets the error
@@ -52,6 +57,33 @@ __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map
 	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
 	             "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
 	             "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(row), "r"(mbar)
+	             : "memory");
+}
+
+// tiled TMA store of a 32-row box from this CTA's shared memory to rows
+// row .. row+31 of a 2-D tensor (bulk async-group of the issuing thread)
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, unsigned src, int row)
+{
+	asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+	                 reinterpret_cast<unsigned long long>(map)),
+	             "r"(0), "r"(row), "r"(src)
+	             : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+
+// the issuing thread's bulk stores have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+
+// the issuing thread's bulk stores are complete (written to global memory)
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+// generic-proxy writes to shared memory become visible to the TMA unit
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+__device__ __forceinline__ void st_shared_v4(unsigned addr, float a, float b, float c, float d)
+{
+	asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
 	             : "memory");
 }
 
@@ -257,6 +289,46 @@ __device__ __forceinline__ void store_chunk(const TcArgs& a, const GemmTile& t, 
 	}
 }
 
+// pass 1, a warp's 32 full rows (tile rows row0 .. row0+31, all inside the
+// matrix): the thread of tile row row0 + lane writes its 128-byte BX row of
+// chunk (n0 + c0) / 32 into the warp's staging tile (hi at stg, lo at
+// stg + 4096; 16-byte piece q of row r at r*128 + (q ^ (r % 8))*16, the
+// TMA unit's 128-byte swizzle of a 1024-aligned box), and lane 0 stores
+// both tiles.  Columns past N are the K padding of pass 2: zeros.
+template <int BN>
+__device__ __forceinline__ void store_chunk_tma(const TcArgs& a, const GemmTile& t, int row0, int c0,
+                                                const float (&v)[32], unsigned stg, int lane)
+{
+	const int col0 = t.n0 + c0;
+	if (col0 >= t.N)
+		return;
+	if (lane == 0)
+		bulk_wait_read(); // the previous chunk's stores have read the tile
+	__syncwarp();
+	const unsigned rowaddr = stg + unsigned(lane) * 128u;
+#pragma unroll
+	for (int q = 0; q < 8; ++q) {
+		float hv[4], lv[4];
+#pragma unroll
+		for (int e = 0; e < 4; ++e) {
+			const float x = (col0 + 4 * q + e < t.N) ? v[4 * q + e] : 0.f;
+			hv[e]         = tf32_rna(x);
+			lv[e]         = tf32_rna(x - hv[e]);
+		}
+		const unsigned off = unsigned((q ^ (lane & 7)) << 4);
+		st_shared_v4(rowaddr + off, hv[0], hv[1], hv[2], hv[3]);
+		st_shared_v4(rowaddr + 4096u + off, lv[0], lv[1], lv[2], lv[3]);
+	}
+	fence_proxy_async();
+	__syncwarp();
+	if (lane == 0) {
+		const int R = int(t.c_off >> 5) + (col0 >> 5) * t.ldc + t.m0 + row0;
+		tma_store_2d(&a.C_hi_map, stg, R);
+		tma_store_2d(&a.C_lo_map, stg + 4096u, R);
+		bulk_commit();
+	}
+}
+
 // the 4 epilogue warps only (named barrier 1)
 __device__ __forceinline__ void epilogue_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
 
@@ -324,12 +396,13 @@ __device__ __forceinline__ void reduce_split(const TcArgs& a, const GemmTile& t,
 
 template <int BN, bool PASS1>
 __device__ void epilogue(const TcArgs& a, unsigned tmem, unsigned accf0, unsigned acce0,
-                         volatile int* abort)
+                         volatile int* abort, unsigned staging)
 {
 	__shared__ int s_last;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int quarter = warp & 3; // TMEM lanes this warp may read
 	const int row     = quarter * 32 + lane;
+	const unsigned stg = staging + unsigned(warp - 2) * 8192u; // pass 1: this warp's tile
 	unsigned  tc      = 0;
 	bool      ok      = true;
 	for (int ti = a.starts[blockIdx.x]; ti < a.starts[blockIdx.x + 1]; ++ti) {
@@ -356,10 +429,15 @@ __device__ void epilogue(const TcArgs& a, unsigned tmem, unsigned accf0, unsigne
 		}
 		tc_fence_after();
 		const bool split = !PASS1 && t.nsplit >= 2;
+		// pass 1: this warp's 32 rows all inside the matrix (the same for
+		// every lane) -> staged TMA stores; a partial row group stores directly
+		const bool staged = PASS1 && t.m0 + quarter * 32 + 32 <= t.M;
 		for (int c0 = 0; c0 < BN; c0 += 32) {
 			tmem_ld32(tmem + (unsigned(quarter * 32) << 16) + b * unsigned(BN) + unsigned(c0), v);
 			if (split)
 				store_partial<BN>(a, t, row, c0, v);
+			else if (staged)
+				store_chunk_tma<BN>(a, t, quarter * 32, c0, v, stg, lane);
 			else
 				store_chunk<BN, PASS1>(a, t, grow, c0, v);
 		}
@@ -387,6 +465,8 @@ __device__ void epilogue(const TcArgs& a, unsigned tmem, unsigned accf0, unsigne
 			}
 		}
 	}
+	if (PASS1 && lane == 0)
+		bulk_wait_all(); // this warp's TMA stores are written before the CTA exits
 	if (!ok && lane == 0)
 		give_up(abort, a.error);
 }
@@ -439,7 +519,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_tf32x3_kernel(const __g
 		if ((threadIdx.x & 31) == 0)
 			mma_issuer<BN, STAGES>(a, base, tmem, full0, empty0, accf0, acce0, drain, &abort_flag);
 	} else {
-		epilogue<BN, PASS1>(a, tmem, accf0, acce0, &abort_flag);
+		epilogue<BN, PASS1>(a, tmem, accf0, acce0, &abort_flag,
+		                    base + unsigned(STAGES * TcLayout<BN>::STAGE_BYTES));
 	}
 	__syncwarp();
 	tc_fence_before();
@@ -487,15 +568,19 @@ pack_tf32_kernel(const double* __restrict__ ops, float* __restrict__ hi, float* 
 	}
 }
 
-template <int BN, int STAGES> constexpr size_t tc_smem()
+// the ring, the 1 KB alignment slack and, in pass 1, four 8 KB staging
+// tiles of the epilogue warps (1024-aligned: the ring's stages are)
+template <int BN, int STAGES, bool PASS1> constexpr size_t tc_smem()
 {
-	return size_t(STAGES) * TcLayout<BN>::STAGE_BYTES + 1024;
+	return size_t(STAGES) * TcLayout<BN>::STAGE_BYTES + 1024 + (PASS1 ? 4 * 8192 : 0);
 }
 
 template <int BN, int STAGES, bool PASS1> cudaError_t tc_init_one()
 {
+	static_assert(tc_smem<BN, STAGES, PASS1>() + 256 <= 232448, "shared memory per CTA");
 	return cudaFuncSetAttribute(tc_gemm_tf32x3_kernel<BN, STAGES, PASS1>,
-	                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(tc_smem<BN, STAGES>()));
+	                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                            int(tc_smem<BN, STAGES, PASS1>()));
 }
 
 // ring depth: as many stages as fit in 227 KB with the 1 KB alignment slack
@@ -504,7 +589,7 @@ constexpr int kStages128 = 3; // 3 x 64 KB
 
 template <int BN, int STAGES, bool PASS1> void launch_one(const TcArgs& a, cudaStream_t stream)
 {
-	tc_gemm_tf32x3_kernel<BN, STAGES, PASS1><<<a.grid, kTcThreads, tc_smem<BN, STAGES>(), stream>>>(a);
+	tc_gemm_tf32x3_kernel<BN, STAGES, PASS1><<<a.grid, kTcThreads, tc_smem<BN, STAGES, PASS1>(), stream>>>(a);
 }
 
 } // namespace

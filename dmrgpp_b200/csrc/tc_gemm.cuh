@@ -12,6 +12,9 @@ struct TcArgs {
 	// the pass's operand buffers as 2-D TMA tensors [row][32 floats]
 	// (kron_plan.h): A with 128-row boxes, B with BN-row boxes; hi and lo
 	CUtensorMap A_hi, A_lo, B_hi, B_lo;
+	// pass 1: the split output buffers (hi, lo) as the same 2-D tensors with
+	// 32-row boxes, for the epilogue's tiled TMA stores
+	CUtensorMap C_hi_map, C_lo_map;
 	float*          C_hi; // pass 1: K-major split output
 	float*          C_lo;
 	double*         Cd;   // pass 2: FP64 column-major output

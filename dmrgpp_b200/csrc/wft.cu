@@ -140,7 +140,7 @@ int dmrgpp_wft_create(const dmrgpp_wft_desc* d, dmrgpp_wft_handle* out)
 	    || (e = dmrgpp::dev_malloc(&h->d_x, bytes(P.dim_in()))) || (e = dmrgpp::dev_malloc(&h->d_y, bytes(P.dim_out()))))
 		return bail(e, "device allocation");
 	if (P.op_elems > 0
-	    && (e = cudaMemcpy(h->d_ops, packed.data(), size_t(P.op_elems) * sizeof(double), cudaMemcpyHostToDevice)))
+	    && (e = dmrgpp::upload_sync(h->d_ops, packed.data(), size_t(P.op_elems) * sizeof(double), h->stream)))
 		return bail(e, "upload transformation blocks");
 	// the four launch lists in one allocation, 16-byte aligned parts
 	std::vector<unsigned char> lists;
@@ -157,7 +157,7 @@ int dmrgpp_wft_create(const dmrgpp_wft_desc* d, dmrgpp_wft_handle* out)
 	add(P.tileB.data(), P.tileB.size() * sizeof(dmrgpp::GemmTile));
 	if ((e = dmrgpp::dev_malloc(&h->d_lists, lists.empty() ? 16 : lists.size())))
 		return bail(e, "device allocation (lists)");
-	if (!lists.empty() && (e = cudaMemcpy(h->d_lists, lists.data(), lists.size(), cudaMemcpyHostToDevice)))
+	if (!lists.empty() && (e = dmrgpp::upload_sync(h->d_lists, lists.data(), lists.size(), h->stream)))
 		return bail(e, "upload lists");
 	unsigned char* base = static_cast<unsigned char*>(h->d_lists);
 	h->segA  = reinterpret_cast<dmrgpp::GemmSeg*>(base + offs[0]);

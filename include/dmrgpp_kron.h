@@ -289,8 +289,9 @@ int dmrgpp_kron_set_config(dmrgpp_kron_handle h, int cfg, int items_per_cta);
 /* Times every configuration on this sector (reps applies each, minimum
  * kept), keeps the fastest and returns it with its time in microseconds.
  * cache_path (may be NULL): text file of earlier choices keyed by a
- * signature of the sector-size histogram and the GPU name; a hit skips the
- * timing, a miss appends the new choice. */
+ * signature of the sector-size histogram (work quartiles and maximum of the
+ * patch dimensions by octave, total work, terms) and the GPU name; a hit
+ * skips the timing, a miss appends the new choice. */
 int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps, int* cfg,
                          double* us);
 

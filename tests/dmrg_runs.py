@@ -92,9 +92,12 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", 
                 bg.autotune(cache, reps=5)
                 t_tune = time.perf_counter() - t0
                 t64_us, t32_us = bg.tuned_times()
+            pool0 = plugin.cached_memory()[0]
             (e, z, st), t_mx = _timed(lambda: bg.solve_lowest(x, tolerance=1e-10, method=method))
+            pool1 = plugin.cached_memory()[0]
             bg.set_precision(plugin.FP64)
             (e64, z64, n64), t_64 = _timed(lambda: bg.lanczos_lowest(x, steps=400, tolerance=1e-10))
+            pool2 = plugin.cached_memory()[0]
         finally:
             bg.close()
         n1 = st.get("mixed_lanczos_steps", st.get("fp64_lanczos_steps", 0))
@@ -108,7 +111,8 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", 
                    refine_seconds=st.get("refine_seconds", 0.0),
                    refine_outer=int(st.get("outer_iterations", -1)),
                    refine_inner_matvecs=int(st.get("inner_matvecs", -1)),
-                   tune_seconds=t_tune, tuned_fp64_us=t64_us, tuned_tf32x3_us=t32_us)
+                   tune_seconds=t_tune, tuned_fp64_us=t64_us, tuned_tf32x3_us=t32_us,
+                   pool_growth_mixed=pool1 - pool0, pool_growth_fp64=pool2 - pool1)
         steps.append(rec)
         if len(steps) % 20 == 0:
             log(f"step {len(steps)} dim {prob.dim} E {e:.12f} dE/site {rec['abs_dE_per_site']:.2e}")

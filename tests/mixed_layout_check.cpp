@@ -280,6 +280,23 @@ int main(int argc, char** argv)
 						}
 				}
 			}
+			if (pass1 && t.c_off % 32 != 0)
+				return fail("BX matrix not on a 32-float row", t.c_off, 0);
+			// pass 1's staged stores: a warp's 32 rows (all inside the matrix)
+			// of one chunk as one 32-row box at buffer row R, which must be
+			// the rows the per-element offsets below name
+			for (int q = 0; pass1 && q < 4; ++q) {
+				if (t.m0 + 32 * q + 32 > t.M)
+					continue;
+				for (int c0 = 0; c0 < bn && t.n0 + c0 < t.N; c0 += 32) {
+					const int       col0 = t.n0 + c0;
+					const long long R    = t.c_off / 32 + (long long)(col0 >> 5) * t.ldc + t.m0 + 32 * q;
+					const long long o0   = t.c_off + (long long)(col0 >> 5) * t.ldc * 32
+					    + (long long)(t.m0 + 32 * q) * 32;
+					if (R < 0 || R > INT_MAX || (R + 32) * 32 > mp.bxs_elems || R * 32 != o0)
+						return fail("staged BX store rows", R, mp.bxs_elems);
+				}
+			}
 			for (int m = 0; m < BM; ++m) {
 				const int grow = t.m0 + m;
 				for (int c0 = 0; c0 < bn; c0 += 32) {

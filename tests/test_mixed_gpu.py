@@ -188,3 +188,35 @@ def test_solve_lowest_auto_follows_the_tuned_times(cuda_lib, cuda_device, which,
     bg.close()
     assert abs(e - e64) <= 1e-9 * abs(e64)
     assert 1.0 - abs(float(torch.dot(z, z64))) <= 1e-6
+
+
+def test_handles_on_a_non_blocking_stream_after_another_handle(cuda_lib, cuda_device, oracle_built):
+    """Handles created on a caller's non-blocking stream (torch's streams are)
+    over pool memory that an earlier handle left dirty: every clear and
+    upload of the create must be ordered on that stream (a legacy-stream
+    clear could land after the operators were packed; seen as a wrong
+    TF32x3 H*x on the 4000-state ladder sector)."""
+    import torch
+    from dmrgpp_b200 import plugin
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        first = sb.c2_problem()
+        bg = mixed(first, stream=s.cuda_stream)
+        xd = torch.from_numpy(sb.random_unit_vector(first.dim, seed=2)).cuda()
+        yd = torch.empty_like(xd)
+        bg.apply_Htarget(xd, yd)
+        s.synchronize()
+        bg.close()
+        for states in (4000, 8000):
+            prob = sb.ladder_problem(total_states=states)
+            x = np.random.default_rng(1).standard_normal(prob.dim)
+            ref = oracle_built.kron_apply(prob, x)
+            for prec, tol in ((plugin.TF32X3, RTOL_MIXED), (plugin.FP64, 1e-12)):
+                bg = plugin.BatchedGemm.from_problem(prob, precision=prec, stream=s.cuda_stream)
+                xd = torch.from_numpy(x).cuda()
+                yd = torch.empty_like(xd)
+                bg.apply_Htarget(xd, yd)
+                s.synchronize()
+                y = yd.cpu().numpy()
+                bg.close()
+                assert rel_err(y, ref) < tol, (states, prec)
