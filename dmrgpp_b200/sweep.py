@@ -54,10 +54,13 @@ def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int 
     # have gone back to the library's memory pool and the pinned staging
     # buffers exist.  Stand-in: one untimed create of the same sector with a
     # few Lanczos steps sized for lanczos_steps (the basis is allocated for
-    # the step limit), then destroyed.
+    # the step limit) and one Davidson iteration (its subspace buffers), then
+    # destroyed.
     warm = plugin.BatchedGemm.from_problem(prob, precision=plugin.TF32X3)
     warm.set_precision(plugin.FP64)
     warm.lanczos_lowest(init, steps=lanczos_steps, min_steps=2, tolerance=1e300)
+    warm.davidson_lowest(init, preconditioner=1, tolerance=1e300, max_iterations=1,
+                         raise_on_no_convergence=False)
     warm.close()
     pool_before = plugin.cached_memory()[0]
     b64 = plugin.BatchedGemm.from_problem(prob, precision=plugin.FP64)
