@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <utility>
 #include <cstdio>
 #include <cstring>
@@ -79,6 +80,22 @@ std::string sector_signature(const KronPlan& P, const char* gpu)
 	char buf[32];
 	std::snprintf(buf, sizeof(buf), "%016llx", h);
 	return buf;
+}
+
+// The GPU's name, queried once per device (cudaGetDeviceProperties fills
+// every property, which costs far more than a cache lookup of a sweep step).
+std::string device_name(int device)
+{
+	static std::mutex                 mu;
+	static std::map<int, std::string> names;
+	std::lock_guard<std::mutex>       g(mu);
+	auto                              it = names.find(device);
+	if (it != names.end())
+		return it->second;
+	cudaDeviceProp prop {};
+	std::string    name = cudaGetDeviceProperties(&prop, device) == cudaSuccess ? prop.name : "unknown";
+	names[device]       = name;
+	return name;
 }
 
 // One line per entry: signature, configuration, items per CTA, the FP64
@@ -171,9 +188,7 @@ int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps,
 		}
 	} restore { h->device, prev };
 
-	cudaDeviceProp prop {};
-	cudaGetDeviceProperties(&prop, h->device);
-	const std::string sig = sector_signature(h->plan, prop.name);
+	const std::string sig = sector_signature(h->plan, device_name(h->device).c_str());
 	int               cfg = 0, ipc = 2;
 	double            us  = 0.0;
 	cudaEvent_t       e0, e1;

@@ -226,10 +226,12 @@ int dmrgpp_kron_setup_profile(dmrgpp_kron_handle h, double* t, size_t n);
 
 /* Device memory of handles and solver workspaces comes from one
  * stream-ordered pool per device that keeps freed memory for the next handle
- * (a sweep destroys and creates a handle of similar size every step).
- * dmrgpp_release_cached_memory returns the unused part to the device
- * (device < 0: the current device); dmrgpp_cached_memory reports the pool's
- * reserved and in-use bytes. */
+ * (a sweep destroys and creates a handle of similar size every step); freed
+ * blocks of 64 MB and more also stay on a free list by size for the next
+ * request of about their size.  dmrgpp_release_cached_memory returns the
+ * unused part to the device (device < 0: the current device);
+ * dmrgpp_cached_memory reports the pool's reserved bytes and the bytes in
+ * use (free-listed blocks not counted). */
 int dmrgpp_release_cached_memory(int device);
 int dmrgpp_cached_memory(int device, size_t* reserved_bytes, size_t* used_bytes);
 

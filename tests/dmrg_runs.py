@@ -70,12 +70,17 @@ def mixed_solve(bg, init, sites, tolerance=1e-10):
     return e, z, st["mixed_lanczos_steps"], st
 
 
-def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", tune=True):
+def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", tune=True,
+       repeats=1):
     """method: the library's solve_lowest method of the measured arm
     ("mixed", or "auto": mixed only where the tuned TF32x3 H*x is at least
     1.5x the tuned FP64 one).  tune: autotune every sector's FP64
     configuration through one tuning cache for the run (its bucketed keys let
-    later steps reuse earlier timings; the tuning seconds are recorded)."""
+    later steps reuse earlier timings; the tuning seconds are recorded).
+    repeats: each step's two solves are timed that many times from the same
+    start (the first result drives the sweep; every time is recorded, and
+    the per-step minimum separates the solvers' own time from stalls that
+    come from outside them)."""
     import tempfile
     import torch
     from dmrgpp_b200 import plugin
@@ -98,6 +103,12 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", 
             bg.set_precision(plugin.FP64)
             (e64, z64, n64), t_64 = _timed(lambda: bg.lanczos_lowest(x, steps=400, tolerance=1e-10))
             pool2 = plugin.cached_memory()[0]
+            t_mx_all, t_64_all = [t_mx], [t_64]
+            for _ in range(repeats - 1):
+                bg.set_precision(plugin.TF32X3)
+                t_mx_all.append(_timed(lambda: bg.solve_lowest(x, tolerance=1e-10, method=method))[1])
+                bg.set_precision(plugin.FP64)
+                t_64_all.append(_timed(lambda: bg.lanczos_lowest(x, steps=400, tolerance=1e-10))[1])
         finally:
             bg.close()
         n1 = st.get("mixed_lanczos_steps", st.get("fp64_lanczos_steps", 0))
@@ -112,7 +123,8 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", 
                    refine_outer=int(st.get("outer_iterations", -1)),
                    refine_inner_matvecs=int(st.get("inner_matvecs", -1)),
                    tune_seconds=t_tune, tuned_fp64_us=t64_us, tuned_tf32x3_us=t32_us,
-                   pool_growth_mixed=pool1 - pool0, pool_growth_fp64=pool2 - pool1)
+                   pool_growth_mixed=pool1 - pool0, pool_growth_fp64=pool2 - pool1,
+                   mixed_seconds_all=t_mx_all, fp64_seconds_all=t_64_all)
         steps.append(rec)
         if len(steps) % 20 == 0:
             log(f"step {len(steps)} dim {prob.dim} E {e:.12f} dE/site {rec['abs_dE_per_site']:.2e}")
@@ -131,6 +143,9 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", 
                max_dim=max(s["dim"] for s in steps),
                solve_seconds_mixed=sum(s["mixed_seconds"] for s in steps),
                solve_seconds_fp64=sum(s["fp64_seconds"] for s in steps),
+               solve_seconds_mixed_min_of_repeats=sum(min(s["mixed_seconds_all"]) for s in steps),
+               solve_seconds_fp64_min_of_repeats=sum(min(s["fp64_seconds_all"]) for s in steps),
+               repeats=repeats,
                tune_seconds=sum(s["tune_seconds"] for s in steps), method=method,
                steps_solved_mixed=sum(s["method"] == "mixed" for s in steps),
                wall_seconds_mixed_run=time.time() - t0, per_step=steps)
@@ -473,6 +488,7 @@ def main(argv=None):
     p.add_argument("--no-fp64-run", action="store_true")
     p.add_argument("--method", default="mixed", choices=["mixed", "auto"])
     p.add_argument("--no-tune", action="store_true")
+    p.add_argument("--repeats", type=int, default=1)
     p.add_argument("--mlp", default=None, help="learned-correction weights (.npz)")
     p.add_argument("--out", default=None)
     a = p.parse_args(argv)
@@ -496,7 +512,7 @@ def main(argv=None):
         return
     if a.what == "c3":
         out = c3(L=a.L, m=a.m or 1000, sweeps=a.sweeps, fp64_run=not a.no_fp64_run,
-                 method=a.method, tune=not a.no_tune)
+                 method=a.method, tune=not a.no_tune, repeats=a.repeats)
     else:
         from dmrgpp_b200.mlp import MLPPreconditioner
         mlp = MLPPreconditioner.load(a.mlp) if a.mlp else None

@@ -285,6 +285,29 @@ def test_memory_pool_reuses_freed_handles(cuda_lib, cuda_device):
     assert u3 <= r3 < r1
 
 
+def test_large_blocks_are_reused_from_the_free_list(cuda_lib, cuda_device, oracle_built):
+    """Blocks of 64 MB and more (here the 8000-state ladder sector's packed
+    operators, 134 MB) go to a free list when a handle is destroyed and serve
+    the next create of the same sector without the pool growing; they are
+    not counted as in use, and releasing the cache returns them."""
+    from dmrgpp_b200 import plugin
+    prob = sb.ladder_problem(total_states=8000)
+    x = np.random.default_rng(4).standard_normal(prob.dim)
+    plugin.BatchedGemm.from_problem(prob).close()
+    r1, u1 = plugin.cached_memory()
+    bg = plugin.BatchedGemm.from_problem(prob)
+    r2, u2 = plugin.cached_memory()
+    y = bg(x)
+    bg.close()
+    r3, u3 = plugin.cached_memory()
+    assert r2 == r1 and r3 == r1
+    assert u2 - u1 >= prob.operator_bytes() and u3 == u1
+    assert rel_err(y, oracle_built.kron_apply(prob, x)) < RTOL
+    plugin.release_cached_memory()
+    r4, _ = plugin.cached_memory()
+    assert r4 < r1 - prob.operator_bytes()
+
+
 @pytest.mark.parametrize("which", ["c2", "ladder", "group"])
 def test_page_locked_host_vectors(cuda_lib, cuda_device, oracle_built, which):
     """Page-locked host x and y (copied in and out around the launch): the
