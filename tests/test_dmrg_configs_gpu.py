@@ -1,6 +1,7 @@
 """The benchmark's DMRG configurations through the CUDA solver (the sweep
 engine is the oracle's two-site driver; tests/dmrg_runs.py holds the runs,
-whose full-length forms are recorded in the design notes).
+here at reduced length: one finite sweep of the Hubbard chain, one ladder
+sector).
 
 * Hubbard chain, t=1, U=4, open BC, half filling, L=64, m=1000 (the
   configuration's size) over the infinite growth and one finite sweep: the
