@@ -199,6 +199,7 @@ SIGNATURES.update({
     "dmrgpp_kron_gather_index": (ctypes.c_int, [ctypes.POINTER(GatherIndexDesc),
                                                 ctypes.POINTER(ctypes.c_int64)]),
     "dmrgpp_kron_tuned_times": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "dmrgpp_set_correction_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dmrgpp_kron_patch_list": (ctypes.c_int, [_sz, ctypes.POINTER(ctypes.c_int64), _sz,
                                               ctypes.POINTER(ctypes.c_int64), _sz,
                                               ctypes.POINTER(ctypes.c_int64), _sz, _szp, _szp,

@@ -102,6 +102,7 @@ struct dmrgpp_kron_s {
 	dmrgpp::GemmTile*   m_tile2 = nullptr;
 	dmrgpp::LanczosWork* lanczos = nullptr;
 	double*             d_diag = nullptr; // diagonal of H (patch order)
+	int                 correction_precond = 0; // dmrgpp_correction_solve: DMRGPP_PRECOND_NONE or _JACOBI
 	dmrgpp::DavidsonWork* davidson = nullptr;
 	dmrgpp::GroupWork*  group = nullptr;   // group Lanczos buffers (group_lanczos.cu)
 	const dmrgpp::CrsSource* crs = nullptr; // create time only: build the blocks from CRS operators

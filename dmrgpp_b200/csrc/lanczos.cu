@@ -1346,10 +1346,217 @@ k_cg_direction(double* __restrict__ p, const double* __restrict__ res, const dou
 		p[i] = res[i] + beta * p[i];
 }
 
+// --- diagonal (Jacobi) preconditioner of the projected correction equation
+// P (H - theta) P t = -P r on the complement of u:  K = diag(H) - theta, kept
+// at least `floor`; the preconditioned direction z = K^-1 res - a K^-1 u with
+// a = <u, K^-1 res> / <u, K^-1 u> stays orthogonal to u (the projected
+// preconditioner P K P of Jacobi-Davidson).  wv = K^-1 u.
+__device__ __forceinline__ double pcg_k(double d, double theta, double floor_)
+{
+	const double k = d - theta;
+	return k > floor_ ? k : floor_;
+}
+
+// wv = K^-1 u, *uw = <u, wv>
+__global__ void __launch_bounds__(kThreads)
+k_pcg_setup(const double* __restrict__ u, const double* __restrict__ diag, double theta, double floor_,
+            double* __restrict__ wv, size_t n, double* uw, double* partial, unsigned* ctr)
+{
+	__shared__ double red[kThreads / 32];
+	double            s = 0.0;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		const double v = u[i] / pcg_k(diag[i], theta, floor_);
+		wv[i]          = v;
+		s += u[i] * v;
+	}
+	s = block_sum(s, red);
+	grid_sum(s, partial, ctr, uw, false, red);
+}
+
+// four sums at once (deterministic: per-block partials in 4 strided slots,
+// the last block adds them in block order): sums[0..3]
+__device__ __forceinline__ void grid_sum4(double (&v)[4], double* partial, unsigned* ctr, double* sums,
+                                          double* red)
+{
+	__shared__ bool last;
+	double          b[4];
+#pragma unroll
+	for (int q = 0; q < 4; ++q)
+		b[q] = block_sum(v[q], red);
+	if (threadIdx.x == 0) {
+#pragma unroll
+		for (int q = 0; q < 4; ++q)
+			partial[size_t(q) * gridDim.x + blockIdx.x] = b[q];
+		last = last_block(ctr);
+	}
+	__syncthreads();
+	if (!last)
+		return;
+#pragma unroll
+	for (int q = 0; q < 4; ++q) {
+		double t = 0.0;
+		for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x)
+			t += __ldcg(partial + size_t(q) * gridDim.x + k);
+		t = block_sum(t, red);
+		if (threadIdx.x == 0)
+			sums[q] = t;
+	}
+}
+
+// sums = <u, K^-1 res>, <res, K^-1 res>, <res, wv>, <res, res>
+__device__ __forceinline__ void pcg_sums_body(const double* __restrict__ res, const double* __restrict__ diag,
+                                              double theta, double floor_, const double* __restrict__ u,
+                                              const double* __restrict__ wv, size_t n, double* sums,
+                                              double* partial, unsigned* ctr, double* red)
+{
+	double v[4] = { 0.0, 0.0, 0.0, 0.0 };
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		const double r = res[i];
+		const double z = r / pcg_k(diag[i], theta, floor_);
+		v[0] += u[i] * z;
+		v[1] += r * z;
+		v[2] += r * wv[i];
+		v[3] += r * r;
+	}
+	grid_sum4(v, partial, ctr, sums, red);
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_pcg_sums(const double* __restrict__ res, const double* __restrict__ diag, double theta, double floor_,
+           const double* __restrict__ u, const double* __restrict__ wv, size_t n, double* sums,
+           double* partial, unsigned* ctr)
+{
+	__shared__ double red[kThreads / 32];
+	pcg_sums_body(res, diag, theta, floor_, u, wv, n, sums, partial, ctr, red);
+}
+
+// alpha = rho / pAp; t += alpha p; res -= alpha Aq; then the four sums of the
+// new res.  A non-positive pAp (or an earlier one, *broken) freezes the
+// iteration: alpha = 0 and *broken = 1.
+__global__ void __launch_bounds__(kThreads)
+k_pcg_update(double* __restrict__ t, double* __restrict__ res, const double* __restrict__ p,
+             const double* __restrict__ Aq, const double* rho, const double* pAp, double* broken,
+             const double* __restrict__ diag, double theta, double floor_, const double* __restrict__ u,
+             const double* __restrict__ wv, size_t n, double* sums, double* partial, unsigned* ctr)
+{
+	__shared__ double red[kThreads / 32];
+	const bool        stop  = *broken != 0.0 || !(*pAp > 0.0);
+	const double      alpha = stop ? 0.0 : *rho / *pAp;
+	if (stop && blockIdx.x == 0 && threadIdx.x == 0)
+		*broken = 1.0;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		t[i] += alpha * p[i];
+		res[i] -= alpha * Aq[i];
+	}
+	// each thread re-reads only the elements it wrote: no grid barrier needed
+	pcg_sums_body(res, diag, theta, floor_, u, wv, n, sums, partial, ctr, red);
+}
+
+// z = K^-1 res - a wv with a = sums[0] / *uw; rho_new = sums[1] - a sums[2];
+// p = z + (rho_new / *rho) p (p = z when first); *rho_next = rho_new.
+// Skipped once the iteration is frozen.
+__global__ void __launch_bounds__(kThreads)
+k_pcg_direction(double* __restrict__ p, const double* __restrict__ res, const double* __restrict__ diag,
+                double theta, double floor_, const double* __restrict__ wv, const double* uw,
+                const double* sums, const double* rho, double* rho_next, const double* broken, int first,
+                size_t n)
+{
+	if (*broken != 0.0)
+		return;
+	const double a       = *uw > 0.0 ? sums[0] / *uw : 0.0;
+	const double rho_new = sums[1] - a * sums[2];
+	const double beta    = first ? 0.0 : (*rho > 0.0 ? rho_new / *rho : 0.0);
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		*rho_next = rho_new;
+	for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n;
+	     i += size_t(gridDim.x) * kThreads) {
+		const double z = res[i] / pcg_k(diag[i], theta, floor_) - a * wv[i];
+		p[i]           = z + beta * p[i];
+	}
+}
+
+} // namespace
+} // namespace dmrgpp
+
+namespace dmrgpp {
+namespace {
+
+// The correction equation by conjugate gradients with the projected
+// diagonal preconditioner (see k_pcg_setup); res (= -P r on entry, as the
+// caller set it) and the Davidson buffers as in dmrgpp_correction_solve;
+// the preconditioner's K^-1 u lives in the Davidson work's free column t.
+int pcg_correction(dmrgpp_kron_handle h, const double* u, double theta, const double* r, double* t,
+                   int max_iterations, double rel_tolerance, int* iterations, double* rel_residual)
+{
+	(void)r;
+	const size_t  D  = size_t(h->plan.dim());
+	DavidsonWork* w  = h->davidson;
+	cudaStream_t  st = h->stream;
+	const int     nb = blocks_for(D);
+	double*       res = w->hu;
+	double*       p   = w->r;
+	double*       Aq  = w->V + D;
+	double*       wv  = w->t;
+	double*       sc  = w->scal; // [0] u.v [1] pAp [4] frozen [5] uw [6..9] sums [10,11] rho
+	const double  floor_ = 1e-3 * std::max(1.0, std::fabs(theta));
+	auto read = [&](double* dev, int count, double* host) {
+		return cudaMemcpyAsync(host, dev, size_t(count) * sizeof(double), cudaMemcpyDeviceToHost, st)
+		        == cudaSuccess
+		    && cudaStreamSynchronize(st) == cudaSuccess;
+	};
+	k_pcg_setup<<<nb, kThreads, 0, st>>>(u, h->d_diag, theta, floor_, wv, D, sc + 5, w->partial, w->ctr + 8);
+	k_pcg_sums<<<nb, kThreads, 0, st>>>(res, h->d_diag, theta, floor_, u, wv, D, sc + 6, w->partial, w->ctr + 9);
+	k_pcg_direction<<<nb, kThreads, 0, st>>>(p, res, h->d_diag, theta, floor_, wv, sc + 5, sc + 6, sc + 10,
+	                                         sc + 10, sc + 4, 1, D);
+	double host[4] = { 0, 0, 0, 0 };
+	if (!read(sc + 9, 1, host))
+		return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+	const double b0  = std::sqrt(host[0]);
+	double       rrh = host[0];
+	int          it  = 0;
+	int          cur = 0; // rho of the current direction lives in sc[10 + cur]
+	cudaError_t  e;
+	while (it < max_iterations && b0 > 0 && std::sqrt(rrh) > rel_tolerance * b0) {
+		const int burst = std::min(8, max_iterations - it);
+		for (int q = 0; q < burst; ++q, ++it) {
+			// Aq = P (H - theta) p  (p orthogonal to u up to round-off)
+			if (int rc = kron_apply_device(h, p, Aq))
+				return rc;
+			k_axpy<<<nb, kThreads, 0, st>>>(-theta, p, Aq, D);
+			k_dot<<<nb, kThreads, 0, st>>>(u, Aq, D, sc + 0, w->partial, w->ctr + 5);
+			k_axpy_neg_dev<<<nb, kThreads, 0, st>>>(sc + 0, u, Aq, D);
+			k_dot<<<nb, kThreads, 0, st>>>(p, Aq, D, sc + 1, w->partial, w->ctr + 7);
+			k_pcg_update<<<nb, kThreads, 0, st>>>(t, res, p, Aq, sc + 10 + cur, sc + 1, sc + 4, h->d_diag,
+			                                      theta, floor_, u, wv, D, sc + 6, w->partial, w->ctr + 9);
+			k_pcg_direction<<<nb, kThreads, 0, st>>>(p, res, h->d_diag, theta, floor_, wv, sc + 5, sc + 6,
+			                                         sc + 10 + cur, sc + 11 - cur, sc + 4, 0, D);
+			cur ^= 1;
+		}
+		if ((e = cudaGetLastError()))
+			return cuda_status(h, e, "correction solve launch");
+		double four[6];
+		if (!read(sc + 4, 6, four))
+			return handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+		rrh = four[5]; // sums[3] = |res|^2
+		if (four[0] != 0.0)
+			break; // the projected operator was not positive definite
+	}
+	if (iterations)
+		*iterations = it;
+	if (rel_residual)
+		*rel_residual = b0 > 0 ? std::sqrt(rrh) / b0 : 0.0;
+	return cudaStreamSynchronize(st) == cudaSuccess ? DMRGPP_OK
+	                                                : handle_fail(h, DMRGPP_CUDA_ERROR, "correction solve");
+}
+
 } // namespace
 } // namespace dmrgpp
 
 extern "C" {
+
 
 int dmrgpp_kron_diagonal(dmrgpp_kron_handle h, double* diag)
 {
@@ -1362,6 +1569,16 @@ int dmrgpp_kron_diagonal(dmrgpp_kron_handle h, double* diag)
 	        == cudaSuccess
 	    ? DMRGPP_OK
 	    : DMRGPP_CUDA_ERROR;
+}
+
+int dmrgpp_set_correction_preconditioner(dmrgpp_kron_handle h, int preconditioner)
+{
+	if (!h)
+		return DMRGPP_INVALID_ARG;
+	if (preconditioner != DMRGPP_PRECOND_NONE && preconditioner != DMRGPP_PRECOND_JACOBI)
+		return dmrgpp::handle_fail(h, DMRGPP_INVALID_ARG, "correction preconditioner: none or Jacobi");
+	h->correction_precond = preconditioner;
+	return DMRGPP_OK;
 }
 
 int dmrgpp_correction_solve(dmrgpp_kron_handle h, const double* u, double theta, const double* r,
@@ -1399,6 +1616,8 @@ int dmrgpp_correction_solve(dmrgpp_kron_handle h, const double* u, double theta,
 	k_axpy<<<nb, kThreads, 0, st>>>(-1.0, r, res, D);
 	k_dot<<<nb, kThreads, 0, st>>>(u, res, D, sc + 0, w->partial, w->ctr + 5);
 	k_axpy_neg_dev<<<nb, kThreads, 0, st>>>(sc + 0, u, res, D);
+	if (h->correction_precond == DMRGPP_PRECOND_JACOBI && h->d_diag)
+		return pcg_correction(h, u, theta, r, t, max_iterations, rel_tolerance, iterations, rel_residual);
 	cudaMemcpyAsync(p, res, D * sizeof(double), cudaMemcpyDeviceToDevice, st);
 	k_dot<<<nb, kThreads, 0, st>>>(res, res, D, sc + 2, w->partial, w->ctr + 6);
 	double host[4] = { 0, 0, 0, 0 };

@@ -402,6 +402,16 @@ int dmrgpp_correction_solve(dmrgpp_kron_handle h, const double* u, double theta,
                             double* t, int max_iterations, double rel_tolerance, int* iterations,
                             double* rel_residual);
 
+/* The preconditioner of the correction solves of this handle
+ * (dmrgpp_correction_solve and the FP64 refinement): DMRGPP_PRECOND_NONE
+ * (conjugate gradients on the projected operator, the default) or
+ * DMRGPP_PRECOND_JACOBI (preconditioned by K = diag(H) - theta, kept at
+ * least 1e-3 max(1, |theta|), projected as in Jacobi-Davidson:
+ * z = K^-1 r - (<u, K^-1 r> / <u, K^-1 u>) K^-1 u).  Either solves the same
+ * equation; the refinement's convergence test stays the FP64 residual.  No
+ * counterpart in the reference. */
+int dmrgpp_set_correction_preconditioner(dmrgpp_kron_handle h, int preconditioner);
+
 /* FP64 residual refinement of an approximate lowest eigenvector psi (device,
  * patch order, updated in place), typically the Ritz vector of a solve with
  * mixed-precision matvecs.  Each outer step computes in FP64 the Rayleigh

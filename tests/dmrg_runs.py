@@ -71,7 +71,7 @@ def mixed_solve(bg, init, sites, tolerance=1e-10):
 
 
 def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", tune=True,
-       repeats=1):
+       repeats=1, correction="jacobi"):
     """method: the library's solve_lowest method of the measured arm
     ("mixed", or "auto": mixed only where the tuned TF32x3 H*x is at least
     1.5x the tuned FP64 one).  tune: autotune every sector's FP64
@@ -98,7 +98,8 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", 
                 t_tune = time.perf_counter() - t0
                 t64_us, t32_us = bg.tuned_times()
             pool0 = plugin.cached_memory()[0]
-            (e, z, st), t_mx = _timed(lambda: bg.solve_lowest(x, tolerance=1e-10, method=method))
+            (e, z, st), t_mx = _timed(lambda: bg.solve_lowest(x, tolerance=1e-10, method=method,
+                                                              correction=correction))
             pool1 = plugin.cached_memory()[0]
             bg.set_precision(plugin.FP64)
             (e64, z64, n64), t_64 = _timed(lambda: bg.lanczos_lowest(x, steps=400, tolerance=1e-10))
@@ -106,7 +107,8 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", 
             t_mx_all, t_64_all = [t_mx], [t_64]
             for _ in range(repeats - 1):
                 bg.set_precision(plugin.TF32X3)
-                t_mx_all.append(_timed(lambda: bg.solve_lowest(x, tolerance=1e-10, method=method))[1])
+                t_mx_all.append(_timed(lambda: bg.solve_lowest(x, tolerance=1e-10, method=method,
+                                                              correction=correction))[1])
                 bg.set_precision(plugin.FP64)
                 t_64_all.append(_timed(lambda: bg.lanczos_lowest(x, steps=400, tolerance=1e-10))[1])
         finally:
@@ -145,7 +147,7 @@ def c3(L=64, U=4.0, m=1000, sweeps=6, fp64_run=True, log=print, method="mixed", 
                solve_seconds_fp64=sum(s["fp64_seconds"] for s in steps),
                solve_seconds_mixed_min_of_repeats=sum(min(s["mixed_seconds_all"]) for s in steps),
                solve_seconds_fp64_min_of_repeats=sum(min(s["fp64_seconds_all"]) for s in steps),
-               repeats=repeats,
+               repeats=repeats, correction=correction,
                tune_seconds=sum(s["tune_seconds"] for s in steps), method=method,
                steps_solved_mixed=sum(s["method"] == "mixed" for s in steps),
                wall_seconds_mixed_run=time.time() - t0, per_step=steps)
@@ -489,6 +491,7 @@ def main(argv=None):
     p.add_argument("--method", default="mixed", choices=["mixed", "auto"])
     p.add_argument("--no-tune", action="store_true")
     p.add_argument("--repeats", type=int, default=1)
+    p.add_argument("--correction", default="jacobi", choices=["none", "jacobi"])
     p.add_argument("--mlp", default=None, help="learned-correction weights (.npz)")
     p.add_argument("--out", default=None)
     a = p.parse_args(argv)
@@ -512,7 +515,8 @@ def main(argv=None):
         return
     if a.what == "c3":
         out = c3(L=a.L, m=a.m or 1000, sweeps=a.sweeps, fp64_run=not a.no_fp64_run,
-                 method=a.method, tune=not a.no_tune, repeats=a.repeats)
+                 method=a.method, tune=not a.no_tune, repeats=a.repeats,
+                 correction=a.correction)
     else:
         from dmrgpp_b200.mlp import MLPPreconditioner
         mlp = MLPPreconditioner.load(a.mlp) if a.mlp else None
