@@ -347,8 +347,13 @@ def learned_ablation(torch, bgm, init, stream):
                     "of the batch"}
 
 
+def _capi_precond(name: str) -> int:
+    from dmrgpp_b200 import _capi
+    return _capi.PRECOND_JACOBI if name == "jacobi" else _capi.PRECOND_NONE
+
+
 def serving_measurements(torch, dev, stream, cpu_sample: bool = True, probs=None, meta=None,
-                         workload=None):
+                         workload=None, correction: str = "none"):
     """Serving-style batch: 256 independent ground-state problems (Heisenberg
     and Hubbard chain-shaped sectors, L in [16, 48], m in {64, 128, 256, 512},
     superblock.serving_batch) solved together by the group Lanczos (one
@@ -359,7 +364,10 @@ def serving_measurements(torch, dev, stream, cpu_sample: bool = True, probs=None
     and 1 - |<psi|psi_FP64>| against the single-problem FP64 solves; the
     reference's own LanczosSolver + BatchedGemmCpu (oracle/_ref) timed on a
     sample of the batch.  probs / meta (with "L" per problem) replace the
-    synthetic batch when given (the physical batch of real superblocks)."""
+    synthetic batch when given (the physical batch of real superblocks).
+    correction: the group refinement's correction solves, "none" or "jacobi"
+    (diagonally preconditioned: pays on physical Hamiltonians, whose diagonal
+    carries the spectrum, not on the synthetic batch's N(0,1) blocks)."""
     from dmrgpp_b200 import plugin
     from dmrgpp_b200 import superblock as sb
     if probs is None:
@@ -423,6 +431,8 @@ def serving_measurements(torch, dev, stream, cpu_sample: bool = True, probs=None
         torch.cuda.synchronize()
         return em, conv, st, zm, steps_m, (t1 - t0, time.perf_counter() - t1)
 
+    if correction == "jacobi":
+        bgm.set_correction_preconditioner(_capi_precond("jacobi"))
     mixed_solve()                                      # warm-up (allocations)
     runs = []
     for _ in range(2):
@@ -430,6 +440,7 @@ def serving_measurements(torch, dev, stream, cpu_sample: bool = True, probs=None
         runs.append(mixed_solve())
     em, conv, st, zm, steps_m, split = min(runs, key=lambda r: sum(r[5]))
     tm = sum(split)
+    bgm.set_correction_preconditioner(_capi_precond("none"))
     dav = learned_ablation(torch, bgm, init, stream)
     bgm.close()
     es, t_seq, ovl = [], 0.0, []
@@ -456,7 +467,8 @@ def serving_measurements(torch, dev, stream, cpu_sample: bool = True, probs=None
         "note": f"TF32x3 group Lanczos (no reorthogonalisation: it only supplies the start "
                 f"vectors) to a Ritz-value change of {SERVING_MIXED_TOLERANCE:g}, then "
                 "dmrgpp_refine_lowest_group (FP64 Rayleigh quotients and residuals, |r| <= "
-                "1e-10 max(1, |E|)), handle creation excluded"}
+                "1e-10 max(1, |E|)), handle creation excluded",
+        "correction_solves": correction}
     for v in dav["runs"].values():
         v["max_abs_dE_per_site_vs_single_fp64"] = float((np.abs(v.pop("energies") - es) / sites).max())
     out["group_davidson"] = dav

@@ -393,6 +393,103 @@ k_g_cg_update(double* __restrict__ t, double* __restrict__ res, const double* __
 	}
 }
 
+// ---- diagonal (Jacobi) preconditioner of the group correction solves, per
+// sector as in lanczos.cu (pcg_correction): K = diag(H) - theta[sector], kept
+// at least 1e-3 max(1, |theta|); z = K^-1 res - a K^-1 u with a = <u, K^-1 res>
+// / <u, K^-1 u>, orthogonal to the sector's u.
+__device__ __forceinline__ double g_pcg_k(double d, double th)
+{
+	const double f = 1e-3 * fmax(1.0, fabs(th));
+	const double k = d - th;
+	return k > f ? k : f;
+}
+
+// wv = K^-1 u; partial[ch] = <u, wv> over ch
+__global__ void __launch_bounds__(kThreads)
+k_g_pcg_setup(const double* __restrict__ u, const double* __restrict__ diag, const double* __restrict__ theta,
+              double* __restrict__ wv, const Chunk* __restrict__ chunks, int nch, const int* __restrict__ active,
+              double* __restrict__ partial)
+{
+	__shared__ double red[kThreads / 32];
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk k = chunks[ch];
+		double      s = 0.0;
+		if (active[k.seg]) {
+			const double th = theta[k.seg];
+			for (int i = threadIdx.x; i < k.len; i += kThreads) {
+				const long long q = k.begin + i;
+				const double    v = u[q] / g_pcg_k(diag[q], th);
+				wv[q]             = v;
+				s += u[q] * v;
+			}
+		}
+		s = block_sum(s, red);
+		if (threadIdx.x == 0)
+			partial[ch] = s;
+	}
+}
+
+// partial[ch], [nch + ch], [2 nch + ch] = <u, K^-1 res>, <res, K^-1 res>, <res, wv> over ch
+__global__ void __launch_bounds__(kThreads)
+k_g_pcg_sums(const double* __restrict__ res, const double* __restrict__ diag, const double* __restrict__ theta,
+             const double* __restrict__ u, const double* __restrict__ wv, const Chunk* __restrict__ chunks,
+             int nch, const int* __restrict__ active, double* __restrict__ partial)
+{
+	__shared__ double red[kThreads / 32];
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk k = chunks[ch];
+		double      v0 = 0.0, v1 = 0.0, v2 = 0.0;
+		if (active[k.seg]) {
+			const double th = theta[k.seg];
+			for (int i = threadIdx.x; i < k.len; i += kThreads) {
+				const long long q = k.begin + i;
+				const double    r = res[q];
+				const double    z = r / g_pcg_k(diag[q], th);
+				v0 += u[q] * z;
+				v1 += r * z;
+				v2 += r * wv[q];
+			}
+		}
+		v0 = block_sum(v0, red);
+		v1 = block_sum(v1, red);
+		v2 = block_sum(v2, red);
+		if (threadIdx.x == 0) {
+			partial[ch]           = v0;
+			partial[nch + ch]     = v1;
+			partial[2 * nch + ch] = v2;
+		}
+	}
+}
+
+// p = z + (rho_new / rho) p (p = z when first), rho_new = sums1 - a sums2,
+// a = sums0 / uw; every chunk of a sector computes the same rho_new, and its
+// sector's first chunk stores it in rho_next
+__global__ void __launch_bounds__(kThreads)
+k_g_pcg_direction(double* __restrict__ p, const double* __restrict__ res, const double* __restrict__ diag,
+                  const double* __restrict__ theta, const double* __restrict__ wv, const double* __restrict__ uw,
+                  const double* __restrict__ sums, int nseg, const double* __restrict__ rho,
+                  double* __restrict__ rho_next, int first, const Chunk* __restrict__ chunks, int nch,
+                  const int* __restrict__ seg_chunk, const int* __restrict__ active)
+{
+	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+		const Chunk k = chunks[ch];
+		if (!active[k.seg])
+			continue;
+		const int    sg      = k.seg;
+		const double a       = uw[sg] > 0.0 ? sums[sg] / uw[sg] : 0.0;
+		const double rho_new = sums[nseg + sg] - a * sums[2 * nseg + sg];
+		const double beta    = first ? 0.0 : (rho[sg] > 0.0 ? rho_new / rho[sg] : 0.0);
+		if (threadIdx.x == 0 && ch == seg_chunk[sg])
+			rho_next[sg] = rho_new;
+		const double th = theta[sg];
+		for (int i = threadIdx.x; i < k.len; i += kThreads) {
+			const long long q = k.begin + i;
+			const double    z = res[q] / g_pcg_k(diag[q], th) - a * wv[q];
+			p[q]              = z + beta * p[q];
+		}
+	}
+}
+
 // one thread per sector: stop the sector's CG on a non-positive pAp or once
 // |res| <= tol * b0
 __global__ void k_g_cg_check(const double* __restrict__ pAp, const double* __restrict__ rr_next,
@@ -477,8 +574,10 @@ struct GroupWork {
 	int*    ncols   = nullptr;   // nseg (Ritz vector lengths)
 	double* host    = nullptr;   // pinned: alpha, beta
 	// refinement (dmrgpp_refine_lowest_group), allocated on first use
-	double* rv    = nullptr; // 6 x dim: H psi, r, t, res, p, Aq
+	double* rv    = nullptr; // 7 x dim: H psi, r, t, res, p, Aq, K^-1 psi (Jacobi corrections)
 	double* rsc   = nullptr; // 8 x nseg scalars
+	double* rpsc  = nullptr; // 6 x nseg: Jacobi corrections' <u,K^-1 u>, three sums, rho[2]
+	double* rpart = nullptr; // 3 x nch chunk partials of those sums
 	int*    rint  = nullptr; // 2 x nseg: outer active, CG active
 	double* rhost = nullptr; // pinned: theta, |r| (2 x nseg), then 2 x nseg ints
 	long long* sec_start = nullptr; // nseg + 1 sector offsets
@@ -511,6 +610,8 @@ void release_group(dmrgpp_kron_handle h)
 		cudaFreeHost(w->host);
 	dmrgpp::dev_free(w->rv);
 	dmrgpp::dev_free(w->rsc);
+	dmrgpp::dev_free(w->rpsc);
+	dmrgpp::dev_free(w->rpart);
 	dmrgpp::dev_free(w->rint);
 	if (w->rhost)
 		cudaFreeHost(w->rhost);
@@ -892,8 +993,10 @@ extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int
 	const cudaStream_t st = h->stream;
 	cudaError_t        e;
 	if (!w->rv) {
-		if ((e = dmrgpp::dev_malloc(&w->rv, 6 * D * sizeof(double)))
+		if ((e = dmrgpp::dev_malloc(&w->rv, 7 * D * sizeof(double)))
 		    || (e = dmrgpp::dev_malloc(&w->rsc, 8 * size_t(S) * sizeof(double)))
+		    || (e = dmrgpp::dev_malloc(&w->rpsc, 6 * size_t(S) * sizeof(double)))
+		    || (e = dmrgpp::dev_malloc(&w->rpart, 3 * size_t(std::max(w->nch, 1)) * sizeof(double)))
 		    || (e = dmrgpp::dev_malloc(&w->rint, 2 * size_t(S) * sizeof(int)))
 		    || (e = cudaHostAlloc(&w->rhost, 2 * size_t(S) * (sizeof(double) + sizeof(int)), 0)))
 			return status(h, e, "group refinement allocation");
@@ -923,6 +1026,17 @@ extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int
 	auto dot = [&](const double* x, const double* y, double* out, const int* act, int root) {
 		k_g_dot<<<grid, kThreads, 0, st>>>(x, y, w->chunks, nch, act, w->partial);
 		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, act, out, root);
+	};
+	// Jacobi corrections (dmrgpp_set_correction_preconditioner)
+	const bool jac  = h->correction_precond == DMRGPP_PRECOND_JACOBI && h->d_diag;
+	double*    wv   = w->rv + 6 * D;
+	double*    uw   = w->rpsc;
+	double*    sums = w->rpsc + S; // 3 x S
+	double*    rho[2] = { w->rpsc + 4 * S, w->rpsc + 5 * S };
+	auto pcg_sums = [&]() {
+		k_g_pcg_sums<<<grid, kThreads, 0, st>>>(res, h->d_diag, theta, psi, wv, w->chunks, nch, cg, w->rpart);
+		for (int q = 0; q < 3; ++q)
+			k_g_finish<<<S, kThreads, 0, st>>>(w->rpart + size_t(q) * nch, w->seg_chunk, cg, sums + size_t(q) * S, 0);
 	};
 	// the FP64 group H*x skips converged sectors while this runs
 	struct MaskOff {
@@ -993,6 +1107,13 @@ extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int
 		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, outer, rr[0], 0);
 		k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, outer, b0, 1);
 		k_g_cg_start<<<sgrid, kThreads, 0, st>>>(b0, outer, cg, S);
+		if (jac) { // Jacobi: wv = K^-1 psi, <psi, wv>, then p = z0 and rho0 = <res, z0>
+			k_g_pcg_setup<<<grid, kThreads, 0, st>>>(psi, h->d_diag, theta, wv, w->chunks, nch, cg, w->rpart);
+			k_g_finish<<<S, kThreads, 0, st>>>(w->rpart, w->seg_chunk, cg, uw, 0);
+			pcg_sums();
+			k_g_pcg_direction<<<grid, kThreads, 0, st>>>(pv, res, h->d_diag, theta, wv, uw, sums, S, rho[0],
+			                                             rho[0], 1, w->chunks, nch, w->seg_chunk, cg);
+		}
 		int cur = 0, inner = 0;
 		while (inner < inner_iterations) {
 			const int burst = std::min(8, inner_iterations - inner);
@@ -1008,11 +1129,20 @@ extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int
 				dot(psi, Aq, ua, cg, 0);
 				k_g_axpy<<<grid, kThreads, 0, st>>>(Aq, psi, ua, -1.0, w->chunks, nch, cg);
 				dot(pv, Aq, pAp, cg, 0);
-				k_g_cg_update<<<grid, kThreads, 0, st>>>(t, res, pv, Aq, rr[cur], pAp, w->chunks, nch, cg,
-				                                         w->partial);
+				// alpha = rr / pAp (plain) or rho / pAp (Jacobi); |res|^2 for the check
+				k_g_cg_update<<<grid, kThreads, 0, st>>>(t, res, pv, Aq, jac ? rho[cur] : rr[cur], pAp,
+				                                         w->chunks, nch, cg, w->partial);
 				k_g_finish<<<S, kThreads, 0, st>>>(w->partial, w->seg_chunk, cg, rr[cur ^ 1], 0);
 				k_g_cg_check<<<sgrid, kThreads, 0, st>>>(pAp, rr[cur ^ 1], b0, inner_tolerance, cg, S);
-				k_g_cg_direction<<<grid, kThreads, 0, st>>>(pv, res, rr[cur ^ 1], rr[cur], w->chunks, nch, cg);
+				if (jac) {
+					pcg_sums();
+					k_g_pcg_direction<<<grid, kThreads, 0, st>>>(pv, res, h->d_diag, theta, wv, uw, sums, S,
+					                                             rho[cur], rho[cur ^ 1], 0, w->chunks, nch,
+					                                             w->seg_chunk, cg);
+				} else {
+					k_g_cg_direction<<<grid, kThreads, 0, st>>>(pv, res, rr[cur ^ 1], rr[cur], w->chunks, nch,
+					                                            cg);
+				}
 				cur ^= 1;
 			}
 			if ((e = cudaGetLastError()))

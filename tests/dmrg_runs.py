@@ -471,7 +471,7 @@ def serving(n=256, log=print):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     out = bench.serving_measurements(
-        torch, dev, stream, cpu_sample=True, probs=probs, meta=meta,
+        torch, dev, stream, cpu_sample=True, probs=probs, meta=meta, correction="jacobi",
         workload=f"serving-batch-{n} of real DMRG superblocks (Heisenberg / Hubbard chains, "
                  "L 16-48, U 0-8, m 64-512, last infinite-growth sector)")
     out["dims"] = {"min": int(min(p.dim for p in probs)), "max": int(max(p.dim for p in probs))}

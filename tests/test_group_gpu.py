@@ -133,20 +133,24 @@ def test_group_handle_as_one_sector_with_graph_replay(cuda_lib, cuda_device):
     bg.close()
 
 
-@pytest.mark.parametrize("precision,reortho", [("tf32x3", True), ("tf32x3", False), ("fp64", True)])
-def test_group_refinement_matches_single_fp64_solves(cuda_lib, cuda_device, precision, reortho):
+@pytest.mark.parametrize("precision,reortho,jacobi", [("tf32x3", True, False), ("tf32x3", False, False),
+                                                     ("fp64", True, False), ("tf32x3", False, True)])
+def test_group_refinement_matches_single_fp64_solves(cuda_lib, cuda_device, precision, reortho, jacobi):
     """Serving-style problems in one group handle: a loose lockstep group
     Lanczos (the handle's matvecs: tensor-core TF32x3 or FP64; with or without
     reorthogonalisation, as the start vectors only), then the
     lockstep FP64 refinement (dmrgpp_refine_lowest_group).  Every sector
     converges; its energy is within 1e-9 per site (and 1e-10 relative) of its
     single-problem FP64 Lanczos, its vector has unit norm and overlaps the
-    FP64 Ritz vector to 1e-8."""
+    FP64 Ritz vector to 1e-8.  Also with the diagonally preconditioned
+    correction solves (dmrgpp_set_correction_preconditioner)."""
     import torch
-    from dmrgpp_b200 import plugin
+    from dmrgpp_b200 import _capi, plugin
     probs, meta = sb.serving_batch(8, seed=77)
     prec = plugin.TF32X3 if precision == "tf32x3" else plugin.FP64
     bg = plugin.BatchedGemm.from_problems(probs, precision=prec)
+    if jacobi:
+        bg.set_correction_preconditioner(_capi.PRECOND_JACOBI)
     offs = bg.sector_offsets()
     init = torch.from_numpy(np.random.default_rng(5).standard_normal(bg.dim)).cuda()
     _, z, _ = bg.lanczos_lowest_group(init, steps=100, tolerance=1e-4, reortho=reortho)
