@@ -183,6 +183,10 @@ SIGNATURES.update({
     "dmrgpp_lanczos_lowest_group": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LanczosParams),
                                                    ctypes.c_void_p, ctypes.c_int, _dp,
                                                    ctypes.c_void_p, _szp]),
+    "dmrgpp_lanczos_lowest_group_masked": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LanczosParams),
+                                                          ctypes.c_void_p, ctypes.c_int,
+                                                          ctypes.POINTER(ctypes.c_int), _dp,
+                                                          ctypes.c_void_p, _szp]),
     "dmrgpp_lanczos_lowest": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LanczosParams),
                                              ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_void_p,
                                              _szp]),

@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstdint>
 #include <string>
+#include <limits>
 #include <vector>
 
 namespace dmrgpp {
@@ -683,9 +684,23 @@ int ensure_group_work(dmrgpp_kron_handle h, int cols)
 
 } // namespace dmrgpp
 
+extern "C" int dmrgpp_lanczos_lowest_group_masked(dmrgpp_kron_handle h, const dmrgpp_lanczos_params* p,
+                                                  const double* init, int on_device, const int* mask,
+                                                  double* energies, double* z, size_t* steps_taken);
+
 extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_lanczos_params* p,
                                            const double* init, int on_device, double* energies,
                                            double* z, size_t* steps_taken)
+{
+	return dmrgpp_lanczos_lowest_group_masked(h, p, init, on_device, nullptr, energies, z, steps_taken);
+}
+
+// mask (host, one int per sector; NULL = every sector): sectors with mask 0
+// take no part (no H*x items, no vector work); their energies are NaN, their
+// part of z is zero and their steps_taken 0.
+extern "C" int dmrgpp_lanczos_lowest_group_masked(dmrgpp_kron_handle h, const dmrgpp_lanczos_params* p,
+                                                  const double* init, int on_device, const int* mask,
+                                                  double* energies, double* z, size_t* steps_taken)
 {
 	if (h && h->complex_sector)
 		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
@@ -742,7 +757,12 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 		~MaskOff() { h->sector_active = nullptr; }
 	} mask_off { h };
 
-	std::vector<int> act(size_t(S), 1);
+	std::vector<int> act(size_t(S), 1), skip(size_t(S), 0);
+	for (int s = 0; mask && s < S; ++s)
+		if (!mask[s]) {
+			act[size_t(s)]  = 0;
+			skip[size_t(s)] = 1;
+		}
 	if ((e = cudaMemcpyAsync(w->active, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st))
 	    || (e = cudaMemsetAsync(w->beta, 0, size_t(S) * sizeof(double), st))) // beta_0 = 0
 		return status(h, e, "group solver start");
@@ -770,7 +790,9 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 	std::vector<size_t> j_stop(size_t(S), 0);
 	int                 n_active = S;
 	for (int s = 0; s < S; ++s)
-		if (maxn_s[size_t(s)] == 1) { // nothing to iterate: the 1 x 1 tridiagonal
+		if (skip[size_t(s)]) {
+			--n_active;
+		} else if (maxn_s[size_t(s)] == 1) { // nothing to iterate: the 1 x 1 tridiagonal
 			act[size_t(s)] = 0;
 			--n_active;
 		}
@@ -920,6 +942,13 @@ extern "C" int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_la
 	std::vector<double> coef(ncoef, 0.0);
 	std::vector<int>    ncols(static_cast<size_t>(S));
 	for (int s = 0; s < S; ++s) {
+		if (skip[size_t(s)]) { // no part in this solve: no coefficients, z = 0 there
+			energies[s]      = std::numeric_limits<double>::quiet_NaN();
+			ncols[size_t(s)] = 0;
+			if (steps_taken)
+				steps_taken[s] = 0;
+			continue;
+		}
 		const size_t n = j_stop[size_t(s)] + 1;
 		d.resize(n);
 		off.resize(n);
@@ -1049,8 +1078,9 @@ extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int
 		}
 	} mask_off { h, h->precision };
 
-	std::vector<int> act(size_t(S), 1), done(size_t(S), 0);
-	std::vector<double> th(size_t(S), 0.0), rn(size_t(S), 0.0);
+	std::vector<int> act(size_t(S), 1), done(size_t(S), 0), stall(size_t(S), 0);
+	std::vector<double> th(size_t(S), 0.0), rn(size_t(S), 0.0),
+	    best(size_t(S), std::numeric_limits<double>::infinity());
 	if ((e = cudaMemcpyAsync(outer, act.data(), size_t(S) * sizeof(int), cudaMemcpyHostToDevice, st)))
 		return status(h, e, "group refinement start");
 	dmrgpp_refine_stats s {};
@@ -1084,6 +1114,19 @@ extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int
 			if (rn_h[q] <= tolerance * std::max(1.0, std::fabs(th_h[q]))) {
 				act[size_t(q)]  = 0;
 				done[size_t(q)] = 1;
+				--n_active;
+				changed = true;
+				continue;
+			}
+			// a sector whose residual has not halved over two outer steps
+			// is failing (its start lies above the first excitation, where
+			// the projected correction equation is indefinite): it stops
+			// here, unconverged, instead of holding the lockstep launches
+			if (rn_h[q] < 0.5 * best[size_t(q)]) {
+				best[size_t(q)]  = rn_h[q];
+				stall[size_t(q)] = 0;
+			} else if (++stall[size_t(q)] >= 2) {
+				act[size_t(q)] = 0;
 				--n_active;
 				changed = true;
 			}

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdint>
 #include <string>
+#include <limits>
 #include <vector>
 
 namespace dmrgpp {
@@ -1703,6 +1704,8 @@ int dmrgpp_refine_lowest(dmrgpp_kron_handle h, double* psi, int max_outer, doubl
 	const int     user = h->precision;
 	dmrgpp_refine_stats s {};
 	double        theta = 0.0, rnorm = 0.0;
+	double        best  = std::numeric_limits<double>::infinity();
+	int           stall = 0;
 	int           rc    = DMRGPP_OK;
 	cudaError_t   e;
 	for (int outer = 0; outer <= max_outer; ++outer) {
@@ -1737,6 +1740,14 @@ int dmrgpp_refine_lowest(dmrgpp_kron_handle h, double* psi, int max_outer, doubl
 		}
 		if (outer == max_outer)
 			break;
+		// a residual that has not halved over two outer steps means a failing
+		// refinement (start above the first excitation): stop, unconverged
+		if (rnorm < 0.5 * best) {
+			best  = rnorm;
+			stall = 0;
+		} else if (++stall >= 2) {
+			break;
+		}
 		int    its = 0;
 		double rel = 0.0;
 		if ((rc = dmrgpp_correction_solve(h, psi, theta, r, t, inner_iterations, inner_tolerance, &its,

@@ -230,11 +230,13 @@ class BatchedGemm:
 
     def lanczos_lowest_group(self, init, steps: int = 200, min_steps: int = 4,
                              tolerance: float = 1e-12, eigs_for_stop: int = 1,
-                             reortho: bool = True, check_every: int = 8):
+                             reortho: bool = True, check_every: int = 8, mask=None):
         """Lowest eigenpair of every sector of a group handle, all sectors in
         lockstep (dmrgpp_lanczos_lowest_group).  Returns (energies array,
         concatenated Ritz vectors, steps array); numpy or torch CUDA like
-        lanczos_lowest."""
+        lanczos_lowest.  mask (one bool per sector) restricts the solve to
+        the sectors set in it (dmrgpp_lanczos_lowest_group_masked): the
+        others get NaN energies and zero vectors at no cost."""
         L = self._lib
         p = _capi.LanczosParams()
         L.dmrgpp_lanczos_params_init(ctypes.byref(p))
@@ -245,20 +247,26 @@ class BatchedGemm:
         n = np.zeros(nsec, dtype=np.uint64)
         dp = ctypes.POINTER(ctypes.c_double)
         szp = ctypes.POINTER(ctypes.c_size_t)
+        m = None
+        if mask is not None:
+            m = np.ascontiguousarray(np.asarray(mask, dtype=bool).astype(np.int32))
+            if m.size != nsec:
+                raise ValueError(f"mask needs {nsec} entries")
+        mp = m.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if m is not None else None
         if hasattr(init, "data_ptr"):
             import torch
             z = torch.empty_like(init)
             self._pointers(init, z)
-            rc = L.dmrgpp_lanczos_lowest_group(self._h, ctypes.byref(p), init.data_ptr(), 1,
-                                               e.ctypes.data_as(dp), z.data_ptr(),
-                                               n.ctypes.data_as(szp))
+            rc = L.dmrgpp_lanczos_lowest_group_masked(self._h, ctypes.byref(p), init.data_ptr(), 1,
+                                                      mp, e.ctypes.data_as(dp), z.data_ptr(),
+                                                      n.ctypes.data_as(szp))
         else:
             init = np.ascontiguousarray(init, dtype=np.float64)
             z = np.empty(self.dim)
             self._pointers(init, z)
-            rc = L.dmrgpp_lanczos_lowest_group(self._h, ctypes.byref(p), init.ctypes.data, 0,
-                                               e.ctypes.data_as(dp), z.ctypes.data,
-                                               n.ctypes.data_as(szp))
+            rc = L.dmrgpp_lanczos_lowest_group_masked(self._h, ctypes.byref(p), init.ctypes.data, 0,
+                                                      mp, e.ctypes.data_as(dp), z.ctypes.data,
+                                                      n.ctypes.data_as(szp))
         _capi.check(rc, self._h)
         return e, z, n.astype(np.int64)
 
@@ -481,11 +489,81 @@ class BatchedGemm:
             st = dict(st, method="mixed", mixed_lanczos_steps=n1, fallback=0,
                       mixed_lanczos_seconds=t1 - t0, refine_seconds=clock() - t1)
             if not st["converged"]:
+                # from the refined state plus a small seeded perturbation (see
+                # solve_lowest_group)
+                import torch
+                g = torch.from_numpy(np.random.default_rng(7).standard_normal(self.dim)).to(z.device)
+                z = z + 1e-3 * torch.linalg.vector_norm(z) * g / torch.linalg.vector_norm(g)
                 self.set_precision(FP64)
                 t0 = clock()
                 e, z, n2 = self.lanczos_lowest(z, steps=fp64_steps, tolerance=tolerance)
                 st.update(fallback=1, converged=1, fp64_lanczos_steps=n2,
                           fp64_lanczos_seconds=clock() - t0)
+            return e, z, st
+        finally:
+            self.set_precision(user)
+
+    def solve_lowest_group(self, init, tolerance: float = 1e-10, mixed_tolerance: float = 1e-5,
+                           mixed_steps: int = 200, correction: str = "jacobi",
+                           fp64_steps: int = 200):
+        """Lowest eigenpair of every sector of a group handle created with
+        TF32x3 (init: torch CUDA tensor, the concatenated start vectors):
+        the TF32x3 group Lanczos without reorthogonalisation (it only supplies
+        start vectors; up to mixed_steps steps or a mixed_tolerance Ritz-value
+        change), then the lockstep FP64 group refinement to
+        |r| <= tolerance max(1, |E|) with the given correction solves ("jacobi"
+        or "none"); a sector whose refinement did not converge (its start above
+        the first excitation of a nearly gapless sector) is then finished by an
+        FP64 group Lanczos started from the refined vectors, whose result is
+        taken for those sectors only.  Returns (energies, vectors, stats dict:
+        lanczos_steps, refine stats, fallbacks and the seconds of each phase).
+        The handle's precision and correction preconditioner are left as they
+        were."""
+        import torch
+        if correction not in ("none", "jacobi"):
+            raise ValueError(f"unknown correction {correction!r}")
+        user = self.get_precision()
+        clock = time.perf_counter   # each phase ends in a host read of its result
+        try:
+            self.set_precision(TF32X3)
+            t0 = clock()
+            _, z, steps = self.lanczos_lowest_group(init, steps=mixed_steps,
+                                                    tolerance=mixed_tolerance, reortho=False)
+            t1 = clock()
+            if correction == "jacobi":
+                self.set_correction_preconditioner(_capi.PRECOND_JACOBI)
+            try:
+                e, conv, st = self.refine_lowest_group(z, max_outer=12, tolerance=tolerance,
+                                                       inner_iterations=80, inner_tolerance=1e-2,
+                                                       raise_on_no_convergence=False)
+            finally:
+                if correction == "jacobi":
+                    self.set_correction_preconditioner(_capi.PRECOND_NONE)
+            t2 = clock()
+            st = dict(st, lanczos_steps=steps, fallbacks=int((~conv).sum()),
+                      mixed_lanczos_seconds=t1 - t0, refine_seconds=t2 - t1,
+                      fallback_seconds=0.0)
+            if not conv.all():
+                # only the unconverged sectors, each from its refined vector
+                # plus a seeded perturbation of relative size 1e-3 (a start
+                # that already is an eigenvector makes the first Lanczos step
+                # break down; the reference's Lanczos, mirrored here, keeps
+                # the pre-reorthogonalisation beta)
+                offs = self.sector_offsets()
+                g = torch.from_numpy(np.random.default_rng(7).standard_normal(self.dim)).to(z.device)
+                start = z.clone()
+                for q in np.flatnonzero(~conv):
+                    gs = g[offs[q]:offs[q + 1]]
+                    start[offs[q]:offs[q + 1]] += 1e-3 * gs / torch.linalg.vector_norm(gs)
+                self.set_precision(FP64)
+                e64, z64, _ = self.lanczos_lowest_group(start, steps=fp64_steps, tolerance=1e-12,
+                                                        mask=~conv)
+                for q in np.flatnonzero(~conv):
+                    e[q] = e64[q]
+                    z[offs[q]:offs[q + 1]] = z64[offs[q]:offs[q + 1]]
+                torch.cuda.synchronize()
+                st["fallback_seconds"] = clock() - t2
+            st["converged"] = 1
             return e, z, st
         finally:
             self.set_precision(user)

@@ -353,6 +353,17 @@ int dmrgpp_lanczos_lowest_group(dmrgpp_kron_handle h, const dmrgpp_lanczos_param
                                 const double* init, int on_device, double* energies, double* z,
                                 size_t* steps_taken);
 
+/* dmrgpp_lanczos_lowest_group restricted to the sectors with mask[s] != 0
+ * (mask: host array, one int per sector; NULL = every sector).  The others
+ * take no part (their H*x items and vector work are skipped): their
+ * energies are NaN, their part of z is zero and their steps_taken 0.  For
+ * finishing a few sectors of a group (e.g. those whose refinement did not
+ * converge) at the cost of those sectors only.  No counterpart in the
+ * reference.  Synchronous. */
+int dmrgpp_lanczos_lowest_group_masked(dmrgpp_kron_handle h, const dmrgpp_lanczos_params* p,
+                                       const double* init, int on_device, const int* mask,
+                                       double* energies, double* z, size_t* steps_taken);
+
 /* ---- Davidson with a preconditioned correction (no counterpart in the
  * reference, whose only eigensolver for this path is Lanczos) ---- */
 typedef struct dmrgpp_mlp_s* dmrgpp_mlp_handle;

@@ -216,3 +216,56 @@ def test_group_lanczos_reuses_larger_work_buffers(cuda_lib, cuda_device):
     fresh.close()
     assert np.array_equal(e1, e2) and np.array_equal(n1, n2)
     assert torch.equal(z1, z2)
+
+
+@pytest.mark.parametrize("tolerance", [1e-10, 1e-17])
+def test_solve_lowest_group_with_fallback(cuda_lib, cuda_device, tolerance):
+    """The library's group solve (TF32x3 group Lanczos, lockstep FP64
+    refinement with Jacobi correction solves, FP64 group Lanczos for the
+    sectors left unconverged) on serving-style problems: energies within
+    1e-9 per site of single-problem FP64 Lanczos.  With an unreachable
+    refinement tolerance (1e-17) every sector takes the FP64 fallback."""
+    import torch
+    from dmrgpp_b200 import plugin
+    probs, meta = sb.serving_batch(8, seed=77)
+    bg = plugin.BatchedGemm.from_problems(probs, precision=plugin.TF32X3)
+    offs = bg.sector_offsets()
+    init = torch.from_numpy(np.random.default_rng(5).standard_normal(bg.dim)).cuda()
+    e, z, st = bg.solve_lowest_group(init, tolerance=tolerance)
+    assert bg.get_precision() == plugin.TF32X3
+    bg.close()
+    if tolerance < 1e-16:
+        assert st["fallbacks"] == len(probs)
+    for s, p in enumerate(probs):
+        single = plugin.BatchedGemm.from_problem(p)
+        e1, z1, _ = single.lanczos_lowest(init[offs[s]:offs[s + 1]].contiguous(), tolerance=1e-12)
+        single.close()
+        assert abs(e[s] - e1) / meta[s]["L"] <= 1e-9, (meta[s], e[s], e1, st["fallbacks"])
+        zs = z[offs[s]:offs[s + 1]]
+        assert 1.0 - abs(float(torch.dot(zs, z1))) < 1e-6, s
+
+
+def test_masked_group_lanczos(cuda_lib, cuda_device):
+    """dmrgpp_lanczos_lowest_group_masked: the sectors in the mask get the
+    energies and vectors of the unmasked solve (each sector's arithmetic does
+    not depend on the others); the rest get NaN and zeros."""
+    import torch
+    from dmrgpp_b200 import plugin
+    probs, meta = sb.serving_batch(8, seed=78)
+    bg = plugin.BatchedGemm.from_problems(probs)
+    offs = bg.sector_offsets()
+    init = torch.from_numpy(np.random.default_rng(6).standard_normal(bg.dim)).cuda()
+    e_all, z_all, n_all = bg.lanczos_lowest_group(init, steps=200, tolerance=1e-12)
+    mask = np.zeros(len(probs), dtype=bool)
+    mask[[1, 4]] = True
+    e_m, z_m, n_m = bg.lanczos_lowest_group(init, steps=200, tolerance=1e-12, mask=mask)
+    bg.close()
+    for s in range(len(probs)):
+        zs = z_m[offs[s]:offs[s + 1]]
+        if mask[s]:
+            assert abs(e_m[s] - e_all[s]) <= 1e-13 * abs(e_all[s]), s
+            assert n_m[s] == n_all[s]
+            assert float(torch.linalg.vector_norm(zs - z_all[offs[s]:offs[s + 1]])) <= 1e-10
+        else:
+            assert np.isnan(e_m[s]) and n_m[s] == 0
+            assert float(torch.abs(zs).max()) == 0.0
