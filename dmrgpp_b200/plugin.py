@@ -561,7 +561,8 @@ class BatchedGemm:
                 for q in np.flatnonzero(~conv):
                     e[q] = e64[q]
                     z[offs[q]:offs[q + 1]] = z64[offs[q]:offs[q + 1]]
-                torch.cuda.synchronize()
+                if z.is_cuda:
+                    torch.cuda.synchronize(z.device)
                 st["fallback_seconds"] = clock() - t2
             st["converged"] = 1
             return e, z, st
