@@ -191,8 +191,9 @@ def test_learned_preconditioner_training_and_ablation(cuda_lib, cuda_device, fam
         bg.close()
     summary = {k: float(np.mean(v)) for k, v in its.items()}
     print(family, "Davidson iterations (none, Jacobi, learned):", summary)
-    if os.path.isdir("gpurun_out"):
-        with open(os.path.join("gpurun_out", f"mlp_ablation_{family}.json"), "w") as f:
+    out_dir = os.environ.get("DMRGPP_ABLATION_OUT")   # optional record of the ablation
+    if out_dir and os.path.isdir(out_dir):
+        with open(os.path.join(out_dir, f"mlp_ablation_{family}.json"), "w") as f:
             json.dump({"iterations": its, "mean": summary}, f)
     assert summary[2] <= summary[1]
     assert summary[2] <= 1.05 * min(summary[0], summary[1])

@@ -1,7 +1,7 @@
 """The device Lanczos against the reference's own PsimagLite::LanczosSolver.
 
-Parity bar: |E_gpu - E_ref| <= 1e-12 |E_ref| (the north-star tolerance for
-the plain FP64 method), the stopping step within 2 of the reference's, and
+Parity bar: |E_gpu - E_ref| <= 1e-12 |E_ref| (the tolerance asked of the
+plain FP64 method), the stopping step within 2 of the reference's, and
 the Ritz vector's residual and overlap with the reference's."""
 import json
 import os
