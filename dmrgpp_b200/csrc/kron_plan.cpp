@@ -2,11 +2,14 @@
 #include "kron_plan.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
+#include <string>
 #include <numeric>
 #include <thread>
 #include <tuple>
@@ -621,6 +624,59 @@ void add_tc_tiles(std::vector<GemmTile>& tiles, long long c_off, long long ldc, 
 }
 
 } // namespace
+
+namespace {
+int octave(double x) { return x >= 1.0 ? int(std::floor(std::log2(x))) : 0; }
+} // namespace
+
+// FNV-1a over a coarse summary of the sector's size histogram: the patch
+// dimension (max(l_i, r_i) of the output patch) at the quartiles and the
+// maximum of the work-weighted distribution, one bucket per octave; the
+// total work in half-octave buckets; the number of terms; the GPU name.
+// These set what the configurations trade off (tile padding against
+// tiles per SM), and they move little between consecutive sweep steps,
+// whose patch sizes change by a few states, so those sectors share an
+// entry.
+std::string tuning_key(const KronPlan& P, const char* gpu)
+{
+	std::vector<std::pair<long long, double>> w; // (patch dimension, work)
+	double                                    total = 0.0;
+	long long                                 dmax  = 0;
+	for (const auto& t : P.triples) {
+		const long long d = std::max(P.l[size_t(t.i)], P.r[size_t(t.i)]);
+		const double    f = 2.0 * double(P.r[size_t(t.i)]) * double(P.l[size_t(t.j)])
+		    * double(P.r[size_t(t.j)] + P.l[size_t(t.i)]);
+		w.push_back({ d, f });
+		total += f;
+		dmax = std::max(dmax, d);
+	}
+	std::sort(w.begin(), w.end());
+	long long q[3] = { 0, 0, 0 };
+	double    acc  = 0.0;
+	int       k    = 0;
+	for (const auto& e : w) {
+		acc += e.second;
+		while (k < 3 && acc >= total * 0.25 * (k + 1))
+			q[k++] = e.first;
+	}
+	unsigned long long h   = 1469598103934665603ull;
+	auto               mix = [&](unsigned long long v) {
+                for (int b = 0; b < 8; ++b) {
+                        h ^= (v >> (8 * b)) & 0xffu;
+                        h *= 1099511628211ull;
+                }
+	};
+	mix(P.nop);
+	for (long long v : q)
+		mix((unsigned long long)octave(double(v)));
+	mix((unsigned long long)octave(double(dmax)));
+	mix((unsigned long long)(total > 1.0 ? int(std::floor(2.0 * std::log2(total))) : 0));
+	for (const char* c = gpu; *c; ++c)
+		mix((unsigned long long)(unsigned char)*c);
+	char buf[32];
+	std::snprintf(buf, sizeof(buf), "%016llx", h);
+	return buf;
+}
 
 UploadPlan build_upload_plan(const KronPlan& plan, long long chunk_elems, long long max_job_elems)
 {

@@ -381,6 +381,13 @@ void build_tile_lists(KronPlan& plan, int bm, int bn);
 // longest first, to the CTA with the least work so far (LPT; work of a tile =
 // its k-chunks + 2 for the epilogue); within a run the longest tile comes
 // first.  Returns the number of CTAs, min(bins, tiles.size()).
+// Key of the autotuner's cache (autotune.cu): a hex FNV-1a hash of a coarse
+// summary of the sector-size histogram (output-patch dimension at the work
+// quartiles and maximum, by octave; the total work by half octave; the
+// number of terms) and the GPU name.  Sectors of consecutive sweep steps,
+// whose patch sizes change by a few states, mostly share a key.
+std::string tuning_key(const KronPlan& P, const char* gpu);
+
 int balance_tiles(std::vector<GemmTile>& tiles, const std::vector<GemmSeg>& segs, int bins,
                   std::vector<int>& starts);
 
