@@ -1,7 +1,8 @@
 """Davidson, the FP64 refinement of the mixed-precision mode, and the learned
 preconditioner: gradients against the FP64 oracle, training, and an ablation
-of what the trained network gains.  (No counterpart in the reference; the
-judge is the FP64 residual and the reference Lanczos energy.)"""
+of what the trained network gains.  (No counterpart in the reference;
+convergence is decided by the FP64 residual, and energies are checked
+against the reference Lanczos.)"""
 import json
 import os
 
