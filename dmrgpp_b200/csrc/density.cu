@@ -364,48 +364,24 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 	std::vector<long long> eoff(ng + 1, 0);
 	for (size_t g = 0; g < ng; ++g)
 		eoff[g + 1] = eoff[g] + (long long)d->group_size[g];
-	struct GroupEig {
-		std::vector<double> d, off, hv, beta;
-		bool                ok = true;
-	};
-	std::vector<GroupEig> ge(ng);
-	// largest groups first: the biggest one is the critical path
+	// largest groups first (the order of the eigenvector work below)
 	std::vector<size_t> by_size(ng);
 	std::iota(by_size.begin(), by_size.end(), size_t(0));
 	std::stable_sort(by_size.begin(), by_size.end(),
 	                 [&](size_t x, size_t y) { return d->group_size[x] > d->group_size[y]; });
-	auto eig_group = [&](size_t g, int threads) {
-		const int n = int(d->group_size[g]);
-		if (n == 0)
-			return;
-		GroupEig& G = ge[g];
-		double*   a = h_rho + goff[g];
-		for (int j = 0; j < n; ++j) // symmetrise the round-off of the two triangles
-			for (int i = 0; i < j; ++i) {
-				const double s = 0.5 * (a[i + (long long)j * n] + a[j + (long long)i * n]);
-				a[i + (long long)j * n] = a[j + (long long)i * n] = s;
-			}
-		if (n == 1) {
-			G.d.assign(1, a[0]);
-			G.off.assign(1, 0.0);
-		} else {
-			householder_tridiag_parallel(n, a, G.d, G.off, G.hv, G.beta, threads);
-		}
-		double* w = eigenvalues + eoff[g];
-		std::copy(G.d.begin(), G.d.end(), w);
-		G.ok = tridiag_eigen(n, w, G.off.data(), nullptr); // ascending
-	};
-	// the largest group, when big, first on all host cores (a team sharing
-	// each Householder step), then the others one per core; running the team
-	// beside the others oversubscribed the cores and was slower
-	const int    hw    = int(std::max(2u, std::thread::hardware_concurrency()));
-	const size_t first = d->group_size[by_size[0]] >= 256 ? 1 : 0;
-	if (first)
-		eig_group(by_size[0], hw);
-	parallel_for(ng - first, [&](size_t t) { eig_group(by_size[t + first], 1); });
-	for (size_t g = 0; g < ng; ++g)
-		if (!ge[g].ok)
-			return fail(DMRGPP_NOT_CONVERGED, "eigensolver of group " + std::to_string(g) + " did not converge");
+	std::vector<double*> ga(ng), gw(ng);
+	for (size_t g = 0; g < ng; ++g) {
+		ga[g] = h_rho + goff[g];
+		gw[g] = eigenvalues + eoff[g];
+	}
+	std::vector<GroupReduction> ge;
+	if (!group_eigenvalues(ng, d->group_size, ga.data(), gw.data(), ge,
+	                       int(std::max(2u, std::thread::hardware_concurrency())))) {
+		size_t g = 0;
+		while (g < ng && ge[g].ok)
+			++g;
+		return fail(DMRGPP_NOT_CONVERGED, "eigensolver of group " + std::to_string(g) + " did not converge");
+	}
 
 	g_trunc_times[DMRGPP_TRUNC_EIGENVALUES] = seconds_since(tp);
 	tp                                      = Clock::now();
@@ -452,7 +428,7 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 			const int    n = int(d->group_size[g]), k = int(kept[g]);
 			if (k == 0)
 				return;
-			const GroupEig& G = ge[g];
+			const GroupReduction& G = ge[g];
 			tridiag_eigenvectors(n, G.d.data(), G.off.data(), eigenvalues + eoff[g] + (n - k), k,
 			                     zk + koff[g]);
 			std::copy(G.hv.begin(), G.hv.end(), hv + goff[g]);

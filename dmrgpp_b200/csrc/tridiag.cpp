@@ -13,6 +13,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <numeric>
 #include <random>
 #include <atomic>
@@ -100,7 +101,78 @@ template <class Rot> bool ql_iterate(int n, double* d, const double* off, Rot ro
 	return true;
 }
 
+// Eigenvalues alone by the square-root-free QL iteration of Pal, Walker and
+// Kahan (B. N. Parlett, The Symmetric Eigenvalue Problem, section 8.15):
+// the sweep runs on the squared off-diagonal elements e2 with the squared
+// cosine and sine of each rotation, so a rotation costs divisions but no
+// square root (one per sweep, for the shift).  Shifts and deflation tests
+// are those of ql_iterate (squared).  Each step forms both p / r and r / p
+// from the same operands, so the next p = gamma^2 / c^2 = gamma^2 (r / p)
+// waits for one division instead of two.  The squares need the matrix norm
+// well inside the exponent range (callers check).  d ends unsorted.
+bool ql_values_rootfree(int n, double* d, const double* off, double anorm)
+{
+	std::vector<double> e2(size_t(n), 0.0);
+	for (int i = 0; i + 1 < n; ++i)
+		e2[size_t(i)] = off[i] * off[i];
+	const double eps2 = DBL_EPSILON * DBL_EPSILON, tn = eps2 * anorm * anorm;
+	for (int l = 0; l < n; ++l) {
+		int iter = 0;
+		for (;;) {
+			int m = l;
+			for (; m + 1 < n; ++m) {
+				const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+				if (e2[size_t(m)] <= eps2 * dd * dd || e2[size_t(m)] <= tn)
+					break;
+			}
+			if (m == l)
+				break;
+			if (++iter > 60)
+				return false;
+			// shift: eigenvalue of the leading 2x2 block closer to d[l]
+			const double el    = std::sqrt(e2[size_t(l)]);
+			const double t     = (d[l + 1] - d[l]) / (2.0 * el);
+			const double sigma = d[l] - el / (t + std::copysign(safe_hypot(t, 1.0), t));
+			double       c2 = 1.0, s2 = 0.0, gamma = d[m] - sigma, p = gamma * gamma;
+			for (int i = m - 1; i >= l; --i) {
+				const double bb = e2[size_t(i)], r = p + bb;
+				if (i != m - 1)
+					e2[size_t(i) + 1] = s2 * r;
+				const double oldc = c2, q = r / p;
+				c2                = p / r;
+				s2                = bb / r;
+				const double oldg = gamma, alpha = d[i];
+				gamma             = c2 * (alpha - sigma) - s2 * oldg;
+				d[i + 1]          = oldg + (alpha - gamma);
+				p                 = c2 != 0.0 ? gamma * gamma * q : oldc * bb;
+			}
+			e2[size_t(l)] = s2 * p;
+			d[l]          = sigma + gamma;
+		}
+	}
+	return true;
+}
+
 } // namespace
+
+bool tridiag_values(int n, double* d, const double* off)
+{
+	if (n <= 0)
+		return true;
+	double anorm = 0.0;
+	for (int i = 0; i < n; ++i)
+		anorm = std::max(anorm, std::fabs(d[i]) + (i + 1 < n ? std::fabs(off[i]) : 0.0));
+	std::vector<double> d0(d, d + n);
+	if (!(anorm > 1e-100 && anorm < 1e100) || !ql_values_rootfree(n, d, off, anorm)) {
+		// outside the range of the squares, or no convergence: the QL
+		// iteration with rotations from the same input
+		std::copy(d0.begin(), d0.end(), d);
+		if (!ql_iterate(n, d, off, [](int, double, double) {}))
+			return false;
+	}
+	std::sort(d, d + n);
+	return true;
+}
 
 bool tridiag_eigen(int n, double* d, const double* off, double* z)
 {
@@ -332,6 +404,163 @@ void tridiag_inverse_iteration(int n, const double* d, const double* off, double
 
 namespace dmrgpp {
 
+namespace {
+
+// Four doubles at any 8-byte alignment (GCC vector extension; SSE2 pairs in
+// the baseline build, one AVX register in the AVX2 clone below).  The
+// helpers taking and returning them are always inlined, so the note that
+// their calling convention differs between the two builds does not apply.
+#pragma GCC diagnostic ignored "-Wpsabi"
+typedef double v4d __attribute__((vector_size(32), aligned(8)));
+
+inline __attribute__((always_inline)) v4d load4(const double* x)
+{
+	v4d v;
+	std::memcpy(&v, x, sizeof v);
+	return v;
+}
+inline __attribute__((always_inline)) void store4(double* x, v4d v) { std::memcpy(x, &v, sizeof v); }
+inline __attribute__((always_inline)) double hsum(v4d v) { return (v[0] + v[1]) + (v[2] + v[3]); }
+
+// One pass of a Householder step over columns [c0, c1) of the lower triangle
+// of the trailing block (len x len; column j at a + j * ld, rows i >= j).
+// UPD: the previous step's rank-2 update, A(i, j) -= hp[i] qp[j] + qp[i] hp[j].
+// PROD: then this step's product p += A h, from the lower triangle alone:
+// p[i] += A(i, j) h[j] (i >= j) and p[j] += A(i, j) h[i] (i > j).
+// Columns go in pairs that share the loads of hp, qp, h and p; the order of
+// every sum is fixed (no contraction into fused multiply-adds: -std=c++17
+// turns it off), so both instruction-set builds round alike.
+template <bool UPD, bool PROD>
+inline __attribute__((always_inline)) void pass_cols(int len, double* a, size_t ld, int c0, int c1, const double* hp,
+                                                     const double* qp, const double* h, double* p)
+{
+	int j = c0;
+	for (; j + 1 < c1; j += 2) {
+		double*      x0 = a + size_t(j) * ld;
+		double*      x1 = x0 + ld;
+		const double q0 = UPD ? qp[j] : 0.0, g0 = UPD ? hp[j] : 0.0;
+		const double q1 = UPD ? qp[j + 1] : 0.0, g1 = UPD ? hp[j + 1] : 0.0;
+		const double h0 = PROD ? h[j] : 0.0, h1 = PROD ? h[j + 1] : 0.0;
+		if (UPD) {
+			x0[j] -= hp[j] * q0 + qp[j] * g0;
+			x0[j + 1] -= hp[j + 1] * q0 + qp[j + 1] * g0;
+			x1[j + 1] -= hp[j + 1] * q1 + qp[j + 1] * g1;
+		}
+		double s0 = 0.0, s1 = 0.0;
+		if (PROD) {
+			s0 = x0[j] * h0 + x0[j + 1] * h1;
+			s1 = x1[j + 1] * h1;
+			p[j + 1] += x0[j + 1] * h0;
+		}
+		v4d vs0 = { 0.0, 0.0, 0.0, 0.0 }, vs1 = vs0;
+		int i   = j + 2;
+		for (; i + 4 <= len; i += 4) {
+			v4d a0 = load4(x0 + i), a1 = load4(x1 + i);
+			if (UPD) {
+				const v4d vh = load4(hp + i), vq = load4(qp + i);
+				a0 -= vh * q0 + vq * g0;
+				a1 -= vh * q1 + vq * g1;
+				store4(x0 + i, a0);
+				store4(x1 + i, a1);
+			}
+			if (PROD) {
+				const v4d vx = load4(h + i);
+				vs0 += a0 * vx;
+				vs1 += a1 * vx;
+				store4(p + i, load4(p + i) + (a0 * h0 + a1 * h1));
+			}
+		}
+		for (; i < len; ++i) {
+			double a0 = x0[i], a1 = x1[i];
+			if (UPD) {
+				a0 -= hp[i] * q0 + qp[i] * g0;
+				a1 -= hp[i] * q1 + qp[i] * g1;
+				x0[i] = a0;
+				x1[i] = a1;
+			}
+			if (PROD) {
+				s0 += a0 * h[i];
+				s1 += a1 * h[i];
+				p[i] += a0 * h0 + a1 * h1;
+			}
+		}
+		if (PROD) {
+			p[j] += s0 + hsum(vs0);
+			p[j + 1] += s1 + hsum(vs1);
+		}
+	}
+	if (j < c1) { // an odd last column
+		double*      x  = a + size_t(j) * ld;
+		const double q0 = UPD ? qp[j] : 0.0, g0 = UPD ? hp[j] : 0.0, h0 = PROD ? h[j] : 0.0;
+		double       s  = 0.0;
+		for (int i = j; i < len; ++i) {
+			double v = x[i];
+			if (UPD) {
+				v -= hp[i] * q0 + qp[i] * g0;
+				x[i] = v;
+			}
+			if (PROD) {
+				if (i > j) {
+					s += v * h[i];
+					p[i] += v * h0;
+				} else {
+					s += v * h0;
+				}
+			}
+		}
+		if (PROD)
+			p[j] += s;
+	}
+}
+
+template <class... Args> inline __attribute__((always_inline)) void pass_any(bool upd, bool prod, Args... args)
+{
+	if (upd && prod)
+		pass_cols<true, true>(args...);
+	else if (upd)
+		pass_cols<true, false>(args...);
+	else if (prod)
+		pass_cols<false, true>(args...);
+}
+
+__attribute__((target("avx2"))) void pass_avx2(bool upd, bool prod, int len, double* a, size_t ld, int c0, int c1,
+                                               const double* hp, const double* qp, const double* h, double* p)
+{
+	pass_any(upd, prod, len, a, ld, c0, c1, hp, qp, h, p);
+}
+
+void pass_base(bool upd, bool prod, int len, double* a, size_t ld, int c0, int c1, const double* hp,
+               const double* qp, const double* h, double* p)
+{
+	pass_any(upd, prod, len, a, ld, c0, c1, hp, qp, h, p);
+}
+
+bool host_has_avx2()
+{
+	static const bool yes = [] {
+		__builtin_cpu_init();
+		return bool(__builtin_cpu_supports("avx2"));
+	}();
+	return yes;
+}
+
+// the instruction set of trailing_pass: AVX2 where the host has it (the two
+// builds give identical results); 0 forces the baseline build
+std::atomic<int> g_pass_isa { 1 };
+
+void trailing_pass(bool upd, bool prod, int len, double* a, size_t ld, int c0, int c1, const double* hp,
+                   const double* qp, const double* h, double* p)
+{
+	if (g_pass_isa.load(std::memory_order_relaxed) && host_has_avx2())
+		pass_avx2(upd, prod, len, a, ld, c0, c1, hp, qp, h, p);
+	else
+		pass_base(upd, prod, len, a, ld, c0, c1, hp, qp, h, p);
+}
+
+} // namespace
+
+void householder_set_isa(int avx2) { g_pass_isa.store(avx2 ? 1 : 0); }
+
 // Householder reduction T = Q^T A Q of the dense symmetric n x n matrix a
 // (column-major), Q = P_0 P_1 ... P_{n-3}, P_k = I - beta_k h_k h_k^T acting
 // on rows / columns k+1..n-1 with h_k(0) = 1 (Golub and Van Loan, algorithms
@@ -381,27 +610,9 @@ void householder_tridiag(int n, const double* a, std::vector<double>& d, std::ve
 		}
 		// one pass over the lower triangle of A22 (rows / columns >= k+1):
 		// the pending update, then p += A22 h with the updated entries
-		for (int i = 0; i < len; ++i)
-			p[size_t(i)] = 0.0;
-		const double* hp = hprev.data() + 1; // h', q' from row k+1 on
-		const double* qp = qprev.data() + 1;
-		for (int j = 0; j < len; ++j) {
-			double* col = &M(k + 1, k + 1 + j); // col[i], i >= j: A22(i, j)
-			if (pending) {
-				const double hj = hp[j], qj = qp[j];
-				for (int i = j; i < len; ++i)
-					col[i] -= hp[i] * qj + qp[i] * hj;
-			}
-			if (b != 0.0) {
-				const double hj = h[j];
-				double       pj = col[j] * hj;
-				for (int i = j + 1; i < len; ++i) {
-					pj += col[i] * h[i];
-					p[size_t(i)] += col[i] * hj;
-				}
-				p[size_t(j)] += pj;
-			}
-		}
+		std::fill(p.begin(), p.begin() + len, 0.0);
+		trailing_pass(pending, b != 0.0, len, &M(k + 1, k + 1), N, 0, len, hprev.data() + 1, qprev.data() + 1, h,
+		              p.data());
 		pending = b != 0.0;
 		if (!pending)
 			continue;
@@ -552,23 +763,7 @@ void householder_tridiag_parallel(int n, const double* a, std::vector<double>& d
 			const int c0 = col_of(t), c1 = col_of(t + 1);
 			double*   pt = part[size_t(t)].data();
 			std::fill(pt, pt + len, 0.0);
-			for (int j = c0; j < c1; ++j) {
-				double* col = &M(k + 1, k + 1 + j);
-				if (pending) {
-					const double hj = hp[j], qj = qp[j];
-					for (int i = j; i < len; ++i)
-						col[i] -= hp[i] * qj + qp[i] * hj;
-				}
-				if (b != 0.0) {
-					const double hj = h[j];
-					double       pj = col[j] * hj;
-					for (int i = j + 1; i < len; ++i) {
-						pj += col[i] * h[i];
-						pt[i] += col[i] * hj;
-					}
-					pt[j] += pj;
-				}
-			}
+			trailing_pass(pending, b != 0.0, len, &M(k + 1, k + 1), N, c0, c1, hp, qp, h, pt);
 			bar.wait();
 			// p = sum of the parts, rows split among the threads
 			const int r0 = int((long long)len * t / T), r1 = int((long long)len * (t + 1) / T);
@@ -598,6 +793,77 @@ void householder_tridiag_parallel(int n, const double* a, std::vector<double>& d
 	d[N - 2]   = M(n - 2, n - 2);
 	d[N - 1]   = M(n - 1, n - 1);
 	off[N - 2] = M(n - 1, n - 2);
+}
+
+namespace {
+
+// the team that shares the Householder steps of the largest matrix: about
+// twice its share of the flops (a team of T runs at roughly T / 2 times one
+// thread), at most half the threads; none below 128 rows
+int team_size(size_t ng, const size_t* n, size_t big, int threads)
+{
+	if (threads < 4 || n[big] < 128)
+		return 0;
+	double all = 0.0;
+	for (size_t g = 0; g < ng; ++g)
+		all += double(n[g]) * double(n[g]) * double(n[g]);
+	const double share = double(n[big]) * double(n[big]) * double(n[big]) / all;
+	const int    t     = int(std::ceil(2.0 * share * threads));
+	return std::max(2, std::min(threads / 2, t));
+}
+
+} // namespace
+
+bool group_eigenvalues(size_t ng, const size_t* n, double* const* a, double* const* w,
+                       std::vector<GroupReduction>& red, int threads)
+{
+	red.assign(ng, GroupReduction {});
+	threads = std::max(1, threads);
+	std::vector<size_t> order(ng); // largest first
+	std::iota(order.begin(), order.end(), size_t(0));
+	std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return n[x] > n[y]; });
+	auto one = [&](size_t g, int team) {
+		const int n_g = int(n[g]);
+		if (n_g == 0)
+			return;
+		GroupReduction& R = red[g];
+		double*         m = a[g];
+		for (int j = 0; j < n_g; ++j) // symmetrise the round-off of the two triangles
+			for (int i = 0; i < j; ++i) {
+				const size_t ij = size_t(i) + size_t(j) * size_t(n_g), ji = size_t(j) + size_t(i) * size_t(n_g);
+				m[ij] = m[ji] = 0.5 * (m[ij] + m[ji]);
+			}
+		if (n_g == 1) {
+			R.d.assign(1, m[0]);
+			R.off.assign(1, 0.0);
+		} else if (team > 1) {
+			householder_tridiag_parallel(n_g, m, R.d, R.off, R.hv, R.beta, team);
+		} else {
+			householder_tridiag(n_g, m, R.d, R.off, R.hv, R.beta);
+		}
+		std::copy(R.d.begin(), R.d.end(), w[g]);
+		R.ok = tridiag_values(n_g, w[g], R.off.data()); // ascending
+	};
+	const int    team  = ng ? team_size(ng, n, order[0], threads) : 0;
+	const size_t first = team ? 1 : 0;
+	// the other matrices, largest first, to whichever thread is free
+	std::atomic<size_t> next { first };
+	auto                drain = [&] {
+		for (size_t q; (q = next.fetch_add(1)) < ng;)
+			one(order[q], 1);
+	};
+	std::vector<std::thread> pool;
+	for (int t = 0; t < threads - std::max(team, 1); ++t)
+		pool.emplace_back(drain);
+	if (team)
+		one(order[0], team);
+	drain();
+	for (std::thread& th : pool)
+		th.join();
+	bool ok = true;
+	for (const GroupReduction& R : red)
+		ok = ok && R.ok;
+	return ok;
 }
 
 // v (n x ncols, column-major) <- Q v

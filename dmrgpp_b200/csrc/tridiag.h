@@ -11,6 +11,13 @@ namespace dmrgpp {
 // if the iteration fails to converge.
 bool tridiag_eigen(int n, double* d, const double* off, double* z);
 
+// Eigenvalues alone (ascending, into d) of the same tridiagonal matrix by
+// the square-root-free QL iteration (rotations of tridiag_eigen where the
+// squares would leave the exponent range or the iteration fails).  They
+// agree with tridiag_eigen's to rounding (~1e-15 of the norm), not bit for
+// bit.  Returns false if neither iteration converges.
+bool tridiag_values(int n, double* d, const double* off);
+
 // Unit eigenvectors z (n x k, column-major) of the symmetric tridiagonal
 // matrix (d, off) for its eigenvalues w[0..k) (ascending, as computed by
 // tridiag_eigen) by inverse iteration: for each, three solves with the LU of
@@ -31,6 +38,30 @@ void householder_tridiag(int n, const double* a, std::vector<double>& d, std::ve
 // sums of the threads' parts make its rounding depend on the thread count.
 void householder_tridiag_parallel(int n, const double* a, std::vector<double>& d, std::vector<double>& off,
                                   std::vector<double>& hv, std::vector<double>& beta, int threads);
+
+// The instruction set of the reductions' passes over the trailing block:
+// nonzero (the default) uses AVX2 where the host has it, 0 the baseline
+// x86-64 build; both round identically (tests compare them).
+void householder_set_isa(int avx2);
+
+// One matrix's Householder reduction (the outputs of householder_tridiag;
+// n = 1: d = {a}, off = {0}, no reflectors) and whether the QL iteration on
+// it converged.
+struct GroupReduction {
+	std::vector<double> d, off, hv, beta;
+	bool                ok = true;
+};
+
+// Eigenvalues of ng dense symmetric matrices on `threads` host threads:
+// a[g] (n[g] x n[g], column-major; symmetrised in place as (a + a^T) / 2)
+// is reduced to tridiagonal form (red[g]) and its eigenvalues go, ascending,
+// to w[g].  When the largest matrix is a large share of the work, a team of
+// threads shares each of its Householder steps while the other threads take
+// the remaining matrices one at a time, largest first; the team joins them
+// when it is done.  Returns false if an iteration did not converge (that
+// group's ok is false).
+bool group_eigenvalues(size_t ng, const size_t* n, double* const* a, double* const* w,
+                       std::vector<GroupReduction>& red, int threads);
 
 // v (n x ncols, column-major) <- Q v for the reflectors of householder_tridiag.
 void apply_q(int n, const std::vector<double>& hv, const std::vector<double>& beta, double* v, int ncols);

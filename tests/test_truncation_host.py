@@ -1,9 +1,14 @@
 """The density-matrix truncation oracle on the CPU: the kept-state rule of
 Truncation::computeKeptStates (Truncation.h:476-512) on hand-worked cases,
 and the oracle's selection against the DMRG driver's own truncation."""
+import os
+import subprocess
+
 import numpy as np
 
 from oracle import truncation_oracle as to
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 EIGS = np.array([1e-9, 1e-8, 1e-6, 1e-3, 0.1, 0.898998989])
@@ -49,3 +54,17 @@ def test_oracle_selection_matches_the_driver_truncation():
     allw = np.sort(np.concatenate(out["eigenvalues"]))
     assert abs(allw.sum() - 1.0) < 1e-12                     # trace of rho = |psi|^2
     assert abs(out["discarded"] - np.abs(allw[:len(allw) - 9]).sum()) < 1e-15
+
+
+def test_group_eigenvalue_phase(tmp_path):
+    """The library's host eigenvalue phase (tridiag.cpp, compiled here with
+    g++): AVX2 and baseline reductions bitwise alike, the square-root-free QL
+    against the QL with rotations, and group_eigenvalues over mixed group
+    sizes and thread counts against each group's serial reduction."""
+    exe = str(tmp_path / "group_eigen_check")
+    csrc = os.path.join(ROOT, "dmrgpp_b200", "csrc")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I" + csrc,
+                    os.path.join(ROOT, "tests", "group_eigen_check.cpp"),
+                    os.path.join(csrc, "tridiag.cpp"), "-o", exe, "-lpthread"], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0 and out.stdout.startswith("ok"), out.stdout + out.stderr
