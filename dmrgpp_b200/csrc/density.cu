@@ -375,8 +375,8 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 		gw[g] = eigenvalues + eoff[g];
 	}
 	std::vector<GroupReduction> ge;
-	if (!group_eigenvalues(ng, d->group_size, ga.data(), gw.data(), ge,
-	                       int(std::max(2u, std::thread::hardware_concurrency())))) {
+	const int                   hw = int(std::max(2u, std::thread::hardware_concurrency()));
+	if (!group_eigenvalues(ng, d->group_size, ga.data(), gw.data(), ge, hw)) {
 		size_t g = 0;
 		while (g < ng && ge[g].ok)
 			++g;
@@ -423,16 +423,19 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 		if (!hv || !zk || !vo)
 			return fail(DMRGPP_OOM, "page-locked host buffers for the eigenvectors");
 		std::vector<double> bt(size_t(std::max<long long>(eoff[ng], 1)), 0.0);
+		std::vector<const double*> gwk(ng);
+		std::vector<double*>       gz(ng);
+		for (size_t g = 0; g < ng; ++g) {
+			gwk[g] = eigenvalues + eoff[g] + (long long)(d->group_size[g] - kept[g]);
+			gz[g]  = zk + koff[g];
+		}
+		group_eigenvectors(ng, d->group_size, kept, ge.data(), gwk.data(), gz.data(), hw);
 		parallel_for(ng, [&](size_t t) {
 			const size_t g = by_size[t];
-			const int    n = int(d->group_size[g]), k = int(kept[g]);
-			if (k == 0)
+			if (kept[g] == 0)
 				return;
-			const GroupReduction& G = ge[g];
-			tridiag_eigenvectors(n, G.d.data(), G.off.data(), eigenvalues + eoff[g] + (n - k), k,
-			                     zk + koff[g]);
-			std::copy(G.hv.begin(), G.hv.end(), hv + goff[g]);
-			std::copy(G.beta.begin(), G.beta.end(), bt.begin() + eoff[g]);
+			std::copy(ge[g].hv.begin(), ge[g].hv.end(), hv + goff[g]);
+			std::copy(ge[g].beta.begin(), ge[g].beta.end(), bt.begin() + eoff[g]);
 		});
 		g_trunc_times[DMRGPP_TRUNC_VECTORS_HOST] = seconds_since(tp);
 		tp                                       = Clock::now();

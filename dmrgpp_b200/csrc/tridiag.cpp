@@ -411,7 +411,9 @@ namespace {
 // helpers taking and returning them are always inlined, so the note that
 // their calling convention differs between the two builds does not apply.
 #pragma GCC diagnostic ignored "-Wpsabi"
-typedef double v4d __attribute__((vector_size(32), aligned(8)));
+// They may alias plain doubles: scratch arrays of them live in
+// std::vector<double> storage.
+typedef double v4d __attribute__((vector_size(32), aligned(8), may_alias));
 
 inline __attribute__((always_inline)) v4d load4(const double* x)
 {
@@ -419,8 +421,8 @@ inline __attribute__((always_inline)) v4d load4(const double* x)
 	std::memcpy(&v, x, sizeof v);
 	return v;
 }
-inline __attribute__((always_inline)) void store4(double* x, v4d v) { std::memcpy(x, &v, sizeof v); }
-inline __attribute__((always_inline)) double hsum(v4d v) { return (v[0] + v[1]) + (v[2] + v[3]); }
+inline __attribute__((always_inline)) void store4(double* x, const v4d& v) { std::memcpy(x, &v, sizeof v); }
+inline __attribute__((always_inline)) double hsum(const v4d& v) { return (v[0] + v[1]) + (v[2] + v[3]); }
 
 // One pass of a Householder step over columns [c0, c1) of the lower triangle
 // of the trailing block (len x len; column j at a + j * ld, rows i >= j).
@@ -929,119 +931,351 @@ bool sym_eigen_full(int n, const double* a, double* w, double* v)
 
 namespace dmrgpp {
 
-void tridiag_eigenvectors(int n, const double* d, const double* off, const double* w, int k, double* z)
+namespace {
+
+// uniform in [-1, 1) from (seed, index): the splitmix64 finaliser (Steele,
+// Lea and Flood, OOPSLA 2014) of their combination, top 53 bits
+inline double start_value(uint64_t seed, uint64_t i)
 {
-	if (n <= 0 || k <= 0)
-		return;
-	const size_t N = size_t(n);
-	if (n == 1) {
-		for (int j = 0; j < k; ++j)
-			z[j] = 1.0;
-		return;
-	}
+	uint64_t x = seed + 0x9e3779b97f4a7c15ULL * (i + 1);
+	x          = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+	x          = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+	x ^= x >> 31;
+	return double(x >> 11) * 0x1.0p-52 - 1.0;
+}
+
+// |T|_inf of the tridiagonal (d, off)
+double tridiag_norm(int n, const double* d, const double* off)
+{
 	double norm = 0.0;
 	for (int i = 0; i < n; ++i)
 		norm = std::max(norm, std::fabs(d[i]) + (i > 0 ? std::fabs(off[i - 1]) : 0.0)
 		                         + (i + 1 < n ? std::fabs(off[i]) : 0.0));
-	if (!(norm > 0.0)) { // the zero matrix: any orthonormal set
-		std::fill(z, z + N * size_t(k), 0.0);
-		for (int j = 0; j < k; ++j)
-			z[size_t(j) * N + size_t(j % n)] = 1.0;
-		return;
+	return norm;
+}
+
+typedef long long v4l __attribute__((vector_size(32), aligned(8), may_alias));
+
+// One vector by inverse iteration (n >= 2): the LU of T - w_j I with row
+// interchanges (as tridiag_inverse_iteration), then from the start vector
+// seeded by j three solves, each followed by Gram-Schmidt against the
+// cluster's earlier vectors ys[0..ny) and a normalisation; the largest
+// component made positive.  The arithmetic is written so that
+// eigenvectors_batch4 repeats it operation for operation.
+void eigenvector_one(int n, const double* d, const double* off, double wj, int j, double tiny, const double* const* ys,
+                     int ny, double* x, double* rp, double* u1, double* u2, double* m, char* sw)
+{
+	const size_t N = size_t(n);
+	double       a = d[0] - wj, b = off[0];
+	for (int i = 0; i + 1 < n; ++i) {
+		const double l = off[i], dd = d[i + 1] - wj, uu = i + 2 < n ? off[i + 1] : 0.0;
+		if (std::fabs(a) >= std::fabs(l)) {
+			if (a == 0.0)
+				a = tiny;
+			const double r = 1.0 / a;
+			rp[i]          = r;
+			u1[i]          = b;
+			u2[i]          = 0.0;
+			m[i]           = l * r;
+			sw[i]          = 0;
+			a              = dd - m[i] * b;
+			b              = uu;
+		} else {
+			const double r  = 1.0 / l;
+			rp[i]           = r;
+			u1[i]           = dd;
+			u2[i]           = uu;
+			m[i]            = a * r;
+			sw[i]           = 1;
+			const double na = b - m[i] * dd;
+			b               = -(m[i] * uu);
+			a               = na;
+		}
 	}
-	const double ortol = 1e-3 * norm;
-	const double tiny  = norm * 1e-15;
-	std::vector<double> u0(N), u1(N), u2(N), m(N);
-	std::vector<char>   sw(N);
-	int                 cluster = 0; // first vector of the current cluster
-	for (int j = 0; j < k; ++j) {
-		if (j > 0 && w[j] - w[j - 1] > ortol)
-			cluster = j;
-		// LU of T - w_j I with row interchanges (as tridiag_inverse_iteration)
-		std::fill(u1.begin(), u1.end(), 0.0);
-		std::fill(u2.begin(), u2.end(), 0.0);
-		std::fill(m.begin(), m.end(), 0.0);
-		std::fill(sw.begin(), sw.end(), 0);
-		double a = d[0] - w[j], b = off[0];
+	rp[N - 1] = 1.0 / (a == 0.0 ? tiny : a);
+	for (int i = 0; i < n; ++i)
+		x[i] = start_value(uint64_t(j), uint64_t(i));
+	for (int iter = 0; iter < 3; ++iter) {
 		for (int i = 0; i + 1 < n; ++i) {
-			const double l = off[i], dd = d[i + 1] - w[j], uu = i + 2 < n ? off[i + 1] : 0.0;
-			if (std::fabs(a) >= std::fabs(l)) {
-				if (a == 0.0)
-					a = tiny;
-				u0[size_t(i)] = a;
-				u1[size_t(i)] = b;
-				m[size_t(i)]  = l / a;
-				a             = dd - m[size_t(i)] * b;
-				b             = uu;
+			const double xi = x[i], xi1 = x[i + 1];
+			if (sw[i]) {
+				x[i]     = xi1;
+				x[i + 1] = xi - m[i] * xi1;
 			} else {
-				u0[size_t(i)] = l;
-				u1[size_t(i)] = dd;
-				u2[size_t(i)] = uu;
-				m[size_t(i)]  = a / l;
-				sw[size_t(i)] = 1;
-				const double na = b - m[size_t(i)] * dd;
-				b               = -m[size_t(i)] * uu;
-				a               = na;
+				x[i + 1] = xi1 - m[i] * xi;
 			}
 		}
-		u0[N - 1] = a == 0.0 ? tiny : a;
-		// seeded start vector, three solves, each followed by Gram-Schmidt
-		// against the earlier vectors of the cluster (the grouping of LAPACK's
-		// dstein: eigenvalues closer than 1e-3 |T|)
-		double*                                x = z + size_t(j) * N;
-		std::mt19937_64                        rng(0x9e3779b97f4a7c15ULL + uint64_t(j));
-		std::uniform_real_distribution<double> uni(-1.0, 1.0);
+		for (int i = n - 1; i >= 0; --i) {
+			double s = x[i];
+			if (i + 1 < n)
+				s -= u1[i] * x[i + 1];
+			if (i + 2 < n)
+				s -= u2[i] * x[i + 2];
+			x[i] = s * rp[i];
+		}
+		for (int q = 0; q < ny; ++q) {
+			const double* y = ys[q];
+			double        p = 0.0;
+			for (int i = 0; i < n; ++i)
+				p += y[i] * x[i];
+			for (int i = 0; i < n; ++i)
+				x[i] -= p * y[i];
+		}
+		double nrm = 0.0;
 		for (int i = 0; i < n; ++i)
-			x[i] = uni(rng);
-		for (int iter = 0; iter < 3; ++iter) {
-			for (int i = 0; i + 1 < n; ++i) {
-				if (sw[size_t(i)]) {
-					const double t = x[i];
-					x[i]           = x[i + 1];
-					x[i + 1]       = t - m[size_t(i)] * x[i + 1];
-				} else {
-					x[i + 1] -= m[size_t(i)] * x[i];
-				}
-			}
-			for (int i = n - 1; i >= 0; --i) {
-				double s = x[i];
-				if (i + 1 < n)
-					s -= u1[size_t(i)] * x[i + 1];
-				if (i + 2 < n)
-					s -= u2[size_t(i)] * x[i + 2];
-				x[i] = s / u0[size_t(i)];
-			}
-			for (int q = cluster; q < j; ++q) {
-				const double* y = z + size_t(q) * N;
-				double        p = 0.0;
-				for (int i = 0; i < n; ++i)
-					p += y[i] * x[i];
-				for (int i = 0; i < n; ++i)
-					x[i] -= p * y[i];
-			}
-			double nrm = 0.0;
-			for (int i = 0; i < n; ++i)
-				nrm += x[i] * x[i];
-			nrm = std::sqrt(nrm);
-			if (!(nrm > 0.0) || !std::isfinite(nrm)) { // start again from a unit vector
-				std::fill(x, x + N, 0.0);
-				x[j % n] = 1.0;
-				continue;
-			}
-			for (int i = 0; i < n; ++i)
-				x[i] /= nrm;
+			nrm += x[i] * x[i];
+		nrm = std::sqrt(nrm);
+		if (!(nrm > 0.0) || !std::isfinite(nrm)) { // start again from a unit vector
+			std::fill(x, x + N, 0.0);
+			x[j % n] = 1.0;
+			continue;
 		}
+		const double r = 1.0 / nrm;
+		for (int i = 0; i < n; ++i)
+			x[i] *= r;
+	}
+	double big = 0.0;
+	int    arg = 0;
+	for (int i = 0; i < n; ++i)
+		if (std::fabs(x[i]) > big) {
+			big = std::fabs(x[i]);
+			arg = i;
+		}
+	if (x[arg] < 0.0)
+		for (int i = 0; i < n; ++i)
+			x[i] = -x[i];
+}
+
+// Four vectors that need no Gram-Schmidt (each starts its cluster) at once,
+// one per lane: eigenvector_one's operations with the pivot choice and the
+// row interchanges as lane masks, so each lane's result is bitwise the one
+// eigenvector_one gives.  xs[l]: the output columns; scratch X, RP, U1, U2,
+// M (n each) and SW.
+inline __attribute__((always_inline)) void batch4_body(int n, const double* d, const double* off, const double* wj,
+                                                       const int* jj, double tiny, double* const* xs, v4d* X, v4d* RP,
+                                                       v4d* U1, v4d* U2, v4d* M, v4l* SW)
+{
+	const size_t N    = size_t(n);
+	const v4d    zero = { 0.0, 0.0, 0.0, 0.0 };
+	const v4d    w    = { wj[0], wj[1], wj[2], wj[3] };
+	v4d          a = d[0] - w, b = zero + off[0];
+	for (int i = 0; i + 1 < n; ++i) {
+		const double l = off[i], uu = i + 2 < n ? off[i + 1] : 0.0;
+		const v4d    dd = d[i + 1] - w;
+		const v4d    al = a < 0.0 ? -a : a;
+		const v4l    keep = al >= std::fabs(l); // no interchange
+		a                 = (keep & (a == 0.0)) ? zero + tiny : a;
+		const v4d piv     = keep ? a : zero + l;
+		const v4d r       = 1.0 / piv;
+		RP[i]             = r;
+		U1[i]             = keep ? b : dd;
+		U2[i]             = keep ? zero : zero + uu;
+		const v4d mm      = (keep ? zero + l : a) * r;
+		M[i]              = mm;
+		SW[i]             = ~keep;
+		const v4d na      = keep ? dd - mm * b : b - mm * dd;
+		b                 = keep ? zero + uu : -(mm * uu);
+		a                 = na;
+	}
+	RP[N - 1] = 1.0 / ((a == 0.0) ? zero + tiny : a);
+	for (int i = 0; i < n; ++i)
+		X[i] = v4d { start_value(uint64_t(jj[0]), uint64_t(i)), start_value(uint64_t(jj[1]), uint64_t(i)),
+			     start_value(uint64_t(jj[2]), uint64_t(i)), start_value(uint64_t(jj[3]), uint64_t(i)) };
+	for (int iter = 0; iter < 3; ++iter) {
+		for (int i = 0; i + 1 < n; ++i) {
+			const v4d xi = X[i], xi1 = X[i + 1];
+			const v4l s  = SW[i];
+			X[i]         = s ? xi1 : xi;
+			X[i + 1]     = s ? xi - M[i] * xi1 : xi1 - M[i] * xi;
+		}
+		for (int i = n - 1; i >= 0; --i) {
+			v4d s = X[i];
+			if (i + 1 < n)
+				s -= U1[i] * X[i + 1];
+			if (i + 2 < n)
+				s -= U2[i] * X[i + 2];
+			X[i] = s * RP[i];
+		}
+		v4d nrm = zero;
+		for (int i = 0; i < n; ++i)
+			nrm += X[i] * X[i];
+		v4d r = zero;
+		for (int q = 0; q < 4; ++q) {
+			const double t = std::sqrt(nrm[q]);
+			if (!(t > 0.0) || !std::isfinite(t)) { // this lane starts again from a unit vector
+				for (int i = 0; i < n; ++i)
+					X[i][q] = i == jj[q] % n ? 1.0 : 0.0;
+				r[q] = 1.0;
+			} else {
+				r[q] = 1.0 / t;
+			}
+		}
+		for (int i = 0; i < n; ++i)
+			X[i] *= r;
+	}
+	for (int q = 0; q < 4; ++q) {
 		double big = 0.0;
 		int    arg = 0;
 		for (int i = 0; i < n; ++i)
-			if (std::fabs(x[i]) > big) {
-				big = std::fabs(x[i]);
+			if (std::fabs(X[i][q]) > big) {
+				big = std::fabs(X[i][q]);
 				arg = i;
 			}
-		if (x[arg] < 0.0)
-			for (int i = 0; i < n; ++i)
-				x[i] = -x[i];
+		const double sgn = X[size_t(arg)][q] < 0.0 ? -1.0 : 1.0;
+		double*      x   = xs[q];
+		for (int i = 0; i < n; ++i)
+			x[i] = sgn < 0.0 ? -X[i][q] : X[i][q];
 	}
+}
+
+__attribute__((target("avx2"))) void batch4_avx2(int n, const double* d, const double* off, const double* wj,
+                                                 const int* jj, double tiny, double* const* xs, v4d* X, v4d* RP,
+                                                 v4d* U1, v4d* U2, v4d* M, v4l* SW)
+{
+	batch4_body(n, d, off, wj, jj, tiny, xs, X, RP, U1, U2, M, SW);
+}
+
+void batch4_base(int n, const double* d, const double* off, const double* wj, const int* jj, double tiny,
+                 double* const* xs, v4d* X, v4d* RP, v4d* U1, v4d* U2, v4d* M, v4l* SW)
+{
+	batch4_body(n, d, off, wj, jj, tiny, xs, X, RP, U1, U2, M, SW);
+}
+
+// 0 turns the four-lane batches off (tests compare the two)
+std::atomic<int> g_batch_vectors { 1 };
+
+// Vectors j0 .. j1 - 1 of tridiag_eigenvectors (n >= 2, norm > 0); j0 starts
+// a cluster, so the range needs no vector before it.  The vectors that start
+// their cluster (no Gram-Schmidt) go four at a time, the others follow one
+// by one in order, after the earlier vectors of their cluster.
+void eigenvectors_range(int n, const double* d, const double* off, const double* w, int j0, int j1, double norm,
+                        double* z)
+{
+	const size_t N     = size_t(n);
+	const double ortol = 1e-3 * norm;
+	const double tiny  = norm * 1e-15;
+	auto         col   = [&](int j) { return z + size_t(j - j0) * N; };
+	auto         starts = [&](int j) { return j == j0 || w[j] - w[j - 1] > ortol; };
+	std::vector<int> lone, rest;
+	for (int j = j0; j < j1; ++j)
+		(starts(j) ? lone : rest).push_back(j);
+	size_t done = 0;
+	if (g_batch_vectors.load(std::memory_order_relaxed) && lone.size() >= 4) {
+		std::vector<double>    buf(20 * N); // X, RP, U1, U2, M: four lanes per row
+		std::vector<long long> swb(4 * N);
+		v4d* const             X    = reinterpret_cast<v4d*>(buf.data());
+		v4d* const             RP   = X + N;
+		v4d* const             U1   = RP + N;
+		v4d* const             U2   = U1 + N;
+		v4d* const             M    = U2 + N;
+		v4l* const             SW   = reinterpret_cast<v4l*>(swb.data());
+		const bool             avx2 = g_pass_isa.load(std::memory_order_relaxed) && host_has_avx2();
+		for (; done + 4 <= lone.size(); done += 4) {
+			const int     jj[4] = { lone[done], lone[done + 1], lone[done + 2], lone[done + 3] };
+			const double  wj[4] = { w[jj[0]], w[jj[1]], w[jj[2]], w[jj[3]] };
+			double* const xs[4] = { col(jj[0]), col(jj[1]), col(jj[2]), col(jj[3]) };
+			if (avx2)
+				batch4_avx2(n, d, off, wj, jj, tiny, xs, X, RP, U1, U2, M, SW);
+			else
+				batch4_base(n, d, off, wj, jj, tiny, xs, X, RP, U1, U2, M, SW);
+		}
+	}
+	std::vector<double>        rp(N), u1(N), u2(N), m(N);
+	std::vector<char>          sw(N);
+	std::vector<const double*> ys;
+	auto one = [&](int j) {
+		ys.clear();
+		int c = j; // first vector of j's cluster
+		while (!starts(c))
+			--c;
+		for (int q = c; q < j; ++q)
+			ys.push_back(col(q));
+		eigenvector_one(n, d, off, w[j], j, tiny, ys.data(), int(ys.size()), col(j), rp.data(), u1.data(),
+		                u2.data(), m.data(), sw.data());
+	};
+	for (; done < lone.size(); ++done)
+		one(lone[done]);
+	for (int j : rest)
+		one(j);
+}
+
+// the matrices where every vector is fixed without iterating: n = 1, and the
+// zero matrix (any orthonormal set); true when z was filled here
+bool trivial_eigenvectors(int n, int k, double norm, double* z)
+{
+	const size_t N = size_t(n);
+	if (n == 1) {
+		for (int j = 0; j < k; ++j)
+			z[j] = 1.0;
+		return true;
+	}
+	if (!(norm > 0.0)) {
+		std::fill(z, z + N * size_t(k), 0.0);
+		for (int j = 0; j < k; ++j)
+			z[size_t(j) * N + size_t(j % n)] = 1.0;
+		return true;
+	}
+	return false;
+}
+
+} // namespace
+
+void eigenvectors_set_batch(int on) { g_batch_vectors.store(on ? 1 : 0); }
+
+void tridiag_eigenvectors(int n, const double* d, const double* off, const double* w, int k, double* z)
+{
+	if (n <= 0 || k <= 0)
+		return;
+	const double norm = n > 1 ? tridiag_norm(n, d, off) : 0.0;
+	if (trivial_eigenvectors(n, k, norm, z))
+		return;
+	eigenvectors_range(n, d, off, w, 0, k, norm, z);
+}
+
+void group_eigenvectors(size_t ng, const size_t* n, const size_t* k, const GroupReduction* red,
+                        const double* const* w, double* const* z, int threads)
+{
+	// work items: runs of at least 16 vectors of one group, cut only where a
+	// cluster ends, so each item computes what the serial call would
+	struct Item {
+		size_t g;
+		int    j0, j1;
+		double cost;
+	};
+	std::vector<Item>   items;
+	std::vector<double> norm(ng, 0.0);
+	for (size_t g = 0; g < ng; ++g) {
+		const int n_g = int(n[g]), k_g = int(k[g]);
+		if (n_g <= 0 || k_g <= 0)
+			continue;
+		norm[g] = n_g > 1 ? tridiag_norm(n_g, red[g].d.data(), red[g].off.data()) : 0.0;
+		if (trivial_eigenvectors(n_g, k_g, norm[g], z[g]))
+			continue;
+		const double ortol = 1e-3 * norm[g];
+		int          j0    = 0;
+		for (int j = 1; j <= k_g; ++j)
+			if (j == k_g || (j - j0 >= 16 && w[g][j] - w[g][j - 1] > ortol)) {
+				items.push_back({ g, j0, j, double(j - j0) * double(n_g) });
+				j0 = j;
+			}
+	}
+	std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
+	std::atomic<size_t> next { 0 };
+	auto                drain = [&] {
+		for (size_t q; (q = next.fetch_add(1)) < items.size();) {
+			const Item& it = items[q];
+			const int   n_g = int(n[it.g]);
+			eigenvectors_range(n_g, red[it.g].d.data(), red[it.g].off.data(), w[it.g], it.j0, it.j1, norm[it.g],
+			                   z[it.g] + size_t(it.j0) * size_t(n_g));
+		}
+	};
+	std::vector<std::thread> pool;
+	const int                nt = int(std::min<size_t>(size_t(std::max(1, threads)), std::max<size_t>(items.size(), 1)));
+	for (int t = 1; t < nt; ++t)
+		pool.emplace_back(drain);
+	drain();
+	for (std::thread& th : pool)
+		th.join();
 }
 
 } // namespace dmrgpp

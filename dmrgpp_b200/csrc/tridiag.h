@@ -21,10 +21,16 @@ bool tridiag_values(int n, double* d, const double* off);
 // Unit eigenvectors z (n x k, column-major) of the symmetric tridiagonal
 // matrix (d, off) for its eigenvalues w[0..k) (ascending, as computed by
 // tridiag_eigen) by inverse iteration: for each, three solves with the LU of
-// T - w_j I from a seeded start vector, each followed by Gram-Schmidt against
-// the earlier vectors of its cluster (eigenvalues closer than 1e-3 |T|, the
-// grouping of LAPACK's dstein); the largest component is made positive.
+// T - w_j I from a start vector seeded by j, each followed by Gram-Schmidt
+// against the earlier vectors of its cluster (eigenvalues closer than
+// 1e-3 |T|, the grouping of LAPACK's dstein); the largest component is made
+// positive.
 void tridiag_eigenvectors(int n, const double* d, const double* off, const double* w, int k, double* z);
+
+// Vectors that start their cluster go four at a time through vector lanes
+// (bitwise the one-at-a-time result); 0 turns that off, nonzero (the
+// default) on.
+void eigenvectors_set_batch(int on);
 
 // Householder reduction T = Q^T A Q of the dense symmetric n x n matrix a
 // (column-major, n >= 2), Q = P_0 ... P_{n-3}, P_k = I - beta_k h_k h_k^T
@@ -62,6 +68,13 @@ struct GroupReduction {
 // group's ok is false).
 bool group_eigenvalues(size_t ng, const size_t* n, double* const* a, double* const* w,
                        std::vector<GroupReduction>& red, int threads);
+
+// tridiag_eigenvectors of the tridiagonals red[g] for k[g] eigenvalues
+// w[g][0..k[g]) into z[g] (n[g] x k[g]), all groups on `threads` threads:
+// the vectors of a group go in runs cut only where a cluster ends, so the
+// result is the serial one whatever the thread count.
+void group_eigenvectors(size_t ng, const size_t* n, const size_t* k, const GroupReduction* red,
+                        const double* const* w, double* const* z, int threads);
 
 // v (n x ncols, column-major) <- Q v for the reflectors of householder_tridiag.
 void apply_q(int n, const std::vector<double>& hv, const std::vector<double>& beta, double* v, int ncols);

@@ -60,8 +60,8 @@ def density_truncate(lsz: Sequence[int], rsz: Sequence[int], patch_group: Sequen
     evals, evecs, e0, v0 = [], [], 0, 0
     for n, k in zip(gs.astype(np.int64), kept.astype(np.int64)):
         evals.append(eig[e0:e0 + n].copy())
-        if vectors:
-            evecs.append(vec[v0:v0 + n * k].reshape(n, k, order="F").copy())
+        if vectors:   # views into the one packed output buffer
+            evecs.append(vec[v0:v0 + n * k].reshape(n, k, order="F"))
         e0 += n
         v0 += n * k
     return {"eigenvalues": evals, "vectors": evecs if vectors else None,
