@@ -801,7 +801,8 @@ namespace {
 
 // the team that shares the Householder steps of the largest matrix: about
 // twice its share of the flops (a team of T runs at roughly T / 2 times one
-// thread), at most half the threads; none below 128 rows
+// thread), at most half the threads and at most 8 (three barriers per step
+// cost more than a larger team saves); none below 128 rows
 int team_size(size_t ng, const size_t* n, size_t big, int threads)
 {
 	if (threads < 4 || n[big] < 128)
@@ -811,7 +812,7 @@ int team_size(size_t ng, const size_t* n, size_t big, int threads)
 		all += double(n[g]) * double(n[g]) * double(n[g]);
 	const double share = double(n[big]) * double(n[big]) * double(n[big]) / all;
 	const int    t     = int(std::ceil(2.0 * share * threads));
-	return std::max(2, std::min(threads / 2, t));
+	return std::max(2, std::min(std::min(threads / 2, 8), t));
 }
 
 } // namespace
