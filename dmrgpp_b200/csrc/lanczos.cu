@@ -930,17 +930,18 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
 	if (maxn == 1)
 		j_stop = 0;
 
-	// Ritz vector of the (j_stop+1)-dimensional tridiagonal (LanczosSolver.h:76-84)
+	// Ritz vector of the (j_stop+1)-dimensional tridiagonal (LanczosSolver.h:76-84):
+	// the lowest of the QL eigenvalues and its eigenvector (by inverse
+	// iteration, O(n), unless the next eigenvalue coincides with it)
 	const size_t        n = j_stop + 1;
-	std::vector<double> d(hb, hb + n), off(hb + w->cols + 1, hb + w->cols + n), zt(n * n);
+	std::vector<double> d(hb, hb + n), off(hb + w->cols + 1, hb + w->cols + n), zt(n);
 	if (maxn == 1) { // no loop ran: alpha[0] has not been read back yet
 		if ((e = dmrgpp::download_sync(w->host, w->scal, sizeof(double), h->stream)))
 			return cuda_status(h, e, "read alpha");
 		d[0] = w->host[0];
 	}
-	if (!tridiag_eigen(int(n), d.data(), off.data(), zt.data()))
+	if (!tridiag_lowest(int(n), d.data(), off.data(), energy, zt.data()))
 		return handle_fail(h, DMRGPP_NOT_CONVERGED, "tridiagonal eigensolve failed");
-	*energy = d[0];
 	if ((e = cudaMemcpyAsync(w->r, zt.data(), n * sizeof(double), cudaMemcpyHostToDevice, st)))
 		return cuda_status(h, e, "upload Ritz coefficients");
 	double* zdst = on_device ? z : col(j_stop + 1); // that column is free after the solve

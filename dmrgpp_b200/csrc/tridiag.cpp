@@ -400,6 +400,29 @@ void tridiag_inverse_iteration(int n, const double* d, const double* off, double
 	}
 }
 
+bool tridiag_lowest(int n, const double* d, const double* off, double* theta, double* z)
+{
+	if (n <= 0)
+		return true;
+	std::vector<double> ev(d, d + n);
+	if (!tridiag_eigen(n, ev.data(), off, nullptr))
+		return false;
+	*theta = ev[0];
+	double norm = 0.0;
+	for (double x : ev)
+		norm = std::max(norm, std::fabs(x));
+	if (n == 1 || ev[1] - ev[0] > 1e-8 * std::max(1.0, norm)) {
+		tridiag_inverse_iteration(n, d, off, ev[0], z);
+		return true;
+	}
+	// the two lowest coincide: every eigenvector by QL, the first one kept
+	std::vector<double> dv(d, d + n), zz(size_t(n) * size_t(n));
+	if (!tridiag_eigen(n, dv.data(), off, zz.data()))
+		return false;
+	std::copy(zz.begin(), zz.begin() + n, z);
+	return true;
+}
+
 } // namespace dmrgpp
 
 namespace dmrgpp {

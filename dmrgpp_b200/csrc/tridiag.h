@@ -114,4 +114,13 @@ double tridiag_kth_lowest(int n, const double* d, const double* off, int k);
 // T - theta I); the component of largest magnitude is made positive.
 void tridiag_inverse_iteration(int n, const double* d, const double* off, double theta, double* z);
 
+// The lowest eigenpair of the symmetric tridiagonal (d, off): *theta the
+// lowest of tridiag_eigen's eigenvalues (bitwise), z (n) its unit
+// eigenvector by tridiag_inverse_iteration, O(n), when the next eigenvalue
+// lies more than 1e-8 max(1, |T|) above it; otherwise (a near-degenerate
+// pair, or copies of a converged value from a Lanczos run without
+// reorthogonalisation) the first of tridiag_eigen's eigenvectors, O(n^3).
+// Returns false if the QL iteration fails.
+bool tridiag_lowest(int n, const double* d, const double* off, double* theta, double* z);
+
 } // namespace dmrgpp

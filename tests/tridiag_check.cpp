@@ -7,6 +7,7 @@
 // Prints "ok <worst eigenvalue error> <worst residual>" or "FAIL ...".
 #include "tridiag.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <random>
@@ -225,6 +226,50 @@ int main()
 			return 1;
 		}
 		worst_e = std::max(worst_e, de / scale * 1e-1);
+	}
+	// the lowest eigenpair for the Lanczos Ritz vector (tridiag_lowest):
+	// the energy bitwise tridiag_eigen's, the vector QL's first up to sign;
+	// a pair degenerate to the last bit (two decoupled copies of one block,
+	// as a Lanczos run without reorthogonalisation makes) takes QL's vector
+	for (int trial = 0; trial < 60; ++trial) {
+		const int           n    = 1 + (trial * 29) % 400;
+		const bool          copy = trial % 6 == 5 && n >= 4;
+		std::vector<double> d(static_cast<size_t>(n)), e(static_cast<size_t>(n), 0.0);
+		for (int i = 0; i < n; ++i) {
+			d[size_t(i)] = -2533.0 + 50.0 * u(rng);
+			e[size_t(i)] = 20.0 + 5.0 * u(rng);
+		}
+		if (copy)
+			for (int i = 0; i < n / 2; ++i) {
+				d[size_t(n / 2 + i)] = d[size_t(i)];
+				e[size_t(n / 2 + i)] = i + 1 < n / 2 ? e[size_t(i)] : 0.0;
+				if (i + 1 == n / 2)
+					e[size_t(i)] = 0.0;
+			}
+		std::vector<double> w(d), Z(size_t(n) * size_t(n)), z(static_cast<size_t>(n));
+		dmrgpp::tridiag_eigen(n, w.data(), e.data(), Z.data());
+		double theta = 0.0;
+		if (!dmrgpp::tridiag_lowest(n, d.data(), e.data(), &theta, z.data()) || theta != w[0]) {
+			std::printf("FAIL lowest value %d\n", trial);
+			return 1;
+		}
+		double ov = 0.0, res = 0.0;
+		for (int i = 0; i < n; ++i) {
+			ov += z[size_t(i)] * Z[size_t(i)];
+			double t = (d[size_t(i)] - theta) * z[size_t(i)];
+			if (i > 0)
+				t += e[size_t(i - 1)] * z[size_t(i - 1)];
+			if (i + 1 < n)
+				t += e[size_t(i)] * z[size_t(i + 1)];
+			res = std::max(res, std::fabs(t));
+		}
+		const bool degenerate = n >= 2 && w[1] - w[0] <= 1e-8 * std::max(1.0, std::fabs(w[0]));
+		if ((copy && !degenerate) || (degenerate && !std::equal(z.begin(), z.end(), Z.begin()))
+		    || std::fabs(1.0 - std::fabs(ov)) > 1e-12 || res > 1e-11 * std::fabs(theta)) {
+			std::printf("FAIL lowest vector %d n %d %g %g\n", trial, n, 1.0 - std::fabs(ov), res);
+			return 1;
+		}
+		worst_r = std::max(worst_r, res / std::fabs(theta));
 	}
 	if (worst_e > 1e-13 || worst_r > 1e-12) {
 		std::printf("FAIL %g %g\n", worst_e, worst_r);
