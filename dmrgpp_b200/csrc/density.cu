@@ -471,7 +471,9 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 			    || (e = cudaMemcpyAsync(vo, v, size_t(koff[ng]) * sizeof(double), cudaMemcpyDeviceToHost, st))
 			    || (e = cudaStreamSynchronize(st)))
 				return cuda_fail(e, "eigenvectors");
-			std::copy(vo, vo + koff[ng], vectors);
+			parallel_for(ng, [&](size_t g) { // to the caller's (pageable) buffer, group by group
+				std::copy(vo + koff[g], vo + koff[g + 1], vectors + koff[g]);
+			});
 		}
 	}
 	if (vectors)
