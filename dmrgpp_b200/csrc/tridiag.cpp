@@ -1,4 +1,5 @@
-// Symmetric tridiagonal eigensolver for the Lanczos and Davidson drivers.
+// Host eigensolvers in FP64: the tridiagonal problems of the Lanczos and
+// Davidson drivers, and the density-matrix groups of the truncation.
 //
 // The reference obtains the Ritz values of its Lanczos tridiagonal with
 // LAPACK dstedc (PsimagLite/src/PsimagLite/TridiagonalMatrix.cpp:21) and the
@@ -6,7 +7,13 @@
 // (LanczosSolver.h:76-84).  Here both come from one implementation of the
 // implicit QL algorithm with shifts taken from the leading 2x2 block
 // (Bowdler, Martin, Reinsch and Wilkinson, Numer. Math. 11 (1968) 293-306;
-// Golub and Van Loan, Matrix Computations, section 8.3), in FP64.
+// Golub and Van Loan, Matrix Computations, section 8.3); the lowest Ritz
+// vector alone by inverse iteration.  The truncation's groups (the
+// reference's per-group SVD, DensityMatrixSvd.h:355-410) go through a
+// Householder reduction to tridiagonal form (vectorised passes, a thread
+// team for the largest group), the square-root-free QL for the eigenvalues
+// and inverse iteration for the kept eigenvectors, spread over the host's
+// threads.
 #include "tridiag.h"
 
 #include <algorithm>

@@ -1,4 +1,5 @@
-// Symmetric tridiagonal eigensolver (tridiag.cpp).
+// Host eigensolvers (tridiag.cpp): symmetric tridiagonal problems of the
+// Lanczos and Davidson drivers, and the truncation's density-matrix groups.
 #pragma once
 
 #include <vector>
