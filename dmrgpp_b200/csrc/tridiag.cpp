@@ -855,12 +855,12 @@ bool group_eigenvalues(size_t ng, const size_t* n, double* const* a, double* con
 	std::vector<size_t> order(ng); // largest first
 	std::iota(order.begin(), order.end(), size_t(0));
 	std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return n[x] > n[y]; });
-	auto one = [&](size_t g, int team) {
-		const int n_g = int(n[g]);
-		if (n_g == 0)
-			return;
-		GroupReduction& R = red[g];
-		double*         m = a[g];
+	// the reduction of one matrix (symmetrised first), by a team of `team`
+	// threads when team > 1; then its eigenvalues
+	auto reduce = [&](size_t g, int team) {
+		const int       n_g = int(n[g]);
+		GroupReduction& R   = red[g];
+		double*         m   = a[g];
 		for (int j = 0; j < n_g; ++j) // symmetrise the round-off of the two triangles
 			for (int i = 0; i < j; ++i) {
 				const size_t ij = size_t(i) + size_t(j) * size_t(n_g), ji = size_t(j) + size_t(i) * size_t(n_g);
@@ -874,8 +874,11 @@ bool group_eigenvalues(size_t ng, const size_t* n, double* const* a, double* con
 		} else {
 			householder_tridiag(n_g, m, R.d, R.off, R.hv, R.beta);
 		}
+	};
+	auto values = [&](size_t g) {
+		GroupReduction& R = red[g];
 		std::copy(R.d.begin(), R.d.end(), w[g]);
-		R.ok = tridiag_values(n_g, w[g], R.off.data()); // ascending
+		R.ok = tridiag_values(int(n[g]), w[g], R.off.data()); // ascending
 	};
 	const int    team  = ng ? team_size(ng, n, order[0], threads) : 0;
 	const size_t first = team ? 1 : 0;
@@ -883,13 +886,20 @@ bool group_eigenvalues(size_t ng, const size_t* n, double* const* a, double* con
 	std::atomic<size_t> next { first };
 	auto                drain = [&] {
 		for (size_t q; (q = next.fetch_add(1)) < ng;)
-			one(order[q], 1);
+			if (n[order[q]] > 0) {
+				reduce(order[q], 1);
+				values(order[q]);
+			}
 	};
 	std::vector<std::thread> pool;
 	for (int t = 0; t < threads - std::max(team, 1); ++t)
 		pool.emplace_back(drain);
-	if (team)
-		one(order[0], team);
+	if (team) {
+		reduce(order[0], team);
+		for (int t = 1; t < team; ++t) // the team's other threads take matrices now
+			pool.emplace_back(drain);
+		values(order[0]);
+	}
 	drain();
 	for (std::thread& th : pool)
 		th.join();
