@@ -866,6 +866,25 @@ bool group_eigenvalues(size_t ng, const size_t* n, double* const* a, double* con
 				const size_t ij = size_t(i) + size_t(j) * size_t(n_g), ji = size_t(j) + size_t(i) * size_t(n_g);
 				m[ij] = m[ji] = 0.5 * (m[ij] + m[ji]);
 			}
+		// largest entry outside [2^-64, 2^64]: reduce 2^shift m instead
+		// (exact; the reflectors do not change), so that the squares of the
+		// eigenvalue iteration and the growth of inverse iteration (up to
+		// 1e15 / |T|) stay far inside the exponent range
+		const size_t        nn   = size_t(n_g) * size_t(n_g);
+		double              amax = 0.0;
+		std::vector<double> scaled;
+		for (size_t q = 0; q < nn; ++q)
+			amax = std::max(amax, std::fabs(m[q]));
+		R.shift = 0;
+		if (amax > 0.0 && std::isfinite(amax) && (amax < 0x1p-64 || amax > 0x1p64)) {
+			int e = 0;
+			std::frexp(amax, &e);
+			R.shift = -e;
+			scaled.resize(nn);
+			for (size_t q = 0; q < nn; ++q)
+				scaled[q] = std::ldexp(m[q], R.shift);
+			m = scaled.data();
+		}
 		if (n_g == 1) {
 			R.d.assign(1, m[0]);
 			R.off.assign(1, 0.0);
@@ -879,6 +898,11 @@ bool group_eigenvalues(size_t ng, const size_t* n, double* const* a, double* con
 		GroupReduction& R = red[g];
 		std::copy(R.d.begin(), R.d.end(), w[g]);
 		R.ok = tridiag_values(int(n[g]), w[g], R.off.data()); // ascending
+		if (R.shift) {
+			R.scaled_values.assign(w[g], w[g] + n[g]);
+			for (size_t i = 0; i < n[g]; ++i)
+				w[g][i] = std::ldexp(w[g][i], -R.shift);
+		}
 	};
 	const int    team  = ng ? team_size(ng, n, order[0], threads) : 0;
 	const size_t first = team ? 1 : 0;
@@ -1054,14 +1078,18 @@ void eigenvector_one(int n, const double* d, const double* off, double wj, int j
 				s -= u2[i] * x[i + 2];
 			x[i] = s * rp[i];
 		}
-		for (int q = 0; q < ny; ++q) {
-			const double* y = ys[q];
-			double        p = 0.0;
-			for (int i = 0; i < n; ++i)
-				p += y[i] * x[i];
-			for (int i = 0; i < n; ++i)
-				x[i] -= p * y[i];
-		}
+		// Gram-Schmidt against the cluster's earlier vectors; after the last
+		// solve twice, since the solve leaves x almost entirely in their span
+		// and one pass keeps rounding errors of that size ("twice is enough")
+		for (int pass = 0; pass < (iter == 2 ? 2 : 1); ++pass)
+			for (int q = 0; q < ny; ++q) {
+				const double* y = ys[q];
+				double        p = 0.0;
+				for (int i = 0; i < n; ++i)
+					p += y[i] * x[i];
+				for (int i = 0; i < n; ++i)
+					x[i] -= p * y[i];
+			}
 		double nrm = 0.0;
 		for (int i = 0; i < n; ++i)
 			nrm += x[i] * x[i];
@@ -1259,6 +1287,51 @@ bool trivial_eigenvectors(int n, int k, double norm, double* z)
 	return false;
 }
 
+// The kept vectors whose eigenvalues are rounding noise (at most n eps |T|
+// in magnitude: a density matrix of lower rank than its group) span a part
+// of the numerical null space that inverse iteration cannot resolve; each
+// Gram-Schmidt pass inside that cluster carries over the errors of the
+// earlier vectors, which renormalisation amplifies.  Since a group's kept
+// vectors are its largest, every eigenvector above such a vector is kept
+// too: they are projected out of the null vectors (twice), and the null
+// vectors are orthonormalised again among themselves (twice).  z: n x k for
+// the ascending eigenvalues w[0..k).
+void clean_null_vectors(int n, int k, const double* w, double norm, double* z)
+{
+	const size_t N    = size_t(n);
+	const double null = double(n) * DBL_EPSILON * norm;
+	int          jn   = 0; // vectors [0, jn) are null
+	while (jn < k && std::fabs(w[jn]) <= null)
+		++jn;
+	if (jn == 0 || (jn == 1 && jn == k))
+		return;
+	auto project = [&](double* x, const double* y) {
+		double p = 0.0;
+		for (size_t i = 0; i < N; ++i)
+			p += y[i] * x[i];
+		for (size_t i = 0; i < N; ++i)
+			x[i] -= p * y[i];
+	};
+	for (int j = 0; j < jn; ++j) {
+		double* x = z + size_t(j) * N;
+		for (int pass = 0; pass < 2; ++pass) {
+			for (int q = jn; q < k; ++q)
+				project(x, z + size_t(q) * N);
+			for (int q = 0; q < j; ++q)
+				project(x, z + size_t(q) * N);
+		}
+		double nrm = 0.0;
+		for (size_t i = 0; i < N; ++i)
+			nrm += x[i] * x[i];
+		nrm = std::sqrt(nrm);
+		if (nrm > 0.0 && std::isfinite(nrm)) {
+			const double r = 1.0 / nrm;
+			for (size_t i = 0; i < N; ++i)
+				x[i] *= r;
+		}
+	}
+}
+
 } // namespace
 
 void eigenvectors_set_batch(int on) { g_batch_vectors.store(on ? 1 : 0); }
@@ -1271,6 +1344,7 @@ void tridiag_eigenvectors(int n, const double* d, const double* off, const doubl
 	if (trivial_eigenvectors(n, k, norm, z))
 		return;
 	eigenvectors_range(n, d, off, w, 0, k, norm, z);
+	clean_null_vectors(n, k, w, norm, z);
 }
 
 void group_eigenvectors(size_t ng, const size_t* n, const size_t* k, const GroupReduction* red,
@@ -1285,6 +1359,13 @@ void group_eigenvectors(size_t ng, const size_t* n, const size_t* k, const Group
 	};
 	std::vector<Item>   items;
 	std::vector<double> norm(ng, 0.0);
+	// a group reduced as 2^shift A: its own eigenvalues of that matrix (the
+	// unscaled ones may have lost bits below the normal range)
+	std::vector<const double*> ws(w, w + ng);
+	for (size_t g = 0; g < ng; ++g)
+		if (red[g].shift && k[g] > 0 && red[g].scaled_values.size() == n[g])
+			ws[g] = red[g].scaled_values.data() + (n[g] - k[g]);
+	w = ws.data();
 	for (size_t g = 0; g < ng; ++g) {
 		const int n_g = int(n[g]), k_g = int(k[g]);
 		if (n_g <= 0 || k_g <= 0)
@@ -1315,6 +1396,19 @@ void group_eigenvectors(size_t ng, const size_t* n, const size_t* k, const Group
 	for (int t = 1; t < nt; ++t)
 		pool.emplace_back(drain);
 	drain();
+	for (std::thread& th : pool)
+		th.join();
+	// the groups' null vectors, once all their vectors are there
+	std::atomic<size_t> ng_next { 0 };
+	auto                clean = [&] {
+		for (size_t g; (g = ng_next.fetch_add(1)) < ng;)
+			if (n[g] >= 2 && k[g] > 0 && norm[g] > 0.0)
+				clean_null_vectors(int(n[g]), int(k[g]), w[g], norm[g], z[g]);
+	};
+	pool.clear();
+	for (int t = 1; t < nt; ++t)
+		pool.emplace_back(clean);
+	clean();
 	for (std::thread& th : pool)
 		th.join();
 }

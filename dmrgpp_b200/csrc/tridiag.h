@@ -53,10 +53,15 @@ void householder_set_isa(int avx2);
 
 // One matrix's Householder reduction (the outputs of householder_tridiag;
 // n = 1: d = {a}, off = {0}, no reflectors) and whether the QL iteration on
-// it converged.
+// it converged.  d and off are those of 2^shift A: a matrix whose largest
+// entry lies outside [2^-64, 2^64] (a group of negligible weight, say) is
+// reduced scaled by a power of two, exactly, which leaves the reflectors as
+// they are.
 struct GroupReduction {
 	std::vector<double> d, off, hv, beta;
-	bool                ok = true;
+	std::vector<double> scaled_values; // shift != 0: the eigenvalues of 2^shift A
+	int                 shift = 0;
+	bool                ok    = true;
 };
 
 // Eigenvalues of ng dense symmetric matrices on `threads` host threads:
@@ -65,13 +70,16 @@ struct GroupReduction {
 // to w[g].  When the largest matrix is a large share of the work, a team of
 // threads shares each of its Householder steps while the other threads take
 // the remaining matrices one at a time, largest first; the team joins them
-// when it is done.  Returns false if an iteration did not converge (that
+// when it is done.  w[g] holds the eigenvalues of a[g] itself (scaled back
+// from 2^shift a[g]).  Returns false if an iteration did not converge (that
 // group's ok is false).
 bool group_eigenvalues(size_t ng, const size_t* n, double* const* a, double* const* w,
                        std::vector<GroupReduction>& red, int threads);
 
 // tridiag_eigenvectors of the tridiagonals red[g] for k[g] eigenvalues
-// w[g][0..k[g]) into z[g] (n[g] x k[g]), all groups on `threads` threads:
+// w[g][0..k[g]) (of the unscaled matrices, as group_eigenvalues returns
+// them: the group's largest; a scaled group uses its scaled_values instead)
+// into z[g] (n[g] x k[g]), all groups on `threads` threads:
 // the vectors of a group go in runs cut only where a cluster ends, so the
 // result is the serial one whatever the thread count.
 void group_eigenvectors(size_t ng, const size_t* n, const size_t* k, const GroupReduction* red,

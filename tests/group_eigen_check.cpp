@@ -9,7 +9,8 @@
 // the kept eigenvectors by inverse iteration four lanes at a time bitwise
 // equal to one at a time, group_eigenvectors bitwise equal to the serial
 // tridiag_eigenvectors of each group, with small residuals and orthonormal
-// columns, on matrices with clusters and exactly repeated eigenvalues.
+// columns, on matrices with clusters and exactly repeated eigenvalues; and
+// groups of subnormal or huge entries reduced scaled by a power of two.
 // Prints "ok <worst eigenvalue difference / norm>" or "FAIL ...".
 #include "tridiag.h"
 
@@ -295,6 +296,47 @@ int main()
 					std::printf("FAIL group_eigenvectors %zu threads %d\n", g, threads);
 					return 1;
 				}
+		}
+	}
+	// 5. groups near the underflow threshold and far above 1: reduced scaled
+	// by a power of two; eigenvalues and kept vectors those of the exactly
+	// rescaled matrix
+	for (int e2 : { -1060, -1030, -150, 620 }) {
+		const int           n = 70;
+		std::vector<double> b = matrix(n, 2); // normal range: the reference
+		std::vector<double> a(b.size());
+		for (size_t q = 0; q < b.size(); ++q) {
+			a[q] = std::ldexp(b[q], e2);        // the group as given (possibly subnormal)
+			b[q] = std::ldexp(a[q], -e2);       // exactly what the scaled reduction sees
+		}
+		std::vector<double> wa(static_cast<size_t>(n)), wb(static_cast<size_t>(n));
+		double*             ap[1] = { a.data() };
+		double*             wp[1] = { wa.data() };
+		const size_t        nn[1] = { size_t(n) };
+		std::vector<dmrgpp::GroupReduction> red;
+		if (!dmrgpp::group_eigenvalues(1, nn, ap, wp, red, 1)) {
+			std::printf("FAIL scaled group %d converge\n", e2);
+			return 1;
+		}
+		std::vector<double> d, e, h, b2;
+		dmrgpp::householder_tridiag(n, b.data(), d, e, h, b2);
+		wb = d;
+		dmrgpp::tridiag_values(n, wb.data(), e.data());
+		for (int i = 0; i < n; ++i)
+			if (wa[size_t(i)] != std::ldexp(wb[size_t(i)], e2)) {
+				std::printf("FAIL scaled group %d eigenvalue %d\n", e2, i);
+				return 1;
+			}
+		const int           kk = n / 2;
+		std::vector<double> z1(size_t(n) * size_t(kk)), z2(z1.size());
+		const double*       wk[1] = { wa.data() + (n - kk) };
+		double*             zp[1] = { z1.data() };
+		const size_t        kv[1] = { size_t(kk) };
+		dmrgpp::group_eigenvectors(1, nn, kv, red.data(), wk, zp, 2);
+		dmrgpp::tridiag_eigenvectors(n, d.data(), e.data(), wb.data() + (n - kk), kk, z2.data());
+		if (z1 != z2) {
+			std::printf("FAIL scaled group %d vectors\n", e2);
+			return 1;
 		}
 	}
 	std::printf("ok %.3e\n", worst);
