@@ -9,6 +9,7 @@
 // work, Kronecker terms) and the GPU name, so that sectors of similar shape
 // in later sweep steps or runs skip the timing.
 #include "dmrgpp_kron.h"
+#include "trace.h"
 #include "handle.h"
 #include "kron_fused.cuh"
 #include "kron_persistent.cuh"
@@ -119,6 +120,7 @@ int dmrgpp_kron_set_config(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 int dmrgpp_kron_autotune(dmrgpp_kron_handle h, const char* cache_path, int reps, int* cfg_out,
                          double* us_out)
 {
+	DMRGPP_TRACE("dmrgpp_kron_autotune");
 	using namespace dmrgpp;
 	if (!h)
 		return DMRGPP_INVALID_ARG;

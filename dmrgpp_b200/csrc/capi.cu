@@ -1,5 +1,6 @@
 // C ABI of the Kronecker H*x engine (include/dmrgpp_kron.h).
 #include "dmrgpp_kron.h"
+#include "trace.h"
 #include "kron_gemm.cuh"
 #include "kron_fused.cuh"
 #include "kron_persistent.cuh"
@@ -714,6 +715,7 @@ int dmrgpp_kron_plan_info_get(const dmrgpp_kron_desc* d, dmrgpp_kron_plan_info* 
 
 int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 {
+	DMRGPP_TRACE("dmrgpp_kron_create");
 	if (!out)
 		return fail(nullptr, DMRGPP_INVALID_ARG, "null output handle");
 	*out = nullptr;
@@ -753,6 +755,7 @@ int dmrgpp_kron_create(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 
 int dmrgpp_kron_create_crs(const dmrgpp_kron_crs_desc* d, dmrgpp_kron_handle* out)
 {
+	DMRGPP_TRACE("dmrgpp_kron_create_crs");
 	if (!out)
 		return fail(nullptr, DMRGPP_INVALID_ARG, "null output handle");
 	*out = nullptr;
@@ -791,6 +794,7 @@ int dmrgpp_kron_create_crs(const dmrgpp_kron_crs_desc* d, dmrgpp_kron_handle* ou
 
 int dmrgpp_kron_create_complex(const dmrgpp_kron_desc* d, dmrgpp_kron_handle* out)
 {
+	DMRGPP_TRACE("dmrgpp_kron_create_complex");
 	if (!out)
 		return fail(nullptr, DMRGPP_INVALID_ARG, "null output handle");
 	*out = nullptr;
@@ -890,6 +894,7 @@ int dmrgpp_kron_is_complex(dmrgpp_kron_handle h, int* is_complex)
 
 int dmrgpp_kron_create_group(const dmrgpp_kron_desc* descs, size_t nsectors, dmrgpp_kron_handle* out)
 {
+	DMRGPP_TRACE("dmrgpp_kron_create_group");
 	if (!out)
 		return fail(nullptr, DMRGPP_INVALID_ARG, "null output handle");
 	*out = nullptr;
@@ -1003,6 +1008,7 @@ int dmrgpp_kron_flops(dmrgpp_kron_handle h, double* f)
 
 int dmrgpp_kron_apply(dmrgpp_kron_handle h, const double* x, double* y, int on_device)
 {
+	DMRGPP_TRACE("dmrgpp_kron_apply");
 	if (!h)
 		return fail(nullptr, DMRGPP_INVALID_ARG, "null handle");
 	if (!x || !y)

@@ -15,6 +15,7 @@
 // formed on the device from the recorded QL rotations and Householder
 // reflectors, and the kept number follows computeKeptStates.
 #include "devmem.h"
+#include "trace.h"
 #include "dmrgpp_kron.h"
 #include "handle.h"
 #include "kron_gemm.cuh"
@@ -192,6 +193,7 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
                                        size_t m_min, double* eigenvalues, double* vectors, size_t* kept,
                                        size_t* kept_total, double* discarded)
 {
+	DMRGPP_TRACE("dmrgpp_density_truncate");
 	using namespace dmrgpp;
 	if (!d || !eigenvalues || !kept || !kept_total || !discarded)
 		return fail(DMRGPP_INVALID_ARG, "null argument");

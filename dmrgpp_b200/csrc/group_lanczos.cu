@@ -20,6 +20,7 @@
 // cross a sector boundary; every kernel walks chunks, so each block knows its
 // sector, and every sum runs in a fixed order (bitwise reproducible).
 #include "dmrgpp_kron.h"
+#include "trace.h"
 #include "devmem.h"
 #include "handle.h"
 #include "mlp.h"
@@ -702,6 +703,7 @@ extern "C" int dmrgpp_lanczos_lowest_group_masked(dmrgpp_kron_handle h, const dm
                                                   const double* init, int on_device, const int* mask,
                                                   double* energies, double* z, size_t* steps_taken)
 {
+	DMRGPP_TRACE("dmrgpp_lanczos_lowest_group_masked");
 	if (h && h->complex_sector)
 		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
@@ -991,6 +993,7 @@ extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int
                                           double inner_tolerance, double* energies, int* converged,
                                           dmrgpp_refine_stats* stats)
 {
+	DMRGPP_TRACE("dmrgpp_refine_lowest_group");
 	if (h && h->complex_sector)
 		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
@@ -1237,6 +1240,7 @@ extern "C" int dmrgpp_davidson_lowest_group(dmrgpp_kron_handle h, const dmrgpp_d
                                             const double* init, int on_device, double* energies,
                                             double* z, int* converged, dmrgpp_davidson_stats* stats)
 {
+	DMRGPP_TRACE("dmrgpp_davidson_lowest_group");
 	if (h && h->complex_sector)
 		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;

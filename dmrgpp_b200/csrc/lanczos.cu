@@ -18,6 +18,7 @@
 // Reductions are deterministic: per-block partials in fixed-size grids, the
 // last block to finish (arrival counter) sums them in block order.
 #include "dmrgpp_kron.h"
+#include "trace.h"
 #include "devmem.h"
 #include "handle.h"
 #include "tridiag.h"
@@ -644,6 +645,7 @@ int dmrgpp_tridiag_eigen(size_t n, const double* diag, const double* offdiag, do
 
 int dmrgpp_gather(const double* src, const int64_t* idx, double* dst, size_t n, void* stream)
 {
+	DMRGPP_TRACE("dmrgpp_gather");
 	if (n == 0)
 		return DMRGPP_OK;
 	if (!src || !idx || !dst)
@@ -656,6 +658,7 @@ int dmrgpp_gather(const double* src, const int64_t* idx, double* dst, size_t n, 
 
 int dmrgpp_scatter(const double* src, const int64_t* idx, double* dst, size_t n, void* stream)
 {
+	DMRGPP_TRACE("dmrgpp_scatter");
 	if (n == 0)
 		return DMRGPP_OK;
 	if (!src || !idx || !dst)
@@ -674,6 +677,7 @@ int dmrgpp_lanczos_lowest(dmrgpp_kron_handle          h,
                           double*                     z,
                           size_t*                     steps_taken)
 {
+	DMRGPP_TRACE("dmrgpp_lanczos_lowest");
 	if (h && h->complex_sector)
 		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
@@ -1104,6 +1108,7 @@ int dmrgpp_davidson_lowest(dmrgpp_kron_handle            h,
                            double*                       z,
                            dmrgpp_davidson_stats*        stats)
 {
+	DMRGPP_TRACE("dmrgpp_davidson_lowest");
 	if (h && h->complex_sector)
 		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
@@ -1587,6 +1592,7 @@ int dmrgpp_correction_solve(dmrgpp_kron_handle h, const double* u, double theta,
                             double* t, int max_iterations, double rel_tolerance, int* iterations,
                             double* rel_residual)
 {
+	DMRGPP_TRACE("dmrgpp_correction_solve");
 	if (h && h->complex_sector)
 		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;
@@ -1676,6 +1682,7 @@ int dmrgpp_refine_lowest(dmrgpp_kron_handle h, double* psi, int max_outer, doubl
                          int inner_iterations, double inner_tolerance, double* energy,
                          dmrgpp_refine_stats* stats)
 {
+	DMRGPP_TRACE("dmrgpp_refine_lowest");
 	if (h && h->complex_sector)
 		return dmrgpp::handle_fail(h, DMRGPP_NOT_SUPPORTED, "the device eigensolvers take real sectors");
 	using namespace dmrgpp;

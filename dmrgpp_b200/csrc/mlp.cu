@@ -28,6 +28,7 @@
 // The earlier CUDA-core inference (BF16 weights widened to FP32, h1 kept in
 // FP32) stays selectable (dmrgpp_mlp_set_inference).
 #include "devmem.h"
+#include "trace.h"
 #include "dmrgpp_kron.h"
 #include "mlp.h"
 #include "tc_common.cuh"
@@ -907,6 +908,7 @@ int dmrgpp_mlp_features(const double* diag, const double* r, double theta, doubl
 
 int dmrgpp_mlp_forward(dmrgpp_mlp_handle m, const float* x, int rows, float* out, void* stream)
 {
+	DMRGPP_TRACE("dmrgpp_mlp_forward");
 	using namespace dmrgpp;
 	if (!m || !x || rows < 1)
 		return DMRGPP_INVALID_ARG;
@@ -923,6 +925,7 @@ int dmrgpp_mlp_forward(dmrgpp_mlp_handle m, const float* x, int rows, float* out
 int dmrgpp_mlp_backward(dmrgpp_mlp_handle m, const float* x, const float* y, const float* weight,
                         double* loss, void* stream)
 {
+	DMRGPP_TRACE("dmrgpp_mlp_backward");
 	using namespace dmrgpp;
 	if (!m || !x || !y || m->last_rows < 1)
 		return DMRGPP_INVALID_ARG;
@@ -953,6 +956,7 @@ int dmrgpp_mlp_backward(dmrgpp_mlp_handle m, const float* x, const float* y, con
 
 int dmrgpp_mlp_adam_step(dmrgpp_mlp_handle m, float lr, void* stream)
 {
+	DMRGPP_TRACE("dmrgpp_mlp_adam_step");
 	using namespace dmrgpp;
 	if (!m)
 		return DMRGPP_INVALID_ARG;
@@ -968,6 +972,7 @@ int dmrgpp_mlp_adam_step(dmrgpp_mlp_handle m, float lr, void* stream)
 int dmrgpp_mlp_precondition(dmrgpp_mlp_handle m, const double* diag, const double* r, double theta,
                             double rnorm, double* t, size_t n, void* stream)
 {
+	DMRGPP_TRACE("dmrgpp_mlp_precondition");
 	return dmrgpp::mlp_precondition(m, diag, r, theta, rnorm, t, n, static_cast<cudaStream_t>(stream));
 }
 
@@ -975,6 +980,7 @@ int dmrgpp_mlp_precondition_group(dmrgpp_mlp_handle m, const double* diag, const
                                   const long long* sector_start, const double* theta,
                                   const double* rnorm, int nsectors, double* t, size_t n, void* stream)
 {
+	DMRGPP_TRACE("dmrgpp_mlp_precondition_group");
 	return dmrgpp::mlp_precondition_group(m, diag, r, sector_start, theta, rnorm, nsectors, t, n,
 	                                      static_cast<cudaStream_t>(stream));
 }

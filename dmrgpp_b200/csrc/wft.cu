@@ -2,6 +2,7 @@
 // dmrgpp_kron.h, plan in wft_plan.h): two grouped FP64 GEMM launches per
 // apply, on the FP64 tensor pipe (kron_gemm.cuh).
 #include "devmem.h"
+#include "trace.h"
 #include "dmrgpp_kron.h"
 #include "kron_gemm.cuh"
 #include "wft_plan.h"
@@ -101,6 +102,7 @@ extern "C" {
 
 int dmrgpp_wft_create(const dmrgpp_wft_desc* d, dmrgpp_wft_handle* out)
 {
+	DMRGPP_TRACE("dmrgpp_wft_create");
 	if (!out)
 		return wft_fail(nullptr, DMRGPP_INVALID_ARG, "null output handle");
 	*out = nullptr;
@@ -170,6 +172,7 @@ int dmrgpp_wft_create(const dmrgpp_wft_desc* d, dmrgpp_wft_handle* out)
 
 int dmrgpp_wft_apply(dmrgpp_wft_handle h, const double* x, double* y, int on_device)
 {
+	DMRGPP_TRACE("dmrgpp_wft_apply");
 	if (!h)
 		return wft_fail(nullptr, DMRGPP_INVALID_ARG, "null handle");
 	if (!x || !y)
