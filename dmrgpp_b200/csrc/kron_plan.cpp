@@ -750,24 +750,6 @@ void fill_upload_chunk(const UploadPlan& up, size_t c, size_t first, size_t last
 	}
 }
 
-void sector_diagonal(const KronPlan& plan, std::vector<double>& diag)
-{
-	diag.assign(size_t(plan.dim()), 0.0);
-	for (size_t t = 0; t < plan.triples.size(); ++t) {
-		const Triple& tr = plan.triples[t];
-		if (tr.i != tr.j)
-			continue;
-		const BlockRef& bl = plan.blocks[t];
-		const long long li = plan.l[tr.i], ri = plan.r[tr.i];
-		double*         d  = diag.data() + plan.xy_start[tr.i];
-		for (long long il = 0; il < li; ++il) {
-			const double a = bl.A[il + il * (long long)bl.ldA];
-			for (long long ir = 0; ir < ri; ++ir)
-				d[ir + il * ri] += a * bl.B[ir + ir * (long long)bl.ldB];
-		}
-	}
-}
-
 void split_tf32(double v, float* hi, float* lo)
 {
 	const float h = tf32_round(float(v));

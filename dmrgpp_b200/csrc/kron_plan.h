@@ -362,11 +362,6 @@ UploadPlan build_upload_plan(const KronPlan& plan, long long chunk_elems, long l
 // of the staged upload; jobs [first, last) of the chunk).
 void fill_upload_chunk(const UploadPlan& up, size_t c, size_t first, size_t last, double* buf);
 
-// Diagonal of the sector's H in patch order: element (iR, iL) of patch i is
-// sum_k A_k(i,i)(iL,iL) * B_k(i,i)(iR,iR) over the contributing diagonal
-// triples (the input of diagonal preconditioners); reads plan.blocks.
-void sector_diagonal(const KronPlan& plan, std::vector<double>& diag);
-
 // Splits v into a TF32 high part and a TF32 remainder (host side of the
 // operator packing; round to nearest, ties away from zero, like the
 // device conversion cvt.rna.tf32.f32).
