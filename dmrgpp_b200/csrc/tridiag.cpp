@@ -460,8 +460,9 @@ inline __attribute__((always_inline)) double hsum(const v4d& v) { return (v[0] +
 // PROD: then this step's product p += A h, from the lower triangle alone:
 // p[i] += A(i, j) h[j] (i >= j) and p[j] += A(i, j) h[i] (i > j).
 // Columns go in pairs that share the loads of hp, qp, h and p; the order of
-// every sum is fixed (no contraction into fused multiply-adds: -std=c++17
-// turns it off), so both instruction-set builds round alike.
+// every sum is fixed, and neither target (baseline x86-64, AVX2 without
+// FMA) has fused multiply-add instructions that GCC could contract the
+// products and sums into, so both instruction-set builds round alike.
 template <bool UPD, bool PROD>
 inline __attribute__((always_inline)) void pass_cols(int len, double* a, size_t ld, int c0, int c1, const double* hp,
                                                      const double* qp, const double* h, double* p)
