@@ -27,7 +27,7 @@ def checker(tmp_path_factory):
 
 @pytest.mark.parametrize("seed,np_,nop,maxs", [
     (1, 1, 1, 1), (2, 3, 2, 9), (3, 6, 3, 40), (4, 4, 2, 130), (5, 12, 5, 70),
-    (6, 2, 2, 200), (7, 20, 4, 20)])
+    (6, 2, 2, 200), (7, 20, 4, 20), (11, 40, 3, 3), (12, 2, 2, 300)])
 def test_persistent_items_loads_stores_and_result(checker, seed, np_, nop, maxs):
     out = subprocess.run([checker, str(seed), str(np_), str(nop), str(maxs)],
                          capture_output=True, text=True, timeout=300)
@@ -44,7 +44,8 @@ def group_checker(tmp_path_factory):
 
 
 @pytest.mark.parametrize("seed,nsec,maxp,maxk,maxs", [
-    (1, 1, 4, 3, 30), (2, 4, 5, 3, 30), (3, 7, 3, 4, 20), (4, 2, 8, 5, 60), (5, 12, 2, 2, 12)])
+    (1, 1, 4, 3, 30), (2, 4, 5, 3, 30), (3, 7, 3, 4, 20), (4, 2, 8, 5, 60), (5, 12, 2, 2, 12),
+    (23, 50, 1, 1, 1)])
 def test_group_items_stay_in_their_sector(group_checker, seed, nsec, maxp, maxk, maxs):
     """Sectors of a group launch are isolated: pass-2 segments depend only on
     their own sector's patches, and with any one sector's items skipped (as
