@@ -377,7 +377,7 @@ extern "C" int dmrgpp_density_truncate(const dmrgpp_density_desc* d, size_t m, d
 		gw[g] = eigenvalues + eoff[g];
 	}
 	std::vector<GroupReduction> ge;
-	const int                   hw = int(std::min(std::max(2u, std::thread::hardware_concurrency()), 32u));
+	const int                   hw = host_threads();
 	if (!group_eigenvalues(ng, d->group_size, ga.data(), gw.data(), ge, hw)) {
 		size_t g = 0;
 		while (g < ng && ge[g].ok)

@@ -18,18 +18,46 @@
 #include <thread>
 #include <cstddef>
 #include <cstdint>
+#include <cstdlib>
 #include <string>
 #include <memory>
 #include <utility>
 #include <vector>
 
+#include <sched.h>
+
 namespace dmrgpp {
 
-// f(0..n-1) on the host's cores (dynamic assignment; every f(i) writes its
-// own disjoint output, so the result does not depend on the thread count)
+// Host threads of the library's parallel host phases: DMRGPP_HOST_THREADS
+// when it is set (1 to 256), otherwise the CPUs this process may run on (its
+// affinity mask, so taskset, MPI binding and container CPU sets are
+// honoured), at most 32.  Read once per process.
+inline int host_threads()
+{
+	static const int n = [] {
+		if (const char* e = std::getenv("DMRGPP_HOST_THREADS")) {
+			const int v = std::atoi(e);
+			if (v >= 1)
+				return std::min(v, 256);
+		}
+		int       c = 0;
+		cpu_set_t set;
+		CPU_ZERO(&set);
+		if (sched_getaffinity(0, sizeof set, &set) == 0)
+			c = CPU_COUNT(&set);
+		if (c <= 0)
+			c = int(std::thread::hardware_concurrency());
+		return std::max(1, std::min(c, 32));
+	}();
+	return n;
+}
+
+// f(0..n-1) on host_threads() threads (dynamic assignment; every f(i)
+// writes its own disjoint output, so the result does not depend on the
+// thread count)
 template <class F> void parallel_for(size_t n, F f)
 {
-	size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 32);
+	size_t nt = size_t(host_threads());
 	nt        = std::min(nt, n);
 	if (nt < 2) {
 		for (size_t i = 0; i < n; ++i)

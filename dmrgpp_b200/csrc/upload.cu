@@ -295,7 +295,7 @@ int upload_operators(dmrgpp_kron_handle h, double* seconds_fill)
 	                            cudaMemcpyHostToDevice, h->stream)))
 		return cleanup(DMRGPP_CUDA_ERROR, std::string("upload jobs: ") + cudaGetErrorString(e));
 
-	const size_t helpers = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 32) - 1;
+	const size_t helpers = size_t(host_threads()) - 1;
 	Team         team(helpers);
 	double       fill_s = 0.0;
 	for (size_t c = 0; c < up.chunks(); ++c) {
