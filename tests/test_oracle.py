@@ -149,3 +149,43 @@ def test_reference_nonbatched_path_matches_restatement(oracle_built, threads):
         y = oracle_built.RefKronConn(prob).apply(x, threads=threads)
         ref = oracle_built.kron_apply(prob, x)
         assert np.abs(y - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.skipif(not os.path.isdir(oracle.REFERENCE_TREE) and
+                    not os.path.exists(oracle.REF_KC_SO), reason="reference harness not built")
+def test_reference_kron_methods_on_the_kronutil_test_grid(oracle_built):
+    """The grid of the reference's own KronUtil test (dmrg/KronUtil/test1.cpp:
+    A blocks of 1, 4, 7 rows and columns, B blocks of 1, 4, 7, 10 rows and
+    1, 4, 7 columns, each entry kept with probability 1 - threshold for
+    thresholds 0, 0.1, ..., 1.1), untransposed as the plugin path uses them:
+    a two-patch sector whose one term couples patch 1 into patch 0 with such
+    blocks, through the reference's den_kron_mult (which picks method 1, 2 or
+    3 from the blocks' nonzero counts; at threshold 1.1 a block is all zero
+    and the term drops out) against the restatement.  Every threshold pair,
+    three block shapes each."""
+    from dmrgpp_b200.superblock import KronProblem
+    rng = np.random.default_rng(7)
+    shapes = [(ra, ca, rb, cb) for ra in (1, 4, 7) for ca in (1, 4, 7)
+              for rb in (1, 4, 7, 10) for cb in (1, 4, 7)]
+    count = 0
+    for ia in range(12):
+        for ib in range(12):
+            for q in range(3):
+                ra, ca, rb, cb = shapes[(37 * (12 * ia + ib) + 11 * q) % len(shapes)]
+
+                def sparse(rows, cols, thr):
+                    m = rng.standard_normal((rows, cols))
+                    m[rng.random((rows, cols)) < thr] = 0.0
+                    return np.asfortranarray(m)
+
+                A = {(0, 1, 0): sparse(ra, ca, 0.1 * ia)}
+                B = {(0, 1, 0): sparse(rb, cb, 0.1 * ib)}
+                prob = KronProblem(np.array([ra, ca], dtype=np.int64), np.array([rb, cb], dtype=np.int64),
+                                   1, A, B, name="kronutil-grid")
+                x = rng.standard_normal(prob.dim)
+                y = oracle_built.RefKronConn(prob).apply(x, threads=1)
+                ref = oracle_built.kron_apply(prob, x)
+                assert np.abs(y - ref).max(initial=0.0) <= 1e-13 * max(1.0, np.abs(ref).max(initial=0.0)), \
+                    (ia, ib, ra, ca, rb, cb)
+                count += 1
+    assert count == 432
