@@ -482,6 +482,11 @@ int configure_schedule(dmrgpp_kron_handle h, int cfg, int items_per_cta)
 	if (tile != P.bm || P.tile1.size() + P.tile2.size() == 0)
 		build_tile_lists(P, tile, tile);
 	build_persistent_schedule(P, bk, grid, items_per_cta);
+	if (validation_requested()) { // debug mode: bounds of the work list before any launch
+		const std::string v = validate_persistent_schedule(P, tile);
+		if (!v.empty())
+			return fail(h, DMRGPP_INVALID_ARG, "schedule check: " + v);
+	}
 	h->cfg           = cfg;
 	h->grid          = grid;
 	h->tile          = tile;

@@ -7,6 +7,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -416,6 +417,97 @@ void build_persistent_schedule(KronPlan& plan, int bk, int grid, int items_per_c
 		if (w.seg_end > w.seg_begin)
 			w.seg0 = segs[size_t(w.seg_begin)];
 	}
+}
+
+bool validation_requested()
+{
+	static const bool on = [] {
+		const char* e = std::getenv("DMRGPP_VALIDATE");
+		return e && std::atoi(e) != 0;
+	}();
+	return on;
+}
+
+std::string validate_persistent_schedule(const KronPlan& plan, int tile)
+{
+	const long long dim = plan.dim(), ops = plan.op_elems, bx = plan.bx_elems;
+	auto            at  = [](const char* what, size_t q) { return std::string(what) + " (item " + std::to_string(q) + ")"; };
+	// [lo, hi] of rows [m0, m1) x k [0, K) of a column-major operand at off
+	auto range_ok = [](long long off, long long r0, long long r1, long long cols, long long ld, long long lo,
+	                   long long hi) {
+		if (r1 <= r0 || cols <= 0)
+			return true;
+		const long long first = off + r0, last = off + (r1 - 1) + (cols - 1) * ld;
+		return first >= lo && last < hi && ld >= 1;
+	};
+	if (plan.n1_items < 0 || size_t(plan.n1_items) > plan.items.size() || plan.n1_of_j.size() != plan.np)
+		return "item counts";
+	std::vector<long long> area(plan.np, 0);
+	std::vector<int>       n1(plan.np, 0);
+	std::vector<int>       slot_use(size_t(std::max<long long>(plan.partial_slots, 0)), 0);
+	for (size_t q = 0; q < plan.items.size(); ++q) {
+		const KronItem& w    = plan.items[q];
+		const bool      p1   = q < size_t(plan.n1_items);
+		const auto&     segs = p1 ? plan.seg1 : plan.pseg2;
+		if (p1 != (w.kind == 0) || w.seg_begin < 0 || w.seg_end < w.seg_begin || size_t(w.seg_end) > segs.size())
+			return at("kind or segment range", q);
+		if (w.seg_end - w.seg_begin > kMaxItemSegs)
+			return at("too many segments", q);
+		if (w.M < 0 || w.N < 0 || w.m0 < 0 || w.n0 < 0 || w.m0 >= std::max(w.M, 1) || w.n0 >= std::max(w.N, 1))
+			return at("tile origin", q);
+		const long long m1 = std::min<long long>(w.m0 + tile, w.M), n1c = std::min<long long>(w.n0 + tile, w.N);
+		const long long ncols = n1c - w.n0;
+		// the output tile
+		const long long out_lo = p1 ? 0 : 0, out_hi = p1 ? bx : dim;
+		if (ncols > 0 && m1 > w.m0
+		    && !range_ok(w.c_off + (long long)w.n0 * w.ldc, w.m0, m1, ncols, w.ldc, out_lo, out_hi))
+			return at(p1 ? "BX store out of range" : "y store out of range", q);
+		for (int e = w.seg_begin; e < w.seg_end; ++e) {
+			const GemmSeg& g = segs[size_t(e)];
+			if (g.dep < 0 || size_t(g.dep) >= plan.np || g.K < 0)
+				return at("segment dependency", q);
+			if (p1) {
+				// A: Bstack_j rows m, k < K in the operators; B: X_j k < K, columns n
+				if (!range_ok(g.a_off, w.m0, m1, g.K, g.lda, 0, ops))
+					return at("pass-1 A load out of the operators", q);
+				const long long xlo = plan.xy_start[size_t(g.dep)], xhi = plan.xy_start[size_t(g.dep) + 1];
+				if (g.K > 0 && ncols > 0 && !range_ok(g.b_off + (long long)w.n0 * g.ldb, 0, g.K, ncols, g.ldb, xlo, xhi))
+					return at("pass-1 x load out of X_j", q);
+			} else {
+				const long long blo = plan.bx_off[size_t(g.dep)];
+				const long long bhi = blo + plan.M[size_t(g.dep)] * plan.l[size_t(g.dep)];
+				if (!range_ok(g.a_off, w.m0, m1, g.K, g.lda, blo, bhi))
+					return at("pass-2 BX load outside its dependency", q);
+				if (g.K > 0 && ncols > 0 && !range_ok(g.b_off + (long long)w.n0 * g.ldb, 0, g.K, ncols, g.ldb, 0, ops))
+					return at("pass-2 A^T load out of the operators", q);
+			}
+		}
+		if (p1) {
+			if (w.producer < 0 || size_t(w.producer) >= plan.np || w.seg_end - w.seg_begin != 1
+			    || plan.seg1[size_t(w.seg_begin)].dep != w.producer)
+				return at("pass-1 producer", q);
+			const size_t j = size_t(w.producer);
+			if (w.c_off != plan.bx_off[j] || w.M != plan.M[j] || w.N != plan.l[j] || w.ldc != plan.M[j])
+				return at("pass-1 output is not BX_j", q);
+			area[j] += (m1 - w.m0) * ncols;
+			++n1[j];
+		} else if (w.kind == 2) {
+			if (w.nsplit < 2 || w.part < 0 || w.part >= w.nsplit || w.slot < 0
+			    || (long long)w.slot + w.nsplit > plan.partial_slots || w.tile < 0 || w.tile >= plan.n_split_tiles)
+				return at("split part", q);
+			if (slot_use[size_t(w.slot + w.part)]++)
+				return at("split slot used twice", q);
+		} else if (w.kind != 1) {
+			return at("item kind", q);
+		}
+	}
+	for (size_t j = 0; j < plan.np; ++j)
+		if (n1[j] != plan.n1_of_j[j] || area[j] != plan.M[j] * plan.l[j])
+			return "pass-1 tiles do not cover BX_" + std::to_string(j) + " exactly once";
+	for (size_t s = 0; s < slot_use.size(); ++s)
+		if (slot_use[s] != 1)
+			return "split slot " + std::to_string(s) + " unused";
+	return "";
 }
 
 void build_fused_schedule(KronPlan& plan, int bm, int bn, int cw, int cluster, int rounds,

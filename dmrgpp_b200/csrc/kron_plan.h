@@ -422,6 +422,20 @@ constexpr int kMaxItemSegs = 32;
 // k boundary) when there are fewer than items_per_cta tiles per CTA.
 void build_persistent_schedule(KronPlan& plan, int bk, int grid, int items_per_cta = 2);
 
+// Checks the persistent work list against the buffers before a launch (the
+// host-side bounds check of the debug mode, DMRGPP_VALIDATE=1): for every
+// item, with tile x tile output tiles, the first and last element of each
+// operand range (rows m0 .. min(m0 + tile, M) - 1, K, columns) lies inside
+// its buffer (packed operators, x, BX, y), a pass-2 segment reads inside the
+// BX of the patch it depends on, pass-1 items tile each BX_j exactly
+// (n1_of_j of them), split parts agree on their tile and use their own
+// slots, and no item holds more than kMaxItemSegs segments.  Returns "" or
+// the first violation.
+std::string validate_persistent_schedule(const KronPlan& plan, int tile);
+
+// DMRGPP_VALIDATE set to a nonzero number (read once per process).
+bool validation_requested();
+
 // Builds plan.fitems / funits for the fused launch: output tiles of bm rows
 // and bn columns (columns past bn repeat the first product per column tile),
 // units cw input columns wide, each tile's units cut into at most `cluster`

@@ -144,6 +144,9 @@ int main(int argc, char** argv)
 			for (int grid : grids) {
 				build_tile_lists(plan, tile, tile);
 				build_persistent_schedule(plan, bk, grid, 2);
+				const std::string verdict = validate_persistent_schedule(plan, tile);
+				if (!verdict.empty())
+					return fail(("the validator rejects a good group schedule: " + verdict).c_str());
 				const auto&      W = plan.items;
 				std::vector<int> sec(W.size());
 				for (size_t q = 0; q < W.size(); ++q) // as the group handle assigns them

@@ -11,7 +11,9 @@
 //     that patch's pass-1 items (the kernel waits on exactly those);
 //   * every BX and every Y element is written exactly once, split tiles
 //     through their partial slots summed in part order;
-//   * the result equals H*x computed directly from the caller's blocks.
+//   * the result equals H*x computed directly from the caller's blocks;
+//   * validate_persistent_schedule (the library's debug-mode check) accepts
+//     every schedule and rejects spoilt copies of one.
 // Usage: persistent_schedule_check seed npatches noperator max_size
 // Prints "ok <max relative error> <items>" or "FAIL <reason>" (exit code 1).
 #include "kron_plan.h"
@@ -121,6 +123,33 @@ int main(int argc, char** argv)
 				for (int ipc : ipcs) {
 					build_tile_lists(plan, tile, tile);
 					build_persistent_schedule(plan, bk, grid, ipc);
+					const std::string verdict = validate_persistent_schedule(plan, tile);
+					if (!verdict.empty())
+						return fail(("the validator rejects a good schedule: " + verdict).c_str());
+					if (tile == 32 && bk == 16 && grid == 592 && ipc == 4) { // and rejects broken ones
+						auto broken = [&](auto&& spoil) {
+							KronPlan bad = plan;
+							spoil(bad);
+							return !validate_persistent_schedule(bad, tile).empty();
+						};
+						if (plan.n1_items > 0 && !broken([&](KronPlan& b) { b.items[0].c_off += 1; }))
+							return fail("validator missed a moved pass-1 tile");
+						if (plan.n1_items > 0
+						    && !broken([&](KronPlan& b) { b.n1_of_j[size_t(b.items[0].producer)] += 1; }))
+							return fail("validator missed a wrong pass-1 count");
+						if (plan.items.size() > size_t(plan.n1_items)
+						    && plan.items[size_t(plan.n1_items)].seg_end > plan.items[size_t(plan.n1_items)].seg_begin
+						    && !broken([&](KronPlan& b) {
+							       b.pseg2[size_t(b.items[size_t(b.n1_items)].seg_begin)].a_off += b.bx_elems;
+						       }))
+							return fail("validator missed a BX load out of range");
+						for (size_t q = size_t(plan.n1_items); q < plan.items.size(); ++q)
+							if (plan.items[q].kind == 2) {
+								if (!broken([&](KronPlan& b) { b.items[q].part = (b.items[q].part + 1) % b.items[q].nsplit; }))
+									return fail("validator missed a reused split slot");
+								break;
+							}
+					}
 					const auto& W = plan.items;
 					items += W.size();
 					const double nan = std::numeric_limits<double>::quiet_NaN();
