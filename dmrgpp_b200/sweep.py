@@ -1,20 +1,18 @@
 """Sector eigensolves as they occur in one finite-sweep step, timed on the
 device: the plain FP64 method (Lanczos with full reorthogonalisation, the
-reference's PsimagLite::LanczosSolver configuration) against the
-mixed-precision Davidson with FP64 refinement and a learned (or diagonal)
-preconditioner.  Energies are compared per site and states by overlap."""
+reference's PsimagLite::LanczosSolver configuration) against FP64 Davidson
+and the mixed-precision solve (TF32x3 Lanczos, then the FP64 refinement),
+from a random and from a warm start, and the attribution of the mixed
+solve's gain to its scheme and its precision.  Energies are compared per
+site and states by overlap."""
 from __future__ import annotations
 
-import os
 import time
 from typing import Dict
 
 import numpy as np
 
 from . import plugin
-
-HERE = os.path.dirname(os.path.abspath(__file__))
-LADDER_WEIGHTS = os.path.join(HERE, "weights", "ladder_mlp.npz")
 
 
 def _timed(fn):
@@ -151,13 +149,6 @@ def sector_solves(prob, sites: int, mlp=None, seed: int = 7, lanczos_steps: int 
             preconditioner="learned" if mlp is not None else "jacobi", **compare(e_m, z_m))
     bg.close()
     return out
-
-
-def load_ladder_mlp():
-    from .mlp import MLPPreconditioner
-    if os.path.exists(LADDER_WEIGHTS):
-        return MLPPreconditioner.load(LADDER_WEIGHTS)
-    return None
 
 
 def step_attribution(prob, sites: int, repeats: int = 5, seed: int = 7,
