@@ -102,9 +102,10 @@ k_g_finish(const double* __restrict__ partial, const int* __restrict__ seg_chunk
 }
 
 // y = x * f(scal[sector]): mode 0 f = 1/sqrt(v) (v a squared norm), mode 1
-// f = 1/v when v > 0 (else y = x); active sectors only
+// f = 1/v when v > 0 (else y = x); active sectors only.  y may be x (each
+// element is read and then written by one thread), so they are not restrict.
 __global__ void __launch_bounds__(kThreads)
-k_g_scale(const double* __restrict__ x, double* __restrict__ y, const double* __restrict__ scal,
+k_g_scale(const double* x, double* y, const double* __restrict__ scal,
           int mode, const Chunk* __restrict__ chunks, int nch, const int* __restrict__ active)
 {
 	for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
@@ -1157,7 +1158,8 @@ extern "C" int dmrgpp_refine_lowest_group(dmrgpp_kron_handle h, double* psi, int
 			k_g_pcg_setup<<<grid, kThreads, 0, st>>>(psi, h->d_diag, theta, wv, w->chunks, nch, cg, w->rpart);
 			k_g_finish<<<S, kThreads, 0, st>>>(w->rpart, w->seg_chunk, cg, uw, 0);
 			pcg_sums();
-			k_g_pcg_direction<<<grid, kThreads, 0, st>>>(pv, res, h->d_diag, theta, wv, uw, sums, S, rho[0],
+			// first = 1: rho is not read, the other half of its double buffer stands in
+			k_g_pcg_direction<<<grid, kThreads, 0, st>>>(pv, res, h->d_diag, theta, wv, uw, sums, S, rho[1],
 			                                             rho[0], 1, w->chunks, nch, w->seg_chunk, cg);
 		}
 		int cur = 0, inner = 0;
