@@ -451,6 +451,11 @@ int configure_fused(dmrgpp_kron_handle h, int fcfg, int parts_per_sm)
 	}
 	build_fused_schedule(P, s.bm, s.bn, s.cw, s.cluster, parts_per_sm, h->fused_clusters * s.cluster,
 	                     sector_of_patch.empty() ? nullptr : &sector_of_patch);
+	if (validation_requested()) { // debug mode: bounds of the work list before any launch
+		const std::string v = validate_fused_schedule(P, s.bm, s.bn, s.cluster);
+		if (!v.empty())
+			return fail(h, DMRGPP_INVALID_ARG, "schedule check: " + v);
+	}
 	if (P.fitems.size() > size_t(INT_MAX) || P.funits.size() > size_t(INT_MAX))
 		return fail(h, DMRGPP_INVALID_ARG, "sector too large for the fused form");
 	const size_t ib = P.fitems.size() * sizeof(FusedItem), ub = P.funits.size() * sizeof(FusedUnit);

@@ -510,6 +510,46 @@ std::string validate_persistent_schedule(const KronPlan& plan, int tile)
 	return "";
 }
 
+std::string validate_fused_schedule(const KronPlan& plan, int bm, int bn, int cluster)
+{
+	const long long dim = plan.dim(), ops = plan.op_elems;
+	const auto&     I   = plan.fitems;
+	const auto&     U   = plan.funits;
+	auto at = [](const char* what, size_t q) { return std::string(what) + " (item " + std::to_string(q) + ")"; };
+	auto in = [](long long first, long long last, long long hi) { return first >= 0 && last >= first && last < hi; };
+	if (cluster < 1 || I.size() % size_t(cluster) != 0)
+		return "items are not whole clusters";
+	for (size_t q = 0; q < I.size(); ++q) {
+		const FusedItem& it = I[q];
+		if (it.nparts == 0)
+			continue;
+		const int rank = int(q % size_t(cluster));
+		if (it.nparts < 0 || it.part < 0 || it.part >= it.nparts || it.rank0 < 0 || it.rank0 + it.nparts > cluster
+		    || it.rank0 + it.part != rank)
+			return at("part placement", q);
+		if (it.u_begin < 0 || it.u_end < it.u_begin || size_t(it.u_end) > U.size())
+			return at("unit range", q);
+		if (it.M < 1 || it.N < 1 || it.m0 < 0 || it.n0 < 0 || it.m0 >= it.M || it.n0 >= it.N)
+			return at("tile origin", q);
+		const long long Mt = std::min<long long>(bm, it.M - it.m0), Nt = std::min<long long>(bn, it.N - it.n0);
+		if (!in(it.y_off + (long long)it.n0 * it.M + it.m0, it.y_off + (long long)(it.n0 + Nt - 1) * it.M + it.m0 + Mt - 1,
+		        dim))
+			return at("y tile out of range", q);
+		for (int u = it.u_begin; u < it.u_end; ++u) {
+			const FusedUnit& d = U[size_t(u)];
+			if (d.rj < 1 || d.cw < 1 || d.lj < d.cw || d.ldb < 1)
+				return at("unit shape", q);
+			if (!in(d.b_off + it.m0, d.b_off + (long long)(d.rj - 1) * d.ldb + it.m0 + Mt - 1, ops))
+				return at("B load out of the operators", q);
+			if (!in(d.x_off, d.x_off + (long long)(d.cw - 1) * d.rj + d.rj - 1, dim))
+				return at("x load out of range", q);
+			if (!in(d.at_off + (long long)it.n0 * d.lj, d.at_off + (long long)(it.n0 + Nt - 1) * d.lj + d.cw - 1, ops))
+				return at("A^T load out of the operators", q);
+		}
+	}
+	return "";
+}
+
 void build_fused_schedule(KronPlan& plan, int bm, int bn, int cw, int cluster, int rounds,
                           int ctas, const std::vector<int>* sector_of_patch)
 {

@@ -433,6 +433,13 @@ void build_persistent_schedule(KronPlan& plan, int bk, int grid, int items_per_c
 // the first violation.
 std::string validate_persistent_schedule(const KronPlan& plan, int tile);
 
+// The same check for the fused work list (bm x bn output tiles, clusters of
+// `cluster` CTAs): every non-empty item sits at rank rank0 + part of its
+// cluster with rank0 + nparts <= cluster, its units are in range, and the
+// first and last element of each unit's B, x and A^T ranges and of the
+// item's Y tile lie inside their buffers.  Returns "" or the first violation.
+std::string validate_fused_schedule(const KronPlan& plan, int bm, int bn, int cluster);
+
 // DMRGPP_VALIDATE set to a nonzero number (read once per process).
 bool validation_requested();
 

@@ -11,7 +11,9 @@
 //     lies inside its block of the packed operators or of x, and every store
 //     inside Y_i;
 //   * the per-part products summed in part order (the cluster reduction)
-//     reproduce H*x computed directly from the caller's blocks.
+//     reproduce H*x computed directly from the caller's blocks;
+//   * validate_fused_schedule (the library's debug-mode check) accepts every
+//     schedule and rejects spoilt copies.
 // Usage: fused_schedule_check seed npatches noperator max_size
 // Prints "ok <max relative error> <items>" or "FAIL <reason>" (exit code 1).
 #include "kron_plan.h"
@@ -120,6 +122,19 @@ int main(int argc, char** argv)
 	size_t      items = 0;
 	for (const Shape& s : shapes) {
 		build_fused_schedule(plan, s.bm, s.bn, s.cw, s.cluster, s.parts_per_sm, s.sms);
+		const std::string verdict = validate_fused_schedule(plan, s.bm, s.bn, s.cluster);
+		if (!verdict.empty())
+			return fail(("the validator rejects a good schedule: " + verdict).c_str());
+		if (!plan.funits.empty()) { // and rejects spoilt copies
+			KronPlan bad = plan;
+			bad.funits.back().x_off += dim;
+			if (validate_fused_schedule(bad, s.bm, s.bn, s.cluster).empty())
+				return fail("validator missed an x load out of range");
+			bad = plan;
+			bad.funits.front().at_off += plan.op_elems;
+			if (validate_fused_schedule(bad, s.bm, s.bn, s.cluster).empty())
+				return fail("validator missed an A^T load out of range");
+		}
 		const auto& I = plan.fitems;
 		const auto& U = plan.funits;
 		items += I.size();
