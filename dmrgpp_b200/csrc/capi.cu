@@ -296,6 +296,13 @@ void mixed_host_plan(dmrgpp_kron_handle h, int sms, MixedHost& out)
 	out.msg = build_mixed_plan(h->plan, bn, nullptr, nullptr, &out.xmap, sms);
 	if (!out.msg.empty())
 		return;
+	if (validation_requested()) { // debug mode: bounds of the layout before any launch
+		const std::string v = validate_mixed_plan(h->plan);
+		if (!v.empty()) {
+			out.msg = "schedule check: " + v;
+			return;
+		}
+	}
 	MixedPlan& mp = h->plan.mixed;
 	out.grid1     = balance_tiles(mp.tile1, mp.seg1, sms, out.starts1);
 	out.grid2     = balance_tiles(mp.tile2, mp.seg2, sms, out.starts2);

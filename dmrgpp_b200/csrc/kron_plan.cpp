@@ -550,6 +550,93 @@ std::string validate_fused_schedule(const KronPlan& plan, int bm, int bn, int cl
 	return "";
 }
 
+std::string validate_mixed_plan(const KronPlan& plan)
+{
+	const MixedPlan& mp = plan.mixed;
+	const long long  D  = plan.dim();
+	const int        BM = mp.bm, BN = mp.bn;
+	if (mp.ops_elems % 32 || mp.xs_elems % 32 || mp.bxs_elems % 32)
+		return "an operand buffer is not a whole number of 32-float rows";
+	std::map<int, std::vector<int>> parts; // split tile -> its parts seen
+	std::map<int, int>              nsplit;
+	auto pass = [&](const std::vector<GemmSeg>& segs, const std::vector<GemmTile>& tiles, long long arows,
+	                long long brows, bool pass1) -> std::string {
+		const char* name = pass1 ? "pass 1" : "pass 2";
+		for (size_t q = 0; q < tiles.size(); ++q) {
+			const GemmTile& t   = tiles[q];
+			auto            bad = [&](const char* what) {
+                return std::string(name) + ": " + what + " (tile " + std::to_string(q) + ")";
+			};
+			if (t.seg_begin < 0 || t.seg_end < t.seg_begin || size_t(t.seg_end) > segs.size())
+				return bad("segment range");
+			if (t.M < 1 || t.N < 1 || t.m0 < 0 || t.n0 < 0 || t.m0 >= t.M || t.n0 >= t.N)
+				return bad("tile origin");
+			const int vm = std::min(BM, t.M - t.m0), vn = std::min(BN, t.N - t.n0);
+			for (int e = t.seg_begin; e < t.seg_end; ++e) {
+				const GemmSeg& g = segs[size_t(e)];
+				if (g.K < 0 || g.K % 32 != 0 || g.lda <= 0 || g.ldb <= 0 || g.lda % 8 != 0 || g.ldb % 8 != 0)
+					return bad("segment fields");
+				if (t.m0 + vm > g.lda || t.n0 + vn > g.ldb)
+					return bad("valid rows past the matrix");
+				if (g.K == 0)
+					continue;
+				const long long c1 = g.K / 32 - 1;
+				const long long ya0 = g.a_off + t.m0, ya1 = ya0 + c1 * g.lda;
+				const long long yb0 = g.b_off + t.n0, yb1 = yb0 + c1 * g.ldb;
+				if (ya0 < 0 || yb0 < 0 || ya1 >= arows || yb1 >= brows || ya1 > INT_MAX || yb1 > INT_MAX)
+					return bad("a tiled load starts outside its buffer");
+			}
+			const long long last_c0 = t.n0 + 32LL * ((vn - 1) / 32); // first column of the last 32-column group
+			if (pass1) {
+				if (t.c_off < 0 || t.c_off % 32 != 0)
+					return bad("BX matrix not on a 32-float row");
+				int qmax = -1; // the last full 32-row group of the tile
+				for (int g = 0; g < 4; ++g)
+					if (t.m0 + 32 * g + 32 <= t.M && 32 * g < BM)
+						qmax = g;
+				if (qmax >= 0) {
+					const long long R = t.c_off / 32 + (last_c0 >> 5) * t.ldc + t.m0 + 32 * qmax;
+					if (R < 0 || R > INT_MAX || (R + 32) * 32 > mp.bxs_elems)
+						return bad("staged BX store outside the buffer");
+				}
+				const long long o = t.c_off + (last_c0 >> 5) * (long long)t.ldc * 32 + (long long)(t.m0 + vm - 1) * 32 + 31;
+				if (o >= mp.bxs_elems)
+					return bad("BX store out of bounds");
+			} else {
+				const long long o0 = t.c_off + (long long)t.n0 * t.ldc + t.m0;
+				const long long o1 = t.c_off + (long long)(t.n0 + vn - 1) * t.ldc + t.m0 + vm - 1;
+				if (o0 < 0 || o1 >= D)
+					return bad("y store out of bounds");
+				if (t.nsplit >= 2) {
+					if (t.slot < 0 || t.split_part < 0 || t.split_part >= t.nsplit
+					    || (long long)t.slot + t.nsplit > mp.split_slots || t.split_tile < 0
+					    || t.split_tile >= mp.n_split_tiles)
+						return bad("split slot out of range");
+					parts[t.split_tile].push_back(t.split_part);
+					nsplit[t.split_tile] = t.nsplit;
+				}
+			}
+		}
+		return "";
+	};
+	std::string v = pass(mp.seg1, mp.tile1, mp.ops_elems / 32, mp.xs_elems / 32, true);
+	if (v.empty())
+		v = pass(mp.seg2, mp.tile2, mp.bxs_elems / 32, mp.ops_elems / 32, false);
+	if (!v.empty())
+		return v;
+	if (int(parts.size()) != mp.n_split_tiles)
+		return "split tiles without parts";
+	for (auto& kv : parts) {
+		std::sort(kv.second.begin(), kv.second.end());
+		for (int p = 0; p < int(kv.second.size()); ++p)
+			if (kv.second[size_t(p)] != p)
+				return "split tile " + std::to_string(kv.first) + " with a missing or repeated part";
+		if (int(kv.second.size()) != nsplit[kv.first])
+			return "split tile " + std::to_string(kv.first) + " missing parts";
+	}
+	return "";
+}
+
 void build_fused_schedule(KronPlan& plan, int bm, int bn, int cw, int cluster, int rounds,
                           int ctas, const std::vector<int>* sector_of_patch)
 {

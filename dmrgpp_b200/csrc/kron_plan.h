@@ -440,6 +440,16 @@ std::string validate_persistent_schedule(const KronPlan& plan, int tile);
 // item's Y tile lie inside their buffers.  Returns "" or the first violation.
 std::string validate_fused_schedule(const KronPlan& plan, int bm, int bn, int cluster);
 
+// The same check for the TF32x3 form (plan.mixed): every operand buffer a
+// whole number of 32-float rows; for every tile and segment the K chunks a
+// multiple of 32 and the leading dimensions of 8, the tile's valid rows
+// inside its matrix, the start row of every tiled load inside its buffer;
+// pass-1 outputs on 32-float rows with their staged stores and element
+// stores inside the BX buffer; pass-2 stores inside y; split parts with
+// slots in range and every part of a split tile present.  Returns "" or the
+// first violation.
+std::string validate_mixed_plan(const KronPlan& plan);
+
 // DMRGPP_VALIDATE set to a nonzero number (read once per process).
 bool validation_requested();
 

@@ -18,7 +18,9 @@
 //     exceeds their rows;
 //   * the epilogue's stores stay inside their buffers;
 //   * pass 1 + pass 2 computed from these buffers (hi*hi + hi*lo + lo*hi in
-//     double) reproduce the FP64 H*x.
+//     double) reproduce the FP64 H*x;
+//   * validate_mixed_plan (the library's debug-mode check) accepts the plan
+//     and rejects spoilt copies.
 // Usage: mixed_layout_check seed npatches noperator max_size bn
 // Prints "ok <max relative error>" or "FAIL <reason>" (exit code 1).
 #include "kron_plan.h"
@@ -107,6 +109,22 @@ int main(int argc, char** argv)
 	msg = build_mixed_plan(plan, bn, &ohi, &olo, &xmap);
 	if (!msg.empty())
 		return fail(msg.c_str());
+	// the library's debug-mode check accepts the plan and rejects spoilt copies
+	msg = validate_mixed_plan(plan);
+	if (!msg.empty())
+		return fail(("the validator rejects a good plan: " + msg).c_str());
+	if (!plan.mixed.seg2.empty()) {
+		KronPlan bad = plan;
+		bad.mixed.seg2.back().a_off += bad.mixed.bxs_elems / 32;
+		if (validate_mixed_plan(bad).empty())
+			return fail("validator missed a load outside its buffer");
+	}
+	if (!plan.mixed.tile2.empty()) {
+		KronPlan bad = plan;
+		bad.mixed.tile2.back().c_off += plan.dim();
+		if (validate_mixed_plan(bad).empty())
+			return fail("validator missed a y store out of bounds");
+	}
 	// per-CTA runs (balance_tiles): a permutation of the tiles, runs cover all
 	for (int pass_no = 0; pass_no < 2; ++pass_no) {
 		std::vector<GemmTile>&       tl   = pass_no ? plan.mixed.tile2 : plan.mixed.tile1;
